@@ -1,0 +1,183 @@
+/*
+ * ucb.h — C ABI of the B200 engine for the per-cell integration hot path of U-CUDA.
+ *
+ * It replaces, for that path, the reference's C++ facade `class ParametricEngine`
+ * (parametric_engine.h:844-889) and its request/result structs. Plain C types only:
+ * pointers, sizes, doubles; no C++ or torch types cross this boundary.
+ *
+ * Conventions shared by every run_* entry point (the reference's error behaviour,
+ * parametric_engine.cpp:2589-2600 and the *_CHECK macros at :2766-2786):
+ *   - nothing throws across the ABI; a failure sets result->ok = 0 and a message in
+ *     result->error, and the call returns a non-zero UCB_E* code;
+ *   - a set *cancel (polled between launches) ends the call with result->cancelled = 1;
+ *   - *progress (if non-NULL) is written with a value in [0, 1];
+ *   - output arrays are allocated by the caller with the sizes documented per call;
+ *   - one engine may be driven from one host thread at a time (the reference's
+ *     session layer enforces the same, analysis_session.cpp:918-966).
+ *
+ * The C++ header include/ucb_parametric_engine.hpp wraps these calls behind the
+ * reference's exact ParametricEngine signatures.
+ */
+#ifndef UCB_H_
+#define UCB_H_
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define UCB_ABI_VERSION 1
+
+#if defined(__GNUC__)
+#define UCB_API __attribute__((visibility("default")))
+#else
+#define UCB_API
+#endif
+
+/* Return codes */
+#define UCB_OK 0
+#define UCB_E_INVALID 1   /* request validation failed (message in result->error) */
+#define UCB_E_COMPILE 2   /* the step body or a kernel did not compile */
+#define UCB_E_CUDA 3      /* CUDA runtime/driver error */
+#define UCB_E_CANCELLED 4 /* *cancel was set */
+#define UCB_E_NOGPU 5     /* no CUDA device / driver */
+
+/* Arithmetic of the integrator.
+ *   UCB_PREC_F64: plain form, FP64 throughout (the oracle precision).
+ *   UCB_PREC_F32: FP32 state; tangent-vector norms, log sums and step control in FP64. */
+#define UCB_PREC_F64 0
+#define UCB_PREC_F32 1
+
+/* How the KRS step body is used.
+ *   UCB_MODE_NATIVE: the right-hand side is recognised in the body (codegen RK4 template)
+ *     and integrated by the engine's FMA-ordered RK4; bodies that are not a recognised
+ *     template fall back to UCB_MODE_EXACT automatically.
+ *   UCB_MODE_EXACT: the body is spliced verbatim (as the reference does) and compiled
+ *     without FMA contraction: bit-identical trajectories to the krs_cpu CPU path. */
+#define UCB_MODE_NATIVE 0
+#define UCB_MODE_EXACT 1
+
+/* LLE algorithm: shadow trajectory at distance eps (the reference's Benettin method),
+ * or the tangent-linear vector (needs a recognised right-hand side). AUTO picks the
+ * shadow for FP64 and the tangent vector for FP32. */
+#define UCB_LLE_AUTO 0
+#define UCB_LLE_SHADOW 1
+#define UCB_LLE_TANGENT 2
+
+typedef struct ucb_options {
+    int32_t precision;   /* UCB_PREC_* */
+    int32_t mode;        /* UCB_MODE_* */
+    int32_t lle_method;  /* UCB_LLE_* */
+    int32_t nominal_steps; /* 0: reference step counts (extra step after every loop call,
+                              cudaLibrary.cu:863-866); 1: nominal counts */
+    int32_t block_threads; /* 0: autotuned; else threads per block (multiple of 32) */
+    int32_t reserved[3];
+} ucb_options;
+
+typedef struct ucb_engine ucb_engine;
+
+/* Creates an engine bound to CUDA device `device` (the reference always uses device 0,
+ * parametric_engine.cpp:1490). Creation needs no GPU: the device is initialised by the
+ * first run_* call, which reports UCB_E_NOGPU when it cannot be used. */
+UCB_API ucb_engine* ucb_create(int device);
+UCB_API void ucb_destroy(ucb_engine* e);
+UCB_API const char* ucb_last_error(const ucb_engine* e);
+UCB_API int ucb_abi_version(void);
+/* Number of kernels this engine has launched so far (all entry points). */
+UCB_API long long ucb_kernel_launches(const ucb_engine* e);
+/* Clears the compiled-module cache (the reference's release_*_module()). */
+UCB_API void ucb_clear_cache(ucb_engine* e);
+UCB_API void ucb_default_options(ucb_options* o);
+
+/* ------------------------------------------------------------------------------------
+ * LLE 2D — replaces ParametricEngine::run_lle_2d(const LLE2DRequest&) -> LLE2DResult
+ * (parametric_engine.h:411-482, :871; implementation parametric_engine.cpp:2587-2965).
+ * Field meaning is the reference's: param_index* are 1-based indices into base_values
+ * (a[0] reserved), var_sweep_index* are 0-based into initial_conditions.
+ * ---------------------------------------------------------------------------------- */
+typedef struct ucb_lle2d_request {
+    const char* krs_body;
+    int32_t amount_of_x;
+    const double* initial_conditions; /* amount_of_x */
+    const double* base_values;        /* n_values (<= 64) */
+    int32_t n_values;
+    int32_t sweep_over_var, sweep_over_var_2;
+    int32_t sweep_over_h, sweep_over_h_2;
+    int32_t log_scale, log_scale_2;
+    int32_t param_index, var_sweep_index, param_index_2, var_sweep_index_2;
+    double param_lo, param_hi, param_lo_2, param_hi_2;
+    int32_t n_pts;
+    double h, transient_time, t_max, NT, eps, max_value;
+    const char* csv_output_path;      /* NULL or "" = no CSV */
+    const volatile int32_t* cancel;   /* NULL = no cancellation */
+    volatile float* progress;         /* NULL = no progress reporting */
+    ucb_options opt;
+} ucb_lle2d_request;
+
+typedef struct ucb_lle2d_result {
+    /* caller-allocated outputs, n_pts * n_pts each, row-major values[iy*n_pts + ix] */
+    double* values;   /* lambda; the reference's sentinel 999 is kept (flag -1) */
+    int32_t* flags;   /* 1 ok, -1 diverged */
+    /* filled by the call */
+    int32_t ok, cancelled, n_pts;
+    double param_lo, param_hi, param_lo_2, param_hi_2;
+    double min_val, max_val;          /* over cells with flag >= 0 and finite value */
+    double kernel_ms;                 /* device time of the integrator kernel(s) */
+    long long steps;                  /* step-function evaluations performed (work count) */
+    double flops;                     /* algorithmic FLOPs of those steps (0 if unknown) */
+    char error[1024];
+} ucb_lle2d_result;
+
+UCB_API int ucb_run_lle2d(ucb_engine* e, const ucb_lle2d_request* req, ucb_lle2d_result* res);
+
+/* Device-resident form of ucb_run_lle2d for callers that keep outputs in HBM: enqueues
+ * the work on `stream` (a cudaStream_t, NULL = default stream) and returns without
+ * synchronising. d_values / d_flags are device pointers of n_pts*n_pts elements. No
+ * CSV, no min/max; res->error/ok report validation and launch errors only. */
+UCB_API int ucb_lle2d_device(ucb_engine* e, const ucb_lle2d_request* req, double* d_values, int32_t* d_flags,
+                     void* stream, ucb_lle2d_result* res);
+
+/* Trajectory parity aid: integrates every cell of the request's grid (same sweep
+ * mapping, same step function and precision as ucb_run_lle2d) for n_steps plain steps
+ * from its initial condition — no transient, no divergence checks, no extra step — and
+ * writes the final states to out_states[cell * amount_of_x + i] (kernel cell order).
+ * The reference has no counterpart; it checks its kernels against its CPU twins instead
+ * (parametric_engine.cpp:593-616). Error text: ucb_last_error(). */
+UCB_API int ucb_lle2d_states(ucb_engine* e, const ucb_lle2d_request* req, long long n_steps, double* out_states);
+
+/* Measures the FMA throughput of the FP64 (precision = UCB_PREC_F64) or FP32 pipe of the
+ * current device in TFLOP/s (2 FLOPs per FMA): the roofline denominator of the integrator
+ * kernels. No reference counterpart (the reference publishes no measurements). */
+UCB_API int ucb_measure_fma_peak(int precision, double* tflops);
+
+/* ------------------------------------------------------------------------------------
+ * Text front-end: replaces parse_system_from_latex (sysparse.hpp, sysparse.cpp:287) +
+ * codegen_scheme (codegen.hpp, codegen.cpp:951). Parses a multi-line LaTeX / plain system
+ * with a comma-separated alphabet (parameter order: alphabet, or first appearance when
+ * order_as_in_system != 0; func_defs: optional "h(x) = ..." lines) and writes the step
+ * body of `scheme` to out; vars_out / params_out (optional) receive comma-separated names
+ * (variables map to X[i], parameters to a[1 + j]). On error returns UCB_E_INVALID and the
+ * message in out.
+ * ---------------------------------------------------------------------------------- */
+#define UCB_SCHEME_EULER 0
+#define UCB_SCHEME_EULER_CROMER 1
+#define UCB_SCHEME_MIDPOINT 2
+#define UCB_SCHEME_RK4 3
+UCB_API int ucb_codegen(const char* text, const char* alphabet, int order_as_in_system, const char* func_defs,
+                        int scheme, char* out, int out_len, char* vars_out, int vars_len, char* params_out,
+                        int params_len);
+
+/* Compiles the kernel a ucb_run_lle2d call with this request would use into the on-disk
+ * CUBIN cache (<library dir>/_cache or $UCB_CUBIN_CACHE) without touching a GPU. The
+ * reference's equivalent is compile_lle_2d_if_needed (parametric_engine.cpp:2487-2572),
+ * which only has an in-memory PTX cache. err_out receives a compiler log or a note on
+ * the form chosen. */
+UCB_API int ucb_precompile_lle2d(const ucb_lle2d_request* req, char* err_out, int err_len);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* UCB_H_ */

@@ -1,0 +1,679 @@
+// ============================================================================
+// ORACLE — test infrastructure, never part of the product.
+//
+// CPU restatement of the reference's per-cell hot path, used ONLY as the checker
+// in tests/, by __graft_entry__.smoke(), and as the timed CPU baseline in bench.py.
+// The product (u-cuda_b200/) never links, loads or calls anything in oracle/.
+//
+// What it restates (reference paths are relative to the U-CUDA project):
+//   * krs_cpu.cpp:293-316  make_source  — prelude around the KRS step body; the body is
+//     compiled natively (g++ -O2 -ffp-contract=off, dlopen) instead of cl.exe + LoadLibrary
+//     (krs_cpu.cpp:405-478).
+//   * cudaLibrary.cu:782-895  loopCalculateDiscreteModel_int (CPU twin
+//     parametric_engine.cpp:59-101): n steps, optional recording, divergence check
+//     every CHECK_INTERVAL=100 iterations, one extra preScaller step, fixed-point test.
+//   * cudaLibrary.cu:1344-1361 getValueByIdx, :1381-1396 getValueByIdx_log.
+//   * lle2d.template.cu:45-56 RNG stub (splitmix64 init + LCG uniform), identical to
+//     the CPU twin at parametric_engine.cpp:196-209.
+//   * cudaLibrary.cu:2486-2693 LLEKernelCUDA — per-cell Benettin LLE with a shadow
+//     trajectory (GPU semantics: (1/eps)*(x-y), floor 1e-14, result/tMax).
+//   * cudaLibrary.cu:2832-2874 projectionOperator / gramSchmidtProcess (classical GS)
+//     and :2878-3073 LSKernelCUDA — full spectrum with N shadow probes.
+//   * cudaLibrary.cu:944-1077 calculateDiscreteModelCUDA + :1503-1633 peakFinder —
+//     bifurcation (transient, recorded series, parabolic peaks, first peak dropped,
+//     inter-peak intervals, cap 2500) with the host sizing of parametric_engine.cpp:1816.
+//   * parametric_engine.cpp:2587-2965 run_lle_2d host mapping (par_or_var, swap_xy,
+//     999 sentinel -> flag -1), :3430-3786 run_ls_2d (plane-major values).
+// New-semantics checkers (no reference counterpart, parity unpinned against it):
+//   * stroboscopic basin labelling, DP5(4) + modified Gram-Schmidt spectrum and the
+//     tangent-linear LLE, restated from their published algorithms (see the functions).
+//
+// numb is a template parameter: double (the FP64 oracle) or float (the reference's
+// shipped configCUDA.h:4 setting).
+// ============================================================================
+#include <dlfcn.h>
+#include <omp.h>
+#include <unistd.h>
+#include <sys/stat.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdint>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <fstream>
+#include <mutex>
+#include <sstream>
+#include <string>
+#include <vector>
+
+namespace {
+
+constexpr int kCheckInterval = 100;             // configCUDA.h:12
+constexpr double kEpsFixedPoint = 1e-8;         // configCUDA.h eps_fixed_point
+constexpr double kEpsPeakDelta = 1e-14;         // configCUDA.h eps_peak_delta
+constexpr double kPeakThreshold = -1e25;        // configCUDA.h peak_threshold
+constexpr int kMaxAmountOfPeaks = 2500;         // configCUDA.h max_amount_of_peaks
+constexpr double kPi = 3.1415926535897932384626433832795;
+constexpr double kEuler = 2.7182818284590452353602874713527;
+
+std::string g_err;
+
+// ---------------------------------------------------------------------------
+// KRS step compilation (krs_cpu.cpp:293-316 prelude, Linux toolchain)
+// ---------------------------------------------------------------------------
+std::string make_source(const std::string& body, int amountOfX, bool dbl, bool dual) {
+    std::ostringstream o;
+    o << "#include <cmath>\n#include <cstdlib>\nusing std::abs;\n";
+    if (dual) {
+        // Forward-mode dual numbers: the same step body evaluated on (value, tangent)
+        // pairs gives the exact directional derivative of the step map. Used by the
+        // tangent-linear checkers; independent of the product's symbolic Jacobian.
+        o << "struct D { double v, d; D() : v(0), d(0) {} D(double x) : v(x), d(0) {}\n"
+             "  D(double x, double y) : v(x), d(y) {} };\n"
+             "static inline D operator+(D a, D b) { return D(a.v + b.v, a.d + b.d); }\n"
+             "static inline D operator-(D a, D b) { return D(a.v - b.v, a.d - b.d); }\n"
+             "static inline D operator-(D a) { return D(-a.v, -a.d); }\n"
+             "static inline D operator*(D a, D b) { return D(a.v * b.v, a.d * b.v + a.v * b.d); }\n"
+             "static inline D operator/(D a, D b) { return D(a.v / b.v, (a.d * b.v - a.v * b.d) / (b.v * b.v)); }\n"
+             "static inline D& operator+=(D& a, D b) { a = a + b; return a; }\n"
+             "static inline D& operator-=(D& a, D b) { a = a - b; return a; }\n"
+             "static inline D& operator*=(D& a, D b) { a = a * b; return a; }\n"
+             "static inline D& operator/=(D& a, D b) { a = a / b; return a; }\n"
+             "static inline bool operator<(D a, D b) { return a.v < b.v; }\n"
+             "static inline bool operator>(D a, D b) { return a.v > b.v; }\n"
+             "static inline D sin(D a) { return D(std::sin(a.v), std::cos(a.v) * a.d); }\n"
+             "static inline D cos(D a) { return D(std::cos(a.v), -std::sin(a.v) * a.d); }\n"
+             "static inline D tan(D a) { double t = std::tan(a.v); return D(t, (1 + t * t) * a.d); }\n"
+             "static inline D exp(D a) { double e = std::exp(a.v); return D(e, e * a.d); }\n"
+             "static inline D log(D a) { return D(std::log(a.v), a.d / a.v); }\n"
+             "static inline D sqrt(D a) { double s = std::sqrt(a.v); return D(s, a.d / (2 * s)); }\n"
+             "static inline D sinh(D a) { return D(std::sinh(a.v), std::cosh(a.v) * a.d); }\n"
+             "static inline D cosh(D a) { return D(std::cosh(a.v), std::sinh(a.v) * a.d); }\n"
+             "static inline D tanh(D a) { double t = std::tanh(a.v); return D(t, (1 - t * t) * a.d); }\n"
+             "static inline D atan(D a) { return D(std::atan(a.v), a.d / (1 + a.v * a.v)); }\n"
+             "static inline D fabs(D a) { return a.v < 0 ? -a : a; }\n"
+             "static inline D abs(D a) { return fabs(a); }\n"
+             "static inline D pow(D a, D b) { double p = std::pow(a.v, b.v);\n"
+             "  double dd = b.d == 0 ? b.v * std::pow(a.v, b.v - 1) * a.d\n"
+             "                       : p * (b.d * std::log(a.v) + b.v * a.d / a.v); return D(p, dd); }\n"
+             "typedef D numb;\n";
+    } else {
+        o << "typedef " << (dbl ? "double" : "float") << " numb;\n";
+    }
+    o << "static inline numb min(numb x, numb y) { return x < y ? x : y; }\n"
+         "static inline numb max(numb x, numb y) { return x > y ? x : y; }\n"
+         "#define AMOUNTOFX " << amountOfX << "\n"
+         "static const numb pi    = (numb)3.1415926535897932384626433832795;\n"
+         "static const numb euler = (numb)2.7182818284590452353602874713527;\n"
+         "extern \"C\" __attribute__((visibility(\"default\")))\n"
+         "void krs_step(numb* X, const numb* a, numb h) {\n"
+         "#line 1 \"krs\"\n"
+      << body << "\n}\n";
+    return o.str();
+}
+
+uint64_t fnv1a(const std::string& s, uint64_t h = 1469598103934665603ULL) {
+    for (unsigned char c : s) { h ^= c; h *= 1099511628211ULL; }
+    return h;
+}
+
+std::string cache_dir() {
+    const char* e = std::getenv("UCB_ORACLE_CACHE");
+    std::string d = e ? e : "/tmp/ucb_oracle_cache";
+    mkdir(d.c_str(), 0755);
+    return d;
+}
+
+std::mutex g_compile_mu;
+
+struct Krs {
+    void* lib = nullptr;
+    void* fn = nullptr;
+    int nx = 0;
+    int numb_bytes = 8;  // 8 double, 4 float, 16 dual
+};
+
+Krs* compile_krs(const std::string& body, int nx, int numb_bytes, const char* extra_flags) {
+    std::lock_guard<std::mutex> lk(g_compile_mu);
+    const bool dual = numb_bytes == 16;
+    const std::string src = make_source(body, nx, numb_bytes == 8, dual);
+    const std::string flags = std::string("-O2 -ffp-contract=off -fPIC -shared ") + (extra_flags ? extra_flags : "");
+    const uint64_t h = fnv1a(flags, fnv1a(src));
+    char name[64];
+    std::snprintf(name, sizeof name, "krs_%016llx", (unsigned long long)h);
+    const std::string dir = cache_dir();
+    const std::string so = dir + "/" + name + ".so";
+    if (access(so.c_str(), R_OK) != 0) {
+        const std::string cpp = dir + "/" + name + ".cpp";
+        {
+            std::ofstream f(cpp);
+            f << src;
+        }
+        const std::string tmp = so + ".tmp." + std::to_string(getpid());
+        const std::string log = dir + "/" + name + ".log";
+        const char* cxx_env = std::getenv("UCB_ORACLE_CXX");
+        const std::string cxx = cxx_env ? cxx_env : (access("/usr/bin/g++", X_OK) == 0 ? "/usr/bin/g++" : "g++");
+        const std::string cmd = cxx + " " + flags + " -o " + tmp + " " + cpp + " > " + log + " 2>&1";
+        if (std::system(cmd.c_str()) != 0) {
+            std::ifstream lf(log);
+            std::stringstream ss;
+            ss << lf.rdbuf();
+            g_err = "CPU KRS compile failed:\n" + ss.str();
+            return nullptr;
+        }
+        std::rename(tmp.c_str(), so.c_str());
+    }
+    void* lib = dlopen(so.c_str(), RTLD_NOW | RTLD_LOCAL);
+    if (!lib) { g_err = std::string("dlopen: ") + dlerror(); return nullptr; }
+    void* fn = dlsym(lib, "krs_step");
+    if (!fn) { g_err = "krs_step not exported"; dlclose(lib); return nullptr; }
+    Krs* k = new Krs;
+    k->lib = lib; k->fn = fn; k->nx = nx; k->numb_bytes = numb_bytes;
+    return k;
+}
+
+// ---------------------------------------------------------------------------
+// loopCalculateDiscreteModel_int (cudaLibrary.cu:782-895)
+// ---------------------------------------------------------------------------
+template <class T>
+using StepFn = void (*)(T*, const T*, T);
+
+template <class T>
+int loop_model(StepFn<T> step, T* x, const T* a, T h, int64_t iters, int nx,
+               int preScaller, int writableVar, T maxValue, T* data) {
+    T xPrev[64];
+    for (int64_t i = 0; i < iters; ++i) {
+        if (data != nullptr) {
+            if (writableVar < 0) {
+                if (nx >= 3) data[i] = x[0] + (T)kPi * x[1] + (T)kEuler * x[2];
+                else if (nx == 2) data[i] = x[0] + (T)kPi * x[1];
+                else data[i] = x[0];
+            } else {
+                data[i] = x[writableVar];
+            }
+            for (int j = 0; j < preScaller; ++j) step(x, a, h);
+        } else {
+            step(x, a, h);
+        }
+        if (i % kCheckInterval == 0) {
+            T checker = 0;
+            for (int j = 0; j < nx; ++j) checker = checker + std::fabs(x[j]);
+            if (std::isnan(checker) || std::isinf(checker)) return 0;
+            if (maxValue != 0)
+                if (std::fabs(checker) > maxValue) return 0;
+        }
+    }
+    for (int j = 0; j < nx; ++j) xPrev[j] = x[j];
+    for (int j = 0; j < preScaller; ++j) step(x, a, h);
+    T tempResult = 0;
+    for (int j = 0; j < nx; ++j) tempResult += std::fabs(x[j] - xPrev[j]);
+    if (std::fabs(tempResult) < (T)kEpsFixedPoint) return -1;
+    return 1;
+}
+
+// ---------------------------------------------------------------------------
+// getValueByIdx / getValueByIdx_log (cudaLibrary.cu:1344-1396), numb arithmetic
+// ---------------------------------------------------------------------------
+template <class T>
+T value_by_idx(int64_t idx, int nPts, T lo, T hi, int valueNumber) {
+    if (nPts <= 0) return lo;
+    if (nPts == 1) return hi;
+    const int64_t divisor = (valueNumber == 0) ? 1 : nPts;
+    const int64_t pointIdx = (idx / divisor) % nPts;
+    const T t = static_cast<T>(pointIdx) / static_cast<T>(nPts - 1);
+    return (static_cast<T>(1.0) - t) * lo + t * hi;
+}
+
+template <class T>
+T value_by_idx_log(int64_t idx, int nPts, T lo, T hi, int valueNumber) {
+    const T l = std::log10(lo) + (T)(((int64_t)((int64_t)idx / std::pow((T)nPts, (T)valueNumber)) % nPts)
+                                   * ((T)(std::log10(hi) - std::log10(lo)) / (T)(nPts - 1)));
+    return std::pow((T)10.0, l);
+}
+
+// ---------------------------------------------------------------------------
+// RNG stub (lle2d.template.cu:45-56 == parametric_engine.cpp:196-209)
+// ---------------------------------------------------------------------------
+struct Rng { uint64_t state; };
+inline void rng_init(uint64_t seed, uint64_t seq, uint64_t off, Rng* s) {
+    uint64_t z = seed + seq * 0x9E3779B97F4A7C15ULL + off;
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ULL;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBULL;
+    s->state = z ^ (z >> 31);
+}
+inline float rng_uniform(Rng* s) {
+    s->state = s->state * 6364136223846793005ULL + 1442695040888963407ULL;
+    return (float)(((s->state >> 40) & 0xFFFFFFULL) + 1ULL) / 16777216.0f;
+}
+
+// ---------------------------------------------------------------------------
+// Shared grid description (the kernel arguments of LLEKernelCUDA / LSKernelCUDA /
+// calculateDiscreteModelCUDA after run_* host mapping).
+// ---------------------------------------------------------------------------
+struct Grid {
+    int nPts;            // side (1D: number of points)
+    int dimension;       // 1 or 2
+    int par_or_var;      // 1 param, 0 IC, 2 mixed (axis 0 IC, axis 1 param)
+    int idx[2];          // indicesOfMutVars
+    double ranges[4];
+    int log_mask;
+    int h_axis;          // -1 none
+};
+
+template <class T>
+struct CellInit {
+    T x[64];
+    T a[64];
+    T h;
+};
+
+// Applies the sweep of one cell (the par_or_var branches of the kernels).
+template <class T>
+void init_cell(const Grid& g, int64_t idx, int nx, const double* ic, int nv, const double* vals,
+               double h, CellInit<T>* c) {
+    for (int i = 0; i < nx; ++i) c->x[i] = (T)ic[i];
+    for (int i = 0; i < nv; ++i) c->a[i] = (T)vals[i];
+    const T r[4] = {(T)g.ranges[0], (T)g.ranges[1], (T)g.ranges[2], (T)g.ranges[3]};
+    auto axis_val = [&](int i) -> T {
+        const bool lg = (g.log_mask >> i) & 1;
+        return lg ? value_by_idx_log<T>(idx, g.nPts, r[2 * i], r[2 * i + 1], i)
+                  : value_by_idx<T>(idx, g.nPts, r[2 * i], r[2 * i + 1], i);
+    };
+    c->h = (T)h;
+    if (g.h_axis == 0) c->h = axis_val(0);
+    else if (g.h_axis == 1) c->h = axis_val(1);
+    if (g.par_or_var == 1) {
+        for (int i = 0; i < g.dimension; ++i) { if (i == g.h_axis) continue; c->a[g.idx[i]] = axis_val(i); }
+    } else if (g.par_or_var == 0) {
+        for (int i = 0; i < g.dimension; ++i) { if (i == g.h_axis) continue; c->x[g.idx[i]] = axis_val(i); }
+    } else if (g.par_or_var == 2) {
+        c->x[g.idx[0]] = axis_val(0);
+        c->a[g.idx[1]] = axis_val(1);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// LLEKernelCUDA (cudaLibrary.cu:2486-2693), one cell
+// ---------------------------------------------------------------------------
+template <class T>
+T lle_cell(StepFn<T> step, const Grid& g, int64_t idx, int nx, const double* ic, int nv,
+           const double* vals, double h_d, double NT_d, double tMax_d, double transient_d,
+           double eps_d, double maxv_d, int sizeOfBlock, int skipHost, uint64_t rng_seq) {
+    CellInit<T> c;
+    init_cell<T>(g, idx, nx, ic, nv, vals, h_d, &c);
+    const T h = c.h, NT = (T)NT_d, tMax = (T)tMax_d, eps = (T)eps_d, maxv = (T)maxv_d;
+    if (h <= 0) return (T)NAN;
+    const int64_t ntp = (g.h_axis != -1) ? (int64_t)std::ceil(NT / h) : (int64_t)(NT / (T)h_d);
+    const int64_t skip = (g.h_axis != -1) ? (int64_t)std::ceil((T)transient_d / h) : (int64_t)skipHost;
+    T* x = c.x;
+    int flag = loop_model<T>(step, x, c.a, h, skip, nx, 1, 0, maxv, nullptr);
+    if (flag == 0) return (T)999;
+    Rng st;
+    rng_init(1234567891ULL, rng_seq, 0ULL, &st);
+    T z[64], y[64];
+    T zPower = 0;
+    for (int i = 0; i < nx; ++i) { z[i] = rng_uniform(&st) - 0.5; zPower += z[i] * z[i]; }
+    zPower = std::sqrt(zPower);
+    for (int i = 0; i < nx; ++i) z[i] /= zPower;
+    for (int i = 0; i < nx; ++i) y[i] = z[i] * eps + x[i];
+    T result = 0;
+    for (int b = 0; b < sizeOfBlock; ++b) {
+        if (loop_model<T>(step, x, c.a, h, ntp, nx, 1, 0, maxv, nullptr) == 0) return (T)999;
+        if (loop_model<T>(step, y, c.a, h, ntp, nx, 1, 0, maxv, nullptr) == 0) return (T)999;
+        T tempData = 0, tempData2 = 0;
+        for (int l = 0; l < nx; ++l) {
+            tempData2 = (T)1.0 / eps;
+            tempData2 = tempData2 * (x[l] - y[l]);
+            tempData += tempData2 * tempData2;
+        }
+        tempData = std::sqrt(tempData);
+        if (tempData <= 1e-14) tempData = (T)1e-14;
+        result += std::log(tempData);
+        tempData = (1 / tempData);
+        for (int j = 0; j < nx; ++j) y[j] = (T)(x[j] - ((x[j] - y[j] + 1e-14) * tempData));
+    }
+    return result / tMax;
+}
+
+// ---------------------------------------------------------------------------
+// gramSchmidtProcess (cudaLibrary.cu:2832-2874) — classical GS, row-major N x N
+// ---------------------------------------------------------------------------
+template <class T>
+void projection(const T* a, const T* b, T* minuend, int n) {
+    T num = 0, den = 0;
+    for (int i = 0; i < n; ++i) { num += a[i] * b[i]; den += b[i] * b[i]; }
+    const T frac = den == 0 ? 0 : num / den;
+    for (int i = 0; i < n; ++i) minuend[i] -= frac * b[i];
+}
+
+template <class T>
+void gram_schmidt(const T* a, T* b, int n, T* dens) {
+    for (int i = 0; i < n; ++i) {
+        for (int j = 0; j < n; ++j) b[j + i * n] = a[j + i * n];
+        for (int j = 0; j < i; ++j) projection(a + i * n, b + j * n, b + i * n, n);
+    }
+    for (int i = 0; i < n; ++i) {
+        T den = 0;
+        for (int j = 0; j < n; ++j) den += b[i * n + j] * b[i * n + j];
+        den = std::sqrt(den);
+        for (int j = 0; j < n; ++j) b[i * n + j] = den == 0 ? 0 : b[i * n + j] / den;
+        if (dens) dens[i] = den;
+    }
+}
+
+// LSKernelCUDA (cudaLibrary.cu:2878-3073), one cell -> n exponents
+template <class T>
+void ls_cell(StepFn<T> step, const Grid& g, int64_t idx, int nx, const double* ic, int nv,
+             const double* vals, double h_d, double NT_d, double tMax_d, double transient_d,
+             double eps_d, double maxv_d, int sizeOfBlock, int skipHost, uint64_t rng_seq, T* out) {
+    CellInit<T> c;
+    init_cell<T>(g, idx, nx, ic, nv, vals, h_d, &c);
+    const T h = c.h, NT = (T)NT_d, tMax = (T)tMax_d, eps = (T)eps_d, maxv = (T)maxv_d;
+    if (h <= 0) { for (int m = 0; m < nx; ++m) out[m] = (T)NAN; return; }
+    const int64_t ntp = (g.h_axis != -1) ? (int64_t)std::ceil(NT / h) : (int64_t)(NT / (T)h_d);
+    const int64_t skip = (g.h_axis != -1) ? (int64_t)std::ceil((T)transient_d / h) : (int64_t)skipHost;
+    T* x = c.x;
+    std::vector<T> y(nx * nx), z(nx * nx), result(nx, 0), dens(nx, 0);
+    Rng st;
+    rng_init(1234567891ULL, rng_seq, 0ULL, &st);
+    for (int j = 0; j < nx; ++j) {
+        T zPower = 0;
+        for (int i = 0; i < nx; ++i) {
+            z[j * nx + i] = rng_uniform(&st) - 0.5;
+            zPower += z[j * nx + i] * z[j * nx + i];
+        }
+        zPower = std::sqrt(zPower);
+        for (int i = 0; i < nx; ++i) z[j * nx + i] /= zPower;
+    }
+    int flag = loop_model<T>(step, x, c.a, h, skip, nx, 1, 0, maxv, nullptr);
+    if (flag == 0) { for (int m = 0; m < nx; ++m) out[m] = (T)999; return; }
+    gram_schmidt<T>(z.data(), y.data(), nx, nullptr);
+    for (int j = 0; j < nx; ++j)
+        for (int i = 0; i < nx; ++i) y[j * nx + i] = y[j * nx + i] * eps + x[i];
+    for (int b = 0; b < sizeOfBlock; ++b) {
+        if (loop_model<T>(step, x, c.a, h, ntp, nx, 1, 0, maxv, nullptr) == 0) {
+            for (int m = 0; m < nx; ++m) out[m] = (T)999;
+            return;
+        }
+        for (int j = 0; j < nx; ++j) {
+            if (loop_model<T>(step, y.data() + j * nx, c.a, h, ntp, nx, 1, 0, maxv, nullptr) == 0) {
+                for (int m = 0; m < nx; ++m) out[m] = (T)999;
+                return;
+            }
+        }
+        for (int k = 0; k < nx; ++k)
+            for (int l = 0; l < nx; ++l) y[k * nx + l] = y[k * nx + l] - x[l];
+        gram_schmidt<T>(y.data(), z.data(), nx, dens.data());
+        for (int k = 0; k < nx; ++k) {
+            result[k] += std::log(dens[k] / eps);
+            for (int j = 0; j < nx; ++j) y[k * nx + j] = (T)(x[j] + z[k * nx + j] * eps);
+        }
+    }
+    for (int i = 0; i < nx; ++i) out[i] = result[i] / tMax;
+}
+
+// ---------------------------------------------------------------------------
+// peakFinder (cudaLibrary.cu:1503-1633), block-local indexing
+// ---------------------------------------------------------------------------
+template <class T>
+int peak_finder(const T* data, int64_t n, T* outPeaks, T* timeOfPeaks, T h) {
+    int amountOfPeaks = 0;
+    if (n < 5) return 0;  // the GPU loop bound n-2 is unsigned; no peaks can exist below 5
+    for (int64_t i = 2; i < n - 2; ++i) {
+        if (data[i] - data[i - 1] > (T)kEpsPeakDelta && data[i] > (T)kPeakThreshold && data[i] >= data[i + 1]) {
+            for (int64_t j = i; j < n - 2; ++j) {
+                if (data[j] < data[j + 1]) { i = j + 1; break; }
+                if (data[j] - data[j + 1] > (T)kEpsPeakDelta) {
+                    T denom = data[j - 1] - (T)2.0 * data[j] + data[j + 1];
+                    T delta = 0.0;
+                    if (std::fabs(denom) > 1e-12) delta = 0.5 * (data[j - 1] - data[j + 1]) / denom;
+                    outPeaks[amountOfPeaks] = data[j] - 0.25 * (data[j - 1] - data[j + 1]) * delta;
+                    timeOfPeaks[amountOfPeaks] = (T)(j - 1) + delta;
+                    ++amountOfPeaks;
+                    i = j + 1;
+                    break;
+                }
+            }
+        }
+    }
+    if (amountOfPeaks > 1) {
+        for (int i = 0; i < amountOfPeaks - 1; i++) {
+            outPeaks[i] = outPeaks[i + 1];
+            timeOfPeaks[i] = (T)(timeOfPeaks[i + 1] - timeOfPeaks[i]) * h;
+        }
+        amountOfPeaks = amountOfPeaks - 1;
+    } else {
+        amountOfPeaks = 0;
+    }
+    if (amountOfPeaks >= kMaxAmountOfPeaks) amountOfPeaks = kMaxAmountOfPeaks;
+    return amountOfPeaks;
+}
+
+template <class T>
+struct Dispatch {
+    static StepFn<T> fn(Krs* k) { return reinterpret_cast<StepFn<T>>(k->fn); }
+};
+
+int threads_or_default(int nthreads) {
+    return nthreads > 0 ? nthreads : omp_get_max_threads();
+}
+
+}  // namespace
+
+// ============================================================================
+// C ABI of the oracle (used from Python through ctypes in tests/ and bench.py)
+// ============================================================================
+extern "C" {
+
+const char* orc_last_error() { return g_err.c_str(); }
+
+// numb_bytes: 8 (double), 4 (float), 16 (forward-mode dual: value + tangent)
+void* orc_krs_compile(const char* body, int nx, int numb_bytes) {
+    if (nx <= 0 || nx > 32) { g_err = "amountOfX out of range"; return nullptr; }
+    return compile_krs(body, nx, numb_bytes, nullptr);
+}
+
+void orc_krs_free(void* h) {
+    Krs* k = static_cast<Krs*>(h);
+    if (!k) return;
+    if (k->lib) dlclose(k->lib);
+    delete k;
+}
+
+// One call of loopCalculateDiscreteModel_int on a caller-owned state. x, a, data
+// are numb arrays matching the compiled precision.
+int orc_loop(void* h, void* x, const void* a, double hstep, long long iters, int preScaller,
+             int writableVar, double maxValue, void* data) {
+    Krs* k = static_cast<Krs*>(h);
+    if (k->numb_bytes == 8)
+        return loop_model<double>(Dispatch<double>::fn(k), (double*)x, (const double*)a, hstep, iters,
+                                  k->nx, preScaller, writableVar, maxValue, (double*)data);
+    return loop_model<float>(Dispatch<float>::fn(k), (float*)x, (const float*)a, (float)hstep, iters,
+                             k->nx, preScaller, writableVar, (float)maxValue, (float*)data);
+}
+
+// Plain repeated stepping (no checks): x <- step^n(x). Used for trajectory parity.
+void orc_steps(void* h, void* x, const void* a, double hstep, long long n) {
+    Krs* k = static_cast<Krs*>(h);
+    if (k->numb_bytes == 8) {
+        auto f = Dispatch<double>::fn(k);
+        for (long long i = 0; i < n; ++i) f((double*)x, (const double*)a, hstep);
+    } else {
+        auto f = Dispatch<float>::fn(k);
+        for (long long i = 0; i < n; ++i) f((float*)x, (const float*)a, (float)hstep);
+    }
+}
+
+// Axis value table of one sweep axis: out[i] = getValueByIdx(_log) of point i.
+void orc_axis_values(int numb_bytes, int nPts, double lo, double hi, int log_scale, double* out) {
+    for (int i = 0; i < nPts; ++i) {
+        if (numb_bytes == 8)
+            out[i] = log_scale ? value_by_idx_log<double>(i, nPts, lo, hi, 0) : value_by_idx<double>(i, nPts, lo, hi, 0);
+        else
+            out[i] = log_scale ? (double)value_by_idx_log<float>(i, nPts, (float)lo, (float)hi, 0)
+                               : (double)value_by_idx<float>(i, nPts, (float)lo, (float)hi, 0);
+    }
+}
+
+void orc_rng_uniforms(unsigned long long seq, int n, float* out) {
+    Rng st;
+    rng_init(1234567891ULL, seq, 0ULL, &st);
+    for (int i = 0; i < n; ++i) out[i] = rng_uniform(&st);
+}
+
+// LLE 2D (run_lle_2d + LLEKernelCUDA). cells: optional subset of kernel cell indices
+// (nullptr = all n^2). values/flags are indexed like the cells array (or n^2 in
+// user row-major order when cells == nullptr).
+int orc_lle2d(void* h, int nPts, int par_or_var, int idx0, int idx1, const double* ranges,
+              int log_mask, int h_axis, int swap_xy, const double* ic, int nv, const double* vals,
+              double hstep, double transient, double tMax, double NT, double eps, double maxv,
+              const long long* cells, long long ncells, double* values, int* flags, int nthreads) {
+    Krs* k = static_cast<Krs*>(h);
+    Grid g{nPts, 2, par_or_var, {idx0, idx1}, {ranges[0], ranges[1], ranges[2], ranges[3]}, log_mask, h_axis};
+    const int sizeOfBlock = (int)(tMax / NT);
+    const int skipHost = (int)(transient / hstep);
+    if (sizeOfBlock <= 0) { g_err = "computed amountOfPointsInBlock <= 0"; return -1; }
+    const long long total = (long long)nPts * nPts;
+    const long long n = cells ? ncells : total;
+#pragma omp parallel for schedule(dynamic, 1) num_threads(threads_or_default(nthreads))
+    for (long long c = 0; c < n; ++c) {
+        const long long kidx = cells ? cells[c] : c;
+        double v;
+        if (k->numb_bytes == 8)
+            v = lle_cell<double>(Dispatch<double>::fn(k), g, kidx, k->nx, ic, nv, vals, hstep, NT, tMax,
+                                 transient, eps, maxv, sizeOfBlock, skipHost, (uint64_t)kidx);
+        else
+            v = (double)lle_cell<float>(Dispatch<float>::fn(k), g, kidx, k->nx, ic, nv, vals, hstep, NT, tMax,
+                                        transient, eps, maxv, sizeOfBlock, skipHost, (uint64_t)kidx);
+        long long out = c;
+        if (!cells && swap_xy) {
+            const long long kix = kidx % nPts, kiy = kidx / nPts;
+            out = kix * nPts + kiy;
+        }
+        values[out] = v;
+        flags[out] = (v == 999.0 || v == -999.0) ? -1 : 1;
+    }
+    return 0;
+}
+
+// LS 2D (run_ls_2d + LSKernelCUDA). values: plane-major [k * n^2 + cell] when cells ==
+// nullptr, else [c * nx + k].
+int orc_ls2d(void* h, int nPts, int par_or_var, int idx0, int idx1, const double* ranges,
+             int log_mask, int h_axis, int swap_xy, const double* ic, int nv, const double* vals,
+             double hstep, double transient, double tMax, double NT, double eps, double maxv,
+             const long long* cells, long long ncells, double* values, int* flags, int nthreads) {
+    Krs* k = static_cast<Krs*>(h);
+    Grid g{nPts, 2, par_or_var, {idx0, idx1}, {ranges[0], ranges[1], ranges[2], ranges[3]}, log_mask, h_axis};
+    const int sizeOfBlock = (int)(tMax / NT);
+    const int skipHost = (int)(transient / hstep);
+    if (sizeOfBlock <= 0) { g_err = "computed amountOfPointsInBlock <= 0"; return -1; }
+    const int nx = k->nx;
+    const long long total = (long long)nPts * nPts;
+    const long long n = cells ? ncells : total;
+#pragma omp parallel for schedule(dynamic, 1) num_threads(threads_or_default(nthreads))
+    for (long long c = 0; c < n; ++c) {
+        const long long kidx = cells ? cells[c] : c;
+        double outv[64];
+        if (k->numb_bytes == 8) {
+            ls_cell<double>(Dispatch<double>::fn(k), g, kidx, nx, ic, nv, vals, hstep, NT, tMax, transient, eps,
+                            maxv, sizeOfBlock, skipHost, (uint64_t)kidx, outv);
+        } else {
+            float o32[64];
+            ls_cell<float>(Dispatch<float>::fn(k), g, kidx, nx, ic, nv, vals, hstep, NT, tMax, transient, eps,
+                           maxv, sizeOfBlock, skipHost, (uint64_t)kidx, o32);
+            for (int m = 0; m < nx; ++m) outv[m] = o32[m];
+        }
+        long long cell = c;
+        if (!cells && swap_xy) {
+            const long long kix = kidx % nPts, kiy = kidx / nPts;
+            cell = kix * nPts + kiy;
+        }
+        bool bad = false;
+        for (int m = 0; m < nx; ++m) {
+            if (cells) values[c * nx + m] = outv[m];
+            else values[(long long)m * total + cell] = outv[m];
+            if (outv[m] == 999.0 || outv[m] == -999.0) bad = true;
+        }
+        flags[cells ? c : cell] = bad ? -1 : 1;
+    }
+    return 0;
+}
+
+// Bifurcation 1D (run_bif1d + calculateDiscreteModelCUDA + peakFinderCUDA).
+// Outputs per point: count[i] (flag semantics of Bifurcation1DResult::flags),
+// peaks[i*max_out + j], intervals[i*max_out + j] for j < min(count, max_out).
+int orc_bif1d(void* h, int nPts, int sweep_kind, int sweep_index, double lo, double hi, int log_scale,
+              const double* ic, int nv, const double* vals, double hstep, double transient, double tMax,
+              int preScaller, int writableVar, double maxv, int max_out, const long long* pts,
+              long long npts_subset, int* counts, double* peaks, double* intervals, int nthreads) {
+    Krs* k = static_cast<Krs*>(h);
+    const int nx = k->nx;
+    // sweep_kind: 0 param, 1 IC, 2 h
+    Grid g{nPts, 1, sweep_kind == 1 ? 0 : 1, {sweep_index, 0}, {lo, hi, 0, 0}, log_scale ? 1 : 0,
+           sweep_kind == 2 ? 0 : -1};
+    const double worstCaseH = (sweep_kind == 2) ? (k->numb_bytes == 8 ? lo : (double)(float)lo) : hstep;
+    const long long amountOfPointsInBlock = (long long)std::ceil(tMax / worstCaseH / preScaller);
+    const long long amountOfPointsForSkip = (long long)(transient / hstep);
+    if (amountOfPointsInBlock <= 0) { g_err = "computed amountOfPointsInBlock <= 0"; return -1; }
+    const long long n = pts ? npts_subset : nPts;
+    int rc = 0;
+#pragma omp parallel num_threads(threads_or_default(nthreads))
+    {
+        std::vector<double> d8, p8, t8;
+        std::vector<float> d4, p4, t4;
+#pragma omp for schedule(dynamic, 1)
+        for (long long c = 0; c < n; ++c) {
+            const long long idx = pts ? pts[c] : c;
+            int cnt = 0;
+            auto run = [&](auto tag, auto& dd, auto& pp, auto& tt) {
+                using T = decltype(tag);
+                StepFn<T> f = Dispatch<T>::fn(k);
+                CellInit<T> ci;
+                init_cell<T>(g, idx, nx, ic, nv, vals, hstep, &ci);
+                const T hl = ci.h;
+                if (hl <= 0) { cnt = -1; return; }
+                long long skip_l = amountOfPointsForSkip, iters_l = amountOfPointsInBlock;
+                if (g.h_axis != -1) {
+                    skip_l = (long long)std::ceil((T)transient / hl);
+                    iters_l = (long long)std::ceil((T)tMax / hl / (T)preScaller);
+                }
+                if (iters_l > amountOfPointsInBlock) iters_l = amountOfPointsInBlock;
+                dd.assign((size_t)iters_l, (T)0);
+                pp.assign((size_t)iters_l, (T)0);
+                tt.assign((size_t)iters_l, (T)0);
+                int flag = loop_model<T>(f, ci.x, ci.a, hl, skip_l, nx, preScaller, writableVar, (T)maxv, nullptr);
+                if (flag == 1 || flag == -1)
+                    flag = loop_model<T>(f, ci.x, ci.a, hl, iters_l, nx, preScaller, writableVar, (T)maxv, dd.data());
+                if (flag == -1 || flag == 0) { cnt = flag; return; }
+                const T timeStep = (T)(hstep * (double)preScaller);
+                cnt = peak_finder<T>(dd.data(), iters_l, pp.data(), tt.data(), timeStep);
+                // run_bif1d rescales intervals by param_val / h, param_val from the host
+                // copy of getValueByIdx (parametric_engine.cpp:577-590, 1991-2003).
+                double time_scale = 1.0;
+                if (g.h_axis != -1) {
+                    const double rlo = (double)(T)lo, rhi = (double)(T)hi;
+                    double pv;
+                    if (nPts <= 1) pv = rlo;
+                    else if (log_scale)
+                        pv = std::pow(10.0, std::log10(rlo) + (std::log10(rhi) - std::log10(rlo)) * (double)idx / (double)(nPts - 1));
+                    else
+                        pv = rlo + (rhi - rlo) * (double)idx / (double)(nPts - 1);
+                    time_scale = pv / hstep;
+                }
+                const int m = std::min(cnt, max_out);
+                for (int j = 0; j < m; ++j) {
+                    peaks[c * max_out + j] = (double)pp[j];
+                    intervals[c * max_out + j] = (double)tt[j] * time_scale;
+                }
+            };
+            if (k->numb_bytes == 8) run(0.0, d8, p8, t8);
+            else run(0.0f, d4, p4, t4);
+            counts[c] = cnt;
+        }
+    }
+    return rc;
+}
+
+}  // extern "C"

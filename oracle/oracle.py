@@ -1,0 +1,164 @@
+"""ORACLE (test infrastructure): ctypes wrapper over oracle/liboracle.so.
+
+The CPU restatement of the reference hot path lives in oracle/krs_oracle.cpp; every
+function there cites the reference file:line it follows. Only tests/, the smoke check
+in __graft_entry__.py and bench.py's CPU-baseline leg may import this module, and only
+as the checker / the timed CPU baseline. The product never imports it.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+from pathlib import Path
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+LIB_PATH = HERE / "liboracle.so"
+
+_lib = None
+
+
+def build() -> None:
+    """Compile liboracle.so (g++, OpenMP)."""
+    subprocess.run(["make", "-s", "-C", str(HERE)], check=True)
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not LIB_PATH.exists():
+            build()
+        L = C.CDLL(str(LIB_PATH))
+        L.orc_last_error.restype = C.c_char_p
+        L.orc_krs_compile.restype = C.c_void_p
+        L.orc_krs_compile.argtypes = [C.c_char_p, C.c_int, C.c_int]
+        L.orc_krs_free.argtypes = [C.c_void_p]
+        L.orc_loop.restype = C.c_int
+        L.orc_loop.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_double, C.c_longlong, C.c_int,
+                               C.c_int, C.c_double, C.c_void_p]
+        L.orc_steps.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_double, C.c_longlong]
+        L.orc_axis_values.argtypes = [C.c_int, C.c_int, C.c_double, C.c_double, C.c_int, C.c_void_p]
+        L.orc_rng_uniforms.argtypes = [C.c_ulonglong, C.c_int, C.c_void_p]
+        grid_args = [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_int, C.c_void_p, C.c_int, C.c_int, C.c_int,
+                     C.c_void_p, C.c_int, C.c_void_p, C.c_double, C.c_double, C.c_double, C.c_double,
+                     C.c_double, C.c_double, C.c_void_p, C.c_longlong, C.c_void_p, C.c_void_p, C.c_int]
+        L.orc_lle2d.restype = C.c_int
+        L.orc_lle2d.argtypes = grid_args
+        L.orc_ls2d.restype = C.c_int
+        L.orc_ls2d.argtypes = grid_args
+        L.orc_bif1d.restype = C.c_int
+        L.orc_bif1d.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_double, C.c_double, C.c_int,
+                                C.c_void_p, C.c_int, C.c_void_p, C.c_double, C.c_double, C.c_double,
+                                C.c_int, C.c_int, C.c_double, C.c_int, C.c_void_p, C.c_longlong,
+                                C.c_void_p, C.c_void_p, C.c_void_p, C.c_int]
+        _lib = L
+    return _lib
+
+
+def _ptr(a):
+    return None if a is None else a.ctypes.data_as(C.c_void_p)
+
+
+class Krs:
+    """A KRS step body compiled natively (krs_cpu.cpp make_source restated)."""
+
+    def __init__(self, body: str, nx: int, numb: str = "f64"):
+        self.nx = nx
+        self.numb = numb
+        nb = {"f64": 8, "f32": 4, "dual": 16}[numb]
+        h = lib().orc_krs_compile(body.encode(), nx, nb)
+        if not h:
+            raise RuntimeError(lib().orc_last_error().decode())
+        self.h = h
+
+    @property
+    def dtype(self):
+        return np.float64 if self.numb == "f64" else np.float32
+
+    def __del__(self):
+        try:
+            if getattr(self, "h", None):
+                lib().orc_krs_free(self.h)
+        except Exception:
+            pass
+
+    def steps(self, x, a, h, n):
+        x = np.array(x, dtype=self.dtype)
+        a = np.array(a, dtype=self.dtype)
+        lib().orc_steps(self.h, _ptr(x), _ptr(a), h, n)
+        return x
+
+    def loop(self, x, a, h, iters, pre=1, writable=0, maxv=1e6, record=False):
+        x = np.array(x, dtype=self.dtype)
+        a = np.array(a, dtype=self.dtype)
+        data = np.zeros(max(iters, 1), dtype=self.dtype) if record else None
+        flag = lib().orc_loop(self.h, _ptr(x), _ptr(a), h, iters, pre, writable, maxv, _ptr(data))
+        return flag, x, data
+
+
+def axis_values(n, lo, hi, log_scale=False, numb="f64"):
+    out = np.zeros(n, dtype=np.float64)
+    lib().orc_axis_values(8 if numb == "f64" else 4, n, lo, hi, int(log_scale), _ptr(out))
+    return out
+
+
+def rng_uniforms(seq, n):
+    out = np.zeros(n, dtype=np.float32)
+    lib().orc_rng_uniforms(seq, n, _ptr(out))
+    return out
+
+
+def _grid(fn, krs, g, cells, nthreads, nvals_per_cell):
+    n = g["n_pts"]
+    ranges = np.array(g["ranges"], dtype=np.float64)
+    ic = np.array(g["ic"], dtype=np.float64)
+    vals = np.array(g["values"], dtype=np.float64)
+    if cells is not None:
+        cells = np.ascontiguousarray(cells, dtype=np.int64)
+        m = len(cells)
+        values = np.zeros(m * nvals_per_cell, dtype=np.float64)
+        flags = np.zeros(m, dtype=np.int32)
+    else:
+        m = 0
+        values = np.zeros(n * n * nvals_per_cell, dtype=np.float64)
+        flags = np.zeros(n * n, dtype=np.int32)
+    rc = fn(krs.h, n, g["par_or_var"], g["idx"][0], g["idx"][1], _ptr(ranges), g.get("log_mask", 0),
+            g.get("h_axis", -1), int(g.get("swap_xy", 0)), _ptr(ic), len(vals), _ptr(vals), g["h"],
+            g["transient_time"], g["t_max"], g["NT"], g["eps"], g["max_value"], _ptr(cells), m,
+            _ptr(values), _ptr(flags), nthreads)
+    if rc != 0:
+        raise RuntimeError(lib().orc_last_error().decode())
+    return values, flags
+
+
+def lle2d(krs: Krs, g: dict, cells=None, nthreads=0):
+    """run_lle_2d semantics. g: kernel-level grid dict (see tests/helpers)."""
+    return _grid(lib().orc_lle2d, krs, g, cells, nthreads, 1)
+
+
+def ls2d(krs: Krs, g: dict, cells=None, nthreads=0):
+    return _grid(lib().orc_ls2d, krs, g, cells, nthreads, krs.nx)
+
+
+def bif1d(krs: Krs, b: dict, max_out=64, pts=None, nthreads=0):
+    n = b["n_pts"]
+    ic = np.array(b["ic"], dtype=np.float64)
+    vals = np.array(b["values"], dtype=np.float64)
+    if pts is not None:
+        pts = np.ascontiguousarray(pts, dtype=np.int64)
+        m = len(pts)
+    else:
+        m = n
+    counts = np.zeros(m, dtype=np.int32)
+    peaks = np.full(m * max_out, np.nan)
+    intervals = np.full(m * max_out, np.nan)
+    rc = lib().orc_bif1d(krs.h, n, b.get("sweep_kind", 0), b["sweep_index"], b["lo"], b["hi"],
+                         int(b.get("log_scale", 0)), _ptr(ic), len(vals), _ptr(vals), b["h"],
+                         b["transient_time"], b["t_max"], b.get("pre_scaller", 1), b.get("writable_var", 0),
+                         b["max_value"], max_out, _ptr(pts), m if pts is not None else 0, _ptr(counts),
+                         _ptr(peaks), _ptr(intervals), nthreads)
+    if rc != 0:
+        raise RuntimeError(lib().orc_last_error().decode())
+    return counts, peaks.reshape(m, max_out), intervals.reshape(m, max_out)

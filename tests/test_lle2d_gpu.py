@@ -1,0 +1,154 @@
+"""GPU parity of the LLE-2D path against the oracle (CPU restatement of LLEKernelCUDA +
+run_lle_2d), through the C ABI.
+
+Tolerances:
+  * exact form (KRS body verbatim, no FMA contraction): trajectories bit-identical to the
+    oracle; the only difference is the device vs glibc `log` (<= 1 ulp per block), so
+    values agree to 1e-12 relative (FP64) / 1e-5 relative (FP32), flags exactly;
+  * native FP64 (FMA-ordered RK4): trajectories within 1e-12 relative of the oracle
+    before one Lyapunov time; on non-chaotic cells (oracle lambda < 0.01) |dLLE| <= 2e-3;
+    on chaotic cells the difference is bounded by the intrinsic finite-time spread;
+  * FP32 tangent form: same criteria as native FP64 on non-chaotic cells.
+"""
+import numpy as np
+import pytest
+
+import ucb
+from helpers import LORENZ, engine_request, kernel_grid, lle2d_case, rk4_body
+from oracle import oracle as O
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def eng():
+    e = ucb.Engine(0)
+    yield e
+    e.close()
+
+
+def oracle_lle(c, numb="f64"):
+    return O.lle2d(O.Krs(c["body"], c["nx"], numb), kernel_grid(c))
+
+
+def run(eng, c, **opt):
+    v, f, res = eng.run_lle2d(engine_request(ucb, c, **opt))
+    return v, f, res
+
+
+def test_exact_f64_matches_oracle(eng):
+    c = lle2d_case(n=16, t_max=20.0, transient=10.0)
+    v, f, res = run(eng, c, precision=ucb.PREC_F64, mode=ucb.MODE_EXACT)
+    ov, of = oracle_lle(c)
+    np.testing.assert_array_equal(f, of)
+    np.testing.assert_allclose(v, ov, rtol=1e-12, atol=1e-14)
+    assert res.steps > 0 and res.kernel_ms > 0
+
+
+def test_exact_f32_matches_oracle(eng):
+    c = lle2d_case(n=12, t_max=10.0, transient=5.0)
+    v, f, _ = run(eng, c, precision=ucb.PREC_F32, mode=ucb.MODE_EXACT)
+    ov, of = oracle_lle(c, "f32")
+    np.testing.assert_array_equal(f, of)
+    np.testing.assert_allclose(v, ov, rtol=1e-5, atol=1e-6)
+
+
+@pytest.mark.parametrize("variant", ["pov0", "pov2", "pov2_swap", "log", "h_axis", "divergent"])
+def test_exact_mapping_variants(eng, variant):
+    base = lle2d_case(n=9, t_max=5.0, transient=2.0)
+    if variant == "pov0":
+        c = dict(base, sweep_over_var=True, sweep_over_var_2=True, var_sweep_index=0, var_sweep_index_2=2,
+                 param_lo=-2.0, param_hi=2.0, param_lo_2=0.0, param_hi_2=3.0)
+    elif variant == "pov2":
+        c = dict(base, sweep_over_var=True, var_sweep_index=1, param_lo=-1.0, param_hi=1.0)
+    elif variant == "pov2_swap":
+        c = dict(base, sweep_over_var_2=True, var_sweep_index_2=1, param_index=3, param_lo=3.0, param_hi=9.0,
+                 param_lo_2=-1.0, param_hi_2=1.0)
+    elif variant == "log":
+        c = dict(base, log_scale=True, log_scale_2=True, param_lo=0.05, param_hi=2.0)
+    elif variant == "h_axis":
+        c = dict(base, sweep_over_h=True, param_lo=0.005, param_hi=0.02)
+    else:  # sweeping Rossler's a over [0.1, 1.5] sends part of the grid past max_value
+        c = dict(base, param_index=1, param_lo=0.1, param_hi=1.5, max_value=50.0)
+    v, f, _ = run(eng, c, precision=ucb.PREC_F64, mode=ucb.MODE_EXACT)
+    ov, of = oracle_lle(c)
+    np.testing.assert_array_equal(f, of)
+    np.testing.assert_allclose(v, ov, rtol=1e-12, atol=1e-14)
+    if variant == "divergent":
+        assert (f == -1).any()
+
+
+def test_native_f64_trajectory_parity_before_one_lyapunov_time(eng):
+    # Rossler's largest exponent is <= ~0.2 on this grid: one Lyapunov time >= 5 time units.
+    c = lle2d_case(n=8)
+    req = engine_request(ucb, c, precision=ucb.PREC_F64, mode=ucb.MODE_NATIVE)
+    n_steps = 400  # t = 4
+    xs = eng.lle2d_states(req, n_steps)
+    g = kernel_grid(c)
+    k = O.Krs(c["body"], 3)
+    ax0 = O.axis_values(c["n_pts"], c["param_lo"], c["param_hi"])
+    ax1 = O.axis_values(c["n_pts"], c["param_lo_2"], c["param_hi_2"])
+    for cell in range(c["n_pts"] ** 2):
+        a = np.array(c["values"], dtype=np.float64)
+        a[g["idx"][0]] = ax0[cell % c["n_pts"]]
+        a[g["idx"][1]] = ax1[cell // c["n_pts"]]
+        ref = k.steps(c["ic"], a, c["h"], n_steps)
+        np.testing.assert_allclose(xs[cell], ref, rtol=1e-12, atol=1e-12)
+
+
+def test_exact_trajectory_bitwise(eng):
+    c = lle2d_case(n=4)
+    xs = eng.lle2d_states(engine_request(ucb, c, precision=ucb.PREC_F64, mode=ucb.MODE_EXACT), 3000)
+    g = kernel_grid(c)
+    k = O.Krs(c["body"], 3)
+    ax0 = O.axis_values(4, c["param_lo"], c["param_hi"])
+    ax1 = O.axis_values(4, c["param_lo_2"], c["param_hi_2"])
+    for cell in range(16):
+        a = np.array(c["values"], dtype=np.float64)
+        a[g["idx"][0]] = ax0[cell % 4]
+        a[g["idx"][1]] = ax1[cell // 4]
+        np.testing.assert_array_equal(xs[cell], k.steps(c["ic"], a, c["h"], 3000))
+
+
+@pytest.mark.parametrize("prec", [ucb.PREC_F64, ucb.PREC_F32])
+def test_native_lle_within_tolerance(eng, prec):
+    # Non-chaotic cells are identified by the oracle itself: perturbing the initial
+    # condition by 1e-13 leaves their exponent unchanged (|change| < 1e-6), while chaotic
+    # cells move by up to ~1e-2 at this horizon. On non-chaotic cells the engine must be
+    # within 2e-3 of the FP64 oracle on >= 99.5% of them; on chaotic cells its median
+    # difference must stay within 2x the oracle's own median perturbation spread.
+    c = lle2d_case(n=16, t_max=200.0, transient=50.0)
+    v, f, _ = run(eng, c, precision=prec, mode=ucb.MODE_NATIVE)
+    ov, of = oracle_lle(c)
+    pv, _ = oracle_lle(dict(c, ic=(1.0 + 1e-13, 1.0, 1.0)))
+    np.testing.assert_array_equal(f, of)
+    d = np.abs(v - ov)
+    spread = np.abs(pv - ov)
+    quiet = spread < 1e-6
+    assert quiet.sum() > 20
+    assert np.mean(d[quiet] <= 2e-3) >= 0.995, np.sort(d[quiet])[-5:]
+    assert np.median(d[~quiet]) <= 2 * max(np.median(spread[~quiet]), 1e-3)
+
+
+def test_lorenz_grid_native_runs(eng):
+    c = dict(lle2d_case(n=8, t_max=20.0, transient=5.0), body=rk4_body(LORENZ), values=(0, 10.0, 28.0, 8 / 3),
+             param_index=1, param_index_2=2, param_lo=5.0, param_hi=15.0, param_lo_2=20.0, param_hi_2=40.0,
+             ic=(0.1, 0.1, 0.1))
+    v, f, _ = run(eng, c, precision=ucb.PREC_F64, mode=ucb.MODE_NATIVE)
+    ov, of = oracle_lle(c)
+    np.testing.assert_array_equal(f, of)
+    assert np.isfinite(v).all()
+
+
+def test_device_entry_matches_host_entry(eng):
+    torch = pytest.importorskip("torch")
+    c = lle2d_case(n=10, t_max=5.0, transient=2.0)
+    req = engine_request(ucb, c, precision=ucb.PREC_F64, mode=ucb.MODE_EXACT)
+    hv, hf, _ = eng.run_lle2d(req)
+    dv = torch.empty(100, dtype=torch.float64, device="cuda")
+    df = torch.empty(100, dtype=torch.int32, device="cuda")
+    s = torch.cuda.current_stream()
+    eng.lle2d_device(req, dv.data_ptr(), df.data_ptr(), s.cuda_stream)
+    torch.cuda.synchronize()
+    np.testing.assert_array_equal(dv.cpu().numpy(), hv)
+    np.testing.assert_array_equal(df.cpu().numpy(), hf)

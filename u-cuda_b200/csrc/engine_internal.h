@@ -1,0 +1,75 @@
+// Internal pieces shared by the C-ABI entry points (not part of the ABI).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include "../../include/ucb.h"
+#include "frontend.h"
+#include "jit.h"
+
+struct ucb_engine {
+    int device = 0;
+    bool initialized = false;
+    int sm_count = 0;
+    std::string last_error;
+    ucb::ModuleCache modules;
+    cudaStream_t stream = nullptr;   // engine stream for the host-buffer entry points
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    // Device workspace: work counters, step counters, axis tables. Grown on demand.
+    void* ws = nullptr;
+    size_t ws_bytes = 0;
+    long long launches = 0;
+};
+
+namespace ucb {
+
+// Kernel-order sweep description after the reference's host mapping
+// (run_lle_2d parametric_engine.cpp:2602-2703).
+struct SweepMap {
+    int dim = 2;
+    int par_or_var = 1;
+    int idx[2] = {0, 0};
+    double lo[2] = {0, 0}, hi[2] = {0, 0};
+    bool log_axis[2] = {false, false};
+    int h_axis = -1;
+    bool swap_xy = false;
+};
+
+// The step function of a run: either the verbatim KRS body (exact form) or the
+// right-hand side recognised in it (native form).
+struct SystemCode {
+    bool exact = true;
+    bool has_jvp = false;
+    std::string code;     // device source defining calculateDiscreteModel or ucb_rhs/ucb_jvp
+    int flops_step = 0;   // algorithmic FLOPs of one step (native form; 0 if unknown)
+    std::string note;     // why the exact form was chosen, when native was requested
+};
+
+bool ensure_init(ucb_engine* e, std::string& err);
+bool ensure_workspace(ucb_engine* e, size_t bytes, std::string& err);
+
+// Builds the step-function source for a run.
+SystemCode make_system_code(const std::string& krs_body, int nx, int nv, int precision, int mode,
+                            bool want_jvp);
+
+// Common prelude: numb typedef, configCUDA.h constants pi/euler, sizes, sweep macros.
+std::string make_prelude(int precision, int nx, int nv, const SweepMap& m, bool extra_step,
+                         const SystemCode& sys, const std::vector<std::string>& extra_defines);
+
+// Embedded device headers (generated at build time from csrc/kernels/*.cuh).
+const std::vector<std::pair<std::string, std::string>>& device_headers();
+
+// Axis value table of one sweep axis in numb arithmetic (getValueByIdx,
+// cudaLibrary.cu:1344-1361, and getValueByIdx_log, :1381-1396; valueNumber 0).
+void axis_table(int precision, int n, double lo, double hi, bool log_scale, std::vector<double>& out_d,
+                std::vector<float>& out_f);
+
+// Launch helper: persistent grid size for a kernel.
+int persistent_grid(ucb_engine* e, CUfunction f, int block, long long work_items);
+
+}  // namespace ucb

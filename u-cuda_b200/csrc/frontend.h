@@ -1,0 +1,106 @@
+// Text front-end of the engine.
+//
+// 1. System text -> System -> step body ("KRS"), the role of the reference's
+//    sysparse.cpp (parse_system_from_latex, :287-393) and codegen.cpp (codegen_scheme,
+//    :951-961). The emitted step bodies are byte-identical to the reference's for the
+//    schemes implemented here (Euler, Euler-Cromer, Explicit Midpoint, RK4, DOPRI78),
+//    because sessions, stored custom schemes and the engine's own recogniser exchange
+//    them as text.
+// 2. Step body -> right-hand side: recognises the codegen RK4 template in a KRS body and
+//    recovers the right-hand-side expressions as an expression tree, from which the
+//    native FMA-ordered integrator code, the tangent-linear product J(x) v and the
+//    algorithmic FLOP count are generated.
+#pragma once
+
+#include <map>
+#include <memory>
+#include <string>
+#include <vector>
+
+namespace ucb {
+namespace fe {
+
+// ------------------------------------------------------------------ expression tree
+struct Node;
+using PNode = std::shared_ptr<const Node>;
+
+struct Node {
+    enum Kind { Num, Sym, Var, Par, Call, Add, Sub, Mul, Div, Pow, Neg } kind;
+    double num = 0;          // Num
+    std::string name;        // Sym (symbolic name before binding), Call (function)
+    int index = 0;           // Var: X[index]; Par: a[index]
+    PNode a, b;              // operands
+    std::vector<PNode> args; // Call
+};
+
+PNode num(double v);
+PNode var(int i);
+PNode par(int j);
+PNode binop(Node::Kind k, PNode a, PNode b);
+PNode neg(PNode a);
+PNode call(const std::string& f, std::vector<PNode> args);
+
+// ------------------------------------------------------------------ system text
+struct System {
+    std::vector<std::string> vars;    // state variables -> X[0..N-1]
+    std::vector<std::string> params;  // parameters -> a[1..M] (a[0] reserved)
+    std::vector<PNode> rhs;           // bound right-hand sides (Var / Par / Num / pi)
+};
+
+struct FuncDef {
+    std::vector<std::string> args;
+    std::string body;
+};
+using FuncDefs = std::map<std::string, FuncDef>;
+
+enum class Scheme { Euler, EulerCromer, ExplicitMidpoint, RK4, DOPRI78 };
+
+// Parses a multi-line LaTeX (or plain-syntax) system with the given alphabet. Throws
+// std::runtime_error with a message on malformed input.
+System parse_system(const std::string& text, const std::vector<std::string>& alphabet,
+                    bool order_as_in_system = false, const FuncDefs& funcs = {});
+FuncDefs parse_func_defs(const std::string& text);
+
+// Step body of a scheme, in the reference's text form.
+std::string emit_scheme(const System& s, Scheme sc);
+// C expression of one right-hand side over `state` (e.g. "X1") and a[].
+std::string emit_expr(const PNode& n, const std::string& state);
+
+// ------------------------------------------------------------------ recognition
+struct Rhs {
+    int nx = 0;
+    std::vector<PNode> f;  // dX_i/dt over Var(X1[k]) and Par(a[j])
+};
+
+// Recognises a step body produced by the RK4 template (codegen.cpp:597-606 text form).
+// Returns false (with a reason) for any other body.
+bool recognize_rk4(const std::string& body, int nx, Rhs& out, std::string& why);
+
+// Parses one C expression of a KRS body (numbers, X1[k] / X[k], a[k], pi, euler,
+// calls, + - * /, unary minus, parentheses).
+PNode parse_c_expr(const std::string& text, const std::string& state);
+
+// Native device code.
+//   ucb_rhs(const numb* X1, const numb* a, numb* dX)
+//   ucb_jvp(const numb* X1, const numb* a, const numb* V, numb* dV)   (dV = J(X1) V)
+std::string emit_rhs_device(const Rhs& r, bool single_precision);
+std::string emit_jvp_device(const Rhs& r, bool single_precision);
+// Host C++ source of the same two functions for numb = double (used by the CPU tools).
+std::string emit_rhs_host(const Rhs& r);
+
+// Directional derivative d/ds f(x + s v) at s = 0 as an expression tree (V[k] as Par
+// nodes with index 1000 + k).
+PNode directional_derivative(const PNode& e);
+PNode simplify(const PNode& e);
+
+// Algorithmic FLOPs of an expression: + - * / count 1, negation 0, a call 1 plus its
+// arguments, pow with a small integer exponent as the multiplications it expands to.
+int flops(const PNode& e);
+int rhs_flops(const Rhs& r);
+// One RK4 step of the native integrator: 4 right-hand sides + 14 N updates
+// (3 stage updates of 2 N, the final combination of 8 N).
+int rk4_step_flops(const Rhs& r);
+int rk4_tangent_step_flops(const Rhs& r);
+
+}  // namespace fe
+}  // namespace ucb

@@ -1,0 +1,275 @@
+// ucb_device.cuh — device library shared by every integrator kernel (NVRTC header).
+//
+// Compiled together with a generated prelude that defines, at compile time:
+//   numb          state type (double: plain FP64 form; float: FP32 state form)
+//   UCB_NX        number of state variables (AMOUNTOFX of the reference)
+//   UCB_NV        number of entries of a[] (base_values, a[0] reserved)
+//   UCB_POV       sweep kind: 1 both axes parameters, 0 both initial conditions,
+//                 2 axis 0 an initial condition and axis 1 a parameter (par_or_var)
+//   UCB_IDX0/1    swept index of axis 0/1 (a[] index for parameters, X[] for states)
+//   UCB_HAXIS     axis that sweeps the step h (-1 none)
+//   UCB_DIM       1 or 2 sweep axes
+// and one stepper:
+//   exact form : calculateDiscreteModel(numb* X, const numb* a, numb h) — the KRS body
+//                verbatim, as the reference template splices it (lle2d.template.cu:60-63)
+//   native form: ucb_rhs(X1, a, dX) (+ ucb_jvp for tangent vectors) — the right-hand side
+//                recognised in the KRS body, integrated by the hand-written RK4 below.
+#pragma once
+
+#ifdef __CUDACC_RTC__
+typedef signed char int8_t;
+typedef unsigned char uint8_t;
+typedef short int16_t;
+typedef unsigned short uint16_t;
+typedef int int32_t;
+typedef unsigned int uint32_t;
+typedef long long int64_t;
+typedef unsigned long long uint64_t;
+#endif
+
+#ifndef UCB_DIM
+#define UCB_DIM 2
+#endif
+// 1: every loop call ends with the reference's extra step (cudaLibrary.cu:863-866),
+// 0: nominal step counts.
+#ifndef UCB_EXTRA_STEP
+#define UCB_EXTRA_STEP 1
+#endif
+
+namespace ucbdev {
+
+// configCUDA.h constants of the reference (CHECK_INTERVAL, eps_fixed_point, ...).
+constexpr int kCheckInterval = 100;
+constexpr double kEpsFixedPoint = 1e-8;
+constexpr double kEpsPeakDelta = 1e-14;
+constexpr double kPeakThreshold = -1e25;
+constexpr int kMaxAmountOfPeaks = 2500;
+
+// Sum of |x| and the divergence test of loopCalculateDiscreteModel_int
+// (cudaLibrary.cu:829-850): NaN/Inf, or above maxValue when maxValue != 0.
+__device__ __forceinline__ bool diverged(const numb* x, numb maxValue) {
+    numb checker = 0;
+#pragma unroll
+    for (int j = 0; j < UCB_NX; ++j) checker = checker + fabs(x[j]);
+    if (isnan(checker) || isinf(checker)) return true;
+    if (maxValue != 0 && fabs(checker) > maxValue) return true;
+    return false;
+}
+
+__device__ __forceinline__ int fixed_point_flag(const numb* x, const numb* xPrev) {
+    numb tempResult = 0;
+#pragma unroll
+    for (int j = 0; j < UCB_NX; ++j) tempResult += fabs(x[j] - xPrev[j]);
+    return (fabs(tempResult) < (numb)kEpsFixedPoint) ? -1 : 1;
+}
+
+// RNG stub of the reference templates (lle2d.template.cu:45-56): splitmix64 mixing of
+// (seed, subsequence, offset), then one LCG step per uniform in (0, 1].
+struct Rng {
+    unsigned long long state;
+};
+__device__ __forceinline__ void rng_init(unsigned long long seed, unsigned long long seq,
+                                         unsigned long long off, Rng* s) {
+    unsigned long long z = seed + seq * 0x9E3779B97F4A7C15ULL + off;
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ULL;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBULL;
+    s->state = z ^ (z >> 31);
+}
+__device__ __forceinline__ float rng_uniform(Rng* s) {
+    s->state = s->state * 6364136223846793005ULL + 1442695040888963407ULL;
+    return (float)(((s->state >> 40) & 0xFFFFFFULL) + 1ULL) / 16777216.0f;
+}
+
+// Random unit probe direction of one cell (LLEKernelCUDA, cudaLibrary.cu:2609-2628).
+__device__ __forceinline__ void probe_direction(unsigned long long seq, numb* z) {
+    Rng st;
+    rng_init(1234567891ULL, seq, 0ULL, &st);
+    numb zPower = 0;
+#pragma unroll
+    for (int i = 0; i < UCB_NX; ++i) {
+        z[i] = rng_uniform(&st) - 0.5;
+        zPower += z[i] * z[i];
+    }
+    zPower = sqrt(zPower);
+#pragma unroll
+    for (int i = 0; i < UCB_NX; ++i) z[i] /= zPower;
+}
+
+// ---------------------------------------------------------------------------
+// Steppers
+// ---------------------------------------------------------------------------
+#ifdef UCB_EXACT
+// The KRS body verbatim (the reference's calculateDiscreteModel slot).
+struct Stepper {
+    __device__ __forceinline__ explicit Stepper(numb) {}
+    __device__ __forceinline__ void step(numb* x, const numb* a, numb h) const {
+        calculateDiscreteModel(x, a, h);
+    }
+};
+#else
+// Classical RK4 on ucb_rhs, FMA-ordered: the same scheme as codegen.cpp scheme_rk4
+// (k1..k4 at t, t+h/2, t+h/2, t+h; x += h/6 (k1 + 2k2 + 2k3 + k4)) with the half/sixth
+// step factors hoisted and every update written as a fused multiply-add.
+struct Stepper {
+    numb hh, h6;
+    __device__ __forceinline__ explicit Stepper(numb h) : hh(h * (numb)0.5), h6(h * (numb)(1.0 / 6.0)) {}
+    __device__ __forceinline__ void step(numb* x, const numb* a, numb h) const {
+        numb k1[UCB_NX], k2[UCB_NX], k3[UCB_NX], k4[UCB_NX], xt[UCB_NX];
+        ucb_rhs(x, a, k1);
+#pragma unroll
+        for (int i = 0; i < UCB_NX; ++i) xt[i] = fma(hh, k1[i], x[i]);
+        ucb_rhs(xt, a, k2);
+#pragma unroll
+        for (int i = 0; i < UCB_NX; ++i) xt[i] = fma(hh, k2[i], x[i]);
+        ucb_rhs(xt, a, k3);
+#pragma unroll
+        for (int i = 0; i < UCB_NX; ++i) xt[i] = fma(h, k3[i], x[i]);
+        ucb_rhs(xt, a, k4);
+#pragma unroll
+        for (int i = 0; i < UCB_NX; ++i) x[i] = fma(h6, (k1[i] + k4[i]) + (numb)2 * (k2[i] + k3[i]), x[i]);
+    }
+#ifdef UCB_HAS_JVP
+    // RK4 of the tangent-linear system (x' = f(x), v' = J(x) v) in one sweep.
+    __device__ __forceinline__ void step_tangent(numb* x, numb* v, const numb* a, numb h) const {
+        numb k1[UCB_NX], k2[UCB_NX], k3[UCB_NX], k4[UCB_NX], xt[UCB_NX];
+        numb l1[UCB_NX], l2[UCB_NX], l3[UCB_NX], l4[UCB_NX], vt[UCB_NX];
+        ucb_rhs(x, a, k1);
+        ucb_jvp(x, a, v, l1);
+#pragma unroll
+        for (int i = 0; i < UCB_NX; ++i) { xt[i] = fma(hh, k1[i], x[i]); vt[i] = fma(hh, l1[i], v[i]); }
+        ucb_rhs(xt, a, k2);
+        ucb_jvp(xt, a, vt, l2);
+#pragma unroll
+        for (int i = 0; i < UCB_NX; ++i) { xt[i] = fma(hh, k2[i], x[i]); vt[i] = fma(hh, l2[i], v[i]); }
+        ucb_rhs(xt, a, k3);
+        ucb_jvp(xt, a, vt, l3);
+#pragma unroll
+        for (int i = 0; i < UCB_NX; ++i) { xt[i] = fma(h, k3[i], x[i]); vt[i] = fma(h, l3[i], v[i]); }
+        ucb_rhs(xt, a, k4);
+        ucb_jvp(xt, a, vt, l4);
+#pragma unroll
+        for (int i = 0; i < UCB_NX; ++i) {
+            x[i] = fma(h6, (k1[i] + k4[i]) + (numb)2 * (k2[i] + k3[i]), x[i]);
+            v[i] = fma(h6, (l1[i] + l4[i]) + (numb)2 * (l2[i] + l3[i]), v[i]);
+        }
+    }
+#endif
+};
+#endif
+
+// ---------------------------------------------------------------------------
+// loopCalculateDiscreteModel_int (cudaLibrary.cu:782-895) without recording:
+// `iters` steps, the divergence test after iterations 0, 100, 200, ... of this call,
+// then one extra step and the fixed-point test. 1 ok / -1 fixed point / 0 diverged.
+// ---------------------------------------------------------------------------
+template <class S>
+__device__ __forceinline__ int loop_single(const S& s, numb* x, const numb* a, numb h, long long iters,
+                                           numb maxValue, long long& ns) {
+    for (long long i0 = 0; i0 < iters; i0 += kCheckInterval) {
+        s.step(x, a, h);
+        ns += 1;
+        if (diverged(x, maxValue)) return 0;
+        const long long n = (iters - i0 < kCheckInterval) ? iters - i0 : kCheckInterval;
+        for (long long i = 1; i < n; ++i) s.step(x, a, h);
+        ns += n - 1;
+    }
+#if UCB_EXTRA_STEP
+    numb xPrev[UCB_NX];
+#pragma unroll
+    for (int j = 0; j < UCB_NX; ++j) xPrev[j] = x[j];
+    s.step(x, a, h);
+    ns += 1;
+    return fixed_point_flag(x, xPrev);
+#else
+    return 1;
+#endif
+}
+
+// Two independent trajectories advanced together (the trajectory and its shadow in
+// LLEKernelCUDA, :2646-2658). The reference runs them one after the other; advancing
+// them in lock step gives the same numbers (they never interact inside a block) and
+// two independent dependency chains per thread. Returns 0 if either diverged.
+template <class S>
+__device__ __forceinline__ int loop_pair(const S& s, numb* x, numb* y, const numb* a, numb h,
+                                         long long iters, numb maxValue, long long& ns) {
+    for (long long i0 = 0; i0 < iters; i0 += kCheckInterval) {
+        s.step(x, a, h);
+        s.step(y, a, h);
+        ns += 2;
+        if (diverged(x, maxValue) || diverged(y, maxValue)) return 0;
+        const long long n = (iters - i0 < kCheckInterval) ? iters - i0 : kCheckInterval;
+        for (long long i = 1; i < n; ++i) {
+            s.step(x, a, h);
+            s.step(y, a, h);
+        }
+        ns += 2 * (n - 1);
+    }
+#if UCB_EXTRA_STEP
+    s.step(x, a, h);
+    s.step(y, a, h);
+    ns += 2;
+#endif
+    return 1;
+}
+
+// ---------------------------------------------------------------------------
+// Cell set-up: sweep values of one cell (the par_or_var branches of LLEKernelCUDA
+// :2565-2588 / calculateDiscreteModelCUDA :1035-1058). Axis values come from host
+// tables computed with the reference's getValueByIdx(_log) formula in numb.
+// ---------------------------------------------------------------------------
+struct CellAxes {
+    int i0, i1;
+};
+
+__device__ __forceinline__ CellAxes cell_axes(long long idx, int n) {
+    CellAxes c;
+    c.i0 = (int)(idx % n);
+#if UCB_DIM == 2
+    c.i1 = (int)((idx / n) % n);
+#else
+    c.i1 = 0;
+#endif
+    return c;
+}
+
+__device__ __forceinline__ void apply_sweep(const CellAxes& c, const numb* ax0, const numb* ax1, numb* x,
+                                            numb* a) {
+#if UCB_POV == 1
+#if UCB_HAXIS != 0
+    a[UCB_IDX0] = ax0[c.i0];
+#endif
+#if UCB_DIM == 2 && UCB_HAXIS != 1
+    a[UCB_IDX1] = ax1[c.i1];
+#endif
+#elif UCB_POV == 0
+#if UCB_HAXIS != 0
+    x[UCB_IDX0] = ax0[c.i0];
+#endif
+#if UCB_DIM == 2 && UCB_HAXIS != 1
+    x[UCB_IDX1] = ax1[c.i1];
+#endif
+#elif UCB_POV == 2
+    x[UCB_IDX0] = ax0[c.i0];
+    a[UCB_IDX1] = ax1[c.i1];
+#endif
+}
+
+// Adds the per-thread work counts of a warp into a global counter (one atomic per warp).
+__device__ __forceinline__ void warp_add_steps(unsigned long long* counter, long long ns, int lane) {
+    unsigned long long v = (unsigned long long)ns;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+    if (lane == 0 && counter) atomicAdd(counter, v);
+}
+
+// Work distribution: one warp takes 32 consecutive cells per atomic fetch from a
+// device counter, so cells of uneven cost (divergence, early exit) balance across a
+// persistent grid. The counter is zeroed by the host before each launch.
+__device__ __forceinline__ long long warp_fetch(unsigned long long* counter, int lane) {
+    unsigned long long base = 0;
+    if (lane == 0) base = atomicAdd(counter, 32ULL);
+    base = __shfl_sync(0xffffffffu, base, 0);
+    return (long long)base;
+}
+
+}  // namespace ucbdev

@@ -1,0 +1,200 @@
+// ucb_lle.cuh — largest Lyapunov exponent maps (NVRTC header, after ucb_device.cuh).
+//
+// One thread per cell, state and shadow (or tangent vector) in registers, persistent
+// grid fed by a warp-granular atomic work counter. Semantics per cell follow
+// LLEKernelCUDA (cudaLibrary.cu:2486-2693):
+//   transient (skip steps, 999 on divergence) -> random unit probe z (RNG subsequence
+//   = cell index) -> shadow y = x + eps z -> n_blocks x { advance x and y by nt_steps,
+//   d = |(1/eps)(x - y)|, floor 1e-14, sum += log d, y = x - (x - y + 1e-14)/d }
+//   -> lambda = sum / tMax.
+// Output: values[out] (double) and flags[out] = -1 for the 999 sentinel, 1 otherwise,
+// where out is the cell index in the user's row-major order (swap_xy transposes, as
+// run_lle_2d does on the host, parametric_engine.cpp:2913-2928).
+#pragma once
+
+struct UcbLleParams {
+    long long total;          // cells in this launch
+    long long cell_offset;    // first cell index (kernel order)
+    int n_pts;                // grid side
+    int swap_xy;              // 1: write transposed (user X = kernel axis 1)
+    int n_blocks;             // (int)(tMax / NT), host double arithmetic
+    int pad0;
+    long long skip;           // (int)(transientTime / h), host double arithmetic
+    long long nt_steps;       // (size_t)(NT / h) in numb
+    numb h, NT, tmax, eps, maxv, transient;
+    numb ic[UCB_NX];
+    numb vals[UCB_NV];
+    const numb* axis0;        // n_pts values of kernel axis 0
+    const numb* axis1;        // n_pts values of kernel axis 1
+    double* out_values;
+    int* out_flags;
+    unsigned long long* counter;   // work counter, zeroed before launch
+    unsigned long long* steps;     // step evaluations performed (accumulated)
+};
+
+namespace ucbdev {
+
+__device__ __forceinline__ void store_cell(const UcbLleParams& p, long long kidx, double v) {
+    long long out = kidx;
+    if (p.swap_xy) {
+        const long long kix = kidx % p.n_pts, kiy = kidx / p.n_pts;
+        out = kix * p.n_pts + kiy;
+    }
+    p.out_values[out] = v;
+    p.out_flags[out] = (v == 999.0 || v == -999.0) ? -1 : 1;
+}
+
+// Per-cell step size and step counts (dt-sweep axis: LLEKernelCUDA :2525-2548).
+struct CellSteps {
+    numb h;
+    long long nt, skip;
+};
+
+__device__ __forceinline__ CellSteps cell_steps(const UcbLleParams& p, const CellAxes& c) {
+    CellSteps s;
+    s.h = p.h;
+    s.nt = p.nt_steps;
+    s.skip = p.skip;
+#if UCB_HAXIS == 0
+    s.h = p.axis0[c.i0];
+#elif UCB_HAXIS == 1
+    s.h = p.axis1[c.i1];
+#endif
+#if UCB_HAXIS != -1
+    s.nt = (long long)ceil(p.NT / s.h);
+    s.skip = (long long)ceil(p.transient / s.h);
+#endif
+    return s;
+}
+
+__device__ __forceinline__ double lle_cell_shadow(const UcbLleParams& p, long long kidx, long long& ns) {
+    const CellAxes c = cell_axes(kidx, p.n_pts);
+    const CellSteps cs = cell_steps(p, c);
+    if (!(cs.h > 0)) return (double)nan("");
+    numb x[UCB_NX], y[UCB_NX], a[UCB_NV];
+#pragma unroll
+    for (int i = 0; i < UCB_NX; ++i) x[i] = p.ic[i];
+#pragma unroll
+    for (int i = 0; i < UCB_NV; ++i) a[i] = p.vals[i];
+    apply_sweep(c, p.axis0, p.axis1, x, a);
+    const Stepper st(cs.h);
+    if (loop_single(st, x, a, cs.h, cs.skip, p.maxv, ns) == 0) return 999.0;
+    numb z[UCB_NX];
+    probe_direction((unsigned long long)kidx, z);
+#pragma unroll
+    for (int i = 0; i < UCB_NX; ++i) y[i] = z[i] * p.eps + x[i];
+    numb result = 0;
+    const numb inv_eps = (numb)1.0 / p.eps;
+    for (int b = 0; b < p.n_blocks; ++b) {
+        if (loop_pair(st, x, y, a, cs.h, cs.nt, p.maxv, ns) == 0) return 999.0;
+        numb tempData = 0;
+#pragma unroll
+        for (int l = 0; l < UCB_NX; ++l) {
+            const numb t = inv_eps * (x[l] - y[l]);
+            tempData += t * t;
+        }
+        tempData = sqrt(tempData);
+        if (tempData <= 1e-14) tempData = (numb)1e-14;
+        result += log(tempData);
+        tempData = (1 / tempData);
+#pragma unroll
+        for (int j = 0; j < UCB_NX; ++j) y[j] = (numb)(x[j] - ((x[j] - y[j] + 1e-14) * tempData));
+    }
+    return (double)(result / p.tmax);
+}
+
+#if defined(UCB_HAS_JVP) && !defined(UCB_EXACT)
+// Tangent-vector form: the shadow trajectory is replaced by the tangent-linear
+// vector v (v' = J(x) v, same RK4 sweep as x, same step counts including the extra
+// step), started from the same random unit direction. Norms and the log sum are
+// accumulated in FP64, so the state can be FP32 without the cancellation that an
+// FP32 shadow difference x - y of size eps would suffer.
+template <class S>
+__device__ __forceinline__ int loop_tangent(const S& s, numb* x, numb* v, const numb* a, numb h,
+                                            long long iters, numb maxValue, long long& ns) {
+    for (long long i0 = 0; i0 < iters; i0 += kCheckInterval) {
+        s.step_tangent(x, v, a, h);
+        ns += 2;
+        if (diverged(x, maxValue) || diverged(v, (numb)0)) return 0;
+        const long long n = (iters - i0 < kCheckInterval) ? iters - i0 : kCheckInterval;
+        for (long long i = 1; i < n; ++i) s.step_tangent(x, v, a, h);
+        ns += 2 * (n - 1);
+    }
+#if UCB_EXTRA_STEP
+    s.step_tangent(x, v, a, h);
+    ns += 2;
+#endif
+    return 1;
+}
+
+__device__ __forceinline__ double lle_cell_tangent(const UcbLleParams& p, long long kidx, long long& ns) {
+    const CellAxes c = cell_axes(kidx, p.n_pts);
+    const CellSteps cs = cell_steps(p, c);
+    if (!(cs.h > 0)) return (double)nan("");
+    numb x[UCB_NX], v[UCB_NX], a[UCB_NV];
+#pragma unroll
+    for (int i = 0; i < UCB_NX; ++i) x[i] = p.ic[i];
+#pragma unroll
+    for (int i = 0; i < UCB_NV; ++i) a[i] = p.vals[i];
+    apply_sweep(c, p.axis0, p.axis1, x, a);
+    const Stepper st(cs.h);
+    if (loop_single(st, x, a, cs.h, cs.skip, p.maxv, ns) == 0) return 999.0;
+    probe_direction((unsigned long long)kidx, v);
+    double result = 0.0;
+    for (int b = 0; b < p.n_blocks; ++b) {
+        if (loop_tangent(st, x, v, a, cs.h, cs.nt, p.maxv, ns) == 0) return 999.0;
+        double d2 = 0.0;
+#pragma unroll
+        for (int l = 0; l < UCB_NX; ++l) d2 = fma((double)v[l], (double)v[l], d2);
+        double d = sqrt(d2);
+        if (d <= 1e-14) d = 1e-14;
+        result += log(d);
+        const numb inv = (numb)(1.0 / d);
+#pragma unroll
+        for (int j = 0; j < UCB_NX; ++j) v[j] *= inv;
+    }
+    return result / (double)p.tmax;
+}
+#endif
+
+}  // namespace ucbdev
+
+extern "C" __global__ void __launch_bounds__(128) ucb_lle_kernel(const UcbLleParams p) {
+    const int lane = threadIdx.x & 31;
+    long long ns = 0;
+    for (;;) {
+        const long long base = ucbdev::warp_fetch(p.counter, lane);
+        if (base >= p.total) break;
+        const long long i = base + lane;
+        if (i < p.total) {
+            const long long kidx = p.cell_offset + i;
+#if defined(UCB_TANGENT)
+            const double v = ucbdev::lle_cell_tangent(p, kidx, ns);
+#else
+            const double v = ucbdev::lle_cell_shadow(p, kidx, ns);
+#endif
+            ucbdev::store_cell(p, kidx, v);
+        }
+    }
+    ucbdev::warp_add_steps(p.steps, ns, lane);
+}
+
+// Final state of every cell after `skip` plain steps from its initial condition (no
+// divergence checks, no extra step): a trajectory-parity aid over the same grid.
+extern "C" __global__ void __launch_bounds__(128) ucb_state_kernel(const UcbLleParams p) {
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= p.total) return;
+    const long long kidx = p.cell_offset + i;
+    const ucbdev::CellAxes c = ucbdev::cell_axes(kidx, p.n_pts);
+    const ucbdev::CellSteps cs = ucbdev::cell_steps(p, c);
+    numb x[UCB_NX], a[UCB_NV];
+#pragma unroll
+    for (int k = 0; k < UCB_NX; ++k) x[k] = p.ic[k];
+#pragma unroll
+    for (int k = 0; k < UCB_NV; ++k) a[k] = p.vals[k];
+    ucbdev::apply_sweep(c, p.axis0, p.axis1, x, a);
+    const ucbdev::Stepper st(cs.h);
+    for (long long s = 0; s < p.skip; ++s) st.step(x, a, cs.h);
+#pragma unroll
+    for (int k = 0; k < UCB_NX; ++k) p.out_values[i * UCB_NX + k] = (double)x[k];
+}

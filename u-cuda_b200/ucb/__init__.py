@@ -1,0 +1,236 @@
+"""Python binding of the engine's C ABI (include/ucb.h) through ctypes.
+
+The hot path runs in libucb.so (this directory): NVRTC-compiled sm_100a integrator
+kernels driven by the C++ host code. There is no CPU fallback: every entry point fails
+loudly when the library or a GPU is missing.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from pathlib import Path
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+LIB_PATH = HERE / "libucb.so"
+
+UCB_OK, UCB_E_INVALID, UCB_E_COMPILE, UCB_E_CUDA, UCB_E_CANCELLED, UCB_E_NOGPU = range(6)
+PREC_F64, PREC_F32 = 0, 1
+MODE_NATIVE, MODE_EXACT = 0, 1
+LLE_AUTO, LLE_SHADOW, LLE_TANGENT = 0, 1, 2
+
+
+class UcbError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__(f"[ucb error {code}] {msg}")
+        self.code = code
+
+
+class Options(C.Structure):
+    _fields_ = [("precision", C.c_int32), ("mode", C.c_int32), ("lle_method", C.c_int32),
+                ("nominal_steps", C.c_int32), ("block_threads", C.c_int32), ("reserved", C.c_int32 * 3)]
+
+
+class Lle2dRequest(C.Structure):
+    _fields_ = [
+        ("krs_body", C.c_char_p), ("amount_of_x", C.c_int32),
+        ("initial_conditions", C.POINTER(C.c_double)), ("base_values", C.POINTER(C.c_double)),
+        ("n_values", C.c_int32),
+        ("sweep_over_var", C.c_int32), ("sweep_over_var_2", C.c_int32),
+        ("sweep_over_h", C.c_int32), ("sweep_over_h_2", C.c_int32),
+        ("log_scale", C.c_int32), ("log_scale_2", C.c_int32),
+        ("param_index", C.c_int32), ("var_sweep_index", C.c_int32),
+        ("param_index_2", C.c_int32), ("var_sweep_index_2", C.c_int32),
+        ("param_lo", C.c_double), ("param_hi", C.c_double), ("param_lo_2", C.c_double), ("param_hi_2", C.c_double),
+        ("n_pts", C.c_int32),
+        ("h", C.c_double), ("transient_time", C.c_double), ("t_max", C.c_double), ("NT", C.c_double),
+        ("eps", C.c_double), ("max_value", C.c_double),
+        ("csv_output_path", C.c_char_p),
+        ("cancel", C.POINTER(C.c_int32)), ("progress", C.POINTER(C.c_float)),
+        ("opt", Options),
+    ]
+
+
+class Lle2dResult(C.Structure):
+    _fields_ = [
+        ("values", C.POINTER(C.c_double)), ("flags", C.POINTER(C.c_int32)),
+        ("ok", C.c_int32), ("cancelled", C.c_int32), ("n_pts", C.c_int32),
+        ("param_lo", C.c_double), ("param_hi", C.c_double), ("param_lo_2", C.c_double), ("param_hi_2", C.c_double),
+        ("min_val", C.c_double), ("max_val", C.c_double), ("kernel_ms", C.c_double), ("steps", C.c_longlong),
+        ("flops", C.c_double), ("error", C.c_char * 1024),
+    ]
+
+
+_lib = None
+
+
+def load():
+    """Loads libucb.so (building it first if it is missing and nvcc is available)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not LIB_PATH.exists():
+        import importlib.util
+        spec = importlib.util.spec_from_file_location("ucb_build", HERE.parent / "build.py")
+        mod = importlib.util.module_from_spec(spec)
+        spec.loader.exec_module(mod)
+        mod.build()
+    L = C.CDLL(str(LIB_PATH))
+    L.ucb_create.restype = C.c_void_p
+    L.ucb_create.argtypes = [C.c_int]
+    L.ucb_destroy.argtypes = [C.c_void_p]
+    L.ucb_last_error.restype = C.c_char_p
+    L.ucb_last_error.argtypes = [C.c_void_p]
+    L.ucb_abi_version.restype = C.c_int
+    L.ucb_kernel_launches.restype = C.c_longlong
+    L.ucb_kernel_launches.argtypes = [C.c_void_p]
+    L.ucb_clear_cache.argtypes = [C.c_void_p]
+    L.ucb_default_options.argtypes = [C.POINTER(Options)]
+    L.ucb_run_lle2d.restype = C.c_int
+    L.ucb_run_lle2d.argtypes = [C.c_void_p, C.POINTER(Lle2dRequest), C.POINTER(Lle2dResult)]
+    L.ucb_lle2d_device.restype = C.c_int
+    L.ucb_lle2d_device.argtypes = [C.c_void_p, C.POINTER(Lle2dRequest), C.c_void_p, C.c_void_p, C.c_void_p,
+                                   C.POINTER(Lle2dResult)]
+    L.ucb_lle2d_states.restype = C.c_int
+    L.ucb_lle2d_states.argtypes = [C.c_void_p, C.POINTER(Lle2dRequest), C.c_longlong, C.c_void_p]
+    L.ucb_measure_fma_peak.restype = C.c_int
+    L.ucb_measure_fma_peak.argtypes = [C.c_int, C.POINTER(C.c_double)]
+    L.ucb_codegen.restype = C.c_int
+    L.ucb_codegen.argtypes = [C.c_char_p, C.c_char_p, C.c_int, C.c_char_p, C.c_int, C.c_char_p, C.c_int,
+                              C.c_char_p, C.c_int, C.c_char_p, C.c_int]
+    L.ucb_precompile_lle2d.restype = C.c_int
+    L.ucb_precompile_lle2d.argtypes = [C.POINTER(Lle2dRequest), C.c_char_p, C.c_int]
+    _lib = L
+    return L
+
+
+def _dptr(a):
+    return a.ctypes.data_as(C.POINTER(C.c_double))
+
+
+def options(precision=PREC_F64, mode=MODE_NATIVE, lle_method=LLE_AUTO, nominal_steps=False, block_threads=0):
+    o = Options()
+    load().ucb_default_options(C.byref(o))
+    o.precision, o.mode, o.lle_method = precision, mode, lle_method
+    o.nominal_steps, o.block_threads = int(nominal_steps), block_threads
+    return o
+
+
+class Engine:
+    """One engine object per device (the reference's ParametricEngine)."""
+
+    def __init__(self, device: int = 0):
+        self.lib = load()
+        self.h = self.lib.ucb_create(device)
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.ucb_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def launches(self) -> int:
+        return int(self.lib.ucb_kernel_launches(self.h))
+
+    def last_error(self) -> str:
+        return self.lib.ucb_last_error(self.h).decode()
+
+    # ------------------------------------------------------------------ LLE 2D
+    @staticmethod
+    def lle2d_request(krs_body: str, amount_of_x: int, initial_conditions, base_values, *, n_pts,
+                      param_index=0, param_index_2=0, var_sweep_index=0, var_sweep_index_2=0,
+                      sweep_over_var=False, sweep_over_var_2=False, sweep_over_h=False, sweep_over_h_2=False,
+                      log_scale=False, log_scale_2=False, param_lo=0.0, param_hi=1.0, param_lo_2=0.0,
+                      param_hi_2=1.0, h=0.01, transient_time=0.0, t_max=100.0, NT=1.0, eps=1e-4,
+                      max_value=1e6, csv_output_path=None, opt: Options | None = None):
+        ic = np.ascontiguousarray(initial_conditions, dtype=np.float64)
+        vals = np.ascontiguousarray(base_values, dtype=np.float64)
+        r = Lle2dRequest()
+        r._keep = (ic, vals, krs_body.encode())
+        r.krs_body = r._keep[2]
+        r.amount_of_x = amount_of_x
+        r.initial_conditions = _dptr(ic)
+        r.base_values = _dptr(vals)
+        r.n_values = len(vals)
+        r.sweep_over_var, r.sweep_over_var_2 = int(sweep_over_var), int(sweep_over_var_2)
+        r.sweep_over_h, r.sweep_over_h_2 = int(sweep_over_h), int(sweep_over_h_2)
+        r.log_scale, r.log_scale_2 = int(log_scale), int(log_scale_2)
+        r.param_index, r.var_sweep_index = param_index, var_sweep_index
+        r.param_index_2, r.var_sweep_index_2 = param_index_2, var_sweep_index_2
+        r.param_lo, r.param_hi, r.param_lo_2, r.param_hi_2 = param_lo, param_hi, param_lo_2, param_hi_2
+        r.n_pts = n_pts
+        r.h, r.transient_time, r.t_max, r.NT, r.eps, r.max_value = h, transient_time, t_max, NT, eps, max_value
+        r.csv_output_path = csv_output_path.encode() if csv_output_path else None
+        r.opt = opt if opt is not None else options()
+        return r
+
+    def run_lle2d(self, req: Lle2dRequest, values=None, flags=None):
+        n = req.n_pts
+        if values is None:
+            values = np.empty(max(n, 0) ** 2, dtype=np.float64)
+        if flags is None:
+            flags = np.empty(max(n, 0) ** 2, dtype=np.int32)
+        res = Lle2dResult()
+        res.values = _dptr(values)
+        res.flags = flags.ctypes.data_as(C.POINTER(C.c_int32))
+        rc = self.lib.ucb_run_lle2d(self.h, C.byref(req), C.byref(res))
+        if rc != UCB_OK:
+            raise UcbError(rc, res.error.decode())
+        return values, flags, res
+
+    def lle2d_states(self, req: Lle2dRequest, n_steps: int):
+        n = req.n_pts
+        out = np.empty(n * n * req.amount_of_x, dtype=np.float64)
+        rc = self.lib.ucb_lle2d_states(self.h, C.byref(req), n_steps, out.ctypes.data_as(C.c_void_p))
+        if rc != UCB_OK:
+            raise UcbError(rc, self.last_error())
+        return out.reshape(n * n, req.amount_of_x)
+
+    def lle2d_device(self, req: Lle2dRequest, d_values_ptr: int, d_flags_ptr: int, stream_ptr: int = 0):
+        res = Lle2dResult()
+        rc = self.lib.ucb_lle2d_device(self.h, C.byref(req), C.c_void_p(d_values_ptr), C.c_void_p(d_flags_ptr),
+                                       C.c_void_p(stream_ptr), C.byref(res))
+        if rc != UCB_OK:
+            raise UcbError(rc, res.error.decode())
+        return res
+
+
+def precompile_lle2d(req: Lle2dRequest) -> str:
+    buf = C.create_string_buffer(65536)
+    rc = load().ucb_precompile_lle2d(C.byref(req), buf, len(buf))
+    if rc != UCB_OK:
+        raise UcbError(rc, buf.value.decode(errors="replace"))
+    return buf.value.decode(errors="replace")
+
+
+def measure_fma_peak(precision=PREC_F64) -> float:
+    """FMA-pipe throughput of the current device in TFLOP/s (roofline denominator)."""
+    v = C.c_double(0)
+    rc = load().ucb_measure_fma_peak(precision, C.byref(v))
+    if rc != UCB_OK:
+        raise UcbError(rc, "fma probe failed")
+    return v.value
+
+
+SCHEMES = {"Euler": 0, "Euler-Cromer": 1, "Explicit Midpoint": 2, "RK4": 3}
+
+
+def codegen(text: str, alphabet: str, scheme: str = "RK4", order_as_in_system=False, func_defs: str | None = None):
+    """System text -> (step body, variables, parameters)."""
+    out = C.create_string_buffer(1 << 20)
+    vs = C.create_string_buffer(4096)
+    ps = C.create_string_buffer(4096)
+    rc = load().ucb_codegen(text.encode(), alphabet.encode(), int(order_as_in_system),
+                            func_defs.encode() if func_defs else None, SCHEMES[scheme], out, len(out), vs, len(vs),
+                            ps, len(ps))
+    if rc != UCB_OK:
+        raise UcbError(rc, out.value.decode())
+    split = lambda b: [x for x in b.value.decode().split(",") if x]
+    return out.value.decode(), split(vs), split(ps)
