@@ -139,6 +139,51 @@ UCB_API int ucb_run_lle2d(ucb_engine* e, const ucb_lle2d_request* req, ucb_lle2d
 UCB_API int ucb_lle2d_device(ucb_engine* e, const ucb_lle2d_request* req, double* d_values, int32_t* d_flags,
                      void* stream, ucb_lle2d_result* res);
 
+/* ------------------------------------------------------------------------------------
+ * Bifurcation 1D — replaces ParametricEngine::run_bifurcation_1d (parametric_engine.h:27-126,
+ * :853; classical sweep of parametric_engine.cpp:1674-2091; the continuation branch is
+ * sequential by construction and not part of this path).
+ * ---------------------------------------------------------------------------------- */
+typedef struct ucb_bif1d_request {
+    const char* krs_body;
+    int32_t amount_of_x;
+    const double* initial_conditions;
+    const double* base_values;
+    int32_t n_values;
+    int32_t param_index;      /* 1-based a[] index (parameter sweep) */
+    int32_t sweep_over_var;   /* sweep initial condition var_sweep_index instead */
+    int32_t var_sweep_index;
+    int32_t sweep_over_h;     /* sweep the step h over [param_lo, param_hi] */
+    int32_t log_scale;
+    double param_lo, param_hi;
+    int32_t n_pts;
+    int32_t writable_var;     /* recorded variable; -1 = x0 + pi x1 + e x2 */
+    double h, transient_time, t_max;
+    int32_t pre_scaller;
+    double max_value;
+    int32_t max_peaks;        /* peaks/intervals kept per point (the reference keeps up to 2500) */
+    const char* csv_output_path;
+    const volatile int32_t* cancel;
+    volatile float* progress;
+    ucb_options opt;
+} ucb_bif1d_request;
+
+typedef struct ucb_bif1d_result {
+    /* caller-allocated: counts[n_pts], peaks[n_pts * max_peaks], intervals[n_pts * max_peaks] */
+    int32_t* counts;          /* the reference's flags[]: number of peaks (<= 2500), -1 fixed
+                                 point, 0 diverged; peaks beyond max_peaks are counted, not stored */
+    double* peaks;            /* peak values (first peak of the series dropped) */
+    double* intervals;        /* inter-peak intervals (time units) */
+    int32_t ok, cancelled, n_pts, record_steps;
+    double param_lo, param_hi;
+    double kernel_ms;
+    long long steps;
+    double flops;
+    char error[1024];
+} ucb_bif1d_result;
+
+UCB_API int ucb_run_bif1d(ucb_engine* e, const ucb_bif1d_request* req, ucb_bif1d_result* res);
+
 /* Trajectory parity aid: integrates every cell of the request's grid (same sweep
  * mapping, same step function and precision as ucb_run_lle2d) for n_steps plain steps
  * from its initial condition — no transient, no divergence checks, no extra step — and

@@ -1,0 +1,113 @@
+"""GPU parity of the fused bifurcation kernel (integration + streaming peak capture)
+against the oracle's restatement of calculateDiscreteModelCUDA + peakFinder.
+
+Exact form: bit-identical recorded series, hence identical peak counts and peak/interval
+values (the interpolation runs with the same operation order and no FMA contraction).
+Native form: counts and peaks agree exactly on the transient-free short horizon of
+periodic points; on chaotic points the peak sets sample the same attractor (checked via
+the Hausdorff distance of the peak sets)."""
+import numpy as np
+import pytest
+
+import ucb
+from helpers import LORENZ, rk4_body
+from oracle import oracle as O
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def eng():
+    e = ucb.Engine(0)
+    yield e
+    e.close()
+
+
+def case(**kw):
+    d = dict(body=rk4_body(LORENZ), nx=3, ic=(0.1, 0.1, 0.1), values=(0, 10.0, 28.0, 8 / 3), n_pts=64,
+             param_index=2, param_lo=20.0, param_hi=200.0, h=0.01, transient_time=10.0, t_max=40.0,
+             writable_var=0, pre_scaller=1, max_value=1e6, max_peaks=64)
+    d.update(kw)
+    return d
+
+
+def run_both(eng, c, **opt):
+    req = ucb.Engine.bif1d_request(c["body"], c["nx"], c["ic"], c["values"], n_pts=c["n_pts"],
+                                   param_index=c["param_index"], param_lo=c["param_lo"], param_hi=c["param_hi"],
+                                   h=c["h"], transient_time=c["transient_time"], t_max=c["t_max"],
+                                   writable_var=c["writable_var"], pre_scaller=c["pre_scaller"],
+                                   max_value=c["max_value"], max_peaks=c["max_peaks"],
+                                   sweep_over_var=c.get("sweep_over_var", False),
+                                   var_sweep_index=c.get("var_sweep_index", 0),
+                                   sweep_over_h=c.get("sweep_over_h", False), log_scale=c.get("log_scale", False),
+                                   opt=ucb.options(**opt))
+    counts, peaks, intervals, res = eng.run_bif1d(req)
+    b = dict(n_pts=c["n_pts"], sweep_kind=2 if c.get("sweep_over_h") else (1 if c.get("sweep_over_var") else 0),
+             sweep_index=c.get("var_sweep_index", 0) if c.get("sweep_over_var") else c["param_index"],
+             lo=c["param_lo"], hi=c["param_hi"], log_scale=c.get("log_scale", False), ic=c["ic"], values=c["values"],
+             h=c["h"], transient_time=c["transient_time"], t_max=c["t_max"], pre_scaller=c["pre_scaller"],
+             writable_var=c["writable_var"], max_value=c["max_value"])
+    numb = "f64" if opt.get("precision", 0) == ucb.PREC_F64 else "f32"
+    oc, op, oi = O.bif1d(O.Krs(c["body"], 3, numb), b, max_out=c["max_peaks"])
+    return (counts, peaks, intervals, res), (oc, op, oi)
+
+
+@pytest.mark.parametrize("variant", ["base", "writable_combo", "prescaller", "ic_sweep", "log", "h_sweep", "few"])
+def test_exact_bifurcation_matches_oracle(eng, variant):
+    kw = {}
+    if variant == "writable_combo":
+        kw = dict(writable_var=-1)
+    elif variant == "prescaller":
+        kw = dict(pre_scaller=3, t_max=60.0)
+    elif variant == "ic_sweep":
+        kw = dict(sweep_over_var=True, var_sweep_index=2, param_lo=-5.0, param_hi=5.0)
+    elif variant == "log":
+        kw = dict(log_scale=True, param_lo=1.0, param_hi=300.0)
+    elif variant == "h_sweep":
+        kw = dict(sweep_over_h=True, param_lo=0.005, param_hi=0.02)
+    elif variant == "few":
+        kw = dict(max_peaks=3, n_pts=5)
+    c = case(**kw)
+    (counts, peaks, intervals, res), (oc, op, oi) = run_both(eng, c, precision=ucb.PREC_F64, mode=ucb.MODE_EXACT)
+    np.testing.assert_array_equal(counts, oc)
+    m = np.isfinite(op)
+    np.testing.assert_array_equal(np.isfinite(peaks), m)
+    np.testing.assert_array_equal(peaks[m], op[m])
+    np.testing.assert_array_equal(intervals[m], oi[m])
+    assert (counts > 0).any()
+
+
+def test_exact_f32_bifurcation_matches_oracle(eng):
+    c = case(n_pts=32)
+    (counts, peaks, intervals, _), (oc, op, oi) = run_both(eng, c, precision=ucb.PREC_F32, mode=ucb.MODE_EXACT)
+    np.testing.assert_array_equal(counts, oc)
+    m = np.isfinite(op)
+    np.testing.assert_array_equal(peaks[m], op[m])
+
+
+def test_fixed_point_and_divergence_flags(eng):
+    # rho < 1: the origin is a stable fixed point (count -1); a tiny max_value forces 0.
+    c = case(n_pts=4, param_lo=0.2, param_hi=0.8)
+    (counts, _, _, _), (oc, _, _) = run_both(eng, c, precision=ucb.PREC_F64, mode=ucb.MODE_EXACT)
+    np.testing.assert_array_equal(counts, oc)
+    assert (counts == -1).all()
+    c = case(n_pts=4, max_value=1.0)
+    (counts, _, _, _), (oc, _, _) = run_both(eng, c, precision=ucb.PREC_F64, mode=ucb.MODE_EXACT)
+    np.testing.assert_array_equal(counts, oc)
+    assert (counts == 0).all()
+
+
+def hausdorff(a, b):
+    if len(a) == 0 or len(b) == 0:
+        return 0.0 if len(a) == len(b) else np.inf
+    d = np.abs(a[:, None] - b[None, :])
+    return max(d.min(axis=1).max(), d.min(axis=0).max())
+
+
+def test_native_bifurcation_peak_sets(eng):
+    c = case(n_pts=64, t_max=100.0, transient_time=50.0)
+    (counts, peaks, _, _), (oc, op, _) = run_both(eng, c, precision=ucb.PREC_F64, mode=ucb.MODE_NATIVE)
+    # peak sets of the same point sample the same attractor
+    hd = [hausdorff(peaks[i][np.isfinite(peaks[i])], op[i][np.isfinite(op[i])]) for i in range(64)]
+    assert np.median(hd) < 2.0
+    assert (np.sign(counts) == np.sign(oc)).mean() > 0.95

@@ -1,0 +1,30 @@
+// CSV output of the run_* entry points: the reference's data_export wire format
+// (data_export.cpp — *_config.csv headers and the grid / row layouts), so that results
+// drop into existing post-processing unchanged.
+#pragma once
+
+#include <string>
+#include <vector>
+
+namespace ucb {
+namespace csv {
+
+struct Common {
+    std::vector<double> values;  // a[]
+    std::vector<double> ic;      // X0[]
+};
+
+void bif1d(const std::string& path, const Common& c, double tMax, double transient, double h, int pre,
+           int writable_var, int index_of_mut_var, double lo, double hi, int n_pts, const int* counts,
+           const double* peaks, const double* intervals, int max_peaks);
+
+void lle2d(const std::string& path, const Common& c, int par_or_var, double tMax, double NT, double transient,
+           double h, double eps, int idx1, int idx2, double r1lo, double r1hi, double r2lo, double r2hi, int n_pts,
+           const double* values);
+
+void ls2d(const std::string& path, const Common& c, int par_or_var, double tMax, double NT, double transient,
+          double h, double eps, int idx1, int idx2, double r1lo, double r1hi, double r2lo, double r2hi, int n_pts,
+          int n_exp, const double* plane_major_values);
+
+}  // namespace csv
+}  // namespace ucb

@@ -69,6 +69,30 @@ const std::vector<std::pair<std::string, std::string>>& device_headers();
 void axis_table(int precision, int n, double lo, double hi, bool log_scale, std::vector<double>& out_d,
                 std::vector<float>& out_f);
 
+// Packs a kernel parameter struct field by field with natural alignment (the layout a
+// single by-value struct parameter has on the device).
+struct ParamPack {
+    std::vector<char> buf;
+    template <class T>
+    void put(const T& v) {
+        while (buf.size() % alignof(T)) buf.push_back(0);
+        const char* c = reinterpret_cast<const char*>(&v);
+        buf.insert(buf.end(), c, c + sizeof(T));
+    }
+    // numb-typed value (double or float by precision)
+    void put_numb(int precision, double v) {
+        if (precision == UCB_PREC_F64) put<double>(v);
+        else put<float>((float)v);
+    }
+    void finish() {
+        while (buf.size() % 8) buf.push_back(0);
+    }
+};
+
+// Launches a kernel with one by-value struct parameter.
+bool launch_packed(ucb_engine* e, CUfunction f, int grid, int block, cudaStream_t stream, ParamPack& pk,
+                   std::string& err);
+
 // Launch helper: persistent grid size for a kernel.
 int persistent_grid(ucb_engine* e, CUfunction f, int block, long long work_items);
 

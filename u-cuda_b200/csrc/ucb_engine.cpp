@@ -21,6 +21,7 @@
 #include <limits>
 #include <sstream>
 
+#include "csv_export.h"
 #include "engine_internal.h"
 
 namespace ucb {
@@ -184,6 +185,21 @@ SystemCode make_system_code(const std::string& krs_body, int nx, int nv, int pre
     s.exact = true;
     s.code = o.str();
     return s;
+}
+
+bool launch_packed(ucb_engine* e, CUfunction f, int grid, int block, cudaStream_t stream, ParamPack& pk,
+                   std::string& err) {
+    pk.finish();
+    size_t psize = pk.buf.size();
+    void* cfg[] = {CU_LAUNCH_PARAM_BUFFER_POINTER, pk.buf.data(), CU_LAUNCH_PARAM_BUFFER_SIZE, &psize,
+                   CU_LAUNCH_PARAM_END};
+    CUresult r = driver().cuLaunchKernel(f, grid, 1, 1, block, 1, 1, 0, (CUstream)stream, nullptr, cfg);
+    if (r != CUDA_SUCCESS) {
+        err = "cuLaunchKernel: " + cu_error_string(r);
+        return false;
+    }
+    e->launches += 1;
+    return true;
 }
 
 int persistent_grid(ucb_engine* e, CUfunction f, int block, long long work_items) {
@@ -437,23 +453,6 @@ int enqueue_lle(ucb_engine* e, const ucb_lle2d_request& q, const LlePlan& plan, 
     return enqueue_lle_fn(e, q, plan, L, d_values, d_flags, stream, err, -1, true);
 }
 
-void write_lle2d_csv(const std::string& path, const ucb_lle2d_request& q, const LlePlan& plan,
-                     const double* values) {
-    // data_export::write_lle2d_grid layout: n_pts rows of n_pts comma-separated values.
-    std::ofstream out(path);
-    if (!out) return;
-    out << std::setprecision(15);
-    const int n = q.n_pts;
-    for (int iy = 0; iy < n; ++iy) {
-        for (int ix = 0; ix < n; ++ix) {
-            if (ix) out << ", ";
-            out << values[(size_t)iy * n + ix];
-        }
-        out << "\n";
-    }
-    (void)plan;
-}
-
 }  // namespace
 
 }  // namespace ucb
@@ -578,7 +577,14 @@ int ucb_run_lle2d(ucb_engine* e, const ucb_lle2d_request* req, ucb_lle2d_result*
     } else {
         res->min_val = res->max_val = 0.0;
     }
-    if (q.csv_output_path && *q.csv_output_path) write_lle2d_csv(q.csv_output_path, q, plan, res->values);
+    if (q.csv_output_path && *q.csv_output_path) {
+        csv::Common cc{std::vector<double>(q.base_values, q.base_values + q.n_values),
+                       std::vector<double>(q.initial_conditions, q.initial_conditions + q.amount_of_x)};
+        csv::lle2d(q.csv_output_path, cc, plan.map.par_or_var, q.t_max, q.NT, q.transient_time, q.h, q.eps,
+                   q.sweep_over_var ? q.var_sweep_index : q.param_index,
+                   q.sweep_over_var_2 ? q.var_sweep_index_2 : q.param_index_2, q.param_lo, q.param_hi, q.param_lo_2,
+                   q.param_hi_2, n, res->values);
+    }
     if (!L.sys.note.empty()) e->last_error = L.sys.note;
     res->ok = 1;
     return UCB_OK;

@@ -62,6 +62,28 @@ class Lle2dResult(C.Structure):
     ]
 
 
+class Bif1dRequest(C.Structure):
+    _fields_ = [
+        ("krs_body", C.c_char_p), ("amount_of_x", C.c_int32),
+        ("initial_conditions", C.POINTER(C.c_double)), ("base_values", C.POINTER(C.c_double)),
+        ("n_values", C.c_int32), ("param_index", C.c_int32), ("sweep_over_var", C.c_int32),
+        ("var_sweep_index", C.c_int32), ("sweep_over_h", C.c_int32), ("log_scale", C.c_int32),
+        ("param_lo", C.c_double), ("param_hi", C.c_double), ("n_pts", C.c_int32), ("writable_var", C.c_int32),
+        ("h", C.c_double), ("transient_time", C.c_double), ("t_max", C.c_double), ("pre_scaller", C.c_int32),
+        ("max_value", C.c_double), ("max_peaks", C.c_int32), ("csv_output_path", C.c_char_p),
+        ("cancel", C.POINTER(C.c_int32)), ("progress", C.POINTER(C.c_float)), ("opt", Options),
+    ]
+
+
+class Bif1dResult(C.Structure):
+    _fields_ = [
+        ("counts", C.POINTER(C.c_int32)), ("peaks", C.POINTER(C.c_double)), ("intervals", C.POINTER(C.c_double)),
+        ("ok", C.c_int32), ("cancelled", C.c_int32), ("n_pts", C.c_int32), ("record_steps", C.c_int32),
+        ("param_lo", C.c_double), ("param_hi", C.c_double), ("kernel_ms", C.c_double), ("steps", C.c_longlong),
+        ("flops", C.c_double), ("error", C.c_char * 1024),
+    ]
+
+
 _lib = None
 
 
@@ -92,6 +114,8 @@ def load():
     L.ucb_lle2d_device.restype = C.c_int
     L.ucb_lle2d_device.argtypes = [C.c_void_p, C.POINTER(Lle2dRequest), C.c_void_p, C.c_void_p, C.c_void_p,
                                    C.POINTER(Lle2dResult)]
+    L.ucb_run_bif1d.restype = C.c_int
+    L.ucb_run_bif1d.argtypes = [C.c_void_p, C.POINTER(Bif1dRequest), C.POINTER(Bif1dResult)]
     L.ucb_lle2d_states.restype = C.c_int
     L.ucb_lle2d_states.argtypes = [C.c_void_p, C.POINTER(Lle2dRequest), C.c_longlong, C.c_void_p]
     L.ucb_measure_fma_peak.restype = C.c_int
@@ -184,6 +208,44 @@ class Engine:
         if rc != UCB_OK:
             raise UcbError(rc, res.error.decode())
         return values, flags, res
+
+    # ------------------------------------------------------------------ bifurcation 1D
+    @staticmethod
+    def bif1d_request(krs_body: str, amount_of_x: int, initial_conditions, base_values, *, n_pts, param_index=0,
+                      sweep_over_var=False, var_sweep_index=0, sweep_over_h=False, log_scale=False, param_lo=0.0,
+                      param_hi=1.0, writable_var=0, h=0.01, transient_time=0.0, t_max=100.0, pre_scaller=1,
+                      max_value=1e6, max_peaks=64, csv_output_path=None, opt: Options | None = None):
+        ic = np.ascontiguousarray(initial_conditions, dtype=np.float64)
+        vals = np.ascontiguousarray(base_values, dtype=np.float64)
+        r = Bif1dRequest()
+        r._keep = (ic, vals, krs_body.encode())
+        r.krs_body = r._keep[2]
+        r.amount_of_x = amount_of_x
+        r.initial_conditions = _dptr(ic)
+        r.base_values = _dptr(vals)
+        r.n_values = len(vals)
+        r.param_index, r.sweep_over_var, r.var_sweep_index = param_index, int(sweep_over_var), var_sweep_index
+        r.sweep_over_h, r.log_scale = int(sweep_over_h), int(log_scale)
+        r.param_lo, r.param_hi, r.n_pts, r.writable_var = param_lo, param_hi, n_pts, writable_var
+        r.h, r.transient_time, r.t_max, r.pre_scaller = h, transient_time, t_max, pre_scaller
+        r.max_value, r.max_peaks = max_value, max_peaks
+        r.csv_output_path = csv_output_path.encode() if csv_output_path else None
+        r.opt = opt if opt is not None else options()
+        return r
+
+    def run_bif1d(self, req: Bif1dRequest):
+        n, mp = req.n_pts, max(req.max_peaks, 0)
+        counts = np.empty(max(n, 0), dtype=np.int32)
+        peaks = np.empty(max(n, 0) * mp, dtype=np.float64)
+        intervals = np.empty(max(n, 0) * mp, dtype=np.float64)
+        res = Bif1dResult()
+        res.counts = counts.ctypes.data_as(C.POINTER(C.c_int32))
+        res.peaks = _dptr(peaks)
+        res.intervals = _dptr(intervals)
+        rc = self.lib.ucb_run_bif1d(self.h, C.byref(req), C.byref(res))
+        if rc != UCB_OK:
+            raise UcbError(rc, res.error.decode())
+        return counts, peaks.reshape(n, mp), intervals.reshape(n, mp), res
 
     def lle2d_states(self, req: Lle2dRequest, n_steps: int):
         n = req.n_pts
