@@ -1,0 +1,295 @@
+// ucb_parametric_engine.hpp — header-only drop-in for the reference's ParametricEngine
+// facade (parametric_engine.h:27-889) on the per-cell integration path.
+//
+// Same class name, same request/result struct names and field names, same result
+// conventions (ok / cancelled / error, NaN or sentinel + flags, row-major iy*n+ix, plane-
+// major spectra), same shared_ptr<atomic<...>> cancel / progress tokens. Every call goes
+// through the C ABI in ucb.h (libucb.so). Entry points of the reference that are not on
+// this path (DFT, 2-D bifurcation with DBSCAN, Fast Synchro, basin re-clustering,
+// continuation sweeps) are not provided.
+//
+// Extension: ParametricEngine::options() selects the arithmetic of the B200 engine
+// (UCB_PREC_F64 plain form by default; UCB_PREC_F32 state form; exact or native step).
+#pragma once
+
+#include <atomic>
+#include <cmath>
+#include <limits>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "ucb.h"
+
+namespace data_export {
+struct Bif1DSnapshot {
+    std::vector<double> values, initial_conditions;
+    double tMax = 0.0, transientTime = 0.0, h = 0.0;
+    int preScaller = 0, writableVar = 0, indexOfMutVar = 0;
+    double range_lo = 0.0, range_hi = 0.0;
+};
+struct LLE2DSnapshot {
+    std::vector<double> values, initial_conditions;
+    int par_or_var = 1;
+    double tMax = 0.0, NT = 0.0, transientTime = 0.0, h = 0.0, eps = 0.0;
+    int indexOfMutVar = 0, indexOfMutVar2 = 0;
+    double range1_lo = 0.0, range1_hi = 0.0, range2_lo = 0.0, range2_hi = 0.0;
+    int n_pts = 0;
+};
+}  // namespace data_export
+
+struct Bifurcation1DRequest {
+    std::string krs_body;
+    int amountOfX = 0;
+    std::vector<double> initial_conditions;
+    std::vector<double> base_values;
+    int param_index = 0;
+    bool sweep_over_var = false;
+    int var_sweep_index = 0;
+    bool sweep_over_h = false;
+    bool log_scale = false;
+    bool continuation = false;          // not on this path: rejected with an error
+    bool continuation_reverse = false;
+    bool use_cpu = false;               // ignored: there is no CPU path in this engine
+    double param_lo = 0.0;
+    double param_hi = 1.0;
+    int n_pts = 1000;
+    int writable_var = 0;
+    double h = 0.01;
+    double transient_time = 0.0;
+    double t_max = 0.0;
+    int pre_scaller = 1;
+    double max_value = 1.0e6;
+    std::string csv_output_path;
+    std::shared_ptr<std::atomic<bool>> cancel;
+    std::shared_ptr<std::atomic<float>> progress;
+};
+
+struct Bifurcation1DResult {
+    bool ok = false;
+    bool cancelled = false;
+    std::string error;
+    bool continuation_reverse = false;
+    double param_lo = 0.0;
+    double param_hi = 1.0;
+    int n_pts = 0;
+    int record_steps = 0;
+    std::vector<std::vector<double>> bifurcation_points;
+    std::vector<std::vector<double>> peak_times;
+    std::vector<int> flags;
+    data_export::Bif1DSnapshot snapshot;
+};
+
+struct LLE2DRequest {
+    std::string krs_body;
+    int amountOfX = 0;
+    std::vector<double> initial_conditions;
+    std::vector<double> base_values;
+    bool sweep_over_var = false;
+    bool sweep_over_var_2 = false;
+    bool sweep_over_h = false;
+    bool sweep_over_h_2 = false;
+    bool log_scale = false;
+    bool log_scale_2 = false;
+    int param_index = 0;
+    int var_sweep_index = 0;
+    int param_index_2 = 0;
+    int var_sweep_index_2 = 0;
+    double param_lo = 0.0;
+    double param_hi = 1.0;
+    double param_lo_2 = 0.0;
+    double param_hi_2 = 1.0;
+    int n_pts = 200;
+    double h = 0.01;
+    double transient_time = 0.0;
+    double t_max = 100.0;
+    double NT = 1.0;
+    double eps = 1.0e-4;
+    double max_value = 1.0e6;
+    std::string csv_output_path;
+    std::shared_ptr<std::atomic<bool>> cancel;
+    std::shared_ptr<std::atomic<float>> progress;
+};
+
+struct LLE2DResult {
+    bool ok = false;
+    bool cancelled = false;
+    std::string error;
+    int n_pts = 0;
+    double param_lo = 0.0, param_hi = 1.0, param_lo_2 = 0.0, param_hi_2 = 1.0;
+    std::vector<double> values;
+    std::vector<int> flags;
+    double min_val = 0.0;
+    double max_val = 0.0;
+    data_export::LLE2DSnapshot snapshot;
+};
+
+class ParametricEngine {
+public:
+    ParametricEngine() : e_(ucb_create(0)) { ucb_default_options(&opt_); }
+    ~ParametricEngine() { ucb_destroy(e_); }
+    ParametricEngine(const ParametricEngine&) = delete;
+    ParametricEngine& operator=(const ParametricEngine&) = delete;
+
+    ucb_options& options() { return opt_; }
+
+    Bifurcation1DResult run_bifurcation_1d(const Bifurcation1DRequest& r) {
+        Bifurcation1DResult res;
+        if (r.continuation) {
+            res.error = "continuation sweeps are not supported by this engine";
+            return res;
+        }
+        const int mp = 2500;  // max_amount_of_peaks (configCUDA.h)
+        ucb_bif1d_request q{};
+        q.krs_body = r.krs_body.c_str();
+        q.amount_of_x = r.amountOfX;
+        q.initial_conditions = r.initial_conditions.data();
+        if ((int)r.initial_conditions.size() != r.amountOfX) {
+            res.error = "initial_conditions.size() != amountOfX";
+            return res;
+        }
+        q.base_values = r.base_values.data();
+        q.n_values = (int)r.base_values.size();
+        q.param_index = r.param_index;
+        q.sweep_over_var = r.sweep_over_var;
+        q.var_sweep_index = r.var_sweep_index;
+        q.sweep_over_h = r.sweep_over_h;
+        q.log_scale = r.log_scale;
+        q.param_lo = r.param_lo;
+        q.param_hi = r.param_hi;
+        q.n_pts = r.n_pts;
+        q.writable_var = r.writable_var;
+        q.h = r.h;
+        q.transient_time = r.transient_time;
+        q.t_max = r.t_max;
+        q.pre_scaller = r.pre_scaller;
+        q.max_value = r.max_value;
+        q.max_peaks = mp;
+        q.csv_output_path = r.csv_output_path.c_str();
+        q.opt = opt_;
+        int32_t cancel_now = (r.cancel && r.cancel->load()) ? 1 : 0;
+        q.cancel = &cancel_now;
+        float prog = 0.0f;
+        q.progress = &prog;
+        const size_t n = r.n_pts > 0 ? (size_t)r.n_pts : 0;
+        std::vector<int32_t> counts(n);
+        std::vector<double> peaks(n * mp), intervals(n * mp);
+        ucb_bif1d_result o{};
+        o.counts = counts.data();
+        o.peaks = peaks.data();
+        o.intervals = intervals.data();
+        ucb_run_bif1d(e_, &q, &o);
+        if (r.progress) r.progress->store(prog);
+        res.ok = o.ok != 0;
+        res.cancelled = o.cancelled != 0;
+        res.error = o.error;
+        if (!res.ok) return res;
+        res.n_pts = o.n_pts;
+        res.record_steps = o.record_steps;
+        res.param_lo = r.param_lo;
+        res.param_hi = r.param_hi;
+        res.flags.assign(counts.begin(), counts.end());
+        res.bifurcation_points.assign(n, {});
+        res.peak_times.assign(n, {});
+        for (size_t i = 0; i < n; ++i) {
+            const int k = counts[i] > 0 ? counts[i] : 0;
+            res.bifurcation_points[i].assign(peaks.begin() + i * mp, peaks.begin() + i * mp + k);
+            res.peak_times[i].assign(intervals.begin() + i * mp, intervals.begin() + i * mp + k);
+        }
+        auto& s = res.snapshot;
+        s.values = r.base_values;
+        s.initial_conditions = r.initial_conditions;
+        s.tMax = r.t_max;
+        s.transientTime = r.transient_time;
+        s.h = r.h;
+        s.preScaller = r.pre_scaller;
+        s.writableVar = r.writable_var;
+        s.indexOfMutVar = r.sweep_over_var ? r.var_sweep_index : r.param_index;
+        s.range_lo = r.param_lo;
+        s.range_hi = r.param_hi;
+        return res;
+    }
+
+    LLE2DResult run_lle_2d(const LLE2DRequest& r) {
+        LLE2DResult res;
+        if ((int)r.initial_conditions.size() != r.amountOfX) {
+            res.error = "initial_conditions.size() != amountOfX";
+            return res;
+        }
+        ucb_lle2d_request q{};
+        q.krs_body = r.krs_body.c_str();
+        q.amount_of_x = r.amountOfX;
+        q.initial_conditions = r.initial_conditions.data();
+        q.base_values = r.base_values.data();
+        q.n_values = (int)r.base_values.size();
+        q.sweep_over_var = r.sweep_over_var;
+        q.sweep_over_var_2 = r.sweep_over_var_2;
+        q.sweep_over_h = r.sweep_over_h;
+        q.sweep_over_h_2 = r.sweep_over_h_2;
+        q.log_scale = r.log_scale;
+        q.log_scale_2 = r.log_scale_2;
+        q.param_index = r.param_index;
+        q.var_sweep_index = r.var_sweep_index;
+        q.param_index_2 = r.param_index_2;
+        q.var_sweep_index_2 = r.var_sweep_index_2;
+        q.param_lo = r.param_lo;
+        q.param_hi = r.param_hi;
+        q.param_lo_2 = r.param_lo_2;
+        q.param_hi_2 = r.param_hi_2;
+        q.n_pts = r.n_pts;
+        q.h = r.h;
+        q.transient_time = r.transient_time;
+        q.t_max = r.t_max;
+        q.NT = r.NT;
+        q.eps = r.eps;
+        q.max_value = r.max_value;
+        q.csv_output_path = r.csv_output_path.c_str();
+        int32_t cancel_now = (r.cancel && r.cancel->load()) ? 1 : 0;
+        q.cancel = &cancel_now;
+        float prog = 0.0f;
+        q.progress = &prog;
+        q.opt = opt_;
+        const size_t n = r.n_pts > 0 ? (size_t)r.n_pts * (size_t)r.n_pts : 0;
+        res.values.assign(n, 0.0);
+        res.flags.assign(n, 0);
+        std::vector<int32_t> f32(n);
+        ucb_lle2d_result o{};
+        o.values = res.values.data();
+        o.flags = f32.data();
+        ucb_run_lle2d(e_, &q, &o);
+        if (r.progress) r.progress->store(prog);
+        res.ok = o.ok != 0;
+        res.cancelled = o.cancelled != 0;
+        res.error = o.error;
+        if (!res.ok) return res;
+        res.flags.assign(f32.begin(), f32.end());
+        res.n_pts = o.n_pts;
+        res.param_lo = o.param_lo;
+        res.param_hi = o.param_hi;
+        res.param_lo_2 = o.param_lo_2;
+        res.param_hi_2 = o.param_hi_2;
+        res.min_val = o.min_val;
+        res.max_val = o.max_val;
+        auto& s = res.snapshot;
+        s.values = r.base_values;
+        s.initial_conditions = r.initial_conditions;
+        s.par_or_var = (r.sweep_over_var == r.sweep_over_var_2) ? (r.sweep_over_var ? 0 : 1) : 2;
+        s.tMax = r.t_max;
+        s.NT = r.NT;
+        s.transientTime = r.transient_time;
+        s.h = r.h;
+        s.eps = r.eps;
+        s.indexOfMutVar = r.sweep_over_var ? r.var_sweep_index : r.param_index;
+        s.indexOfMutVar2 = r.sweep_over_var_2 ? r.var_sweep_index_2 : r.param_index_2;
+        s.range1_lo = r.param_lo;
+        s.range1_hi = r.param_hi;
+        s.range2_lo = r.param_lo_2;
+        s.range2_hi = r.param_hi_2;
+        s.n_pts = r.n_pts;
+        return res;
+    }
+
+private:
+    ucb_engine* e_;
+    ucb_options opt_;
+};

@@ -1,0 +1,49 @@
+// Drives the header-only ParametricEngine shim the way the reference's session layer
+// calls ParametricEngine (analysis_session.cpp builds a Request, calls run_*, reads the
+// Result). argv[1] = "invalid" (no GPU needed) or "lle2d" / "bif1d" (GPU); the RK4 body
+// is read from stdin.
+#include <cstdio>
+#include <cstring>
+#include <iostream>
+#include <iterator>
+#include <string>
+
+#include "ucb_parametric_engine.hpp"
+
+int main(int argc, char** argv) {
+    const std::string mode = argc > 1 ? argv[1] : "invalid";
+    std::string body((std::istreambuf_iterator<char>(std::cin)), std::istreambuf_iterator<char>());
+    ParametricEngine eng;
+    if (mode == "invalid" || mode == "lle2d") {
+        LLE2DRequest r;
+        r.krs_body = body;
+        r.amountOfX = 3;
+        r.initial_conditions = {1, 1, 1};
+        r.base_values = {0, 0.2, 0.2, 5.7};
+        r.param_index = 2;
+        r.param_index_2 = 3;
+        r.param_lo = 0.05; r.param_hi = 2.0; r.param_lo_2 = 2.0; r.param_hi_2 = 20.0;
+        r.n_pts = mode == "invalid" ? 0 : 8;
+        r.h = 0.01; r.transient_time = 5; r.t_max = 10; r.NT = 0.1;
+        r.progress = std::make_shared<std::atomic<float>>(0.0f);
+        LLE2DResult res = eng.run_lle_2d(r);
+        std::printf("ok=%d error=%s n=%d min=%.6f max=%.6f progress=%.1f\n", (int)res.ok, res.error.c_str(), res.n_pts,
+                    res.min_val, res.max_val, r.progress->load());
+        if (mode == "lle2d")
+            for (size_t i = 0; i < res.values.size(); ++i) std::printf("%.17g %d\n", res.values[i], res.flags[i]);
+        return 0;
+    }
+    Bifurcation1DRequest b;
+    b.krs_body = body;
+    b.amountOfX = 3;
+    b.initial_conditions = {0.1, 0.1, 0.1};
+    b.base_values = {0, 10.0, 28.0, 8.0 / 3.0};
+    b.param_index = 2;
+    b.param_lo = 20; b.param_hi = 200; b.n_pts = 8;
+    b.h = 0.01; b.transient_time = 10; b.t_max = 30;
+    Bifurcation1DResult res = eng.run_bifurcation_1d(b);
+    std::printf("ok=%d error=%s n=%d record_steps=%d\n", (int)res.ok, res.error.c_str(), res.n_pts, res.record_steps);
+    for (int i = 0; i < res.n_pts; ++i)
+        std::printf("%d %zu\n", res.flags[i], res.bifurcation_points[i].size());
+    return 0;
+}

@@ -86,11 +86,13 @@ def test_exact_f32_bifurcation_matches_oracle(eng):
 
 
 def test_fixed_point_and_divergence_flags(eng):
-    # rho < 1: the origin is a stable fixed point (count -1); a tiny max_value forces 0.
+    # rho < 1: the origin is a stable fixed point (count -1 once the state has settled;
+    # a point still decaying at the end of the record has no peaks, count 0); a tiny
+    # max_value forces the divergence flag 0.
     c = case(n_pts=4, param_lo=0.2, param_hi=0.8)
     (counts, _, _, _), (oc, _, _) = run_both(eng, c, precision=ucb.PREC_F64, mode=ucb.MODE_EXACT)
     np.testing.assert_array_equal(counts, oc)
-    assert (counts == -1).all()
+    assert (counts[:3] == -1).all() and (counts <= 0).all()
     c = case(n_pts=4, max_value=1.0)
     (counts, _, _, _), (oc, _, _) = run_both(eng, c, precision=ucb.PREC_F64, mode=ucb.MODE_EXACT)
     np.testing.assert_array_equal(counts, oc)

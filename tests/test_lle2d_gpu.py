@@ -112,13 +112,15 @@ def test_exact_trajectory_bitwise(eng):
 
 @pytest.mark.parametrize("prec", [ucb.PREC_F64, ucb.PREC_F32])
 def test_native_lle_within_tolerance(eng, prec):
-    # Non-chaotic cells (oracle lambda <= 0.02: fixed points and limit cycles) must agree
-    # with the FP64 oracle to 2e-3 on >= 99.5% of them. On chaotic cells no arithmetic
-    # that is not bit-identical can: rounding differences are amplified until the
-    # finite-time exponent is just another sample of the attractor. There the engine's
-    # median difference must stay within 3x the oracle's own median change under a 1e-7
-    # relative perturbation of the swept parameters (the size of FP32 parameter rounding).
-    c = lle2d_case(n=16, t_max=200.0, transient=50.0)
+    # Well-conditioned cells — those whose FP64 oracle exponent moves by < 1e-5 under a
+    # 1e-7 relative perturbation of the swept parameters (the size of FP32 rounding):
+    # fixed points, limit cycles, and chaotic cells not yet decorrelated at this horizon —
+    # must agree with the FP64 oracle to 2e-3 on >= 99.5% of them. On the other cells no
+    # arithmetic that is not bit-identical can: rounding differences are amplified until
+    # the finite-time exponent is just another sample of the attractor. There the
+    # engine's median difference must stay within 3x the oracle's own median change under
+    # that perturbation.
+    c = lle2d_case(n=24, t_max=200.0, transient=50.0)
     v, f, _ = run(eng, c, precision=prec, mode=ucb.MODE_NATIVE)
     ov, of = oracle_lle(c)
     np.testing.assert_array_equal(f, of)
@@ -127,7 +129,7 @@ def test_native_lle_within_tolerance(eng, prec):
     pv, _ = oracle_lle(pert)
     d = np.abs(v - ov)
     spread = np.abs(pv - ov)
-    quiet = ov <= 0.02
+    quiet = spread < 1e-5
     assert quiet.sum() > 20 and (~quiet).sum() > 20
     assert np.mean(d[quiet] <= 2e-3) >= 0.995, np.sort(d[quiet])[-5:]
     assert np.median(d[~quiet]) <= 3 * np.median(spread[~quiet]) + 1e-3
