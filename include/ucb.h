@@ -184,6 +184,33 @@ typedef struct ucb_bif1d_result {
 
 UCB_API int ucb_run_bif1d(ucb_engine* e, const ucb_bif1d_request* req, ucb_bif1d_result* res);
 
+/* LLE map without device allocation (no counterpart in the reference).
+ *
+ * ucb_lle2d_device() keeps its scratch (work-queue counter, step counter, axis value
+ * tables) in an engine workspace that it cudaMalloc()s on first use. Callers that cannot
+ * allocate device memory — applications that own all of it through their own pool or a
+ * fixed pre-reserved budget, and time-critical loops that must not reach cudaMalloc /
+ * cudaFree (cudaFree synchronises the device) — use this variant instead: the same
+ * kernel, with its scratch in a fixed-size array inside this library that every GPU
+ * loading the library holds until the process exits. The caller still provides
+ * d_values / d_flags (n_pts * n_pts each).
+ *
+ * Limits and rules:
+ *   - n_pts <= UCB_NOALLOC_MAX_PTS, otherwise UCB_E_INVALID with a message;
+ *   - ucb_prepare_lle2d() must have been called for an equivalent request (same body,
+ *     sizes, sweep kinds and options) on this engine: it compiles and loads the kernel,
+ *     which allocates, and looks up the scratch array's device address; the no-alloc
+ *     call returns UCB_E_INVALID otherwise. If only the scratch address is missing for
+ *     the device, the first no-alloc call on that device looks it up; make that first
+ *     call before any stream capture;
+ *   - all calls share the one array and it keeps the last call's contents; every call
+ *     resets the counters it needs, but calls that overlap on the GPU (other streams,
+ *     other engines in the process) race on it and must be serialised by the caller. */
+#define UCB_NOALLOC_MAX_PTS 4096
+UCB_API int ucb_prepare_lle2d(ucb_engine* e, const ucb_lle2d_request* req);
+UCB_API int ucb_lle2d_device_noalloc(ucb_engine* e, const ucb_lle2d_request* req, double* d_values,
+                                     int32_t* d_flags, void* stream, ucb_lle2d_result* res);
+
 /* Trajectory parity aid: integrates every cell of the request's grid (same sweep
  * mapping, same step function and precision as ucb_run_lle2d) for n_steps plain steps
  * from its initial condition — no transient, no divergence checks, no extra step — and

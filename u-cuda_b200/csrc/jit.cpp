@@ -227,6 +227,13 @@ std::shared_ptr<Module> ModuleCache::get(const CompileRequest& rq, std::string& 
     return m;
 }
 
+std::shared_ptr<Module> ModuleCache::find(const CompileRequest& rq) const {
+    const uint64_t key = request_key(rq);
+    std::lock_guard<std::mutex> lk(mu_);
+    auto it = cache_.find(key);
+    return it == cache_.end() ? nullptr : it->second;
+}
+
 size_t ModuleCache::size() const {
     std::lock_guard<std::mutex> lk(mu_);
     return cache_.size();

@@ -71,6 +71,8 @@ bool precompile_to_disk(const CompileRequest& rq, std::string& err);
 class ModuleCache {
 public:
     std::shared_ptr<Module> get(const CompileRequest& rq, std::string& err);
+    // Already-loaded module for this request, or nullptr (never compiles or loads).
+    std::shared_ptr<Module> find(const CompileRequest& rq) const;
     size_t size() const;
     void clear();
 

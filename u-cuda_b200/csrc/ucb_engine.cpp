@@ -397,14 +397,17 @@ bool prepare_lle(ucb_engine* e, const ucb_lle2d_request& q, const LlePlan& plan,
 // [256..] axis tables.
 int enqueue_lle_fn(ucb_engine* e, const ucb_lle2d_request& q, const LlePlan& plan, const LleLaunch& L,
                    double* d_values, int32_t* d_flags, cudaStream_t stream, std::string& err, long long skip_override,
-                   bool persistent) {
+                   bool persistent, char* scratch) {
     const int n = q.n_pts;
     const int prec = q.opt.precision;
     const size_t esz = prec == UCB_PREC_F64 ? 8 : 4;
     const size_t tab_bytes = (size_t)n * esz;
     const size_t off_ax0 = 256, off_ax1 = 256 + ((tab_bytes + 255) / 256) * 256;
-    if (!ensure_workspace(e, off_ax1 + tab_bytes + 256, err)) return UCB_E_CUDA;
-    char* ws = static_cast<char*>(e->ws);
+    char* ws = scratch;
+    if (!ws) {
+        if (!ensure_workspace(e, off_ax1 + tab_bytes + 256, err)) return UCB_E_CUDA;
+        ws = static_cast<char*>(e->ws);
+    }
     std::vector<double> t0d, t1d;
     std::vector<float> t0f, t1f;
     axis_table(prec, n, plan.map.lo[0], plan.map.hi[0], plan.map.log_axis[0], t0d, t0f);
@@ -450,10 +453,44 @@ int enqueue_lle_fn(ucb_engine* e, const ucb_lle2d_request& q, const LlePlan& pla
 
 int enqueue_lle(ucb_engine* e, const ucb_lle2d_request& q, const LlePlan& plan, const LleLaunch& L,
                 double* d_values, int32_t* d_flags, cudaStream_t stream, std::string& err) {
-    return enqueue_lle_fn(e, q, plan, L, d_values, d_flags, stream, err, -1, true);
+    return enqueue_lle_fn(e, q, plan, L, d_values, d_flags, stream, err, -1, true, nullptr);
 }
 
 }  // namespace
+
+// Internal hooks used by the scratch-array entry point (noalloc.cu).
+int lle2d_plan_and_find(ucb_engine* e, const ucb_lle2d_request& q, bool load_if_missing, std::string& err,
+                        void** plan_out, void** launch_out) {
+    auto* plan = new LlePlan;
+    if (!plan_lle2d(q, *plan, err)) { delete plan; return UCB_E_INVALID; }
+    if (!ensure_init(e, err)) { delete plan; return UCB_E_NOGPU; }
+    auto* L = new LleLaunch;
+    CompileRequest rq = lle_compile_request(q, *plan, *L);
+    L->mod = load_if_missing ? e->modules.get(rq, err) : e->modules.find(rq);
+    if (!L->mod) {
+        if (!load_if_missing)
+            err = "kernel not prepared for this request: call ucb_prepare_lle2d first (loading a module allocates "
+                  "device memory)";
+        delete plan;
+        delete L;
+        return load_if_missing ? UCB_E_COMPILE : UCB_E_INVALID;
+    }
+    L->fn = L->mod->functions["ucb_lle_kernel"];
+    *plan_out = plan;
+    *launch_out = L;
+    return UCB_OK;
+}
+
+int lle2d_enqueue_with_scratch(ucb_engine* e, const ucb_lle2d_request& q, void* plan, void* launch, double* d_values,
+                               int32_t* d_flags, cudaStream_t stream, char* scratch, std::string& err) {
+    return enqueue_lle_fn(e, q, *static_cast<LlePlan*>(plan), *static_cast<LleLaunch*>(launch), d_values, d_flags,
+                          stream, err, -1, true, scratch);
+}
+
+void lle2d_release(void* plan, void* launch) {
+    delete static_cast<LlePlan*>(plan);
+    delete static_cast<LleLaunch*>(launch);
+}
 
 }  // namespace ucb
 
@@ -609,7 +646,7 @@ int ucb_lle2d_states(ucb_engine* e, const ucb_lle2d_request* req, long long n_st
     ucb_lle2d_request q = *req;
     LleLaunch L2 = L;
     L2.fn = L.mod->functions["ucb_state_kernel"];
-    int rc = enqueue_lle_fn(e, q, p2, L2, d_out, nullptr, e->stream, err, n_steps, /*persistent=*/false);
+    int rc = enqueue_lle_fn(e, q, p2, L2, d_out, nullptr, e->stream, err, n_steps, /*persistent=*/false, nullptr);
     if (rc == UCB_OK) {
         if ((ce = cudaMemcpyAsync(out_states, d_out, bytes, cudaMemcpyDeviceToHost, e->stream)) != cudaSuccess ||
             (ce = cudaStreamSynchronize(e->stream)) != cudaSuccess) {

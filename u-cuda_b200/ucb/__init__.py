@@ -116,6 +116,11 @@ def load():
                                    C.POINTER(Lle2dResult)]
     L.ucb_run_bif1d.restype = C.c_int
     L.ucb_run_bif1d.argtypes = [C.c_void_p, C.POINTER(Bif1dRequest), C.POINTER(Bif1dResult)]
+    L.ucb_prepare_lle2d.restype = C.c_int
+    L.ucb_prepare_lle2d.argtypes = [C.c_void_p, C.POINTER(Lle2dRequest)]
+    L.ucb_lle2d_device_noalloc.restype = C.c_int
+    L.ucb_lle2d_device_noalloc.argtypes = [C.c_void_p, C.POINTER(Lle2dRequest), C.c_void_p, C.c_void_p,
+                                           C.c_void_p, C.POINTER(Lle2dResult)]
     L.ucb_lle2d_states.restype = C.c_int
     L.ucb_lle2d_states.argtypes = [C.c_void_p, C.POINTER(Lle2dRequest), C.c_longlong, C.c_void_p]
     L.ucb_measure_fma_peak.restype = C.c_int
@@ -246,6 +251,23 @@ class Engine:
         if rc != UCB_OK:
             raise UcbError(rc, res.error.decode())
         return counts, peaks.reshape(n, mp), intervals.reshape(n, mp), res
+
+    def prepare_lle2d(self, req: Lle2dRequest):
+        """One-time set-up for lle2d_device_noalloc (compiles/loads the kernel, finds the
+        scratch array's device address)."""
+        rc = self.lib.ucb_prepare_lle2d(self.h, C.byref(req))
+        if rc != UCB_OK:
+            raise UcbError(rc, self.last_error())
+
+    def lle2d_device_noalloc(self, req: Lle2dRequest, d_values_ptr: int, d_flags_ptr: int, stream_ptr: int = 0):
+        """LLE map into caller-owned device buffers with no device allocation (scratch in a
+        fixed array of the library; n_pts <= 4096; calls overlapping on the GPU race)."""
+        res = Lle2dResult()
+        rc = self.lib.ucb_lle2d_device_noalloc(self.h, C.byref(req), C.c_void_p(d_values_ptr),
+                                               C.c_void_p(d_flags_ptr), C.c_void_p(stream_ptr), C.byref(res))
+        if rc != UCB_OK:
+            raise UcbError(rc, res.error.decode())
+        return res
 
     def lle2d_states(self, req: Lle2dRequest, n_steps: int):
         n = req.n_pts
