@@ -183,6 +183,117 @@ typedef struct ucb_bif1d_result {
 } ucb_bif1d_result;
 
 UCB_API int ucb_run_bif1d(ucb_engine* e, const ucb_bif1d_request* req, ucb_bif1d_result* res);
+/* Compile-only (no GPU) counterpart, like ucb_precompile_lle2d. */
+UCB_API int ucb_precompile_bif1d(const ucb_bif1d_request* req, char* err_out, int err_len);
+
+/* ------------------------------------------------------------------------------------
+ * Lyapunov spectrum 2D — replaces ParametricEngine::run_ls_2d(const LS2DRequest&)
+ * (parametric_engine.h:581-648, :874; implementation parametric_engine.cpp:3430-3786).
+ * Two methods:
+ *   UCB_LS_FIXED — the reference's: fixed step h, N shadow probes at distance eps,
+ *                  classical Gram-Schmidt every NT (LSKernelCUDA, cudaLibrary.cu:2878);
+ *   UCB_LS_DP5   — adaptive Dormand-Prince 5(4) with N tangent-linear vectors and
+ *                  modified Gram-Schmidt every gs_every accepted steps over the interval
+ *                  [transient_time, transient_time + t_end]; needs a recognised RK4 body
+ *                  (the right-hand side is taken from it). No reference counterpart.
+ * ---------------------------------------------------------------------------------- */
+#define UCB_LS_FIXED 0
+#define UCB_LS_DP5 1
+
+typedef struct ucb_ls2d_request {
+    const char* krs_body;
+    int32_t amount_of_x;
+    const double* initial_conditions;
+    const double* base_values;
+    int32_t n_values;
+    int32_t sweep_over_var, sweep_over_var_2;
+    int32_t sweep_over_h, sweep_over_h_2;
+    int32_t log_scale, log_scale_2;
+    int32_t param_index, var_sweep_index, param_index_2, var_sweep_index_2;
+    double param_lo, param_hi, param_lo_2, param_hi_2;
+    int32_t n_pts;
+    double h, transient_time, t_max, NT, eps, max_value;
+    const char* csv_output_path;
+    const volatile int32_t* cancel;
+    volatile float* progress;
+    ucb_options opt;
+    /* method selection and the adaptive method's controls */
+    int32_t method;          /* UCB_LS_FIXED / UCB_LS_DP5 */
+    int32_t gs_every;        /* accepted steps between modified Gram-Schmidt passes (DP5) */
+    double rtol, atol;       /* DP5 error tolerances (0 = 1e-8 / 1e-5 for FP64 / FP32, atol = rtol) */
+    double t_end;            /* DP5 measured interval length (0 = t_max) */
+    double h0;               /* DP5 initial step (0 = h) */
+    long long max_steps;     /* DP5 cap on step attempts per cell (0 = 10^8) */
+} ucb_ls2d_request;
+
+typedef struct ucb_ls2d_result {
+    double* values;          /* caller-allocated, amount_of_x * n_pts^2, plane-major
+                                values[k * n_pts^2 + iy * n_pts + ix] */
+    int32_t* flags;          /* n_pts^2: 1 ok, -1 diverged (sentinel 999 in every plane) */
+    double* min_val;         /* amount_of_x (may be NULL) */
+    double* max_val;         /* amount_of_x (may be NULL) */
+    int32_t ok, cancelled, n_pts, n_exponents;
+    double kernel_ms;
+    long long steps;         /* FIXED: trajectory steps; DP5: step attempts */
+    double flops;
+    char error[1024];
+} ucb_ls2d_result;
+
+UCB_API int ucb_run_ls2d(ucb_engine* e, const ucb_ls2d_request* req, ucb_ls2d_result* res);
+/* Compile-only (no GPU) counterpart, like ucb_precompile_lle2d. */
+UCB_API int ucb_precompile_ls2d(const ucb_ls2d_request* req, char* err_out, int err_len);
+
+/* ------------------------------------------------------------------------------------
+ * Basins of attraction — replaces ParametricEngine::run_basins (parametric_engine.h:659-723,
+ * :877) on this path with stroboscopic classification (no reference counterpart for the
+ * labelling itself; the reference clusters peak features with DBSCAN, :6035-6440):
+ * initial conditions (axis_x_var, axis_y_var) on an n_pts x n_pts grid, other variables
+ * from initial_conditions; RK4 with step h = period / steps_per_period; a cell converges
+ * when its stroboscopic point repeats with the smallest period k <= 8 to within match_tol
+ * for match_count consecutive periods, and exits early; cap max_periods.
+ * labels[iy*n + ix]: >= 1 attractor id (ordered by period, then canonical point), 0 not
+ * converged within the cap, -1 diverged (max_value / NaN).
+ * ---------------------------------------------------------------------------------- */
+typedef struct ucb_basins_request {
+    const char* krs_body;
+    int32_t amount_of_x;
+    const double* initial_conditions;
+    const double* base_values;
+    int32_t n_values;
+    int32_t axis_x_var, axis_y_var;   /* 0-based state indices */
+    double axis_x_lo, axis_x_hi, axis_y_lo, axis_y_hi;
+    int32_t n_pts;
+    double period;                    /* forcing period (stroboscope interval), > 0 */
+    int32_t steps_per_period;         /* h = period / steps_per_period */
+    int32_t max_periods;              /* cap (2000 in the benchmark configuration) */
+    int32_t match_count;              /* consecutive period matches to converge (20) */
+    double match_tol;                 /* max-norm match tolerance (1e-6) */
+    int32_t phase_var;                /* state index of the forcing phase (reset every period), -1 none */
+    double max_value;
+    double merge_radius;              /* canonical points closer than this are one attractor (0 = 1e-4) */
+    const char* csv_output_path;
+    const volatile int32_t* cancel;
+    volatile float* progress;
+    ucb_options opt;
+} ucb_basins_request;
+
+#define UCB_BASINS_MAX_ATTRACTORS 256
+typedef struct ucb_basins_result {
+    int32_t* labels;                  /* caller-allocated n_pts^2 */
+    int32_t* periods;                 /* caller-allocated n_pts^2 (may be NULL): period, 0, -1 */
+    int32_t* iterations;              /* caller-allocated n_pts^2 (may be NULL): periods integrated */
+    int32_t ok, cancelled, n_pts;
+    int32_t n_attractors;
+    int32_t attractor_period[UCB_BASINS_MAX_ATTRACTORS];
+    double attractor_point[UCB_BASINS_MAX_ATTRACTORS][2];
+    double kernel_ms;
+    long long steps;
+    double flops;
+    char error[1024];
+} ucb_basins_result;
+
+UCB_API int ucb_run_basins(ucb_engine* e, const ucb_basins_request* req, ucb_basins_result* res);
+UCB_API int ucb_precompile_basins(const ucb_basins_request* req, char* err_out, int err_len);
 
 /* LLE map without device allocation (no counterpart in the reference).
  *

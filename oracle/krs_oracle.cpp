@@ -63,7 +63,7 @@ std::string g_err;
 // ---------------------------------------------------------------------------
 // KRS step compilation (krs_cpu.cpp:293-316 prelude, Linux toolchain)
 // ---------------------------------------------------------------------------
-std::string make_source(const std::string& body, int amountOfX, bool dbl, bool dual) {
+std::string make_source(const std::string& body, int amountOfX, bool dbl, bool dual, bool rhs = false) {
     std::ostringstream o;
     o << "#include <cmath>\n#include <cstdlib>\nusing std::abs;\n";
     if (dual) {
@@ -107,10 +107,12 @@ std::string make_source(const std::string& body, int amountOfX, bool dbl, bool d
          "#define AMOUNTOFX " << amountOfX << "\n"
          "static const numb pi    = (numb)3.1415926535897932384626433832795;\n"
          "static const numb euler = (numb)2.7182818284590452353602874713527;\n"
-         "extern \"C\" __attribute__((visibility(\"default\")))\n"
-         "void krs_step(numb* X, const numb* a, numb h) {\n"
-         "#line 1 \"krs\"\n"
-      << body << "\n}\n";
+         "extern \"C\" __attribute__((visibility(\"default\")))\n";
+    if (rhs)
+        o << "void krs_rhs(const numb* X1, const numb* a, numb* dX) {\n";
+    else
+        o << "void krs_step(numb* X, const numb* a, numb h) {\n";
+    o << "#line 1 \"krs\"\n" << body << "\n}\n";
     return o.str();
 }
 
@@ -135,10 +137,10 @@ struct Krs {
     int numb_bytes = 8;  // 8 double, 4 float, 16 dual
 };
 
-Krs* compile_krs(const std::string& body, int nx, int numb_bytes, const char* extra_flags) {
+Krs* compile_krs(const std::string& body, int nx, int numb_bytes, const char* extra_flags, bool rhs = false) {
     std::lock_guard<std::mutex> lk(g_compile_mu);
     const bool dual = numb_bytes == 16;
-    const std::string src = make_source(body, nx, numb_bytes == 8, dual);
+    const std::string src = make_source(body, nx, numb_bytes == 8, dual, rhs);
     const std::string flags = std::string("-O2 -ffp-contract=off -fPIC -shared ") + (extra_flags ? extra_flags : "");
     const uint64_t h = fnv1a(flags, fnv1a(src));
     char name[64];
@@ -167,8 +169,8 @@ Krs* compile_krs(const std::string& body, int nx, int numb_bytes, const char* ex
     }
     void* lib = dlopen(so.c_str(), RTLD_NOW | RTLD_LOCAL);
     if (!lib) { g_err = std::string("dlopen: ") + dlerror(); return nullptr; }
-    void* fn = dlsym(lib, "krs_step");
-    if (!fn) { g_err = "krs_step not exported"; dlclose(lib); return nullptr; }
+    void* fn = dlsym(lib, rhs ? "krs_rhs" : "krs_step");
+    if (!fn) { g_err = "step function not exported"; dlclose(lib); return nullptr; }
     Krs* k = new Krs;
     k->lib = lib; k->fn = fn; k->nx = nx; k->numb_bytes = numb_bytes;
     return k;
@@ -451,6 +453,170 @@ int peak_finder(const T* data, int64_t n, T* outPeaks, T* timeOfPeaks, T h) {
     return amountOfPeaks;
 }
 
+// ---------------------------------------------------------------------------
+// Tangent-linear spectrum with adaptive Dormand-Prince 5(4) (new semantics; no reference
+// counterpart). Published pair of Dormand & Prince (1980): FSAL, RMS error norm over the
+// augmented state (x, V) with sc_i = atol + rtol max(|y_i|, |y_new_i|) (the state alone
+// while not measuring), accept if err <= 1, step factor
+// 0.9 err^(-1/5) clamped to [0.2, 5] (upper clamp 2 right after a rejection). The N
+// tangent vectors follow v' = J(x) v with the same stages (J v from forward-mode dual
+// numbers of the right-hand side), modified Gram-Schmidt every gs_every accepted steps
+// and at the end; lambda_k = sum log(norm_k) / t_end over [transient, transient + t_end].
+// ---------------------------------------------------------------------------
+struct Dual { double v, d; };
+using RhsFn = void (*)(const double*, const double*, double*);
+using RhsDualFn = void (*)(const Dual*, const Dual*, Dual*);
+
+struct Dp5Coef {
+    double a[7][6] = {{0}};
+    double b[7] = {35.0 / 384, 0, 500.0 / 1113, 125.0 / 192, -2187.0 / 6784, 11.0 / 84, 0};
+    double e[7] = {71.0 / 57600, 0, -71.0 / 16695, 71.0 / 1920, -17253.0 / 339200, 22.0 / 525, -1.0 / 40};
+    Dp5Coef() {
+        a[1][0] = 1.0 / 5;
+        a[2][0] = 3.0 / 40; a[2][1] = 9.0 / 40;
+        a[3][0] = 44.0 / 45; a[3][1] = -56.0 / 15; a[3][2] = 32.0 / 9;
+        a[4][0] = 19372.0 / 6561; a[4][1] = -25360.0 / 2187; a[4][2] = 64448.0 / 6561; a[4][3] = -212.0 / 729;
+        a[5][0] = 9017.0 / 3168; a[5][1] = -355.0 / 33; a[5][2] = 46732.0 / 5247; a[5][3] = 49.0 / 176;
+        a[5][4] = -5103.0 / 18656;
+    }
+};
+
+void jvp(RhsDualFn fd, const double* x, const double* av, int nv, const double* v, double* out, int nx) {
+    Dual X[64], A[64], D[64];
+    for (int i = 0; i < nx; ++i) X[i] = {x[i], v[i]};
+    for (int i = 0; i < nv; ++i) A[i] = {av[i], 0.0};
+    fd(X, A, D);
+    for (int i = 0; i < nx; ++i) out[i] = D[i].d;
+}
+
+bool mgs_cpu(std::vector<double>& V, int n, double* acc) {
+    for (int k = 0; k < n; ++k) {
+        for (int j = 0; j < k; ++j) {
+            double d = 0;
+            for (int l = 0; l < n; ++l) d += V[k * n + l] * V[j * n + l];
+            for (int l = 0; l < n; ++l) V[k * n + l] -= d * V[j * n + l];
+        }
+        double n2 = 0;
+        for (int l = 0; l < n; ++l) n2 += V[k * n + l] * V[k * n + l];
+        const double nrm = std::sqrt(n2);
+        if (!(nrm > 0) || !std::isfinite(nrm)) return false;
+        if (acc) acc[k] += std::log(nrm);
+        for (int l = 0; l < n; ++l) V[k * n + l] /= nrm;
+    }
+    return true;
+}
+
+void ls_cell_dp5_cpu(RhsFn f, RhsDualFn fd, int nx, const double* x0, const double* av, int nv, double transient,
+                     double t_end, double rtol, double atol, double h0, int gs_every, long long max_steps,
+                     double maxv, uint64_t seq, double* out) {
+    static const Dp5Coef C;
+    std::vector<double> x(x0, x0 + nx), V((size_t)nx * nx), K(7 * (size_t)nx), xs(nx), xn(nx);
+    Rng st;
+    rng_init(1234567891ULL, seq, 0ULL, &st);
+    for (int j = 0; j < nx; ++j)
+        for (int i = 0; i < nx; ++i) V[j * nx + i] = rng_uniform(&st) - 0.5;
+    std::vector<double> acc(nx, 0.0);
+    bool ok = mgs_cpu(V, nx, nullptr);
+    double t = 0.0, h = h0, facmax = 5.0;
+    const double t_stop = transient + t_end;
+    bool measuring = !(transient > 0);
+    int since = 0;
+    // Early orthonormalisation when the accumulated spread (time since the last pass x
+    // running lambda_1 - lambda_N) exceeds the FP64 budget of 20 nats.
+    double t_gs = 0.0, t_meas = 0.0, spread = 1e300;
+    long long attempts = 0;
+    std::vector<double> stage((size_t)6 * nx);  // stage points X1..X6
+    f(x.data(), av, &K[0]);
+    while (ok && t < t_stop) {
+        if (++attempts > max_steps) { ok = false; break; }
+        const double target = measuring ? t_stop : transient;
+        bool last = false;
+        if (t + h >= target) { h = target - t; last = true; }
+        for (int i = 0; i < nx; ++i) stage[i] = x[i];
+        for (int s = 1; s < 6; ++s) {
+            for (int i = 0; i < nx; ++i) {
+                double acc_s = 0;
+                for (int j = 0; j < s; ++j) acc_s += C.a[s][j] * K[j * nx + i];
+                stage[s * nx + i] = x[i] + h * acc_s;
+            }
+            f(&stage[s * nx], av, &K[s * nx]);
+        }
+        for (int i = 0; i < nx; ++i) {
+            double acc_s = 0;
+            for (int j = 0; j < 6; ++j) acc_s += C.b[j] * K[j * nx + i];
+            xn[i] = x[i] + h * acc_s;
+        }
+        f(xn.data(), av, &K[6 * nx]);
+        double err2 = 0;
+        for (int i = 0; i < nx; ++i) {
+            double e = 0;
+            for (int j = 0; j < 7; ++j) e += C.e[j] * K[j * nx + i];
+            e *= h;
+            const double sc = atol + rtol * std::max(std::fabs(x[i]), std::fabs(xn[i]));
+            err2 += (e / sc) * (e / sc);
+        }
+        double err = std::sqrt(err2 / nx);
+        std::vector<double> Vn(V.size());
+        if (err <= 1.0 && measuring) {
+            std::vector<double> L((size_t)7 * nx), vt(nx);
+            double ev2 = 0;
+            for (int k = 0; k < nx; ++k) {
+                const double* v = &V[k * nx];
+                double* vn = &Vn[k * nx];
+                for (int s = 0; s < 6; ++s) {
+                    for (int i = 0; i < nx; ++i) {
+                        double a_s = 0;
+                        for (int j = 0; j < s; ++j) a_s += C.a[s][j] * L[j * nx + i];
+                        vt[i] = v[i] + h * a_s;
+                    }
+                    jvp(fd, &stage[s * nx], av, nv, vt.data(), &L[s * nx], nx);
+                }
+                for (int i = 0; i < nx; ++i) {
+                    double b_s = 0;
+                    for (int j = 0; j < 6; ++j) b_s += C.b[j] * L[j * nx + i];
+                    vn[i] = v[i] + h * b_s;
+                }
+                jvp(fd, xn.data(), av, nv, vn, &L[6 * nx], nx);
+                for (int i = 0; i < nx; ++i) {
+                    double e = 0;
+                    for (int j = 0; j < 7; ++j) e += C.e[j] * L[j * nx + i];
+                    e *= h;
+                    const double sc = atol + rtol * std::max(std::fabs(v[i]), std::fabs(vn[i]));
+                    ev2 += (e / sc) * (e / sc);
+                }
+            }
+            err = std::sqrt((err2 + ev2) / (nx + nx * nx));
+        }
+        if (!std::isfinite(err)) { ok = false; break; }
+        if (err <= 1.0) {
+            if (measuring) V = Vn;
+            const double t_new = last ? target : t + h;
+            if (measuring) t_gs += t_new - t;
+            t = t_new;
+            for (int i = 0; i < nx; ++i) { x[i] = xn[i]; K[i] = K[6 * nx + i]; }
+            double checker = 0;
+            for (int i = 0; i < nx; ++i) checker += std::fabs(x[i]);
+            if (std::isnan(checker) || std::isinf(checker) || (maxv != 0 && checker > maxv)) { ok = false; break; }
+            if (measuring && (++since >= gs_every || last || t_gs * spread > 20.0)) {
+                ok = mgs_cpu(V, nx, acc.data());
+                since = 0;
+                t_meas += t_gs;
+                t_gs = 0.0;
+                spread = std::max(0.0, (acc[0] - acc[nx - 1]) / t_meas);
+            }
+            if (last && !measuring) measuring = true;
+            const double fac = err > 0 ? 0.9 * std::pow(err, -0.2) : facmax;
+            h *= std::min(facmax, std::max(0.2, fac));
+            facmax = 5.0;
+        } else {
+            h *= std::max(0.2, 0.9 * std::pow(err, -0.2));
+            facmax = 2.0;
+            if (!(h > 1e-14)) { ok = false; break; }
+        }
+    }
+    for (int k = 0; k < nx; ++k) out[k] = ok ? acc[k] / t_end : 999.0;
+}
+
 template <class T>
 struct Dispatch {
     static StepFn<T> fn(Krs* k) { return reinterpret_cast<StepFn<T>>(k->fn); }
@@ -468,6 +634,108 @@ int threads_or_default(int nthreads) {
 extern "C" {
 
 const char* orc_last_error() { return g_err.c_str(); }
+
+// Right-hand side "dX[i] = ...;" statements over X1[] and a[] (numb_bytes 8 or 16).
+void* orc_rhs_compile(const char* body, int nx, int numb_bytes) {
+    if (nx <= 0 || nx > 32) { g_err = "amountOfX out of range"; return nullptr; }
+    return compile_krs(body, nx, numb_bytes, nullptr, true);
+}
+
+// DP5(4) tangent-linear spectrum over a 2-D grid (kernel cell order; values[c*nx + k]).
+int orc_ls2d_dp5(void* hrhs, void* hdual, int nPts, int par_or_var, int idx0, int idx1, const double* ranges,
+                 int log_mask, const double* ic, int nv, const double* vals, double transient, double t_end,
+                 double rtol, double atol, double h0, int gs_every, long long max_steps, double maxv,
+                 const long long* cells, long long ncells, double* values, int* flags, int nthreads) {
+    Krs* kr = static_cast<Krs*>(hrhs);
+    Krs* kd = static_cast<Krs*>(hdual);
+    const int nx = kr->nx;
+    Grid g{nPts, 2, par_or_var, {idx0, idx1}, {ranges[0], ranges[1], ranges[2], ranges[3]}, log_mask, -1};
+    const long long n = cells ? ncells : (long long)nPts * nPts;
+#pragma omp parallel for schedule(dynamic, 1) num_threads(threads_or_default(nthreads))
+    for (long long c = 0; c < n; ++c) {
+        const long long kidx = cells ? cells[c] : c;
+        CellInit<double> ci;
+        init_cell<double>(g, kidx, nx, ic, nv, vals, 0.01, &ci);
+        double out[64];
+        ls_cell_dp5_cpu(reinterpret_cast<RhsFn>(kr->fn), reinterpret_cast<RhsDualFn>(kd->fn), nx, ci.x, ci.a, nv,
+                        transient, t_end, rtol, atol, h0, gs_every, max_steps, maxv, (uint64_t)kidx, out);
+        bool bad = false;
+        for (int k = 0; k < nx; ++k) {
+            values[c * nx + k] = out[k];
+            if (out[k] == 999.0) bad = true;
+        }
+        flags[c] = bad ? -1 : 1;
+    }
+    return 0;
+}
+
+// Stroboscopic basin classification of one grid (new semantics; no reference
+// counterpart): per cell, RK4 steps_per_period steps per forcing period, the phase
+// variable reset after each period, stroboscopic point P_n = the other state variables;
+// converged when for the smallest k <= 8 |P_n - P_{n-k}|_inf < tol for match_count
+// consecutive periods; canonical point = smallest first (then second) coordinate of the
+// k points of the cycle. out_period: k, 0 (not converged by max_periods), -1 (diverged).
+int orc_basins(void* h, int nPts, int ax, int ay, double lox, double hix, double loy, double hiy, const double* ic,
+               int nv, const double* vals, double period, int steps_per_period, int max_periods, int match_count,
+               double tol, int phase_var, double maxv, const long long* cells, long long ncells, int* out_period,
+               double* out_cx, double* out_cy, int* out_iters, int nthreads) {
+    Krs* k = static_cast<Krs*>(h);
+    if (k->numb_bytes != 8) { g_err = "basins oracle is FP64"; return -1; }
+    const int nx = k->nx;
+    StepFn<double> f = Dispatch<double>::fn(k);
+    const double hs = period / steps_per_period;
+    const long long n = cells ? ncells : (long long)nPts * nPts;
+#pragma omp parallel for schedule(dynamic, 1) num_threads(threads_or_default(nthreads))
+    for (long long c = 0; c < n; ++c) {
+        const long long cell = cells ? cells[c] : c;
+        double x[64], a[64];
+        for (int i = 0; i < nx; ++i) x[i] = ic[i];
+        for (int i = 0; i < nv; ++i) a[i] = vals[i];
+        x[ax] = value_by_idx<double>(cell % nPts, nPts, lox, hix, 0);
+        x[ay] = value_by_idx<double>((cell / nPts) % nPts, nPts, loy, hiy, 0);
+        const int K = 8;
+        std::vector<std::vector<double>> hist;  // hist[j] = P_{n-1-j}
+        int run[8] = {0};
+        int per = 0, it = 0;
+        double cx = 0, cy = 0;
+        for (it = 1; it <= max_periods; ++it) {
+            for (int s = 0; s < steps_per_period; ++s) f(x, a, hs);
+            if (phase_var >= 0) x[phase_var] = ic[phase_var];
+            double checker = 0;
+            for (int i = 0; i < nx; ++i) checker += std::fabs(x[i]);
+            if (std::isnan(checker) || std::isinf(checker) || (maxv != 0 && checker > maxv)) { per = -1; break; }
+            std::vector<double> P;
+            for (int i = 0; i < nx; ++i)
+                if (i != phase_var) P.push_back(x[i]);
+            int found = 0;
+            for (int kk = 1; kk <= K; ++kk) {
+                if (it > kk) {
+                    double d = 0;
+                    for (size_t i = 0; i < P.size(); ++i) d = std::max(d, std::fabs(P[i] - hist[kk - 1][i]));
+                    run[kk - 1] = d < tol ? run[kk - 1] + 1 : 0;
+                    if (!found && run[kk - 1] >= match_count) found = kk;
+                }
+            }
+            if (found) {
+                per = found;
+                cx = P[0];
+                cy = P.size() > 1 ? P[1] : 0.0;
+                for (int j = 0; j + 1 < found; ++j) {
+                    const double px = hist[j][0], py = P.size() > 1 ? hist[j][1] : 0.0;
+                    if (px < cx || (px == cx && py < cy)) { cx = px; cy = py; }
+                }
+                break;
+            }
+            hist.insert(hist.begin(), P);
+            if ((int)hist.size() > K) hist.pop_back();
+        }
+        out_period[c] = per;
+        out_cx[c] = cx;
+        out_cy[c] = cy;
+        out_iters[c] = it > max_periods ? max_periods : it;
+    }
+    return 0;
+}
 
 // numb_bytes: 8 (double), 4 (float), 16 (forward-mode dual: value + tangent)
 void* orc_krs_compile(const char* body, int nx, int numb_bytes) {

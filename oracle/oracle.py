@@ -53,6 +53,18 @@ def lib():
                                 C.c_void_p, C.c_int, C.c_void_p, C.c_double, C.c_double, C.c_double,
                                 C.c_int, C.c_int, C.c_double, C.c_int, C.c_void_p, C.c_longlong,
                                 C.c_void_p, C.c_void_p, C.c_void_p, C.c_int]
+        L.orc_rhs_compile.restype = C.c_void_p
+        L.orc_rhs_compile.argtypes = [C.c_char_p, C.c_int, C.c_int]
+        L.orc_ls2d_dp5.restype = C.c_int
+        L.orc_ls2d_dp5.argtypes = [C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_int, C.c_void_p, C.c_int,
+                                   C.c_void_p, C.c_int, C.c_void_p, C.c_double, C.c_double, C.c_double,
+                                   C.c_double, C.c_double, C.c_int, C.c_longlong, C.c_double, C.c_void_p,
+                                   C.c_longlong, C.c_void_p, C.c_void_p, C.c_int]
+        L.orc_basins.restype = C.c_int
+        L.orc_basins.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_double, C.c_double, C.c_double,
+                                 C.c_double, C.c_void_p, C.c_int, C.c_void_p, C.c_double, C.c_int, C.c_int, C.c_int,
+                                 C.c_double, C.c_int, C.c_double, C.c_void_p, C.c_longlong, C.c_void_p, C.c_void_p,
+                                 C.c_void_p, C.c_void_p, C.c_int]
         _lib = L
     return _lib
 
@@ -162,3 +174,71 @@ def bif1d(krs: Krs, b: dict, max_out=64, pts=None, nthreads=0):
     if rc != 0:
         raise RuntimeError(lib().orc_last_error().decode())
     return counts, peaks.reshape(m, max_out), intervals.reshape(m, max_out)
+
+
+def rhs_statements_from_rk4(body: str) -> str:
+    """Right-hand-side statements recovered from a reference RK4 body: its stage lines
+    `k[i][j] = (expr);` (codegen.cpp scheme_rk4) become `dX[i] = (expr);`."""
+    import re
+    out = []
+    for m in re.finditer(r"^\s*k\[(\d+)\]\[j\] = (.*);\s*$", body, re.M):
+        out.append(f"    dX[{m.group(1)}] = {m.group(2)};")
+    return "\n".join(out)
+
+
+class Rhs:
+    """A right-hand side compiled natively twice: in double and in forward-mode duals."""
+
+    def __init__(self, rk4_body: str, nx: int):
+        self.nx = nx
+        text = rhs_statements_from_rk4(rk4_body)
+        self.h = lib().orc_rhs_compile(text.encode(), nx, 8)
+        self.hd = lib().orc_rhs_compile(text.encode(), nx, 16)
+        if not self.h or not self.hd:
+            raise RuntimeError(lib().orc_last_error().decode())
+
+
+def ls2d_dp5(rhs: Rhs, g: dict, *, t_end, rtol=1e-8, atol=None, h0=0.01, gs_every=10, max_steps=10**8,
+             cells=None, nthreads=0):
+    n = g["n_pts"]
+    ranges = np.array(g["ranges"], dtype=np.float64)
+    ic = np.array(g["ic"], dtype=np.float64)
+    vals = np.array(g["values"], dtype=np.float64)
+    if cells is not None:
+        cells = np.ascontiguousarray(cells, dtype=np.int64)
+        m = len(cells)
+    else:
+        m = n * n
+    values = np.zeros(m * rhs.nx)
+    flags = np.zeros(m, dtype=np.int32)
+    rc = lib().orc_ls2d_dp5(rhs.h, rhs.hd, n, g["par_or_var"], g["idx"][0], g["idx"][1], _ptr(ranges),
+                            g.get("log_mask", 0), _ptr(ic), len(vals), _ptr(vals), g["transient_time"], t_end, rtol,
+                            atol if atol is not None else rtol, h0, gs_every, max_steps, g["max_value"],
+                            _ptr(cells), m if cells is not None else 0, _ptr(values), _ptr(flags), nthreads)
+    if rc != 0:
+        raise RuntimeError(lib().orc_last_error().decode())
+    return values.reshape(m, rhs.nx), flags
+
+
+def basins(krs: Krs, b: dict, cells=None, nthreads=0):
+    """Stroboscopic classification per cell: (period, canonical x, canonical y, periods)."""
+    n = b["n_pts"]
+    ic = np.array(b["ic"], dtype=np.float64)
+    vals = np.array(b["values"], dtype=np.float64)
+    if cells is not None:
+        cells = np.ascontiguousarray(cells, dtype=np.int64)
+        m = len(cells)
+    else:
+        m = n * n
+    per = np.zeros(m, dtype=np.int32)
+    cx = np.zeros(m)
+    cy = np.zeros(m)
+    it = np.zeros(m, dtype=np.int32)
+    rc = lib().orc_basins(krs.h, n, b["axis_x_var"], b["axis_y_var"], b["axis_x_lo"], b["axis_x_hi"],
+                          b["axis_y_lo"], b["axis_y_hi"], _ptr(ic), len(vals), _ptr(vals), b["period"],
+                          b["steps_per_period"], b["max_periods"], b["match_count"], b["match_tol"],
+                          b.get("phase_var", -1), b["max_value"], _ptr(cells), m if cells is not None else 0,
+                          _ptr(per), _ptr(cx), _ptr(cy), _ptr(it), nthreads)
+    if rc != 0:
+        raise RuntimeError(lib().orc_last_error().decode())
+    return per, cx, cy, it

@@ -1,0 +1,108 @@
+"""GPU parity of the Lyapunov-spectrum maps.
+
+FIXED (the reference's LSKernelCUDA method): exact form bit-identical trajectories, so
+spectra match the oracle to 1e-12 relative (log is the only difference).
+DP5 (adaptive Dormand-Prince 5(4) + tangent vectors + modified Gram-Schmidt): the oracle
+runs the same algorithm on the CPU with forward-mode duals for J v; step-size sequences may
+part where an error estimate sits at the acceptance threshold, so agreement is checked by
+tolerance: per-exponent 1e-3 on well-conditioned cells, the known Lorenz divergence
+identity sum(lambda) = -(sigma + 1 + beta), and FP32 against FP64."""
+import numpy as np
+import pytest
+
+import ucb
+from helpers import HYPER_ROSSLER, LORENZ, engine_request, kernel_grid, lle2d_case, rk4_body
+from oracle import oracle as O
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def eng():
+    e = ucb.Engine(0)
+    yield e
+    e.close()
+
+
+def hyper_case(n=6, **kw):
+    d = lle2d_case(n=n, body=rk4_body(HYPER_ROSSLER), nx=4, ic=(-10.0, -6.0, 0.0, 10.0), values=(0, 0.25, 0.05),
+                   param_index=1, param_index_2=2, param_lo=0.1, param_hi=0.35, param_lo_2=0.01, param_hi_2=0.1,
+                   h=0.01, transient_time=5.0, t_max=10.0, NT=0.1, eps=1e-6)
+    d.update(kw)
+    return d
+
+
+def lorenz_case(n=4, **kw):
+    d = lle2d_case(n=n, body=rk4_body(LORENZ), nx=3, ic=(0.1, 0.1, 0.1), values=(0, 10.0, 28.0, 8 / 3),
+                   param_index=1, param_index_2=2, param_lo=9.0, param_hi=11.0, param_lo_2=26.0, param_hi_2=30.0,
+                   h=0.01, transient_time=5.0, t_max=20.0, NT=0.1, eps=1e-6)
+    d.update(kw)
+    return d
+
+
+def ls_request(c, method, **opt):
+    kw = {k: c[k] for k in ("n_pts", "param_index", "param_index_2", "param_lo", "param_hi", "param_lo_2",
+                             "param_hi_2", "h", "transient_time", "t_max", "NT", "eps", "max_value")}
+    extra = {k: c[k] for k in ("t_end", "rtol", "gs_every", "sweep_over_var", "sweep_over_var_2", "var_sweep_index",
+                                "var_sweep_index_2") if k in c}
+    return ucb.Engine.ls2d_request(c["body"], c["nx"], c["ic"], c["values"], method=method, opt=ucb.options(**opt),
+                                   **extra, **kw)
+
+
+@pytest.mark.parametrize("case", ["hyper", "lorenz"])
+def test_fixed_exact_matches_oracle(eng, case):
+    c = hyper_case() if case == "hyper" else lorenz_case()
+    v, f, res = eng.run_ls2d(ls_request(c, ucb.LS_FIXED, precision=ucb.PREC_F64, mode=ucb.MODE_EXACT))
+    ov, of = O.ls2d(O.Krs(c["body"], c["nx"]), kernel_grid(c))
+    ov = ov.reshape(c["nx"], -1)
+    np.testing.assert_array_equal(f, of)
+    np.testing.assert_allclose(v, ov, rtol=1e-12, atol=1e-13)
+    assert res.steps > 0
+
+
+def test_fixed_swap_and_min_max(eng):
+    c = hyper_case(sweep_over_var_2=True, var_sweep_index_2=0, param_lo_2=-11.0, param_hi_2=-9.0)
+    v, f, res = eng.run_ls2d(ls_request(c, ucb.LS_FIXED, precision=ucb.PREC_F64, mode=ucb.MODE_EXACT))
+    ov, of = O.ls2d(O.Krs(c["body"], c["nx"]), kernel_grid(c))
+    np.testing.assert_array_equal(f, of)
+    np.testing.assert_allclose(v, ov.reshape(c["nx"], -1), rtol=1e-12, atol=1e-13)
+
+
+@pytest.mark.parametrize("prec", [ucb.PREC_F64, ucb.PREC_F32])
+def test_dp5_lorenz_divergence_identity(eng, prec):
+    c = lorenz_case(n=2, param_lo=10.0, param_hi=10.0, param_lo_2=28.0, param_hi_2=28.0, transient_time=10.0,
+                    t_end=300.0, gs_every=10)
+    v, f, res = eng.run_ls2d(ls_request(c, ucb.LS_DP5, precision=prec))
+    assert (f == 1).all()
+    s = v.sum(axis=0)
+    tol = 1e-3 if prec == ucb.PREC_F64 else 2e-2
+    np.testing.assert_allclose(s, -(10 + 1 + 8 / 3), atol=tol)
+    assert (np.abs(v[0] - 0.906) < 0.08).all()
+
+
+def test_dp5_matches_oracle(eng):
+    c = hyper_case(n=4, transient_time=20.0, t_end=200.0, gs_every=10)
+    v, f, res = eng.run_ls2d(ls_request(c, ucb.LS_DP5, precision=ucb.PREC_F64))
+    g = kernel_grid(c)
+    ov, of = O.ls2d_dp5(O.Rhs(c["body"], 4), g, t_end=200.0, rtol=1e-8, h0=c["h"], gs_every=10)
+    np.testing.assert_array_equal(f, of)
+    ov = ov.T
+    # the sum of the spectrum (the time-averaged divergence) is robust to step-sequence
+    # differences; individual exponents of hyperchaotic cells are finite-time samples
+    np.testing.assert_allclose(v.sum(axis=0), ov.sum(axis=0), atol=5e-3)
+    assert np.median(np.abs(v - ov)) < 5e-3
+
+
+def test_dp5_f32_close_to_f64(eng):
+    # FP32 state and tangent vectors at the FP32 tolerance (rtol 1e-5) against FP64 at the
+    # same tolerance: the strongly contracting 4th exponents (-15 .. -5400 on this grid)
+    # are resolved because the error norm covers the tangent vectors; the remaining
+    # dependence on rtol itself is a property of the method, not of the precision.
+    c = hyper_case(n=4, transient_time=20.0, t_end=100.0, gs_every=10, rtol=1e-5)
+    v64, f64, _ = eng.run_ls2d(ls_request(c, ucb.LS_DP5, precision=ucb.PREC_F64))
+    v32, f32, _ = eng.run_ls2d(ls_request(c, ucb.LS_DP5, precision=ucb.PREC_F32))
+    np.testing.assert_array_equal(f32, f64)
+    ok = f64 == 1
+    assert ok.sum() >= 3
+    s32, s64 = v32.sum(axis=0)[ok], v64.sum(axis=0)[ok]
+    np.testing.assert_allclose(s32, s64, rtol=0.02, atol=0.5)

@@ -47,6 +47,8 @@ struct SystemCode {
     bool has_jvp = false;
     std::string code;     // device source defining calculateDiscreteModel or ucb_rhs/ucb_jvp
     int flops_step = 0;   // algorithmic FLOPs of one step (native form; 0 if unknown)
+    int flops_rhs = 0;    // FLOPs of one right-hand-side evaluation (recognised bodies)
+    int flops_jvp = 0;    // FLOPs of one J(x) v product (recognised bodies)
     std::string note;     // why the exact form was chosen, when native was requested
 };
 
@@ -92,6 +94,11 @@ struct ParamPack {
 // Launches a kernel with one by-value struct parameter.
 bool launch_packed(ucb_engine* e, CUfunction f, int grid, int block, cudaStream_t stream, ParamPack& pk,
                    std::string& err);
+
+// Validation and axis mapping of run_lle_2d (shared by the 2-D maps): kernel-order sweep,
+// (int)(t_max/NT), (int)(transient/h) and (size_t)(NT/h) in numb.
+bool plan_sweep2d(const ucb_lle2d_request& q, SweepMap& m, int& n_blocks, int& skip, long long& nt_steps,
+                  std::string& err);
 
 // Launch helper: persistent grid size for a kernel.
 int persistent_grid(ucb_engine* e, CUfunction f, int block, long long work_items);

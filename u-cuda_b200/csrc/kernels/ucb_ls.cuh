@@ -1,0 +1,464 @@
+// ucb_ls.cuh — full Lyapunov spectrum maps (NVRTC header, after ucb_device.cuh).
+//
+// Two methods, one thread per cell, everything in registers, persistent grid:
+//
+//  * UCB_LS_FIXED (the reference's method, LSKernelCUDA cudaLibrary.cu:2878-3073):
+//    fixed-step trajectory + N shadow probes at distance eps, random unit directions
+//    (RNG subsequence = cell index) orthonormalised once, then every NT block: advance
+//    x and the probes, subtract x, classical Gram-Schmidt (gramSchmidtProcess :2848-2874,
+//    projections against the unnormalised b_j), sum log(|b_k| / eps), re-seat the probes.
+//
+//  * UCB_LS_DP5: tangent-linear spectrum with the adaptive Dormand-Prince 5(4) pair
+//    (Dormand & Prince 1980, FSAL) integrating x' = f(x) and V' = J(x) V for N tangent
+//    vectors, with the mixed absolute/relative RMS error norm taken over the whole
+//    augmented state (x and V: controlling x alone lets the step grow past what the
+//    contracting tangent directions need, and the most negative exponents then follow the
+//    method's stability function instead of the flow), step factor 0.9 err^-1/5 clamped
+//    to [0.2, 5] (2 after a rejection), with
+//    modified Gram-Schmidt every `gs_every` accepted steps — or earlier, when the time
+//    since the last pass times the running estimate of lambda_1 - lambda_N exceeds the
+//    precision's budget (UCB_GS_BUDGET nats: 20 for FP64, 8 for FP32), because beyond it
+//    the most contracted direction sinks below the rounding of the stored tangent vectors;
+//    the norms, log sums, time and the error norm are FP64 whatever numb is.
+#pragma once
+
+struct UcbLsParams {
+    long long total;
+    long long cell_offset;
+    int n_pts;
+    int swap_xy;
+    int n_blocks;          // (int)(tMax / NT)   [fixed]
+    int gs_every;          // accepted steps between MGS   [dp5]
+    long long skip;        // (int)(transient / h)        [fixed]
+    long long nt_steps;    // (size_t)(NT / h) in numb     [fixed]
+    long long max_steps;   // step attempt cap per cell   [dp5]
+    numb h, NT, tmax, eps, maxv, transient;
+    double rtol, atol, t_end, h0;   // [dp5]
+    numb ic[UCB_NX];
+    numb vals[UCB_NV];
+    const numb* axis0;
+    const numb* axis1;
+    double* out_values;    // plane-major: values[k * n^2 + cell]
+    int* out_flags;
+    unsigned long long* counter;
+    unsigned long long* steps;
+};
+
+namespace ucbdev {
+
+__device__ __forceinline__ long long ls_out_cell(const UcbLsParams& p, long long kidx) {
+    if (!p.swap_xy) return kidx;
+    const long long kix = kidx % p.n_pts, kiy = kidx / p.n_pts;
+    return kix * p.n_pts + kiy;
+}
+
+__device__ __forceinline__ void ls_store(const UcbLsParams& p, long long kidx, const double* v) {
+    const long long cell = ls_out_cell(p, kidx);
+    const long long plane = (long long)p.n_pts * p.n_pts;
+    bool bad = false;
+#pragma unroll
+    for (int k = 0; k < UCB_NX; ++k) {
+        p.out_values[k * plane + cell] = v[k];
+        if (v[k] == 999.0 || v[k] == -999.0) bad = true;
+    }
+    p.out_flags[cell] = bad ? -1 : 1;
+}
+
+#if defined(UCB_LS_FIXED)
+// gramSchmidtProcess(a -> b, dens): classical GS, rows are vectors.
+__device__ __forceinline__ void gram_schmidt_classical(const numb (*a)[UCB_NX], numb (*b)[UCB_NX], numb* dens) {
+#pragma unroll
+    for (int i = 0; i < UCB_NX; ++i) {
+#pragma unroll
+        for (int j = 0; j < UCB_NX; ++j) b[i][j] = a[i][j];
+#pragma unroll
+        for (int j = 0; j < i; ++j) {
+            numb num = 0, den = 0;
+#pragma unroll
+            for (int l = 0; l < UCB_NX; ++l) {
+                num += a[i][l] * b[j][l];
+                den += b[j][l] * b[j][l];
+            }
+            const numb frac = den == 0 ? 0 : num / den;
+#pragma unroll
+            for (int l = 0; l < UCB_NX; ++l) b[i][l] -= frac * b[j][l];
+        }
+    }
+#pragma unroll
+    for (int i = 0; i < UCB_NX; ++i) {
+        numb den = 0;
+#pragma unroll
+        for (int j = 0; j < UCB_NX; ++j) den += b[i][j] * b[i][j];
+        den = sqrt(den);
+#pragma unroll
+        for (int j = 0; j < UCB_NX; ++j) b[i][j] = den == 0 ? 0 : b[i][j] / den;
+        if (dens) dens[i] = den;
+    }
+}
+
+// x and the N probes advanced in lock step (the reference advances them one after the
+// other; they never interact inside a block). 0 if any diverged.
+template <class S>
+__device__ __forceinline__ int loop_probes(const S& s, numb* x, numb (*y)[UCB_NX], const numb* a, numb h,
+                                           long long iters, numb maxValue, long long& ns) {
+    for (long long i0 = 0; i0 < iters; i0 += kCheckInterval) {
+        s.step(x, a, h);
+#pragma unroll
+        for (int j = 0; j < UCB_NX; ++j) s.step(y[j], a, h);
+        ns += UCB_NX + 1;
+        bool bad = diverged(x, maxValue);
+#pragma unroll
+        for (int j = 0; j < UCB_NX; ++j) bad = bad || diverged(y[j], maxValue);
+        if (bad) return 0;
+        const long long n = (iters - i0 < kCheckInterval) ? iters - i0 : kCheckInterval;
+        for (long long i = 1; i < n; ++i) {
+            s.step(x, a, h);
+#pragma unroll
+            for (int j = 0; j < UCB_NX; ++j) s.step(y[j], a, h);
+        }
+        ns += (long long)(UCB_NX + 1) * (n - 1);
+    }
+#if UCB_EXTRA_STEP
+    s.step(x, a, h);
+#pragma unroll
+    for (int j = 0; j < UCB_NX; ++j) s.step(y[j], a, h);
+    ns += UCB_NX + 1;
+#endif
+    return 1;
+}
+
+__device__ __forceinline__ void ls_cell_fixed(const UcbLsParams& p, long long kidx, long long& ns) {
+    double outv[UCB_NX];
+    const CellAxes c = cell_axes(kidx, p.n_pts);
+    numb h = p.h;
+    long long nt = p.nt_steps, skip = p.skip;
+#if UCB_HAXIS == 0
+    h = p.axis0[c.i0];
+#elif UCB_HAXIS == 1
+    h = p.axis1[c.i1];
+#endif
+#if UCB_HAXIS != -1
+    nt = (long long)ceil(p.NT / h);
+    skip = (long long)ceil(p.transient / h);
+#endif
+    if (!(h > 0)) {
+#pragma unroll
+        for (int m = 0; m < UCB_NX; ++m) outv[m] = (double)nan("");
+        ls_store(p, kidx, outv);
+        return;
+    }
+    numb x[UCB_NX], a[UCB_NV];
+#pragma unroll
+    for (int i = 0; i < UCB_NX; ++i) x[i] = p.ic[i];
+#pragma unroll
+    for (int i = 0; i < UCB_NV; ++i) a[i] = p.vals[i];
+    apply_sweep(c, p.axis0, p.axis1, x, a);
+    numb y[UCB_NX][UCB_NX], z[UCB_NX][UCB_NX], dens[UCB_NX];
+    double result[UCB_NX];
+    {
+        Rng st;
+        rng_init(1234567891ULL, (unsigned long long)kidx, 0ULL, &st);
+#pragma unroll
+        for (int j = 0; j < UCB_NX; ++j) {
+            numb zPower = 0;
+#pragma unroll
+            for (int i = 0; i < UCB_NX; ++i) {
+                z[j][i] = rng_uniform(&st) - 0.5;
+                zPower += z[j][i] * z[j][i];
+            }
+            zPower = sqrt(zPower);
+#pragma unroll
+            for (int i = 0; i < UCB_NX; ++i) z[j][i] /= zPower;
+        }
+    }
+    const Stepper st(h);
+    if (loop_single(st, x, a, h, skip, p.maxv, ns) == 0) {
+#pragma unroll
+        for (int m = 0; m < UCB_NX; ++m) outv[m] = 999.0;
+        ls_store(p, kidx, outv);
+        return;
+    }
+    gram_schmidt_classical(z, y, nullptr);
+#pragma unroll
+    for (int j = 0; j < UCB_NX; ++j)
+#pragma unroll
+        for (int i = 0; i < UCB_NX; ++i) y[j][i] = y[j][i] * p.eps + x[i];
+    numb res_n[UCB_NX];
+#pragma unroll
+    for (int k = 0; k < UCB_NX; ++k) res_n[k] = 0;
+    for (int b = 0; b < p.n_blocks; ++b) {
+        if (loop_probes(st, x, y, a, h, nt, p.maxv, ns) == 0) {
+#pragma unroll
+            for (int m = 0; m < UCB_NX; ++m) outv[m] = 999.0;
+            ls_store(p, kidx, outv);
+            return;
+        }
+#pragma unroll
+        for (int k = 0; k < UCB_NX; ++k)
+#pragma unroll
+            for (int l = 0; l < UCB_NX; ++l) y[k][l] = y[k][l] - x[l];
+        gram_schmidt_classical(y, z, dens);
+#pragma unroll
+        for (int k = 0; k < UCB_NX; ++k) {
+            res_n[k] += log(dens[k] / p.eps);
+#pragma unroll
+            for (int j = 0; j < UCB_NX; ++j) y[k][j] = (numb)(x[j] + z[k][j] * p.eps);
+        }
+    }
+#pragma unroll
+    for (int k = 0; k < UCB_NX; ++k) result[k] = (double)(res_n[k] / p.tmax);
+    ls_store(p, kidx, result);
+}
+#endif  // UCB_LS_FIXED
+
+#if defined(UCB_LS_DP5)
+#ifndef UCB_GS_BUDGET
+#define UCB_GS_BUDGET 20.0
+#endif
+// Dormand-Prince 5(4) coefficients (Dormand & Prince, J. Comp. Appl. Math. 6, 1980).
+#define DP_A21 (1.0 / 5.0)
+#define DP_A31 (3.0 / 40.0)
+#define DP_A32 (9.0 / 40.0)
+#define DP_A41 (44.0 / 45.0)
+#define DP_A42 (-56.0 / 15.0)
+#define DP_A43 (32.0 / 9.0)
+#define DP_A51 (19372.0 / 6561.0)
+#define DP_A52 (-25360.0 / 2187.0)
+#define DP_A53 (64448.0 / 6561.0)
+#define DP_A54 (-212.0 / 729.0)
+#define DP_A61 (9017.0 / 3168.0)
+#define DP_A62 (-355.0 / 33.0)
+#define DP_A63 (46732.0 / 5247.0)
+#define DP_A64 (49.0 / 176.0)
+#define DP_A65 (-5103.0 / 18656.0)
+#define DP_B1 (35.0 / 384.0)
+#define DP_B3 (500.0 / 1113.0)
+#define DP_B4 (125.0 / 192.0)
+#define DP_B5 (-2187.0 / 6784.0)
+#define DP_B6 (11.0 / 84.0)
+#define DP_E1 (71.0 / 57600.0)
+#define DP_E3 (-71.0 / 16695.0)
+#define DP_E4 (71.0 / 1920.0)
+#define DP_E5 (-17253.0 / 339200.0)
+#define DP_E6 (22.0 / 525.0)
+#define DP_E7 (-1.0 / 40.0)
+
+// Modified Gram-Schmidt on the rows of V; log of the norms added to acc (FP64).
+__device__ __forceinline__ bool mgs(numb (*V)[UCB_NX], double* acc) {
+#pragma unroll
+    for (int k = 0; k < UCB_NX; ++k) {
+#pragma unroll
+        for (int j = 0; j < k; ++j) {
+            double d = 0;
+#pragma unroll
+            for (int l = 0; l < UCB_NX; ++l) d = fma((double)V[k][l], (double)V[j][l], d);
+            const numb dn = (numb)d;
+#pragma unroll
+            for (int l = 0; l < UCB_NX; ++l) V[k][l] = fma(-dn, V[j][l], V[k][l]);
+        }
+        double n2 = 0;
+#pragma unroll
+        for (int l = 0; l < UCB_NX; ++l) n2 = fma((double)V[k][l], (double)V[k][l], n2);
+        const double nrm = sqrt(n2);
+        if (!(nrm > 0) || !isfinite(nrm)) return false;
+        acc[k] += log(nrm);
+        const numb inv = (numb)(1.0 / nrm);
+#pragma unroll
+        for (int l = 0; l < UCB_NX; ++l) V[k][l] *= inv;
+    }
+    return true;
+}
+
+// One DP5 step of the state: stage points X2..X6, the 5th-order solution xn and its
+// derivative k7 (FSAL), and the RMS error norm of the embedded 4th-order difference.
+struct Dp5State {
+    numb X[6][UCB_NX];  // stage points X1 (= x) .. X6
+    numb k1[UCB_NX], k7[UCB_NX], xn[UCB_NX];
+};
+
+__device__ __forceinline__ double dp5_state_step(Dp5State& S, const numb* a, numb hn, double h, double rtol,
+                                                 double atol) {  // returns the sum of squared scaled errors
+    numb k2[UCB_NX], k3[UCB_NX], k4[UCB_NX], k5[UCB_NX], k6[UCB_NX];
+    const numb* x = S.X[0];
+#pragma unroll
+    for (int i = 0; i < UCB_NX; ++i) S.X[1][i] = x[i] + hn * ((numb)DP_A21 * S.k1[i]);
+    ucb_rhs(S.X[1], a, k2);
+#pragma unroll
+    for (int i = 0; i < UCB_NX; ++i) S.X[2][i] = x[i] + hn * ((numb)DP_A31 * S.k1[i] + (numb)DP_A32 * k2[i]);
+    ucb_rhs(S.X[2], a, k3);
+#pragma unroll
+    for (int i = 0; i < UCB_NX; ++i)
+        S.X[3][i] = x[i] + hn * ((numb)DP_A41 * S.k1[i] + (numb)DP_A42 * k2[i] + (numb)DP_A43 * k3[i]);
+    ucb_rhs(S.X[3], a, k4);
+#pragma unroll
+    for (int i = 0; i < UCB_NX; ++i)
+        S.X[4][i] = x[i] + hn * ((numb)DP_A51 * S.k1[i] + (numb)DP_A52 * k2[i] + (numb)DP_A53 * k3[i] +
+                                 (numb)DP_A54 * k4[i]);
+    ucb_rhs(S.X[4], a, k5);
+#pragma unroll
+    for (int i = 0; i < UCB_NX; ++i)
+        S.X[5][i] = x[i] + hn * ((numb)DP_A61 * S.k1[i] + (numb)DP_A62 * k2[i] + (numb)DP_A63 * k3[i] +
+                                 (numb)DP_A64 * k4[i] + (numb)DP_A65 * k5[i]);
+    ucb_rhs(S.X[5], a, k6);
+#pragma unroll
+    for (int i = 0; i < UCB_NX; ++i)
+        S.xn[i] = x[i] + hn * ((numb)DP_B1 * S.k1[i] + (numb)DP_B3 * k3[i] + (numb)DP_B4 * k4[i] +
+                               (numb)DP_B5 * k5[i] + (numb)DP_B6 * k6[i]);
+    ucb_rhs(S.xn, a, S.k7);
+    double err2 = 0;
+#pragma unroll
+    for (int i = 0; i < UCB_NX; ++i) {
+        const double e = h * ((double)DP_E1 * S.k1[i] + (double)DP_E3 * k3[i] + (double)DP_E4 * k4[i] +
+                              (double)DP_E5 * k5[i] + (double)DP_E6 * k6[i] + (double)DP_E7 * S.k7[i]);
+        const double sc = atol + rtol * fmax(fabs((double)x[i]), fabs((double)S.xn[i]));
+        err2 += (e / sc) * (e / sc);
+    }
+    return err2;
+}
+
+// One tangent vector through the same DP5 stages (v' = J(x) v with J at the stored stage
+// points): writes the 5th-order vn and returns its sum of squared scaled errors.
+__device__ __forceinline__ double dp5_tangent_step(const Dp5State& S, const numb* a, numb hn, double h, double rtol,
+                                                   double atol, const numb* v, numb* vn) {
+    numb L1[UCB_NX], L2[UCB_NX], L3[UCB_NX], L4[UCB_NX], L5[UCB_NX], L6[UCB_NX], vt[UCB_NX];
+    ucb_jvp(S.X[0], a, v, L1);
+#pragma unroll
+    for (int i = 0; i < UCB_NX; ++i) vt[i] = v[i] + hn * ((numb)DP_A21 * L1[i]);
+    ucb_jvp(S.X[1], a, vt, L2);
+#pragma unroll
+    for (int i = 0; i < UCB_NX; ++i) vt[i] = v[i] + hn * ((numb)DP_A31 * L1[i] + (numb)DP_A32 * L2[i]);
+    ucb_jvp(S.X[2], a, vt, L3);
+#pragma unroll
+    for (int i = 0; i < UCB_NX; ++i)
+        vt[i] = v[i] + hn * ((numb)DP_A41 * L1[i] + (numb)DP_A42 * L2[i] + (numb)DP_A43 * L3[i]);
+    ucb_jvp(S.X[3], a, vt, L4);
+#pragma unroll
+    for (int i = 0; i < UCB_NX; ++i)
+        vt[i] = v[i] + hn * ((numb)DP_A51 * L1[i] + (numb)DP_A52 * L2[i] + (numb)DP_A53 * L3[i] + (numb)DP_A54 * L4[i]);
+    ucb_jvp(S.X[4], a, vt, L5);
+#pragma unroll
+    for (int i = 0; i < UCB_NX; ++i)
+        vt[i] = v[i] + hn * ((numb)DP_A61 * L1[i] + (numb)DP_A62 * L2[i] + (numb)DP_A63 * L3[i] +
+                             (numb)DP_A64 * L4[i] + (numb)DP_A65 * L5[i]);
+    ucb_jvp(S.X[5], a, vt, L6);
+#pragma unroll
+    for (int i = 0; i < UCB_NX; ++i)
+        vn[i] = v[i] + hn * ((numb)DP_B1 * L1[i] + (numb)DP_B3 * L3[i] + (numb)DP_B4 * L4[i] + (numb)DP_B5 * L5[i] +
+                             (numb)DP_B6 * L6[i]);
+    ucb_jvp(S.xn, a, vn, L2);  // L7, reusing L2's registers
+    double err2 = 0;
+#pragma unroll
+    for (int i = 0; i < UCB_NX; ++i) {
+        const double e = h * ((double)DP_E1 * L1[i] + (double)DP_E3 * L3[i] + (double)DP_E4 * L4[i] +
+                              (double)DP_E5 * L5[i] + (double)DP_E6 * L6[i] + (double)DP_E7 * L2[i]);
+        const double sc = atol + rtol * fmax(fabs((double)v[i]), fabs((double)vn[i]));
+        err2 += (e / sc) * (e / sc);
+    }
+    return err2;
+}
+
+__device__ __forceinline__ void ls_cell_dp5(const UcbLsParams& p, long long kidx, long long& ns) {
+    double outv[UCB_NX];
+    const CellAxes c = cell_axes(kidx, p.n_pts);
+    Dp5State S;
+    numb a[UCB_NV];
+#pragma unroll
+    for (int i = 0; i < UCB_NX; ++i) S.X[0][i] = p.ic[i];
+#pragma unroll
+    for (int i = 0; i < UCB_NV; ++i) a[i] = p.vals[i];
+    apply_sweep(c, p.axis0, p.axis1, S.X[0], a);
+    numb V[UCB_NX][UCB_NX];
+    {
+        Rng st;
+        rng_init(1234567891ULL, (unsigned long long)kidx, 0ULL, &st);
+#pragma unroll
+        for (int j = 0; j < UCB_NX; ++j)
+#pragma unroll
+            for (int i = 0; i < UCB_NX; ++i) V[j][i] = rng_uniform(&st) - 0.5;
+    }
+    double acc[UCB_NX], junk[UCB_NX];
+#pragma unroll
+    for (int k = 0; k < UCB_NX; ++k) acc[k] = junk[k] = 0;
+    bool ok = mgs(V, junk);
+    // The transient [0, transient) moves the state only; tangents are measured over
+    // [transient, transient + t_end] with MGS every gs_every accepted steps and at the end.
+    double t = 0.0;
+    const double t_stop = (double)p.transient + p.t_end;
+    double h = p.h0, facmax = 5.0;
+    int since_gs = 0;
+    double t_gs = 0.0, t_meas = 0.0, spread = 1e300;  // spread: running lambda_1 - lambda_N
+    bool measuring = !((double)p.transient > 0);
+    long long attempts = 0;
+    ucb_rhs(S.X[0], a, S.k1);
+    while (ok && t < t_stop) {
+        if (++attempts > p.max_steps) { ok = false; break; }
+        const double t_target = measuring ? t_stop : (double)p.transient;
+        bool last = false;
+        if (t + h >= t_target) { h = t_target - t; last = true; }
+        const numb hn = (numb)h;
+        const double ex2 = dp5_state_step(S, a, hn, h, p.rtol, p.atol);
+        ns += 1;
+        double err = sqrt(ex2 / UCB_NX);
+        numb Vn[UCB_NX][UCB_NX];
+        if (err <= 1.0 && measuring) {
+            double ev2 = 0;
+#pragma unroll
+            for (int k = 0; k < UCB_NX; ++k) ev2 += dp5_tangent_step(S, a, hn, h, p.rtol, p.atol, V[k], Vn[k]);
+            err = sqrt((ex2 + ev2) / (UCB_NX + UCB_NX * UCB_NX));
+        }
+        if (!isfinite(err)) { ok = false; break; }
+        if (err <= 1.0) {
+            if (measuring) {
+#pragma unroll
+                for (int k = 0; k < UCB_NX; ++k)
+#pragma unroll
+                    for (int i = 0; i < UCB_NX; ++i) V[k][i] = Vn[k][i];
+            }
+            const double t_new = last ? t_target : t + h;
+            if (measuring) t_gs += t_new - t;
+            t = t_new;
+#pragma unroll
+            for (int i = 0; i < UCB_NX; ++i) { S.X[0][i] = S.xn[i]; S.k1[i] = S.k7[i]; }
+            if (diverged(S.X[0], p.maxv)) { ok = false; break; }
+            if (measuring && (++since_gs >= p.gs_every || last || t_gs * spread > UCB_GS_BUDGET)) {
+                ok = mgs(V, acc);
+                since_gs = 0;
+                t_meas += t_gs;
+                t_gs = 0.0;
+                spread = fmax(0.0, (acc[0] - acc[UCB_NX - 1]) / t_meas);
+            }
+            if (last && !measuring) measuring = true;
+            const double fac = (err > 0) ? 0.9 * pow(err, -0.2) : facmax;
+            h *= fmin(facmax, fmax(0.2, fac));
+            facmax = 5.0;
+        } else {
+            h *= fmax(0.2, 0.9 * pow(err, -0.2));
+            facmax = 2.0;
+            if (!(h > 1e-14)) { ok = false; break; }
+        }
+    }
+#pragma unroll
+    for (int k = 0; k < UCB_NX; ++k) outv[k] = ok ? acc[k] / p.t_end : 999.0;
+    ls_store(p, kidx, outv);
+}
+#endif  // UCB_LS_DP5
+
+}  // namespace ucbdev
+
+extern "C" __global__ void __launch_bounds__(128) ucb_ls_kernel(const UcbLsParams p) {
+    const int lane = threadIdx.x & 31;
+    long long ns = 0;
+    for (;;) {
+        const long long base = ucbdev::warp_fetch(p.counter, lane);
+        if (base >= p.total) break;
+        const long long i = base + lane;
+        if (i < p.total) {
+#if defined(UCB_LS_DP5)
+            ucbdev::ls_cell_dp5(p, p.cell_offset + i, ns);
+#else
+            ucbdev::ls_cell_fixed(p, p.cell_offset + i, ns);
+#endif
+        }
+    }
+    ucbdev::warp_add_steps(p.steps, ns, lane);
+}

@@ -44,6 +44,23 @@ bool validate_bif(const ucb_bif1d_request& q, std::string& err) {
     return true;
 }
 
+CompileRequest bif_compile_request(const ucb_bif1d_request& q, SystemCode& sys) {
+    SweepMap m;
+    m.dim = 1;
+    m.par_or_var = q.sweep_over_var ? 0 : 1;
+    m.idx[0] = q.sweep_over_h ? 0 : (q.sweep_over_var ? q.var_sweep_index : q.param_index);
+    m.h_axis = q.sweep_over_h ? 0 : -1;
+    sys = make_system_code(q.krs_body, q.amount_of_x, q.n_values, q.opt.precision, q.opt.mode, false);
+    CompileRequest rq;
+    rq.name = "ucb_bif1d.cu";
+    rq.source = make_prelude(q.opt.precision, q.amount_of_x, q.n_values, m, true, sys, {}) +
+                "#include \"ucb_device.cuh\"\n#include \"ucb_bif.cuh\"\n";
+    rq.headers = device_headers();
+    rq.options.push_back(sys.exact ? "--fmad=false" : "--fmad=true");
+    rq.kernels = {"ucb_bif_kernel"};
+    return rq;
+}
+
 int fail(ucb_engine* e, ucb_bif1d_result* r, int code, const std::string& msg) {
     e->last_error = msg;
     std::snprintf(r->error, sizeof r->error, "%s", msg.c_str());
@@ -52,6 +69,22 @@ int fail(ucb_engine* e, ucb_bif1d_result* r, int code, const std::string& msg) {
 }
 
 }  // namespace
+
+extern "C" int ucb_precompile_bif1d(const ucb_bif1d_request* req, char* err_out, int err_len) {
+    std::string err;
+    if (!req || !validate_bif(*req, err)) {
+        if (err_out && err_len > 0) std::snprintf(err_out, (size_t)err_len, "%s", err.c_str());
+        return UCB_E_INVALID;
+    }
+    SystemCode sys;
+    CompileRequest rq = bif_compile_request(*req, sys);
+    if (!precompile_to_disk(rq, err)) {
+        if (err_out && err_len > 0) std::snprintf(err_out, (size_t)err_len, "%s", err.c_str());
+        return UCB_E_COMPILE;
+    }
+    if (err_out && err_len > 0) std::snprintf(err_out, (size_t)err_len, "%s", sys.note.c_str());
+    return UCB_OK;
+}
 
 extern "C" int ucb_run_bif1d(ucb_engine* e, const ucb_bif1d_request* req, ucb_bif1d_result* res) {
     if (!e || !req || !res) return UCB_E_INVALID;
@@ -79,19 +112,8 @@ extern "C" int ucb_run_bif1d(ucb_engine* e, const ucb_bif1d_request* req, ucb_bi
     if (pointsInBlock <= 0) return fail(e, res, UCB_E_INVALID, "computed amountOfPointsInBlock <= 0");
     if (!ensure_init(e, err)) return fail(e, res, UCB_E_NOGPU, err);
 
-    SweepMap m;
-    m.dim = 1;
-    m.par_or_var = q.sweep_over_var ? 0 : 1;
-    m.idx[0] = q.sweep_over_h ? 0 : (q.sweep_over_var ? q.var_sweep_index : q.param_index);
-    m.h_axis = q.sweep_over_h ? 0 : -1;
-    SystemCode sys = make_system_code(q.krs_body, q.amount_of_x, q.n_values, prec, q.opt.mode, false);
-    CompileRequest rq;
-    rq.name = "ucb_bif1d.cu";
-    rq.source = make_prelude(prec, q.amount_of_x, q.n_values, m, true, sys, {}) +
-                "#include \"ucb_device.cuh\"\n#include \"ucb_bif.cuh\"\n";
-    rq.headers = device_headers();
-    rq.options.push_back(sys.exact ? "--fmad=false" : "--fmad=true");
-    rq.kernels = {"ucb_bif_kernel"};
+    SystemCode sys;
+    CompileRequest rq = bif_compile_request(q, sys);
     auto mod = e->modules.get(rq, err);
     if (!mod) return fail(e, res, UCB_E_COMPILE, err);
     CUfunction fn = mod->functions["ucb_bif_kernel"];

@@ -159,6 +159,8 @@ SystemCode make_system_code(const std::string& krs_body, int nx, int nv, int pre
             s.exact = false;
             s.code = fe::emit_rhs_device(r, precision == UCB_PREC_F32);
             s.flops_step = fe::rk4_step_flops(r);
+            s.flops_rhs = fe::rhs_flops(r);
+            for (auto& f : r.f) s.flops_jvp += fe::flops(fe::directional_derivative(f));
             if (want_jvp) {
                 s.code += fe::emit_jvp_device(r, precision == UCB_PREC_F32);
                 s.has_jvp = true;
@@ -457,6 +459,17 @@ int enqueue_lle(ucb_engine* e, const ucb_lle2d_request& q, const LlePlan& plan, 
 }
 
 }  // namespace
+
+bool plan_sweep2d(const ucb_lle2d_request& q, SweepMap& m, int& n_blocks, int& skip, long long& nt_steps,
+                  std::string& err) {
+    LlePlan p;
+    if (!plan_lle2d(q, p, err)) return false;
+    m = p.map;
+    n_blocks = p.amountOfPointsInBlock;
+    skip = p.amountOfPointsForSkip;
+    nt_steps = p.nt_steps;
+    return true;
+}
 
 // Internal hooks used by the scratch-array entry point (noalloc.cu).
 int lle2d_plan_and_find(ucb_engine* e, const ucb_lle2d_request& q, bool load_if_missing, std::string& err,

@@ -1,0 +1,238 @@
+// Lyapunov spectrum 2D host orchestration (run_ls_2d, parametric_engine.cpp:3430-3786):
+// the LLE-2D validation and axis mapping, plane-major results, per-plane min/max over
+// valid cells, CSV. Device side: ucb_ls.cuh.
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <limits>
+
+#include "csv_export.h"
+#include "engine_internal.h"
+
+using namespace ucb;
+
+namespace {
+
+int fail(ucb_engine* e, ucb_ls2d_result* r, int code, const std::string& msg) {
+    e->last_error = msg;
+    std::snprintf(r->error, sizeof r->error, "%s", msg.c_str());
+    r->ok = 0;
+    return code;
+}
+
+ucb_lle2d_request as_lle(const ucb_ls2d_request& q) {
+    ucb_lle2d_request l{};
+    l.krs_body = q.krs_body;
+    l.amount_of_x = q.amount_of_x;
+    l.initial_conditions = q.initial_conditions;
+    l.base_values = q.base_values;
+    l.n_values = q.n_values;
+    l.sweep_over_var = q.sweep_over_var;
+    l.sweep_over_var_2 = q.sweep_over_var_2;
+    l.sweep_over_h = q.sweep_over_h;
+    l.sweep_over_h_2 = q.sweep_over_h_2;
+    l.log_scale = q.log_scale;
+    l.log_scale_2 = q.log_scale_2;
+    l.param_index = q.param_index;
+    l.var_sweep_index = q.var_sweep_index;
+    l.param_index_2 = q.param_index_2;
+    l.var_sweep_index_2 = q.var_sweep_index_2;
+    l.param_lo = q.param_lo;
+    l.param_hi = q.param_hi;
+    l.param_lo_2 = q.param_lo_2;
+    l.param_hi_2 = q.param_hi_2;
+    l.n_pts = q.n_pts;
+    l.h = q.h;
+    l.transient_time = q.transient_time;
+    l.t_max = q.t_max;
+    l.NT = q.NT;
+    l.eps = q.eps;
+    l.max_value = q.max_value;
+    l.opt = q.opt;
+    return l;
+}
+
+CompileRequest ls_compile_request(const ucb_ls2d_request& q, const SweepMap& m, SystemCode& sys) {
+    const bool dp5 = q.method == UCB_LS_DP5;
+    const int prec = q.opt.precision;
+    sys = make_system_code(q.krs_body, q.amount_of_x, q.n_values, prec, dp5 ? UCB_MODE_NATIVE : q.opt.mode, dp5);
+    CompileRequest rq;
+    rq.name = "ucb_ls2d.cu";
+    rq.source = make_prelude(prec, q.amount_of_x, q.n_values, m, q.opt.nominal_steps == 0, sys,
+                             {dp5 ? "UCB_LS_DP5 1" : "UCB_LS_FIXED 1",
+                              prec == UCB_PREC_F64 ? "UCB_GS_BUDGET 20.0" : "UCB_GS_BUDGET 8.0"}) +
+                "#include \"ucb_device.cuh\"\n#include \"ucb_ls.cuh\"\n";
+    rq.headers = device_headers();
+    rq.options.push_back(sys.exact ? "--fmad=false" : "--fmad=true");
+    rq.kernels = {"ucb_ls_kernel"};
+    return rq;
+}
+
+}  // namespace
+
+extern "C" int ucb_precompile_ls2d(const ucb_ls2d_request* req, char* err_out, int err_len) {
+    std::string err;
+    SweepMap m;
+    int nb = 0, sk = 0;
+    long long nt = 0;
+    if (!req || !plan_sweep2d(as_lle(*req), m, nb, sk, nt, err)) {
+        if (err_out && err_len > 0) std::snprintf(err_out, (size_t)err_len, "%s", err.c_str());
+        return UCB_E_INVALID;
+    }
+    SystemCode sys;
+    CompileRequest rq = ls_compile_request(*req, m, sys);
+    if (req->method == UCB_LS_DP5 && !sys.has_jvp) {
+        if (err_out && err_len > 0) std::snprintf(err_out, (size_t)err_len, "%s", sys.note.c_str());
+        return UCB_E_INVALID;
+    }
+    if (!precompile_to_disk(rq, err)) {
+        if (err_out && err_len > 0) std::snprintf(err_out, (size_t)err_len, "%s", err.c_str());
+        return UCB_E_COMPILE;
+    }
+    if (err_out && err_len > 0) std::snprintf(err_out, (size_t)err_len, "%s", sys.note.c_str());
+    return UCB_OK;
+}
+
+extern "C" int ucb_run_ls2d(ucb_engine* e, const ucb_ls2d_request* req, ucb_ls2d_result* res) {
+    if (!e || !req || !res) return UCB_E_INVALID;
+    const ucb_ls2d_request& q = *req;
+    res->ok = res->cancelled = 0;
+    res->error[0] = 0;
+    res->kernel_ms = 0;
+    res->steps = 0;
+    res->flops = 0;
+    std::string err;
+    SweepMap m;
+    int n_blocks = 0, skip = 0;
+    long long nt = 0;
+    const ucb_lle2d_request l = as_lle(q);
+    if (!plan_sweep2d(l, m, n_blocks, skip, nt, err)) return fail(e, res, UCB_E_INVALID, err);
+    const bool dp5 = q.method == UCB_LS_DP5;
+    if (q.method != UCB_LS_FIXED && !dp5) return fail(e, res, UCB_E_INVALID, "unknown LS method");
+    if (dp5 && (m.h_axis != -1)) return fail(e, res, UCB_E_INVALID, "the DP5 method does not sweep h");
+    if (dp5 && q.gs_every < 0) return fail(e, res, UCB_E_INVALID, "gs_every must be >= 0");
+    if (!res->values || !res->flags) return fail(e, res, UCB_E_INVALID, "result buffers are NULL");
+    if (q.cancel && *q.cancel) {
+        res->cancelled = 1;
+        return fail(e, res, UCB_E_CANCELLED, "Cancelled by user");
+    }
+    if (!ensure_init(e, err)) return fail(e, res, UCB_E_NOGPU, err);
+    const int prec = q.opt.precision;
+    const int nx = q.amount_of_x;
+    SystemCode sys;
+    CompileRequest rq = ls_compile_request(q, m, sys);
+    if (dp5 && !sys.has_jvp)
+        return fail(e, res, UCB_E_INVALID, "the DP5 method needs a recognised RK4 body: " + sys.note);
+    auto mod = e->modules.get(rq, err);
+    if (!mod) return fail(e, res, UCB_E_COMPILE, err);
+    CUfunction fn = mod->functions["ucb_ls_kernel"];
+
+    const int n = q.n_pts;
+    const long long total = (long long)n * n;
+    std::vector<double> t0d, t1d;
+    std::vector<float> t0f, t1f;
+    axis_table(prec, n, m.lo[0], m.hi[0], m.log_axis[0], t0d, t0f);
+    axis_table(prec, n, m.lo[1], m.hi[1], m.log_axis[1], t1d, t1f);
+    const size_t esz = prec == UCB_PREC_F64 ? 8 : 4;
+    const size_t tab_bytes = (size_t)n * esz;
+    const size_t off0 = 256, off1 = 256 + ((tab_bytes + 255) / 256) * 256;
+    if (!ensure_workspace(e, off1 + tab_bytes + 256, err)) return fail(e, res, UCB_E_CUDA, err);
+    char* ws = static_cast<char*>(e->ws);
+    cudaMemcpyAsync(ws + off0, prec == UCB_PREC_F64 ? (const void*)t0d.data() : (const void*)t0f.data(), tab_bytes,
+                    cudaMemcpyHostToDevice, e->stream);
+    cudaMemcpyAsync(ws + off1, prec == UCB_PREC_F64 ? (const void*)t1d.data() : (const void*)t1f.data(), tab_bytes,
+                    cudaMemcpyHostToDevice, e->stream);
+    cudaMemsetAsync(ws, 0, 16, e->stream);
+    double* d_values = nullptr;
+    int32_t* d_flags = nullptr;
+    cudaError_t ce;
+    if ((ce = cudaMallocAsync((void**)&d_values, (size_t)total * nx * 8, e->stream)) != cudaSuccess ||
+        (ce = cudaMallocAsync((void**)&d_flags, (size_t)total * 4, e->stream)) != cudaSuccess)
+        return fail(e, res, UCB_E_CUDA, std::string("cudaMallocAsync: ") + cudaGetErrorString(ce));
+
+    const double rtol = q.rtol > 0 ? q.rtol : (prec == UCB_PREC_F64 ? 1e-8 : 1e-5);
+    const double atol = q.atol > 0 ? q.atol : rtol;
+    const double t_end = q.t_end > 0 ? q.t_end : q.t_max;
+    ParamPack pk;
+    pk.put<long long>(total);
+    pk.put<long long>(0);
+    pk.put<int>(n);
+    pk.put<int>(m.swap_xy ? 1 : 0);
+    pk.put<int>(n_blocks);
+    pk.put<int>(q.gs_every > 0 ? q.gs_every : 10);
+    pk.put<long long>(skip);
+    pk.put<long long>(nt);
+    pk.put<long long>(q.max_steps > 0 ? q.max_steps : 100000000LL);
+    for (double v : {q.h, q.NT, q.t_max, q.eps, q.max_value, q.transient_time}) pk.put_numb(prec, v);
+    pk.put<double>(rtol);
+    pk.put<double>(atol);
+    pk.put<double>(t_end);
+    pk.put<double>(q.h0 > 0 ? q.h0 : q.h);
+    for (int i = 0; i < nx; ++i) pk.put_numb(prec, q.initial_conditions[i]);
+    for (int i = 0; i < std::max(q.n_values, 1); ++i) pk.put_numb(prec, i < q.n_values ? q.base_values[i] : 0.0);
+    pk.put<const void*>(ws + off0);
+    pk.put<const void*>(ws + off1);
+    pk.put<void*>(d_values);
+    pk.put<void*>(d_flags);
+    pk.put<void*>(ws);
+    pk.put<void*>(ws + 8);
+    const int block = 128;
+    const int grid = persistent_grid(e, fn, block, total);
+    cudaEventRecord(e->ev0, e->stream);
+    int rc = launch_packed(e, fn, grid, block, e->stream, pk, err) ? UCB_OK : UCB_E_CUDA;
+    cudaEventRecord(e->ev1, e->stream);
+    unsigned long long steps = 0;
+    if (rc == UCB_OK) {
+        if ((ce = cudaMemcpyAsync(res->values, d_values, (size_t)total * nx * 8, cudaMemcpyDeviceToHost, e->stream)) !=
+                cudaSuccess ||
+            (ce = cudaMemcpyAsync(res->flags, d_flags, (size_t)total * 4, cudaMemcpyDeviceToHost, e->stream)) !=
+                cudaSuccess ||
+            (ce = cudaMemcpyAsync(&steps, ws + 8, 8, cudaMemcpyDeviceToHost, e->stream)) != cudaSuccess ||
+            (ce = cudaStreamSynchronize(e->stream)) != cudaSuccess) {
+            rc = UCB_E_CUDA;
+            err = std::string("CUDA ls2d: ") + cudaGetErrorString(ce);
+        }
+    }
+    cudaFreeAsync(d_values, e->stream);
+    cudaFreeAsync(d_flags, e->stream);
+    cudaStreamSynchronize(e->stream);
+    if (rc != UCB_OK) return fail(e, res, rc, err);
+    float ms = 0;
+    cudaEventElapsedTime(&ms, e->ev0, e->ev1);
+    res->kernel_ms = ms;
+    res->steps = (long long)steps;
+    if (dp5) {
+        // per step attempt: 6 right-hand sides + stage combinations and error norm of the
+        // state (about 56 N), and for the tangent block N x (6 J v products + 40 N)
+        const double per = 6.0 * sys.flops_rhs + 56.0 * nx + nx * (6.0 * sys.flops_jvp + 40.0 * nx);
+        res->flops = (double)steps * per;
+    } else {
+        res->flops = (double)steps * (double)sys.flops_step;
+    }
+    res->n_pts = n;
+    res->n_exponents = nx;
+    for (int k = 0; k < nx; ++k) {
+        double vmin = std::numeric_limits<double>::infinity(), vmax = -vmin;
+        for (long long c = 0; c < total; ++c) {
+            if (res->flags[c] < 0) continue;
+            const double v = res->values[(size_t)k * total + c];
+            if (!std::isfinite(v)) continue;
+            vmin = std::min(vmin, v);
+            vmax = std::max(vmax, v);
+        }
+        if (!std::isfinite(vmin)) vmin = vmax = 0.0;
+        if (res->min_val) res->min_val[k] = vmin;
+        if (res->max_val) res->max_val[k] = vmax;
+    }
+    if (q.csv_output_path && *q.csv_output_path) {
+        csv::Common cc{std::vector<double>(q.base_values, q.base_values + q.n_values),
+                       std::vector<double>(q.initial_conditions, q.initial_conditions + nx)};
+        csv::ls2d(q.csv_output_path, cc, m.par_or_var, q.t_max, q.NT, q.transient_time, q.h, q.eps,
+                  q.sweep_over_var ? q.var_sweep_index : q.param_index,
+                  q.sweep_over_var_2 ? q.var_sweep_index_2 : q.param_index_2, q.param_lo, q.param_hi, q.param_lo_2,
+                  q.param_hi_2, n, nx, res->values);
+    }
+    if (q.progress) *q.progress = 1.0f;
+    res->ok = 1;
+    return UCB_OK;
+}

@@ -84,6 +84,48 @@ class Bif1dResult(C.Structure):
     ]
 
 
+class Ls2dRequest(C.Structure):
+    _fields_ = Lle2dRequest._fields_ + [
+        ("method", C.c_int32), ("gs_every", C.c_int32), ("rtol", C.c_double), ("atol", C.c_double),
+        ("t_end", C.c_double), ("h0", C.c_double), ("max_steps", C.c_longlong),
+    ]
+
+
+class Ls2dResult(C.Structure):
+    _fields_ = [
+        ("values", C.POINTER(C.c_double)), ("flags", C.POINTER(C.c_int32)),
+        ("min_val", C.POINTER(C.c_double)), ("max_val", C.POINTER(C.c_double)),
+        ("ok", C.c_int32), ("cancelled", C.c_int32), ("n_pts", C.c_int32), ("n_exponents", C.c_int32),
+        ("kernel_ms", C.c_double), ("steps", C.c_longlong), ("flops", C.c_double), ("error", C.c_char * 1024),
+    ]
+
+
+class BasinsRequest(C.Structure):
+    _fields_ = [
+        ("krs_body", C.c_char_p), ("amount_of_x", C.c_int32),
+        ("initial_conditions", C.POINTER(C.c_double)), ("base_values", C.POINTER(C.c_double)),
+        ("n_values", C.c_int32), ("axis_x_var", C.c_int32), ("axis_y_var", C.c_int32),
+        ("axis_x_lo", C.c_double), ("axis_x_hi", C.c_double), ("axis_y_lo", C.c_double), ("axis_y_hi", C.c_double),
+        ("n_pts", C.c_int32), ("period", C.c_double), ("steps_per_period", C.c_int32), ("max_periods", C.c_int32),
+        ("match_count", C.c_int32), ("match_tol", C.c_double), ("phase_var", C.c_int32),
+        ("max_value", C.c_double), ("merge_radius", C.c_double), ("csv_output_path", C.c_char_p),
+        ("cancel", C.POINTER(C.c_int32)), ("progress", C.POINTER(C.c_float)), ("opt", Options),
+    ]
+
+
+MAX_ATTRACTORS = 256
+
+
+class BasinsResult(C.Structure):
+    _fields_ = [
+        ("labels", C.POINTER(C.c_int32)), ("periods", C.POINTER(C.c_int32)), ("iterations", C.POINTER(C.c_int32)),
+        ("ok", C.c_int32), ("cancelled", C.c_int32), ("n_pts", C.c_int32), ("n_attractors", C.c_int32),
+        ("attractor_period", C.c_int32 * MAX_ATTRACTORS), ("attractor_point", (C.c_double * 2) * MAX_ATTRACTORS),
+        ("kernel_ms", C.c_double), ("steps", C.c_longlong), ("flops", C.c_double), ("error", C.c_char * 1024),
+    ]
+
+
+LS_FIXED, LS_DP5 = 0, 1
 _lib = None
 
 
@@ -114,6 +156,16 @@ def load():
     L.ucb_lle2d_device.restype = C.c_int
     L.ucb_lle2d_device.argtypes = [C.c_void_p, C.POINTER(Lle2dRequest), C.c_void_p, C.c_void_p, C.c_void_p,
                                    C.POINTER(Lle2dResult)]
+    L.ucb_run_ls2d.restype = C.c_int
+    L.ucb_run_ls2d.argtypes = [C.c_void_p, C.POINTER(Ls2dRequest), C.POINTER(Ls2dResult)]
+    L.ucb_precompile_ls2d.restype = C.c_int
+    L.ucb_precompile_ls2d.argtypes = [C.POINTER(Ls2dRequest), C.c_char_p, C.c_int]
+    L.ucb_precompile_bif1d.restype = C.c_int
+    L.ucb_precompile_bif1d.argtypes = [C.POINTER(Bif1dRequest), C.c_char_p, C.c_int]
+    L.ucb_run_basins.restype = C.c_int
+    L.ucb_run_basins.argtypes = [C.c_void_p, C.POINTER(BasinsRequest), C.POINTER(BasinsResult)]
+    L.ucb_precompile_basins.restype = C.c_int
+    L.ucb_precompile_basins.argtypes = [C.POINTER(BasinsRequest), C.c_char_p, C.c_int]
     L.ucb_run_bif1d.restype = C.c_int
     L.ucb_run_bif1d.argtypes = [C.c_void_p, C.POINTER(Bif1dRequest), C.POINTER(Bif1dResult)]
     L.ucb_prepare_lle2d.restype = C.c_int
@@ -214,6 +266,75 @@ class Engine:
             raise UcbError(rc, res.error.decode())
         return values, flags, res
 
+    # ------------------------------------------------------------------ LS 2D
+    @staticmethod
+    def ls2d_request(krs_body, amount_of_x, initial_conditions, base_values, *, method=0, gs_every=10, rtol=0.0,
+                     atol=0.0, t_end=0.0, h0=0.0, max_steps=0, **kw):
+        base = Engine.lle2d_request(krs_body, amount_of_x, initial_conditions, base_values, **kw)
+        r = Ls2dRequest()
+        for name, _ in Lle2dRequest._fields_:
+            setattr(r, name, getattr(base, name))
+        r._keep = base._keep
+        r.method, r.gs_every, r.rtol, r.atol, r.t_end, r.h0, r.max_steps = method, gs_every, rtol, atol, t_end, h0, \
+            max_steps
+        return r
+
+    def run_ls2d(self, req: Ls2dRequest):
+        n, nx = req.n_pts, req.amount_of_x
+        values = np.empty(max(n, 0) ** 2 * nx, dtype=np.float64)
+        flags = np.empty(max(n, 0) ** 2, dtype=np.int32)
+        mn = np.empty(nx, dtype=np.float64)
+        mx = np.empty(nx, dtype=np.float64)
+        res = Ls2dResult()
+        res.values = _dptr(values)
+        res.flags = flags.ctypes.data_as(C.POINTER(C.c_int32))
+        res.min_val = _dptr(mn)
+        res.max_val = _dptr(mx)
+        rc = self.lib.ucb_run_ls2d(self.h, C.byref(req), C.byref(res))
+        if rc != UCB_OK:
+            raise UcbError(rc, res.error.decode())
+        return values.reshape(nx, n * n), flags, res
+
+    # ------------------------------------------------------------------ basins
+    @staticmethod
+    def basins_request(krs_body, amount_of_x, initial_conditions, base_values, *, n_pts, axis_x_var=0,
+                       axis_y_var=1, axis_x_lo=-1.0, axis_x_hi=1.0, axis_y_lo=-1.0, axis_y_hi=1.0, period=1.0,
+                       steps_per_period=100, max_periods=2000, match_count=20, match_tol=1e-6, phase_var=-1,
+                       max_value=1e6, merge_radius=0.0, csv_output_path=None, opt: Options | None = None):
+        ic = np.ascontiguousarray(initial_conditions, dtype=np.float64)
+        vals = np.ascontiguousarray(base_values, dtype=np.float64)
+        r = BasinsRequest()
+        r._keep = (ic, vals, krs_body.encode())
+        r.krs_body = r._keep[2]
+        r.amount_of_x = amount_of_x
+        r.initial_conditions = _dptr(ic)
+        r.base_values = _dptr(vals)
+        r.n_values = len(vals)
+        r.axis_x_var, r.axis_y_var = axis_x_var, axis_y_var
+        r.axis_x_lo, r.axis_x_hi, r.axis_y_lo, r.axis_y_hi = axis_x_lo, axis_x_hi, axis_y_lo, axis_y_hi
+        r.n_pts, r.period, r.steps_per_period, r.max_periods = n_pts, period, steps_per_period, max_periods
+        r.match_count, r.match_tol, r.phase_var = match_count, match_tol, phase_var
+        r.max_value, r.merge_radius = max_value, merge_radius
+        r.csv_output_path = csv_output_path.encode() if csv_output_path else None
+        r.opt = opt if opt is not None else options()
+        return r
+
+    def run_basins(self, req: BasinsRequest):
+        n = req.n_pts
+        labels = np.empty(n * n, dtype=np.int32)
+        periods = np.empty(n * n, dtype=np.int32)
+        iters = np.empty(n * n, dtype=np.int32)
+        res = BasinsResult()
+        res.labels = labels.ctypes.data_as(C.POINTER(C.c_int32))
+        res.periods = periods.ctypes.data_as(C.POINTER(C.c_int32))
+        res.iterations = iters.ctypes.data_as(C.POINTER(C.c_int32))
+        rc = self.lib.ucb_run_basins(self.h, C.byref(req), C.byref(res))
+        if rc != UCB_OK:
+            raise UcbError(rc, res.error.decode())
+        att = [(res.attractor_period[i], res.attractor_point[i][0], res.attractor_point[i][1])
+               for i in range(min(res.n_attractors, MAX_ATTRACTORS))]
+        return labels, periods, iters, att, res
+
     # ------------------------------------------------------------------ bifurcation 1D
     @staticmethod
     def bif1d_request(krs_body: str, amount_of_x: int, initial_conditions, base_values, *, n_pts, param_index=0,
@@ -286,9 +407,12 @@ class Engine:
         return res
 
 
-def precompile_lle2d(req: Lle2dRequest) -> str:
+def precompile_lle2d(req) -> str:
+    """Compiles the sm_100a kernel a run with this request would use (no GPU needed)."""
+    fn = {Lle2dRequest: "ucb_precompile_lle2d", Ls2dRequest: "ucb_precompile_ls2d",
+          Bif1dRequest: "ucb_precompile_bif1d", BasinsRequest: "ucb_precompile_basins"}[type(req)]
     buf = C.create_string_buffer(65536)
-    rc = load().ucb_precompile_lle2d(C.byref(req), buf, len(buf))
+    rc = getattr(load(), fn)(C.byref(req), buf, len(buf))
     if rc != UCB_OK:
         raise UcbError(rc, buf.value.decode(errors="replace"))
     return buf.value.decode(errors="replace")
@@ -318,3 +442,6 @@ def codegen(text: str, alphabet: str, scheme: str = "RK4", order_as_in_system=Fa
         raise UcbError(rc, out.value.decode())
     split = lambda b: [x for x in b.value.decode().split(",") if x]
     return out.value.decode(), split(vs), split(ps)
+
+
+precompile = precompile_lle2d
