@@ -223,7 +223,8 @@ typedef struct ucb_ls2d_request {
     double rtol, atol;       /* DP5 error tolerances (0 = 1e-8 / 1e-5 for FP64 / FP32, atol = rtol) */
     double t_end;            /* DP5 measured interval length (0 = t_max) */
     double h0;               /* DP5 initial step (0 = h) */
-    long long max_steps;     /* DP5 cap on step attempts per cell (0 = 10^8) */
+    long long max_steps;     /* DP5 cap on step attempts per cell (0 = 2 x 10^7); cells that hit
+                                it are reported as diverged (999, flag -1) */
 } ucb_ls2d_request;
 
 typedef struct ucb_ls2d_result {
@@ -267,7 +268,8 @@ typedef struct ucb_basins_request {
     int32_t steps_per_period;         /* h = period / steps_per_period */
     int32_t max_periods;              /* cap (2000 in the benchmark configuration) */
     int32_t match_count;              /* consecutive period matches to converge (20) */
-    double match_tol;                 /* max-norm match tolerance (1e-6) */
+    double match_tol;                 /* max-norm match tolerance (1e-6); the FP32 form uses at
+                                         least 1e-5 (FP32 resolves a stroboscopic point to ~1e-6) */
     int32_t phase_var;                /* state index of the forcing phase (reset every period), -1 none */
     double max_value;
     double merge_radius;              /* canonical points closer than this are one attractor (0 = 1e-4) */

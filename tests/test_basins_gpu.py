@@ -10,8 +10,10 @@ a different oracle class).
 FP32: here every converging cell needs 45-56 periods (280-350 time units) and the
 transients are chaotic, while FP32 trajectories decorrelate from FP64 ones after about
 16/lambda time units (rounding 6e-8 amplified by e^{lambda t}); cells can then settle on
-the other attractor. FP32 must find the same attractors (period and canonical point)
-and agree on >= 95 % of the cells; the FP64 forms carry the 99.9 % criterion."""
+the other attractor. The FP32 form also matches stroboscopic points to 1e-5 instead of
+1e-6 (FP32 resolves them to about 1e-6). FP32 must find the same attractors (period and
+canonical point) and agree on >= 95 % of the cells; the FP64 forms carry the 99.9 %
+criterion."""
 import math
 
 import numpy as np

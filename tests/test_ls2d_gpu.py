@@ -80,8 +80,14 @@ def test_dp5_lorenz_divergence_identity(eng, prec):
     assert (np.abs(v[0] - 0.906) < 0.08).all()
 
 
+# The hyperchaotic window around the classic parameters (0.25, 0.05): every cell on the
+# attractor or escaping, 4th exponent -15 .. -80 (the full configuration grid also holds
+# near-escape cells with exponents near -5000 that need ~1e6 tiny steps each).
+WINDOW = dict(param_lo=0.24, param_hi=0.26, param_lo_2=0.045, param_hi_2=0.055)
+
+
 def test_dp5_matches_oracle(eng):
-    c = hyper_case(n=4, transient_time=20.0, t_end=200.0, gs_every=10)
+    c = hyper_case(n=4, transient_time=20.0, t_end=200.0, gs_every=10, **WINDOW)
     v, f, res = eng.run_ls2d(ls_request(c, ucb.LS_DP5, precision=ucb.PREC_F64))
     g = kernel_grid(c)
     ov, of = O.ls2d_dp5(O.Rhs(c["body"], 4), g, t_end=200.0, rtol=1e-8, h0=c["h"], gs_every=10)
@@ -98,7 +104,7 @@ def test_dp5_f32_close_to_f64(eng):
     # same tolerance: the strongly contracting 4th exponents (-15 .. -5400 on this grid)
     # are resolved because the error norm covers the tangent vectors; the remaining
     # dependence on rtol itself is a property of the method, not of the precision.
-    c = hyper_case(n=4, transient_time=20.0, t_end=100.0, gs_every=10, rtol=1e-5)
+    c = hyper_case(n=4, transient_time=20.0, t_end=100.0, gs_every=10, rtol=1e-5, **WINDOW)
     v64, f64, _ = eng.run_ls2d(ls_request(c, ucb.LS_DP5, precision=ucb.PREC_F64))
     v32, f32, _ = eng.run_ls2d(ls_request(c, ucb.LS_DP5, precision=ucb.PREC_F32))
     np.testing.assert_array_equal(f32, f64)

@@ -169,8 +169,8 @@ __device__ __forceinline__ int loop_single(const S& s, numb* x, const numb* a, n
         s.step(x, a, h);
         ns += 1;
         if (diverged(x, maxValue)) return 0;
-        const long long n = (iters - i0 < kCheckInterval) ? iters - i0 : kCheckInterval;
-        for (long long i = 1; i < n; ++i) s.step(x, a, h);
+        const int n = (iters - i0 < kCheckInterval) ? (int)(iters - i0) : kCheckInterval;
+        for (int i = 1; i < n; ++i) s.step(x, a, h);
         ns += n - 1;
     }
 #if UCB_EXTRA_STEP
@@ -197,8 +197,8 @@ __device__ __forceinline__ int loop_pair(const S& s, numb* x, numb* y, const num
         s.step(y, a, h);
         ns += 2;
         if (diverged(x, maxValue) || diverged(y, maxValue)) return 0;
-        const long long n = (iters - i0 < kCheckInterval) ? iters - i0 : kCheckInterval;
-        for (long long i = 1; i < n; ++i) {
+        const int n = (iters - i0 < kCheckInterval) ? (int)(iters - i0) : kCheckInterval;
+        for (int i = 1; i < n; ++i) {
             s.step(x, a, h);
             s.step(y, a, h);
         }
@@ -211,6 +211,49 @@ __device__ __forceinline__ int loop_pair(const S& s, numb* x, numb* y, const num
 #endif
     return 1;
 }
+
+#ifdef UCB_NT
+// loop_pair for a block length known at compile time (UCB_NT <= kCheckInterval steps):
+// the same sequence — first step of both, divergence test, the remaining UCB_NT - 1
+// steps, the extra step — fully unrolled, without loop control.
+template <class S>
+__device__ __forceinline__ int loop_pair_nt(const S& s, numb* x, numb* y, const numb* a, numb h, numb maxValue,
+                                            long long& ns) {
+    s.step(x, a, h);
+    s.step(y, a, h);
+    if (diverged(x, maxValue) || diverged(y, maxValue)) {
+        ns += 2;
+        return 0;
+    }
+#pragma unroll
+    for (int i = 1; i < UCB_NT; ++i) {
+        s.step(x, a, h);
+        s.step(y, a, h);
+    }
+#if UCB_EXTRA_STEP
+    s.step(x, a, h);
+    s.step(y, a, h);
+    ns += 2 * (UCB_NT + 1);
+#else
+    ns += 2 * UCB_NT;
+#endif
+    return 1;
+}
+#endif
+
+// Running product of positive factors as mantissa x 2^exponent (FP64): a sum of logs
+// taken with one log at the end instead of one per block.
+struct LogProduct {
+    double m;
+    long long e;
+    __device__ __forceinline__ LogProduct() : m(1.0), e(0) {}
+    __device__ __forceinline__ void mul(double f) {
+        int k;
+        m = frexp(m * f, &k);
+        e += k;
+    }
+    __device__ __forceinline__ double log_value() const { return log(m) + (double)e * 0.69314718055994530942; }
+};
 
 // ---------------------------------------------------------------------------
 // Cell set-up: sweep values of one cell (the par_or_var branches of LLEKernelCUDA

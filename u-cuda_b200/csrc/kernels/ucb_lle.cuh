@@ -30,6 +30,7 @@ struct UcbLleParams {
     int* out_flags;
     unsigned long long* counter;   // work counter, zeroed before launch
     unsigned long long* steps;     // step evaluations performed (accumulated)
+    const long long* cell_list;    // optional: kernel cell indices to compute (total entries)
 };
 
 namespace ucbdev {
@@ -83,10 +84,18 @@ __device__ __forceinline__ double lle_cell_shadow(const UcbLleParams& p, long lo
     probe_direction((unsigned long long)kidx, z);
 #pragma unroll
     for (int i = 0; i < UCB_NX; ++i) y[i] = z[i] * p.eps + x[i];
-    numb result = 0;
     const numb inv_eps = (numb)1.0 / p.eps;
+#ifdef UCB_EXACT
+    numb result = 0;  // the reference's numb sum of per-block logs
+#else
+    LogProduct prod;  // same sum, one log at the end
+#endif
     for (int b = 0; b < p.n_blocks; ++b) {
+#if defined(UCB_NT) && UCB_HAXIS == -1
+        if (loop_pair_nt(st, x, y, a, cs.h, p.maxv, ns) == 0) return 999.0;
+#else
         if (loop_pair(st, x, y, a, cs.h, cs.nt, p.maxv, ns) == 0) return 999.0;
+#endif
         numb tempData = 0;
 #pragma unroll
         for (int l = 0; l < UCB_NX; ++l) {
@@ -95,12 +104,20 @@ __device__ __forceinline__ double lle_cell_shadow(const UcbLleParams& p, long lo
         }
         tempData = sqrt(tempData);
         if (tempData <= 1e-14) tempData = (numb)1e-14;
+#ifdef UCB_EXACT
         result += log(tempData);
+#else
+        prod.mul((double)tempData);
+#endif
         tempData = (1 / tempData);
 #pragma unroll
         for (int j = 0; j < UCB_NX; ++j) y[j] = (numb)(x[j] - ((x[j] - y[j] + 1e-14) * tempData));
     }
+#ifdef UCB_EXACT
     return (double)(result / p.tmax);
+#else
+    return prod.log_value() / (double)p.tmax;
+#endif
 }
 
 #if defined(UCB_HAS_JVP) && !defined(UCB_EXACT)
@@ -112,14 +129,24 @@ __device__ __forceinline__ double lle_cell_shadow(const UcbLleParams& p, long lo
 template <class S>
 __device__ __forceinline__ int loop_tangent(const S& s, numb* x, numb* v, const numb* a, numb h,
                                             long long iters, numb maxValue, long long& ns) {
+#if defined(UCB_NT) && UCB_HAXIS == -1
+    (void)iters;
+    s.step_tangent(x, v, a, h);
+    ns += 2;
+    if (diverged(x, maxValue) || diverged(v, (numb)0)) return 0;
+#pragma unroll
+    for (int i = 1; i < UCB_NT; ++i) s.step_tangent(x, v, a, h);
+    ns += 2 * (UCB_NT - 1);
+#else
     for (long long i0 = 0; i0 < iters; i0 += kCheckInterval) {
         s.step_tangent(x, v, a, h);
         ns += 2;
         if (diverged(x, maxValue) || diverged(v, (numb)0)) return 0;
-        const long long n = (iters - i0 < kCheckInterval) ? iters - i0 : kCheckInterval;
-        for (long long i = 1; i < n; ++i) s.step_tangent(x, v, a, h);
+        const int n = (iters - i0 < kCheckInterval) ? (int)(iters - i0) : kCheckInterval;
+        for (int i = 1; i < n; ++i) s.step_tangent(x, v, a, h);
         ns += 2 * (n - 1);
     }
+#endif
 #if UCB_EXTRA_STEP
     s.step_tangent(x, v, a, h);
     ns += 2;
@@ -140,20 +167,33 @@ __device__ __forceinline__ double lle_cell_tangent(const UcbLleParams& p, long l
     const Stepper st(cs.h);
     if (loop_single(st, x, a, cs.h, cs.skip, p.maxv, ns) == 0) return 999.0;
     probe_direction((unsigned long long)kidx, v);
-    double result = 0.0;
+    // lambda = sum_b log(|v_b,end| / |v_b,start|) / tMax. The rescale between blocks is an
+    // FP32 reciprocal square root, so |v_b,start| is 1 only to FP32 rounding; both norms
+    // are accumulated exactly as FP64 products of squares (one log each at the end).
+    LogProduct end2, start2;
+    double n2 = 0.0;
+#pragma unroll
+    for (int j = 0; j < UCB_NX; ++j) n2 = fma((double)v[j], (double)v[j], n2);
     for (int b = 0; b < p.n_blocks; ++b) {
+        start2.mul(n2);
         if (loop_tangent(st, x, v, a, cs.h, cs.nt, p.maxv, ns) == 0) return 999.0;
         double d2 = 0.0;
 #pragma unroll
         for (int l = 0; l < UCB_NX; ++l) d2 = fma((double)v[l], (double)v[l], d2);
-        double d = sqrt(d2);
-        if (d <= 1e-14) d = 1e-14;
-        result += log(d);
-        const numb inv = (numb)(1.0 / d);
+        if (d2 < 1e-28) {  // the reference's floor of the norm at 1e-14
+            d2 = 1e-28;
+            if (!(fabs((double)v[0]) > 0)) v[0] = (numb)1e-14;
+        }
+        end2.mul(d2);
+        const numb inv = (numb)rsqrt(d2);
+        n2 = 0.0;
 #pragma unroll
-        for (int j = 0; j < UCB_NX; ++j) v[j] *= inv;
+        for (int j = 0; j < UCB_NX; ++j) {
+            v[j] *= inv;
+            n2 = fma((double)v[j], (double)v[j], n2);
+        }
     }
-    return result / (double)p.tmax;
+    return 0.5 * (end2.log_value() - start2.log_value()) / (double)p.tmax;
 }
 #endif
 
@@ -167,7 +207,7 @@ extern "C" __global__ void __launch_bounds__(128) ucb_lle_kernel(const UcbLlePar
         if (base >= p.total) break;
         const long long i = base + lane;
         if (i < p.total) {
-            const long long kidx = p.cell_offset + i;
+            const long long kidx = p.cell_list ? p.cell_list[i] : p.cell_offset + i;
 #if defined(UCB_TANGENT)
             const double v = ucbdev::lle_cell_tangent(p, kidx, ns);
 #else

@@ -146,7 +146,7 @@ extern "C" int ucb_run_basins(ucb_engine* e, const ucb_basins_request* req, ucb_
     pk.put<int>(0);
     pk.put_numb(prec, h);
     pk.put_numb(prec, q.max_value);
-    pk.put_numb(prec, q.match_tol);
+    pk.put_numb(prec, prec == UCB_PREC_F32 ? std::max(q.match_tol, 1e-5) : q.match_tol);
     const double merge = q.merge_radius > 0 ? q.merge_radius : 1e-4;
     pk.put<double>(merge);
     for (int i = 0; i < q.amount_of_x; ++i) pk.put_numb(prec, q.initial_conditions[i]);

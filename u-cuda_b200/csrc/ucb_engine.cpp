@@ -330,7 +330,7 @@ struct LleParamsT {
 template <class T>
 std::vector<char> pack_lle_params(const LleParamsT<T>& head, const double* ic, int nx, const double* vals, int nv,
                                   const void* ax0, const void* ax1, double* out_v, int32_t* out_f, void* counter,
-                                  void* steps) {
+                                  void* steps, const void* cell_list = nullptr) {
     std::vector<char> buf;
     auto put = [&](const void* p, size_t n, size_t align) {
         while (buf.size() % align) buf.push_back(0);
@@ -356,6 +356,7 @@ std::vector<char> pack_lle_params(const LleParamsT<T>& head, const double* ic, i
     put(&out_f, 8, 8);
     put(&counter, 8, 8);
     put(&steps, 8, 8);
+    put(&cell_list, 8, 8);
     while (buf.size() % 8) buf.push_back(0);
     return buf;
 }
@@ -377,6 +378,9 @@ CompileRequest lle_compile_request(const ucb_lle2d_request& q, const LlePlan& pl
     L.tangent = tangent;
     std::vector<std::string> defs;
     if (tangent) defs.push_back("UCB_TANGENT 1");
+    // Block length known at compile time (no h sweep): the block loop unrolls fully.
+    if (plan.map.h_axis == -1 && plan.nt_steps >= 1 && plan.nt_steps <= 100)
+        defs.push_back("UCB_NT " + std::to_string(plan.nt_steps));
     CompileRequest rq;
     rq.name = "ucb_lle2d.cu";
     rq.source = make_prelude(prec, q.amount_of_x, q.n_values, plan.map, q.opt.nominal_steps == 0, L.sys, defs) +
@@ -399,7 +403,7 @@ bool prepare_lle(ucb_engine* e, const ucb_lle2d_request& q, const LlePlan& plan,
 // [256..] axis tables.
 int enqueue_lle_fn(ucb_engine* e, const ucb_lle2d_request& q, const LlePlan& plan, const LleLaunch& L,
                    double* d_values, int32_t* d_flags, cudaStream_t stream, std::string& err, long long skip_override,
-                   bool persistent, char* scratch) {
+                   bool persistent, char* scratch, const long long* d_cell_list = nullptr, long long n_list = 0) {
     const int n = q.n_pts;
     const int prec = q.opt.precision;
     const size_t esz = prec == UCB_PREC_F64 ? 8 : 4;
@@ -423,21 +427,21 @@ int enqueue_lle_fn(ucb_engine* e, const ucb_lle2d_request& q, const LlePlan& pla
         err = std::string("CUDA upload: ") + cudaGetErrorString(ce);
         return UCB_E_CUDA;
     }
-    const long long total = (long long)n * n;
+    const long long total = d_cell_list ? n_list : (long long)n * n;
     std::vector<char> params;
     if (prec == UCB_PREC_F64) {
         LleParamsT<double> hd{total, 0, n, plan.map.swap_xy ? 1 : 0, plan.amountOfPointsInBlock, 0,
                               skip_override >= 0 ? skip_override : plan.amountOfPointsForSkip, plan.nt_steps, q.h,
                               q.NT, q.t_max, q.eps, q.max_value, q.transient_time};
         params = pack_lle_params<double>(hd, q.initial_conditions, q.amount_of_x, q.base_values, q.n_values,
-                                         ws + off_ax0, ws + off_ax1, d_values, d_flags, ws, ws + 8);
+                                         ws + off_ax0, ws + off_ax1, d_values, d_flags, ws, ws + 8, d_cell_list);
     } else {
         LleParamsT<float> hd{total, 0, n, plan.map.swap_xy ? 1 : 0, plan.amountOfPointsInBlock, 0,
                              skip_override >= 0 ? skip_override : plan.amountOfPointsForSkip, plan.nt_steps,
                              (float)q.h, (float)q.NT, (float)q.t_max,
                              (float)q.eps, (float)q.max_value, (float)q.transient_time};
         params = pack_lle_params<float>(hd, q.initial_conditions, q.amount_of_x, q.base_values, q.n_values,
-                                        ws + off_ax0, ws + off_ax1, d_values, d_flags, ws, ws + 8);
+                                        ws + off_ax0, ws + off_ax1, d_values, d_flags, ws, ws + 8, d_cell_list);
     }
     const int block = 128;
     const int grid = persistent ? persistent_grid(e, L.fn, block, total) : (int)((total + block - 1) / block);

@@ -162,7 +162,7 @@ extern "C" int ucb_run_ls2d(ucb_engine* e, const ucb_ls2d_request* req, ucb_ls2d
     pk.put<int>(q.gs_every > 0 ? q.gs_every : 10);
     pk.put<long long>(skip);
     pk.put<long long>(nt);
-    pk.put<long long>(q.max_steps > 0 ? q.max_steps : 100000000LL);
+    pk.put<long long>(q.max_steps > 0 ? q.max_steps : 20000000LL);
     for (double v : {q.h, q.NT, q.t_max, q.eps, q.max_value, q.transient_time}) pk.put_numb(prec, v);
     pk.put<double>(rtol);
     pk.put<double>(atol);
