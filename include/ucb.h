@@ -361,6 +361,114 @@ UCB_API int ucb_codegen(const char* text, const char* alphabet, int order_as_in_
  * the form chosen. */
 UCB_API int ucb_precompile_lle2d(const ucb_lle2d_request* req, char* err_out, int err_len);
 
+/* LLE of an explicit list of cells of the request's grid (kernel cell order: cell =
+ * iy * n_pts + ix before any swap), written compactly: d_values[i] / d_flags[i] belong to
+ * d_cells[i]. Same kernel and semantics as ucb_lle2d_device; used for held-out subsets
+ * and re-integration. No reference counterpart. */
+UCB_API int ucb_lle2d_cells(ucb_engine* e, const ucb_lle2d_request* req, const long long* d_cells, long long n_cells,
+                            double* d_values, int32_t* d_flags, void* stream, ucb_lle2d_result* res);
+
+/* ------------------------------------------------------------------------------------
+ * BF16 MLP surrogate (no counterpart in the reference). Input: a point u in [0, 1]^2 (the
+ * two sweep coordinates of a map, normalised); Fourier features sin / cos(2 pi u B^T)
+ * with a fixed Gaussian B (fourier x 2, std fourier_scale); `layers` hidden layers of
+ * width `hidden` with exact GELU; outputs mean and log-variance of the target, trained on
+ * the Gaussian negative log-likelihood (beta-NLL weighting: each row's loss is scaled by
+ * a constant sigma^(2 beta)) with Adam and a cosine learning-rate decay. Matrix products
+ * run on the tensor cores (tcgen05.mma, BF16 operands, FP32 accumulation in tensor
+ * memory); masters and Adam moments are FP32.
+ *
+ * Parameter vector layout (ucb_mlp_get_params): for each layer l = 0..layers (the last is
+ * the output layer with 2 outputs), W_l[out][in] row-major, then b_l[out].
+ * ---------------------------------------------------------------------------------- */
+typedef struct ucb_mlp_config {
+    int32_t fourier;        /* frequencies; 2 * fourier must be a multiple of 128 (default 64) */
+    int32_t hidden;         /* hidden width, a multiple of 128 (default 256) */
+    int32_t layers;         /* hidden layers, 1..8 (default 4) */
+    float fourier_scale;    /* std of the frequency matrix entries (default 6) */
+    uint64_t seed;          /* initialisation, frequency matrix and mini-batch sampling (default 0) */
+    int32_t batch;          /* rows per Adam step, a multiple of 128 (default 8192) */
+    int32_t train_steps;    /* Adam steps of ucb_mlp_fit (default 2000) */
+    float lr;               /* initial learning rate (default 2e-3) */
+    float lr_final;         /* learning rate at the last step, cosine decay (default 2e-5) */
+    float beta_nll;         /* 0 = plain Gaussian NLL, 1 = mean-squared-error-like (default 0.5) */
+    int32_t reserved[5];
+} ucb_mlp_config;
+
+typedef struct ucb_mlp ucb_mlp;
+
+UCB_API void ucb_mlp_default_config(ucb_mlp_config* c);
+/* Creates the network on the engine's device (parameters initialised from cfg->seed).
+ * NULL on failure (message: ucb_last_error(e)). */
+UCB_API ucb_mlp* ucb_mlp_create(ucb_engine* e, const ucb_mlp_config* cfg);
+UCB_API void ucb_mlp_destroy(ucb_mlp* m);
+UCB_API long long ucb_mlp_param_count(const ucb_mlp* m);
+/* Host copies of the FP32 parameters (n = ucb_mlp_param_count) and of the frequency
+ * matrix B (fourier x 2, row-major). set_params also refreshes the BF16 copies. */
+UCB_API int ucb_mlp_get_params(ucb_mlp* m, float* out, long long n);
+UCB_API int ucb_mlp_set_params(ucb_mlp* m, const float* in, long long n);
+UCB_API int ucb_mlp_get_fourier(ucb_mlp* m, float* out, long long n);
+/* Target standardisation (y - mean) / std used by the loss; predictions undo it.
+ * ucb_mlp_fit sets it from the training targets. */
+UCB_API int ucb_mlp_set_target_scale(ucb_mlp* m, float mean, float std);
+/* Mean loss and its gradient with respect to every parameter (host array of
+ * ucb_mlp_param_count) for the rows u (n x 2, host) with targets y (host), computed by the
+ * training kernels (forward, loss, backward) without an update. */
+UCB_API int ucb_mlp_loss_grad(ucb_mlp* m, const float* u, const float* y, long long n, float* loss, float* grad);
+/* Trains on n rows (device arrays u: n x 2, y: n); loss_out: loss of the last step. */
+UCB_API int ucb_mlp_fit(ucb_mlp* m, const float* d_u, const float* d_y, long long n, void* stream, float* loss_out);
+/* Predicted mean and standard deviation for n rows (device arrays). */
+UCB_API int ucb_mlp_predict(ucb_mlp* m, const float* d_u, long long n, float* d_mean, float* d_std, void* stream);
+
+/* ------------------------------------------------------------------------------------
+ * Surrogate-refined LLE map (no counterpart in the reference). The map of `map` (n =
+ * map.n_pts) is computed as:
+ *   1. samples: one cell drawn at random in each block of a train_pts x train_pts
+ *      partition of the grid, integrated with sample_precision (UCB_PREC_F64: the plain
+ *      method); one in eight (by a hash of the block) is held out for calibration;
+ *   2. the MLP (mlp) is trained on the others on this GPU;
+ *   3. it predicts mean and standard deviation for every cell;
+ *   4. calibration: the held-out samples, ordered by predicted std, give the largest std
+ *      threshold below which at least `coverage` of them lie within `tol` of their
+ *      integrated value (capped by sigma_max when > 0);
+ *   5. cells with std above the threshold, |mean| < lle_band, or a 4-neighbour in another
+ *      regime (lambda < -lle_band, |lambda| <= lle_band, lambda > lle_band) or differing
+ *      by more than jump (when jump > 0) are re-integrated with refine_precision straight
+ *      into the map; sample cells keep their integrated value;
+ *   6. every other cell takes the predicted mean.
+ * flags: 1 integrated, 2 predicted, -1 diverged (as ucb_run_lle2d). Outputs are device
+ * arrays of n * n in map order (as ucb_lle2d_device); phase times in the result.
+ * ---------------------------------------------------------------------------------- */
+typedef struct ucb_surrogate_request {
+    ucb_lle2d_request map;
+    int32_t train_pts;          /* samples per axis (default 256) */
+    int32_t sample_precision;   /* default UCB_PREC_F64 (plain samples) */
+    int32_t refine_precision;   /* precision of re-integrated cells (default UCB_PREC_F32) */
+    int32_t pad0;
+    double tol;                 /* error tolerance of a predicted cell (default 2e-3) */
+    double coverage;            /* calibrated fraction within tol (default 0.995) */
+    double sigma_max;           /* cap on the std threshold, 0 = none */
+    double lle_band;            /* default 0.05; 0 = no band / regime rule */
+    double jump;                /* default 0 = off */
+    ucb_mlp_config mlp;
+} ucb_surrogate_request;
+
+typedef struct ucb_surrogate_result {
+    int32_t ok;
+    int32_t n_pts;
+    long long n_samples, n_calib, n_refined, n_predicted, n_diverged;
+    double sigma_threshold;     /* calibrated std threshold (-1: nothing predicted) */
+    double calib_within_tol;    /* fraction of held-out samples under the threshold within tol */
+    double sample_ms, train_ms, predict_ms, select_ms, refine_ms, total_ms;
+    float final_loss;
+    float pad0;
+    char error[1024];
+} ucb_surrogate_result;
+
+UCB_API void ucb_default_surrogate_request(ucb_surrogate_request* r);
+UCB_API int ucb_run_lle2d_surrogate(ucb_engine* e, const ucb_surrogate_request* req, double* d_values,
+                                    int32_t* d_flags, void* stream, ucb_surrogate_result* res);
+
 #ifdef __cplusplus
 }
 #endif

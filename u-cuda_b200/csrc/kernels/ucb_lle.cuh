@@ -20,7 +20,7 @@ struct UcbLleParams {
     int n_blocks;             // (int)(tMax / NT), host double arithmetic
     int pad0;
     long long skip;           // (int)(transientTime / h), host double arithmetic
-    long long nt_steps;       // (size_t)(NT / h) in numb
+    long long nt_steps;       // (size_t)(NT / h): numb (exact form) or double (native form)
     numb h, NT, tmax, eps, maxv, transient;
     numb ic[UCB_NX];
     numb vals[UCB_NV];
@@ -31,13 +31,16 @@ struct UcbLleParams {
     unsigned long long* counter;   // work counter, zeroed before launch
     unsigned long long* steps;     // step evaluations performed (accumulated)
     const long long* cell_list;    // optional: kernel cell indices to compute (total entries)
+    int list_compact;              // with cell_list: entry i is stored at i instead of its cell
 };
 
 namespace ucbdev {
 
-__device__ __forceinline__ void store_cell(const UcbLleParams& p, long long kidx, double v) {
+__device__ __forceinline__ void store_cell(const UcbLleParams& p, long long i, long long kidx, double v) {
     long long out = kidx;
-    if (p.swap_xy) {
+    if (p.cell_list && p.list_compact) {
+        out = i;
+    } else if (p.swap_xy) {
         const long long kix = kidx % p.n_pts, kiy = kidx / p.n_pts;
         out = kix * p.n_pts + kiy;
     }
@@ -213,7 +216,7 @@ extern "C" __global__ void __launch_bounds__(128) ucb_lle_kernel(const UcbLlePar
 #else
             const double v = ucbdev::lle_cell_shadow(p, kidx, ns);
 #endif
-            ucbdev::store_cell(p, kidx, v);
+            ucbdev::store_cell(p, i, kidx, v);
         }
     }
     ucbdev::warp_add_steps(p.steps, ns, lane);

@@ -1,0 +1,1140 @@
+// BF16 MLP surrogate: tcgen05 tensor-core GEMMs, elementwise kernels and the training /
+// prediction host code (no reference counterpart).
+//
+// GEMM: C[M, N] = A[M, K] B[N, K]^T with A and B K-contiguous ("TN"), M % 128 == 0,
+// N % 128 == 0, K % 64 == 0. One CTA of 128 threads computes a 128 x 128 tile: the K loop
+// stages 128 x 64 tiles of A and B into 128-byte-swizzled shared memory (two buffers, so
+// the copy of tile k+1 overlaps the MMAs of tile k), one elected thread issues
+// tcgen05.mma (CuTe SM100_MMA_F16BF16_SS, cta_group::1, BF16 x BF16 -> FP32) into a
+// 128-column TMEM accumulator and commits to the buffer's mbarrier (waits are bounded;
+// on a timeout the kernel records an error, drains and frees TMEM). The epilogue reads
+// TMEM with tcgen05.ld (32 data-path lanes x 32 bit: thread t owns row t) and applies
+// bias / GELU, storing FP32, BF16 and / or transposed BF16 copies; split-K launches add
+// their partial tiles atomically. Backward products are the same TN GEMM on transposed
+// copies, which the forward epilogue and the GELU-backward kernel write as they go.
+#include <cuda_runtime.h>
+
+#include <cute/tensor.hpp>
+#include <cute/arch/tmem_allocator_sm100.hpp>
+#include <cute/atom/mma_traits_sm100.hpp>
+#include <cute/atom/copy_traits_sm100.hpp>
+#include <cute/algorithm/cooperative_copy.hpp>
+#include <cutlass/arch/barrier.h>
+#include <cutlass/numeric_types.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <memory>
+#include <mutex>
+#include <random>
+#include <string>
+#include <vector>
+
+#include "engine_internal.h"
+#include "mlp.h"
+
+namespace ucbmlp {
+
+using namespace cute;
+using bf16 = cutlass::bfloat16_t;
+
+constexpr int kBM = 128;
+constexpr int kBN = 128;
+constexpr int kBK = 64;
+constexpr long long kWaitLimit = 1LL << 22;  // try_wait polls before a wait gives up
+
+using MmaOp = SM100_MMA_F16BF16_SS<bf16, bf16, float, kBM, kBN, UMMA::Major::K, UMMA::Major::K>;
+using TiledMma = decltype(make_tiled_mma(MmaOp{}));
+using SmemLayoutA = decltype(UMMA::tile_to_mma_shape(
+    UMMA::Layout_K_SW128_Atom<bf16>{}, partition_shape_A(TiledMma{}, make_shape(Int<kBM>{}, Int<kBK>{}))));
+using SmemLayoutB = decltype(UMMA::tile_to_mma_shape(
+    UMMA::Layout_K_SW128_Atom<bf16>{}, partition_shape_B(TiledMma{}, make_shape(Int<kBN>{}, Int<kBK>{}))));
+
+constexpr int kStageLd = kBN + 1;  // staging row stride (floats): conflict-free both ways
+
+struct GemmSmem {
+    union {
+        struct {
+            alignas(1024) cute::ArrayEngine<bf16, cosize_v<SmemLayoutA>> A[2];
+            alignas(1024) cute::ArrayEngine<bf16, cosize_v<SmemLayoutB>> B[2];
+        } ab;
+        float stage[kBM * kStageLd];  // epilogue staging (after the last MMA has completed)
+    };
+    alignas(16) cute::uint64_t bar[2];
+    alignas(16) cute::uint32_t tmem_base;
+};
+
+struct Epilogue {
+    const float* bias;  // bias[n] for n < nb (0 beyond)
+    int nb;
+    int gelu;           // outh / outt receive GELU(v) instead of v
+    float* outf;        // FP32 result (pre-activation), row stride ldf
+    int ldf;
+    int atomic;         // outf += v (split-K partial tiles)
+    bf16* outh;         // BF16 copy, row stride ldh
+    int ldh;
+    bf16* outt;         // BF16 transposed copy outt[n * ldt + m]
+    int ldt;
+    int m_store, n_store;  // only rows m < m_store and columns n < n_store are stored
+};
+
+// mbarrier phase wait with a poll limit (each try_wait itself suspends for a bounded time).
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, int phase) {
+    const uint32_t addr = cute::cast_smem_ptr_to_uint(bar);
+    for (long long i = 0; i < kWaitLimit; ++i) {
+        uint32_t done;
+        asm volatile(
+            "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+            : "=r"(done)
+            : "r"(addr), "r"(phase)
+            : "memory");
+        if (done) return true;
+    }
+    return false;
+}
+
+__device__ __forceinline__ void cp_async16(uint32_t smem_addr, const void* gptr) {
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(smem_addr), "l"(gptr) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+    asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
+}
+
+// One 128 x 64 BF16 tile (rows row0.., columns kt*64..) of a K-contiguous matrix into the
+// 128-byte-swizzled K-major shared-memory layout of the MMA (Layout_K_SW128_Atom): row r
+// occupies bytes [128 r, 128 r + 128) of the tile and its 16-byte chunk j sits at chunk
+// j ^ (r % 8). Eight threads read one row's 128 bytes (coalesced 16-byte accesses).
+__device__ __forceinline__ void load_tile(uint32_t smem, const bf16* X, int K, int row0, int kt) {
+    const char* g = reinterpret_cast<const char*>(X + (size_t)row0 * K + (size_t)kt * kBK);
+#pragma unroll
+    for (int it = 0; it < 8; ++it) {
+        const int c = it * 128 + (int)threadIdx.x;
+        const int r = c >> 3, j = c & 7;
+        cp_async16(smem + r * 128 + ((j ^ (r & 7)) << 4), g + (size_t)r * K * 2 + j * 16);
+    }
+}
+
+// GELU in its tanh form, 0.5 z (1 + tanh(sqrt(2/pi) (z + 0.044715 z^3))) (Hendrycks and
+// Gimpel, 2016), with the hardware tanh (tanh.approx.f32, relative error about 2^-11, far
+// below the BF16 rounding that follows).
+__device__ __forceinline__ float tanh_hw(float x) {
+    float y;
+    asm("tanh.approx.f32 %0, %1;" : "=f"(y) : "f"(x));
+    return y;
+}
+constexpr float kGeluC0 = 0.7978845608028654f;  // sqrt(2 / pi)
+constexpr float kGeluC1 = 0.044715f;
+__device__ __forceinline__ float gelu(float z) {
+    const float t = tanh_hw(kGeluC0 * fmaf(kGeluC1 * z * z, z, z));
+    return 0.5f * z * (1.0f + t);
+}
+__device__ __forceinline__ float gelu_grad(float z) {
+    const float z2 = z * z;
+    const float t = tanh_hw(kGeluC0 * fmaf(kGeluC1 * z2, z, z));
+    return 0.5f * (1.0f + t) + 0.5f * z * (1.0f - t * t) * kGeluC0 * fmaf(3.0f * kGeluC1, z2, 1.0f);
+}
+
+__global__ void __launch_bounds__(128) gemm_tn_kernel(const bf16* __restrict__ A, const bf16* __restrict__ B, int M,
+                                                      int N, int K, int kt_per_split, Epilogue ep, int* err) {
+    TiledMma tiled_mma;
+    const int m0 = blockIdx.x * kBM, n0 = blockIdx.y * kBN;
+    Tensor cC = make_identity_tensor(make_shape(M, N));
+    Tensor gcC = local_tile(cC, make_shape(Int<kBM>{}, Int<kBN>{}, Int<kBK>{}), make_coord(blockIdx.x, blockIdx.y, _),
+                            Step<_1, _1, X>{});
+
+    extern __shared__ __align__(1024) char smem_raw[];
+    GemmSmem& ss = *reinterpret_cast<GemmSmem*>(smem_raw);
+    Tensor sA0 = make_tensor(make_smem_ptr(ss.ab.A[0].begin()), SmemLayoutA{});
+    Tensor sA1 = make_tensor(make_smem_ptr(ss.ab.A[1].begin()), SmemLayoutA{});
+    Tensor sB0 = make_tensor(make_smem_ptr(ss.ab.B[0].begin()), SmemLayoutB{});
+    Tensor sB1 = make_tensor(make_smem_ptr(ss.ab.B[1].begin()), SmemLayoutB{});
+    const uint32_t uA[2] = {cute::cast_smem_ptr_to_uint(ss.ab.A[0].begin()),
+                            cute::cast_smem_ptr_to_uint(ss.ab.A[1].begin())};
+    const uint32_t uB[2] = {cute::cast_smem_ptr_to_uint(ss.ab.B[0].begin()),
+                            cute::cast_smem_ptr_to_uint(ss.ab.B[1].begin())};
+
+    ThrMMA cta_mma = tiled_mma.get_slice(0);
+    Tensor tCcC = cta_mma.partition_C(gcC);
+    Tensor fA0 = cta_mma.make_fragment_A(sA0);
+    Tensor fA1 = cta_mma.make_fragment_A(sA1);
+    Tensor fB0 = cta_mma.make_fragment_B(sB0);
+    Tensor fB1 = cta_mma.make_fragment_B(sB1);
+    Tensor tAcc = cta_mma.make_fragment_C(tCcC);
+
+    const int warp = threadIdx.x / 32, lane = threadIdx.x & 31;
+    cute::TMEM::Allocator1Sm tmem;
+    if (warp == 0) tmem.allocate(kBN, &ss.tmem_base);
+    if (threadIdx.x == 0) {
+        cute::initialize_barrier(ss.bar[0], 1);
+        cute::initialize_barrier(ss.bar[1], 1);
+        cutlass::arch::fence_barrier_init();
+    }
+    __syncthreads();
+    tAcc.data() = ss.tmem_base;
+
+    const int kt_total = K / kBK;
+    const int kt0 = blockIdx.z * kt_per_split;
+    const int nk = min(kt_total, kt0 + kt_per_split) - kt0;
+    tiled_mma.accumulate_ = UMMA::ScaleOut::Zero;
+    auto issue = [&](auto const& fA, auto const& fB) {
+        CUTE_UNROLL
+        for (int kb = 0; kb < size<2>(fA); ++kb) {
+            gemm(tiled_mma, fA(_, _, kb), fB(_, _, kb), tAcc);
+            tiled_mma.accumulate_ = UMMA::ScaleOut::One;
+        }
+    };
+    // Two-stage pipeline: the copy of tile i+1 is in flight while the MMAs of tile i run;
+    // a buffer is refilled only after the commit of the MMAs that read it has arrived.
+    bool failed = false;
+    int issued = 0;
+    if (nk > 0) {
+        load_tile(uA[0], A, K, m0, kt0);
+        load_tile(uB[0], B, K, n0, kt0);
+        cp_async_commit();
+    }
+    for (int i = 0; i < nk; ++i) {
+        const int s = i & 1;
+        bool timed_out = false;
+        if (i + 1 < nk) {
+            if (i >= 1) timed_out = !mbar_wait_bounded(&ss.bar[s ^ 1], ((i - 1) >> 1) & 1);
+            if (!timed_out) {
+                load_tile(uA[s ^ 1], A, K, m0, kt0 + i + 1);
+                load_tile(uB[s ^ 1], B, K, n0, kt0 + i + 1);
+            }
+            cp_async_commit();
+            cp_async_wait<1>();
+        } else {
+            cp_async_wait<0>();
+        }
+        cutlass::arch::fence_view_async_shared();
+        if (__syncthreads_or(timed_out)) {
+            failed = true;
+            break;
+        }
+        if (warp == 0) {
+            if (s == 0) issue(fA0, fB0);
+            else issue(fA1, fB1);
+            cutlass::arch::umma_arrive(&ss.bar[s]);
+        }
+        issued = i + 1;
+    }
+    cp_async_wait<0>();
+    // The last commit covers every MMA issued before it.
+    if (issued > 0) {
+        const int j = issued - 1;
+        const bool timed_out = !mbar_wait_bounded(&ss.bar[j & 1], (j >> 1) & 1);
+        failed = __syncthreads_or(timed_out) || failed;
+    }
+    if (failed) {
+        if (threadIdx.x == 0) atomicExch(err, 1);
+    } else if (issued > 0) {
+        // TMEM -> registers (thread t holds tile row t), bias, transposed copy straight from
+        // registers (consecutive threads write consecutive rows), then the row-major
+        // outputs through a per-warp staging block so that a warp stores whole row segments.
+        TiledCopy t2r = make_tmem_copy(SM100_TMEM_LOAD_32dp32b32x{}, tAcc);
+        ThrCopy thr = t2r.get_slice(threadIdx.x);
+        Tensor tDcC = thr.partition_D(tCcC);
+        Tensor tDrAcc = make_tensor<float>(shape(tDcC));
+        Tensor tDtAcc = thr.partition_S(tAcc);
+        copy(t2r, tDtAcc, tDrAcc);
+        float* stage = ss.stage;
+        CUTE_UNROLL
+        for (int i = 0; i < size(tDrAcc); ++i) {
+            const int m = get<0>(tDcC(i)), n = get<1>(tDcC(i));
+            float v = tDrAcc(i);
+            if (ep.bias && n < ep.nb) v += ep.bias[n];
+            stage[(m - m0) * kStageLd + (n - n0)] = v;
+            if (ep.outt && m < ep.m_store && n < ep.n_store)
+                ep.outt[(size_t)n * ep.ldt + m] = bf16(ep.gelu ? gelu(v) : v);
+        }
+        __syncthreads();
+        if (ep.outf || ep.outh) {
+#pragma unroll 2
+            for (int rr = 0; rr < 32; ++rr) {
+                const int r = warp * 32 + rr;
+                const int m = m0 + r;
+                if (m >= ep.m_store) break;
+#pragma unroll
+                for (int q = 0; q < kBN / 32; ++q) {
+                    const int c = q * 32 + lane;
+                    const int n = n0 + c;
+                    if (n >= ep.n_store) continue;
+                    const float v = stage[r * kStageLd + c];
+                    if (ep.outf) {
+                        float* p = ep.outf + (size_t)m * ep.ldf + n;
+                        if (ep.atomic) atomicAdd(p, v);
+                        else *p = v;
+                    }
+                    if (ep.outh) ep.outh[(size_t)m * ep.ldh + n] = bf16(ep.gelu ? gelu(v) : v);
+                }
+            }
+        }
+    }
+    __syncthreads();
+    if (warp == 0) {
+        tmem.release_allocation_lock();
+        tmem.free(ss.tmem_base, kBN);
+    }
+}
+
+// ------------------------------------------------------------------ elementwise kernels
+struct FeatureArgs {
+    const float* u;            // n x 2, or nullptr: points from cells / grid
+    const long long* cells;    // optional kernel-order cells
+    long long n;
+    int grid_n;
+    long long row0;            // first input row of this chunk
+    // mini-batch mode: rows drawn at random from the n inputs with a per-step hash
+    const unsigned long long* step;  // device step counter (nullptr: sequential rows)
+    unsigned long long seed;
+    const float* y;            // targets of the n inputs (training)
+    float y_mean, y_inv_std;
+    float* yb;                 // standardised targets of the batch rows
+    const float* Bf;           // fourier x 2
+    int fourier;
+    int rows;                  // rows of this chunk (multiple of 128)
+    bf16* X;                   // rows x 2 fourier
+    bf16* Xt;                  // 2 fourier x rows (optional)
+};
+
+__device__ __forceinline__ unsigned long long mix64(unsigned long long z) {
+    z += 0x9E3779B97F4A7C15ULL;
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ULL;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBULL;
+    return z ^ (z >> 31);
+}
+
+__device__ __forceinline__ void input_point(const FeatureArgs& a, long long i, float& u0, float& u1) {
+    if (a.u) {
+        u0 = a.u[2 * i];
+        u1 = a.u[2 * i + 1];
+    } else {
+        const long long c = a.cells ? a.cells[i] : i;
+        const float inv = a.grid_n > 1 ? 1.0f / (float)(a.grid_n - 1) : 0.0f;
+        u0 = (float)(c % a.grid_n) * inv;
+        u1 = (float)(c / a.grid_n) * inv;
+    }
+}
+
+// One thread per (row, frequency): X[r, j] = sin(2 pi u.B_j), X[r, F/2 + j] = cos(...).
+__global__ void features_kernel(FeatureArgs a) {
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= (long long)a.rows * a.fourier) return;
+    const int r = (int)(t / a.fourier);
+    const int j = (int)(t % a.fourier);
+    long long i;
+    bool valid;
+    if (a.step) {
+        const unsigned long long h = mix64(a.seed ^ mix64(*a.step * 0x100000001B3ULL + (unsigned long long)r));
+        i = (long long)(h % (unsigned long long)a.n);
+        valid = a.n > 0;
+    } else {
+        i = a.row0 + r;
+        valid = i < a.n;
+    }
+    float s = 0.f, c = 0.f;
+    if (valid) {
+        float u0, u1;
+        input_point(a, i, u0, u1);
+        const float ph = 6.283185307179586f * (u0 * a.Bf[2 * j] + u1 * a.Bf[2 * j + 1]);
+        sincosf(ph, &s, &c);
+    }
+    const int F = 2 * a.fourier;
+    a.X[(size_t)r * F + j] = bf16(s);
+    a.X[(size_t)r * F + a.fourier + j] = bf16(c);
+    if (a.Xt) {
+        a.Xt[(size_t)j * a.rows + r] = bf16(s);
+        a.Xt[(size_t)(a.fourier + j) * a.rows + r] = bf16(c);
+    }
+    if (j == 0 && a.yb) a.yb[r] = valid ? (a.y[i] - a.y_mean) * a.y_inv_std : 0.f;
+}
+
+// Gaussian NLL of the standardised target with beta weighting. out: rows x 2 (mean,
+// log-variance). Writes dOut (rows x 64, columns >= 2 stay zero), dOut^T rows 0 and 1
+// (128 x rows, other rows stay zero), the output-layer bias gradient and the mean loss.
+__global__ void nll_kernel(const float* out, const float* yb, int rows, int n_valid, float beta, bf16* dout,
+                           bf16* doutT, float* db, float* loss) {
+    const int r = blockIdx.x * blockDim.x + threadIdx.x;
+    float g0 = 0.f, g1 = 0.f, l = 0.f;
+    if (r < rows && r < n_valid) {
+        const float mu = out[2 * r];
+        const float lv_raw = out[2 * r + 1];
+        const float lv = fminf(fmaxf(lv_raw, -16.f), 16.f);
+        const float iv = expf(-lv);
+        const float d = mu - yb[r];
+        const float w = beta > 0.f ? expf(beta * lv) : 1.f;  // constant weight sigma^(2 beta)
+        const float inv_n = 1.f / (float)n_valid;
+        l = w * 0.5f * (lv + d * d * iv) * inv_n;
+        g0 = w * d * iv * inv_n;
+        g1 = (lv_raw == lv) ? w * 0.5f * (1.f - d * d * iv) * inv_n : 0.f;
+    }
+    if (r < rows) {
+        dout[(size_t)r * 64] = bf16(g0);
+        dout[(size_t)r * 64 + 1] = bf16(g1);
+        doutT[r] = bf16(g0);
+        doutT[(size_t)rows + r] = bf16(g1);
+    }
+    // block sums of the (BF16-rounded, as the GEMMs see them) bias gradients and the loss
+    __shared__ float s0[256], s1[256], sl[256];
+    s0[threadIdx.x] = float(bf16(g0));
+    s1[threadIdx.x] = float(bf16(g1));
+    sl[threadIdx.x] = l;
+    __syncthreads();
+    for (int w = blockDim.x / 2; w > 0; w >>= 1) {
+        if (threadIdx.x < w) {
+            s0[threadIdx.x] += s0[threadIdx.x + w];
+            s1[threadIdx.x] += s1[threadIdx.x + w];
+            sl[threadIdx.x] += sl[threadIdx.x + w];
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        atomicAdd(&db[0], s0[0]);
+        atomicAdd(&db[1], s1[0]);
+        atomicAdd(loss, sl[0]);
+    }
+}
+
+// dZ = dH * GELU'(Z) -> BF16 dZ (rows x N) and dZ^T (N x rows); db[c] += sum_r dZ[r, c]
+// (of the BF16-rounded values the GEMMs use). Block 32 x 8 over a 32 x 32 tile.
+__global__ void gelu_back_kernel(const float* dH, const float* Z, int rows, int N, bf16* dZ, bf16* dZt, float* db) {
+    __shared__ float tile[32][33];
+    const int c0 = blockIdx.x * 32, r0 = blockIdx.y * 32;
+    const int tx = threadIdx.x, ty = threadIdx.y;
+    for (int k = 0; k < 32; k += 8) {
+        const int r = r0 + ty + k, c = c0 + tx;
+        float v = 0.f;
+        if (r < rows && c < N) {
+            const bf16 b = bf16(dH[(size_t)r * N + c] * gelu_grad(Z[(size_t)r * N + c]));
+            dZ[(size_t)r * N + c] = b;
+            v = float(b);
+        }
+        tile[ty + k][tx] = v;
+    }
+    __syncthreads();
+    for (int k = 0; k < 32; k += 8) {
+        const int c = c0 + ty + k, r = r0 + tx;
+        if (c < N && r < rows) dZt[(size_t)c * rows + r] = bf16(tile[tx][ty + k]);
+    }
+    if (ty == 0 && c0 + tx < N) {
+        float s = 0.f;
+        for (int k = 0; k < 32; ++k) s += tile[k][tx];
+        atomicAdd(&db[c0 + tx], s);
+    }
+}
+
+// Adam with cosine learning-rate decay; the step counter lives on the device so that a
+// captured training step replays unchanged.
+struct AdamArgs {
+    float* w;
+    const float* g;
+    float* m;
+    float* v;
+    long long n;
+    const unsigned long long* step;
+    int total_steps;
+    float lr0, lr1, b1, b2, eps;
+};
+
+__global__ void adam_kernel(AdamArgs a) {
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= a.n) return;
+    const unsigned long long t = *a.step;  // 0-based
+    const float frac = a.total_steps > 1 ? fminf((float)t / (float)(a.total_steps - 1), 1.f) : 1.f;
+    const float lr = a.lr1 + 0.5f * (a.lr0 - a.lr1) * (1.f + cospif(frac));
+    const float c1 = 1.f - powf(a.b1, (float)(t + 1));
+    const float c2 = 1.f - powf(a.b2, (float)(t + 1));
+    const float gi = a.g[i];
+    const float mi = a.b1 * a.m[i] + (1.f - a.b1) * gi;
+    const float vi = a.b2 * a.v[i] + (1.f - a.b2) * gi * gi;
+    a.m[i] = mi;
+    a.v[i] = vi;
+    a.w[i] -= lr * (mi / c1) / (sqrtf(vi / c2) + a.eps);
+}
+
+// BF16 copies of every layer's weights: W (out_pad x in, rows >= out zero) for the
+// forward product and W^T (in x outk, columns >= out zero) for the backward product.
+constexpr int kMaxLayers = 9;
+struct RefreshArgs {
+    int n_layers;
+    const float* p;
+    long long w_off[kMaxLayers];
+    int out[kMaxLayers], in[kMaxLayers], out_pad[kMaxLayers], outk[kMaxLayers];
+    bf16* W[kMaxLayers];
+    bf16* Wt[kMaxLayers];
+    long long start[kMaxLayers + 1];  // prefix sums of out_pad * in
+    unsigned long long* step;         // incremented once per call when non-null
+};
+
+__global__ void refresh_kernel(RefreshArgs a) {
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t == 0 && a.step) *a.step += 1;
+    if (t >= a.start[a.n_layers]) return;
+    int l = 0;
+    while (t >= a.start[l + 1]) ++l;
+    const long long k = t - a.start[l];
+    const int o = (int)(k / a.in[l]), c = (int)(k % a.in[l]);
+    const float val = o < a.out[l] ? a.p[a.w_off[l] + (long long)o * a.in[l] + c] : 0.f;
+    a.W[l][(size_t)o * a.in[l] + c] = bf16(val);
+    if (a.Wt[l] && o < a.outk[l]) a.Wt[l][(size_t)c * a.outk[l] + o] = bf16(val);
+}
+
+// Undoes the target standardisation: mean = mu * std_y + mean_y, std = exp(lv / 2) std_y.
+__global__ void unscale_kernel(const float* out, int rows, long long n_left, float y_mean, float y_std, float* mean,
+                               float* sd) {
+    const int r = blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= rows || r >= n_left) return;
+    mean[r] = out[2 * r] * y_std + y_mean;
+    sd[r] = expf(0.5f * fminf(fmaxf(out[2 * r + 1], -16.f), 16.f)) * y_std;
+}
+
+}  // namespace ucbmlp
+
+// ====================================================================== host side
+namespace ucb {
+
+using ucbmlp::bf16;
+
+namespace {
+
+bool cu_ok(cudaError_t e, std::string& err, const char* what) {
+    if (e == cudaSuccess) return true;
+    err = std::string(what) + ": " + cudaGetErrorString(e);
+    return false;
+}
+
+template <class T>
+T* dalloc(size_t count, std::vector<void*>& owned, std::string& err, const char* what) {
+    void* p = nullptr;
+    if (cudaMalloc(&p, std::max<size_t>(count, 1) * sizeof(T)) != cudaSuccess) {
+        err = std::string("cudaMalloc(") + what + ") failed";
+        return nullptr;
+    }
+    cudaMemset(p, 0, std::max<size_t>(count, 1) * sizeof(T));
+    owned.push_back(p);
+    return static_cast<T*>(p);
+}
+
+}  // namespace
+
+struct Mlp {
+    ucb_engine* e = nullptr;
+    ucb_mlp_config cfg{};
+    int F = 0, H = 0, L = 0;
+    std::vector<int> in, out, out_pad, outk;
+    std::vector<long long> w_off, b_off;
+    long long n_params = 0;
+    std::vector<void*> owned;      // device allocations of the network
+    std::vector<void*> act_owned;  // batch-size dependent
+    float *p = nullptr, *g = nullptr, *m1 = nullptr, *m2 = nullptr, *Bf = nullptr;
+    std::vector<bf16*> W, Wt;
+    unsigned long long* step = nullptr;
+    int* err = nullptr;
+    float* loss = nullptr;
+    float y_mean = 0.f, y_std = 1.f;
+    int rows = 0;                  // activation capacity (rows)
+    bf16 *X = nullptr, *Xt = nullptr;
+    std::vector<float*> Z;
+    std::vector<bf16*> Hb, Ht;
+    float* outp = nullptr;         // rows x 2
+    float* yb = nullptr;
+    bf16 *dout = nullptr, *doutT = nullptr, *dZ = nullptr, *dZt = nullptr;
+    float* dH = nullptr;
+    // prediction buffers (ping-pong activations, no backward copies)
+    std::vector<void*> pred_owned;
+    int pred_rows = 0;
+    bf16* pX = nullptr;
+    bf16* pH[2] = {nullptr, nullptr};
+    float* pOut = nullptr;
+    cudaGraphExec_t graph = nullptr;
+    long long graph_nodes = 0;
+    MlpInputs graph_in;
+    const float* graph_y = nullptr;
+    float graph_y_mean = 0.f, graph_y_std = 0.f;
+
+    ~Mlp() {
+        if (graph) cudaGraphExecDestroy(graph);
+        for (void* q : act_owned) cudaFree(q);
+        for (void* q : pred_owned) cudaFree(q);
+        for (void* q : owned) cudaFree(q);
+    }
+};
+
+namespace {
+
+std::mutex g_attr_mu;
+std::vector<int> g_attr_devices;
+
+int gemm_smem_bytes() { return (int)sizeof(ucbmlp::GemmSmem); }
+
+// Dynamic shared memory above 48 KB is opted in once per device, before launches and
+// before any stream capture.
+bool set_gemm_attributes(int device, std::string& err) {
+    std::lock_guard<std::mutex> lk(g_attr_mu);
+    if (std::find(g_attr_devices.begin(), g_attr_devices.end(), device) != g_attr_devices.end()) return true;
+    const cudaError_t ce = cudaFuncSetAttribute(ucbmlp::gemm_tn_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                gemm_smem_bytes());
+    if (!cu_ok(ce, err, "cudaFuncSetAttribute(gemm)")) return false;
+    g_attr_devices.push_back(device);
+    return true;
+}
+
+// C = A B^T (+ epilogue); split-K when the epilogue accumulates atomically.
+bool gemm(Mlp& m, const bf16* A, const bf16* B, int M, int N, int K, const ucbmlp::Epilogue& ep, cudaStream_t st,
+          std::string& err) {
+    if (M <= 0 || N <= 0 || K <= 0 || M % ucbmlp::kBM || N % ucbmlp::kBN || K % ucbmlp::kBK) {
+        err = "gemm: unsupported shape " + std::to_string(M) + "x" + std::to_string(N) + "x" + std::to_string(K);
+        return false;
+    }
+    const int tiles = (M / ucbmlp::kBM) * (N / ucbmlp::kBN);
+    const int kt = K / ucbmlp::kBK;
+    int per = kt;
+    if (ep.atomic) {
+        const int want = std::max(1, std::min(kt, (2 * std::max(m.e->sm_count, 1) + tiles - 1) / tiles));
+        per = (kt + want - 1) / want;
+    }
+    const int splits = (kt + per - 1) / per;
+    dim3 grid(M / ucbmlp::kBM, N / ucbmlp::kBN, splits);
+    ucbmlp::gemm_tn_kernel<<<grid, 128, gemm_smem_bytes(), st>>>(A, B, M, N, K, per, ep, m.err);
+    m.e->launches += 1;
+    return cu_ok(cudaPeekAtLastError(), err, "gemm launch");
+}
+
+ucbmlp::Epilogue epi() {
+    ucbmlp::Epilogue ep{};
+    ep.m_store = 1 << 30;
+    ep.n_store = 1 << 30;
+    return ep;
+}
+
+bool ensure_rows(Mlp& m, int rows, std::string& err) {
+    if (rows <= m.rows) return true;
+    if (m.graph) {
+        cudaGraphExecDestroy(m.graph);
+        m.graph = nullptr;
+    }
+    for (void* q : m.act_owned) cudaFree(q);
+    m.act_owned.clear();
+    m.Z.clear();
+    m.Hb.clear();
+    m.Ht.clear();
+    m.rows = 0;
+    auto& o = m.act_owned;
+    const size_t R = rows;
+    if (!(m.X = dalloc<bf16>(R * m.F, o, err, "features")) || !(m.Xt = dalloc<bf16>(R * m.F, o, err, "features^T")))
+        return false;
+    for (int l = 0; l < m.L; ++l) {
+        float* z = dalloc<float>(R * m.H, o, err, "Z");
+        bf16* h = dalloc<bf16>(R * m.H, o, err, "H");
+        bf16* ht = dalloc<bf16>(R * m.H, o, err, "H^T");
+        if (!z || !h || !ht) return false;
+        m.Z.push_back(z);
+        m.Hb.push_back(h);
+        m.Ht.push_back(ht);
+    }
+    if (!(m.outp = dalloc<float>(R * 2, o, err, "out")) || !(m.yb = dalloc<float>(R, o, err, "y batch")) ||
+        !(m.dout = dalloc<bf16>(R * 64, o, err, "dOut")) || !(m.doutT = dalloc<bf16>(R * 128, o, err, "dOut^T")) ||
+        !(m.dZ = dalloc<bf16>(R * m.H, o, err, "dZ")) || !(m.dZt = dalloc<bf16>(R * m.H, o, err, "dZ^T")) ||
+        !(m.dH = dalloc<float>(R * m.H, o, err, "dH")))
+        return false;
+    m.rows = rows;
+    return true;
+}
+
+bool ensure_pred_rows(Mlp& m, int rows, std::string& err) {
+    if (rows <= m.pred_rows) return true;
+    for (void* q : m.pred_owned) cudaFree(q);
+    m.pred_owned.clear();
+    m.pred_rows = 0;
+    auto& o = m.pred_owned;
+    const size_t R = rows;
+    if (!(m.pX = dalloc<bf16>(R * m.F, o, err, "features")) || !(m.pH[0] = dalloc<bf16>(R * m.H, o, err, "H")) ||
+        !(m.pH[1] = dalloc<bf16>(R * m.H, o, err, "H")) || !(m.pOut = dalloc<float>(R * 2, o, err, "out")))
+        return false;
+    m.pred_rows = rows;
+    return true;
+}
+
+bool refresh(Mlp& m, cudaStream_t st, bool count_step, std::string& err) {
+    ucbmlp::RefreshArgs a{};
+    a.n_layers = m.L + 1;
+    a.p = m.p;
+    a.start[0] = 0;
+    for (int l = 0; l <= m.L; ++l) {
+        a.w_off[l] = m.w_off[l];
+        a.out[l] = m.out[l];
+        a.in[l] = m.in[l];
+        a.out_pad[l] = m.out_pad[l];
+        a.outk[l] = m.outk[l];
+        a.W[l] = m.W[l];
+        a.Wt[l] = m.Wt[l];
+        a.start[l + 1] = a.start[l] + (long long)m.out_pad[l] * m.in[l];
+    }
+    a.step = count_step ? m.step : nullptr;
+    const long long total = a.start[a.n_layers];
+    ucbmlp::refresh_kernel<<<(unsigned)((total + 255) / 256), 256, 0, st>>>(a);
+    m.e->launches += 1;
+    return cu_ok(cudaPeekAtLastError(), err, "refresh launch");
+}
+
+ucbmlp::FeatureArgs feature_args(Mlp& m, const MlpInputs& in, long long row0, int rows, bool train) {
+    ucbmlp::FeatureArgs a{};
+    a.u = in.u;
+    a.cells = in.cells;
+    a.n = in.n;
+    a.grid_n = in.grid_n;
+    a.row0 = row0;
+    a.step = train ? m.step : nullptr;
+    a.seed = m.cfg.seed * 0x9E3779B97F4A7C15ULL + 12345;
+    a.y_mean = m.y_mean;
+    a.y_inv_std = 1.f / m.y_std;
+    a.Bf = m.Bf;
+    a.fourier = m.cfg.fourier;
+    a.rows = rows;
+    a.X = m.X;
+    a.Xt = train ? m.Xt : nullptr;
+    return a;
+}
+
+bool features(Mlp& m, const ucbmlp::FeatureArgs& a, cudaStream_t st, std::string& err) {
+    const long long t = (long long)a.rows * a.fourier;
+    ucbmlp::features_kernel<<<(unsigned)((t + 255) / 256), 256, 0, st>>>(a);
+    m.e->launches += 1;
+    return cu_ok(cudaPeekAtLastError(), err, "features launch");
+}
+
+// Forward pass over `rows` rows of m.X. keep: store Z and H^T for the backward pass.
+bool forward(Mlp& m, int rows, bool keep, cudaStream_t st, std::string& err) {
+    const bf16* x = m.X;
+    int k = m.F;
+    for (int l = 0; l < m.L; ++l) {
+        ucbmlp::Epilogue ep = epi();
+        ep.bias = m.p + m.b_off[l];
+        ep.nb = m.H;
+        ep.gelu = 1;
+        ep.outf = keep ? m.Z[l] : nullptr;
+        ep.ldf = m.H;
+        ep.outh = m.Hb[l];
+        ep.ldh = m.H;
+        ep.outt = keep ? m.Ht[l] : nullptr;
+        ep.ldt = rows;
+        if (!gemm(m, x, m.W[l], rows, m.H, k, ep, st, err)) return false;
+        x = m.Hb[l];
+        k = m.H;
+    }
+    ucbmlp::Epilogue ep = epi();
+    ep.bias = m.p + m.b_off[m.L];
+    ep.nb = 2;
+    ep.outf = m.outp;
+    ep.ldf = 2;
+    ep.n_store = 2;
+    return gemm(m, x, m.W[m.L], rows, m.out_pad[m.L], m.H, ep, st, err);
+}
+
+// Inference forward pass over `rows` rows of m.pX (activations ping-pong in m.pH).
+bool forward_infer(Mlp& m, int rows, cudaStream_t st, std::string& err) {
+    const bf16* x = m.pX;
+    int k = m.F;
+    for (int l = 0; l < m.L; ++l) {
+        ucbmlp::Epilogue ep = epi();
+        ep.bias = m.p + m.b_off[l];
+        ep.nb = m.H;
+        ep.gelu = 1;
+        ep.outh = m.pH[l & 1];
+        ep.ldh = m.H;
+        if (!gemm(m, x, m.W[l], rows, m.H, k, ep, st, err)) return false;
+        x = m.pH[l & 1];
+        k = m.H;
+    }
+    ucbmlp::Epilogue ep = epi();
+    ep.bias = m.p + m.b_off[m.L];
+    ep.nb = 2;
+    ep.outf = m.pOut;
+    ep.ldf = 2;
+    ep.n_store = 2;
+    return gemm(m, x, m.W[m.L], rows, m.out_pad[m.L], m.H, ep, st, err);
+}
+
+// Loss, backward pass and gradient (m.g) for the batch in m.X / m.yb (n_valid rows).
+bool backward(Mlp& m, int rows, int n_valid, cudaStream_t st, std::string& err) {
+    if (!cu_ok(cudaMemsetAsync(m.g, 0, sizeof(float) * m.n_params, st), err, "memset grad") ||
+        !cu_ok(cudaMemsetAsync(m.loss, 0, sizeof(float), st), err, "memset loss"))
+        return false;
+    ucbmlp::nll_kernel<<<(rows + 255) / 256, 256, 0, st>>>(m.outp, m.yb, rows, n_valid, m.cfg.beta_nll, m.dout,
+                                                          m.doutT, m.g + m.b_off[m.L], m.loss);
+    m.e->launches += 1;
+    if (!cu_ok(cudaPeekAtLastError(), err, "nll launch")) return false;
+    const int Lo = m.L;
+    // output layer: dH = dOut W (K padded to 64), dW = dOut^T H (M padded to 128)
+    {
+        ucbmlp::Epilogue ep = epi();
+        ep.outf = m.dH;
+        ep.ldf = m.H;
+        if (!gemm(m, m.dout, m.Wt[Lo], rows, m.H, 64, ep, st, err)) return false;
+        ucbmlp::Epilogue eg = epi();
+        eg.outf = m.g + m.w_off[Lo];
+        eg.ldf = m.H;
+        eg.atomic = 1;
+        eg.m_store = 2;
+        if (!gemm(m, m.doutT, m.Ht[Lo - 1], 128, m.H, rows, eg, st, err)) return false;
+    }
+    for (int l = Lo - 1; l >= 0; --l) {
+        dim3 gb((m.H + 31) / 32, (rows + 31) / 32);
+        ucbmlp::gelu_back_kernel<<<gb, dim3(32, 8), 0, st>>>(m.dH, m.Z[l], rows, m.H, m.dZ, m.dZt,
+                                                             m.g + m.b_off[l]);
+        m.e->launches += 1;
+        if (!cu_ok(cudaPeekAtLastError(), err, "gelu_back launch")) return false;
+        const bf16* prevT = l > 0 ? m.Ht[l - 1] : m.Xt;
+        const int in = m.in[l];
+        ucbmlp::Epilogue eg = epi();
+        eg.outf = m.g + m.w_off[l];
+        eg.ldf = in;
+        eg.atomic = 1;
+        if (!gemm(m, m.dZt, prevT, m.H, in, rows, eg, st, err)) return false;
+        if (l > 0) {
+            ucbmlp::Epilogue ep = epi();
+            ep.outf = m.dH;
+            ep.ldf = m.H;
+            if (!gemm(m, m.dZ, m.Wt[l], rows, in, m.H, ep, st, err)) return false;
+        }
+    }
+    return true;
+}
+
+bool adam(Mlp& m, cudaStream_t st, std::string& err) {
+    ucbmlp::AdamArgs a{m.p, m.g, m.m1, m.m2, m.n_params, m.step, m.cfg.train_steps,
+                       m.cfg.lr, m.cfg.lr_final, 0.9f, 0.999f, 1e-8f};
+    ucbmlp::adam_kernel<<<(unsigned)((m.n_params + 255) / 256), 256, 0, st>>>(a);
+    m.e->launches += 1;
+    return cu_ok(cudaPeekAtLastError(), err, "adam launch");
+}
+
+bool check_kernel_error(Mlp& m, cudaStream_t st, std::string& err) {
+    int h = 0;
+    if (!cu_ok(cudaMemcpyAsync(&h, m.err, sizeof(int), cudaMemcpyDeviceToHost, st), err, "read error flag") ||
+        !cu_ok(cudaStreamSynchronize(st), err, "mlp"))
+        return false;
+    if (h) {
+        err = "tensor-core GEMM timed out waiting for its MMAs";
+        return false;
+    }
+    return true;
+}
+
+// One training step (features of a random batch, forward, loss, backward, Adam, BF16
+// refresh + step count): the sequence that is captured into a CUDA graph.
+bool train_step(Mlp& m, const MlpInputs& in, const float* d_y, cudaStream_t st, std::string& err) {
+    const int rows = m.cfg.batch;
+    ucbmlp::FeatureArgs fa = feature_args(m, in, 0, rows, true);
+    fa.y = d_y;
+    fa.yb = m.yb;
+    return features(m, fa, st, err) && forward(m, rows, true, st, err) && backward(m, rows, rows, st, err) &&
+           adam(m, st, err) && refresh(m, st, true, err);
+}
+
+}  // namespace
+
+Mlp* mlp_create(ucb_engine* e, const ucb_mlp_config& c, std::string& err) {
+    if (c.fourier <= 0 || (2 * c.fourier) % 128 || c.hidden <= 0 || c.hidden % 128 || c.layers < 1 ||
+        c.layers > ucbmlp::kMaxLayers - 1 || c.batch <= 0 || c.batch % 128 || c.train_steps < 0 ||
+        !(c.fourier_scale >= 0.f)) {
+        err = "invalid MLP configuration (2*fourier % 128 == 0, hidden % 128 == 0, 1 <= layers <= 8, "
+              "batch % 128 == 0, train_steps >= 0)";
+        return nullptr;
+    }
+    if (!ensure_init(e, err)) return nullptr;
+    if (!set_gemm_attributes(e->device, err)) return nullptr;
+    auto m = std::make_unique<Mlp>();
+    m->e = e;
+    m->cfg = c;
+    m->F = 2 * c.fourier;
+    m->H = c.hidden;
+    m->L = c.layers;
+    long long off = 0;
+    for (int l = 0; l <= m->L; ++l) {
+        const int i = l == 0 ? m->F : m->H;
+        const int o = l == m->L ? 2 : m->H;
+        m->in.push_back(i);
+        m->out.push_back(o);
+        m->out_pad.push_back(l == m->L ? 128 : o);
+        m->outk.push_back(l == m->L ? 64 : o);
+        m->w_off.push_back(off);
+        off += (long long)o * i;
+        m->b_off.push_back(off);
+        off += o;
+    }
+    m->n_params = off;
+    auto& ow = m->owned;
+    if (!(m->p = dalloc<float>(off, ow, err, "params")) || !(m->g = dalloc<float>(off, ow, err, "grad")) ||
+        !(m->m1 = dalloc<float>(off, ow, err, "adam m")) || !(m->m2 = dalloc<float>(off, ow, err, "adam v")) ||
+        !(m->Bf = dalloc<float>(2 * c.fourier, ow, err, "fourier")) ||
+        !(m->step = dalloc<unsigned long long>(1, ow, err, "step")) || !(m->err = dalloc<int>(1, ow, err, "err")) ||
+        !(m->loss = dalloc<float>(1, ow, err, "loss")))
+        return nullptr;
+    for (int l = 0; l <= m->L; ++l) {
+        bf16* w = dalloc<bf16>((size_t)m->out_pad[l] * m->in[l], ow, err, "W bf16");
+        bf16* wt = l > 0 ? dalloc<bf16>((size_t)m->in[l] * m->outk[l], ow, err, "W^T bf16") : nullptr;
+        if (!w || (l > 0 && !wt)) return nullptr;
+        m->W.push_back(w);
+        m->Wt.push_back(wt);
+    }
+    // Initialisation: W ~ N(0, 2 / in) for hidden layers (GELU), N(0, 0.1 / in) for the
+    // output layer, biases 0; frequency matrix ~ N(0, fourier_scale^2).
+    std::mt19937_64 rng(c.seed);
+    std::normal_distribution<float> nd(0.f, 1.f);
+    std::vector<float> hp(off, 0.f);
+    for (int l = 0; l <= m->L; ++l) {
+        const float sd = std::sqrt((l == m->L ? 0.1f : 2.0f) / (float)m->in[l]);
+        for (long long k = 0; k < (long long)m->out[l] * m->in[l]; ++k) hp[m->w_off[l] + k] = sd * nd(rng);
+    }
+    std::vector<float> hb(2 * c.fourier);
+    for (auto& v : hb) v = c.fourier_scale * nd(rng);
+    if (!cu_ok(cudaMemcpy(m->p, hp.data(), off * sizeof(float), cudaMemcpyHostToDevice), err, "upload params") ||
+        !cu_ok(cudaMemcpy(m->Bf, hb.data(), hb.size() * sizeof(float), cudaMemcpyHostToDevice), err, "upload B"))
+        return nullptr;
+    if (!refresh(*m, e->stream, false, err) || !cu_ok(cudaStreamSynchronize(e->stream), err, "init")) return nullptr;
+    return m.release();
+}
+
+void mlp_destroy(Mlp* m) {
+    if (!m) return;
+    cudaDeviceSynchronize();
+    delete m;
+}
+
+long long mlp_param_count(const Mlp* m) { return m ? m->n_params : 0; }
+int mlp_features(const Mlp* m) { return m ? m->F : 0; }
+
+bool mlp_predict(Mlp* m, const MlpInputs& in, float* d_mean, float* d_std, cudaStream_t st, std::string& err) {
+    if (in.n <= 0) return true;
+    const long long chunk = 1 << 18;
+    const long long rows_needed = std::min<long long>(chunk, ((in.n + 127) / 128) * 128);
+    if (!ensure_pred_rows(*m, (int)rows_needed, err)) return false;
+    for (long long r0 = 0; r0 < in.n; r0 += chunk) {
+        const long long left = in.n - r0;
+        const int rows = (int)std::min<long long>(chunk, ((left + 127) / 128) * 128);
+        ucbmlp::FeatureArgs fa = feature_args(*m, in, r0, rows, false);
+        fa.X = m->pX;
+        if (!features(*m, fa, st, err) || !forward_infer(*m, rows, st, err)) return false;
+        ucbmlp::unscale_kernel<<<(rows + 255) / 256, 256, 0, st>>>(m->pOut, rows, left, m->y_mean, m->y_std,
+                                                                   d_mean + r0, d_std + r0);
+        m->e->launches += 1;
+        if (!cu_ok(cudaPeekAtLastError(), err, "unscale launch")) return false;
+    }
+    return true;
+}
+
+bool mlp_fit(Mlp* m, const MlpInputs& in, const float* d_y, cudaStream_t st, float* loss_out, std::string& err) {
+    if (in.n <= 0) {
+        err = "no training rows";
+        return false;
+    }
+    // target standardisation from the training targets
+    std::vector<float> hy(in.n);
+    if (!cu_ok(cudaMemcpyAsync(hy.data(), d_y, in.n * sizeof(float), cudaMemcpyDeviceToHost, st), err, "read y") ||
+        !cu_ok(cudaStreamSynchronize(st), err, "read y"))
+        return false;
+    double s = 0, s2 = 0;
+    for (float v : hy) {
+        s += v;
+        s2 += (double)v * v;
+    }
+    const double mean = s / in.n;
+    const double var = std::max(s2 / in.n - mean * mean, 1e-12);
+    m->y_mean = (float)mean;
+    m->y_std = (float)std::sqrt(var);
+    if (!ensure_rows(*m, m->cfg.batch, err)) return false;
+    if (!cu_ok(cudaMemsetAsync(m->step, 0, sizeof(unsigned long long), st), err, "reset step") ||
+        !cu_ok(cudaMemsetAsync(m->m1, 0, m->n_params * sizeof(float), st), err, "reset adam") ||
+        !cu_ok(cudaMemsetAsync(m->m2, 0, m->n_params * sizeof(float), st), err, "reset adam") ||
+        !cu_ok(cudaMemsetAsync(m->err, 0, sizeof(int), st), err, "reset err"))
+        return false;
+    if (m->cfg.train_steps == 0) return true;
+    // The captured step bakes in the inputs and the target scale.
+    const bool same = m->graph && m->graph_in.u == in.u && m->graph_in.cells == in.cells && m->graph_in.n == in.n &&
+                      m->graph_in.grid_n == in.grid_n && m->graph_y == d_y && m->graph_y_mean == m->y_mean &&
+                      m->graph_y_std == m->y_std;
+    if (!same) {
+        if (m->graph) {
+            cudaGraphExecDestroy(m->graph);
+            m->graph = nullptr;
+        }
+        // Capture one step on a private stream (capture does not run the kernels, so the
+        // launch counter is restored and advanced per replay instead).
+        cudaStream_t cs;
+        if (!cu_ok(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking), err, "capture stream")) return false;
+        const long long l0 = m->e->launches;
+        cudaGraph_t g = nullptr;
+        bool ok = cu_ok(cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal), err, "begin capture");
+        if (ok) {
+            ok = train_step(*m, in, d_y, cs, err);
+            const cudaError_t ce = cudaStreamEndCapture(cs, &g);
+            ok = ok && cu_ok(ce, err, "end capture");
+        }
+        m->graph_nodes = m->e->launches - l0;
+        m->e->launches = l0;
+        if (ok) ok = cu_ok(cudaGraphInstantiate(&m->graph, g, 0), err, "graph instantiate");
+        if (g) cudaGraphDestroy(g);
+        cudaStreamDestroy(cs);
+        if (!ok) return false;
+        m->graph_in = in;
+        m->graph_y = d_y;
+        m->graph_y_mean = m->y_mean;
+        m->graph_y_std = m->y_std;
+    }
+    for (int t = 0; t < m->cfg.train_steps; ++t) {
+        if (!cu_ok(cudaGraphLaunch(m->graph, st), err, "graph launch")) return false;
+    }
+    m->e->launches += m->graph_nodes * m->cfg.train_steps;
+    if (!check_kernel_error(*m, st, err)) return false;
+    if (loss_out && !cu_ok(cudaMemcpy(loss_out, m->loss, sizeof(float), cudaMemcpyDeviceToHost), err, "read loss"))
+        return false;
+    return true;
+}
+
+}  // namespace ucb
+
+// ====================================================================== C ABI
+using namespace ucb;
+
+struct ucb_mlp {
+    ucb_engine* e;
+    Mlp* m;
+};
+
+extern "C" {
+
+void ucb_mlp_default_config(ucb_mlp_config* c) {
+    std::memset(c, 0, sizeof *c);
+    c->fourier = 64;
+    c->hidden = 256;
+    c->layers = 4;
+    c->fourier_scale = 6.0f;
+    c->seed = 0;
+    c->batch = 8192;
+    c->train_steps = 2000;
+    c->lr = 2e-3f;
+    c->lr_final = 2e-5f;
+    c->beta_nll = 0.5f;
+}
+
+ucb_mlp* ucb_mlp_create(ucb_engine* e, const ucb_mlp_config* cfg) {
+    if (!e || !cfg) return nullptr;
+    std::string err;
+    cudaSetDevice(e->device);
+    Mlp* m = mlp_create(e, *cfg, err);
+    if (!m) {
+        e->last_error = err;
+        return nullptr;
+    }
+    return new ucb_mlp{e, m};
+}
+
+void ucb_mlp_destroy(ucb_mlp* m) {
+    if (!m) return;
+    cudaSetDevice(m->e->device);
+    mlp_destroy(m->m);
+    delete m;
+}
+
+long long ucb_mlp_param_count(const ucb_mlp* m) { return m ? m->m->n_params : 0; }
+
+int ucb_mlp_get_params(ucb_mlp* m, float* out, long long n) {
+    if (!m || !out || n != m->m->n_params) return UCB_E_INVALID;
+    cudaSetDevice(m->e->device);
+    return cudaMemcpy(out, m->m->p, n * sizeof(float), cudaMemcpyDeviceToHost) == cudaSuccess ? UCB_OK : UCB_E_CUDA;
+}
+
+int ucb_mlp_set_params(ucb_mlp* m, const float* in, long long n) {
+    if (!m || !in || n != m->m->n_params) return UCB_E_INVALID;
+    cudaSetDevice(m->e->device);
+    std::string err;
+    if (cudaMemcpy(m->m->p, in, n * sizeof(float), cudaMemcpyHostToDevice) != cudaSuccess) return UCB_E_CUDA;
+    if (!refresh(*m->m, m->e->stream, false, err) || cudaStreamSynchronize(m->e->stream) != cudaSuccess) {
+        m->e->last_error = err;
+        return UCB_E_CUDA;
+    }
+    return UCB_OK;
+}
+
+int ucb_mlp_get_fourier(ucb_mlp* m, float* out, long long n) {
+    if (!m || !out || n != 2LL * m->m->cfg.fourier) return UCB_E_INVALID;
+    cudaSetDevice(m->e->device);
+    return cudaMemcpy(out, m->m->Bf, n * sizeof(float), cudaMemcpyDeviceToHost) == cudaSuccess ? UCB_OK : UCB_E_CUDA;
+}
+
+int ucb_mlp_set_target_scale(ucb_mlp* m, float mean, float sd) {
+    if (!m || !(sd > 0.f)) return UCB_E_INVALID;
+    m->m->y_mean = mean;
+    m->m->y_std = sd;
+    return UCB_OK;
+}
+
+int ucb_mlp_loss_grad(ucb_mlp* h, const float* u, const float* y, long long n, float* loss, float* grad) {
+    if (!h || !u || !y || !loss || !grad || n <= 0 || n > (1 << 20)) return UCB_E_INVALID;
+    cudaSetDevice(h->e->device);
+    Mlp& m = *h->m;
+    std::string err;
+    const int rows = (int)(((n + 127) / 128) * 128);
+    float *du = nullptr, *dy = nullptr;
+    int rc = UCB_OK;
+    cudaStream_t st = h->e->stream;
+    if (!ensure_rows(m, rows, err) || !cu_ok(cudaMalloc(&du, n * 2 * sizeof(float)), err, "alloc u") ||
+        !cu_ok(cudaMalloc(&dy, n * sizeof(float)), err, "alloc y") ||
+        !cu_ok(cudaMemcpy(du, u, n * 2 * sizeof(float), cudaMemcpyHostToDevice), err, "upload u") ||
+        !cu_ok(cudaMemcpy(dy, y, n * sizeof(float), cudaMemcpyHostToDevice), err, "upload y") ||
+        !cu_ok(cudaMemsetAsync(m.err, 0, sizeof(int), st), err, "reset err")) {
+        rc = UCB_E_CUDA;
+    } else {
+        MlpInputs in;
+        in.u = du;
+        in.n = n;
+        ucbmlp::FeatureArgs fa = feature_args(m, in, 0, rows, false);
+        fa.Xt = m.Xt;
+        fa.y = dy;
+        fa.yb = m.yb;
+        if (!features(m, fa, st, err) || !forward(m, rows, true, st, err) || !backward(m, rows, (int)n, st, err) ||
+            !check_kernel_error(m, st, err) ||
+            !cu_ok(cudaMemcpy(grad, m.g, m.n_params * sizeof(float), cudaMemcpyDeviceToHost), err, "read grad") ||
+            !cu_ok(cudaMemcpy(loss, m.loss, sizeof(float), cudaMemcpyDeviceToHost), err, "read loss"))
+            rc = UCB_E_CUDA;
+    }
+    if (du) cudaFree(du);
+    if (dy) cudaFree(dy);
+    if (rc != UCB_OK) h->e->last_error = err;
+    return rc;
+}
+
+int ucb_mlp_fit(ucb_mlp* h, const float* d_u, const float* d_y, long long n, void* stream, float* loss_out) {
+    if (!h || !d_u || !d_y || n <= 0) return UCB_E_INVALID;
+    cudaSetDevice(h->e->device);
+    std::string err;
+    MlpInputs in;
+    in.u = d_u;
+    in.n = n;
+    if (!mlp_fit(h->m, in, d_y, stream ? (cudaStream_t)stream : h->e->stream, loss_out, err)) {
+        h->e->last_error = err;
+        return UCB_E_CUDA;
+    }
+    return UCB_OK;
+}
+
+int ucb_mlp_predict(ucb_mlp* h, const float* d_u, long long n, float* d_mean, float* d_std, void* stream) {
+    if (!h || !d_u || !d_mean || !d_std || n < 0) return UCB_E_INVALID;
+    cudaSetDevice(h->e->device);
+    std::string err;
+    MlpInputs in;
+    in.u = d_u;
+    in.n = n;
+    cudaStream_t st = stream ? (cudaStream_t)stream : h->e->stream;
+    if (!mlp_predict(h->m, in, d_mean, d_std, st, err) || !check_kernel_error(*h->m, st, err)) {
+        h->e->last_error = err;
+        return UCB_E_CUDA;
+    }
+    return UCB_OK;
+}
+
+}  // extern "C"

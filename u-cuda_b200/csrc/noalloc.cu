@@ -16,14 +16,6 @@
 
 #include "engine_internal.h"
 
-namespace ucb {
-int lle2d_plan_and_find(ucb_engine* e, const ucb_lle2d_request& q, bool load_if_missing, std::string& err,
-                        void** plan_out, void** launch_out);
-int lle2d_enqueue_with_scratch(ucb_engine* e, const ucb_lle2d_request& q, void* plan, void* launch, double* d_values,
-                               int32_t* d_flags, cudaStream_t stream, char* scratch, std::string& err);
-void lle2d_release(void* plan, void* launch);
-}  // namespace ucb
-
 namespace {
 
 // Layout used by the LLE kernel launch: [0, 8) work counter, [8, 16) step counter,

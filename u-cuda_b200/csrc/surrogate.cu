@@ -1,0 +1,389 @@
+// Surrogate-refined LLE map (no reference counterpart): plain-method samples -> BF16 MLP
+// trained on this GPU -> predicted map -> re-integration of the cells the network cannot
+// vouch for. The integrations are the LLE-2D kernel of ucb_engine.cpp run over cell lists;
+// the network is mlp.cu.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "engine_internal.h"
+#include "mlp.h"
+
+namespace ucbsur {
+
+__device__ __forceinline__ unsigned long long mix64(unsigned long long z) {
+    z += 0x9E3779B97F4A7C15ULL;
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ULL;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBULL;
+    return z ^ (z >> 31);
+}
+
+// One cell drawn uniformly inside each block of a tp x tp partition of the n x n grid
+// (kernel order: cell = iy * n + ix).
+__global__ void sample_cells_kernel(int n, int tp, unsigned long long seed, long long* cells) {
+    const long long s = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= (long long)tp * tp) return;
+    const int si = (int)(s % tp), sj = (int)(s / tp);
+    const long long x0 = (long long)si * n / tp, x1 = (long long)(si + 1) * n / tp;
+    const long long y0 = (long long)sj * n / tp, y1 = (long long)(sj + 1) * n / tp;
+    const unsigned long long h = mix64(seed ^ mix64((unsigned long long)s));
+    const long long ix = x0 + (long long)((h & 0xffffffffULL) % (unsigned long long)(x1 - x0));
+    const long long iy = y0 + (long long)((h >> 32) % (unsigned long long)(y1 - y0));
+    cells[s] = iy * n + ix;
+}
+
+__device__ __forceinline__ long long map_pos(long long cell, int n, int swap_xy) {
+    if (!swap_xy) return cell;
+    return (cell % n) * n + cell / n;
+}
+
+// Sample values into the map; mask marks the sample cells.
+__global__ void scatter_samples_kernel(const long long* cells, long long ns, const double* sv, const int* sf, int n,
+                                       int swap_xy, unsigned char* mask, double* values, int* flags) {
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= ns) return;
+    const long long c = cells[i];
+    mask[c] = 1;
+    const long long o = map_pos(c, n, swap_xy);
+    values[o] = sv[i];
+    flags[o] = sf[i];
+}
+
+__device__ __forceinline__ int regime(float v, float band) { return v > band ? 1 : (v < -band ? -1 : 0); }
+
+// Per non-sample cell: re-integrate (append to list) when the prediction is uncertain
+// (std above the calibrated threshold), near zero, or on a regime boundary (a 4-neighbour
+// in another class of {lambda < -band, |lambda| <= band, lambda > band}, or differing by
+// more than jump); band <= 0 / jump <= 0 switch those rules off. Otherwise the cell takes
+// the predicted mean with flag 2.
+__global__ void select_kernel(const float* mean, const float* sd, const unsigned char* mask, int n, int swap_xy,
+                              float sigma_max, float band, float jump, long long* list, unsigned long long* count,
+                              double* values, int* flags) {
+    const long long total = (long long)n * n;
+    const long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    bool refine = false;
+    bool active = c < total && !mask[c];
+    if (active) {
+        const float m = mean[c];
+        refine = !(sd[c] <= sigma_max) || (band > 0.f && fabsf(m) < band) || !isfinite(m);
+        if (!refine && (band > 0.f || jump > 0.f)) {
+            const int ix = (int)(c % n), iy = (int)(c / n);
+            const int rc = regime(m, band);
+            const long long nb[4] = {ix > 0 ? c - 1 : -1, ix + 1 < n ? c + 1 : -1, iy > 0 ? c - n : -1,
+                                     iy + 1 < n ? c + n : -1};
+#pragma unroll
+            for (int k = 0; k < 4; ++k) {
+                if (nb[k] < 0) continue;
+                const float v = mean[nb[k]];
+                if ((band > 0.f && regime(v, band) != rc) || (jump > 0.f && fabsf(v - m) > jump)) refine = true;
+            }
+        }
+        if (!refine) {
+            const long long o = map_pos(c, n, swap_xy);
+            values[o] = (double)m;
+            flags[o] = 2;
+        }
+    }
+    // warp-aggregated append
+    const unsigned ballot = __ballot_sync(0xffffffffu, active && refine);
+    if (ballot) {
+        const int lane = threadIdx.x & 31;
+        const int leader = __ffs(ballot) - 1;
+        unsigned long long base = 0;
+        if (lane == leader) base = atomicAdd(count, (unsigned long long)__popc(ballot));
+        base = __shfl_sync(0xffffffffu, base, leader);
+        if (active && refine) list[base + __popc(ballot & ((1u << lane) - 1u))] = c;
+    }
+}
+
+__global__ void gather_kernel(const float* mean, const float* sd, const long long* cells, long long n, float* gm,
+                              float* gs) {
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    gm[i] = mean[cells[i]];
+    gs[i] = sd[cells[i]];
+}
+
+__global__ void count_flag_kernel(const int* flags, long long total, int value, unsigned long long* count) {
+    unsigned long long local = 0;
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < total;
+         i += (long long)gridDim.x * blockDim.x)
+        local += flags[i] == value;
+    for (int o = 16; o > 0; o >>= 1) local += __shfl_down_sync(0xffffffffu, local, o);
+    if ((threadIdx.x & 31) == 0 && local) atomicAdd(count, local);
+}
+
+}  // namespace ucbsur
+
+namespace ucb {
+namespace {
+
+void set_err(char* dst, const std::string& msg) { std::snprintf(dst, 1024, "%s", msg.c_str()); }
+
+struct DevFree {
+    cudaStream_t st;
+    std::vector<void*> ptrs;
+    ~DevFree() {
+        for (void* p : ptrs) cudaFreeAsync(p, st);
+        cudaStreamSynchronize(st);
+    }
+    template <class T>
+    T* alloc(size_t count, std::string& err, const char* what) {
+        void* p = nullptr;
+        const cudaError_t ce = cudaMallocAsync(&p, std::max<size_t>(count, 1) * sizeof(T), st);
+        if (ce != cudaSuccess) {
+            err = std::string("cudaMallocAsync(") + what + "): " + cudaGetErrorString(ce);
+            return nullptr;
+        }
+        ptrs.push_back(p);
+        return static_cast<T*>(p);
+    }
+};
+
+struct LaunchHandle {
+    void* plan = nullptr;
+    void* launch = nullptr;
+    ~LaunchHandle() {
+        if (plan) lle2d_release(plan, launch);
+    }
+};
+
+}  // namespace
+}  // namespace ucb
+
+using namespace ucb;
+
+extern "C" {
+
+void ucb_default_surrogate_request(ucb_surrogate_request* r) {
+    std::memset(r, 0, sizeof *r);
+    r->map.opt.precision = UCB_PREC_F32;
+    r->map.opt.mode = UCB_MODE_NATIVE;
+    r->train_pts = 256;
+    r->sample_precision = UCB_PREC_F64;
+    r->refine_precision = UCB_PREC_F32;
+    r->tol = 2e-3;
+    r->coverage = 0.995;
+    r->sigma_max = 0.0;
+    r->lle_band = 0.05;
+    r->jump = 0.0;
+    ucb_mlp_default_config(&r->mlp);
+}
+
+int ucb_run_lle2d_surrogate(ucb_engine* e, const ucb_surrogate_request* rq, double* d_values, int32_t* d_flags,
+                            void* stream, ucb_surrogate_result* res) {
+    if (!e || !rq || !res) return UCB_E_INVALID;
+    std::memset(res, 0, sizeof *res);
+    const auto t_start = std::chrono::steady_clock::now();
+    const ucb_surrogate_request& r = *rq;
+    const int n = r.map.n_pts;
+    auto fail = [&](int code, const std::string& msg) {
+        e->last_error = msg;
+        set_err(res->error, msg);
+        res->ok = 0;
+        return code;
+    };
+    if (!d_values || !d_flags) return fail(UCB_E_INVALID, "output buffers are NULL");
+    if (n < 2) return fail(UCB_E_INVALID, "surrogate map needs n_pts >= 2");
+    const int tp = std::min(r.train_pts > 0 ? r.train_pts : 256, n);
+    auto prec_ok = [](int p) { return p == UCB_PREC_F64 || p == UCB_PREC_F32; };
+    if (!prec_ok(r.sample_precision) || !prec_ok(r.refine_precision))
+        return fail(UCB_E_INVALID, "sample_precision / refine_precision must be UCB_PREC_F64 or UCB_PREC_F32");
+    if (!(r.sigma_max >= 0) || !(r.lle_band >= 0) || !(r.jump >= 0) || !(r.tol > 0) ||
+        !(r.coverage > 0 && r.coverage <= 1))
+        return fail(UCB_E_INVALID, "need tol > 0, 0 < coverage <= 1, sigma_max / lle_band / jump >= 0");
+    std::string err;
+    if (!ensure_init(e, err)) return fail(UCB_E_NOGPU, err);
+    cudaStream_t st = stream ? (cudaStream_t)stream : e->stream;
+
+    ucb_lle2d_request qs = r.map, qr = r.map;
+    qs.opt.precision = r.sample_precision;
+    qr.opt.precision = r.refine_precision;
+    qs.csv_output_path = qr.csv_output_path = nullptr;
+    LaunchHandle hs, hr;
+    int rc = lle2d_plan_and_find(e, qs, true, err, &hs.plan, &hs.launch);
+    if (rc != UCB_OK) return fail(rc, err);
+    rc = lle2d_plan_and_find(e, qr, true, err, &hr.plan, &hr.launch);
+    if (rc != UCB_OK) return fail(rc, err);
+    SweepMap map;
+    int n_blocks = 0, skip = 0;
+    long long nt = 0;
+    if (!plan_sweep2d(r.map, map, n_blocks, skip, nt, err)) return fail(UCB_E_INVALID, err);
+
+    const long long total = (long long)n * n;
+    const long long ns = (long long)tp * tp;
+    cudaEvent_t ev[6];
+    for (auto& x : ev) cudaEventCreate(&x);
+    struct EvFree {
+        cudaEvent_t* ev;
+        ~EvFree() {
+            for (int i = 0; i < 6; ++i) cudaEventDestroy(ev[i]);
+        }
+    } evf{ev};
+    DevFree mem{st, {}};
+    long long* d_cells = mem.alloc<long long>(ns, err, "sample cells");
+    double* d_sv = mem.alloc<double>(ns, err, "sample values");
+    int* d_sf = mem.alloc<int>(ns, err, "sample flags");
+    unsigned char* d_mask = mem.alloc<unsigned char>(total, err, "mask");
+    float* d_mean = mem.alloc<float>(total, err, "mean");
+    float* d_sd = mem.alloc<float>(total, err, "std");
+    long long* d_list = mem.alloc<long long>(total, err, "refine list");
+    unsigned long long* d_count = mem.alloc<unsigned long long>(2, err, "counters");
+    if (!d_cells || !d_sv || !d_sf || !d_mask || !d_mean || !d_sd || !d_list || !d_count) return fail(UCB_E_CUDA, err);
+    cudaMemsetAsync(d_mask, 0, total, st);
+    cudaMemsetAsync(d_count, 0, 2 * sizeof(unsigned long long), st);
+
+    // 1. samples
+    cudaEventRecord(ev[0], st);
+    ucbsur::sample_cells_kernel<<<(unsigned)((ns + 255) / 256), 256, 0, st>>>(n, tp, r.mlp.seed ^ 0xC0FFEEULL,
+                                                                             d_cells);
+    e->launches += 1;
+    rc = lle2d_enqueue_cells(e, qs, hs.plan, hs.launch, d_cells, ns, true, d_sv, d_sf, st, err);
+    if (rc != UCB_OK) return fail(rc, err);
+    cudaEventRecord(ev[1], st);
+    std::vector<long long> hc(ns);
+    std::vector<double> hv(ns);
+    std::vector<int> hf(ns);
+    if (cudaMemcpyAsync(hc.data(), d_cells, ns * 8, cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+        cudaMemcpyAsync(hv.data(), d_sv, ns * 8, cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+        cudaMemcpyAsync(hf.data(), d_sf, ns * 4, cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+        cudaStreamSynchronize(st) != cudaSuccess)
+        return fail(UCB_E_CUDA, std::string("samples: ") + cudaGetErrorString(cudaGetLastError()));
+    // One sample in eight (by a hash of its block) is held out for calibration.
+    std::vector<float> hu, hy;
+    std::vector<long long> cal_cells;
+    std::vector<double> cal_y;
+    hu.reserve(2 * ns);
+    hy.reserve(ns);
+    const float inv = 1.0f / (float)(n - 1);
+    for (long long i = 0; i < ns; ++i) {
+        if (hf[i] != 1 || !std::isfinite(hv[i])) continue;
+        unsigned long long z = (unsigned long long)i * 0x9E3779B97F4A7C15ULL + r.mlp.seed;
+        z ^= z >> 31;
+        if (z % 8 == 0) {
+            cal_cells.push_back(hc[i]);
+            cal_y.push_back(hv[i]);
+            continue;
+        }
+        hu.push_back((float)(hc[i] % n) * inv);
+        hu.push_back((float)(hc[i] / n) * inv);
+        hy.push_back((float)hv[i]);
+    }
+    const long long n_train = (long long)hy.size();
+    const long long n_cal = (long long)cal_y.size();
+    res->n_samples = ns;
+    res->n_calib = n_cal;
+
+    // 2. training
+    std::unique_ptr<Mlp, void (*)(Mlp*)> net(nullptr, mlp_destroy);
+    float* d_u = mem.alloc<float>(std::max<long long>(2 * n_train, 1), err, "train u");
+    float* d_y = mem.alloc<float>(std::max<long long>(n_train, 1), err, "train y");
+    if (!d_u || !d_y) return fail(UCB_E_CUDA, err);
+    if (n_train > 0) {
+        cudaMemcpyAsync(d_u, hu.data(), hu.size() * 4, cudaMemcpyHostToDevice, st);
+        cudaMemcpyAsync(d_y, hy.data(), hy.size() * 4, cudaMemcpyHostToDevice, st);
+        net.reset(mlp_create(e, r.mlp, err));
+        if (!net) return fail(UCB_E_INVALID, err);
+        MlpInputs tin;
+        tin.u = d_u;
+        tin.n = n_train;
+        if (!mlp_fit(net.get(), tin, d_y, st, &res->final_loss, err)) return fail(UCB_E_CUDA, err);
+    }
+    cudaEventRecord(ev[2], st);
+
+    // 3. prediction over the grid (no training rows: everything is re-integrated)
+    if (n_train > 0) {
+        MlpInputs pin;
+        pin.n = total;
+        pin.grid_n = n;
+        if (!mlp_predict(net.get(), pin, d_mean, d_sd, st, err)) return fail(UCB_E_CUDA, err);
+    } else {
+        cudaMemsetAsync(d_mean, 0, total * 4, st);
+        cudaMemsetAsync(d_sd, 0, total * 4, st);
+    }
+    // calibration: the largest std threshold under which >= coverage of the held-out
+    // samples lie within tol of their integrated value
+    double thr = -1.0, within = 0.0;
+    if (n_train > 0 && n_cal > 0) {
+        long long* d_cc = mem.alloc<long long>(n_cal, err, "calibration cells");
+        float* d_gm = mem.alloc<float>(n_cal, err, "calibration mean");
+        float* d_gs = mem.alloc<float>(n_cal, err, "calibration std");
+        if (!d_cc || !d_gm || !d_gs) return fail(UCB_E_CUDA, err);
+        std::vector<float> gm(n_cal), gs(n_cal);
+        cudaMemcpyAsync(d_cc, cal_cells.data(), n_cal * 8, cudaMemcpyHostToDevice, st);
+        ucbsur::gather_kernel<<<(unsigned)((n_cal + 255) / 256), 256, 0, st>>>(d_mean, d_sd, d_cc, n_cal, d_gm, d_gs);
+        e->launches += 1;
+        if (cudaMemcpyAsync(gm.data(), d_gm, n_cal * 4, cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+            cudaMemcpyAsync(gs.data(), d_gs, n_cal * 4, cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+            cudaStreamSynchronize(st) != cudaSuccess)
+            return fail(UCB_E_CUDA, std::string("calibration: ") + cudaGetErrorString(cudaGetLastError()));
+        std::vector<long long> order(n_cal);
+        for (long long i = 0; i < n_cal; ++i) order[i] = i;
+        std::sort(order.begin(), order.end(), [&](long long a, long long b) { return gs[a] < gs[b]; });
+        long long good = 0;
+        const long long min_count = std::min<long long>(n_cal, 32);
+        for (long long k = 0; k < n_cal; ++k) {
+            const long long i = order[k];
+            good += std::fabs((double)gm[i] - cal_y[i]) <= r.tol;
+            const long long cnt = k + 1;
+            if (cnt >= min_count && (double)good >= r.coverage * (double)cnt &&
+                (k + 1 == n_cal || gs[order[k + 1]] > gs[i])) {
+                thr = gs[i];
+                within = (double)good / (double)cnt;
+            }
+        }
+        if (r.sigma_max > 0 && thr > r.sigma_max) thr = r.sigma_max;
+    }
+    res->sigma_threshold = thr;
+    res->calib_within_tol = within;
+    cudaEventRecord(ev[3], st);
+
+    // 4. selection
+    ucbsur::scatter_samples_kernel<<<(unsigned)((ns + 255) / 256), 256, 0, st>>>(
+        d_cells, ns, d_sv, d_sf, n, map.swap_xy ? 1 : 0, d_mask, d_values, d_flags);
+    const float sigma = (float)thr;  // < 0 (no network or no calibrated threshold): refine all
+    ucbsur::select_kernel<<<(unsigned)((total + 255) / 256), 256, 0, st>>>(
+        d_mean, d_sd, d_mask, n, map.swap_xy ? 1 : 0, sigma, (float)r.lle_band, (float)r.jump, d_list, d_count,
+        d_values, d_flags);
+    e->launches += 2;
+    unsigned long long n_ref = 0;
+    if (cudaMemcpyAsync(&n_ref, d_count, 8, cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+        cudaStreamSynchronize(st) != cudaSuccess)
+        return fail(UCB_E_CUDA, std::string("select: ") + cudaGetErrorString(cudaGetLastError()));
+    cudaEventRecord(ev[4], st);
+
+    // 5. re-integration straight into the map
+    rc = lle2d_enqueue_cells(e, qr, hr.plan, hr.launch, d_list, (long long)n_ref, false, d_values, d_flags, st, err);
+    if (rc != UCB_OK) return fail(rc, err);
+    cudaEventRecord(ev[5], st);
+    ucbsur::count_flag_kernel<<<e->sm_count * 4, 256, 0, st>>>(d_flags, total, -1, d_count + 1);
+    e->launches += 1;
+    unsigned long long n_div = 0;
+    if (cudaMemcpyAsync(&n_div, d_count + 1, 8, cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+        cudaStreamSynchronize(st) != cudaSuccess)
+        return fail(UCB_E_CUDA, std::string("refine: ") + cudaGetErrorString(cudaGetLastError()));
+    float ms[5] = {0, 0, 0, 0, 0};
+    for (int i = 0; i < 5; ++i) cudaEventElapsedTime(&ms[i], ev[i], ev[i + 1]);
+    res->sample_ms = ms[0];
+    res->train_ms = ms[1];
+    res->predict_ms = ms[2];
+    res->select_ms = ms[3];
+    res->refine_ms = ms[4];
+    res->n_refined = (long long)n_ref;
+    res->n_predicted = total - ns - (long long)n_ref;  // sample cells are integrated
+    res->n_diverged = (long long)n_div;
+    res->n_pts = n;
+    res->total_ms =
+        std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t_start).count();
+    res->ok = 1;
+    return UCB_OK;
+}
+
+}  // extern "C"

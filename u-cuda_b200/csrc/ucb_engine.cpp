@@ -306,7 +306,10 @@ bool plan_lle2d(const ucb_lle2d_request& q, LlePlan& p, std::string& err) {
     p.amountOfPointsInBlock = (int)(q.t_max / q.NT);
     p.amountOfPointsForSkip = (int)(q.transient_time / q.h);
     if (p.amountOfPointsInBlock <= 0) { err = "computed amountOfPointsInBlock <= 0 (t_max / NT too small)"; return false; }
-    if (q.opt.precision == UCB_PREC_F64)
+    // (size_t)(NT / h) is evaluated in numb inside the reference kernel (cudaLibrary.cu:2547);
+    // in float it truncates 0.02f / 0.002f to 9. The exact form keeps that; the native FP32
+    // form counts in double so that its blocks span the same time as the FP64 plain form.
+    if (q.opt.precision == UCB_PREC_F64 || q.opt.mode == UCB_MODE_NATIVE)
         p.nt_steps = (long long)(q.NT / q.h);
     else
         p.nt_steps = (long long)((float)q.NT / (float)q.h);
@@ -330,7 +333,7 @@ struct LleParamsT {
 template <class T>
 std::vector<char> pack_lle_params(const LleParamsT<T>& head, const double* ic, int nx, const double* vals, int nv,
                                   const void* ax0, const void* ax1, double* out_v, int32_t* out_f, void* counter,
-                                  void* steps, const void* cell_list = nullptr) {
+                                  void* steps, const void* cell_list = nullptr, int list_compact = 0) {
     std::vector<char> buf;
     auto put = [&](const void* p, size_t n, size_t align) {
         while (buf.size() % align) buf.push_back(0);
@@ -357,6 +360,7 @@ std::vector<char> pack_lle_params(const LleParamsT<T>& head, const double* ic, i
     put(&counter, 8, 8);
     put(&steps, 8, 8);
     put(&cell_list, 8, 8);
+    put(&list_compact, 4, 4);
     while (buf.size() % 8) buf.push_back(0);
     return buf;
 }
@@ -403,7 +407,8 @@ bool prepare_lle(ucb_engine* e, const ucb_lle2d_request& q, const LlePlan& plan,
 // [256..] axis tables.
 int enqueue_lle_fn(ucb_engine* e, const ucb_lle2d_request& q, const LlePlan& plan, const LleLaunch& L,
                    double* d_values, int32_t* d_flags, cudaStream_t stream, std::string& err, long long skip_override,
-                   bool persistent, char* scratch, const long long* d_cell_list = nullptr, long long n_list = 0) {
+                   bool persistent, char* scratch, const long long* d_cell_list = nullptr, long long n_list = 0,
+                   bool list_compact = false) {
     const int n = q.n_pts;
     const int prec = q.opt.precision;
     const size_t esz = prec == UCB_PREC_F64 ? 8 : 4;
@@ -434,14 +439,16 @@ int enqueue_lle_fn(ucb_engine* e, const ucb_lle2d_request& q, const LlePlan& pla
                               skip_override >= 0 ? skip_override : plan.amountOfPointsForSkip, plan.nt_steps, q.h,
                               q.NT, q.t_max, q.eps, q.max_value, q.transient_time};
         params = pack_lle_params<double>(hd, q.initial_conditions, q.amount_of_x, q.base_values, q.n_values,
-                                         ws + off_ax0, ws + off_ax1, d_values, d_flags, ws, ws + 8, d_cell_list);
+                                         ws + off_ax0, ws + off_ax1, d_values, d_flags, ws, ws + 8, d_cell_list,
+                                         list_compact ? 1 : 0);
     } else {
         LleParamsT<float> hd{total, 0, n, plan.map.swap_xy ? 1 : 0, plan.amountOfPointsInBlock, 0,
                              skip_override >= 0 ? skip_override : plan.amountOfPointsForSkip, plan.nt_steps,
                              (float)q.h, (float)q.NT, (float)q.t_max,
                              (float)q.eps, (float)q.max_value, (float)q.transient_time};
         params = pack_lle_params<float>(hd, q.initial_conditions, q.amount_of_x, q.base_values, q.n_values,
-                                        ws + off_ax0, ws + off_ax1, d_values, d_flags, ws, ws + 8, d_cell_list);
+                                        ws + off_ax0, ws + off_ax1, d_values, d_flags, ws, ws + 8, d_cell_list,
+                                         list_compact ? 1 : 0);
     }
     const int block = 128;
     const int grid = persistent ? persistent_grid(e, L.fn, block, total) : (int)((total + block - 1) / block);
@@ -503,6 +510,16 @@ int lle2d_enqueue_with_scratch(ucb_engine* e, const ucb_lle2d_request& q, void* 
     return enqueue_lle_fn(e, q, *static_cast<LlePlan*>(plan), *static_cast<LleLaunch*>(launch), d_values, d_flags,
                           stream, err, -1, true, scratch);
 }
+
+int lle2d_enqueue_cells(ucb_engine* e, const ucb_lle2d_request& q, void* plan, void* launch, const long long* d_cells,
+                        long long n_cells, bool compact, double* d_values, int32_t* d_flags, cudaStream_t stream,
+                        std::string& err) {
+    if (n_cells <= 0) return UCB_OK;
+    return enqueue_lle_fn(e, q, *static_cast<LlePlan*>(plan), *static_cast<LleLaunch*>(launch), d_values, d_flags,
+                          stream, err, -1, true, nullptr, d_cells, n_cells, compact);
+}
+
+long long lle2d_flops_per_step(void* launch) { return static_cast<LleLaunch*>(launch)->sys.flops_step; }
 
 void lle2d_release(void* plan, void* launch) {
     delete static_cast<LlePlan*>(plan);
@@ -707,6 +724,29 @@ int ucb_lle2d_device(ucb_engine* e, const ucb_lle2d_request* req, double* d_valu
     if (!prepare_lle(e, *req, plan, L, err)) return fail(e, res->error, &res->ok, UCB_E_COMPILE, err);
     int rc = enqueue_lle(e, *req, plan, L, d_values, d_flags, (cudaStream_t)stream, err);
     if (rc != UCB_OK) return fail(e, res->error, &res->ok, rc, err);
+    res->n_pts = req->n_pts;
+    res->ok = 1;
+    return UCB_OK;
+}
+
+int ucb_lle2d_cells(ucb_engine* e, const ucb_lle2d_request* req, const long long* d_cells, long long n_cells,
+                    double* d_values, int32_t* d_flags, void* stream, ucb_lle2d_result* res) {
+    if (!e || !req || !res) return UCB_E_INVALID;
+    res->ok = 0;
+    res->error[0] = 0;
+    LlePlan plan;
+    std::string err;
+    if (!plan_lle2d(*req, plan, err)) return fail(e, res->error, &res->ok, UCB_E_INVALID, err);
+    if (n_cells < 0 || (n_cells > 0 && (!d_cells || !d_values || !d_flags)))
+        return fail(e, res->error, &res->ok, UCB_E_INVALID, "cell list or output buffers missing");
+    if (!ensure_init(e, err)) return fail(e, res->error, &res->ok, UCB_E_NOGPU, err);
+    LleLaunch L;
+    if (!prepare_lle(e, *req, plan, L, err)) return fail(e, res->error, &res->ok, UCB_E_COMPILE, err);
+    if (n_cells > 0) {
+        const int rc = enqueue_lle_fn(e, *req, plan, L, d_values, d_flags, (cudaStream_t)stream, err, -1, true,
+                                      nullptr, d_cells, n_cells, true);
+        if (rc != UCB_OK) return fail(e, res->error, &res->ok, rc, err);
+    }
     res->n_pts = req->n_pts;
     res->ok = 1;
     return UCB_OK;

@@ -125,6 +125,27 @@ class BasinsResult(C.Structure):
     ]
 
 
+class MlpConfig(C.Structure):
+    _fields_ = [("fourier", C.c_int32), ("hidden", C.c_int32), ("layers", C.c_int32), ("fourier_scale", C.c_float),
+                ("seed", C.c_uint64), ("batch", C.c_int32), ("train_steps", C.c_int32), ("lr", C.c_float),
+                ("lr_final", C.c_float), ("beta_nll", C.c_float), ("reserved", C.c_int32 * 5)]
+
+
+class SurrogateRequest(C.Structure):
+    _fields_ = [("map", Lle2dRequest), ("train_pts", C.c_int32), ("sample_precision", C.c_int32),
+                ("refine_precision", C.c_int32), ("pad0", C.c_int32), ("tol", C.c_double), ("coverage", C.c_double),
+                ("sigma_max", C.c_double), ("lle_band", C.c_double), ("jump", C.c_double), ("mlp", MlpConfig)]
+
+
+class SurrogateResult(C.Structure):
+    _fields_ = [("ok", C.c_int32), ("n_pts", C.c_int32), ("n_samples", C.c_longlong), ("n_calib", C.c_longlong),
+                ("n_refined", C.c_longlong), ("n_predicted", C.c_longlong), ("n_diverged", C.c_longlong),
+                ("sigma_threshold", C.c_double), ("calib_within_tol", C.c_double), ("sample_ms", C.c_double),
+                ("train_ms", C.c_double), ("predict_ms", C.c_double), ("select_ms", C.c_double),
+                ("refine_ms", C.c_double), ("total_ms", C.c_double), ("final_loss", C.c_float),
+                ("pad0", C.c_float), ("error", C.c_char * 1024)]
+
+
 LS_FIXED, LS_DP5 = 0, 1
 _lib = None
 
@@ -182,6 +203,31 @@ def load():
                               C.c_char_p, C.c_int, C.c_char_p, C.c_int]
     L.ucb_precompile_lle2d.restype = C.c_int
     L.ucb_precompile_lle2d.argtypes = [C.POINTER(Lle2dRequest), C.c_char_p, C.c_int]
+    L.ucb_lle2d_cells.restype = C.c_int
+    L.ucb_lle2d_cells.argtypes = [C.c_void_p, C.POINTER(Lle2dRequest), C.c_void_p, C.c_longlong, C.c_void_p,
+                                  C.c_void_p, C.c_void_p, C.POINTER(Lle2dResult)]
+    L.ucb_mlp_default_config.argtypes = [C.POINTER(MlpConfig)]
+    L.ucb_mlp_create.restype = C.c_void_p
+    L.ucb_mlp_create.argtypes = [C.c_void_p, C.POINTER(MlpConfig)]
+    L.ucb_mlp_destroy.argtypes = [C.c_void_p]
+    L.ucb_mlp_param_count.restype = C.c_longlong
+    L.ucb_mlp_param_count.argtypes = [C.c_void_p]
+    for fn in ("ucb_mlp_get_params", "ucb_mlp_set_params", "ucb_mlp_get_fourier"):
+        getattr(L, fn).restype = C.c_int
+        getattr(L, fn).argtypes = [C.c_void_p, C.c_void_p, C.c_longlong]
+    L.ucb_mlp_set_target_scale.restype = C.c_int
+    L.ucb_mlp_set_target_scale.argtypes = [C.c_void_p, C.c_float, C.c_float]
+    L.ucb_mlp_loss_grad.restype = C.c_int
+    L.ucb_mlp_loss_grad.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_longlong, C.POINTER(C.c_float),
+                                    C.c_void_p]
+    L.ucb_mlp_fit.restype = C.c_int
+    L.ucb_mlp_fit.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_longlong, C.c_void_p, C.POINTER(C.c_float)]
+    L.ucb_mlp_predict.restype = C.c_int
+    L.ucb_mlp_predict.argtypes = [C.c_void_p, C.c_void_p, C.c_longlong, C.c_void_p, C.c_void_p, C.c_void_p]
+    L.ucb_default_surrogate_request.argtypes = [C.POINTER(SurrogateRequest)]
+    L.ucb_run_lle2d_surrogate.restype = C.c_int
+    L.ucb_run_lle2d_surrogate.argtypes = [C.c_void_p, C.POINTER(SurrogateRequest), C.c_void_p, C.c_void_p,
+                                          C.c_void_p, C.POINTER(SurrogateResult)]
     _lib = L
     return L
 
@@ -405,6 +451,120 @@ class Engine:
         if rc != UCB_OK:
             raise UcbError(rc, res.error.decode())
         return res
+
+
+def mlp_config(**kw) -> MlpConfig:
+    c = MlpConfig()
+    load().ucb_mlp_default_config(C.byref(c))
+    for k, v in kw.items():
+        setattr(c, k, v)
+    return c
+
+
+class Mlp:
+    """The BF16 tensor-core MLP of the surrogate (ucb_mlp_* entry points)."""
+
+    def __init__(self, engine: Engine, cfg: MlpConfig | None = None, **kw):
+        self.engine = engine
+        self.lib = engine.lib
+        self.cfg = cfg if cfg is not None else mlp_config(**kw)
+        self.h = self.lib.ucb_mlp_create(engine.h, C.byref(self.cfg))
+        if not self.h:
+            raise UcbError(UCB_E_INVALID, engine.last_error())
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.ucb_mlp_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _check(self, rc):
+        if rc != UCB_OK:
+            raise UcbError(rc, self.engine.last_error())
+
+    @property
+    def n_params(self) -> int:
+        return int(self.lib.ucb_mlp_param_count(self.h))
+
+    def get_params(self) -> np.ndarray:
+        out = np.empty(self.n_params, dtype=np.float32)
+        self._check(self.lib.ucb_mlp_get_params(self.h, out.ctypes.data_as(C.c_void_p), out.size))
+        return out
+
+    def set_params(self, p):
+        p = np.ascontiguousarray(p, dtype=np.float32)
+        self._check(self.lib.ucb_mlp_set_params(self.h, p.ctypes.data_as(C.c_void_p), p.size))
+
+    def fourier(self) -> np.ndarray:
+        out = np.empty((self.cfg.fourier, 2), dtype=np.float32)
+        self._check(self.lib.ucb_mlp_get_fourier(self.h, out.ctypes.data_as(C.c_void_p), out.size))
+        return out
+
+    def set_target_scale(self, mean: float, std: float):
+        self._check(self.lib.ucb_mlp_set_target_scale(self.h, mean, std))
+
+    def loss_grad(self, u, y):
+        u = np.ascontiguousarray(u, dtype=np.float32).reshape(-1, 2)
+        y = np.ascontiguousarray(y, dtype=np.float32).reshape(-1)
+        g = np.empty(self.n_params, dtype=np.float32)
+        loss = C.c_float(0)
+        self._check(self.lib.ucb_mlp_loss_grad(self.h, u.ctypes.data_as(C.c_void_p), y.ctypes.data_as(C.c_void_p),
+                                               len(y), C.byref(loss), g.ctypes.data_as(C.c_void_p)))
+        return float(loss.value), g
+
+    def fit(self, d_u_ptr: int, d_y_ptr: int, n: int, stream_ptr: int = 0) -> float:
+        loss = C.c_float(0)
+        self._check(self.lib.ucb_mlp_fit(self.h, C.c_void_p(d_u_ptr), C.c_void_p(d_y_ptr), n,
+                                         C.c_void_p(stream_ptr), C.byref(loss)))
+        return float(loss.value)
+
+    def predict(self, d_u_ptr: int, n: int, d_mean_ptr: int, d_std_ptr: int, stream_ptr: int = 0):
+        self._check(self.lib.ucb_mlp_predict(self.h, C.c_void_p(d_u_ptr), n, C.c_void_p(d_mean_ptr),
+                                             C.c_void_p(d_std_ptr), C.c_void_p(stream_ptr)))
+
+
+def surrogate_request(map_req: Lle2dRequest, **kw) -> SurrogateRequest:
+    """Surrogate-refined map request around an LLE-2D request (defaults from the library;
+    keyword `mlp` takes a dict of MlpConfig fields)."""
+    r = SurrogateRequest()
+    load().ucb_default_surrogate_request(C.byref(r))
+    r.map = map_req
+    r._keep = map_req._keep
+    mlp = kw.pop("mlp", None)
+    for k, v in kw.items():
+        setattr(r, k, v)
+    if mlp:
+        for k, v in mlp.items():
+            setattr(r.mlp, k, v)
+    return r
+
+
+def _engine_surrogate(self, req: SurrogateRequest, d_values_ptr: int, d_flags_ptr: int, stream_ptr: int = 0):
+    res = SurrogateResult()
+    rc = self.lib.ucb_run_lle2d_surrogate(self.h, C.byref(req), C.c_void_p(d_values_ptr), C.c_void_p(d_flags_ptr),
+                                          C.c_void_p(stream_ptr), C.byref(res))
+    if rc != UCB_OK:
+        raise UcbError(rc, res.error.decode())
+    return res
+
+
+def _engine_cells(self, req: Lle2dRequest, d_cells_ptr: int, n_cells: int, d_values_ptr: int, d_flags_ptr: int,
+                  stream_ptr: int = 0):
+    res = Lle2dResult()
+    rc = self.lib.ucb_lle2d_cells(self.h, C.byref(req), C.c_void_p(d_cells_ptr), n_cells, C.c_void_p(d_values_ptr),
+                                  C.c_void_p(d_flags_ptr), C.c_void_p(stream_ptr), C.byref(res))
+    if rc != UCB_OK:
+        raise UcbError(rc, res.error.decode())
+    return res
+
+
+Engine.run_lle2d_surrogate = _engine_surrogate
+Engine.lle2d_cells = _engine_cells
 
 
 def precompile_lle2d(req) -> str:
