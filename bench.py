@@ -157,14 +157,16 @@ def run_ours(args, rank, world, local):
         if name == "fp32":
             launches_timed = launches
         # work and FLOPs of one map, read back through the host entry once
-        _, flags, res = eng.run_lle2d(req)
+        vals, flags, res = eng.run_lle2d(req)
         results[name] = dict(ms=ms, wall_s=wall, steps=res.steps, flops=res.flops, kernel_ms=res.kernel_ms,
-                             valid_cells=int((flags == 1).sum()), launches=launches)
+                             valid_cells=int((flags == 1).sum()), launches=launches, values=vals.copy())
+    results["surrogate"] = run_surrogate(eng, c, results, args, dev)
     # end-to-end through the public C ABI with host buffers (H2D of the request, D2H of
     # values + flags inside the timed region), chosen form
     req = engine_request(ucb, c, **forms["fp32"])
-    hv = np.empty(cells, dtype=np.float64)
-    hf = np.empty(cells, dtype=np.int32)
+    # page-locked host buffers, as a caller streaming maps to the host would use
+    hv = torch.empty(cells, dtype=torch.float64, pin_memory=True).numpy()
+    hf = torch.empty(cells, dtype=torch.int32, pin_memory=True).numpy()
     e2e_ms = []
     e2e_kernel_ms = []
     for k in range(max(1, min(args.steps, 3))):
@@ -180,6 +182,215 @@ def run_ours(args, rank, world, local):
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         e2e = float(t.item())
     return results, clocks, launches_timed, e2e
+
+
+JUDGE_CELLS = 65536
+
+
+def judge_cells(total: int, seed: int = 0):
+    """The held-out subset the surrogate is judged on: 64k cells drawn without
+    replacement with a fixed seed."""
+    return np.sort(np.random.default_rng(seed).choice(total, size=min(JUDGE_CELLS, total), replace=False))
+
+
+def error_stats(v, ref, tol=2e-3):
+    d = np.abs(np.asarray(v, np.float64) - np.asarray(ref, np.float64))
+    return {"within_2e-3": float((d <= tol).mean()), "median_abs": float(np.median(d)),
+            "p99_abs": float(np.quantile(d, 0.99))}
+
+
+def surrogate_request(ucb, c, **kw):
+    from helpers import engine_request
+    return ucb.surrogate_request(engine_request(ucb, c, precision=ucb.PREC_F32, mode=ucb.MODE_NATIVE), **kw)
+
+
+def run_surrogate(eng, c, results, args, dev):
+    """Surrogate-refined form of the same map: plain FP64 samples on a 256 x 256 stratified
+    partition, BF16 MLP trained on this GPU, held-out calibration at |error| <= 2e-3 for
+    99.5% of predicted cells, everything else re-integrated in the FP32 form. Judged on 64k
+    random cells against the plain FP64 map."""
+    import torch
+    import ucb
+    n = c["n_pts"]
+    req = surrogate_request(ucb, c, train_pts=256, tol=2e-3, coverage=0.995, lle_band=0.05)
+    v = torch.empty(n * n, dtype=torch.float64, device=dev)
+    f = torch.empty(n * n, dtype=torch.int32, device=dev)
+    eng.run_lle2d_surrogate(req, v.data_ptr(), f.data_ptr(), 0)
+    torch.cuda.synchronize(dev)
+    runs = []
+    for _ in range(max(1, min(args.steps, 2))):
+        torch.cuda.synchronize(dev)
+        res = eng.run_lle2d_surrogate(req, v.data_ptr(), f.data_ptr(), 0)
+        torch.cuda.synchronize(dev)
+        runs.append(res.total_ms)
+    ms = float(np.mean(runs))
+    idx = judge_cells(n * n)
+    vals = v.cpu().numpy()[idx]
+    ref = results["plain_fp64"]["values"][idx]
+    return {"ms_per_map": ms, "cells_per_s": n * n / (ms * 1e-3),
+            "vs_plain_fp64": results["plain_fp64"]["ms"] / ms,
+            "predicted_fraction": res.n_predicted / (n * n), "refined_cells": res.n_refined,
+            "samples": res.n_samples, "sigma_threshold": res.sigma_threshold,
+            "calibration_within_tol": res.calib_within_tol,
+            "phases_ms": {"samples": res.sample_ms, "train": res.train_ms, "predict": res.predict_ms,
+                          "select": res.select_ms, "refine": res.refine_ms},
+            "judge_64k_vs_plain_fp64": error_stats(vals, ref),
+            "fp32_judge_64k_vs_plain_fp64": error_stats(results["fp32"]["values"][idx], ref),
+            "rule": "predict a cell only when its std is under the held-out-calibrated threshold "
+                    "(>= 99.5% of held-out samples within 2e-3) and |mean| >= 0.05 with no neighbour "
+                    "in another regime; everything else integrated"}
+
+
+def chen_case(n: int) -> dict:
+    """Chen LLE map: dx=a(y-x), dy=(c-a)x-xz+cy, dz=xy-bz, b=3, a in [30,40] x c in [20,30];
+    RK4 h=0.002, 20 time units of transient (1e4 steps), t_max = 200 (1e5 measured steps),
+    renormalised every 10 steps, x0=(1,1,1)."""
+    from helpers import rk4_body, CHEN
+    return dict(body=rk4_body(CHEN), nx=3, ic=(1.0, 1.0, 1.0), values=(0.0, 35.0, 3.0, 28.0), n_pts=n,
+                param_index=1, param_index_2=3, param_lo=30.0, param_hi=40.0, param_lo_2=20.0, param_hi_2=30.0,
+                h=0.002, transient_time=20.0, t_max=200.0, NT=0.02, eps=1e-4, max_value=1e6)
+
+
+def run_surrogate_chen(eng, dev, n: int, tol: float, coverage: float):
+    """Surrogate-refined Chen map at n x n, judged on 64k random cells integrated with the
+    plain FP64 method (whose rate there is the plain FP64 cells/s of the same kernel)."""
+    import torch
+    import ucb
+    from helpers import engine_request
+    req = surrogate_request(ucb, chen_case(n), train_pts=256, tol=tol, coverage=coverage, lle_band=0.05)
+    warm = surrogate_request(ucb, chen_case(512), train_pts=128, tol=tol, coverage=coverage, lle_band=0.05)
+    v = torch.empty(n * n, dtype=torch.float64, device=dev)
+    f = torch.empty(n * n, dtype=torch.int32, device=dev)
+    eng.run_lle2d_surrogate(warm, v.data_ptr(), f.data_ptr(), 0)
+    torch.cuda.synchronize(dev)
+    res = eng.run_lle2d_surrogate(req, v.data_ptr(), f.data_ptr(), 0)
+    torch.cuda.synchronize(dev)
+    idx = judge_cells(n * n)
+    d_idx = torch.from_numpy(idx).to(dev)
+    sur = v[d_idx].cpu().numpy()
+    out = {}
+    for name, prec in (("plain_fp64", ucb.PREC_F64), ("fp32", ucb.PREC_F32)):
+        jv = torch.empty(len(idx), dtype=torch.float64, device=dev)
+        jf = torch.empty(len(idx), dtype=torch.int32, device=dev)
+        r = engine_request(ucb, chen_case(n), precision=prec, mode=ucb.MODE_NATIVE)
+        eng.lle2d_cells(r, d_idx.data_ptr(), len(idx), jv.data_ptr(), jf.data_ptr(), 0)
+        torch.cuda.synchronize(dev)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        eng.lle2d_cells(r, d_idx.data_ptr(), len(idx), jv.data_ptr(), jf.data_ptr(), 0)
+        e1.record()
+        torch.cuda.synchronize(dev)
+        out[name] = (jv.cpu().numpy(), len(idx) / (e0.elapsed_time(e1) * 1e-3))
+    ref, plain_rate = out["plain_fp64"]
+    total = n * n
+    return {"workload": f"Chen LLE map {n}x{n} (a in [30,40] x c in [20,30], b=3), RK4 h=0.002, 1e4 transient "
+                        f"+ 1e5 measured steps", "tol": tol, "coverage": coverage,
+            "ms_per_map": res.total_ms, "cells_per_s": total / (res.total_ms * 1e-3),
+            "plain_fp64_cells_per_s": plain_rate, "fp32_cells_per_s": out["fp32"][1],
+            "vs_plain_fp64": (total / (res.total_ms * 1e-3)) / plain_rate,
+            "predicted_fraction": res.n_predicted / total, "refined_cells": res.n_refined,
+            "samples": res.n_samples, "sigma_threshold": res.sigma_threshold,
+            "calibration_within_tol": res.calib_within_tol,
+            "phases_ms": {"samples": res.sample_ms, "train": res.train_ms, "predict": res.predict_ms,
+                          "select": res.select_ms, "refine": res.refine_ms},
+            "judge_64k_vs_plain_fp64": error_stats(sur, ref),
+            "fp32_judge_64k_vs_plain_fp64": error_stats(out["fp32"][0], ref),
+            "plain_rate_basis": "plain FP64 kernel over the 64k judge cells (same kernel, random cells)"}
+
+
+def _timed(fn, reps=1):
+    """Wall time (ms) of the last of `reps` calls of fn (the first call compiles)."""
+    out = None
+    t = 0.0
+    for _ in range(reps):
+        t0 = time.perf_counter()
+        out = fn()
+        t = (time.perf_counter() - t0) * 1e3
+    return out, t
+
+
+def run_other_configs(eng):
+    """The other hot-path configurations at their full sizes (one run each after a
+    compiling warm-up), with parity summaries against the oracle on sampled cells."""
+    import ucb
+    from helpers import DUFFING, HYPER_ROSSLER, LORENZ, rk4_body
+    from oracle import oracle as O
+    out = {}
+    # Lorenz bifurcation: rho over 1024 values in [20, 200], x0 = (0.1, 0.1, 0.1), h = 0.01,
+    # 5,000 transient steps then 20,000 recorded, up to 64 maxima of x per rho.
+    body = rk4_body(LORENZ)
+    for name, opt in (("plain_fp64_exact", dict(precision=ucb.PREC_F64, mode=ucb.MODE_EXACT)),
+                      ("plain_fp64_native", dict(precision=ucb.PREC_F64, mode=ucb.MODE_NATIVE)),
+                      ("fp32_native", dict(precision=ucb.PREC_F32, mode=ucb.MODE_NATIVE))):
+        req = ucb.Engine.bif1d_request(body, 3, (0.1, 0.1, 0.1), (0, 10.0, 28.0, 8 / 3), n_pts=1024, param_index=2,
+                                       param_lo=20.0, param_hi=200.0, h=0.01, transient_time=50.0, t_max=200.0,
+                                       writable_var=0, max_peaks=64, opt=ucb.options(**opt))
+        (counts, peaks, intervals, res), ms = _timed(lambda: eng.run_bif1d(req), reps=2)
+        out.setdefault("bif_lorenz_1024", {})[name] = {
+            "wall_ms": ms, "kernel_ms": res.kernel_ms, "points_per_s": 1024 / (res.kernel_ms * 1e-3),
+            "rk4_steps_per_s": res.steps / (res.kernel_ms * 1e-3), "points_with_peaks": int((counts > 0).sum())}
+        if name == "plain_fp64_exact":
+            b = dict(n_pts=1024, sweep_kind=0, sweep_index=2, lo=20.0, hi=200.0, ic=(0.1, 0.1, 0.1),
+                     values=(0, 10.0, 28.0, 8 / 3), h=0.01, transient_time=50.0, t_max=200.0, pre_scaller=1,
+                     writable_var=0, max_value=1e6)
+            t0 = time.perf_counter()
+            oc, op, oi = O.bif1d(O.Krs(body, 3, "f64"), b, max_out=64)
+            cpu_s = time.perf_counter() - t0
+            m = np.isfinite(op)
+            out["bif_lorenz_1024"]["oracle"] = {
+                "cpu_points_per_s": 1024 / cpu_s, "cores": os.cpu_count(),
+                "counts_equal": bool((counts == oc).all()),
+                "peaks_bit_equal": bool(np.array_equal(peaks[m], op[m]) and np.array_equal(intervals[m], oi[m]))}
+    # Hyper-chaotic Rossler spectrum: (0.25, 0.05) swept over [0.1, 0.35] x [0.01, 0.1] on
+    # 512 x 512, DP5(4) with 4 tangent vectors, modified Gram-Schmidt every 10 accepted
+    # steps, t_end = 2e4, rtol 1e-8 (FP64) / 1e-5 (FP32).
+    hb = rk4_body(HYPER_ROSSLER)
+    for name, prec, rtol in (("fp64_rtol1e-8", ucb.PREC_F64, 1e-8), ("fp32_rtol1e-5", ucb.PREC_F32, 1e-5)):
+        def lreq(n):
+            return ucb.Engine.ls2d_request(hb, 4, (-10.0, -6.0, 0.0, 10.0), (0, 0.25, 0.05), method=ucb.LS_DP5,
+                                           gs_every=10, rtol=rtol, t_end=2e4, n_pts=n, param_index=1,
+                                           param_index_2=2, param_lo=0.1, param_hi=0.35, param_lo_2=0.01,
+                                           param_hi_2=0.1, h=0.01, transient_time=0.0, t_max=2e4, NT=1.0, eps=1e-6,
+                                           opt=ucb.options(precision=prec))
+        warm = ucb.Engine.ls2d_request(hb, 4, (-10.0, -6.0, 0.0, 10.0), (0, 0.25, 0.05), method=ucb.LS_DP5,
+                                       gs_every=10, rtol=rtol, t_end=10.0, n_pts=4, param_index=1, param_index_2=2,
+                                       param_lo=0.1, param_hi=0.35, param_lo_2=0.01, param_hi_2=0.1, h=0.01,
+                                       t_max=10.0, NT=1.0, eps=1e-6, opt=ucb.options(precision=prec))
+        eng.run_ls2d(warm)
+        # a 64 x 64 grid over the same window first; the full 512 x 512 grid only when its
+        # projected time stays within two minutes
+        (_, _, pre), _ = _timed(lambda: eng.run_ls2d(lreq(64)))
+        n_ls = 512 if pre.kernel_ms * 64 < 120e3 else 128
+        (vals, flags, res), ms = _timed(lambda: eng.run_ls2d(lreq(n_ls)))
+        v = vals.reshape(4, -1)
+        ok = flags == 1
+        out.setdefault("ls_hyper_rossler_512_dp5", {})[name] = {
+            "grid": n_ls, "wall_ms": ms, "kernel_ms": res.kernel_ms,
+            "cells_per_s": n_ls * n_ls / (res.kernel_ms * 1e-3),
+            "rhs_evals_per_s": res.steps / (res.kernel_ms * 1e-3), "valid_cells": int(ok.sum()),
+            "median_spectrum": [float(np.median(v[k][ok])) for k in range(4)],
+            "median_sum": float(np.median(v[:, ok].sum(axis=0)))}
+    # Forced Duffing basins: 4096 x 4096 initial conditions (x, x') in [-2.5, 2.5]^2,
+    # RK4 h = 2 pi / 200, 20 consecutive period matches to 1e-6, 2,000-period cap.
+    db = rk4_body(DUFFING)
+    for name, prec in (("plain_fp64", ucb.PREC_F64), ("fp32", ucb.PREC_F32)):
+        def breq(n):
+            return ucb.Engine.basins_request(db, 3, (0.0, 0.0, 0.0), (0.0,), n_pts=n, axis_x_var=0, axis_y_var=1,
+                                             axis_x_lo=-2.5, axis_x_hi=2.5, axis_y_lo=-2.5, axis_y_hi=2.5,
+                                             period=2 * np.pi, steps_per_period=200, max_periods=2000,
+                                             match_count=20, match_tol=1e-6, phase_var=2, max_value=1e6,
+                                             opt=ucb.options(precision=prec))
+        eng.run_basins(breq(8))
+        (labels, periods, iters, att, res), ms = _timed(lambda: eng.run_basins(breq(4096)))
+        out.setdefault("basins_duffing_4096", {})[name] = {
+            "wall_ms": ms, "kernel_ms": res.kernel_ms, "cells_per_s": 4096 * 4096 / (res.kernel_ms * 1e-3),
+            "rk4_steps_per_s": res.steps / (res.kernel_ms * 1e-3), "attractors": att,
+            "converged_fraction": float((labels > 0).mean()), "mean_periods": float(iters.mean())}
+        if name == "plain_fp64":
+            ref_labels = labels
+        else:
+            out["basins_duffing_4096"]["fp32_label_agreement"] = float((labels == ref_labels).mean())
+    return out
 
 
 class _Null:
@@ -222,8 +433,12 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--n", type=int, default=1024)
-    ap.add_argument("--cpu-stride", type=int, default=16)
+    ap.add_argument("--cpu-stride", type=int, default=6)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--all-configs", action="store_true",
+                    help="also time the bifurcation, spectrum and basins configurations at full size")
+    ap.add_argument("--surrogate-chen", type=int, default=0, metavar="N",
+                    help="also run the surrogate-refined Chen map at N x N (e.g. 8192)")
     args = ap.parse_args()
     rank, world, local = dist_env()
     cfg = {"workload": f"Rossler LLE map {args.n}x{args.n} (b in [0.05,2] x c in [2,20], a=0.2), RK4 h=0.01, "
@@ -262,6 +477,11 @@ def main():
         cpu = run_cpu_baseline(args.n, args.cpu_stride, 0)
     results, clocks, launches, e2e_ms = run_ours(args, rank, world, local)
     import ucb
+    surrogate_chen = None
+    other_configs = run_other_configs(ucb.Engine(local)) if args.all_configs and rank == 0 else None
+    if args.surrogate_chen and rank == 0:
+        surrogate_chen = [run_surrogate_chen(ucb.Engine(local), torch.device("cuda", local), args.surrogate_chen,
+                                             tol, cov) for tol, cov in ((2e-3, 0.995), (2e-2, 0.99))]
     peak64 = ucb.measure_fma_peak(ucb.PREC_F64)
     peak32 = ucb.measure_fma_peak(ucb.PREC_F32)
     if world > 1:
@@ -274,7 +494,7 @@ def main():
     value = world * cells / (r32["ms"] * 1e-3)
     forms = {}
     for name, r in results.items():
-        if name == "e2e_detail":
+        if name in ("e2e_detail", "surrogate"):
             continue
         forms[name] = {"cells_per_s": world * cells / (r["ms"] * 1e-3),
                        "rk4_steps_per_s": world * r["steps"] / (r["ms"] * 1e-3), "ms_per_map": r["ms"],
@@ -292,6 +512,7 @@ def main():
                      "traffic": None,
                      "peak_source": "measured FMA probe (ucb_measure_fma_peak) on this GPU in this run",
                      "plain_fp64": {"bound": "fp64", "achieved": ach64, "peak": peak64, "frac": ach64 / peak64}},
+        "surrogate": results["surrogate"],
         "clocks": clocks,
         "gpu_launches": launches,
         "e2e": {"value": world * cells / (e2e_ms * 1e-3), "unit": "cells/s", "detail": results["e2e_detail"],
@@ -300,6 +521,10 @@ def main():
     }
     if cpu:
         line["cpu_baseline"] = {k: cpu[k] for k in ("value", "unit", "cores", "kind", "sample")}
+    if surrogate_chen:
+        line["surrogate_chen"] = surrogate_chen
+    if other_configs:
+        line["other_configs"] = other_configs
     print(json.dumps(line))
 
 

@@ -385,10 +385,10 @@ typedef struct ucb_mlp_config {
     int32_t fourier;        /* frequencies; 2 * fourier must be a multiple of 128 (default 64) */
     int32_t hidden;         /* hidden width, a multiple of 128 (default 256) */
     int32_t layers;         /* hidden layers, 1..8 (default 4) */
-    float fourier_scale;    /* std of the frequency matrix entries (default 6) */
+    float fourier_scale;    /* std of the frequency matrix entries (default 3) */
     uint64_t seed;          /* initialisation, frequency matrix and mini-batch sampling (default 0) */
     int32_t batch;          /* rows per Adam step, a multiple of 128 (default 8192) */
-    int32_t train_steps;    /* Adam steps of ucb_mlp_fit (default 2000) */
+    int32_t train_steps;    /* Adam steps of ucb_mlp_fit (default 1500) */
     float lr;               /* initial learning rate (default 2e-3) */
     float lr_final;         /* learning rate at the last step, cosine decay (default 2e-5) */
     float beta_nll;         /* 0 = plain Gaussian NLL, 1 = mean-squared-error-like (default 0.5) */

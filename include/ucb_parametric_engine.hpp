@@ -4,8 +4,8 @@
 // Same class name, same request/result struct names and field names, same result
 // conventions (ok / cancelled / error, NaN or sentinel + flags, row-major iy*n+ix, plane-
 // major spectra), same shared_ptr<atomic<...>> cancel / progress tokens. Every call goes
-// through the C ABI in ucb.h (libucb.so). Entry points of the reference that are not on
-// this path (DFT, 2-D bifurcation with DBSCAN, Fast Synchro, basin re-clustering,
+// through the C ABI in ucb.h (libucb.so): run_bifurcation_1d, run_lle_2d, run_ls_2d.
+// Entry points of the reference that are not on this path (DFT, Fast Synchro,
 // continuation sweeps) are not provided.
 //
 // Extension: ParametricEngine::options() selects the arithmetic of the B200 engine
@@ -35,6 +35,14 @@ struct LLE2DSnapshot {
     int indexOfMutVar = 0, indexOfMutVar2 = 0;
     double range1_lo = 0.0, range1_hi = 0.0, range2_lo = 0.0, range2_hi = 0.0;
     int n_pts = 0;
+};
+struct LS2DSnapshot {
+    std::vector<double> values, initial_conditions;
+    int par_or_var = 1;
+    double tMax = 0.0, NT = 0.0, transientTime = 0.0, h = 0.0, eps = 0.0;
+    int indexOfMutVar = 0, indexOfMutVar2 = 0;
+    double range1_lo = 0.0, range1_hi = 0.0, range2_lo = 0.0, range2_hi = 0.0;
+    int n_pts = 0, n_exponents = 0;
 };
 }  // namespace data_export
 
@@ -122,6 +130,57 @@ struct LLE2DResult {
     double min_val = 0.0;
     double max_val = 0.0;
     data_export::LLE2DSnapshot snapshot;
+};
+
+// LS 2D (parametric_engine.h:581-637): full spectrum per cell, the reference's fixed-step
+// LSKernelCUDA semantics (classical Gram-Schmidt every NT). values are plane-major:
+// values[k * n * n + iy * n + ix]; per-plane min / max over valid cells.
+struct LS2DRequest {
+    std::string krs_body;
+    int amountOfX = 0;
+    std::vector<double> initial_conditions;
+    std::vector<double> base_values;
+    bool sweep_over_var = false;
+    bool sweep_over_var_2 = false;
+    bool sweep_over_h = false;
+    bool sweep_over_h_2 = false;
+    bool log_scale = false;
+    bool log_scale_2 = false;
+    int param_index = 0;
+    int var_sweep_index = 0;
+    int param_index_2 = 0;
+    int var_sweep_index_2 = 0;
+    double param_lo = 0.0;
+    double param_hi = 1.0;
+    double param_lo_2 = 0.0;
+    double param_hi_2 = 1.0;
+    int n_pts = 200;
+    double h = 0.01;
+    double transient_time = 0.0;
+    double t_max = 100.0;
+    double NT = 1.0;
+    double eps = 1.0e-4;
+    double max_value = 1.0e6;
+    std::string csv_output_path;
+    std::shared_ptr<std::atomic<bool>> cancel;
+    std::shared_ptr<std::atomic<float>> progress;
+};
+
+struct LS2DResult {
+    bool ok = false;
+    bool cancelled = false;
+    std::string error;
+    int n_pts = 0;
+    int n_exponents = 0;
+    double param_lo = 0.0;
+    double param_hi = 1.0;
+    double param_lo_2 = 0.0;
+    double param_hi_2 = 1.0;
+    std::vector<double> values;
+    std::vector<int> flags;
+    std::vector<double> min_val;
+    std::vector<double> max_val;
+    data_export::LS2DSnapshot snapshot;
 };
 
 class ParametricEngine {
@@ -286,6 +345,90 @@ public:
         s.range2_lo = r.param_lo_2;
         s.range2_hi = r.param_hi_2;
         s.n_pts = r.n_pts;
+        return res;
+    }
+
+    LS2DResult run_ls_2d(const LS2DRequest& r) {
+        LS2DResult res;
+        if ((int)r.initial_conditions.size() != r.amountOfX) {
+            res.error = "initial_conditions.size() != amountOfX";
+            return res;
+        }
+        ucb_ls2d_request q{};
+        q.krs_body = r.krs_body.c_str();
+        q.amount_of_x = r.amountOfX;
+        q.initial_conditions = r.initial_conditions.data();
+        q.base_values = r.base_values.data();
+        q.n_values = (int)r.base_values.size();
+        q.sweep_over_var = r.sweep_over_var;
+        q.sweep_over_var_2 = r.sweep_over_var_2;
+        q.sweep_over_h = r.sweep_over_h;
+        q.sweep_over_h_2 = r.sweep_over_h_2;
+        q.log_scale = r.log_scale;
+        q.log_scale_2 = r.log_scale_2;
+        q.param_index = r.param_index;
+        q.var_sweep_index = r.var_sweep_index;
+        q.param_index_2 = r.param_index_2;
+        q.var_sweep_index_2 = r.var_sweep_index_2;
+        q.param_lo = r.param_lo;
+        q.param_hi = r.param_hi;
+        q.param_lo_2 = r.param_lo_2;
+        q.param_hi_2 = r.param_hi_2;
+        q.n_pts = r.n_pts;
+        q.h = r.h;
+        q.transient_time = r.transient_time;
+        q.t_max = r.t_max;
+        q.NT = r.NT;
+        q.eps = r.eps;
+        q.max_value = r.max_value;
+        q.csv_output_path = r.csv_output_path.c_str();
+        int32_t cancel_now = (r.cancel && r.cancel->load()) ? 1 : 0;
+        q.cancel = &cancel_now;
+        float prog = 0.0f;
+        q.progress = &prog;
+        q.opt = opt_;
+        q.method = UCB_LS_FIXED;
+        const size_t cells = r.n_pts > 0 ? (size_t)r.n_pts * (size_t)r.n_pts : 0;
+        const size_t nx = r.amountOfX > 0 ? (size_t)r.amountOfX : 0;
+        res.values.assign(cells * nx, 0.0);
+        res.min_val.assign(nx, 0.0);
+        res.max_val.assign(nx, 0.0);
+        std::vector<int32_t> f32(cells);
+        ucb_ls2d_result o{};
+        o.values = res.values.data();
+        o.flags = f32.data();
+        o.min_val = res.min_val.data();
+        o.max_val = res.max_val.data();
+        ucb_run_ls2d(e_, &q, &o);
+        if (r.progress) r.progress->store(prog);
+        res.ok = o.ok != 0;
+        res.cancelled = o.cancelled != 0;
+        res.error = o.error;
+        if (!res.ok) return res;
+        res.flags.assign(f32.begin(), f32.end());
+        res.n_pts = o.n_pts;
+        res.n_exponents = o.n_exponents;
+        res.param_lo = r.param_lo;
+        res.param_hi = r.param_hi;
+        res.param_lo_2 = r.param_lo_2;
+        res.param_hi_2 = r.param_hi_2;
+        auto& s = res.snapshot;
+        s.values = r.base_values;
+        s.initial_conditions = r.initial_conditions;
+        s.par_or_var = (r.sweep_over_var == r.sweep_over_var_2) ? (r.sweep_over_var ? 0 : 1) : 2;
+        s.tMax = r.t_max;
+        s.NT = r.NT;
+        s.transientTime = r.transient_time;
+        s.h = r.h;
+        s.eps = r.eps;
+        s.indexOfMutVar = r.sweep_over_var ? r.var_sweep_index : r.param_index;
+        s.indexOfMutVar2 = r.sweep_over_var_2 ? r.var_sweep_index_2 : r.param_index_2;
+        s.range1_lo = r.param_lo;
+        s.range1_hi = r.param_hi;
+        s.range2_lo = r.param_lo_2;
+        s.range2_hi = r.param_hi_2;
+        s.n_pts = r.n_pts;
+        s.n_exponents = res.n_exponents;
         return res;
     }
 

@@ -156,3 +156,60 @@ def test_mlp_config_validation():
     with pytest.raises(ucb.UcbError, match="invalid MLP configuration"):
         ucb.Mlp(eng, batch=1000)
     eng.close()
+
+
+def _lorenz_stable_case(n):
+    """Lorenz LLE map over sigma in [4, 16] x rho in [0.2, 0.9]: the origin is a stable node
+    there, so the exponent is a smooth function of the parameters (up to the per-cell
+    probe term, ~log|cos|/t_max, kept small by t_max = 2000)."""
+    from helpers import rk4_body, LORENZ
+    return dict(body=rk4_body(LORENZ), nx=3, ic=(0.5, 0.5, 0.5), values=(0.0, 10.0, 0.5, 8.0 / 3.0), n_pts=n,
+                param_index=1, param_index_2=2, param_lo=4.0, param_hi=16.0, param_lo_2=0.2, param_hi_2=0.9,
+                h=0.01, transient_time=10.0, t_max=2000.0, NT=0.1, eps=1e-4, max_value=1e6)
+
+
+@pytest.mark.gpu
+def test_surrogate_map_gain_and_calibrated_error(ucb_engine):
+    """What the trained network gains: on a map with smooth regions it vouches for most cells,
+    so only the samples and a minority of cells are integrated, and the cells it predicts are
+    within the calibrated tolerance of the full plain (FP64) map."""
+    import torch
+    import ucb
+    from helpers import engine_request
+    n = 128
+    c = _lorenz_stable_case(n)
+    dev = torch.device("cuda")
+
+    def full(prec):
+        v = torch.empty(n * n, dtype=torch.float64, device=dev)
+        f = torch.empty(n * n, dtype=torch.int32, device=dev)
+        ucb_engine.lle2d_device(engine_request(ucb, c, precision=prec), v.data_ptr(), f.data_ptr(), 0)
+        torch.cuda.synchronize()
+        return v.cpu().numpy(), f.cpu().numpy()
+
+    ref64, f64 = full(ucb.PREC_F64)
+    ref32, _ = full(ucb.PREC_F32)
+    assert (f64 == 1).all()
+    req = ucb.surrogate_request(engine_request(ucb, c, precision=ucb.PREC_F32), train_pts=32, tol=2e-3,
+                                coverage=0.995, lle_band=0.0,
+                                mlp=dict(batch=1024, train_steps=1500, fourier_scale=1.0, seed=3))
+    v = torch.empty(n * n, dtype=torch.float64, device=dev)
+    f = torch.empty(n * n, dtype=torch.int32, device=dev)
+    res = ucb_engine.run_lle2d_surrogate(req, v.data_ptr(), f.data_ptr(), 0)
+    torch.cuda.synchronize()
+    vals, flags = v.cpu().numpy(), f.cpu().numpy()
+    assert res.n_samples == 32 * 32 and res.n_samples + res.n_refined + res.n_predicted == n * n
+    assert set(np.unique(flags)) <= {1, 2}
+    pred = flags == 2
+    print("predicted", pred.mean(), "threshold", res.sigma_threshold, "calibration", res.calib_within_tol,
+          "train ms", res.train_ms)
+    # the gain: at least half of the map is not integrated
+    assert pred.mean() >= 0.5, pred.mean()
+    err = np.abs(vals[pred] - ref64[pred])
+    assert (err <= 2e-3).mean() >= 0.98, ((err <= 2e-3).mean(), err.max())
+    # integrated cells: samples carry the FP64 value, re-integrated cells the FP32 value
+    integ = flags == 1
+    is64 = vals[integ] == ref64[integ]
+    is32 = vals[integ] == ref32[integ]
+    assert (is64 | is32).all()
+    assert is64.sum() >= res.n_samples - 1

@@ -46,3 +46,17 @@ def test_shim_bif1d_runs(driver):
     assert out[0].startswith("ok=1")
     counts = [int(l.split()[0]) for l in out[1:]]
     assert len(counts) == 8 and max(counts) > 0
+
+
+@pytest.mark.gpu
+def test_shim_ls2d_equals_c_abi(driver):
+    """run_ls_2d through the shim returns what ucb_run_ls2d returns (plane-major spectrum)."""
+    out = run(driver, "ls2d", rk4_body(LORENZ)).splitlines()
+    assert out[0].startswith("ok=1 error= n=6 k=3")
+    vals = np.array([float(l) for l in out[1:]])
+    eng = ucb.Engine(0)
+    req = eng.ls2d_request(rk4_body(LORENZ), 3, (0.1, 0.1, 0.1), (0, 10.0, 28.0, 8.0 / 3.0), n_pts=6, param_index=2,
+                           param_index_2=1, param_lo=20, param_hi=40, param_lo_2=8.0, param_hi_2=12.0, h=0.01,
+                           transient_time=5, t_max=20, NT=0.5, opt=ucb.options(precision=ucb.PREC_F64))
+    ref, _, _ = eng.run_ls2d(req)
+    np.testing.assert_array_equal(vals, ref.ravel())

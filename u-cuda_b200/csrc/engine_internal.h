@@ -5,6 +5,7 @@
 
 #include <cmath>
 #include <cstdint>
+#include <memory>
 #include <string>
 #include <vector>
 
@@ -24,6 +25,9 @@ struct ucb_engine {
     void* ws = nullptr;
     size_t ws_bytes = 0;
     long long launches = 0;
+    // Network of the last surrogate-refined map, kept for reuse by the next call with the
+    // same configuration (owned; released with the engine).
+    std::shared_ptr<void> surrogate_net;
 };
 
 namespace ucb {

@@ -881,23 +881,33 @@ Mlp* mlp_create(ucb_engine* e, const ucb_mlp_config& c, std::string& err) {
         m->W.push_back(w);
         m->Wt.push_back(wt);
     }
+    if (!mlp_reinit(m.get(), err)) return nullptr;
+    return m.release();
+}
+
+bool mlp_reinit(Mlp* m, std::string& err) {
     // Initialisation: W ~ N(0, 2 / in) for hidden layers (GELU), N(0, 0.1 / in) for the
     // output layer, biases 0; frequency matrix ~ N(0, fourier_scale^2).
+    const ucb_mlp_config& c = m->cfg;
     std::mt19937_64 rng(c.seed);
     std::normal_distribution<float> nd(0.f, 1.f);
-    std::vector<float> hp(off, 0.f);
+    std::vector<float> hp(m->n_params, 0.f);
     for (int l = 0; l <= m->L; ++l) {
         const float sd = std::sqrt((l == m->L ? 0.1f : 2.0f) / (float)m->in[l]);
         for (long long k = 0; k < (long long)m->out[l] * m->in[l]; ++k) hp[m->w_off[l] + k] = sd * nd(rng);
     }
     std::vector<float> hb(2 * c.fourier);
     for (auto& v : hb) v = c.fourier_scale * nd(rng);
-    if (!cu_ok(cudaMemcpy(m->p, hp.data(), off * sizeof(float), cudaMemcpyHostToDevice), err, "upload params") ||
+    m->y_mean = 0.f;
+    m->y_std = 1.f;
+    if (!cu_ok(cudaMemcpy(m->p, hp.data(), m->n_params * sizeof(float), cudaMemcpyHostToDevice), err,
+               "upload params") ||
         !cu_ok(cudaMemcpy(m->Bf, hb.data(), hb.size() * sizeof(float), cudaMemcpyHostToDevice), err, "upload B"))
-        return nullptr;
-    if (!refresh(*m, e->stream, false, err) || !cu_ok(cudaStreamSynchronize(e->stream), err, "init")) return nullptr;
-    return m.release();
+        return false;
+    return refresh(*m, m->e->stream, false, err) && cu_ok(cudaStreamSynchronize(m->e->stream), err, "init");
 }
+
+const ucb_mlp_config& mlp_config(const Mlp* m) { return m->cfg; }
 
 void mlp_destroy(Mlp* m) {
     if (!m) return;
@@ -1012,10 +1022,10 @@ void ucb_mlp_default_config(ucb_mlp_config* c) {
     c->fourier = 64;
     c->hidden = 256;
     c->layers = 4;
-    c->fourier_scale = 6.0f;
+    c->fourier_scale = 3.0f;
     c->seed = 0;
     c->batch = 8192;
-    c->train_steps = 2000;
+    c->train_steps = 1500;
     c->lr = 2e-3f;
     c->lr_final = 2e-5f;
     c->beta_nll = 0.5f;

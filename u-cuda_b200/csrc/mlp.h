@@ -26,6 +26,10 @@ struct Mlp;
 
 Mlp* mlp_create(ucb_engine* e, const ucb_mlp_config& cfg, std::string& err);
 void mlp_destroy(Mlp* m);
+// Re-initialises parameters and the frequency matrix from the configuration's seed
+// (buffers are kept).
+bool mlp_reinit(Mlp* m, std::string& err);
+const ucb_mlp_config& mlp_config(const Mlp* m);
 long long mlp_param_count(const Mlp* m);
 int mlp_features(const Mlp* m);
 

@@ -281,20 +281,29 @@ int ucb_run_lle2d_surrogate(ucb_engine* e, const ucb_surrogate_request* rq, doub
     res->n_samples = ns;
     res->n_calib = n_cal;
 
-    // 2. training
-    std::unique_ptr<Mlp, void (*)(Mlp*)> net(nullptr, mlp_destroy);
+    // 2. training (the engine keeps the network's buffers between calls with the same
+    // configuration; parameters are re-initialised from the seed every call)
+    Mlp* net = nullptr;
     float* d_u = mem.alloc<float>(std::max<long long>(2 * n_train, 1), err, "train u");
     float* d_y = mem.alloc<float>(std::max<long long>(n_train, 1), err, "train y");
     if (!d_u || !d_y) return fail(UCB_E_CUDA, err);
     if (n_train > 0) {
         cudaMemcpyAsync(d_u, hu.data(), hu.size() * 4, cudaMemcpyHostToDevice, st);
         cudaMemcpyAsync(d_y, hy.data(), hy.size() * 4, cudaMemcpyHostToDevice, st);
-        net.reset(mlp_create(e, r.mlp, err));
-        if (!net) return fail(UCB_E_INVALID, err);
+        Mlp* cached = static_cast<Mlp*>(e->surrogate_net.get());
+        if (cached && std::memcmp(&mlp_config(cached), &r.mlp, sizeof(ucb_mlp_config)) == 0) {
+            if (!mlp_reinit(cached, err)) return fail(UCB_E_CUDA, err);
+            net = cached;
+        } else {
+            e->surrogate_net.reset();
+            net = mlp_create(e, r.mlp, err);
+            if (!net) return fail(UCB_E_INVALID, err);
+            e->surrogate_net = std::shared_ptr<void>(net, [](void* q) { mlp_destroy(static_cast<Mlp*>(q)); });
+        }
         MlpInputs tin;
         tin.u = d_u;
         tin.n = n_train;
-        if (!mlp_fit(net.get(), tin, d_y, st, &res->final_loss, err)) return fail(UCB_E_CUDA, err);
+        if (!mlp_fit(net, tin, d_y, st, &res->final_loss, err)) return fail(UCB_E_CUDA, err);
     }
     cudaEventRecord(ev[2], st);
 
@@ -303,7 +312,7 @@ int ucb_run_lle2d_surrogate(ucb_engine* e, const ucb_surrogate_request* rq, doub
         MlpInputs pin;
         pin.n = total;
         pin.grid_n = n;
-        if (!mlp_predict(net.get(), pin, d_mean, d_sd, st, err)) return fail(UCB_E_CUDA, err);
+        if (!mlp_predict(net, pin, d_mean, d_sd, st, err)) return fail(UCB_E_CUDA, err);
     } else {
         cudaMemsetAsync(d_mean, 0, total * 4, st);
         cudaMemsetAsync(d_sd, 0, total * 4, st);

@@ -552,6 +552,7 @@ void ucb_destroy(ucb_engine* e) {
     if (e->initialized) {
         cudaSetDevice(e->device);
         if (e->stream) cudaStreamSynchronize(e->stream);
+        e->surrogate_net.reset();
         e->modules.clear();
         if (e->ws) cudaFree(e->ws);
         if (e->ev0) cudaEventDestroy(e->ev0);
