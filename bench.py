@@ -357,10 +357,12 @@ def run_other_configs(eng):
                                        param_lo=0.1, param_hi=0.35, param_lo_2=0.01, param_hi_2=0.1, h=0.01,
                                        t_max=10.0, NT=1.0, eps=1e-6, opt=ucb.options(precision=prec))
         eng.run_ls2d(warm)
-        # a 64 x 64 grid over the same window first; the full 512 x 512 grid only when its
-        # projected time stays within two minutes
+        # A 64 x 64 grid over the same window first. Most cells of this window escape to
+        # max_value through ever smaller steps, and the map takes about as long as its
+        # slowest cell while the grid fits the resident threads (~220k), so the full grid
+        # runs only when the small one ended within 150 s.
         (_, _, pre), _ = _timed(lambda: eng.run_ls2d(lreq(64)))
-        n_ls = 512 if pre.kernel_ms * 64 < 120e3 else 128
+        n_ls = 512 if pre.kernel_ms < 150e3 else 128
         (vals, flags, res), ms = _timed(lambda: eng.run_ls2d(lreq(n_ls)))
         v = vals.reshape(4, -1)
         ok = flags == 1

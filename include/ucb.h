@@ -140,6 +140,61 @@ UCB_API int ucb_lle2d_device(ucb_engine* e, const ucb_lle2d_request* req, double
                      void* stream, ucb_lle2d_result* res);
 
 /* ------------------------------------------------------------------------------------
+ * LLE 1D / LS 1D — replace ParametricEngine::run_lle_1d and run_ls_1d
+ * (parametric_engine.h:864-867, implementations parametric_engine.cpp:2196 and :3066):
+ * the LLE / spectrum kernels over n_pts values of one swept parameter, initial condition
+ * (sweep_over_var) or step h (sweep_over_h). The continuation branch of the reference
+ * (sequential by construction) is not part of this path.
+ * ---------------------------------------------------------------------------------- */
+typedef struct ucb_lle1d_request {
+    const char* krs_body;
+    int32_t amount_of_x;
+    const double* initial_conditions;
+    const double* base_values;
+    int32_t n_values;
+    int32_t sweep_over_var;   /* sweep initial condition var_sweep_index (0-based) */
+    int32_t var_sweep_index;
+    int32_t sweep_over_h;     /* sweep the step h over [param_lo, param_hi] */
+    int32_t log_scale;
+    int32_t param_index;      /* 1-based a[] index (parameter sweep) */
+    double param_lo, param_hi;
+    int32_t n_pts;
+    double h, transient_time, t_max, NT, eps, max_value;
+    const char* csv_output_path;
+    const volatile int32_t* cancel;
+    volatile float* progress;
+    ucb_options opt;
+} ucb_lle1d_request;
+typedef ucb_lle1d_request ucb_ls1d_request;
+
+typedef struct ucb_lle1d_result {
+    double* values;   /* n_pts: lambda; NaN where the kernel returned 999 / -999 (flag -1),
+                         as run_lle_1d does (parametric_engine.cpp:2455-2466) */
+    int32_t* flags;   /* 1 ok, -1 diverged */
+    int32_t ok, cancelled, n_pts;
+    double param_lo, param_hi;
+    double kernel_ms;
+    long long steps;
+    double flops;
+    char error[1024];
+} ucb_lle1d_result;
+
+typedef struct ucb_ls1d_result {
+    double* values;   /* n_pts * amount_of_x, point-major values[i * N + k] (the reference's
+                         spectrum[i][k]); the 999 / -999 sentinels are kept */
+    int32_t* flags;   /* 1 ok, -1 diverged (from the first exponent, as the reference) */
+    int32_t ok, cancelled, n_pts, n_exponents;
+    double param_lo, param_hi;
+    double kernel_ms;
+    long long steps;
+    double flops;
+    char error[1024];
+} ucb_ls1d_result;
+
+UCB_API int ucb_run_lle1d(ucb_engine* e, const ucb_lle1d_request* req, ucb_lle1d_result* res);
+UCB_API int ucb_run_ls1d(ucb_engine* e, const ucb_ls1d_request* req, ucb_ls1d_result* res);
+
+/* ------------------------------------------------------------------------------------
  * Bifurcation 1D — replaces ParametricEngine::run_bifurcation_1d (parametric_engine.h:27-126,
  * :853; classical sweep of parametric_engine.cpp:1674-2091; the continuation branch is
  * sequential by construction and not part of this path).

@@ -1,5 +1,6 @@
 #include "csv_export.h"
 
+#include <cmath>
 #include <fstream>
 #include <iomanip>
 
@@ -118,6 +119,39 @@ void ls2d(const std::string& path, const Common& c, int par_or_var, double tMax,
             out << values[(size_t)k * total + cell];
             if (k + 1 < n_exp) out << ", ";
         }
+        out << '\n';
+    }
+}
+
+void curve1d(const std::string& path, const char* title, const Common& c, double tMax, double NT, double transient,
+             double h, double eps, int index, double lo, double hi, bool log_scale, int n_pts, int n_cols,
+             const double* v) {
+    {
+        std::ofstream cfg(path + "_config.csv");
+        if (!cfg) return;
+        cfg << std::setprecision(kPrecision);
+        cfg << title << "\nParameter estimation\n";
+        values_and_ic(cfg, c);
+        cfg << "CT = " << tMax << "\nNT = " << NT << "\nTT = " << transient << "\n";
+        cfg << "h = " << h << "\neps = " << eps << "\n";
+        cfg << "indexPar = " << index << "\n";
+        cfg << "start value = " << lo << ", stop value = " << hi << "\n";
+    }
+    std::ofstream out(path);
+    if (!out) return;
+    out << std::setprecision(kPrecision);
+    for (int i = 0; i < n_pts; ++i) {
+        double param = lo;
+        if (n_pts > 1) {
+            if (log_scale) {
+                const double l0 = std::log10(lo), l1 = std::log10(hi);
+                param = std::pow(10.0, l0 + (l1 - l0) * (double)i / (double)(n_pts - 1));
+            } else {
+                param = lo + (hi - lo) * (double)i / (double)(n_pts - 1);
+            }
+        }
+        out << param;
+        for (int k = 0; k < n_cols; ++k) out << ", " << v[(size_t)i * n_cols + k];
         out << '\n';
     }
 }

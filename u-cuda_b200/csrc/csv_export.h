@@ -26,5 +26,12 @@ void ls2d(const std::string& path, const Common& c, int par_or_var, double tMax,
           double h, double eps, int idx1, int idx2, double r1lo, double r1hi, double r2lo, double r2hi, int n_pts,
           int n_exp, const double* plane_major_values);
 
+// 1-D LLE / LS (data_export.cpp write_lle1d_config / write_ls1d_config + rows): config
+// title "1D LLE" or "1D LS", rows "param, v0[, v1, ...]" with the parameter value of
+// getValueByIdx(_log)_local (parametric_engine.cpp:577-590).
+void curve1d(const std::string& path, const char* title, const Common& c, double tMax, double NT, double transient,
+             double h, double eps, int index, double lo, double hi, bool log_scale, int n_pts, int n_cols,
+             const double* point_major_values);
+
 }  // namespace csv
 }  // namespace ucb

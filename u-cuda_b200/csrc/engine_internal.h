@@ -104,6 +104,13 @@ bool launch_packed(ucb_engine* e, CUfunction f, int grid, int block, cudaStream_
 bool plan_sweep2d(const ucb_lle2d_request& q, SweepMap& m, int& n_blocks, int& skip, long long& nt_steps,
                   std::string& err);
 
+// Validation and axis mapping of run_lle_1d / run_ls_1d (parametric_engine.cpp:2200-2221,
+// :3070-3100): a one-axis sweep (dim 1) with the same step counts.
+bool plan_sweep1d(const ucb_lle1d_request& q, SweepMap& m, int& n_blocks, int& skip, long long& nt,
+                  std::string& err);
+// The 2-D request with the fields a 1-D run shares (for the common launch code).
+ucb_lle2d_request as_lle2d(const ucb_lle1d_request& q);
+
 // Launch helper: persistent grid size for a kernel.
 int persistent_grid(ucb_engine* e, CUfunction f, int block, long long work_items);
 

@@ -432,7 +432,7 @@ int enqueue_lle_fn(ucb_engine* e, const ucb_lle2d_request& q, const LlePlan& pla
         err = std::string("CUDA upload: ") + cudaGetErrorString(ce);
         return UCB_E_CUDA;
     }
-    const long long total = d_cell_list ? n_list : (long long)n * n;
+    const long long total = d_cell_list ? n_list : (plan.map.dim == 2 ? (long long)n * n : (long long)n);
     std::vector<char> params;
     if (prec == UCB_PREC_F64) {
         LleParamsT<double> hd{total, 0, n, plan.map.swap_xy ? 1 : 0, plan.amountOfPointsInBlock, 0,
@@ -470,6 +470,89 @@ int enqueue_lle(ucb_engine* e, const ucb_lle2d_request& q, const LlePlan& plan, 
 }
 
 }  // namespace
+
+namespace {
+
+// Validation of run_lle_1d (parametric_engine.cpp:2200-2221) and the one-axis mapping of
+// its launch: par_or_var 0 (initial condition) / 1 (parameter), h-sweep axis 0.
+bool plan_lle1d(const ucb_lle1d_request& q, LlePlan& p, std::string& err) {
+    if (!q.krs_body || !*q.krs_body) { err = "krs_body is empty"; return false; }
+    if (q.amount_of_x <= 0 || q.amount_of_x > kMaxAmountOfX) { err = "amountOfX out of range"; return false; }
+    if (!q.initial_conditions) { err = "initial_conditions.size() != amountOfX"; return false; }
+    if (q.n_values > kMaxAmountOfValues) { err = "too many base_values"; return false; }
+    if (q.n_values > 0 && !q.base_values) { err = "base_values is NULL"; return false; }
+    if (q.sweep_over_h) {
+        if (!(q.param_lo > 0.0 && q.param_hi > 0.0)) { err = "h lo/hi must be > 0 with sweep_over_h"; return false; }
+    } else if (q.sweep_over_var) {
+        if (q.var_sweep_index < 0 || q.var_sweep_index >= q.amount_of_x) { err = "var_sweep_index out of range"; return false; }
+    } else {
+        if (q.param_index <= 0 || q.param_index >= q.n_values) { err = "param_index out of range"; return false; }
+    }
+    if (q.n_pts <= 0) { err = "n_pts must be > 0"; return false; }
+    if (!(q.h > 0.0)) { err = "h must be > 0"; return false; }
+    if (!(q.t_max > 0.0)) { err = "t_max must be > 0"; return false; }
+    if (q.transient_time < 0) { err = "transient_time must be >= 0"; return false; }
+    if (!(q.NT > 0.0)) { err = "NT must be > 0"; return false; }
+    if (!(q.eps > 0.0)) { err = "eps must be > 0"; return false; }
+    if (q.log_scale && !(q.param_lo > 0.0 && q.param_hi > 0.0)) { err = "log scale requires param lo/hi > 0"; return false; }
+    SweepMap& m = p.map;
+    m.dim = 1;
+    m.par_or_var = q.sweep_over_var ? 0 : 1;
+    m.idx[0] = q.sweep_over_var ? q.var_sweep_index : q.param_index;
+    m.idx[1] = 0;
+    m.h_axis = q.sweep_over_h ? 0 : -1;
+    m.lo[0] = q.param_lo;
+    m.hi[0] = q.param_hi;
+    m.log_axis[0] = q.log_scale != 0;
+    p.amountOfPointsInBlock = (int)(q.t_max / q.NT);
+    p.amountOfPointsForSkip = (int)(q.transient_time / q.h);
+    if (p.amountOfPointsInBlock <= 0) { err = "computed amountOfPointsInBlock <= 0 (t_max / NT too small)"; return false; }
+    if (q.opt.precision == UCB_PREC_F64 || q.opt.mode == UCB_MODE_NATIVE)
+        p.nt_steps = (long long)(q.NT / q.h);
+    else
+        p.nt_steps = (long long)((float)q.NT / (float)q.h);
+    return true;
+}
+
+}  // namespace
+
+ucb_lle2d_request as_lle2d(const ucb_lle1d_request& q) {
+    ucb_lle2d_request r{};
+    r.krs_body = q.krs_body;
+    r.amount_of_x = q.amount_of_x;
+    r.initial_conditions = q.initial_conditions;
+    r.base_values = q.base_values;
+    r.n_values = q.n_values;
+    r.sweep_over_var = q.sweep_over_var;
+    r.var_sweep_index = q.var_sweep_index;
+    r.sweep_over_h = q.sweep_over_h;
+    r.log_scale = q.log_scale;
+    r.param_index = q.param_index;
+    r.param_lo = q.param_lo;
+    r.param_hi = q.param_hi;
+    r.n_pts = q.n_pts;
+    r.h = q.h;
+    r.transient_time = q.transient_time;
+    r.t_max = q.t_max;
+    r.NT = q.NT;
+    r.eps = q.eps;
+    r.max_value = q.max_value;
+    r.cancel = q.cancel;
+    r.progress = q.progress;
+    r.opt = q.opt;
+    return r;
+}
+
+bool plan_sweep1d(const ucb_lle1d_request& q, SweepMap& m, int& n_blocks, int& skip, long long& nt,
+                  std::string& err) {
+    LlePlan p;
+    if (!plan_lle1d(q, p, err)) return false;
+    m = p.map;
+    n_blocks = p.amountOfPointsInBlock;
+    skip = p.amountOfPointsForSkip;
+    nt = p.nt_steps;
+    return true;
+}
 
 bool plan_sweep2d(const ucb_lle2d_request& q, SweepMap& m, int& n_blocks, int& skip, long long& nt_steps,
                   std::string& err) {
@@ -657,6 +740,78 @@ int ucb_run_lle2d(ucb_engine* e, const ucb_lle2d_request* req, ucb_lle2d_result*
                    q.sweep_over_var_2 ? q.var_sweep_index_2 : q.param_index_2, q.param_lo, q.param_hi, q.param_lo_2,
                    q.param_hi_2, n, res->values);
     }
+    if (!L.sys.note.empty()) e->last_error = L.sys.note;
+    res->ok = 1;
+    return UCB_OK;
+}
+
+int ucb_run_lle1d(ucb_engine* e, const ucb_lle1d_request* req, ucb_lle1d_result* res) {
+    if (!e || !req || !res) return UCB_E_INVALID;
+    res->ok = 0;
+    res->cancelled = 0;
+    res->error[0] = 0;
+    res->kernel_ms = 0;
+    res->steps = 0;
+    res->flops = 0;
+    const ucb_lle1d_request& q1 = *req;
+    LlePlan plan;
+    std::string err;
+    if (!plan_lle1d(q1, plan, err)) return fail(e, res->error, &res->ok, UCB_E_INVALID, err);
+    if (!res->values || !res->flags) return fail(e, res->error, &res->ok, UCB_E_INVALID, "result buffers are NULL");
+    if (q1.cancel && *q1.cancel) {
+        res->cancelled = 1;
+        return fail(e, res->error, &res->ok, UCB_E_CANCELLED, "Cancelled by user");
+    }
+    if (!ensure_init(e, err)) return fail(e, res->error, &res->ok, UCB_E_NOGPU, err);
+    const ucb_lle2d_request q = as_lle2d(q1);
+    LleLaunch L;
+    if (!prepare_lle(e, q, plan, L, err)) return fail(e, res->error, &res->ok, UCB_E_COMPILE, err);
+    if (q1.progress) *q1.progress = 0.0f;
+    const int n = q1.n_pts;
+    double* d_values = nullptr;
+    int32_t* d_flags = nullptr;
+    cudaError_t ce;
+    if ((ce = cudaMallocAsync((void**)&d_values, (size_t)n * sizeof(double), e->stream)) != cudaSuccess ||
+        (ce = cudaMallocAsync((void**)&d_flags, (size_t)n * sizeof(int32_t), e->stream)) != cudaSuccess)
+        return fail(e, res->error, &res->ok, UCB_E_CUDA, std::string("cudaMallocAsync: ") + cudaGetErrorString(ce));
+    cudaEventRecord(e->ev0, e->stream);
+    int rc = enqueue_lle(e, q, plan, L, d_values, d_flags, e->stream, err);
+    cudaEventRecord(e->ev1, e->stream);
+    unsigned long long steps = 0;
+    if (rc == UCB_OK) {
+        if ((ce = cudaMemcpyAsync(res->values, d_values, (size_t)n * sizeof(double), cudaMemcpyDeviceToHost,
+                                  e->stream)) != cudaSuccess ||
+            (ce = cudaMemcpyAsync(res->flags, d_flags, (size_t)n * sizeof(int32_t), cudaMemcpyDeviceToHost,
+                                  e->stream)) != cudaSuccess ||
+            (ce = cudaMemcpyAsync(&steps, static_cast<char*>(e->ws) + 8, 8, cudaMemcpyDeviceToHost, e->stream)) !=
+                cudaSuccess ||
+            (ce = cudaStreamSynchronize(e->stream)) != cudaSuccess) {
+            rc = UCB_E_CUDA;
+            err = std::string("CUDA lle1d: ") + cudaGetErrorString(ce);
+        }
+    }
+    cudaFreeAsync(d_values, e->stream);
+    cudaFreeAsync(d_flags, e->stream);
+    cudaStreamSynchronize(e->stream);
+    if (rc != UCB_OK) return fail(e, res->error, &res->ok, rc, err);
+    float ms = 0;
+    cudaEventElapsedTime(&ms, e->ev0, e->ev1);
+    res->kernel_ms = ms;
+    res->steps = (long long)steps;
+    res->flops = (double)steps * (double)L.sys.flops_step;
+    // sentinel -> NaN, as run_lle_1d does (parametric_engine.cpp:2455-2466)
+    for (int i = 0; i < n; ++i)
+        if (res->flags[i] < 0) res->values[i] = std::numeric_limits<double>::quiet_NaN();
+    res->n_pts = n;
+    res->param_lo = q1.param_lo;
+    res->param_hi = q1.param_hi;
+    if (q1.csv_output_path && *q1.csv_output_path) {
+        csv::Common cc{std::vector<double>(q1.base_values, q1.base_values + q1.n_values),
+                       std::vector<double>(q1.initial_conditions, q1.initial_conditions + q1.amount_of_x)};
+        csv::curve1d(q1.csv_output_path, "1D LLE", cc, q1.t_max, q1.NT, q1.transient_time, q1.h, q1.eps,
+                     plan.map.idx[0], q1.param_lo, q1.param_hi, q1.log_scale != 0, n, 1, res->values);
+    }
+    if (q1.progress) *q1.progress = 1.0f;
     if (!L.sys.note.empty()) e->last_error = L.sys.note;
     res->ok = 1;
     return UCB_OK;

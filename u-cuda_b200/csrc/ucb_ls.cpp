@@ -1,6 +1,6 @@
-// Lyapunov spectrum 2D host orchestration (run_ls_2d, parametric_engine.cpp:3430-3786):
+// Lyapunov spectrum host orchestration: run_ls_2d (parametric_engine.cpp:3430-3786) —
 // the LLE-2D validation and axis mapping, plane-major results, per-plane min/max over
-// valid cells, CSV. Device side: ucb_ls.cuh.
+// valid cells, CSV — and run_ls_1d (:3066) over one swept axis. Device side: ucb_ls.cuh.
 #include <algorithm>
 #include <cmath>
 #include <cstring>
@@ -93,20 +93,13 @@ extern "C" int ucb_precompile_ls2d(const ucb_ls2d_request* req, char* err_out, i
     return UCB_OK;
 }
 
-extern "C" int ucb_run_ls2d(ucb_engine* e, const ucb_ls2d_request* req, ucb_ls2d_result* res) {
-    if (!e || !req || !res) return UCB_E_INVALID;
-    const ucb_ls2d_request& q = *req;
-    res->ok = res->cancelled = 0;
-    res->error[0] = 0;
-    res->kernel_ms = 0;
-    res->steps = 0;
-    res->flops = 0;
+namespace {
+
+// The spectrum launch over a planned sweep (2-D grid, or one axis when m.dim == 1):
+// plane-major values[k * total + cell], flags, per-plane min / max.
+int ls_run(ucb_engine* e, const ucb_ls2d_request& q, const SweepMap& m, int n_blocks, int skip, long long nt,
+           ucb_ls2d_result* res) {
     std::string err;
-    SweepMap m;
-    int n_blocks = 0, skip = 0;
-    long long nt = 0;
-    const ucb_lle2d_request l = as_lle(q);
-    if (!plan_sweep2d(l, m, n_blocks, skip, nt, err)) return fail(e, res, UCB_E_INVALID, err);
     const bool dp5 = q.method == UCB_LS_DP5;
     if (q.method != UCB_LS_FIXED && !dp5) return fail(e, res, UCB_E_INVALID, "unknown LS method");
     if (dp5 && (m.h_axis != -1)) return fail(e, res, UCB_E_INVALID, "the DP5 method does not sweep h");
@@ -128,7 +121,7 @@ extern "C" int ucb_run_ls2d(ucb_engine* e, const ucb_ls2d_request* req, ucb_ls2d
     CUfunction fn = mod->functions["ucb_ls_kernel"];
 
     const int n = q.n_pts;
-    const long long total = (long long)n * n;
+    const long long total = m.dim == 2 ? (long long)n * n : (long long)n;
     std::vector<double> t0d, t1d;
     std::vector<float> t0f, t1f;
     axis_table(prec, n, m.lo[0], m.hi[0], m.log_axis[0], t0d, t0f);
@@ -224,6 +217,27 @@ extern "C" int ucb_run_ls2d(ucb_engine* e, const ucb_ls2d_request* req, ucb_ls2d
         if (res->min_val) res->min_val[k] = vmin;
         if (res->max_val) res->max_val[k] = vmax;
     }
+    return UCB_OK;
+}
+
+}  // namespace
+
+extern "C" int ucb_run_ls2d(ucb_engine* e, const ucb_ls2d_request* req, ucb_ls2d_result* res) {
+    if (!e || !req || !res) return UCB_E_INVALID;
+    const ucb_ls2d_request& q = *req;
+    res->ok = res->cancelled = 0;
+    res->error[0] = 0;
+    res->kernel_ms = 0;
+    res->steps = 0;
+    res->flops = 0;
+    std::string err;
+    SweepMap m;
+    int n_blocks = 0, skip = 0;
+    long long nt = 0;
+    if (!plan_sweep2d(as_lle(q), m, n_blocks, skip, nt, err)) return fail(e, res, UCB_E_INVALID, err);
+    const int rc = ls_run(e, q, m, n_blocks, skip, nt, res);
+    if (rc != UCB_OK) return rc;
+    const int n = q.n_pts, nx = q.amount_of_x;
     if (q.csv_output_path && *q.csv_output_path) {
         csv::Common cc{std::vector<double>(q.base_values, q.base_values + q.n_values),
                        std::vector<double>(q.initial_conditions, q.initial_conditions + nx)};
@@ -233,6 +247,90 @@ extern "C" int ucb_run_ls2d(ucb_engine* e, const ucb_ls2d_request* req, ucb_ls2d
                   q.param_hi_2, n, nx, res->values);
     }
     if (q.progress) *q.progress = 1.0f;
+    res->ok = 1;
+    return UCB_OK;
+}
+
+// run_ls_1d (parametric_engine.cpp:3066): the same kernel over one swept axis; spectrum
+// point-major (spectrum[i][k]) with the 999 / -999 sentinels kept, flag from the first
+// exponent.
+extern "C" int ucb_run_ls1d(ucb_engine* e, const ucb_ls1d_request* req, ucb_ls1d_result* res) {
+    if (!e || !req || !res) return UCB_E_INVALID;
+    const ucb_ls1d_request& q1 = *req;
+    res->ok = res->cancelled = 0;
+    res->error[0] = 0;
+    res->kernel_ms = 0;
+    res->steps = 0;
+    res->flops = 0;
+    auto fail1 = [&](int code, const std::string& msg) {
+        e->last_error = msg;
+        std::snprintf(res->error, sizeof res->error, "%s", msg.c_str());
+        return code;
+    };
+    std::string err;
+    SweepMap m;
+    int n_blocks = 0, skip = 0;
+    long long nt = 0;
+    if (!plan_sweep1d(q1, m, n_blocks, skip, nt, err)) return fail1(UCB_E_INVALID, err);
+    if (!res->values || !res->flags) return fail1(UCB_E_INVALID, "result buffers are NULL");
+    const ucb_lle2d_request l = as_lle2d(q1);
+    ucb_ls2d_request q{};
+    q.krs_body = l.krs_body;
+    q.amount_of_x = l.amount_of_x;
+    q.initial_conditions = l.initial_conditions;
+    q.base_values = l.base_values;
+    q.n_values = l.n_values;
+    q.sweep_over_var = l.sweep_over_var;
+    q.var_sweep_index = l.var_sweep_index;
+    q.sweep_over_h = l.sweep_over_h;
+    q.log_scale = l.log_scale;
+    q.param_index = l.param_index;
+    q.param_lo = l.param_lo;
+    q.param_hi = l.param_hi;
+    q.n_pts = l.n_pts;
+    q.h = l.h;
+    q.transient_time = l.transient_time;
+    q.t_max = l.t_max;
+    q.NT = l.NT;
+    q.eps = l.eps;
+    q.max_value = l.max_value;
+    q.opt = l.opt;
+    q.method = UCB_LS_FIXED;
+    const int n = q1.n_pts, nx = q1.amount_of_x;
+    std::vector<double> plane((size_t)n * nx), mn(nx), mx(nx);
+    ucb_ls2d_result r2{};
+    r2.values = plane.data();
+    r2.flags = res->flags;
+    r2.min_val = mn.data();
+    r2.max_val = mx.data();
+    if (q1.cancel && *q1.cancel) {
+        res->cancelled = 1;
+        return fail1(UCB_E_CANCELLED, "Cancelled by user");
+    }
+    const int rc = ls_run(e, q, m, n_blocks, skip, nt, &r2);
+    if (rc != UCB_OK) {
+        std::snprintf(res->error, sizeof res->error, "%s", r2.error);
+        return rc;
+    }
+    for (int i = 0; i < n; ++i) {
+        for (int k = 0; k < nx; ++k) res->values[(size_t)i * nx + k] = plane[(size_t)k * n + i];
+        const double first = res->values[(size_t)i * nx];
+        res->flags[i] = (first == 999.0 || first == -999.0) ? -1 : 1;
+    }
+    res->n_pts = n;
+    res->n_exponents = nx;
+    res->param_lo = q1.param_lo;
+    res->param_hi = q1.param_hi;
+    res->kernel_ms = r2.kernel_ms;
+    res->steps = r2.steps;
+    res->flops = r2.flops;
+    if (q1.csv_output_path && *q1.csv_output_path) {
+        csv::Common cc{std::vector<double>(q1.base_values, q1.base_values + q1.n_values),
+                       std::vector<double>(q1.initial_conditions, q1.initial_conditions + nx)};
+        csv::curve1d(q1.csv_output_path, "1D LS", cc, q1.t_max, q1.NT, q1.transient_time, q1.h, q1.eps, m.idx[0],
+                     q1.param_lo, q1.param_hi, q1.log_scale != 0, n, nx, res->values);
+    }
+    if (q1.progress) *q1.progress = 1.0f;
     res->ok = 1;
     return UCB_OK;
 }

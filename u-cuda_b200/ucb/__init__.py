@@ -62,6 +62,37 @@ class Lle2dResult(C.Structure):
     ]
 
 
+class Lle1dRequest(C.Structure):
+    _fields_ = [
+        ("krs_body", C.c_char_p), ("amount_of_x", C.c_int32),
+        ("initial_conditions", C.POINTER(C.c_double)), ("base_values", C.POINTER(C.c_double)),
+        ("n_values", C.c_int32), ("sweep_over_var", C.c_int32), ("var_sweep_index", C.c_int32),
+        ("sweep_over_h", C.c_int32), ("log_scale", C.c_int32), ("param_index", C.c_int32),
+        ("param_lo", C.c_double), ("param_hi", C.c_double), ("n_pts", C.c_int32),
+        ("h", C.c_double), ("transient_time", C.c_double), ("t_max", C.c_double), ("NT", C.c_double),
+        ("eps", C.c_double), ("max_value", C.c_double), ("csv_output_path", C.c_char_p),
+        ("cancel", C.POINTER(C.c_int32)), ("progress", C.POINTER(C.c_float)), ("opt", Options),
+    ]
+
+
+class Lle1dResult(C.Structure):
+    _fields_ = [
+        ("values", C.POINTER(C.c_double)), ("flags", C.POINTER(C.c_int32)),
+        ("ok", C.c_int32), ("cancelled", C.c_int32), ("n_pts", C.c_int32),
+        ("param_lo", C.c_double), ("param_hi", C.c_double), ("kernel_ms", C.c_double), ("steps", C.c_longlong),
+        ("flops", C.c_double), ("error", C.c_char * 1024),
+    ]
+
+
+class Ls1dResult(C.Structure):
+    _fields_ = [
+        ("values", C.POINTER(C.c_double)), ("flags", C.POINTER(C.c_int32)),
+        ("ok", C.c_int32), ("cancelled", C.c_int32), ("n_pts", C.c_int32), ("n_exponents", C.c_int32),
+        ("param_lo", C.c_double), ("param_hi", C.c_double), ("kernel_ms", C.c_double), ("steps", C.c_longlong),
+        ("flops", C.c_double), ("error", C.c_char * 1024),
+    ]
+
+
 class Bif1dRequest(C.Structure):
     _fields_ = [
         ("krs_body", C.c_char_p), ("amount_of_x", C.c_int32),
@@ -203,6 +234,10 @@ def load():
                               C.c_char_p, C.c_int, C.c_char_p, C.c_int]
     L.ucb_precompile_lle2d.restype = C.c_int
     L.ucb_precompile_lle2d.argtypes = [C.POINTER(Lle2dRequest), C.c_char_p, C.c_int]
+    L.ucb_run_lle1d.restype = C.c_int
+    L.ucb_run_lle1d.argtypes = [C.c_void_p, C.POINTER(Lle1dRequest), C.POINTER(Lle1dResult)]
+    L.ucb_run_ls1d.restype = C.c_int
+    L.ucb_run_ls1d.argtypes = [C.c_void_p, C.POINTER(Lle1dRequest), C.POINTER(Ls1dResult)]
     L.ucb_lle2d_cells.restype = C.c_int
     L.ucb_lle2d_cells.argtypes = [C.c_void_p, C.POINTER(Lle2dRequest), C.c_void_p, C.c_longlong, C.c_void_p,
                                   C.c_void_p, C.c_void_p, C.POINTER(Lle2dResult)]
@@ -311,6 +346,53 @@ class Engine:
         if rc != UCB_OK:
             raise UcbError(rc, res.error.decode())
         return values, flags, res
+
+    # ------------------------------------------------------------------ LLE / LS 1D
+    @staticmethod
+    def lle1d_request(krs_body: str, amount_of_x: int, initial_conditions, base_values, *, n_pts, param_index=0,
+                      sweep_over_var=False, var_sweep_index=0, sweep_over_h=False, log_scale=False, param_lo=0.0,
+                      param_hi=1.0, h=0.01, transient_time=0.0, t_max=100.0, NT=1.0, eps=1e-4, max_value=1e6,
+                      csv_output_path=None, opt: Options | None = None):
+        ic = np.ascontiguousarray(initial_conditions, dtype=np.float64)
+        vals = np.ascontiguousarray(base_values, dtype=np.float64)
+        r = Lle1dRequest()
+        r._keep = (ic, vals, krs_body.encode())
+        r.krs_body = r._keep[2]
+        r.amount_of_x = amount_of_x
+        r.initial_conditions = _dptr(ic)
+        r.base_values = _dptr(vals)
+        r.n_values = len(vals)
+        r.sweep_over_var, r.var_sweep_index = int(sweep_over_var), var_sweep_index
+        r.sweep_over_h, r.log_scale, r.param_index = int(sweep_over_h), int(log_scale), param_index
+        r.param_lo, r.param_hi, r.n_pts = param_lo, param_hi, n_pts
+        r.h, r.transient_time, r.t_max, r.NT, r.eps, r.max_value = h, transient_time, t_max, NT, eps, max_value
+        r.csv_output_path = csv_output_path.encode() if csv_output_path else None
+        r.opt = opt if opt is not None else options()
+        return r
+
+    def run_lle1d(self, req: Lle1dRequest):
+        n = req.n_pts
+        values = np.empty(max(n, 0), dtype=np.float64)
+        flags = np.empty(max(n, 0), dtype=np.int32)
+        res = Lle1dResult()
+        res.values = _dptr(values)
+        res.flags = flags.ctypes.data_as(C.POINTER(C.c_int32))
+        rc = self.lib.ucb_run_lle1d(self.h, C.byref(req), C.byref(res))
+        if rc != UCB_OK:
+            raise UcbError(rc, res.error.decode())
+        return values, flags, res
+
+    def run_ls1d(self, req: Lle1dRequest):
+        n, nx = req.n_pts, req.amount_of_x
+        values = np.empty(max(n, 0) * nx, dtype=np.float64)
+        flags = np.empty(max(n, 0), dtype=np.int32)
+        res = Ls1dResult()
+        res.values = _dptr(values)
+        res.flags = flags.ctypes.data_as(C.POINTER(C.c_int32))
+        rc = self.lib.ucb_run_ls1d(self.h, C.byref(req), C.byref(res))
+        if rc != UCB_OK:
+            raise UcbError(rc, res.error.decode())
+        return values.reshape(n, nx), flags, res
 
     # ------------------------------------------------------------------ LS 2D
     @staticmethod
