@@ -76,7 +76,8 @@ def test_ls1d_exact_matches_oracle_row():
     np.testing.assert_array_equal(flags, of)
     np.testing.assert_allclose(vals, ov, rtol=1e-12, atol=1e-12)
     assert res.n_exponents == 3
-    # Lorenz divergence: the spectrum sums to -(sigma + 1 + beta) times the step factor 1.1
+    # Lorenz divergence: the spectrum sums to -(sigma + 1 + beta) times the reference's step
+    # factor (NT/h + 1) / (NT/h) = 51/50 (one extra step per block)
     s = vals[flags == 1].sum(axis=1)
-    assert np.all(np.abs(s + 1.1 * (10 + 1 + 8 / 3)) < 0.3)
+    assert np.all(np.abs(s + 51 / 50 * (10 + 1 + 8 / 3)) < 0.05)
     eng.close()

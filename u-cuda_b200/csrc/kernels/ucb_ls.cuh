@@ -38,7 +38,7 @@ struct UcbLsParams {
     numb vals[UCB_NV];
     const numb* axis0;
     const numb* axis1;
-    double* out_values;    // plane-major: values[k * n^2 + cell]
+    double* out_values;    // plane-major: values[k * cells + cell] (cells = n^2, or n for one axis)
     int* out_flags;
     unsigned long long* counter;
     unsigned long long* steps;
@@ -54,7 +54,11 @@ __device__ __forceinline__ long long ls_out_cell(const UcbLsParams& p, long long
 
 __device__ __forceinline__ void ls_store(const UcbLsParams& p, long long kidx, const double* v) {
     const long long cell = ls_out_cell(p, kidx);
+#if UCB_DIM == 2
     const long long plane = (long long)p.n_pts * p.n_pts;
+#else
+    const long long plane = p.n_pts;  // one swept axis: n_pts cells per exponent plane
+#endif
     bool bad = false;
 #pragma unroll
     for (int k = 0; k < UCB_NX; ++k) {

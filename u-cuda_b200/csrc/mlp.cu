@@ -12,6 +12,7 @@
 // bias / GELU, storing FP32, BF16 and / or transposed BF16 copies; split-K launches add
 // their partial tiles atomically. Backward products are the same TN GEMM on transposed
 // copies, which the forward epilogue and the GELU-backward kernel write as they go.
+#include <cuda_bf16.h>
 #include <cuda_runtime.h>
 
 #include <cute/tensor.hpp>
@@ -51,7 +52,7 @@ using SmemLayoutA = decltype(UMMA::tile_to_mma_shape(
 using SmemLayoutB = decltype(UMMA::tile_to_mma_shape(
     UMMA::Layout_K_SW128_Atom<bf16>{}, partition_shape_B(TiledMma{}, make_shape(Int<kBN>{}, Int<kBK>{}))));
 
-constexpr int kStageLd = kBN + 1;  // staging row stride (floats): conflict-free both ways
+constexpr int kStageLd = kBN + 4;  // staging row stride (floats): 16-byte rows, conflict-free float4 access
 
 struct GemmSmem {
     union {
@@ -231,44 +232,101 @@ __global__ void __launch_bounds__(128) gemm_tn_kernel(const bf16* __restrict__ A
     if (failed) {
         if (threadIdx.x == 0) atomicExch(err, 1);
     } else if (issued > 0) {
-        // TMEM -> registers (thread t holds tile row t), bias, transposed copy straight from
-        // registers (consecutive threads write consecutive rows), then the row-major
-        // outputs through a per-warp staging block so that a warp stores whole row segments.
-        TiledCopy t2r = make_tmem_copy(SM100_TMEM_LOAD_32dp32b32x{}, tAcc);
-        ThrCopy thr = t2r.get_slice(threadIdx.x);
-        Tensor tDcC = thr.partition_D(tCcC);
-        Tensor tDrAcc = make_tensor<float>(shape(tDcC));
-        Tensor tDtAcc = thr.partition_S(tAcc);
-        copy(t2r, tDtAcc, tDrAcc);
+        // TMEM -> registers, 32 columns at a time (tcgen05.ld 32x32b.x32: thread t of warp w
+        // holds row 32 w + t), bias; the transposed copy is stored straight from registers
+        // (consecutive threads write consecutive rows); the row-major outputs go through a
+        // per-warp staging block so that each warp stores whole 512-byte row segments.
+        const int row = warp * 32 + lane;
+        const uint32_t taddr = ss.tmem_base + ((uint32_t)(warp * 32) << 16);
         float* stage = ss.stage;
-        CUTE_UNROLL
-        for (int i = 0; i < size(tDrAcc); ++i) {
-            const int m = get<0>(tDcC(i)), n = get<1>(tDcC(i));
-            float v = tDrAcc(i);
-            if (ep.bias && n < ep.nb) v += ep.bias[n];
-            stage[(m - m0) * kStageLd + (n - n0)] = v;
-            if (ep.outt && m < ep.m_store && n < ep.n_store)
-                ep.outt[(size_t)n * ep.ldt + m] = bf16(ep.gelu ? gelu(v) : v);
+#pragma unroll 1
+        for (int c0 = 0; c0 < kBN; c0 += 32) {
+            uint32_t r[32];
+            asm volatile("tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15, %16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31}, [%32];\n"
+                         : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]), "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]), "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
+                         : "r"(taddr + (uint32_t)c0));
+            asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
+            // The bias is added here only for the transposed copy; the row-major pass adds it
+            // per lane (each lane owns 4 fixed columns).
+            float v[32];
+#pragma unroll
+            for (int j = 0; j < 32; ++j) v[j] = __uint_as_float(r[j]);
+            if (ep.outt && ep.bias) {
+#pragma unroll
+                for (int j = 0; j < 32; ++j) {
+                    const int n = n0 + c0 + j;
+                    if (n < ep.nb) v[j] += ep.bias[n];
+                }
+            }
+#pragma unroll
+            for (int j = 0; j < 32; j += 4)
+                *reinterpret_cast<float4*>(&stage[row * kStageLd + c0 + j]) = make_float4(v[j], v[j + 1], v[j + 2], v[j + 3]);
+            if (ep.outt && m0 + row < ep.m_store) {  // v holds the biased values here
+#pragma unroll
+                for (int j = 0; j < 32; ++j) {
+                    const int n = n0 + c0 + j;
+                    if (n < ep.n_store) ep.outt[(size_t)n * ep.ldt + m0 + row] = bf16(ep.gelu ? gelu(v[j]) : v[j]);
+                }
+            }
         }
-        __syncthreads();
+        __syncwarp();
         if (ep.outf || ep.outh) {
+            // vector path: whole 128-column rows, 16-byte FP32 / 8-byte BF16 stores
+            const bool full = n0 + kBN <= ep.n_store;
+            const bool vf = !ep.outf || ((ep.ldf & 3) == 0 && (reinterpret_cast<uintptr_t>(ep.outf) & 15) == 0);
+            const bool vh = !ep.outh || ((ep.ldh & 3) == 0 && (reinterpret_cast<uintptr_t>(ep.outh) & 7) == 0);
+            const int c = lane * 4;
+            // staged values carry the bias already when the transposed copy was written
+            float b[4];
+#pragma unroll
+            for (int j = 0; j < 4; ++j)
+                b[j] = (ep.bias && !ep.outt && n0 + c + j < ep.nb) ? ep.bias[n0 + c + j] : 0.f;
 #pragma unroll 2
             for (int rr = 0; rr < 32; ++rr) {
                 const int r = warp * 32 + rr;
                 const int m = m0 + r;
                 if (m >= ep.m_store) break;
-#pragma unroll
-                for (int q = 0; q < kBN / 32; ++q) {
-                    const int c = q * 32 + lane;
-                    const int n = n0 + c;
-                    if (n >= ep.n_store) continue;
-                    const float v = stage[r * kStageLd + c];
+                float4 q = *reinterpret_cast<const float4*>(&stage[r * kStageLd + c]);
+                q.x += b[0];
+                q.y += b[1];
+                q.z += b[2];
+                q.w += b[3];
+                const float x[4] = {q.x, q.y, q.z, q.w};
+                if (full && vf && vh) {
                     if (ep.outf) {
-                        float* p = ep.outf + (size_t)m * ep.ldf + n;
-                        if (ep.atomic) atomicAdd(p, v);
-                        else *p = v;
+                        float* p = ep.outf + (size_t)m * ep.ldf + n0 + c;
+                        if (ep.atomic) {
+                            atomicAdd(p, x[0]);
+                            atomicAdd(p + 1, x[1]);
+                            atomicAdd(p + 2, x[2]);
+                            atomicAdd(p + 3, x[3]);
+                        } else {
+                            *reinterpret_cast<float4*>(p) = q;
+                        }
                     }
-                    if (ep.outh) ep.outh[(size_t)m * ep.ldh + n] = bf16(ep.gelu ? gelu(v) : v);
+                    if (ep.outh) {
+                        float y[4];
+#pragma unroll
+                        for (int j = 0; j < 4; ++j) y[j] = ep.gelu ? gelu(x[j]) : x[j];
+                        __nv_bfloat162 lo = __floats2bfloat162_rn(y[0], y[1]);
+                        __nv_bfloat162 hi = __floats2bfloat162_rn(y[2], y[3]);
+                        uint2 pk;
+                        pk.x = *reinterpret_cast<uint32_t*>(&lo);
+                        pk.y = *reinterpret_cast<uint32_t*>(&hi);
+                        *reinterpret_cast<uint2*>(ep.outh + (size_t)m * ep.ldh + n0 + c) = pk;
+                    }
+                } else {
+#pragma unroll
+                    for (int j = 0; j < 4; ++j) {
+                        const int n = n0 + c + j;
+                        if (n >= ep.n_store) continue;
+                        if (ep.outf) {
+                            float* p = ep.outf + (size_t)m * ep.ldf + n;
+                            if (ep.atomic) atomicAdd(p, x[j]);
+                            else *p = x[j];
+                        }
+                        if (ep.outh) ep.outh[(size_t)m * ep.ldh + n] = bf16(ep.gelu ? gelu(x[j]) : x[j]);
+                    }
                 }
             }
         }
