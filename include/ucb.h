@@ -140,6 +140,53 @@ UCB_API int ucb_lle2d_device(ucb_engine* e, const ucb_lle2d_request* req, double
                      void* stream, ucb_lle2d_result* res);
 
 /* ------------------------------------------------------------------------------------
+ * Bifurcation 2D (period maps) — replaces ParametricEngine::run_bifurcation_2d
+ * (parametric_engine.h:861, implementation parametric_engine.cpp:5487-5910): per cell of
+ * an n_pts x n_pts grid (same sweep fields and axis mapping as the LLE 2D request) the
+ * trajectory and peaks of the 1-D diagram, then the reference's per-cell dbscan of the
+ * peak values (cudaLibrary.cu:2088-2166, eps_dbscan; intervals weigh 0) whose result is
+ * the cell's "period". values[iy*n + ix] = period, -1 with flag -1 where the dbscan result
+ * is negative (the fixed-point flag of the trajectory); 0 = no peaks / diverged.
+ * ---------------------------------------------------------------------------------- */
+typedef struct ucb_bif2d_request {
+    const char* krs_body;
+    int32_t amount_of_x;
+    const double* initial_conditions;
+    const double* base_values;
+    int32_t n_values;
+    int32_t sweep_over_var, sweep_over_var_2;
+    int32_t sweep_over_h, sweep_over_h_2;
+    int32_t log_scale, log_scale_2;
+    int32_t param_index, var_sweep_index, param_index_2, var_sweep_index_2;
+    double param_lo, param_hi, param_lo_2, param_hi_2;
+    int32_t n_pts;
+    int32_t writable_var;     /* recorded variable; -1 = x0 + pi x1 + e x2 */
+    double h, transient_time, t_max;
+    int32_t pre_scaller;
+    double max_value;
+    double eps_dbscan;        /* > 0 */
+    const char* csv_output_path;
+    const volatile int32_t* cancel;
+    volatile float* progress;
+    ucb_options opt;
+} ucb_bif2d_request;
+
+typedef struct ucb_bif2d_result {
+    double* values;   /* caller-allocated, n_pts * n_pts */
+    int32_t* flags;   /* caller-allocated, n_pts * n_pts: 1 ok, -1 */
+    int32_t ok, cancelled, n_pts;
+    double param_lo, param_hi, param_lo_2, param_hi_2;
+    double min_val, max_val;  /* over cells with flag >= 0 and value >= 0 */
+    double kernel_ms;
+    long long steps;
+    double flops;
+    char error[1024];
+} ucb_bif2d_result;
+
+UCB_API int ucb_run_bif2d(ucb_engine* e, const ucb_bif2d_request* req, ucb_bif2d_result* res);
+UCB_API int ucb_precompile_bif2d(const ucb_bif2d_request* req, char* err_out, int err_len);
+
+/* ------------------------------------------------------------------------------------
  * LLE 1D / LS 1D — replace ParametricEngine::run_lle_1d and run_ls_1d
  * (parametric_engine.h:864-867, implementations parametric_engine.cpp:2196 and :3066):
  * the LLE / spectrum kernels over n_pts values of one swept parameter, initial condition

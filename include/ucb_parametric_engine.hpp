@@ -4,7 +4,8 @@
 // Same class name, same request/result struct names and field names, same result
 // conventions (ok / cancelled / error, NaN or sentinel + flags, row-major iy*n+ix, plane-
 // major spectra), same shared_ptr<atomic<...>> cancel / progress tokens. Every call goes
-// through the C ABI in ucb.h (libucb.so): run_bifurcation_1d, run_lle_2d, run_ls_2d.
+// through the C ABI in ucb.h (libucb.so): run_bifurcation_1d, run_bifurcation_2d,
+// run_lle_2d, run_ls_2d.
 // Entry points of the reference that are not on this path (DFT, Fast Synchro,
 // continuation sweeps) are not provided.
 //
@@ -33,6 +34,16 @@ struct LLE2DSnapshot {
     int par_or_var = 1;
     double tMax = 0.0, NT = 0.0, transientTime = 0.0, h = 0.0, eps = 0.0;
     int indexOfMutVar = 0, indexOfMutVar2 = 0;
+    double range1_lo = 0.0, range1_hi = 0.0, range2_lo = 0.0, range2_hi = 0.0;
+    int n_pts = 0;
+};
+struct Bif2DSnapshot {
+    std::vector<double> values, initial_conditions;
+    int par_or_var = 1;
+    double tMax = 0.0, transientTime = 0.0, h = 0.0;
+    int preScaller = 0;
+    double eps_dbscan = 0.0;
+    int writableVar = 0, indexOfMutVar = 0, indexOfMutVar2 = 0;
     double range1_lo = 0.0, range1_hi = 0.0, range2_lo = 0.0, range2_hi = 0.0;
     int n_pts = 0;
 };
@@ -130,6 +141,56 @@ struct LLE2DResult {
     double min_val = 0.0;
     double max_val = 0.0;
     data_export::LLE2DSnapshot snapshot;
+};
+
+// Bifurcation 2D (parametric_engine.h: Bifurcation2DRequest / Result): period per cell
+// from the reference's dbscan of the peaks; values[iy * n + ix], -1 with flag -1.
+struct Bifurcation2DRequest {
+    std::string krs_body;
+    int amountOfX = 0;
+    std::vector<double> initial_conditions;
+    std::vector<double> base_values;
+    bool sweep_over_var = false;
+    bool sweep_over_h = false;
+    bool log_scale = false;
+    int var_sweep_index = 0;
+    int param_index = 0;
+    bool sweep_over_var_2 = false;
+    bool sweep_over_h_2 = false;
+    bool log_scale_2 = false;
+    int var_sweep_index_2 = 0;
+    int param_index_2 = 0;
+    double param_lo = 0.0;
+    double param_hi = 1.0;
+    double param_lo_2 = 0.0;
+    double param_hi_2 = 1.0;
+    int n_pts = 200;
+    int writable_var = 0;
+    double h = 0.01;
+    double transient_time = 0.0;
+    double t_max = 100.0;
+    int pre_scaller = 1;
+    double max_value = 1.0e6;
+    double eps_dbscan = 0.1;
+    std::string csv_output_path;
+    std::shared_ptr<std::atomic<bool>> cancel;
+    std::shared_ptr<std::atomic<float>> progress;
+};
+
+struct Bifurcation2DResult {
+    bool ok = false;
+    bool cancelled = false;
+    std::string error;
+    int n_pts = 0;
+    double param_lo = 0.0;
+    double param_hi = 1.0;
+    double param_lo_2 = 0.0;
+    double param_hi_2 = 1.0;
+    std::vector<double> values;
+    std::vector<int> flags;
+    double min_val = 0.0;
+    double max_val = 0.0;
+    data_export::Bif2DSnapshot snapshot;
 };
 
 // LS 2D (parametric_engine.h:581-637): full spectrum per cell, the reference's fixed-step
@@ -338,6 +399,86 @@ public:
         s.transientTime = r.transient_time;
         s.h = r.h;
         s.eps = r.eps;
+        s.indexOfMutVar = r.sweep_over_var ? r.var_sweep_index : r.param_index;
+        s.indexOfMutVar2 = r.sweep_over_var_2 ? r.var_sweep_index_2 : r.param_index_2;
+        s.range1_lo = r.param_lo;
+        s.range1_hi = r.param_hi;
+        s.range2_lo = r.param_lo_2;
+        s.range2_hi = r.param_hi_2;
+        s.n_pts = r.n_pts;
+        return res;
+    }
+
+    Bifurcation2DResult run_bifurcation_2d(const Bifurcation2DRequest& r) {
+        Bifurcation2DResult res;
+        if ((int)r.initial_conditions.size() != r.amountOfX) {
+            res.error = "initial_conditions.size() != amountOfX";
+            return res;
+        }
+        ucb_bif2d_request q{};
+        q.krs_body = r.krs_body.c_str();
+        q.amount_of_x = r.amountOfX;
+        q.initial_conditions = r.initial_conditions.data();
+        q.base_values = r.base_values.data();
+        q.n_values = (int)r.base_values.size();
+        q.sweep_over_var = r.sweep_over_var;
+        q.sweep_over_var_2 = r.sweep_over_var_2;
+        q.sweep_over_h = r.sweep_over_h;
+        q.sweep_over_h_2 = r.sweep_over_h_2;
+        q.log_scale = r.log_scale;
+        q.log_scale_2 = r.log_scale_2;
+        q.param_index = r.param_index;
+        q.var_sweep_index = r.var_sweep_index;
+        q.param_index_2 = r.param_index_2;
+        q.var_sweep_index_2 = r.var_sweep_index_2;
+        q.param_lo = r.param_lo;
+        q.param_hi = r.param_hi;
+        q.param_lo_2 = r.param_lo_2;
+        q.param_hi_2 = r.param_hi_2;
+        q.n_pts = r.n_pts;
+        q.writable_var = r.writable_var;
+        q.h = r.h;
+        q.transient_time = r.transient_time;
+        q.t_max = r.t_max;
+        q.pre_scaller = r.pre_scaller;
+        q.max_value = r.max_value;
+        q.eps_dbscan = r.eps_dbscan;
+        q.csv_output_path = r.csv_output_path.c_str();
+        int32_t cancel_now = (r.cancel && r.cancel->load()) ? 1 : 0;
+        q.cancel = &cancel_now;
+        float prog = 0.0f;
+        q.progress = &prog;
+        q.opt = opt_;
+        const size_t cells = r.n_pts > 0 ? (size_t)r.n_pts * (size_t)r.n_pts : 0;
+        res.values.assign(cells, 0.0);
+        std::vector<int32_t> f32(cells);
+        ucb_bif2d_result o{};
+        o.values = res.values.data();
+        o.flags = f32.data();
+        ucb_run_bif2d(e_, &q, &o);
+        if (r.progress) r.progress->store(prog);
+        res.ok = o.ok != 0;
+        res.cancelled = o.cancelled != 0;
+        res.error = o.error;
+        if (!res.ok) return res;
+        res.flags.assign(f32.begin(), f32.end());
+        res.n_pts = o.n_pts;
+        res.param_lo = o.param_lo;
+        res.param_hi = o.param_hi;
+        res.param_lo_2 = o.param_lo_2;
+        res.param_hi_2 = o.param_hi_2;
+        res.min_val = o.min_val;
+        res.max_val = o.max_val;
+        auto& s = res.snapshot;
+        s.values = r.base_values;
+        s.initial_conditions = r.initial_conditions;
+        s.par_or_var = (r.sweep_over_var == r.sweep_over_var_2) ? (r.sweep_over_var ? 0 : 1) : 2;
+        s.tMax = r.t_max;
+        s.transientTime = r.transient_time;
+        s.h = r.h;
+        s.preScaller = r.pre_scaller;
+        s.eps_dbscan = r.eps_dbscan;
+        s.writableVar = r.writable_var;
         s.indexOfMutVar = r.sweep_over_var ? r.var_sweep_index : r.param_index;
         s.indexOfMutVar2 = r.sweep_over_var_2 ? r.var_sweep_index_2 : r.param_index_2;
         s.range1_lo = r.param_lo;

@@ -631,6 +631,55 @@ int threads_or_default(int nthreads) {
 // ============================================================================
 // C ABI of the oracle (used from Python through ctypes in tests/ and bench.py)
 // ============================================================================
+// dbscan of cudaLibrary.cu:2088-2166 (per-cell peak clustering of run_bif2d): the
+// reference's loop as it is, including the stack slots written at amountOfPeaks + k and
+// popped at amountOfPeaks + NumNeibor - 1, the inner bound amountOfPeaks - 1, the labels
+// and stack held in numb, and the result cluster - 1. mult_peak = 1, mult_interval = 0
+// (configCUDA.h), so the intervals enter the distance as zeros.
+template <class T>
+T dbscan_distance(T x1, T y1, T x2, T y2) {
+    if (x1 == x2 && y1 == y2) return 0;
+    const T dx = std::fabs(x2 - x1), dy = std::fabs(y2 - y1);
+    return std::sqrt(dx * dx + dy * dy);
+}
+
+template <class T>
+int dbscan_peaks(const T* peaks, int P, T eps, std::vector<T>& helpful) {
+    if (P == -1) return -1;
+    if (P == 0) return 0;
+    if (P == 1) return 1;
+    std::vector<T> data(peaks, peaks + P), iv((size_t)P, (T)0);
+    for (int i = 0; i < P; ++i) {
+        data[i] = data[i] * (T)1.0;
+        iv[i] = iv[i] * (T)0.0;
+    }
+    helpful.assign((size_t)2 * P + 1, (T)0);
+    int cluster = 0, NumNeibor = 0;
+    for (size_t i = 0; i < (size_t)P; i++) {
+        if (NumNeibor >= 1) {
+            i = (size_t)helpful[(size_t)P + NumNeibor - 1];
+            helpful[(size_t)P + NumNeibor - 1] = 0;
+            NumNeibor = NumNeibor - 1;
+        } else if (helpful[i] == 0) {
+            NumNeibor = 0;
+            ++cluster;
+            helpful[i] = (T)cluster;
+        } else {
+            continue;
+        }
+        for (int k = 0; k < P - 1; k++) {
+            if (i != (size_t)k && helpful[k] == 0) {
+                if (dbscan_distance<T>(data[i], iv[i], data[k], iv[k]) < eps) {
+                    helpful[k] = (T)cluster;
+                    helpful[(size_t)P + k] = (T)k;
+                    ++NumNeibor;
+                }
+            }
+        }
+    }
+    return cluster - 1;
+}
+
 extern "C" {
 
 const char* orc_last_error() { return g_err.c_str(); }
@@ -865,6 +914,70 @@ int orc_ls2d(void* h, int nPts, int par_or_var, int idx0, int idx1, const double
             if (outv[m] == 999.0 || outv[m] == -999.0) bad = true;
         }
         flags[cells ? c : cell] = bad ? -1 : 1;
+    }
+    return 0;
+}
+
+// Bifurcation 2D (run_bif2d, parametric_engine.cpp:5487-5910): per cell the bif1d
+// trajectory + peakFinder, then dbscan of the peaks; values[out] = period (-1 when the
+// dbscan result is negative), flags[out] = -1 / 1; out = cell, transposed with swap_xy
+// (with a cell list, out = list position).
+int orc_bif2d(void* h, int nPts, int par_or_var, int idx0, int idx1, const double* ranges, int log_mask,
+              int h_axis, int swap_xy, const double* ic, int nv, const double* vals, double hstep, double transient,
+              double tMax, int preScaller, int writableVar, double maxv, double eps_dbscan, const long long* cells,
+              long long ncells, double* values, int* flags, int nthreads) {
+    Krs* k = static_cast<Krs*>(h);
+    const int nx = k->nx;
+    Grid g{nPts, 2, par_or_var, {idx0, idx1}, {ranges[0], ranges[1], ranges[2], ranges[3]}, log_mask, h_axis};
+    const double r_h = h_axis == 0 ? ranges[0] : (h_axis == 1 ? ranges[2] : hstep);
+    const double worstCaseH = (h_axis != -1) ? (k->numb_bytes == 8 ? r_h : (double)(float)r_h) : hstep;
+    const long long amountOfPointsInBlock = (long long)std::ceil(tMax / worstCaseH / preScaller);
+    const long long amountOfPointsForSkip = (long long)(transient / hstep);
+    if (amountOfPointsInBlock <= 0) { g_err = "computed amountOfPointsInBlock <= 0"; return -1; }
+    const long long total = (long long)nPts * nPts;
+    const long long n = cells ? ncells : total;
+#pragma omp parallel num_threads(threads_or_default(nthreads))
+    {
+        std::vector<double> d8, p8, t8, h8;
+        std::vector<float> d4, p4, t4, h4;
+#pragma omp for schedule(dynamic, 1)
+        for (long long c = 0; c < n; ++c) {
+            const long long idx = cells ? cells[c] : c;
+            int period = 0;
+            auto run = [&](auto tag, auto& dd, auto& pp, auto& tt, auto& hh) {
+                using T = decltype(tag);
+                StepFn<T> f = Dispatch<T>::fn(k);
+                CellInit<T> ci;
+                init_cell<T>(g, idx, nx, ic, nv, vals, hstep, &ci);
+                const T hl = ci.h;
+                int cnt;
+                if (!(hl > 0)) {
+                    cnt = -1;
+                } else {
+                    long long skip_l = amountOfPointsForSkip, iters_l = amountOfPointsInBlock;
+                    if (g.h_axis != -1) {
+                        skip_l = (long long)std::ceil((T)transient / hl);
+                        iters_l = (long long)std::ceil((T)tMax / hl / (T)preScaller);
+                    }
+                    if (iters_l > amountOfPointsInBlock) iters_l = amountOfPointsInBlock;
+                    dd.assign((size_t)iters_l, (T)0);
+                    pp.assign((size_t)iters_l, (T)0);
+                    tt.assign((size_t)iters_l, (T)0);
+                    int flag = loop_model<T>(f, ci.x, ci.a, hl, skip_l, nx, preScaller, writableVar, (T)maxv, nullptr);
+                    if (flag == 1 || flag == -1)
+                        flag = loop_model<T>(f, ci.x, ci.a, hl, iters_l, nx, preScaller, writableVar, (T)maxv, dd.data());
+                    if (flag == -1 || flag == 0) cnt = flag;
+                    else cnt = peak_finder<T>(dd.data(), iters_l, pp.data(), tt.data(), (T)(hstep * (double)preScaller));
+                }
+                period = dbscan_peaks<T>(pp.data(), cnt, (T)eps_dbscan, hh);
+            };
+            if (k->numb_bytes == 8) run(0.0, d8, p8, t8, h8);
+            else run(0.0f, d4, p4, t4, h4);
+            long long out = cells ? c : idx;
+            if (!cells && swap_xy) out = (idx % nPts) * nPts + idx / nPts;
+            values[out] = period < 0 ? -1.0 : (double)period;
+            flags[out] = period < 0 ? -1 : 1;
+        }
     }
     return 0;
 }

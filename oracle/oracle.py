@@ -53,6 +53,11 @@ def lib():
                                 C.c_void_p, C.c_int, C.c_void_p, C.c_double, C.c_double, C.c_double,
                                 C.c_int, C.c_int, C.c_double, C.c_int, C.c_void_p, C.c_longlong,
                                 C.c_void_p, C.c_void_p, C.c_void_p, C.c_int]
+        L.orc_bif2d.restype = C.c_int
+        L.orc_bif2d.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_int, C.c_void_p, C.c_int, C.c_int,
+                                C.c_int, C.c_void_p, C.c_int, C.c_void_p, C.c_double, C.c_double, C.c_double,
+                                C.c_int, C.c_int, C.c_double, C.c_double, C.c_void_p, C.c_longlong, C.c_void_p,
+                                C.c_void_p, C.c_int]
         L.orc_rhs_compile.restype = C.c_void_p
         L.orc_rhs_compile.argtypes = [C.c_char_p, C.c_int, C.c_int]
         L.orc_ls2d_dp5.restype = C.c_int
@@ -152,6 +157,30 @@ def lle2d(krs: Krs, g: dict, cells=None, nthreads=0):
 
 def ls2d(krs: Krs, g: dict, cells=None, nthreads=0):
     return _grid(lib().orc_ls2d, krs, g, cells, nthreads, krs.nx)
+
+
+def bif2d(krs: Krs, g: dict, eps_dbscan: float, pre_scaller=1, writable_var=0, cells=None, nthreads=0):
+    """run_bif2d semantics: per-cell period from the reference's peak dbscan (values in
+    user order, -1 with flag -1 where the dbscan result is negative). g: kernel-level grid
+    dict (see tests/helpers; NT / eps unused)."""
+    n = g["n_pts"]
+    ranges = np.array(g["ranges"], dtype=np.float64)
+    ic = np.array(g["ic"], dtype=np.float64)
+    vals = np.array(g["values"], dtype=np.float64)
+    if cells is not None:
+        cells = np.ascontiguousarray(cells, dtype=np.int64)
+        m = len(cells)
+    else:
+        m = n * n
+    values = np.zeros(m, dtype=np.float64)
+    flags = np.zeros(m, dtype=np.int32)
+    rc = lib().orc_bif2d(krs.h, n, g["par_or_var"], g["idx"][0], g["idx"][1], _ptr(ranges), g.get("log_mask", 0),
+                         g.get("h_axis", -1), int(g.get("swap_xy", 0)), _ptr(ic), len(vals), _ptr(vals), g["h"],
+                         g["transient_time"], g["t_max"], pre_scaller, writable_var, g["max_value"], eps_dbscan,
+                         _ptr(cells), m if cells is not None else 0, _ptr(values), _ptr(flags), nthreads)
+    if rc != 0:
+        raise RuntimeError(lib().orc_last_error().decode())
+    return values, flags
 
 
 def bif1d(krs: Krs, b: dict, max_out=64, pts=None, nthreads=0):

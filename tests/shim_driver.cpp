@@ -1,6 +1,6 @@
 // Drives the header-only ParametricEngine shim the way the reference's session layer
 // calls ParametricEngine (analysis_session.cpp builds a Request, calls run_*, reads the
-// Result). argv[1] = "invalid" (no GPU needed) or "lle2d" / "ls2d" / "bif1d" (GPU); the RK4 body
+// Result). argv[1] = "invalid" (no GPU needed) or "lle2d" / "ls2d" / "bif1d" / "bif2d" (GPU); the RK4 body
 // is read from stdin.
 #include <cstdio>
 #include <cstring>
@@ -31,6 +31,22 @@ int main(int argc, char** argv) {
                     res.min_val, res.max_val, r.progress->load());
         if (mode == "lle2d")
             for (size_t i = 0; i < res.values.size(); ++i) std::printf("%.17g %d\n", res.values[i], res.flags[i]);
+        return 0;
+    }
+    if (mode == "bif2d") {
+        Bifurcation2DRequest r;
+        r.krs_body = body;
+        r.amountOfX = 3;
+        r.initial_conditions = {0.1, 0.1, 0.1};
+        r.base_values = {0, 10.0, 28.0, 8.0 / 3.0};
+        r.param_index = 2;
+        r.param_index_2 = 1;
+        r.param_lo = 20; r.param_hi = 200; r.param_lo_2 = 5.0; r.param_hi_2 = 15.0;
+        r.n_pts = 6;
+        r.h = 0.01; r.transient_time = 20; r.t_max = 60; r.eps_dbscan = 0.1;
+        Bifurcation2DResult res = eng.run_bifurcation_2d(r);
+        std::printf("ok=%d error=%s n=%d max=%g\n", (int)res.ok, res.error.c_str(), res.n_pts, res.max_val);
+        for (size_t i = 0; i < res.values.size(); ++i) std::printf("%.17g %d\n", res.values[i], res.flags[i]);
         return 0;
     }
     if (mode == "ls2d") {

@@ -60,3 +60,17 @@ def test_shim_ls2d_equals_c_abi(driver):
                            transient_time=5, t_max=20, NT=0.5, opt=ucb.options(precision=ucb.PREC_F64))
     ref, _, _ = eng.run_ls2d(req)
     np.testing.assert_array_equal(vals, ref.ravel())
+
+
+@pytest.mark.gpu
+def test_shim_bif2d_equals_c_abi(driver):
+    """run_bifurcation_2d through the shim returns what ucb_run_bif2d returns."""
+    out = run(driver, "bif2d", rk4_body(LORENZ)).splitlines()
+    assert out[0].startswith("ok=1 error= n=6")
+    vals = np.array([float(l.split()[0]) for l in out[1:]])
+    eng = ucb.Engine(0)
+    req = eng.bif2d_request(rk4_body(LORENZ), 3, (0.1, 0.1, 0.1), (0, 10.0, 28.0, 8.0 / 3.0), n_pts=6, param_index=2,
+                            param_index_2=1, param_lo=20, param_hi=200, param_lo_2=5.0, param_hi_2=15.0, h=0.01,
+                            transient_time=20, t_max=60, eps_dbscan=0.1)
+    ref, _, _ = eng.run_bif2d(req)
+    np.testing.assert_array_equal(vals, ref)

@@ -123,6 +123,30 @@ void ls2d(const std::string& path, const Common& c, int par_or_var, double tMax,
     }
 }
 
+void bif2d(const std::string& path, const Common& c, int par_or_var, double tMax, double transient, double h,
+           int pre, double eps_dbscan, int writable_var, int idx1, int idx2, double r1lo, double r1hi, double r2lo,
+           double r2hi, int n_pts, const double* values) {
+    {
+        std::ofstream cfg(path + "_config.csv");
+        if (!cfg) return;
+        cfg << std::setprecision(kPrecision);
+        cfg << "2D bifurcation (DBSCAN)\n";
+        par_or_var_line(cfg, par_or_var);
+        values_and_ic(cfg, c);
+        cfg << "CT = " << tMax << "\nTT = " << transient << "\nh = " << h << "\ndecimator = " << pre << "\n";
+        cfg << "eps_DBSCAN = " << eps_dbscan << "\n";
+        cfg << "indexVar for peakfinder = " << writable_var << "\n";
+        cfg << "indices = " << idx1 << ", " << idx2 << "\n";
+        cfg << "axis1: " << r1lo << " .. " << r1hi << "\n";
+        cfg << "axis2: " << r2lo << " .. " << r2hi << "\n";
+        cfg << "n_pts = " << n_pts << "x" << n_pts << "\n";
+    }
+    std::ofstream out(path);
+    if (!out) return;
+    out << std::setprecision(kPrecision);
+    grid(out, n_pts, values);
+}
+
 void curve1d(const std::string& path, const char* title, const Common& c, double tMax, double NT, double transient,
              double h, double eps, int index, double lo, double hi, bool log_scale, int n_pts, int n_cols,
              const double* v) {

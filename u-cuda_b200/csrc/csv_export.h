@@ -26,6 +26,11 @@ void ls2d(const std::string& path, const Common& c, int par_or_var, double tMax,
           double h, double eps, int idx1, int idx2, double r1lo, double r1hi, double r2lo, double r2hi, int n_pts,
           int n_exp, const double* plane_major_values);
 
+// 2-D bifurcation (data_export.cpp write_bif2d_config / write_bif2d_grid).
+void bif2d(const std::string& path, const Common& c, int par_or_var, double tMax, double transient, double h,
+           int pre, double eps_dbscan, int writable_var, int idx1, int idx2, double r1lo, double r1hi, double r2lo,
+           double r2hi, int n_pts, const double* values);
+
 // 1-D LLE / LS (data_export.cpp write_lle1d_config / write_ls1d_config + rows): config
 // title "1D LLE" or "1D LS", rows "param, v0[, v1, ...]" with the parameter value of
 // getValueByIdx(_log)_local (parametric_engine.cpp:577-590).

@@ -60,27 +60,37 @@ __device__ __forceinline__ numb recorded_value(const numb* x, int wv) {
     return x[wv];
 }
 
+// Where the peaks of one point go: the first max_out peaks and intervals of a 1-D
+// diagram (Bif1dSink), or every peak the 2-D period count clusters (Bif2dSink).
+struct Bif1dSink {
+    double* peaks;
+    double* intervals;
+    int max_out;
+    numb time_step;
+    __device__ __forceinline__ void put(int k, numb value, numb dt) const {
+        if (k < max_out) {
+            peaks[k] = (double)value;
+            intervals[k] = (double)((numb)dt * time_step);
+        }
+    }
+};
+
 // Emits a peak at position j with the reference's interpolation.
-__device__ __forceinline__ void emit_peak(PeakScan& s, long long j, const UcbBifParams& p, long long cell) {
+template <class Sink>
+__device__ __forceinline__ void emit_peak(PeakScan& s, long long j, const Sink& sink) {
     numb denom = s.d0 - (numb)2.0 * s.d1 + s.d2;
     numb delta = 0.0;
     if (fabs(denom) > 1e-12) delta = 0.5 * (s.d0 - s.d2) / denom;
     const numb value = s.d1 - 0.25 * (s.d0 - s.d2) * delta;
     const numb t = (numb)(j - 1) + delta;
-    if (s.found > 0) {
-        const int k = s.found - 1;
-        if (k < p.max_out) {
-            p.out_peaks[cell * p.max_out + k] = (double)value;
-            p.out_intervals[cell * p.max_out + k] = (double)((numb)(t - s.prev_t) * p.time_step);
-        }
-    }
+    if (s.found > 0) sink.put(s.found - 1, value, t - s.prev_t);
     s.prev_t = t;
     s.found += 1;
 }
 
 // Feeds sample index q (value v). Decides position q-1.
-__device__ __forceinline__ void scan_push(PeakScan& s, long long q, numb v, long long n, const UcbBifParams& p,
-                                          long long cell) {
+template <class Sink>
+__device__ __forceinline__ void scan_push(PeakScan& s, long long q, numb v, long long n, const Sink& sink) {
     s.d0 = s.d1;
     s.d1 = s.d2;
     s.d2 = v;
@@ -91,7 +101,7 @@ __device__ __forceinline__ void scan_push(PeakScan& s, long long q, numb v, long
             s.plateau = false;
             s.next_i = pos + 2;
         } else if (s.d1 - s.d2 > (numb)kEpsPeakDelta) {
-            emit_peak(s, pos, p, cell);
+            emit_peak(s, pos, sink);
             s.plateau = false;
             s.next_i = pos + 2;
         }
@@ -101,7 +111,7 @@ __device__ __forceinline__ void scan_push(PeakScan& s, long long q, numb v, long
     if (s.d1 - s.d0 > (numb)kEpsPeakDelta && s.d1 > (numb)kPeakThreshold && s.d1 >= s.d2) {
         // inner loop starts at j = i with the same window
         if (s.d1 - s.d2 > (numb)kEpsPeakDelta) {
-            emit_peak(s, pos, p, cell);
+            emit_peak(s, pos, sink);
             s.next_i = pos + 2;
         } else {
             s.plateau = true;
@@ -109,12 +119,11 @@ __device__ __forceinline__ void scan_push(PeakScan& s, long long q, numb v, long
     }
 }
 
-template <class S>
+template <class S, class Sink>
 __device__ __forceinline__ int loop_record(const S& st, numb* x, const numb* a, numb h, long long iters, int pre,
-                                           int wv, numb maxv, PeakScan& scan, const UcbBifParams& p, long long cell,
-                                           long long& ns) {
+                                           int wv, numb maxv, PeakScan& scan, const Sink& sink, long long& ns) {
     for (long long i = 0; i < iters; ++i) {
-        scan_push(scan, i, recorded_value(x, wv), iters, p, cell);
+        scan_push(scan, i, recorded_value(x, wv), iters, sink);
         for (int j = 0; j < pre; ++j) st.step(x, a, h);
         ns += pre;
         if (i % kCheckInterval == 0 && diverged(x, maxv)) return 0;
@@ -149,6 +158,7 @@ __device__ __forceinline__ int loop_transient(const S& st, numb* x, const numb* 
 
 }  // namespace ucbdev
 
+#if !defined(UCB_BIF2D)
 extern "C" __global__ void __launch_bounds__(128) ucb_bif_kernel(const UcbBifParams p) {
     const long long cell = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     const int lane = threadIdx.x & 31;
@@ -181,7 +191,9 @@ extern "C" __global__ void __launch_bounds__(128) ucb_bif_kernel(const UcbBifPar
                 ucbdev::PeakScan scan;
                 scan.init();
                 scan.d1 = scan.d2 = 0;
-                flag = ucbdev::loop_record(st, x, a, h, iters, p.pre_scaller, p.writable_var, p.maxv, scan, p, cell, ns);
+                const ucbdev::Bif1dSink sink{p.out_peaks + cell * p.max_out, p.out_intervals + cell * p.max_out,
+                                             p.max_out, p.time_step};
+                flag = ucbdev::loop_record(st, x, a, h, iters, p.pre_scaller, p.writable_var, p.maxv, scan, sink, ns);
                 if (flag == 1) {
                     int n = (scan.found > 1) ? scan.found - 1 : 0;
                     if (n >= ucbdev::kMaxAmountOfPeaks) n = ucbdev::kMaxAmountOfPeaks;
@@ -197,3 +209,160 @@ extern "C" __global__ void __launch_bounds__(128) ucb_bif_kernel(const UcbBifPar
     }
     ucbdev::warp_add_steps(p.steps, ns, lane);
 }
+#endif  // !UCB_BIF2D
+
+#if defined(UCB_BIF2D)
+// ---------------------------------------------------------------------------------------
+// 2-D bifurcation (period) maps: run_bif2d (parametric_engine.cpp:5487-5910) = per cell the
+// 1-D trajectory + peakFinder above, then dbscan of the peaks (cudaLibrary.cu:2088-2166,
+// dbscanCUDA :2321) whose cluster count is the "period". The reference keeps the whole
+// recorded series, the peaks, the intervals and a helper array per cell in HBM and runs
+// three kernels; here the peaks stream straight into a per-cell slice of a scratch buffer
+// (interleaved: entry k of local cell i at k * total + i, so that a warp's accesses to
+// the same k are adjacent) and the same thread clusters them.
+struct UcbBif2dParams {
+    long long total;           // cells in this launch (one chunk)
+    long long cell_offset;     // first kernel cell of the chunk
+    int n_pts;
+    int swap_xy;               // 1: write transposed (user X = kernel axis 1)
+    int pre_scaller;
+    int writable_var;
+    int cap;                   // peaks kept per cell (>= the largest possible count)
+    int pad0;
+    long long skip;            // (int)(transient / h), host double arithmetic
+    long long iters;           // ceil(tMax / worstCaseH / preScaller), host double arithmetic
+    numb h, maxv, transient, tmax, eps;
+    numb ic[UCB_NX];
+    numb vals[UCB_NV];
+    const numb* axis0;
+    const numb* axis1;
+    numb* peaks;               // cap x total
+    numb* helpful;             // (2 cap + 1) x total: dbscan labels [0, P), stack slots [P, 2P)
+    double* out_values;        // period (-1 where the dbscan result is negative)
+    int* out_flags;            // -1 / 1
+    unsigned long long* counter;
+    unsigned long long* steps;
+};
+
+namespace ucbdev {
+
+struct Bif2dSink {
+    numb* peaks;
+    long long stride;
+    int cap;
+    __device__ __forceinline__ void put(int k, numb value, numb) const {
+        if (k < cap) peaks[(long long)k * stride] = value;
+    }
+};
+
+__device__ __forceinline__ numb dbscan_distance(numb x1, numb y1, numb x2, numb y2) {
+    if (x1 == x2 && y1 == y2) return 0;
+    const numb dx = fabs(x2 - x1), dy = fabs(y2 - y1);
+    return sqrt(dx * dx + dy * dy);
+}
+
+// The reference's dbscan step for step: labels and stack in numb, stack slots written at
+// P + k and popped at P + NumNeibor - 1, inner bound P - 1, result cluster - 1. Peaks enter
+// times mult_peak (1) and intervals times mult_interval (0) (configCUDA.h).
+__device__ __forceinline__ int dbscan_cell(const numb* peaks, numb* helpful, long long stride, int P, numb eps) {
+    if (P == -1) return -1;
+    if (P == 0) return 0;
+    if (P == 1) return 1;
+    for (int k = 0; k < 2 * P + 1; ++k) helpful[(long long)k * stride] = 0;
+    const numb y = (numb)0.0 * (numb)0.0;
+    int cluster = 0, nn = 0;
+    for (unsigned long long i = 0; i < (unsigned long long)P; i++) {
+        if (nn >= 1) {
+            const long long slot = ((long long)P + nn - 1) * stride;
+            i = (unsigned long long)helpful[slot];
+            helpful[slot] = 0;
+            nn = nn - 1;
+        } else if (helpful[(long long)i * stride] == 0) {
+            nn = 0;
+            ++cluster;
+            helpful[(long long)i * stride] = (numb)cluster;
+        } else {
+            continue;
+        }
+        const numb xi = peaks[(long long)i * stride] * (numb)1.0;
+        for (int k = 0; k < P - 1; k++) {
+            if (i != (unsigned long long)k && helpful[(long long)k * stride] == 0) {
+                if (dbscan_distance(xi, y, peaks[(long long)k * stride] * (numb)1.0, y) < eps) {
+                    helpful[(long long)k * stride] = (numb)cluster;
+                    helpful[((long long)P + k) * stride] = (numb)k;
+                    ++nn;
+                }
+            }
+        }
+    }
+    return cluster - 1;
+}
+
+// One cell of a 2-D period map.
+__device__ __forceinline__ void bif2d_cell(const UcbBif2dParams& p, long long i, long long& ns) {
+    const long long kidx = p.cell_offset + i;
+    const ucbdev::CellAxes c = ucbdev::cell_axes(kidx, p.n_pts);
+    numb x[UCB_NX], a[UCB_NV];
+#pragma unroll
+    for (int k = 0; k < UCB_NX; ++k) x[k] = p.ic[k];
+#pragma unroll
+    for (int k = 0; k < UCB_NV; ++k) a[k] = p.vals[k];
+    ucbdev::apply_sweep(c, p.axis0, p.axis1, x, a);
+    numb h = p.h;
+    long long skip = p.skip, iters = p.iters;
+#if UCB_HAXIS == 0 || UCB_HAXIS == 1
+#if UCB_HAXIS == 0
+    h = p.axis0[c.i0];
+#else
+    h = p.axis1[c.i1];
+#endif
+    skip = (long long)ceil(p.transient / h);
+    const long long il = (long long)ceil(p.tmax / h / (numb)p.pre_scaller);
+    iters = il > p.iters ? p.iters : il;
+#endif
+    int count;
+    if (!(h > 0)) {
+        count = -1;
+    } else {
+        const ucbdev::Stepper st(h);
+        int flag = ucbdev::loop_transient(st, x, a, h, skip, p.pre_scaller, p.maxv, ns);
+        if (flag == 1 || flag == -1) {
+            ucbdev::PeakScan scan;
+            scan.init();
+            scan.d1 = scan.d2 = 0;
+            const ucbdev::Bif2dSink sink{p.peaks + i, p.total, p.cap};
+            flag = ucbdev::loop_record(st, x, a, h, iters, p.pre_scaller, p.writable_var, p.maxv, scan, sink, ns);
+            if (flag == 1) {
+                int n = (scan.found > 1) ? scan.found - 1 : 0;
+                if (n >= ucbdev::kMaxAmountOfPeaks) n = ucbdev::kMaxAmountOfPeaks;
+                count = (iters < 5) ? 0 : n;
+            } else {
+                count = flag;
+            }
+        } else {
+            count = flag;
+        }
+    }
+    if (count > p.cap) count = p.cap;  // cannot happen: cap covers the largest count
+    const int period = ucbdev::dbscan_cell(p.peaks + i, p.helpful + i, p.total, count, p.eps);
+    long long out = kidx;
+    if (p.swap_xy) out = (kidx % p.n_pts) * p.n_pts + kidx / p.n_pts;
+    p.out_values[out] = period < 0 ? -1.0 : (double)period;
+    p.out_flags[out] = period < 0 ? -1 : 1;
+}
+
+}  // namespace ucbdev
+
+extern "C" __global__ void __launch_bounds__(128) ucb_bif2d_kernel(const UcbBif2dParams p) {
+    const int lane = threadIdx.x & 31;
+    long long ns = 0;
+    for (;;) {
+        const long long base = ucbdev::warp_fetch(p.counter, lane);
+        if (base >= p.total) break;
+        const long long i = base + lane;
+        if (i < p.total) ucbdev::bif2d_cell(p, i, ns);
+    }
+    ucbdev::warp_add_steps(p.steps, ns, lane);
+}
+#endif  // UCB_BIF2D
+

@@ -1,0 +1,278 @@
+// Bifurcation 2D (period maps) host orchestration: run_bif2d (parametric_engine.cpp:
+// 5487-5910) — its validation, the LLE-2D axis mapping (par_or_var / swap_xy / h axis),
+// amountOfPointsInBlock = ceil(tMax / worstCaseH / preScaller) and (int)(transient / h) in
+// double, values = period (-1 with flag -1 where the dbscan result is negative), min / max
+// over the other cells, CSV. The reference chunks the grid by free memory because it
+// keeps the whole recorded series of every cell; here one kernel integrates, captures the
+// peaks into a per-cell scratch slice and clusters them (ucb_bif.cuh), and the grid is
+// chunked only by the size of that peak scratch.
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <limits>
+
+#include "csv_export.h"
+#include "engine_internal.h"
+
+using namespace ucb;
+
+namespace {
+
+constexpr int kMaxAmountOfX = 32;
+constexpr int kMaxAmountOfValues = 64;
+constexpr int kMaxAmountOfPeaks = 2500;  // configCUDA.h max_amount_of_peaks
+
+int fail(ucb_engine* e, ucb_bif2d_result* r, int code, const std::string& msg) {
+    e->last_error = msg;
+    std::snprintf(r->error, sizeof r->error, "%s", msg.c_str());
+    r->ok = 0;
+    return code;
+}
+
+// The LLE-2D request with the same sweep fields (its own NT / eps checks are satisfied by
+// placeholders: the period map has no blocks).
+ucb_lle2d_request as_lle(const ucb_bif2d_request& q) {
+    ucb_lle2d_request l{};
+    l.krs_body = q.krs_body;
+    l.amount_of_x = q.amount_of_x;
+    l.initial_conditions = q.initial_conditions;
+    l.base_values = q.base_values;
+    l.n_values = q.n_values;
+    l.sweep_over_var = q.sweep_over_var;
+    l.sweep_over_var_2 = q.sweep_over_var_2;
+    l.sweep_over_h = q.sweep_over_h;
+    l.sweep_over_h_2 = q.sweep_over_h_2;
+    l.log_scale = q.log_scale;
+    l.log_scale_2 = q.log_scale_2;
+    l.param_index = q.param_index;
+    l.var_sweep_index = q.var_sweep_index;
+    l.param_index_2 = q.param_index_2;
+    l.var_sweep_index_2 = q.var_sweep_index_2;
+    l.param_lo = q.param_lo;
+    l.param_hi = q.param_hi;
+    l.param_lo_2 = q.param_lo_2;
+    l.param_hi_2 = q.param_hi_2;
+    l.n_pts = q.n_pts;
+    l.h = q.h;
+    l.transient_time = q.transient_time;
+    l.t_max = q.t_max;
+    l.NT = q.t_max;
+    l.eps = 1.0;
+    l.max_value = q.max_value;
+    l.opt = q.opt;
+    return l;
+}
+
+// Validation of run_bif2d (parametric_engine.cpp:5490-5572) and the axis mapping.
+bool plan_bif2d(const ucb_bif2d_request& q, SweepMap& m, std::string& err) {
+    if (!q.krs_body || !*q.krs_body) { err = "krs_body is empty"; return false; }
+    if (q.amount_of_x <= 0 || q.amount_of_x > kMaxAmountOfX) { err = "amountOfX out of [1,32]"; return false; }
+    if (!q.initial_conditions) { err = "initial_conditions.size() != amountOfX"; return false; }
+    if (q.n_values > kMaxAmountOfValues) { err = "too many base_values"; return false; }
+    if (q.n_pts <= 0) { err = "n_pts must be > 0"; return false; }
+    if (!(q.h > 0.0)) { err = "h must be > 0"; return false; }
+    if (!(q.t_max > 0.0)) { err = "t_max must be > 0"; return false; }
+    if (q.transient_time < 0) { err = "transient_time must be >= 0"; return false; }
+    if (q.pre_scaller <= 0) { err = "pre_scaller must be > 0"; return false; }
+    if (!(q.eps_dbscan > 0.0)) { err = "eps_dbscan must be > 0"; return false; }
+    if (q.writable_var < -1 || q.writable_var >= q.amount_of_x) { err = "writable_var out of range"; return false; }
+    if ((q.sweep_over_h != 0) != (q.sweep_over_h_2 != 0)) {  // one h axis (both: rejected below)
+        if (q.param_lo <= 0.0 || q.param_hi <= 0.0 || q.param_lo_2 <= 0.0 || q.param_hi_2 <= 0.0) {
+            err = "h lo/hi must be > 0 with sweep_over_h / sweep_over_h_2";
+            return false;
+        }
+    }
+    int n_blocks = 0, skip = 0;
+    long long nt = 0;
+    return plan_sweep2d(as_lle(q), m, n_blocks, skip, nt, err);
+}
+
+CompileRequest bif2d_compile_request(const ucb_bif2d_request& q, const SweepMap& m, SystemCode& sys) {
+    sys = make_system_code(q.krs_body, q.amount_of_x, q.n_values, q.opt.precision, q.opt.mode, false);
+    CompileRequest rq;
+    rq.name = "ucb_bif2d.cu";
+    rq.source = make_prelude(q.opt.precision, q.amount_of_x, q.n_values, m, true, sys, {"UCB_BIF2D 1"}) +
+                "#include \"ucb_device.cuh\"\n#include \"ucb_bif.cuh\"\n";
+    rq.headers = device_headers();
+    rq.options.push_back(sys.exact ? "--fmad=false" : "--fmad=true");
+    rq.kernels = {"ucb_bif2d_kernel"};
+    return rq;
+}
+
+}  // namespace
+
+extern "C" int ucb_precompile_bif2d(const ucb_bif2d_request* req, char* err_out, int err_len) {
+    std::string err;
+    SweepMap m;
+    if (!req || !plan_bif2d(*req, m, err)) {
+        if (err_out && err_len > 0) std::snprintf(err_out, (size_t)err_len, "%s", err.c_str());
+        return UCB_E_INVALID;
+    }
+    SystemCode sys;
+    CompileRequest rq = bif2d_compile_request(*req, m, sys);
+    if (!precompile_to_disk(rq, err)) {
+        if (err_out && err_len > 0) std::snprintf(err_out, (size_t)err_len, "%s", err.c_str());
+        return UCB_E_COMPILE;
+    }
+    if (err_out && err_len > 0) std::snprintf(err_out, (size_t)err_len, "%s", sys.note.c_str());
+    return UCB_OK;
+}
+
+extern "C" int ucb_run_bif2d(ucb_engine* e, const ucb_bif2d_request* req, ucb_bif2d_result* res) {
+    if (!e || !req || !res) return UCB_E_INVALID;
+    const ucb_bif2d_request& q = *req;
+    res->ok = res->cancelled = 0;
+    res->error[0] = 0;
+    res->kernel_ms = 0;
+    res->steps = 0;
+    res->flops = 0;
+    std::string err;
+    SweepMap m;
+    if (!plan_bif2d(q, m, err)) return fail(e, res, UCB_E_INVALID, err);
+    if (!res->values || !res->flags) return fail(e, res, UCB_E_INVALID, "result buffers are NULL");
+    if (q.cancel && *q.cancel) {
+        res->cancelled = 1;
+        return fail(e, res, UCB_E_CANCELLED, "Cancelled by user");
+    }
+    const int prec = q.opt.precision;
+    const size_t esz = prec == UCB_PREC_F64 ? 8 : 4;
+    auto as_numb = [&](double v) { return prec == UCB_PREC_F64 ? v : (double)(float)v; };
+    // ranges[] of run_bif2d are numb, in kernel axis order
+    const double worstCaseH = m.h_axis == 0 ? as_numb(m.lo[0]) : (m.h_axis == 1 ? as_numb(m.lo[1]) : q.h);
+    const long long pointsInBlock = (long long)std::ceil(q.t_max / worstCaseH / q.pre_scaller);
+    const long long pointsForSkip = (long long)(q.transient_time / q.h);
+    if (pointsInBlock <= 0) return fail(e, res, UCB_E_INVALID, "computed amountOfPointsInBlock <= 0");
+    if (!ensure_init(e, err)) return fail(e, res, UCB_E_NOGPU, err);
+
+    SystemCode sys;
+    CompileRequest rq = bif2d_compile_request(q, m, sys);
+    auto mod = e->modules.get(rq, err);
+    if (!mod) return fail(e, res, UCB_E_COMPILE, err);
+    CUfunction fn = mod->functions["ucb_bif2d_kernel"];
+
+    const int n = q.n_pts;
+    const long long total = (long long)n * n;
+    // A peak needs a rise and a fall: at most one per two recorded samples.
+    const int cap = (int)std::min<long long>(kMaxAmountOfPeaks, pointsInBlock / 2 + 2);
+    const size_t per_cell = (size_t)(3 * (size_t)cap + 1) * esz;
+    size_t free_b = 0, total_b = 0;
+    cudaMemGetInfo(&free_b, &total_b);
+    const size_t budget = std::max<size_t>((size_t)(0.4 * (double)free_b), (size_t)64 << 20);
+    const long long chunk = std::max<long long>(1024, std::min<long long>(total, (long long)(budget / per_cell)));
+
+    std::vector<double> t0d, t1d;
+    std::vector<float> t0f, t1f;
+    axis_table(prec, n, m.lo[0], m.hi[0], m.log_axis[0], t0d, t0f);
+    axis_table(prec, n, m.lo[1], m.hi[1], m.log_axis[1], t1d, t1f);
+    const size_t tab_bytes = (size_t)n * esz;
+    const size_t off0 = 256, off1 = 256 + ((tab_bytes + 255) / 256) * 256;
+    if (!ensure_workspace(e, off1 + tab_bytes + 256, err)) return fail(e, res, UCB_E_CUDA, err);
+    char* ws = static_cast<char*>(e->ws);
+    double* d_values = nullptr;
+    int32_t* d_flags = nullptr;
+    char* d_scratch = nullptr;
+    cudaError_t ce;
+    if ((ce = cudaMallocAsync((void**)&d_values, (size_t)total * 8, e->stream)) != cudaSuccess ||
+        (ce = cudaMallocAsync((void**)&d_flags, (size_t)total * 4, e->stream)) != cudaSuccess ||
+        (ce = cudaMallocAsync((void**)&d_scratch, (size_t)std::min(chunk, total) * per_cell, e->stream)) !=
+            cudaSuccess) {
+        if (d_values) cudaFreeAsync(d_values, e->stream);
+        if (d_flags) cudaFreeAsync(d_flags, e->stream);
+        cudaStreamSynchronize(e->stream);
+        return fail(e, res, UCB_E_CUDA, std::string("cudaMallocAsync: ") + cudaGetErrorString(ce));
+    }
+    cudaMemcpyAsync(ws + off0, prec == UCB_PREC_F64 ? (const void*)t0d.data() : (const void*)t0f.data(), tab_bytes,
+                    cudaMemcpyHostToDevice, e->stream);
+    cudaMemcpyAsync(ws + off1, prec == UCB_PREC_F64 ? (const void*)t1d.data() : (const void*)t1f.data(), tab_bytes,
+                    cudaMemcpyHostToDevice, e->stream);
+    cudaMemsetAsync(ws + 8, 0, 8, e->stream);
+    if (q.progress) *q.progress = 0.0f;
+    int rc = UCB_OK;
+    cudaEventRecord(e->ev0, e->stream);
+    for (long long c0 = 0; c0 < total && rc == UCB_OK; c0 += chunk) {
+        if (q.cancel && *q.cancel) {
+            res->cancelled = 1;
+            rc = UCB_E_CANCELLED;
+            err = "Cancelled by user";
+            break;
+        }
+        const long long cells = std::min(chunk, total - c0);
+        cudaMemsetAsync(ws, 0, 8, e->stream);
+        char* peaks = d_scratch;
+        char* helpful = d_scratch + (size_t)cap * (size_t)cells * esz;
+        ParamPack pk;
+        pk.put<long long>(cells);
+        pk.put<long long>(c0);
+        pk.put<int>(n);
+        pk.put<int>(m.swap_xy ? 1 : 0);
+        pk.put<int>(q.pre_scaller);
+        pk.put<int>(q.writable_var);
+        pk.put<int>(cap);
+        pk.put<int>(0);
+        pk.put<long long>(pointsForSkip);
+        pk.put<long long>(pointsInBlock);
+        for (double v : {q.h, q.max_value, q.transient_time, q.t_max, q.eps_dbscan}) pk.put_numb(prec, v);
+        for (int i = 0; i < q.amount_of_x; ++i) pk.put_numb(prec, q.initial_conditions[i]);
+        for (int i = 0; i < std::max(q.n_values, 1); ++i) pk.put_numb(prec, i < q.n_values ? q.base_values[i] : 0.0);
+        pk.put<const void*>(ws + off0);
+        pk.put<const void*>(ws + off1);
+        pk.put<void*>(peaks);
+        pk.put<void*>(helpful);
+        pk.put<void*>(d_values);
+        pk.put<void*>(d_flags);
+        pk.put<void*>(ws);
+        pk.put<void*>(ws + 8);
+        const int block = 128;
+        if (!launch_packed(e, fn, persistent_grid(e, fn, block, cells), block, e->stream, pk, err)) rc = UCB_E_CUDA;
+        if (q.progress) *q.progress = (float)(c0 + cells) / (float)total;
+    }
+    cudaEventRecord(e->ev1, e->stream);
+    unsigned long long steps = 0;
+    if (rc == UCB_OK) {
+        if ((ce = cudaMemcpyAsync(res->values, d_values, (size_t)total * 8, cudaMemcpyDeviceToHost, e->stream)) !=
+                cudaSuccess ||
+            (ce = cudaMemcpyAsync(res->flags, d_flags, (size_t)total * 4, cudaMemcpyDeviceToHost, e->stream)) !=
+                cudaSuccess ||
+            (ce = cudaMemcpyAsync(&steps, ws + 8, 8, cudaMemcpyDeviceToHost, e->stream)) != cudaSuccess ||
+            (ce = cudaStreamSynchronize(e->stream)) != cudaSuccess) {
+            rc = UCB_E_CUDA;
+            err = std::string("CUDA bif2d: ") + cudaGetErrorString(ce);
+        }
+    }
+    cudaFreeAsync(d_values, e->stream);
+    cudaFreeAsync(d_flags, e->stream);
+    cudaFreeAsync(d_scratch, e->stream);
+    cudaStreamSynchronize(e->stream);
+    if (rc != UCB_OK) return fail(e, res, rc, err);
+    float ms = 0;
+    cudaEventElapsedTime(&ms, e->ev0, e->ev1);
+    res->kernel_ms = ms;
+    res->steps = (long long)steps;
+    res->flops = (double)steps * sys.flops_step;
+    double vmin = std::numeric_limits<double>::infinity(), vmax = -vmin;
+    for (long long k = 0; k < total; ++k) {
+        if (res->flags[k] < 0) continue;
+        const double v = res->values[k];
+        if (!std::isfinite(v) || v < 0.0) continue;
+        vmin = std::min(vmin, v);
+        vmax = std::max(vmax, v);
+    }
+    res->min_val = std::isfinite(vmin) ? vmin : 0.0;
+    res->max_val = std::isfinite(vmax) ? vmax : 0.0;
+    res->n_pts = n;
+    res->param_lo = q.param_lo;
+    res->param_hi = q.param_hi;
+    res->param_lo_2 = q.param_lo_2;
+    res->param_hi_2 = q.param_hi_2;
+    if (q.csv_output_path && *q.csv_output_path) {
+        csv::Common cc{std::vector<double>(q.base_values, q.base_values + q.n_values),
+                       std::vector<double>(q.initial_conditions, q.initial_conditions + q.amount_of_x)};
+        csv::bif2d(q.csv_output_path, cc, m.par_or_var, q.t_max, q.transient_time, q.h, q.pre_scaller, q.eps_dbscan,
+                   q.writable_var, q.sweep_over_var ? q.var_sweep_index : q.param_index,
+                   q.sweep_over_var_2 ? q.var_sweep_index_2 : q.param_index_2, q.param_lo, q.param_hi, q.param_lo_2,
+                   q.param_hi_2, n, res->values);
+    }
+    if (q.progress) *q.progress = 1.0f;
+    res->ok = 1;
+    return UCB_OK;
+}

@@ -62,6 +62,34 @@ class Lle2dResult(C.Structure):
     ]
 
 
+class Bif2dRequest(C.Structure):
+    _fields_ = [
+        ("krs_body", C.c_char_p), ("amount_of_x", C.c_int32),
+        ("initial_conditions", C.POINTER(C.c_double)), ("base_values", C.POINTER(C.c_double)),
+        ("n_values", C.c_int32),
+        ("sweep_over_var", C.c_int32), ("sweep_over_var_2", C.c_int32),
+        ("sweep_over_h", C.c_int32), ("sweep_over_h_2", C.c_int32),
+        ("log_scale", C.c_int32), ("log_scale_2", C.c_int32),
+        ("param_index", C.c_int32), ("var_sweep_index", C.c_int32),
+        ("param_index_2", C.c_int32), ("var_sweep_index_2", C.c_int32),
+        ("param_lo", C.c_double), ("param_hi", C.c_double), ("param_lo_2", C.c_double), ("param_hi_2", C.c_double),
+        ("n_pts", C.c_int32), ("writable_var", C.c_int32),
+        ("h", C.c_double), ("transient_time", C.c_double), ("t_max", C.c_double), ("pre_scaller", C.c_int32),
+        ("max_value", C.c_double), ("eps_dbscan", C.c_double), ("csv_output_path", C.c_char_p),
+        ("cancel", C.POINTER(C.c_int32)), ("progress", C.POINTER(C.c_float)), ("opt", Options),
+    ]
+
+
+class Bif2dResult(C.Structure):
+    _fields_ = [
+        ("values", C.POINTER(C.c_double)), ("flags", C.POINTER(C.c_int32)),
+        ("ok", C.c_int32), ("cancelled", C.c_int32), ("n_pts", C.c_int32),
+        ("param_lo", C.c_double), ("param_hi", C.c_double), ("param_lo_2", C.c_double), ("param_hi_2", C.c_double),
+        ("min_val", C.c_double), ("max_val", C.c_double), ("kernel_ms", C.c_double), ("steps", C.c_longlong),
+        ("flops", C.c_double), ("error", C.c_char * 1024),
+    ]
+
+
 class Lle1dRequest(C.Structure):
     _fields_ = [
         ("krs_body", C.c_char_p), ("amount_of_x", C.c_int32),
@@ -234,6 +262,10 @@ def load():
                               C.c_char_p, C.c_int, C.c_char_p, C.c_int]
     L.ucb_precompile_lle2d.restype = C.c_int
     L.ucb_precompile_lle2d.argtypes = [C.POINTER(Lle2dRequest), C.c_char_p, C.c_int]
+    L.ucb_run_bif2d.restype = C.c_int
+    L.ucb_run_bif2d.argtypes = [C.c_void_p, C.POINTER(Bif2dRequest), C.POINTER(Bif2dResult)]
+    L.ucb_precompile_bif2d.restype = C.c_int
+    L.ucb_precompile_bif2d.argtypes = [C.POINTER(Bif2dRequest), C.c_char_p, C.c_int]
     L.ucb_run_lle1d.restype = C.c_int
     L.ucb_run_lle1d.argtypes = [C.c_void_p, C.POINTER(Lle1dRequest), C.POINTER(Lle1dResult)]
     L.ucb_run_ls1d.restype = C.c_int
@@ -343,6 +375,48 @@ class Engine:
         res.values = _dptr(values)
         res.flags = flags.ctypes.data_as(C.POINTER(C.c_int32))
         rc = self.lib.ucb_run_lle2d(self.h, C.byref(req), C.byref(res))
+        if rc != UCB_OK:
+            raise UcbError(rc, res.error.decode())
+        return values, flags, res
+
+    # ------------------------------------------------------------------ bifurcation 2D
+    @staticmethod
+    def bif2d_request(krs_body: str, amount_of_x: int, initial_conditions, base_values, *, n_pts,
+                      param_index=0, param_index_2=0, var_sweep_index=0, var_sweep_index_2=0,
+                      sweep_over_var=False, sweep_over_var_2=False, sweep_over_h=False, sweep_over_h_2=False,
+                      log_scale=False, log_scale_2=False, param_lo=0.0, param_hi=1.0, param_lo_2=0.0,
+                      param_hi_2=1.0, writable_var=0, h=0.01, transient_time=0.0, t_max=100.0, pre_scaller=1,
+                      max_value=1e6, eps_dbscan=0.1, csv_output_path=None, opt: Options | None = None):
+        ic = np.ascontiguousarray(initial_conditions, dtype=np.float64)
+        vals = np.ascontiguousarray(base_values, dtype=np.float64)
+        r = Bif2dRequest()
+        r._keep = (ic, vals, krs_body.encode())
+        r.krs_body = r._keep[2]
+        r.amount_of_x = amount_of_x
+        r.initial_conditions = _dptr(ic)
+        r.base_values = _dptr(vals)
+        r.n_values = len(vals)
+        r.sweep_over_var, r.sweep_over_var_2 = int(sweep_over_var), int(sweep_over_var_2)
+        r.sweep_over_h, r.sweep_over_h_2 = int(sweep_over_h), int(sweep_over_h_2)
+        r.log_scale, r.log_scale_2 = int(log_scale), int(log_scale_2)
+        r.param_index, r.var_sweep_index = param_index, var_sweep_index
+        r.param_index_2, r.var_sweep_index_2 = param_index_2, var_sweep_index_2
+        r.param_lo, r.param_hi, r.param_lo_2, r.param_hi_2 = param_lo, param_hi, param_lo_2, param_hi_2
+        r.n_pts, r.writable_var = n_pts, writable_var
+        r.h, r.transient_time, r.t_max, r.pre_scaller = h, transient_time, t_max, pre_scaller
+        r.max_value, r.eps_dbscan = max_value, eps_dbscan
+        r.csv_output_path = csv_output_path.encode() if csv_output_path else None
+        r.opt = opt if opt is not None else options()
+        return r
+
+    def run_bif2d(self, req: Bif2dRequest):
+        n = req.n_pts
+        values = np.empty(max(n, 0) ** 2, dtype=np.float64)
+        flags = np.empty(max(n, 0) ** 2, dtype=np.int32)
+        res = Bif2dResult()
+        res.values = _dptr(values)
+        res.flags = flags.ctypes.data_as(C.POINTER(C.c_int32))
+        rc = self.lib.ucb_run_bif2d(self.h, C.byref(req), C.byref(res))
         if rc != UCB_OK:
             raise UcbError(rc, res.error.decode())
         return values, flags, res
@@ -652,7 +726,8 @@ Engine.lle2d_cells = _engine_cells
 def precompile_lle2d(req) -> str:
     """Compiles the sm_100a kernel a run with this request would use (no GPU needed)."""
     fn = {Lle2dRequest: "ucb_precompile_lle2d", Ls2dRequest: "ucb_precompile_ls2d",
-          Bif1dRequest: "ucb_precompile_bif1d", BasinsRequest: "ucb_precompile_basins"}[type(req)]
+          Bif1dRequest: "ucb_precompile_bif1d", BasinsRequest: "ucb_precompile_basins",
+          Bif2dRequest: "ucb_precompile_bif2d"}[type(req)]
     buf = C.create_string_buffer(65536)
     rc = getattr(load(), fn)(C.byref(req), buf, len(buf))
     if rc != UCB_OK:
