@@ -399,6 +399,92 @@ typedef struct ucb_basins_result {
 UCB_API int ucb_run_basins(ucb_engine* e, const ucb_basins_request* req, ucb_basins_result* res);
 UCB_API int ucb_precompile_basins(const ucb_basins_request* req, char* err_out, int err_len);
 
+/* ------------------------------------------------------------------------------------
+ * Basins of attraction by the reference's own method — replaces
+ * ParametricEngine::run_basins (parametric_engine.h:659-723, BasinsRequest / BasinsResult;
+ * parametric_engine.cpp:6035-6510) with the same request fields and results:
+ * initial conditions (axis_x_var, axis_y_var) on an n_pts x n_pts grid (numb axis values),
+ * the others from initial_conditions; integration of tMax / h / pre_scaller recorded
+ * samples after (int)(transient_time / h) transient steps; per cell a class (1 oscillating,
+ * -1 fixed point, 0 unbound) and two features of the peaks of writable_var (feature1 /
+ * feature2: the BF_* kinds of configCUDA.h, 0 = mean peak, 1 = mean interval, ...; unknown
+ * kinds give -999; times mult1 / mult2); then DBSCAN (minPts 1) of the features with
+ * eps_dbscan. labels (basin_idx): >= 1 oscillating cluster, <= -1 a cluster that holds a
+ * fixed point, 0 unbound; clusters numbered as the reference's seed order does (fixed-point
+ * clusters by their lowest fixed-point cell, then the others by their lowest cell).
+ * All four arrays row-major iy*n + ix, caller-allocated n_pts^2.
+ * ---------------------------------------------------------------------------------- */
+typedef struct ucb_basins_dbscan_request {
+    const char* krs_body;
+    int32_t amount_of_x;
+    const double* initial_conditions;
+    const double* base_values;
+    int32_t n_values;
+    int32_t axis_x_var, axis_y_var;   /* 0-based state indices, distinct */
+    double axis_x_lo, axis_x_hi, axis_y_lo, axis_y_hi;
+    int32_t n_pts;                    /* n_pts^2 <= 2^31 - 1 */
+    int32_t writable_var;             /* peak variable, -1..amount_of_x-1 */
+    double h, t_max, transient_time;
+    int32_t pre_scaller;
+    double max_value;
+    double eps_dbscan;
+    int32_t feature1, feature2;       /* BF_* kinds (reference defaults 0 and 1) */
+    double mult1, mult2;              /* reference defaults 1 and 1 */
+    const char* csv_output_path;
+    const volatile int32_t* cancel;
+    volatile float* progress;         /* 0..1 within the current phase */
+    volatile int32_t* progress_phase; /* 1 integration, 2 clustering (may be NULL) */
+    ucb_options opt;
+} ucb_basins_dbscan_request;
+
+typedef struct ucb_basins_dbscan_result {
+    int32_t* labels;                  /* caller-allocated n_pts^2: basin_idx */
+    double* avg_peaks;                /* caller-allocated n_pts^2: feature 1 (999 unbound) */
+    double* avg_intervals;            /* caller-allocated n_pts^2: feature 2 */
+    int32_t* classes;                 /* caller-allocated n_pts^2: helpful_array (1, -1, 0) */
+    int32_t ok, cancelled, n_pts;
+    int32_t n_clusters;               /* max label (oscillating clusters) */
+    int32_t min_cluster_idx;          /* min label (-number of fixed-point clusters) */
+    double avg_peaks_min, avg_peaks_max;          /* over finite values other than +-999 */
+    double avg_intervals_min, avg_intervals_max;
+    double kernel_ms;                 /* integration + features */
+    double cluster_ms;                /* clustering */
+    long long steps;
+    char error[1024];
+} ucb_basins_dbscan_result;
+
+UCB_API int ucb_run_basins_dbscan(ucb_engine* e, const ucb_basins_dbscan_request* req,
+                                  ucb_basins_dbscan_result* res);
+UCB_API int ucb_precompile_basins_dbscan(const ucb_basins_dbscan_request* req, char* err_out, int err_len);
+
+/* DBSCAN alone over given features — replaces ParametricEngine::run_basins_recluster
+ * (parametric_engine.h:733-753, BasinsReclusterRequest / Result; parametric_engine.cpp:
+ * 6523-6600): the clustering of ucb_run_basins_dbscan over caller features (mults already
+ * applied) and classes, in the numb of opt.precision. */
+typedef struct ucb_basins_recluster_request {
+    const char* krs_body;             /* checked non-empty, as the reference does */
+    int32_t amount_of_x;
+    int32_t n_pts;
+    double eps_dbscan;
+    const double* avg_peaks;          /* n_pts^2 */
+    const double* avg_intervals;      /* n_pts^2 */
+    const int32_t* classes;           /* n_pts^2 helpful_array: -1 fixed point, 0 unbound, 1 oscillating */
+    const volatile int32_t* cancel;
+    volatile float* progress;
+    ucb_options opt;
+} ucb_basins_recluster_request;
+
+typedef struct ucb_basins_recluster_result {
+    int32_t* labels;                  /* caller-allocated n_pts^2: basin_idx */
+    int32_t ok, cancelled, n_pts;
+    int32_t n_clusters, min_cluster_idx;
+    double cluster_ms;
+    char error[1024];
+} ucb_basins_recluster_result;
+
+UCB_API int ucb_run_basins_recluster(ucb_engine* e, const ucb_basins_recluster_request* req,
+                                     ucb_basins_recluster_result* res);
+
 /* LLE map without device allocation (no counterpart in the reference).
  *
  * ucb_lle2d_device() keeps its scratch (work-queue counter, step counter, axis value

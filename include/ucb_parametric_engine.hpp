@@ -5,7 +5,7 @@
 // conventions (ok / cancelled / error, NaN or sentinel + flags, row-major iy*n+ix, plane-
 // major spectra), same shared_ptr<atomic<...>> cancel / progress tokens. Every call goes
 // through the C ABI in ucb.h (libucb.so): run_bifurcation_1d, run_bifurcation_2d,
-// run_lle_2d, run_ls_2d.
+// run_lle_2d, run_ls_2d, run_basins, run_basins_recluster.
 // Entry points of the reference that are not on this path (DFT, Fast Synchro,
 // continuation sweeps) are not provided.
 //
@@ -46,6 +46,16 @@ struct Bif2DSnapshot {
     int writableVar = 0, indexOfMutVar = 0, indexOfMutVar2 = 0;
     double range1_lo = 0.0, range1_hi = 0.0, range2_lo = 0.0, range2_hi = 0.0;
     int n_pts = 0;
+};
+struct BasinsSnapshot {
+    std::vector<double> values, initial_conditions;
+    double tMax = 0.0, transientTime = 0.0, h = 0.0;
+    int preScaller = 0;
+    double eps_dbscan = 0.0;
+    int writableVar = 0, axis_x_var = 0, axis_y_var = 0;
+    double axis_x_lo = 0.0, axis_x_hi = 0.0, axis_y_lo = 0.0, axis_y_hi = 0.0;
+    int n_pts = 0, feature1 = 0, feature2 = 0;
+    double mult1 = 0.0, mult2 = 0.0;
 };
 struct LS2DSnapshot {
     std::vector<double> values, initial_conditions;
@@ -242,6 +252,78 @@ struct LS2DResult {
     std::vector<double> min_val;
     std::vector<double> max_val;
     data_export::LS2DSnapshot snapshot;
+};
+
+// Basins of attraction (parametric_engine.h:659-723): class and two peak features per
+// initial-condition cell, then DBSCAN of the features. basin_idx >= 1 oscillating cluster,
+// <= -1 cluster holding a fixed point, 0 unbound; all arrays row-major iy*n + ix.
+struct BasinsRequest {
+    std::string krs_body;
+    int amountOfX = 0;
+    std::vector<double> initial_conditions;
+    std::vector<double> base_values;
+    int axis_x_var = 0;
+    int axis_y_var = 1;
+    double axis_x_lo = -10.0, axis_x_hi = 10.0;
+    double axis_y_lo = -10.0, axis_y_hi = 10.0;
+    int n_pts = 200;
+    int writable_var = 0;
+    double h = 0.01;
+    double t_max = 1000.0;
+    double transient_time = 10000.0;
+    int pre_scaller = 1;
+    double max_value = 1.0e6;
+    double eps_dbscan = 0.5;
+    int feature1 = 0;   // BF_AVG_PEAKS
+    int feature2 = 1;   // BF_AVG_INTERVALS
+    double mult1 = 1.0;
+    double mult2 = 1.0;
+    std::string csv_output_path;
+    std::shared_ptr<std::atomic<bool>> cancel;
+    std::shared_ptr<std::atomic<float>> progress;
+    std::shared_ptr<std::atomic<int>> progress_phase;
+};
+
+struct BasinsResult {
+    bool ok = false;
+    bool cancelled = false;
+    std::string error;
+    int n_pts = 0;
+    double axis_x_lo = 0.0, axis_x_hi = 0.0;
+    double axis_y_lo = 0.0, axis_y_hi = 0.0;
+    int axis_x_var = 0, axis_y_var = 1;
+    std::vector<int> basin_idx;
+    std::vector<double> avg_peaks;
+    std::vector<double> avg_intervals;
+    std::vector<int> helpful_array;
+    int n_clusters = 0;
+    int min_cluster_idx = 0;
+    double avg_peaks_min = 0.0, avg_peaks_max = 0.0;
+    double avg_intervals_min = 0.0, avg_intervals_max = 0.0;
+    data_export::BasinsSnapshot snapshot;
+};
+
+// DBSCAN alone over cached features (parametric_engine.h:733-753).
+struct BasinsReclusterRequest {
+    std::string krs_body;
+    int amountOfX = 0;
+    int n_pts = 0;
+    double eps_dbscan = 0.5;
+    std::vector<double> avg_peaks;
+    std::vector<double> avg_intervals;
+    std::vector<int> helpful_array;
+    std::shared_ptr<std::atomic<bool>> cancel;
+    std::shared_ptr<std::atomic<float>> progress;
+};
+
+struct BasinsReclusterResult {
+    bool ok = false;
+    bool cancelled = false;
+    std::string error;
+    int n_pts = 0;
+    std::vector<int> basin_idx;
+    int n_clusters = 0;
+    int min_cluster_idx = 0;
 };
 
 class ParametricEngine {
@@ -570,6 +652,139 @@ public:
         s.range2_hi = r.param_hi_2;
         s.n_pts = r.n_pts;
         s.n_exponents = res.n_exponents;
+        return res;
+    }
+
+    BasinsResult run_basins(const BasinsRequest& r) {
+        BasinsResult res;
+        if ((int)r.initial_conditions.size() != r.amountOfX) {
+            res.error = "initial_conditions.size() != amountOfX";
+            return res;
+        }
+        ucb_basins_dbscan_request q{};
+        q.krs_body = r.krs_body.c_str();
+        q.amount_of_x = r.amountOfX;
+        q.initial_conditions = r.initial_conditions.data();
+        q.base_values = r.base_values.data();
+        q.n_values = (int)r.base_values.size();
+        q.axis_x_var = r.axis_x_var;
+        q.axis_y_var = r.axis_y_var;
+        q.axis_x_lo = r.axis_x_lo;
+        q.axis_x_hi = r.axis_x_hi;
+        q.axis_y_lo = r.axis_y_lo;
+        q.axis_y_hi = r.axis_y_hi;
+        q.n_pts = r.n_pts;
+        q.writable_var = r.writable_var;
+        q.h = r.h;
+        q.t_max = r.t_max;
+        q.transient_time = r.transient_time;
+        q.pre_scaller = r.pre_scaller;
+        q.max_value = r.max_value;
+        q.eps_dbscan = r.eps_dbscan;
+        q.feature1 = r.feature1;
+        q.feature2 = r.feature2;
+        q.mult1 = r.mult1;
+        q.mult2 = r.mult2;
+        q.csv_output_path = r.csv_output_path.c_str();
+        int32_t cancel_now = (r.cancel && r.cancel->load()) ? 1 : 0;
+        q.cancel = &cancel_now;
+        float prog = 0.0f;
+        int32_t phase = 0;
+        q.progress = &prog;
+        q.progress_phase = &phase;
+        q.opt = opt_;
+        const size_t cells = r.n_pts > 0 ? (size_t)r.n_pts * (size_t)r.n_pts : 0;
+        std::vector<int32_t> labels(cells), classes(cells);
+        res.avg_peaks.assign(cells, 0.0);
+        res.avg_intervals.assign(cells, 0.0);
+        ucb_basins_dbscan_result o{};
+        o.labels = labels.data();
+        o.avg_peaks = res.avg_peaks.data();
+        o.avg_intervals = res.avg_intervals.data();
+        o.classes = classes.data();
+        ucb_run_basins_dbscan(e_, &q, &o);
+        if (r.progress) r.progress->store(prog);
+        if (r.progress_phase) r.progress_phase->store(phase);
+        res.ok = o.ok != 0;
+        res.cancelled = o.cancelled != 0;
+        res.error = o.error;
+        if (!res.ok) {
+            res.avg_peaks.clear();
+            res.avg_intervals.clear();
+            return res;
+        }
+        res.n_pts = o.n_pts;
+        res.axis_x_lo = r.axis_x_lo;
+        res.axis_x_hi = r.axis_x_hi;
+        res.axis_y_lo = r.axis_y_lo;
+        res.axis_y_hi = r.axis_y_hi;
+        res.axis_x_var = r.axis_x_var;
+        res.axis_y_var = r.axis_y_var;
+        res.basin_idx.assign(labels.begin(), labels.end());
+        res.helpful_array.assign(classes.begin(), classes.end());
+        res.n_clusters = o.n_clusters;
+        res.min_cluster_idx = o.min_cluster_idx;
+        res.avg_peaks_min = o.avg_peaks_min;
+        res.avg_peaks_max = o.avg_peaks_max;
+        res.avg_intervals_min = o.avg_intervals_min;
+        res.avg_intervals_max = o.avg_intervals_max;
+        auto& s = res.snapshot;
+        s.values = r.base_values;
+        s.initial_conditions = r.initial_conditions;
+        s.tMax = r.t_max;
+        s.transientTime = r.transient_time;
+        s.h = r.h;
+        s.preScaller = r.pre_scaller;
+        s.eps_dbscan = r.eps_dbscan;
+        s.writableVar = r.writable_var;
+        s.axis_x_var = r.axis_x_var;
+        s.axis_y_var = r.axis_y_var;
+        s.axis_x_lo = r.axis_x_lo;
+        s.axis_x_hi = r.axis_x_hi;
+        s.axis_y_lo = r.axis_y_lo;
+        s.axis_y_hi = r.axis_y_hi;
+        s.n_pts = r.n_pts;
+        s.feature1 = r.feature1;
+        s.feature2 = r.feature2;
+        s.mult1 = r.mult1;
+        s.mult2 = r.mult2;
+        return res;
+    }
+
+    BasinsReclusterResult run_basins_recluster(const BasinsReclusterRequest& r) {
+        BasinsReclusterResult res;
+        const size_t cells = r.n_pts > 0 ? (size_t)r.n_pts * (size_t)r.n_pts : 0;
+        if (r.n_pts > 0) {
+            if (r.avg_peaks.size() != cells) { res.error = "avg_peaks: size does not match n_pts^2"; return res; }
+            if (r.avg_intervals.size() != cells) { res.error = "avg_intervals: size does not match n_pts^2"; return res; }
+            if (r.helpful_array.size() != cells) { res.error = "helpful_array: size does not match n_pts^2"; return res; }
+        }
+        std::vector<int32_t> classes(r.helpful_array.begin(), r.helpful_array.end()), labels(cells);
+        ucb_basins_recluster_request q{};
+        q.krs_body = r.krs_body.c_str();
+        q.amount_of_x = r.amountOfX;
+        q.n_pts = r.n_pts;
+        q.eps_dbscan = r.eps_dbscan;
+        q.avg_peaks = r.avg_peaks.data();
+        q.avg_intervals = r.avg_intervals.data();
+        q.classes = classes.data();
+        int32_t cancel_now = (r.cancel && r.cancel->load()) ? 1 : 0;
+        q.cancel = &cancel_now;
+        float prog = 0.0f;
+        q.progress = &prog;
+        q.opt = opt_;
+        ucb_basins_recluster_result o{};
+        o.labels = labels.data();
+        ucb_run_basins_recluster(e_, &q, &o);
+        if (r.progress) r.progress->store(prog);
+        res.ok = o.ok != 0;
+        res.cancelled = o.cancelled != 0;
+        res.error = o.error;
+        if (!res.ok) return res;
+        res.n_pts = o.n_pts;
+        res.basin_idx.assign(labels.begin(), labels.end());
+        res.n_clusters = o.n_clusters;
+        res.min_cluster_idx = o.min_cluster_idx;
         return res;
     }
 

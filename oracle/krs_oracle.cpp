@@ -680,6 +680,41 @@ int dbscan_peaks(const T* peaks, int P, T eps, std::vector<T>& helpful) {
     return cluster - 1;
 }
 
+// Basin features of avgPeakFinderCUDA (cudaLibrary.cu:3310-3425): feature_needs /
+// compute_basin_feature for the 12 feature kinds (avg / rms / stdev of the peaks or the
+// intervals, and their log10 forms).
+template <class T>
+T basin_feature(int feat, T mean_p, T mean_i, T rms_p, T rms_i, T std_p, T std_i) {
+    switch (feat) {
+        case 0: return mean_p;
+        case 1: return mean_i;
+        case 2: return rms_p;
+        case 3: return rms_i;
+        case 4: return std_p;
+        case 5: return std_i;
+        case 6: return mean_p == (T)0 ? (T)0 : (mean_p > 0 ? std::log10(mean_p) : -std::log10(-mean_p));
+        case 7: return mean_i == (T)0 ? (T)0 : (mean_i > 0 ? std::log10(mean_i) : -std::log10(-mean_i));
+        case 8: return rms_p > 0 ? std::log10(rms_p) : (T)-999;
+        case 9: return rms_i > 0 ? std::log10(rms_i) : (T)-999;
+        case 10: return std_p > 0 ? std::log10(std_p) : (T)-999;
+        case 11: return std_i > 0 ? std::log10(std_i) : (T)-999;
+        default: return (T)-999;
+    }
+}
+
+inline void basin_feature_needs(int feat, bool& sp, bool& sp2, bool& si, bool& si2) {
+    sp = sp2 = si = si2 = false;
+    switch (feat) {
+        case 0: case 6: sp = true; break;
+        case 1: case 7: si = true; break;
+        case 2: case 8: sp2 = true; break;
+        case 3: case 9: si2 = true; break;
+        case 4: case 10: sp = sp2 = true; break;
+        case 5: case 11: si = si2 = true; break;
+        default: break;
+    }
+}
+
 extern "C" {
 
 const char* orc_last_error() { return g_err.c_str(); }
@@ -980,6 +1015,162 @@ int orc_bif2d(void* h, int nPts, int par_or_var, int idx0, int idx1, const doubl
         }
     }
     return 0;
+}
+
+// DBSCAN of basin features as run_basins' host loop drives it (parametric_engine.cpp:
+// 6330-6420 with CUDA_dbscan_search_fixed_points_kernel / _clear_points_kernel /
+// CUDA_dbscan_kernel, cudaLibrary.cu:3501-3563), also the whole of run_basins_recluster
+// (:6517-6600): seeds are the lowest-index unlabelled fixed point (helpful -1; cluster ids
+// -1, -2, ...), then the lowest-index unlabelled oscillating cell (helpful 1; ids 1, 2,
+// ...); a member labels every unlabelled cell within eps (sqrt(dx^2 + dy^2) <= eps in numb)
+// and queues it. A queued unbound cell (helpful 0) expands nothing, and its label is reset
+// to 0 while an unlabelled cell remains (the kernel's write of 0; its concurrent writes of
+// the cluster id are taken to lose).
+int orc_dbscan_cells(long long total, const double* f1, const double* f2, const int* helpful, double eps_dbscan,
+                     int numb_bytes, int* labels) {
+    const bool dbl = numb_bytes == 8;
+    for (long long c = 0; c < total; ++c) labels[c] = 0;
+    auto within = [&](long long a, long long b) {
+        if (dbl) {
+            const double dx = f1[a] - f1[b], dy = f2[a] - f2[b];
+            return std::sqrt(dx * dx + dy * dy) <= eps_dbscan;
+        }
+        const float dx = (float)f1[a] - (float)f1[b], dy = (float)f2[a] - (float)f2[b];
+        return std::sqrt(dx * dx + dy * dy) <= (float)eps_dbscan;
+    };
+    int pos = 0, neg = 0;
+    std::vector<long long> nb;
+    for (;;) {
+        long long seed = -1;
+        int id = 0;
+        for (long long c = 0; c < total && seed < 0; ++c)
+            if (helpful[c] == -1 && labels[c] == 0) seed = c;
+        if (seed >= 0) {
+            id = --neg;
+        } else {
+            for (long long c = 0; c < total && seed < 0; ++c)
+                if (labels[c] == 0 && helpful[c] == 1) seed = c;
+            if (seed < 0) break;
+            id = ++pos;
+        }
+        nb.clear();
+        auto expand = [&](long long cur) {
+            labels[cur] = id;
+            bool any = false;
+            std::vector<long long> found;
+            for (long long c = 0; c < total; ++c) {
+                if (labels[c] != 0 || c == cur) continue;
+                any = true;
+                if (helpful[cur] == 0) continue;
+                if (within(cur, c)) found.push_back(c);
+            }
+            if (helpful[cur] == 0 && any) {
+                labels[cur] = 0;
+                return;
+            }
+            for (long long c : found) {
+                labels[c] = id;
+                nb.push_back(c);
+            }
+        };
+        expand(seed);
+        for (size_t ni = 0; ni < nb.size(); ++ni) expand(nb[ni]);
+    }
+    return 0;
+}
+
+// Basins of attraction, reference method (run_basins, parametric_engine.cpp:6035-6510):
+// per cell of the initial-condition grid the trajectory class (1 oscillating, -1 fixed
+// point, 0 unbound) and two features (avgPeakFinderCUDA), then the host-driven DBSCAN of
+// the features (CUDA_dbscan_search_fixed / _clear_points_kernel + CUDA_dbscan_kernel):
+// seeds are the lowest-index unlabelled fixed point (cluster ids -1, -2, ...), then the
+// lowest-index unlabelled oscillating cell (1, 2, ...); a seed's cluster grows over every
+// unlabelled cell within eps (distance <= eps) of a member, through a neighbour list that
+// is expanded in order; an unbound cell reached this way is un-labelled again and not
+// expanded (the reference's kernel resets it to 0).
+int orc_basins_ref(void* h, int nPts, int xvar, int yvar, const double* ranges, const double* ic, int nv,
+                   const double* vals, double hstep, double transient, double tMax, int preScaller, int writableVar,
+                   double maxv, double eps_dbscan, int feature1, int feature2, double mult1, double mult2,
+                   int* labels, double* avg_peaks, double* avg_intervals, int* helpful, int nthreads) {
+    Krs* k = static_cast<Krs*>(h);
+    const int nx = k->nx;
+    Grid g{nPts, 2, 0, {xvar, yvar}, {ranges[0], ranges[1], ranges[2], ranges[3]}, 0, -1};
+    const long long points = (long long)(tMax / hstep / preScaller);
+    const long long skip = (long long)(transient / hstep);
+    if (points <= 0) { g_err = "computed amountOfPointsInBlock <= 0"; return -1; }
+    const long long total = (long long)nPts * nPts;
+    auto features = [&](auto tag, std::vector<double>& f1, std::vector<double>& f2) {
+        using T = decltype(tag);
+#pragma omp parallel num_threads(threads_or_default(nthreads))
+        {
+            std::vector<T> dd, pp, tt;
+#pragma omp for schedule(dynamic, 1)
+            for (long long c = 0; c < total; ++c) {
+                StepFn<T> f = Dispatch<T>::fn(k);
+                CellInit<T> ci;
+                init_cell<T>(g, c, nx, ic, nv, vals, hstep, &ci);
+                const T hl = ci.h;
+                dd.assign((size_t)points, (T)0);
+                pp.assign((size_t)points, (T)0);
+                tt.assign((size_t)points, (T)0);
+                int flag = loop_model<T>(f, ci.x, ci.a, hl, skip, nx, preScaller, writableVar, (T)maxv, nullptr);
+                if (flag == 1 || flag == -1)
+                    flag = loop_model<T>(f, ci.x, ci.a, hl, points, nx, preScaller, writableVar, (T)maxv, dd.data());
+                helpful[c] = flag;
+                T a_out, b_out;
+                if (flag == 0) {
+                    a_out = 999;
+                    b_out = 999;
+                } else if (flag == -1) {
+                    a_out = dd[(size_t)points - 1];
+                    b_out = (T)-1.0;
+                } else {
+                    const int np = peak_finder<T>(dd.data(), points, pp.data(), tt.data(), (T)(hstep * preScaller));
+                    if (np <= 0) {
+                        a_out = -999;
+                        b_out = (T)-1.0;
+                    } else {
+                        bool a1, a2, a3, a4, b1, b2, b3, b4;
+                        basin_feature_needs(feature1, a1, a2, a3, a4);
+                        basin_feature_needs(feature2, b1, b2, b3, b4);
+                        const bool nsp = a1 || b1, nsp2 = a2 || b2, nsi = a3 || b3, nsi2 = a4 || b4;
+                        T sp = 0, sp2 = 0, si = 0, si2 = 0;
+                        for (int i = 0; i < np; ++i) {
+                            if (nsp || nsp2) {
+                                const T pv = pp[i];
+                                if (nsp) sp += pv;
+                                if (nsp2) sp2 += pv * pv;
+                            }
+                            if (nsi || nsi2) {
+                                const T iv = tt[i];
+                                if (nsi) si += iv;
+                                if (nsi2) si2 += iv * iv;
+                            }
+                        }
+                        const T inv = (T)1.0 / (T)np;
+                        const T mp = nsp ? sp * inv : (T)0, mi = nsi ? si * inv : (T)0;
+                        const T rp = nsp2 ? std::sqrt(sp2 * inv) : (T)0, ri = nsi2 ? std::sqrt(si2 * inv) : (T)0;
+                        T sdp = 0, sdi = 0;
+                        if (nsp && nsp2) { const T v = sp2 * inv - mp * mp; sdp = std::sqrt(v < 0 ? (T)0 : v); }
+                        if (nsi && nsi2) { const T v = si2 * inv - mi * mi; sdi = std::sqrt(v < 0 ? (T)0 : v); }
+                        a_out = (T)mult1 * basin_feature<T>(feature1, mp, mi, rp, ri, sdp, sdi);
+                        b_out = (T)mult2 * basin_feature<T>(feature2, mp, mi, rp, ri, sdp, sdi);
+                    }
+                }
+                f1[c] = (double)a_out;
+                f2[c] = (double)b_out;
+            }
+        }
+    };
+    std::vector<double> f1((size_t)total), f2((size_t)total);
+    if (k->numb_bytes == 8) features(0.0, f1, f2);
+    else features(0.0f, f1, f2);
+    for (long long c = 0; c < total; ++c) {
+        avg_peaks[c] = f1[c];
+        avg_intervals[c] = f2[c];
+        labels[c] = 0;
+    }
+    return orc_dbscan_cells(total, f1.data(), f2.data(), helpful, eps_dbscan, k->numb_bytes, labels);
 }
 
 // Bifurcation 1D (run_bif1d + calculateDiscreteModelCUDA + peakFinderCUDA).

@@ -70,6 +70,14 @@ def lib():
                                  C.c_double, C.c_void_p, C.c_int, C.c_void_p, C.c_double, C.c_int, C.c_int, C.c_int,
                                  C.c_double, C.c_int, C.c_double, C.c_void_p, C.c_longlong, C.c_void_p, C.c_void_p,
                                  C.c_void_p, C.c_void_p, C.c_int]
+        L.orc_basins_ref.restype = C.c_int
+        L.orc_basins_ref.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_void_p, C.c_void_p, C.c_int,
+                                     C.c_void_p, C.c_double, C.c_double, C.c_double, C.c_int, C.c_int, C.c_double,
+                                     C.c_double, C.c_int, C.c_int, C.c_double, C.c_double, C.c_void_p, C.c_void_p,
+                                     C.c_void_p, C.c_void_p, C.c_int]
+        L.orc_dbscan_cells.restype = C.c_int
+        L.orc_dbscan_cells.argtypes = [C.c_longlong, C.c_void_p, C.c_void_p, C.c_void_p, C.c_double, C.c_int,
+                                       C.c_void_p]
         _lib = L
     return _lib
 
@@ -181,6 +189,42 @@ def bif2d(krs: Krs, g: dict, eps_dbscan: float, pre_scaller=1, writable_var=0, c
     if rc != 0:
         raise RuntimeError(lib().orc_last_error().decode())
     return values, flags
+
+
+def basins_ref(krs: Krs, b: dict, nthreads=0):
+    """run_basins semantics (reference method): (labels, avg_peaks, avg_intervals, classes),
+    row-major iy*n + ix. b: n_pts, axis_x_var, axis_y_var, axis_x_lo/hi, axis_y_lo/hi, ic,
+    values, h, transient_time, t_max, pre_scaller, writable_var, max_value, eps_dbscan,
+    feature1, feature2, mult1, mult2."""
+    n = b["n_pts"]
+    ranges = np.array([b["axis_x_lo"], b["axis_x_hi"], b["axis_y_lo"], b["axis_y_hi"]], dtype=np.float64)
+    ic = np.array(b["ic"], dtype=np.float64)
+    vals = np.array(b["values"], dtype=np.float64)
+    labels = np.zeros(n * n, dtype=np.int32)
+    f1 = np.zeros(n * n)
+    f2 = np.zeros(n * n)
+    cls = np.zeros(n * n, dtype=np.int32)
+    rc = lib().orc_basins_ref(krs.h, n, b["axis_x_var"], b["axis_y_var"], _ptr(ranges), _ptr(ic), len(vals),
+                              _ptr(vals), b["h"], b["transient_time"], b["t_max"], b.get("pre_scaller", 1),
+                              b.get("writable_var", 0), b["max_value"], b["eps_dbscan"], b.get("feature1", 0),
+                              b.get("feature2", 1), b.get("mult1", 1.0), b.get("mult2", 1.0), _ptr(labels),
+                              _ptr(f1), _ptr(f2), _ptr(cls), nthreads)
+    if rc != 0:
+        raise RuntimeError(lib().orc_last_error().decode())
+    return labels, f1, f2, cls
+
+
+def dbscan_cells(f1, f2, helpful, eps_dbscan: float, numb="f64"):
+    """run_basins_recluster semantics: cluster labels of given features / classes."""
+    f1 = np.ascontiguousarray(f1, dtype=np.float64)
+    f2 = np.ascontiguousarray(f2, dtype=np.float64)
+    helpful = np.ascontiguousarray(helpful, dtype=np.int32)
+    labels = np.zeros(len(f1), dtype=np.int32)
+    rc = lib().orc_dbscan_cells(len(f1), _ptr(f1), _ptr(f2), _ptr(helpful), eps_dbscan, 8 if numb == "f64" else 4,
+                                _ptr(labels))
+    if rc != 0:
+        raise RuntimeError(lib().orc_last_error().decode())
+    return labels
 
 
 def bif1d(krs: Krs, b: dict, max_out=64, pts=None, nthreads=0):

@@ -1,6 +1,7 @@
 // Drives the header-only ParametricEngine shim the way the reference's session layer
 // calls ParametricEngine (analysis_session.cpp builds a Request, calls run_*, reads the
-// Result). argv[1] = "invalid" (no GPU needed) or "lle2d" / "ls2d" / "bif1d" / "bif2d" (GPU); the RK4 body
+// Result). argv[1] = "invalid" (no GPU needed) or "lle2d" / "ls2d" / "bif1d" / "bif2d" / "basins" (GPU);
+// the RK4 body
 // is read from stdin.
 #include <cstdio>
 #include <cstring>
@@ -47,6 +48,35 @@ int main(int argc, char** argv) {
         Bifurcation2DResult res = eng.run_bifurcation_2d(r);
         std::printf("ok=%d error=%s n=%d max=%g\n", (int)res.ok, res.error.c_str(), res.n_pts, res.max_val);
         for (size_t i = 0; i < res.values.size(); ++i) std::printf("%.17g %d\n", res.values[i], res.flags[i]);
+        return 0;
+    }
+    if (mode == "basins") {
+        BasinsRequest r;
+        r.krs_body = body;
+        r.amountOfX = 3;
+        r.initial_conditions = {0.0, 0.0, 25.0};
+        r.base_values = {0, 10.0, 10.0, 8.0 / 3.0};
+        r.axis_x_lo = -20; r.axis_x_hi = 20; r.axis_y_lo = -20; r.axis_y_hi = 20;
+        r.n_pts = 8;
+        r.h = 0.01; r.transient_time = 100; r.t_max = 20; r.eps_dbscan = 0.5;
+        r.progress_phase = std::make_shared<std::atomic<int>>(0);
+        BasinsResult res = eng.run_basins(r);
+        std::printf("ok=%d error=%s n=%d clusters=%d min=%d phase=%d\n", (int)res.ok, res.error.c_str(), res.n_pts,
+                    res.n_clusters, res.min_cluster_idx, r.progress_phase->load());
+        for (size_t i = 0; i < res.basin_idx.size(); ++i)
+            std::printf("%d %.17g %.17g %d\n", res.basin_idx[i], res.avg_peaks[i], res.avg_intervals[i],
+                        res.helpful_array[i]);
+        // DBSCAN again over the cached features, as the reference's GUI re-clusters
+        BasinsReclusterRequest rc;
+        rc.krs_body = body;
+        rc.amountOfX = 3;
+        rc.n_pts = res.n_pts;
+        rc.eps_dbscan = 0.5;
+        rc.avg_peaks = res.avg_peaks;
+        rc.avg_intervals = res.avg_intervals;
+        rc.helpful_array = res.helpful_array;
+        BasinsReclusterResult rr = eng.run_basins_recluster(rc);
+        std::printf("recluster ok=%d same=%d\n", (int)rr.ok, (int)(rr.basin_idx == res.basin_idx));
         return 0;
     }
     if (mode == "ls2d") {

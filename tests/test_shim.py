@@ -74,3 +74,23 @@ def test_shim_bif2d_equals_c_abi(driver):
                             transient_time=20, t_max=60, eps_dbscan=0.1)
     ref, _, _ = eng.run_bif2d(req)
     np.testing.assert_array_equal(vals, ref)
+
+
+@pytest.mark.gpu
+def test_shim_basins_equals_c_abi(driver):
+    """run_basins / run_basins_recluster through the shim return what ucb_run_basins_dbscan
+    returns (basin_idx, features, classes), and reclustering the cached features gives the
+    same labels."""
+    out = run(driver, "basins", rk4_body(LORENZ)).splitlines()
+    assert out[0].startswith("ok=1 error= n=8") and "phase=2" in out[0]
+    assert out[-1] == "recluster ok=1 same=1"
+    rows = [l.split() for l in out[1:-1]]
+    eng = ucb.Engine(0)
+    req = eng.basins_dbscan_request(rk4_body(LORENZ), 3, (0.0, 0.0, 25.0), (0, 10.0, 10.0, 8.0 / 3.0), n_pts=8,
+                                    axis_x_lo=-20, axis_x_hi=20, axis_y_lo=-20, axis_y_hi=20, h=0.01,
+                                    transient_time=100, t_max=20, eps_dbscan=0.5)
+    lab, f1, f2, cls, _ = eng.run_basins_dbscan(req)
+    np.testing.assert_array_equal([int(r[0]) for r in rows], lab)
+    np.testing.assert_array_equal([float(r[1]) for r in rows], f1)
+    np.testing.assert_array_equal([float(r[2]) for r in rows], f2)
+    np.testing.assert_array_equal([int(r[3]) for r in rows], cls)

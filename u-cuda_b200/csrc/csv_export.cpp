@@ -147,6 +147,43 @@ void bif2d(const std::string& path, const Common& c, int par_or_var, double tMax
     grid(out, n_pts, values);
 }
 
+void basins(const std::string& path, const Common& c, double tMax, double transient, double h, int pre,
+            double eps_dbscan, int writable_var, int xvar, int yvar, double xlo, double xhi, double ylo, double yhi,
+            int n_pts, const int* labels, const double* avg_peaks, const double* avg_intervals, const int* classes) {
+    {
+        std::ofstream cfg(path + "_config.csv");
+        if (cfg) {
+            cfg << std::setprecision(kPrecision);
+            cfg << "Basins of attraction\n";
+            values_and_ic(cfg, c);
+            cfg << "CT = " << tMax << "\nTT = " << transient << "\nh = " << h << "\n";
+            cfg << "decimator = " << pre << "\neps_DBSCAN = " << eps_dbscan << "\n";
+            cfg << "indexVar for peakfinder = " << writable_var << "\n";
+            cfg << "indexVar for estimation = " << xvar << ", " << yvar << "\n";
+            cfg << "start value_1 = " << xlo << ", stop value_1 = " << xhi << "\n";
+            cfg << "start value_2 = " << ylo << ", stop value_2 = " << yhi << "\n";
+        }
+    }
+    auto one = [&](const std::string& p, auto at) {
+        std::ofstream o(p);
+        if (!o) return;
+        o << std::setprecision(kPrecision);
+        o << xlo << " " << xhi << "\n" << ylo << " " << yhi << "\n";
+        for (int iy = 0; iy < n_pts; ++iy) {
+            for (int ix = 0; ix < n_pts; ++ix) {
+                o << at((size_t)iy * n_pts + ix);
+                if (ix + 1 < n_pts) o << ", ";
+            }
+            o << '\n';
+        }
+    };
+    auto finite_or_999 = [](double v) { return std::isfinite(v) ? v : 999.0; };
+    one(path, [&](size_t k) { return labels[k]; });
+    one(path + "_1.csv", [&](size_t k) { return finite_or_999(avg_peaks[k]); });
+    one(path + "_2.csv", [&](size_t k) { return finite_or_999(avg_intervals[k]); });
+    one(path + "_3.csv", [&](size_t k) { return classes[k]; });
+}
+
 void curve1d(const std::string& path, const char* title, const Common& c, double tMax, double NT, double transient,
              double h, double eps, int index, double lo, double hi, bool log_scale, int n_pts, int n_cols,
              const double* v) {

@@ -31,6 +31,14 @@ void bif2d(const std::string& path, const Common& c, int par_or_var, double tMax
            int pre, double eps_dbscan, int writable_var, int idx1, int idx2, double r1lo, double r1hi, double r2lo,
            double r2hi, int n_pts, const double* values);
 
+// Basins of attraction, reference method (data_export.cpp write_basins_config /
+// write_basins_ranges / write_basins_grid_*): config, then four files (labels, _1 average
+// peaks, _2 average intervals, _3 classes) each with the two-line ranges header and the
+// n_pts x n_pts grid; non-finite features are written as 999.
+void basins(const std::string& path, const Common& c, double tMax, double transient, double h, int pre,
+            double eps_dbscan, int writable_var, int xvar, int yvar, double xlo, double xhi, double ylo, double yhi,
+            int n_pts, const int* labels, const double* avg_peaks, const double* avg_intervals, const int* classes);
+
 // 1-D LLE / LS (data_export.cpp write_lle1d_config / write_ls1d_config + rows): config
 // title "1D LLE" or "1D LS", rows "param, v0[, v1, ...]" with the parameter value of
 // getValueByIdx(_log)_local (parametric_engine.cpp:577-590).

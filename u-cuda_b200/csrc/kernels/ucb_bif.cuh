@@ -158,7 +158,7 @@ __device__ __forceinline__ int loop_transient(const S& st, numb* x, const numb* 
 
 }  // namespace ucbdev
 
-#if !defined(UCB_BIF2D)
+#if !defined(UCB_BIF2D) && !defined(UCB_BIF_NO_KERNELS)
 extern "C" __global__ void __launch_bounds__(128) ucb_bif_kernel(const UcbBifParams p) {
     const long long cell = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     const int lane = threadIdx.x & 31;
@@ -209,9 +209,9 @@ extern "C" __global__ void __launch_bounds__(128) ucb_bif_kernel(const UcbBifPar
     }
     ucbdev::warp_add_steps(p.steps, ns, lane);
 }
-#endif  // !UCB_BIF2D
+#endif  // 1-D kernel
 
-#if defined(UCB_BIF2D)
+#if defined(UCB_BIF2D) && !defined(UCB_BIF_NO_KERNELS)
 // ---------------------------------------------------------------------------------------
 // 2-D bifurcation (period) maps: run_bif2d (parametric_engine.cpp:5487-5910) = per cell the
 // 1-D trajectory + peakFinder above, then dbscan of the peaks (cudaLibrary.cu:2088-2166,

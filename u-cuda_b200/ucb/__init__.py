@@ -90,6 +90,51 @@ class Bif2dResult(C.Structure):
     ]
 
 
+class BasinsDbscanRequest(C.Structure):
+    _fields_ = [
+        ("krs_body", C.c_char_p), ("amount_of_x", C.c_int32),
+        ("initial_conditions", C.POINTER(C.c_double)), ("base_values", C.POINTER(C.c_double)),
+        ("n_values", C.c_int32), ("axis_x_var", C.c_int32), ("axis_y_var", C.c_int32),
+        ("axis_x_lo", C.c_double), ("axis_x_hi", C.c_double), ("axis_y_lo", C.c_double), ("axis_y_hi", C.c_double),
+        ("n_pts", C.c_int32), ("writable_var", C.c_int32),
+        ("h", C.c_double), ("t_max", C.c_double), ("transient_time", C.c_double), ("pre_scaller", C.c_int32),
+        ("max_value", C.c_double), ("eps_dbscan", C.c_double), ("feature1", C.c_int32), ("feature2", C.c_int32),
+        ("mult1", C.c_double), ("mult2", C.c_double), ("csv_output_path", C.c_char_p),
+        ("cancel", C.POINTER(C.c_int32)), ("progress", C.POINTER(C.c_float)),
+        ("progress_phase", C.POINTER(C.c_int32)), ("opt", Options),
+    ]
+
+
+class BasinsDbscanResult(C.Structure):
+    _fields_ = [
+        ("labels", C.POINTER(C.c_int32)), ("avg_peaks", C.POINTER(C.c_double)),
+        ("avg_intervals", C.POINTER(C.c_double)), ("classes", C.POINTER(C.c_int32)),
+        ("ok", C.c_int32), ("cancelled", C.c_int32), ("n_pts", C.c_int32),
+        ("n_clusters", C.c_int32), ("min_cluster_idx", C.c_int32),
+        ("avg_peaks_min", C.c_double), ("avg_peaks_max", C.c_double),
+        ("avg_intervals_min", C.c_double), ("avg_intervals_max", C.c_double),
+        ("kernel_ms", C.c_double), ("cluster_ms", C.c_double), ("steps", C.c_longlong),
+        ("error", C.c_char * 1024),
+    ]
+
+
+class BasinsReclusterRequest(C.Structure):
+    _fields_ = [
+        ("krs_body", C.c_char_p), ("amount_of_x", C.c_int32), ("n_pts", C.c_int32), ("eps_dbscan", C.c_double),
+        ("avg_peaks", C.POINTER(C.c_double)), ("avg_intervals", C.POINTER(C.c_double)),
+        ("classes", C.POINTER(C.c_int32)), ("cancel", C.POINTER(C.c_int32)), ("progress", C.POINTER(C.c_float)),
+        ("opt", Options),
+    ]
+
+
+class BasinsReclusterResult(C.Structure):
+    _fields_ = [
+        ("labels", C.POINTER(C.c_int32)), ("ok", C.c_int32), ("cancelled", C.c_int32), ("n_pts", C.c_int32),
+        ("n_clusters", C.c_int32), ("min_cluster_idx", C.c_int32), ("cluster_ms", C.c_double),
+        ("error", C.c_char * 1024),
+    ]
+
+
 class Lle1dRequest(C.Structure):
     _fields_ = [
         ("krs_body", C.c_char_p), ("amount_of_x", C.c_int32),
@@ -266,6 +311,13 @@ def load():
     L.ucb_run_bif2d.argtypes = [C.c_void_p, C.POINTER(Bif2dRequest), C.POINTER(Bif2dResult)]
     L.ucb_precompile_bif2d.restype = C.c_int
     L.ucb_precompile_bif2d.argtypes = [C.POINTER(Bif2dRequest), C.c_char_p, C.c_int]
+    L.ucb_run_basins_dbscan.restype = C.c_int
+    L.ucb_run_basins_dbscan.argtypes = [C.c_void_p, C.POINTER(BasinsDbscanRequest), C.POINTER(BasinsDbscanResult)]
+    L.ucb_precompile_basins_dbscan.restype = C.c_int
+    L.ucb_precompile_basins_dbscan.argtypes = [C.POINTER(BasinsDbscanRequest), C.c_char_p, C.c_int]
+    L.ucb_run_basins_recluster.restype = C.c_int
+    L.ucb_run_basins_recluster.argtypes = [C.c_void_p, C.POINTER(BasinsReclusterRequest),
+                                           C.POINTER(BasinsReclusterResult)]
     L.ucb_run_lle1d.restype = C.c_int
     L.ucb_run_lle1d.argtypes = [C.c_void_p, C.POINTER(Lle1dRequest), C.POINTER(Lle1dResult)]
     L.ucb_run_ls1d.restype = C.c_int
@@ -537,6 +589,72 @@ class Engine:
                for i in range(min(res.n_attractors, MAX_ATTRACTORS))]
         return labels, periods, iters, att, res
 
+    # ------------------------------------------------------------------ basins (reference method)
+    @staticmethod
+    def basins_dbscan_request(krs_body, amount_of_x, initial_conditions, base_values, *, n_pts, axis_x_var=0,
+                              axis_y_var=1, axis_x_lo=-10.0, axis_x_hi=10.0, axis_y_lo=-10.0, axis_y_hi=10.0,
+                              writable_var=0, h=0.01, t_max=1000.0, transient_time=10000.0, pre_scaller=1,
+                              max_value=1e6, eps_dbscan=0.5, feature1=0, feature2=1, mult1=1.0, mult2=1.0,
+                              csv_output_path=None, opt: Options | None = None):
+        """Request of run_basins (BasinsRequest, parametric_engine.h:659-691), its defaults."""
+        ic = np.ascontiguousarray(initial_conditions, dtype=np.float64)
+        vals = np.ascontiguousarray(base_values, dtype=np.float64)
+        r = BasinsDbscanRequest()
+        r._keep = (ic, vals, krs_body.encode())
+        r.krs_body = r._keep[2]
+        r.amount_of_x = amount_of_x
+        r.initial_conditions = _dptr(ic)
+        r.base_values = _dptr(vals)
+        r.n_values = len(vals)
+        r.axis_x_var, r.axis_y_var = axis_x_var, axis_y_var
+        r.axis_x_lo, r.axis_x_hi, r.axis_y_lo, r.axis_y_hi = axis_x_lo, axis_x_hi, axis_y_lo, axis_y_hi
+        r.n_pts, r.writable_var = n_pts, writable_var
+        r.h, r.t_max, r.transient_time, r.pre_scaller = h, t_max, transient_time, pre_scaller
+        r.max_value, r.eps_dbscan = max_value, eps_dbscan
+        r.feature1, r.feature2, r.mult1, r.mult2 = feature1, feature2, mult1, mult2
+        r.csv_output_path = csv_output_path.encode() if csv_output_path else None
+        r.opt = opt if opt is not None else options()
+        return r
+
+    def run_basins_dbscan(self, req: BasinsDbscanRequest):
+        """-> (labels, avg_peaks, avg_intervals, classes, result), row-major iy*n + ix."""
+        n = req.n_pts
+        labels = np.empty(max(n, 0) ** 2, dtype=np.int32)
+        f1 = np.empty(max(n, 0) ** 2, dtype=np.float64)
+        f2 = np.empty(max(n, 0) ** 2, dtype=np.float64)
+        cls = np.empty(max(n, 0) ** 2, dtype=np.int32)
+        res = BasinsDbscanResult()
+        res.labels = labels.ctypes.data_as(C.POINTER(C.c_int32))
+        res.avg_peaks = _dptr(f1)
+        res.avg_intervals = _dptr(f2)
+        res.classes = cls.ctypes.data_as(C.POINTER(C.c_int32))
+        rc = self.lib.ucb_run_basins_dbscan(self.h, C.byref(req), C.byref(res))
+        if rc != UCB_OK:
+            raise UcbError(rc, res.error.decode())
+        return labels, f1, f2, cls, res
+
+    def run_basins_recluster(self, krs_body, amount_of_x, n_pts, eps_dbscan, avg_peaks, avg_intervals, classes,
+                             opt: Options | None = None):
+        """DBSCAN of given features (run_basins_recluster) -> (labels, result)."""
+        f1 = np.ascontiguousarray(avg_peaks, dtype=np.float64)
+        f2 = np.ascontiguousarray(avg_intervals, dtype=np.float64)
+        cls = np.ascontiguousarray(classes, dtype=np.int32)
+        if not (len(f1) == len(f2) == len(cls) == n_pts * n_pts):
+            raise UcbError(UCB_E_INVALID, "features / classes: size does not match n_pts^2")
+        req = BasinsReclusterRequest()
+        body = krs_body.encode()
+        req.krs_body, req.amount_of_x, req.n_pts, req.eps_dbscan = body, amount_of_x, n_pts, eps_dbscan
+        req.avg_peaks, req.avg_intervals = _dptr(f1), _dptr(f2)
+        req.classes = cls.ctypes.data_as(C.POINTER(C.c_int32))
+        req.opt = opt if opt is not None else options()
+        labels = np.empty(n_pts * n_pts, dtype=np.int32)
+        res = BasinsReclusterResult()
+        res.labels = labels.ctypes.data_as(C.POINTER(C.c_int32))
+        rc = self.lib.ucb_run_basins_recluster(self.h, C.byref(req), C.byref(res))
+        if rc != UCB_OK:
+            raise UcbError(rc, res.error.decode())
+        return labels, res
+
     # ------------------------------------------------------------------ bifurcation 1D
     @staticmethod
     def bif1d_request(krs_body: str, amount_of_x: int, initial_conditions, base_values, *, n_pts, param_index=0,
@@ -727,7 +845,8 @@ def precompile_lle2d(req) -> str:
     """Compiles the sm_100a kernel a run with this request would use (no GPU needed)."""
     fn = {Lle2dRequest: "ucb_precompile_lle2d", Ls2dRequest: "ucb_precompile_ls2d",
           Bif1dRequest: "ucb_precompile_bif1d", BasinsRequest: "ucb_precompile_basins",
-          Bif2dRequest: "ucb_precompile_bif2d"}[type(req)]
+          Bif2dRequest: "ucb_precompile_bif2d",
+          BasinsDbscanRequest: "ucb_precompile_basins_dbscan"}[type(req)]
     buf = C.create_string_buffer(65536)
     rc = getattr(load(), fn)(C.byref(req), buf, len(buf))
     if rc != UCB_OK:
