@@ -209,7 +209,7 @@ def test_recluster_matches_oracle(kind, seed, prec):
     lab, res = eng.run_basins_recluster("x", 3, n, 0.5, f1, f2, cls, opt=ucb.options(precision=prec))
     ref = O.dbscan_cells(f1, f2, cls, 0.5, "f64" if prec == ucb.PREC_F64 else "f32")
     np.testing.assert_array_equal(lab, ref)
-    assert res.n_clusters == ref.max() and res.min_cluster_idx == ref.min()
+    assert res.n_clusters == max(ref.max(), 0) and res.min_cluster_idx == min(ref.min(), 0)
     eng.close()
 
 
@@ -232,18 +232,38 @@ def test_recluster_1m_cells_matches_component_rule(prec):
     eng.close()
 
 
+# Step bodies that call a transcendental function (the forced Duffing's cos): CUDA's and
+# the host's libm may round it differently in the last bit, so trajectories, and with them
+# the features, agree to rounding instead of bit for bit.
+TRANSCENDENTAL = {"duffing"}
+
+
+def check_against_oracle(name, c, lab, f1, f2, cls, res, numb="f64"):
+    rlab, rf1, rf2, rcls = oracle(c, numb)
+    np.testing.assert_array_equal(cls, rcls)
+    exact = name not in TRANSCENDENTAL
+    for got, want, kind in ((f1, rf1, c["feature1"]), (f2, rf2, c["feature2"])):
+        if not exact:
+            np.testing.assert_allclose(got, want, rtol=1e-5, atol=1e-9)
+        elif kind >= 6:  # log10 features: CUDA's log10 and the host's may differ in the last bit
+            np.testing.assert_allclose(got, want, rtol=1e-14, atol=0)
+        else:
+            np.testing.assert_array_equal(got, want)
+    # the clustering of the features this run produced is the reference's, label for label
+    np.testing.assert_array_equal(lab, O.dbscan_cells(f1, f2, cls, c["eps_dbscan"], numb))
+    if exact:
+        np.testing.assert_array_equal(lab, rlab)
+    # n_clusters / min_cluster_idx: the counts of oscillating / fixed-point clusters
+    assert res.n_clusters == max(lab.max(), 0) and res.min_cluster_idx == min(lab.min(), 0)
+
+
 @pytest.mark.gpu
 @pytest.mark.parametrize("name", list(CASES))
 def test_basins_dbscan_exact_matches_oracle(name, tmp_path):
     c = dict(CASES[name], csv=str(tmp_path / "basins.csv"))
     eng = ucb.Engine(0)
     lab, f1, f2, cls, res = eng.run_basins_dbscan(request(c, precision=ucb.PREC_F64, mode=ucb.MODE_EXACT))
-    rlab, rf1, rf2, rcls = oracle(c)
-    np.testing.assert_array_equal(cls, rcls)
-    np.testing.assert_array_equal(f1, rf1)
-    np.testing.assert_array_equal(f2, rf2)
-    np.testing.assert_array_equal(lab, rlab)
-    assert res.n_clusters == rlab.max() and res.min_cluster_idx == rlab.min()
+    check_against_oracle(name, c, lab, f1, f2, cls, res)
     n = c["n_pts"]
     grid = np.loadtxt(tmp_path / "basins.csv", delimiter=",", skiprows=2, ndmin=2)
     np.testing.assert_array_equal(grid.astype(np.int32).ravel(), lab)
@@ -261,12 +281,8 @@ def test_basins_dbscan_exact_matches_oracle(name, tmp_path):
 def test_basins_dbscan_exact_f32_matches_oracle(name):
     c = CASES[name]
     eng = ucb.Engine(0)
-    lab, f1, f2, cls, _ = eng.run_basins_dbscan(request(c, precision=ucb.PREC_F32, mode=ucb.MODE_EXACT))
-    rlab, rf1, rf2, rcls = oracle(c, "f32")
-    np.testing.assert_array_equal(cls, rcls)
-    np.testing.assert_array_equal(f1, rf1)
-    np.testing.assert_array_equal(f2, rf2)
-    np.testing.assert_array_equal(lab, rlab)
+    lab, f1, f2, cls, res = eng.run_basins_dbscan(request(c, precision=ucb.PREC_F32, mode=ucb.MODE_EXACT))
+    check_against_oracle(name, c, lab, f1, f2, cls, res, "f32")
     eng.close()
 
 

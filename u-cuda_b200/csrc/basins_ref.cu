@@ -117,12 +117,15 @@ __global__ void head_kernel(const long long* bx, const long long* by, const unsi
     head[i] = (bx[a] != bx[b] || by[a] != by[b]) ? 1u : 0u;
 }
 
+// sq_of holds the inclusive scan of the square heads; the square of cell i is one less.
 __global__ void squares_kernel(const long long* bx, const long long* by, const unsigned int* order,
-                               const unsigned int* head, const unsigned int* sq_of, long long n, unsigned int* start,
+                               const unsigned int* head, unsigned int* sq_of, long long n, unsigned int* start,
                                long long* sx, long long* sy) {
     const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n || !head[i]) return;
-    const unsigned int s = sq_of[i];
+    if (i >= n) return;
+    const unsigned int s = sq_of[i] - 1u;
+    sq_of[i] = s;
+    if (!head[i]) return;
     start[s] = (unsigned int)i;
     sx[s] = bx[order[i]];
     sy[s] = by[order[i]];
@@ -181,13 +184,16 @@ __global__ void square_stats_kernel(const double* sf1, const double* sf2, const 
     if (osc != kNone) atomicMin(&min_osc[s], osc);
 }
 
+// Parent links are changed by atomics (in L2) from any SM, so they are read past L1
+// (__ldcg): a stale link could make a CAS below fail forever. Links only ever point to a
+// smaller square index, so the walk ends within nsq steps.
 __device__ __forceinline__ unsigned int find_root(unsigned int* parent, unsigned int v) {
-    unsigned int p = parent[v];
+    unsigned int p = __ldcg(&parent[v]);
     while (p != v) {
-        const unsigned int g = parent[p];
+        const unsigned int g = __ldcg(&parent[p]);
         if (g != p) atomicCAS(&parent[v], p, g);  // path halving
         v = p;
-        p = parent[v];
+        p = __ldcg(&parent[v]);
     }
     return v;
 }
@@ -390,7 +396,7 @@ int fail(ucb_engine* e, R* r, int code, const std::string& msg) {
 
 // Clusters n cells: features f1 / f2 (device, rewritten as float values when single) and
 // classes cls into labels lab. Enqueues everything on st; reads back the square count
-// once (8 bytes). Returns the number of its own kernel launches, or -1 with err set.
+// once (4 bytes). Returns the number of its own kernel launches, or -1 with err set.
 int cluster_features(ucb_engine* e, cudaStream_t st, DeviceArena& mem, double* d_f1, double* d_f2, const int* d_cls,
                      unsigned int N, double eps, int single, int* d_lab, std::string& err) {
     long long* bx = mem.get<long long>(N);
@@ -403,7 +409,7 @@ int cluster_features(ucb_engine* e, cudaStream_t st, DeviceArena& mem, double* d
     unsigned int* sq_of = mem.get<unsigned int>(N);
     double* sf1 = mem.get<double>(N);
     double* sf2 = mem.get<double>(N);
-    unsigned int* counts = mem.get<unsigned int>(4);  // [0] last scan entry, [1] last head, [2] heavy pairs
+    unsigned int* counts = mem.get<unsigned int>(4);  // [2]: heavy square pairs
     if (!bx || !by || !k_in || !k_out || !v_in || !order || !head || !sq_of || !sf1 || !sf2 || !counts) {
         err = mem.err;
         return -1;
@@ -412,7 +418,7 @@ int cluster_features(ucb_engine* e, cudaStream_t st, DeviceArena& mem, double* d
     ucbbr::bin_kernel<<<G, B, 0, st>>>(d_f1, d_f2, d_cls, N, 0.7 * eps, single, bx, by, k_in, v_in);
     size_t sort_bytes = 0, scan_bytes = 0;
     cub::DeviceRadixSort::SortPairs(nullptr, sort_bytes, k_in, k_out, v_in, order, (int)N, 0, 64, st);
-    cub::DeviceScan::ExclusiveSum(nullptr, scan_bytes, head, sq_of, (int)N, st);
+    cub::DeviceScan::InclusiveSum(nullptr, scan_bytes, head, sq_of, (int)N, st);
     const size_t tmp_bytes = std::max(sort_bytes, scan_bytes);
     void* tmp = mem.get<char>(tmp_bytes);
     if (!tmp) {
@@ -425,17 +431,14 @@ int cluster_features(ucb_engine* e, cudaStream_t st, DeviceArena& mem, double* d
     cudaMemcpyAsync(v_in, order, (size_t)N * 4, cudaMemcpyDeviceToDevice, st);
     cub::DeviceRadixSort::SortPairs(tmp, sort_bytes, k_in, k_out, v_in, order, (int)N, 0, 64, st);
     ucbbr::head_kernel<<<G, B, 0, st>>>(bx, by, order, d_f1, d_f2, N, head, sf1, sf2);
-    cub::DeviceScan::ExclusiveSum(tmp, scan_bytes, head, sq_of, (int)N, st);
-    cudaMemcpyAsync(counts, sq_of + (N - 1), 4, cudaMemcpyDeviceToDevice, st);
-    cudaMemcpyAsync(counts + 1, head + (N - 1), 4, cudaMemcpyDeviceToDevice, st);
-    unsigned int hc[2] = {0, 0};
-    cudaMemcpyAsync(hc, counts, 8, cudaMemcpyDeviceToHost, st);
+    cub::DeviceScan::InclusiveSum(tmp, scan_bytes, head, sq_of, (int)N, st);
+    unsigned int nsq = 0;  // squares: the last inclusive-scan entry
+    cudaMemcpyAsync(&nsq, sq_of + (N - 1), 4, cudaMemcpyDeviceToHost, st);
     cudaError_t ce = cudaStreamSynchronize(st);
     if (ce != cudaSuccess) {
         err = std::string("CUDA basins clustering: ") + cudaGetErrorString(ce);
         return -1;
     }
-    const unsigned int nsq = hc[0] + hc[1];
     unsigned int* start = mem.get<unsigned int>((size_t)nsq + 1);
     long long* sx = mem.get<long long>(nsq);
     long long* sy = mem.get<long long>(nsq);
