@@ -309,7 +309,10 @@ def _timed(fn, reps=1):
     return out, t
 
 
-def run_other_configs(eng):
+OTHER_CONFIGS = ("bif", "spectrum", "basins", "bif2d", "basins_dbscan")
+
+
+def run_other_configs(eng, which=OTHER_CONFIGS):
     """The other hot-path configurations at their full sizes (one run each after a
     compiling warm-up), with parity summaries against the oracle on sampled cells."""
     import ucb
@@ -322,6 +325,8 @@ def run_other_configs(eng):
     for name, opt in (("plain_fp64_exact", dict(precision=ucb.PREC_F64, mode=ucb.MODE_EXACT)),
                       ("plain_fp64_native", dict(precision=ucb.PREC_F64, mode=ucb.MODE_NATIVE)),
                       ("fp32_native", dict(precision=ucb.PREC_F32, mode=ucb.MODE_NATIVE))):
+        if "bif" not in which:
+            break
         req = ucb.Engine.bif1d_request(body, 3, (0.1, 0.1, 0.1), (0, 10.0, 28.0, 8 / 3), n_pts=1024, param_index=2,
                                        param_lo=20.0, param_hi=200.0, h=0.01, transient_time=50.0, t_max=200.0,
                                        writable_var=0, max_peaks=64, opt=ucb.options(**opt))
@@ -346,6 +351,9 @@ def run_other_configs(eng):
     # steps, t_end = 2e4, rtol 1e-8 (FP64) / 1e-5 (FP32).
     hb = rk4_body(HYPER_ROSSLER)
     for name, prec, rtol in (("fp64_rtol1e-8", ucb.PREC_F64, 1e-8), ("fp32_rtol1e-5", ucb.PREC_F32, 1e-5)):
+        if "spectrum" not in which:
+            break
+
         def lreq(n):
             return ucb.Engine.ls2d_request(hb, 4, (-10.0, -6.0, 0.0, 10.0), (0, 0.25, 0.05), method=ucb.LS_DP5,
                                            gs_every=10, rtol=rtol, t_end=2e4, n_pts=n, param_index=1,
@@ -376,6 +384,9 @@ def run_other_configs(eng):
     # RK4 h = 2 pi / 200, 20 consecutive period matches to 1e-6, 2,000-period cap.
     db = rk4_body(DUFFING)
     for name, prec in (("plain_fp64", ucb.PREC_F64), ("fp32", ucb.PREC_F32)):
+        if "basins" not in which:
+            break
+
         def breq(n):
             return ucb.Engine.basins_request(db, 3, (0.0, 0.0, 0.0), (0.0,), n_pts=n, axis_x_var=0, axis_y_var=1,
                                              axis_x_lo=-2.5, axis_x_hi=2.5, axis_y_lo=-2.5, axis_y_hi=2.5,
@@ -392,6 +403,46 @@ def run_other_configs(eng):
             ref_labels = labels
         else:
             out["basins_duffing_4096"]["fp32_label_agreement"] = float((labels == ref_labels).mean())
+    # Lorenz period map (run_bifurcation_2d): rho in [20, 200] x sigma in [5, 15] on 512 x 512,
+    # x0 = (0.1, 0.1, 0.1), h = 0.01, 5,000 transient + 20,000 recorded steps, the peaks of x
+    # clustered per cell with eps 0.1.
+    for name, opt in (("plain_fp64_exact", dict(precision=ucb.PREC_F64, mode=ucb.MODE_EXACT)),
+                      ("plain_fp64_native", dict(precision=ucb.PREC_F64, mode=ucb.MODE_NATIVE)),
+                      ("fp32_native", dict(precision=ucb.PREC_F32, mode=ucb.MODE_NATIVE))):
+        if "bif2d" not in which:
+            break
+
+        def b2req(n):
+            return ucb.Engine.bif2d_request(body, 3, (0.1, 0.1, 0.1), (0, 10.0, 28.0, 8 / 3), n_pts=n, param_index=2,
+                                            param_index_2=1, param_lo=20.0, param_hi=200.0, param_lo_2=5.0,
+                                            param_hi_2=15.0, h=0.01, transient_time=50.0, t_max=200.0,
+                                            eps_dbscan=0.1, writable_var=0, opt=ucb.options(**opt))
+        eng.run_bif2d(b2req(4))
+        (vals, flags, res), ms = _timed(lambda: eng.run_bif2d(b2req(512)))
+        out.setdefault("bif2d_lorenz_512", {})[name] = {
+            "wall_ms": ms, "kernel_ms": res.kernel_ms, "cells_per_s": 512 * 512 / (res.kernel_ms * 1e-3),
+            "rk4_steps_per_s": res.steps / (res.kernel_ms * 1e-3), "max_period": res.max_val,
+            "fixed_point_cells": int((flags < 0).sum())}
+    # Basins by the reference's method (run_basins, its request defaults t_max = 1000,
+    # transient_time = 10000, eps_dbscan = 0.5, features mean peak / mean interval) on the
+    # forced Duffing system: 1024 x 1024 initial conditions in [-2.5, 2.5]^2, h = 2 pi / 200.
+    for name, prec in (("plain_fp64_native", ucb.PREC_F64), ("fp32_native", ucb.PREC_F32)):
+        if "basins_dbscan" not in which:
+            break
+
+        def bdreq(n):
+            return ucb.Engine.basins_dbscan_request(db, 3, (0.0, 0.0, 0.0), (0.0,), n_pts=n, axis_x_lo=-2.5,
+                                                    axis_x_hi=2.5, axis_y_lo=-2.5, axis_y_hi=2.5, h=2 * np.pi / 200,
+                                                    t_max=1000.0, transient_time=10000.0, eps_dbscan=0.5,
+                                                    opt=ucb.options(precision=prec))
+        eng.run_basins_dbscan(bdreq(4))
+        (lab, f1, f2, cls, res), ms = _timed(lambda: eng.run_basins_dbscan(bdreq(1024)))
+        out.setdefault("basins_dbscan_duffing_1024", {})[name] = {
+            "wall_ms": ms, "features_kernel_ms": res.kernel_ms, "cluster_ms": res.cluster_ms,
+            "cells_per_s": 1024 * 1024 / ((res.kernel_ms + res.cluster_ms) * 1e-3),
+            "rk4_steps_per_s": res.steps / (res.kernel_ms * 1e-3),
+            "oscillating_clusters": res.n_clusters, "fixed_point_clusters": -res.min_cluster_idx,
+            "classes": {str(k): int((cls == k).sum()) for k in (-1, 0, 1)}}
     return out
 
 
@@ -439,6 +490,8 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--all-configs", action="store_true",
                     help="also time the bifurcation, spectrum and basins configurations at full size")
+    ap.add_argument("--configs", default="",
+                    help=f"comma-separated subset of {','.join(OTHER_CONFIGS)} to time (instead of --all-configs)")
     ap.add_argument("--surrogate-chen", type=int, default=0, metavar="N",
                     help="also run the surrogate-refined Chen map at N x N (e.g. 8192)")
     args = ap.parse_args()
@@ -480,7 +533,8 @@ def main():
     results, clocks, launches, e2e_ms = run_ours(args, rank, world, local)
     import ucb
     surrogate_chen = None
-    other_configs = run_other_configs(ucb.Engine(local)) if args.all_configs and rank == 0 else None
+    which = OTHER_CONFIGS if args.all_configs else tuple(c for c in args.configs.split(",") if c)
+    other_configs = run_other_configs(ucb.Engine(local), which) if which and rank == 0 else None
     if args.surrogate_chen and rank == 0:
         surrogate_chen = [run_surrogate_chen(ucb.Engine(local), torch.device("cuda", local), args.surrogate_chen,
                                              tol, cov) for tol, cov in ((2e-3, 0.995), (2e-2, 0.99))]

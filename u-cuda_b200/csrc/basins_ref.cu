@@ -354,6 +354,7 @@ constexpr int kMaxAmountOfValues = 64;
 // Stream-ordered device allocations of one call, released (and the stream drained) when
 // the call returns.
 struct DeviceArena {
+    ucb_engine* e;
     cudaStream_t st;
     std::vector<void*> ptrs;
     std::string err;
@@ -364,7 +365,7 @@ struct DeviceArena {
     template <class T>
     T* get(size_t count) {
         void* p = nullptr;
-        const cudaError_t ce = cudaMallocAsync(&p, std::max<size_t>(count, 1) * sizeof(T), st);
+        const cudaError_t ce = dev_alloc(e, &p, std::max<size_t>(count, 1) * sizeof(T), st);
         if (ce != cudaSuccess) {
             err = std::string("cudaMallocAsync: ") + cudaGetErrorString(ce);
             return nullptr;
@@ -610,7 +611,7 @@ extern "C" int ucb_run_basins_dbscan(ucb_engine* e, const ucb_basins_dbscan_requ
     const size_t off0 = 256, off1 = 256 + ((tab_bytes + 255) / 256) * 256;
     if (!ensure_workspace(e, off1 + tab_bytes + 256, err)) return fail(e, res, UCB_E_CUDA, err);
     char* ws = static_cast<char*>(e->ws);
-    DeviceArena mem{st, {}, {}};
+    DeviceArena mem{e, st, {}, {}};
     double* d_f1 = mem.get<double>(total);
     double* d_f2 = mem.get<double>(total);
     int* d_cls = mem.get<int>(total);
@@ -722,7 +723,7 @@ extern "C" int ucb_run_basins_recluster(ucb_engine* e, const ucb_basins_recluste
     if (!ensure_init(e, err)) return fail(e, res, UCB_E_NOGPU, err);
     const long long total = (long long)q.n_pts * q.n_pts;
     cudaStream_t st = e->stream;
-    DeviceArena mem{st, {}, {}};
+    DeviceArena mem{e, st, {}, {}};
     double* d_f1 = mem.get<double>(total);
     double* d_f2 = mem.get<double>(total);
     int* d_cls = mem.get<int>(total);

@@ -24,6 +24,9 @@ struct ucb_engine {
     // Device workspace: work counters, step counters, axis tables. Grown on demand.
     void* ws = nullptr;
     size_t ws_bytes = 0;
+    // Stream-ordered allocations of the run_* calls come from this pool, which keeps what
+    // is freed for the next call (no release threshold) until ucb_clear_cache / destroy.
+    cudaMemPool_t pool = nullptr;
     long long launches = 0;
     // Network of the last surrogate-refined map, kept for reuse by the next call with the
     // same configuration (owned; released with the engine).
@@ -58,6 +61,11 @@ struct SystemCode {
 
 bool ensure_init(ucb_engine* e, std::string& err);
 bool ensure_workspace(ucb_engine* e, size_t bytes, std::string& err);
+
+// Stream-ordered device allocation from the engine's pool (released with cudaFreeAsync).
+inline cudaError_t dev_alloc(ucb_engine* e, void** p, size_t bytes, cudaStream_t st) {
+    return e->pool ? cudaMallocFromPoolAsync(p, bytes, e->pool, st) : cudaMallocAsync(p, bytes, st);
+}
 
 // Builds the step-function source for a run.
 SystemCode make_system_code(const std::string& krs_body, int nx, int nv, int precision, int mode,

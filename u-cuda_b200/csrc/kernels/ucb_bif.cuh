@@ -217,12 +217,14 @@ extern "C" __global__ void __launch_bounds__(128) ucb_bif_kernel(const UcbBifPar
 // 1-D trajectory + peakFinder above, then dbscan of the peaks (cudaLibrary.cu:2088-2166,
 // dbscanCUDA :2321) whose cluster count is the "period". The reference keeps the whole
 // recorded series, the peaks, the intervals and a helper array per cell in HBM and runs
-// three kernels; here the peaks stream straight into a per-cell slice of a scratch buffer
-// (interleaved: entry k of local cell i at k * total + i, so that a warp's accesses to
-// the same k are adjacent) and the same thread clusters them.
+// three kernels. Here a warp integrates its 32 cells (one per lane) with the peaks
+// streaming into the warp's own scratch slot (one contiguous row of `cap` peaks per
+// lane), then runs the dbscan of each of the 32 cells in turn with all 32 lanes: the
+// dbscan's control flow (seeds, stack pops) is the same for the whole warp and each scan
+// over the peaks is split across the lanes, so no lane waits on another cell's pops.
+// Scratch is per resident warp, not per cell.
 struct UcbBif2dParams {
-    long long total;           // cells in this launch (one chunk)
-    long long cell_offset;     // first kernel cell of the chunk
+    long long total;           // cells
     int n_pts;
     int swap_xy;               // 1: write transposed (user X = kernel axis 1)
     int pre_scaller;
@@ -236,8 +238,8 @@ struct UcbBif2dParams {
     numb vals[UCB_NV];
     const numb* axis0;
     const numb* axis1;
-    numb* peaks;               // cap x total
-    numb* helpful;             // (2 cap + 1) x total: dbscan labels [0, P), stack slots [P, 2P)
+    numb* peaks;               // per warp slot: 32 x cap
+    int* work;                 // per warp slot: cap labels + cap stack slots
     double* out_values;        // period (-1 where the dbscan result is negative)
     int* out_flags;            // -1 / 1
     unsigned long long* counter;
@@ -248,10 +250,9 @@ namespace ucbdev {
 
 struct Bif2dSink {
     numb* peaks;
-    long long stride;
     int cap;
     __device__ __forceinline__ void put(int k, numb value, numb) const {
-        if (k < cap) peaks[(long long)k * stride] = value;
+        if (k < cap) peaks[k] = value;
     }
 };
 
@@ -261,46 +262,62 @@ __device__ __forceinline__ numb dbscan_distance(numb x1, numb y1, numb x2, numb 
     return sqrt(dx * dx + dy * dy);
 }
 
-// The reference's dbscan step for step: labels and stack in numb, stack slots written at
-// P + k and popped at P + NumNeibor - 1, inner bound P - 1, result cluster - 1. Peaks enter
-// times mult_peak (1) and intervals times mult_interval (0) (configCUDA.h).
-__device__ __forceinline__ int dbscan_cell(const numb* peaks, numb* helpful, long long stride, int P, numb eps) {
+// The reference's dbscan step for step, one warp per cell: labels (helpful[0, P)) and the
+// stack slots (helpful[P, 2P)) as integers — they only ever hold cluster numbers and
+// indices below 2,500, exact in numb — with the slots written at P + k and popped at
+// P + NumNeibor - 1, inner bound P - 1, result cluster - 1. Peaks enter times mult_peak (1)
+// and intervals times mult_interval (0) (configCUDA.h). Within one scan each k touches only
+// its own label and slot and NumNeibor only counts, so the lanes take k = lane, lane + 32,
+// ... and the hits are summed with a ballot.
+__device__ __forceinline__ int dbscan_warp(const numb* peaks, int P, int* lab, int* stk, numb eps, int lane) {
     if (P == -1) return -1;
     if (P == 0) return 0;
     if (P == 1) return 1;
-    for (int k = 0; k < 2 * P + 1; ++k) helpful[(long long)k * stride] = 0;
+    for (int k = lane; k < P; k += 32) {
+        lab[k] = 0;
+        stk[k] = 0;
+    }
+    __syncwarp();
     const numb y = (numb)0.0 * (numb)0.0;
     int cluster = 0, nn = 0;
     for (unsigned long long i = 0; i < (unsigned long long)P; i++) {
         if (nn >= 1) {
-            const long long slot = ((long long)P + nn - 1) * stride;
-            i = (unsigned long long)helpful[slot];
-            helpful[slot] = 0;
+            const int v = stk[nn - 1];
+            __syncwarp();
+            if (lane == 0) stk[nn - 1] = 0;
+            i = (unsigned long long)v;
             nn = nn - 1;
-        } else if (helpful[(long long)i * stride] == 0) {
+        } else if (lab[i] == 0) {
             nn = 0;
             ++cluster;
-            helpful[(long long)i * stride] = (numb)cluster;
+            __syncwarp();
+            if (lane == 0) lab[i] = cluster;
         } else {
             continue;
         }
-        const numb xi = peaks[(long long)i * stride] * (numb)1.0;
-        for (int k = 0; k < P - 1; k++) {
-            if (i != (unsigned long long)k && helpful[(long long)k * stride] == 0) {
-                if (dbscan_distance(xi, y, peaks[(long long)k * stride] * (numb)1.0, y) < eps) {
-                    helpful[(long long)k * stride] = (numb)cluster;
-                    helpful[((long long)P + k) * stride] = (numb)k;
-                    ++nn;
-                }
+        __syncwarp();
+        const numb xi = peaks[i] * (numb)1.0;
+        int hits = 0;
+        for (int k0 = 0; k0 < P - 1; k0 += 32) {
+            const int k = k0 + lane;
+            bool hit = false;
+            if (k < P - 1 && i != (unsigned long long)k && lab[k] == 0)
+                hit = dbscan_distance(xi, y, peaks[k] * (numb)1.0, y) < eps;
+            if (hit) {
+                lab[k] = cluster;
+                stk[k] = k;
             }
+            hits += __popc(__ballot_sync(0xFFFFFFFFu, hit));
         }
+        nn += hits;
+        __syncwarp();
     }
     return cluster - 1;
 }
 
-// One cell of a 2-D period map.
-__device__ __forceinline__ void bif2d_cell(const UcbBif2dParams& p, long long i, long long& ns) {
-    const long long kidx = p.cell_offset + i;
+// Trajectory and peaks of one cell of a 2-D period map: the peak count (or the -1 / 0
+// trajectory flag), peaks in row[0, min(count, cap)).
+__device__ __forceinline__ int bif2d_peaks(const UcbBif2dParams& p, long long kidx, numb* row, long long& ns) {
     const ucbdev::CellAxes c = ucbdev::cell_axes(kidx, p.n_pts);
     numb x[UCB_NX], a[UCB_NV];
 #pragma unroll
@@ -330,7 +347,7 @@ __device__ __forceinline__ void bif2d_cell(const UcbBif2dParams& p, long long i,
             ucbdev::PeakScan scan;
             scan.init();
             scan.d1 = scan.d2 = 0;
-            const ucbdev::Bif2dSink sink{p.peaks + i, p.total, p.cap};
+            const ucbdev::Bif2dSink sink{row, p.cap};
             flag = ucbdev::loop_record(st, x, a, h, iters, p.pre_scaller, p.writable_var, p.maxv, scan, sink, ns);
             if (flag == 1) {
                 int n = (scan.found > 1) ? scan.found - 1 : 0;
@@ -343,24 +360,38 @@ __device__ __forceinline__ void bif2d_cell(const UcbBif2dParams& p, long long i,
             count = flag;
         }
     }
-    if (count > p.cap) count = p.cap;  // cannot happen: cap covers the largest count
-    const int period = ucbdev::dbscan_cell(p.peaks + i, p.helpful + i, p.total, count, p.eps);
-    long long out = kidx;
-    if (p.swap_xy) out = (kidx % p.n_pts) * p.n_pts + kidx / p.n_pts;
-    p.out_values[out] = period < 0 ? -1.0 : (double)period;
-    p.out_flags[out] = period < 0 ? -1 : 1;
+    return count > p.cap ? p.cap : count;  // cannot clip: cap covers the largest count
 }
 
 }  // namespace ucbdev
 
 extern "C" __global__ void __launch_bounds__(128) ucb_bif2d_kernel(const UcbBif2dParams p) {
     const int lane = threadIdx.x & 31;
+    const long long warp = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    numb* slot = p.peaks + warp * 32 * (long long)p.cap;
+    int* lab = p.work + warp * 2 * (long long)p.cap;
+    int* stk = lab + p.cap;
     long long ns = 0;
     for (;;) {
         const long long base = ucbdev::warp_fetch(p.counter, lane);
         if (base >= p.total) break;
         const long long i = base + lane;
-        if (i < p.total) ucbdev::bif2d_cell(p, i, ns);
+        const int count = i < p.total ? ucbdev::bif2d_peaks(p, i, slot + (long long)lane * p.cap, ns) : 0;
+        __syncwarp();
+        int mine = 0;
+        for (int c = 0; c < 32; ++c) {
+            if (base + c >= p.total) break;
+            const int P = __shfl_sync(0xFFFFFFFFu, count, c);
+            const int period = ucbdev::dbscan_warp(slot + (long long)c * p.cap, P, lab, stk, p.eps, lane);
+            if (lane == c) mine = period;
+        }
+        if (i < p.total) {
+            long long out = i;
+            if (p.swap_xy) out = (i % p.n_pts) * p.n_pts + i / p.n_pts;
+            p.out_values[out] = mine < 0 ? -1.0 : (double)mine;
+            p.out_flags[out] = mine < 0 ? -1 : 1;
+        }
+        __syncwarp();
     }
     ucbdev::warp_add_steps(p.steps, ns, lane);
 }

@@ -128,6 +128,7 @@ namespace {
 void set_err(char* dst, const std::string& msg) { std::snprintf(dst, 1024, "%s", msg.c_str()); }
 
 struct DevFree {
+    ucb_engine* e;
     cudaStream_t st;
     std::vector<void*> ptrs;
     ~DevFree() {
@@ -137,7 +138,7 @@ struct DevFree {
     template <class T>
     T* alloc(size_t count, std::string& err, const char* what) {
         void* p = nullptr;
-        const cudaError_t ce = cudaMallocAsync(&p, std::max<size_t>(count, 1) * sizeof(T), st);
+        const cudaError_t ce = dev_alloc(e, &p, std::max<size_t>(count, 1) * sizeof(T), st);
         if (ce != cudaSuccess) {
             err = std::string("cudaMallocAsync(") + what + "): " + cudaGetErrorString(ce);
             return nullptr;
@@ -227,7 +228,7 @@ int ucb_run_lle2d_surrogate(ucb_engine* e, const ucb_surrogate_request* rq, doub
             for (int i = 0; i < 6; ++i) cudaEventDestroy(ev[i]);
         }
     } evf{ev};
-    DevFree mem{st, {}};
+    DevFree mem{e, st, {}};
     long long* d_cells = mem.alloc<long long>(ns, err, "sample cells");
     double* d_sv = mem.alloc<double>(ns, err, "sample values");
     int* d_sf = mem.alloc<int>(ns, err, "sample flags");

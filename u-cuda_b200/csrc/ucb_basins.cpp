@@ -131,9 +131,9 @@ extern "C" int ucb_run_basins(ucb_engine* e, const ucb_basins_request* req, ucb_
     cudaMemsetAsync(ws + off_keys, 0, kTableSlots * 8, st);
     int32_t *d_labels = nullptr, *d_periods = nullptr, *d_iters = nullptr;
     cudaError_t ce;
-    if ((ce = cudaMallocAsync((void**)&d_labels, (size_t)total * 4, st)) != cudaSuccess ||
-        (ce = cudaMallocAsync((void**)&d_periods, (size_t)total * 4, st)) != cudaSuccess ||
-        (ce = cudaMallocAsync((void**)&d_iters, (size_t)total * 4, st)) != cudaSuccess)
+    if ((ce = dev_alloc(e, (void**)&d_labels, (size_t)total * 4, st)) != cudaSuccess ||
+        (ce = dev_alloc(e, (void**)&d_periods, (size_t)total * 4, st)) != cudaSuccess ||
+        (ce = dev_alloc(e, (void**)&d_iters, (size_t)total * 4, st)) != cudaSuccess)
         return fail(e, res, UCB_E_CUDA, std::string("cudaMallocAsync: ") + cudaGetErrorString(ce));
     const double h = q.period / q.steps_per_period;
     ParamPack pk;

@@ -132,9 +132,9 @@ extern "C" int ucb_run_bif1d(ucb_engine* e, const ucb_bif1d_request* req, ucb_bi
     double* d_int = nullptr;
     const size_t pk_elems = (size_t)n * (size_t)std::max(mo, 1);
     cudaError_t ce;
-    if ((ce = cudaMallocAsync((void**)&d_counts, (size_t)n * 4, e->stream)) != cudaSuccess ||
-        (ce = cudaMallocAsync((void**)&d_peaks, pk_elems * 8, e->stream)) != cudaSuccess ||
-        (ce = cudaMallocAsync((void**)&d_int, pk_elems * 8, e->stream)) != cudaSuccess)
+    if ((ce = dev_alloc(e, (void**)&d_counts, (size_t)n * 4, e->stream)) != cudaSuccess ||
+        (ce = dev_alloc(e, (void**)&d_peaks, pk_elems * 8, e->stream)) != cudaSuccess ||
+        (ce = dev_alloc(e, (void**)&d_int, pk_elems * 8, e->stream)) != cudaSuccess)
         return fail(e, res, UCB_E_CUDA, std::string("cudaMallocAsync: ") + cudaGetErrorString(ce));
     cudaMemcpyAsync(ws + 256, prec == UCB_PREC_F64 ? (const void*)tab_d.data() : (const void*)tab_f.data(), tab_bytes,
                     cudaMemcpyHostToDevice, e->stream);

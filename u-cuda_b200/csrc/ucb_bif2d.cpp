@@ -3,9 +3,9 @@
 // amountOfPointsInBlock = ceil(tMax / worstCaseH / preScaller) and (int)(transient / h) in
 // double, values = period (-1 with flag -1 where the dbscan result is negative), min / max
 // over the other cells, CSV. The reference chunks the grid by free memory because it
-// keeps the whole recorded series of every cell; here one kernel integrates, captures the
-// peaks into a per-cell scratch slice and clusters them (ucb_bif.cuh), and the grid is
-// chunked only by the size of that peak scratch.
+// keeps the whole recorded series of every cell; here one persistent kernel integrates,
+// captures the peaks into a scratch slot per resident warp and clusters them
+// (ucb_bif.cuh), so the whole grid is one launch.
 #include <algorithm>
 #include <cmath>
 #include <cstring>
@@ -154,11 +154,17 @@ extern "C" int ucb_run_bif2d(ucb_engine* e, const ucb_bif2d_request* req, ucb_bi
     const long long total = (long long)n * n;
     // A peak needs a rise and a fall: at most one per two recorded samples.
     const int cap = (int)std::min<long long>(kMaxAmountOfPeaks, pointsInBlock / 2 + 2);
-    const size_t per_cell = (size_t)(3 * (size_t)cap + 1) * esz;
+    // Scratch per resident warp: 32 rows of peaks + dbscan labels and stack slots. The
+    // persistent grid is trimmed if the slots would exceed 40 % of the free memory.
+    const int block = 128, warps_per_block = block / 32;
+    const size_t per_warp = (size_t)cap * (32 * esz + 2 * sizeof(int32_t));
+    int grid = persistent_grid(e, fn, block, total);
     size_t free_b = 0, total_b = 0;
     cudaMemGetInfo(&free_b, &total_b);
     const size_t budget = std::max<size_t>((size_t)(0.4 * (double)free_b), (size_t)64 << 20);
-    const long long chunk = std::max<long long>(1024, std::min<long long>(total, (long long)(budget / per_cell)));
+    grid = (int)std::max<long long>(1, std::min<long long>(grid, (long long)(budget / (per_warp * warps_per_block))));
+    const size_t slot_bytes = (size_t)grid * warps_per_block * 32 * cap * esz;
+    const size_t work_bytes = (size_t)grid * warps_per_block * 2 * cap * sizeof(int32_t);
 
     std::vector<double> t0d, t1d;
     std::vector<float> t0f, t1f;
@@ -170,14 +176,15 @@ extern "C" int ucb_run_bif2d(ucb_engine* e, const ucb_bif2d_request* req, ucb_bi
     char* ws = static_cast<char*>(e->ws);
     double* d_values = nullptr;
     int32_t* d_flags = nullptr;
-    char* d_scratch = nullptr;
+    char* d_slots = nullptr;
+    char* d_work = nullptr;
     cudaError_t ce;
-    if ((ce = cudaMallocAsync((void**)&d_values, (size_t)total * 8, e->stream)) != cudaSuccess ||
-        (ce = cudaMallocAsync((void**)&d_flags, (size_t)total * 4, e->stream)) != cudaSuccess ||
-        (ce = cudaMallocAsync((void**)&d_scratch, (size_t)std::min(chunk, total) * per_cell, e->stream)) !=
-            cudaSuccess) {
-        if (d_values) cudaFreeAsync(d_values, e->stream);
-        if (d_flags) cudaFreeAsync(d_flags, e->stream);
+    if ((ce = dev_alloc(e, (void**)&d_values, (size_t)total * 8, e->stream)) != cudaSuccess ||
+        (ce = dev_alloc(e, (void**)&d_flags, (size_t)total * 4, e->stream)) != cudaSuccess ||
+        (ce = dev_alloc(e, (void**)&d_slots, slot_bytes, e->stream)) != cudaSuccess ||
+        (ce = dev_alloc(e, (void**)&d_work, work_bytes, e->stream)) != cudaSuccess) {
+        for (void* ptr : {(void*)d_values, (void*)d_flags, (void*)d_slots})
+            if (ptr) cudaFreeAsync(ptr, e->stream);
         cudaStreamSynchronize(e->stream);
         return fail(e, res, UCB_E_CUDA, std::string("cudaMallocAsync: ") + cudaGetErrorString(ce));
     }
@@ -185,47 +192,33 @@ extern "C" int ucb_run_bif2d(ucb_engine* e, const ucb_bif2d_request* req, ucb_bi
                     cudaMemcpyHostToDevice, e->stream);
     cudaMemcpyAsync(ws + off1, prec == UCB_PREC_F64 ? (const void*)t1d.data() : (const void*)t1f.data(), tab_bytes,
                     cudaMemcpyHostToDevice, e->stream);
-    cudaMemsetAsync(ws + 8, 0, 8, e->stream);
+    cudaMemsetAsync(ws, 0, 16, e->stream);
     if (q.progress) *q.progress = 0.0f;
     int rc = UCB_OK;
+    // UcbBif2dParams field by field
+    ParamPack pk;
+    pk.put<long long>(total);
+    pk.put<int>(n);
+    pk.put<int>(m.swap_xy ? 1 : 0);
+    pk.put<int>(q.pre_scaller);
+    pk.put<int>(q.writable_var);
+    pk.put<int>(cap);
+    pk.put<int>(0);
+    pk.put<long long>(pointsForSkip);
+    pk.put<long long>(pointsInBlock);
+    for (double v : {q.h, q.max_value, q.transient_time, q.t_max, q.eps_dbscan}) pk.put_numb(prec, v);
+    for (int i = 0; i < q.amount_of_x; ++i) pk.put_numb(prec, q.initial_conditions[i]);
+    for (int i = 0; i < std::max(q.n_values, 1); ++i) pk.put_numb(prec, i < q.n_values ? q.base_values[i] : 0.0);
+    pk.put<const void*>(ws + off0);
+    pk.put<const void*>(ws + off1);
+    pk.put<void*>(d_slots);
+    pk.put<void*>(d_work);
+    pk.put<void*>(d_values);
+    pk.put<void*>(d_flags);
+    pk.put<void*>(ws);
+    pk.put<void*>(ws + 8);
     cudaEventRecord(e->ev0, e->stream);
-    for (long long c0 = 0; c0 < total && rc == UCB_OK; c0 += chunk) {
-        if (q.cancel && *q.cancel) {
-            res->cancelled = 1;
-            rc = UCB_E_CANCELLED;
-            err = "Cancelled by user";
-            break;
-        }
-        const long long cells = std::min(chunk, total - c0);
-        cudaMemsetAsync(ws, 0, 8, e->stream);
-        char* peaks = d_scratch;
-        char* helpful = d_scratch + (size_t)cap * (size_t)cells * esz;
-        ParamPack pk;
-        pk.put<long long>(cells);
-        pk.put<long long>(c0);
-        pk.put<int>(n);
-        pk.put<int>(m.swap_xy ? 1 : 0);
-        pk.put<int>(q.pre_scaller);
-        pk.put<int>(q.writable_var);
-        pk.put<int>(cap);
-        pk.put<int>(0);
-        pk.put<long long>(pointsForSkip);
-        pk.put<long long>(pointsInBlock);
-        for (double v : {q.h, q.max_value, q.transient_time, q.t_max, q.eps_dbscan}) pk.put_numb(prec, v);
-        for (int i = 0; i < q.amount_of_x; ++i) pk.put_numb(prec, q.initial_conditions[i]);
-        for (int i = 0; i < std::max(q.n_values, 1); ++i) pk.put_numb(prec, i < q.n_values ? q.base_values[i] : 0.0);
-        pk.put<const void*>(ws + off0);
-        pk.put<const void*>(ws + off1);
-        pk.put<void*>(peaks);
-        pk.put<void*>(helpful);
-        pk.put<void*>(d_values);
-        pk.put<void*>(d_flags);
-        pk.put<void*>(ws);
-        pk.put<void*>(ws + 8);
-        const int block = 128;
-        if (!launch_packed(e, fn, persistent_grid(e, fn, block, cells), block, e->stream, pk, err)) rc = UCB_E_CUDA;
-        if (q.progress) *q.progress = (float)(c0 + cells) / (float)total;
-    }
+    if (!launch_packed(e, fn, grid, block, e->stream, pk, err)) rc = UCB_E_CUDA;
     cudaEventRecord(e->ev1, e->stream);
     unsigned long long steps = 0;
     if (rc == UCB_OK) {
@@ -241,7 +234,8 @@ extern "C" int ucb_run_bif2d(ucb_engine* e, const ucb_bif2d_request* req, ucb_bi
     }
     cudaFreeAsync(d_values, e->stream);
     cudaFreeAsync(d_flags, e->stream);
-    cudaFreeAsync(d_scratch, e->stream);
+    cudaFreeAsync(d_slots, e->stream);
+    cudaFreeAsync(d_work, e->stream);
     cudaStreamSynchronize(e->stream);
     if (rc != UCB_OK) return fail(e, res, rc, err);
     float ms = 0;

@@ -60,6 +60,19 @@ bool ensure_init(ucb_engine* e, std::string& err) {
     }
     d.cuInit(0);
     cudaDeviceGetAttribute(&e->sm_count, cudaDevAttrMultiProcessorCount, e->device);
+    {
+        cudaMemPoolProps props{};
+        props.allocType = cudaMemAllocationTypePinned;
+        props.location.type = cudaMemLocationTypeDevice;
+        props.location.id = e->device;
+        if (cudaMemPoolCreate(&e->pool, &props) == cudaSuccess) {
+            unsigned long long keep = ~0ULL;
+            cudaMemPoolSetAttribute(e->pool, cudaMemPoolAttrReleaseThreshold, &keep);
+        } else {
+            e->pool = nullptr;  // the device's default pool then
+            cudaGetLastError();
+        }
+    }
     if ((ce = cudaStreamCreateWithFlags(&e->stream, cudaStreamNonBlocking)) != cudaSuccess ||
         (ce = cudaEventCreate(&e->ev0)) != cudaSuccess || (ce = cudaEventCreate(&e->ev1)) != cudaSuccess) {
         err = std::string("stream/event creation: ") + cudaGetErrorString(ce);
@@ -641,6 +654,7 @@ void ucb_destroy(ucb_engine* e) {
         if (e->ev0) cudaEventDestroy(e->ev0);
         if (e->ev1) cudaEventDestroy(e->ev1);
         if (e->stream) cudaStreamDestroy(e->stream);
+        if (e->pool) cudaMemPoolDestroy(e->pool);
     }
     delete e;
 }
@@ -650,7 +664,12 @@ const char* ucb_last_error(const ucb_engine* e) { return e ? e->last_error.c_str
 long long ucb_kernel_launches(const ucb_engine* e) { return e ? e->launches : 0; }
 
 void ucb_clear_cache(ucb_engine* e) {
-    if (e) e->modules.clear();
+    if (!e) return;
+    e->modules.clear();
+    if (e->pool) {
+        if (e->stream) cudaStreamSynchronize(e->stream);
+        cudaMemPoolTrimTo(e->pool, 0);
+    }
 }
 
 static int fail(ucb_engine* e, char* error, int32_t* ok, int code, const std::string& msg) {
@@ -686,8 +705,8 @@ int ucb_run_lle2d(ucb_engine* e, const ucb_lle2d_request* req, ucb_lle2d_result*
     double* d_values = nullptr;
     int32_t* d_flags = nullptr;
     cudaError_t ce;
-    if ((ce = cudaMallocAsync((void**)&d_values, total * sizeof(double), e->stream)) != cudaSuccess ||
-        (ce = cudaMallocAsync((void**)&d_flags, total * sizeof(int32_t), e->stream)) != cudaSuccess)
+    if ((ce = dev_alloc(e, (void**)&d_values, total * sizeof(double), e->stream)) != cudaSuccess ||
+        (ce = dev_alloc(e, (void**)&d_flags, total * sizeof(int32_t), e->stream)) != cudaSuccess)
         return fail(e, res->error, &res->ok, UCB_E_CUDA, std::string("cudaMallocAsync: ") + cudaGetErrorString(ce));
     cudaEventRecord(e->ev0, e->stream);
     int rc = enqueue_lle(e, q, plan, L, d_values, d_flags, e->stream, err);
@@ -771,8 +790,8 @@ int ucb_run_lle1d(ucb_engine* e, const ucb_lle1d_request* req, ucb_lle1d_result*
     double* d_values = nullptr;
     int32_t* d_flags = nullptr;
     cudaError_t ce;
-    if ((ce = cudaMallocAsync((void**)&d_values, (size_t)n * sizeof(double), e->stream)) != cudaSuccess ||
-        (ce = cudaMallocAsync((void**)&d_flags, (size_t)n * sizeof(int32_t), e->stream)) != cudaSuccess)
+    if ((ce = dev_alloc(e, (void**)&d_values, (size_t)n * sizeof(double), e->stream)) != cudaSuccess ||
+        (ce = dev_alloc(e, (void**)&d_flags, (size_t)n * sizeof(int32_t), e->stream)) != cudaSuccess)
         return fail(e, res->error, &res->ok, UCB_E_CUDA, std::string("cudaMallocAsync: ") + cudaGetErrorString(ce));
     cudaEventRecord(e->ev0, e->stream);
     int rc = enqueue_lle(e, q, plan, L, d_values, d_flags, e->stream, err);
@@ -829,7 +848,7 @@ int ucb_lle2d_states(ucb_engine* e, const ucb_lle2d_request* req, long long n_st
     const long long total = (long long)req->n_pts * req->n_pts;
     const size_t bytes = (size_t)total * req->amount_of_x * sizeof(double);
     double* d_out = nullptr;
-    cudaError_t ce = cudaMallocAsync((void**)&d_out, bytes, e->stream);
+    cudaError_t ce = dev_alloc(e, (void**)&d_out, bytes, e->stream);
     if (ce != cudaSuccess) { e->last_error = cudaGetErrorString(ce); return UCB_E_CUDA; }
     LlePlan p2 = plan;
     p2.amountOfPointsForSkip = (int)n_steps;

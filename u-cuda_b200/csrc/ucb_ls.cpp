@@ -139,8 +139,8 @@ int ls_run(ucb_engine* e, const ucb_ls2d_request& q, const SweepMap& m, int n_bl
     double* d_values = nullptr;
     int32_t* d_flags = nullptr;
     cudaError_t ce;
-    if ((ce = cudaMallocAsync((void**)&d_values, (size_t)total * nx * 8, e->stream)) != cudaSuccess ||
-        (ce = cudaMallocAsync((void**)&d_flags, (size_t)total * 4, e->stream)) != cudaSuccess)
+    if ((ce = dev_alloc(e, (void**)&d_values, (size_t)total * nx * 8, e->stream)) != cudaSuccess ||
+        (ce = dev_alloc(e, (void**)&d_flags, (size_t)total * 4, e->stream)) != cudaSuccess)
         return fail(e, res, UCB_E_CUDA, std::string("cudaMallocAsync: ") + cudaGetErrorString(ce));
 
     const double rtol = q.rtol > 0 ? q.rtol : (prec == UCB_PREC_F64 ? 1e-8 : 1e-5);
