@@ -72,11 +72,34 @@ typedef struct ucb_options {
     int32_t lle_method;  /* UCB_LLE_* */
     int32_t nominal_steps; /* 0: reference step counts (extra step after every loop call,
                               cudaLibrary.cu:863-866); 1: nominal counts */
-    int32_t block_threads; /* 0: autotuned; else threads per block (multiple of 32) */
-    int32_t reserved[3];
+    /* Launch shape. 0 in a field: the value an earlier ucb_autotune_* call chose for this
+     * kernel build on this device (kept by the engine and in the table beside the CUBIN
+     * cache), else the default (128 threads, the compiler's register choice, 1 step per
+     * chunk). Set explicitly, a field overrides the tuned value. None changes results. */
+    int32_t block_threads; /* threads per block, multiple of 32, 32..1024 */
+    int32_t max_registers; /* registers per thread cap (--maxrregcount), 0 = compiler's choice */
+    int32_t unroll;        /* steps per unrolled chunk of the run-time-length step loops, 1..16 */
+    int32_t reserved[1];
 } ucb_options;
 
 typedef struct ucb_engine ucb_engine;
+
+/* Outcome of an autotuning search (ucb_autotune_*; no reference counterpart): the launch
+ * shape chosen for one kernel build and what it measured on the trial workload (the
+ * request's own kernel on a coarser grid over the same window with a shortened horizon). */
+typedef struct ucb_tune_report {
+    int32_t block_threads, max_registers, unroll;
+    int32_t candidates;        /* configurations timed */
+    int32_t registers;         /* registers per thread of the chosen build */
+    int32_t blocks_per_sm;     /* resident blocks per SM of the chosen build */
+    double best_ms;            /* trial kernel time, chosen shape */
+    double default_ms;         /* trial kernel time, default shape */
+    double wall_ms;            /* whole search, compiles included */
+    int32_t trial_n_pts;       /* trial grid */
+    int32_t from_table;        /* 1: found in the tuned table, nothing timed */
+    char key[32];              /* kernel build identity (hash) */
+    char error[256];
+} ucb_tune_report;
 
 /* Creates an engine bound to CUDA device `device` (the reference always uses device 0,
  * parametric_engine.cpp:1490). Creation needs no GPU: the device is initialised by the
@@ -485,6 +508,22 @@ typedef struct ucb_basins_recluster_result {
 UCB_API int ucb_run_basins_recluster(ucb_engine* e, const ucb_basins_recluster_request* req,
                                      ucb_basins_recluster_result* res);
 
+/* ------------------------------------------------------------------------------------
+ * Autotuning (no reference counterpart). Searches the launch shape (threads per block,
+ * register cap, steps per unrolled chunk; ucb_options) of the kernel build the request
+ * would run: each candidate runs the request's own entry point on a trial workload (the
+ * same window on a coarser grid, horizon shortened to about 1.2e10 steps; the Bif-2D trial
+ * keeps the horizon), timed with CUDA events; coordinate descent, 2 % to win. The chosen
+ * shape is used by later calls of any engine on this device whose option fields are 0
+ * (it is kept by the engine and appended to the table beside the CUBIN cache). force = 0
+ * returns a shape already in the table without timing anything. Results never change:
+ * the shape is not part of the arithmetic.
+ * ---------------------------------------------------------------------------------- */
+UCB_API int ucb_autotune_lle2d(ucb_engine* e, const ucb_lle2d_request* req, int32_t force, ucb_tune_report* rep);
+UCB_API int ucb_autotune_ls2d(ucb_engine* e, const ucb_ls2d_request* req, int32_t force, ucb_tune_report* rep);
+UCB_API int ucb_autotune_basins(ucb_engine* e, const ucb_basins_request* req, int32_t force, ucb_tune_report* rep);
+UCB_API int ucb_autotune_bif2d(ucb_engine* e, const ucb_bif2d_request* req, int32_t force, ucb_tune_report* rep);
+
 /* LLE map without device allocation (no counterpart in the reference).
  *
  * ucb_lle2d_device() keeps its scratch (work-queue counter, step counter, axis value
@@ -522,7 +561,9 @@ UCB_API int ucb_lle2d_states(ucb_engine* e, const ucb_lle2d_request* req, long l
 
 /* Measures the FMA throughput of the FP64 (precision = UCB_PREC_F64) or FP32 pipe of the
  * current device in TFLOP/s (2 FLOPs per FMA): the roofline denominator of the integrator
- * kernels. No reference counterpart (the reference publishes no measurements). */
+ * kernels; UCB_PEAK_F32X2 measures packed FP32 pairs (two FMAs per instruction, sm_100).
+ * No reference counterpart (the reference publishes no measurements). */
+#define UCB_PEAK_F32X2 2
 UCB_API int ucb_measure_fma_peak(int precision, double* tflops);
 
 /* ------------------------------------------------------------------------------------

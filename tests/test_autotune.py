@@ -1,0 +1,85 @@
+"""Launch-shape autotuning (ucb_autotune_*): the shape knobs compile for every kernel, bad
+option values are rejected the reference's way, a search picks a shape that later runs
+use, and no shape changes a single result bit."""
+import numpy as np
+import pytest
+
+import ucb
+from helpers import DUFFING, LORENZ, engine_request, lle2d_case, rk4_body
+
+SHAPES = [dict(block_threads=256), dict(block_threads=64, unroll=4), dict(max_registers=64, unroll=2),
+          dict(block_threads=512, max_registers=64)]
+
+
+@pytest.mark.parametrize("shape", SHAPES)
+def test_shapes_compile_for_every_kernel(shape):
+    for prec, mode in ((ucb.PREC_F64, ucb.MODE_EXACT), (ucb.PREC_F32, ucb.MODE_NATIVE)):
+        opt = dict(precision=prec, mode=mode, **shape)
+        ucb.precompile(engine_request(ucb, lle2d_case(), **opt))
+        ucb.precompile(ucb.Engine.bif2d_request(rk4_body(LORENZ), 3, (0.1, 0.1, 0.1), (0, 10.0, 28.0, 8 / 3),
+                                                n_pts=8, param_index=2, param_index_2=1, param_lo=20, param_hi=30,
+                                                param_lo_2=5, param_hi_2=15, opt=ucb.options(**opt)))
+        ucb.precompile(ucb.Engine.basins_request(rk4_body(DUFFING), 3, (0, 0, 0), (0.0,), n_pts=8, phase_var=2,
+                                                 period=2 * np.pi, opt=ucb.options(**opt)))
+        ucb.precompile(ucb.Engine.basins_dbscan_request(rk4_body(LORENZ), 3, (0, 0, 25.0), (0, 10.0, 10.0, 8 / 3),
+                                                        n_pts=8, opt=ucb.options(**opt)))
+
+
+@pytest.mark.parametrize("field,value,msg", [("block_threads", 48, "block_threads must be"),
+                                             ("block_threads", 2048, "block_threads must be"),
+                                             ("max_registers", 8, "max_registers must be"),
+                                             ("unroll", 17, "unroll must be")])
+def test_bad_shape_options_are_rejected(field, value, msg):
+    with pytest.raises(ucb.UcbError, match=msg):
+        ucb.precompile(engine_request(ucb, lle2d_case(), **{field: value}))
+
+
+@pytest.mark.gpu
+def test_autotune_lle2d_keeps_results_and_is_reused(tmp_path, monkeypatch):
+    monkeypatch.setenv("UCB_TUNE_TABLE", str(tmp_path / "tuned.tsv"))
+    c = lle2d_case(n=48, t_max=10.0, transient=5.0)
+    eng = ucb.Engine(0)
+    req = engine_request(ucb, c, precision=ucb.PREC_F64, mode=ucb.MODE_EXACT)
+    ref, rflags, _ = eng.run_lle2d(req)
+    rep = eng.autotune(req, force=True)
+    assert rep["candidates"] >= 3 and rep["from_table"] == 0
+    assert rep["block_threads"] in (64, 128, 256, 512) and rep["unroll"] in (1, 2, 4)
+    assert rep["best_ms"] > 0 and rep["best_ms"] <= rep["default_ms"] and rep["registers"] > 0
+    # the tuned shape is used by later runs and changes nothing
+    vals, flags, _ = eng.run_lle2d(req)
+    np.testing.assert_array_equal(vals, ref)
+    np.testing.assert_array_equal(flags, rflags)
+    for shape in SHAPES:
+        v, _, _ = eng.run_lle2d(engine_request(ucb, c, precision=ucb.PREC_F64, mode=ucb.MODE_EXACT, **shape))
+        np.testing.assert_array_equal(v, ref)
+    eng.close()
+    # a new engine finds the shape in the table
+    eng2 = ucb.Engine(0)
+    rep2 = eng2.autotune(req)
+    assert rep2["from_table"] == 1 and rep2["key"] == rep["key"]
+    assert (rep2["block_threads"], rep2["max_registers"], rep2["unroll"]) == \
+        (rep["block_threads"], rep["max_registers"], rep["unroll"])
+    eng2.close()
+
+
+@pytest.mark.gpu
+def test_autotune_basins_and_bif2d(tmp_path, monkeypatch):
+    monkeypatch.setenv("UCB_TUNE_TABLE", str(tmp_path / "tuned.tsv"))
+    eng = ucb.Engine(0)
+    breq = ucb.Engine.basins_request(rk4_body(DUFFING), 3, (0.0, 0.0, 0.0), (0.0,), n_pts=32, axis_x_lo=-2.5,
+                                     axis_x_hi=2.5, axis_y_lo=-2.5, axis_y_hi=2.5, period=2 * np.pi,
+                                     steps_per_period=200, max_periods=60, phase_var=2,
+                                     opt=ucb.options(precision=ucb.PREC_F64, mode=ucb.MODE_EXACT))
+    ref = eng.run_basins(breq)[0]
+    rep = eng.autotune(breq, force=True)
+    assert rep["candidates"] >= 3
+    np.testing.assert_array_equal(eng.run_basins(breq)[0], ref)
+    b2 = ucb.Engine.bif2d_request(rk4_body(LORENZ), 3, (0.1, 0.1, 0.1), (0, 10.0, 28.0, 8 / 3), n_pts=24,
+                                  param_index=2, param_index_2=1, param_lo=20.0, param_hi=200.0, param_lo_2=5.0,
+                                  param_hi_2=15.0, h=0.01, transient_time=20.0, t_max=40.0, eps_dbscan=0.1,
+                                  opt=ucb.options(precision=ucb.PREC_F64, mode=ucb.MODE_EXACT))
+    ref2 = eng.run_bif2d(b2)[0]
+    rep2 = eng.autotune(b2, force=True)
+    assert rep2["candidates"] >= 3
+    np.testing.assert_array_equal(eng.run_bif2d(b2)[0], ref2)
+    eng.close()

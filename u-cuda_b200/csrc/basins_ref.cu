@@ -564,6 +564,11 @@ extern "C" int ucb_precompile_basins_dbscan(const ucb_basins_dbscan_request* req
     }
     SystemCode sys;
     CompileRequest rq = features_request(*req, sys);
+    TuneConfig shape;
+    if (!tune_request(nullptr, req->opt, 128, rq, shape, err)) {
+        if (err_out && err_len > 0) std::snprintf(err_out, (size_t)err_len, "%s", err.c_str());
+        return UCB_E_INVALID;
+    }
     if (!precompile_to_disk(rq, err)) {
         if (err_out && err_len > 0) std::snprintf(err_out, (size_t)err_len, "%s", err.c_str());
         return UCB_E_COMPILE;
@@ -595,6 +600,8 @@ extern "C" int ucb_run_basins_dbscan(ucb_engine* e, const ucb_basins_dbscan_requ
     if (!ensure_init(e, err)) return fail(e, res, UCB_E_NOGPU, err);
     SystemCode sys;
     CompileRequest rq = features_request(q, sys);
+    TuneConfig shape;
+    if (!tune_request(e, q.opt, 128, rq, shape, err)) return fail(e, res, UCB_E_INVALID, err);
     auto mod = e->modules.get(rq, err);
     if (!mod) return fail(e, res, UCB_E_COMPILE, err);
     CUfunction fn = mod->functions["ucb_basins_ref_kernel"];
@@ -647,7 +654,7 @@ extern "C" int ucb_run_basins_dbscan(ucb_engine* e, const ucb_basins_dbscan_requ
     pk.put<void*>(ws + 8);
     EventPair cev;
     cudaEventRecord(e->ev0, st);
-    if (!launch_packed(e, fn, persistent_grid(e, fn, 128, total), 128, st, pk, err))
+    if (!launch_packed(e, fn, persistent_grid(e, fn, shape.block, total), shape.block, st, pk, err))
         return fail(e, res, UCB_E_CUDA, err);
     cudaEventRecord(e->ev1, st);
 

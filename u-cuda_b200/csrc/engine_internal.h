@@ -3,8 +3,11 @@
 
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cmath>
 #include <cstdint>
+#include <functional>
+#include <map>
 #include <memory>
 #include <string>
 #include <vector>
@@ -12,6 +15,17 @@
 #include "../../include/ucb.h"
 #include "frontend.h"
 #include "jit.h"
+
+namespace ucb {
+// Launch shape of a kernel build (see ucb_options): threads per block, registers per
+// thread cap (0 = compiler's choice), steps per unrolled chunk of the step loops.
+struct TuneConfig {
+    int block = 128;
+    int maxreg = 0;
+    int unroll = 1;
+    bool operator==(const TuneConfig& o) const { return block == o.block && maxreg == o.maxreg && unroll == o.unroll; }
+};
+}  // namespace ucb
 
 struct ucb_engine {
     int device = 0;
@@ -28,6 +42,10 @@ struct ucb_engine {
     // is freed for the next call (no release threshold) until ucb_clear_cache / destroy.
     cudaMemPool_t pool = nullptr;
     long long launches = 0;
+    // Launch shapes chosen by the autotuner, by kernel-build key (plus the entries of the
+    // on-disk table for this device, read on first use).
+    std::map<std::string, ucb::TuneConfig> tuned;
+    bool tuned_loaded = false;
     // Network of the last surrogate-refined map, kept for reuse by the next call with the
     // same configuration (owned; released with the engine).
     std::shared_ptr<void> surrogate_net;
@@ -65,6 +83,35 @@ bool ensure_workspace(ucb_engine* e, size_t bytes, std::string& err);
 // Stream-ordered device allocation from the engine's pool (released with cudaFreeAsync).
 inline cudaError_t dev_alloc(ucb_engine* e, void** p, size_t bytes, cudaStream_t st) {
     return e->pool ? cudaMallocFromPoolAsync(p, bytes, e->pool, st) : cudaMallocAsync(p, bytes, st);
+}
+
+// ---- autotuning (autotune.cpp) ----
+// Identity of a kernel build without its launch-shape knobs (hex of a 64-bit hash).
+std::string tune_key(const CompileRequest& rq);
+// The launch shape a run uses: explicit option fields first, then the shape tuned for
+// this key (engine memory or the on-disk table; e may be null), else the defaults (with
+// `default_block` threads). False with a message for invalid option fields.
+bool resolve_tuning(ucb_engine* e, const ucb_options& o, const std::string& key, int default_block, TuneConfig& out,
+                    std::string& err);
+// Adds the knobs of a non-default shape to a compile request (defines, --maxrregcount).
+void apply_tuning(CompileRequest& rq, const TuneConfig& c);
+// Resolves and applies in one go; returns the launch shape.
+bool tune_request(ucb_engine* e, const ucb_options& o, int default_block, CompileRequest& rq, TuneConfig& out,
+                  std::string& err);
+// Coordinate search over block size, unroll and register cap. `trial` runs the request's
+// kernel on the trial workload with the given shape (as explicit options) and returns its
+// kernel milliseconds (< 0: the shape failed); `build` gives the compile request of a
+// shape (for the register count and occupancy of the chosen build). The best shape is
+// stored for `key` (engine + on-disk table). force = false returns a stored shape as is.
+int autotune_search(ucb_engine* e, const std::string& key, int default_block, bool force,
+                    const std::function<double(const TuneConfig&)>& trial,
+                    const std::function<CompileRequest(const TuneConfig&)>& build, ucb_tune_report* rep);
+
+// Horizon factor of an autotuning trial: about `target_steps` steps over `cells` cells of
+// `steps_per_cell` steps each (1 when the request is already that small).
+inline double trial_scale(double cells, double steps_per_cell, double target_steps = 1.2e10) {
+    const double full = cells * std::max(steps_per_cell, 1.0);
+    return full <= target_steps ? 1.0 : target_steps / full;
 }
 
 // Builds the step-function source for a run.

@@ -158,6 +158,8 @@ void write_file_atomic(const std::string& path, const std::string& data) {
 
 }  // namespace
 
+std::string cubin_cache_dir() { return cache_dir(); }
+
 bool precompile_to_disk(const CompileRequest& rq, std::string& err) {
     const uint64_t key = request_key(rq);
     const std::string dir = cache_dir();

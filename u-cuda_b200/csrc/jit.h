@@ -83,4 +83,7 @@ private:
 
 uint64_t fnv1a64(const std::string& s, uint64_t h = 1469598103934665603ULL);
 
+// Directory of the on-disk CUBIN cache ("" when unknown).
+std::string cubin_cache_dir();
+
 }  // namespace ucb

@@ -104,6 +104,7 @@ __device__ __forceinline__ void basins_cell(const UcbBasinsParams& p, long long 
     for (int k = 0; k < UCB_MAXK; ++k) run[k] = 0;
     int label = 0, period = 0, n = 0;
     for (n = 1; n <= p.max_periods; ++n) {
+        UCB_STEP_LOOP
         for (int s = 0; s < p.steps_per_period; ++s) st.step(x, a, p.h);
         ns += p.steps_per_period;
 #if UCB_PHASE >= 0
@@ -161,7 +162,7 @@ __device__ __forceinline__ void basins_cell(const UcbBasinsParams& p, long long 
 
 }  // namespace ucbdev
 
-extern "C" __global__ void __launch_bounds__(128) ucb_basins_kernel(const UcbBasinsParams p) {
+extern "C" __global__ void __launch_bounds__(UCB_BLOCK) ucb_basins_kernel(const UcbBasinsParams p) {
     const int lane = threadIdx.x & 31;
     long long ns = 0;
     for (;;) {

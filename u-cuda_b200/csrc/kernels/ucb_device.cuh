@@ -35,6 +35,18 @@ typedef unsigned long long uint64_t;
 #ifndef UCB_EXTRA_STEP
 #define UCB_EXTRA_STEP 1
 #endif
+// Launch-shape knobs set by the autotuner (or the caller's options): threads per block
+// (the kernels' __launch_bounds__) and the number of steps per unrolled chunk of the step
+// loops whose trip count is only known at run time.
+#ifndef UCB_BLOCK
+#define UCB_BLOCK 128
+#endif
+#ifndef UCB_UNROLL
+#define UCB_UNROLL 1
+#endif
+#define UCB_STR_(x) #x
+#define UCB_PRAGMA_(x) _Pragma(UCB_STR_(x))
+#define UCB_STEP_LOOP UCB_PRAGMA_(unroll UCB_UNROLL)
 
 namespace ucbdev {
 
@@ -170,6 +182,7 @@ __device__ __forceinline__ int loop_single(const S& s, numb* x, const numb* a, n
         ns += 1;
         if (diverged(x, maxValue)) return 0;
         const int n = (iters - i0 < kCheckInterval) ? (int)(iters - i0) : kCheckInterval;
+        UCB_STEP_LOOP
         for (int i = 1; i < n; ++i) s.step(x, a, h);
         ns += n - 1;
     }
@@ -198,6 +211,7 @@ __device__ __forceinline__ int loop_pair(const S& s, numb* x, numb* y, const num
         ns += 2;
         if (diverged(x, maxValue) || diverged(y, maxValue)) return 0;
         const int n = (iters - i0 < kCheckInterval) ? (int)(iters - i0) : kCheckInterval;
+        UCB_STEP_LOOP
         for (int i = 1; i < n; ++i) {
             s.step(x, a, h);
             s.step(y, a, h);

@@ -146,6 +146,7 @@ __device__ __forceinline__ int loop_tangent(const S& s, numb* x, numb* v, const 
         ns += 2;
         if (diverged(x, maxValue) || diverged(v, (numb)0)) return 0;
         const int n = (iters - i0 < kCheckInterval) ? (int)(iters - i0) : kCheckInterval;
+        UCB_STEP_LOOP
         for (int i = 1; i < n; ++i) s.step_tangent(x, v, a, h);
         ns += 2 * (n - 1);
     }
@@ -202,7 +203,7 @@ __device__ __forceinline__ double lle_cell_tangent(const UcbLleParams& p, long l
 
 }  // namespace ucbdev
 
-extern "C" __global__ void __launch_bounds__(128) ucb_lle_kernel(const UcbLleParams p) {
+extern "C" __global__ void __launch_bounds__(UCB_BLOCK) ucb_lle_kernel(const UcbLleParams p) {
     const int lane = threadIdx.x & 31;
     long long ns = 0;
     for (;;) {
@@ -224,7 +225,7 @@ extern "C" __global__ void __launch_bounds__(128) ucb_lle_kernel(const UcbLlePar
 
 // Final state of every cell after `skip` plain steps from its initial condition (no
 // divergence checks, no extra step): a trajectory-parity aid over the same grid.
-extern "C" __global__ void __launch_bounds__(128) ucb_state_kernel(const UcbLleParams p) {
+extern "C" __global__ void __launch_bounds__(UCB_BLOCK) ucb_state_kernel(const UcbLleParams p) {
     const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= p.total) return;
     const long long kidx = p.cell_offset + i;

@@ -449,7 +449,7 @@ __device__ __forceinline__ void ls_cell_dp5(const UcbLsParams& p, long long kidx
 
 }  // namespace ucbdev
 
-extern "C" __global__ void __launch_bounds__(128) ucb_ls_kernel(const UcbLsParams p) {
+extern "C" __global__ void __launch_bounds__(UCB_BLOCK) ucb_ls_kernel(const UcbLsParams p) {
     const int lane = threadIdx.x & 31;
     long long ns = 0;
     for (;;) {

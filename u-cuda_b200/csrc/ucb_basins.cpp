@@ -72,6 +72,11 @@ extern "C" int ucb_precompile_basins(const ucb_basins_request* req, char* err_ou
     }
     SystemCode sys;
     CompileRequest rq = basins_compile_request(*req, sys);
+    TuneConfig shape;
+    if (!tune_request(nullptr, req->opt, 128, rq, shape, err)) {
+        if (err_out && err_len > 0) std::snprintf(err_out, (size_t)err_len, "%s", err.c_str());
+        return UCB_E_INVALID;
+    }
     if (!precompile_to_disk(rq, err)) {
         if (err_out && err_len > 0) std::snprintf(err_out, (size_t)err_len, "%s", err.c_str());
         return UCB_E_COMPILE;
@@ -99,6 +104,8 @@ extern "C" int ucb_run_basins(ucb_engine* e, const ucb_basins_request* req, ucb_
     if (!ensure_init(e, err)) return fail(e, res, UCB_E_NOGPU, err);
     SystemCode sys;
     CompileRequest rq = basins_compile_request(q, sys);
+    TuneConfig shape;
+    if (!tune_request(e, q.opt, 128, rq, shape, err)) return fail(e, res, UCB_E_INVALID, err);
     auto mod = e->modules.get(rq, err);
     if (!mod) return fail(e, res, UCB_E_COMPILE, err);
     CUfunction fn = mod->functions["ucb_basins_kernel"];
@@ -162,7 +169,7 @@ extern "C" int ucb_run_basins(ucb_engine* e, const ucb_basins_request* req, ucb_
     pk.put<void*>(ws + 16);
     pk.put<void*>(ws);
     pk.put<void*>(ws + 8);
-    const int block = 128;
+    const int block = shape.block;
     cudaEventRecord(e->ev0, st);
     int rc = launch_packed(e, fn, persistent_grid(e, fn, block, total), block, st, pk, err) ? UCB_OK : UCB_E_CUDA;
     // attractor table -> host: merge, order, map
@@ -267,4 +274,60 @@ extern "C" int ucb_run_basins(ucb_engine* e, const ucb_basins_request* req, ucb_
     if (q.progress) *q.progress = 1.0f;
     res->ok = 1;
     return UCB_OK;
+}
+
+extern "C" int ucb_autotune_basins(ucb_engine* e, const ucb_basins_request* req, int32_t force, ucb_tune_report* rep) {
+    if (!e || !req || !rep) return UCB_E_INVALID;
+    std::memset(rep, 0, sizeof *rep);
+    std::string err;
+    auto bad = [&](int code, const std::string& msg) {
+        e->last_error = msg;
+        std::snprintf(rep->error, sizeof rep->error, "%s", msg.c_str());
+        return code;
+    };
+    if (!validate(*req, err)) return bad(UCB_E_INVALID, err);
+    if (!ensure_init(e, err)) return bad(UCB_E_NOGPU, err);
+    ucb_basins_request base = *req;
+    base.opt.block_threads = base.opt.max_registers = base.opt.unroll = 0;
+    base.csv_output_path = nullptr;
+    base.cancel = nullptr;
+    base.progress = nullptr;
+    SystemCode sys;
+    const std::string key = tune_key(basins_compile_request(base, sys));
+    // trial: the same window on at most 768^2 cells; the period cap scaled to about 1.2e10
+    // steps in all (at least 3 x match_count periods, so that converging cells still exit)
+    ucb_basins_request t = base;
+    t.n_pts = std::min(base.n_pts, 768);
+    const double f = trial_scale((double)t.n_pts * t.n_pts, (double)base.max_periods * base.steps_per_period);
+    if (f < 1.0)
+        t.max_periods = std::min(base.max_periods, std::max(3 * base.match_count, (int)(base.max_periods * f)));
+    const size_t cells = (size_t)t.n_pts * t.n_pts;
+    std::vector<int32_t> labels(cells), periods(cells), iters(cells);
+    auto with = [&](const TuneConfig& c) {
+        ucb_basins_request q = t;
+        q.opt.block_threads = c.block;
+        q.opt.max_registers = c.maxreg;
+        q.opt.unroll = c.unroll;
+        return q;
+    };
+    auto trial = [&](const TuneConfig& c) -> double {
+        ucb_basins_request q = with(c);
+        ucb_basins_result r{};
+        r.labels = labels.data();
+        r.periods = periods.data();
+        r.iterations = iters.data();
+        return ucb_run_basins(e, &q, &r) == UCB_OK ? r.kernel_ms : -1.0;
+    };
+    auto build = [&](const TuneConfig& c) {
+        ucb_basins_request q = with(c);
+        SystemCode s2;
+        CompileRequest rq = basins_compile_request(q, s2);
+        TuneConfig shape;
+        std::string e2;
+        tune_request(e, q.opt, 128, rq, shape, e2);
+        return rq;
+    };
+    const int rc = autotune_search(e, key, 128, force != 0, trial, build, rep);
+    rep->trial_n_pts = t.n_pts;
+    return rc;
 }

@@ -78,6 +78,11 @@ extern "C" int ucb_precompile_bif1d(const ucb_bif1d_request* req, char* err_out,
     }
     SystemCode sys;
     CompileRequest rq = bif_compile_request(*req, sys);
+    TuneConfig shape;
+    if (!tune_request(nullptr, req->opt, 32, rq, shape, err)) {
+        if (err_out && err_len > 0) std::snprintf(err_out, (size_t)err_len, "%s", err.c_str());
+        return UCB_E_INVALID;
+    }
     if (!precompile_to_disk(rq, err)) {
         if (err_out && err_len > 0) std::snprintf(err_out, (size_t)err_len, "%s", err.c_str());
         return UCB_E_COMPILE;
@@ -114,6 +119,8 @@ extern "C" int ucb_run_bif1d(ucb_engine* e, const ucb_bif1d_request* req, ucb_bi
 
     SystemCode sys;
     CompileRequest rq = bif_compile_request(q, sys);
+    TuneConfig shape;
+    if (!tune_request(e, q.opt, 32, rq, shape, err)) return fail(e, res, UCB_E_INVALID, err);
     auto mod = e->modules.get(rq, err);
     if (!mod) return fail(e, res, UCB_E_COMPILE, err);
     CUfunction fn = mod->functions["ucb_bif_kernel"];
@@ -156,7 +163,7 @@ extern "C" int ucb_run_bif1d(ucb_engine* e, const ucb_bif1d_request* req, ucb_bi
     pk.put<void*>(d_int);
     pk.put<void*>(ws);
     pk.put<void*>(ws + 8);
-    const int block = 32;  // latency-bound: spread the few sweep points over many SMs
+    const int block = shape.block;  // default 32: latency-bound, spread the few points over many SMs
     cudaEventRecord(e->ev0, e->stream);
     const bool launched = launch_packed(e, fn, (n + block - 1) / block, block, e->stream, pk, err);
     cudaEventRecord(e->ev1, e->stream);

@@ -110,6 +110,11 @@ extern "C" int ucb_precompile_bif2d(const ucb_bif2d_request* req, char* err_out,
     }
     SystemCode sys;
     CompileRequest rq = bif2d_compile_request(*req, m, sys);
+    TuneConfig shape;
+    if (!tune_request(nullptr, req->opt, 128, rq, shape, err)) {
+        if (err_out && err_len > 0) std::snprintf(err_out, (size_t)err_len, "%s", err.c_str());
+        return UCB_E_INVALID;
+    }
     if (!precompile_to_disk(rq, err)) {
         if (err_out && err_len > 0) std::snprintf(err_out, (size_t)err_len, "%s", err.c_str());
         return UCB_E_COMPILE;
@@ -146,6 +151,8 @@ extern "C" int ucb_run_bif2d(ucb_engine* e, const ucb_bif2d_request* req, ucb_bi
 
     SystemCode sys;
     CompileRequest rq = bif2d_compile_request(q, m, sys);
+    TuneConfig shape;
+    if (!tune_request(e, q.opt, 128, rq, shape, err)) return fail(e, res, UCB_E_INVALID, err);
     auto mod = e->modules.get(rq, err);
     if (!mod) return fail(e, res, UCB_E_COMPILE, err);
     CUfunction fn = mod->functions["ucb_bif2d_kernel"];
@@ -156,7 +163,7 @@ extern "C" int ucb_run_bif2d(ucb_engine* e, const ucb_bif2d_request* req, ucb_bi
     const int cap = (int)std::min<long long>(kMaxAmountOfPeaks, pointsInBlock / 2 + 2);
     // Scratch per resident warp: 32 rows of peaks + dbscan labels and stack slots. The
     // persistent grid is trimmed if the slots would exceed 40 % of the free memory.
-    const int block = 128, warps_per_block = block / 32;
+    const int block = shape.block, warps_per_block = block / 32;
     const size_t per_warp = (size_t)cap * (32 * esz + 2 * sizeof(int32_t));
     int grid = persistent_grid(e, fn, block, total);
     size_t free_b = 0, total_b = 0;
@@ -269,4 +276,59 @@ extern "C" int ucb_run_bif2d(ucb_engine* e, const ucb_bif2d_request* req, ucb_bi
     if (q.progress) *q.progress = 1.0f;
     res->ok = 1;
     return UCB_OK;
+}
+
+extern "C" int ucb_autotune_bif2d(ucb_engine* e, const ucb_bif2d_request* req, int32_t force, ucb_tune_report* rep) {
+    if (!e || !req || !rep) return UCB_E_INVALID;
+    std::memset(rep, 0, sizeof *rep);
+    std::string err;
+    auto bad = [&](int code, const std::string& msg) {
+        e->last_error = msg;
+        std::snprintf(rep->error, sizeof rep->error, "%s", msg.c_str());
+        return code;
+    };
+    SweepMap m;
+    if (!plan_bif2d(*req, m, err)) return bad(UCB_E_INVALID, err);
+    if (!ensure_init(e, err)) return bad(UCB_E_NOGPU, err);
+    ucb_bif2d_request base = *req;
+    base.opt.block_threads = base.opt.max_registers = base.opt.unroll = 0;
+    base.csv_output_path = nullptr;
+    base.cancel = nullptr;
+    base.progress = nullptr;
+    SystemCode sys;
+    const std::string key = tune_key(bif2d_compile_request(base, m, sys));
+    // trial: the same window on at most 512^2 cells, the same horizon (the per-cell peak
+    // count, and with it the dbscan's share, depends on it)
+    ucb_bif2d_request t = base;
+    t.n_pts = std::min(base.n_pts, 512);
+    std::vector<double> vals((size_t)t.n_pts * t.n_pts);
+    std::vector<int32_t> flags(vals.size());
+    auto with = [&](const TuneConfig& c) {
+        ucb_bif2d_request q = t;
+        q.opt.block_threads = c.block;
+        q.opt.max_registers = c.maxreg;
+        q.opt.unroll = c.unroll;
+        return q;
+    };
+    auto trial = [&](const TuneConfig& c) -> double {
+        ucb_bif2d_request q = with(c);
+        ucb_bif2d_result r{};
+        r.values = vals.data();
+        r.flags = flags.data();
+        return ucb_run_bif2d(e, &q, &r) == UCB_OK ? r.kernel_ms : -1.0;
+    };
+    auto build = [&](const TuneConfig& c) {
+        ucb_bif2d_request q = with(c);
+        SweepMap m2;
+        std::string e2;
+        plan_bif2d(q, m2, e2);
+        SystemCode s2;
+        CompileRequest rq = bif2d_compile_request(q, m2, s2);
+        TuneConfig shape;
+        tune_request(e, q.opt, 128, rq, shape, e2);
+        return rq;
+    };
+    const int rc = autotune_search(e, key, 128, force != 0, trial, build, rep);
+    rep->trial_n_pts = t.n_pts;
+    return rc;
 }

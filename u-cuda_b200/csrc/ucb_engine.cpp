@@ -383,6 +383,7 @@ struct LleLaunch {
     CUfunction fn = nullptr;
     SystemCode sys;
     bool tangent = false;
+    TuneConfig shape;  // launch shape (block size used by the launch)
 };
 
 CompileRequest lle_compile_request(const ucb_lle2d_request& q, const LlePlan& plan, LleLaunch& L) {
@@ -408,8 +409,17 @@ CompileRequest lle_compile_request(const ucb_lle2d_request& q, const LlePlan& pl
     return rq;
 }
 
+// The compile request with the launch shape of this run applied (e may be null: explicit
+// options only).
+bool lle_tuned_request(ucb_engine* e, const ucb_lle2d_request& q, const LlePlan& plan, LleLaunch& L,
+                       CompileRequest& rq, std::string& err) {
+    rq = lle_compile_request(q, plan, L);
+    return tune_request(e, q.opt, 128, rq, L.shape, err);
+}
+
 bool prepare_lle(ucb_engine* e, const ucb_lle2d_request& q, const LlePlan& plan, LleLaunch& L, std::string& err) {
-    CompileRequest rq = lle_compile_request(q, plan, L);
+    CompileRequest rq;
+    if (!lle_tuned_request(e, q, plan, L, rq, err)) return false;
     L.mod = e->modules.get(rq, err);
     if (!L.mod) return false;
     L.fn = L.mod->functions["ucb_lle_kernel"];
@@ -463,7 +473,7 @@ int enqueue_lle_fn(ucb_engine* e, const ucb_lle2d_request& q, const LlePlan& pla
                                         ws + off_ax0, ws + off_ax1, d_values, d_flags, ws, ws + 8, d_cell_list,
                                          list_compact ? 1 : 0);
     }
-    const int block = 128;
+    const int block = L.shape.block;
     const int grid = persistent ? persistent_grid(e, L.fn, block, total) : (int)((total + block - 1) / block);
     size_t psize = params.size();
     void* cfg[] = {CU_LAUNCH_PARAM_BUFFER_POINTER, params.data(), CU_LAUNCH_PARAM_BUFFER_SIZE, &psize,
@@ -585,7 +595,12 @@ int lle2d_plan_and_find(ucb_engine* e, const ucb_lle2d_request& q, bool load_if_
     if (!plan_lle2d(q, *plan, err)) { delete plan; return UCB_E_INVALID; }
     if (!ensure_init(e, err)) { delete plan; return UCB_E_NOGPU; }
     auto* L = new LleLaunch;
-    CompileRequest rq = lle_compile_request(q, *plan, *L);
+    CompileRequest rq;
+    if (!lle_tuned_request(e, q, *plan, *L, rq, err)) {
+        delete plan;
+        delete L;
+        return UCB_E_INVALID;
+    }
     L->mod = load_if_missing ? e->modules.get(rq, err) : e->modules.find(rq);
     if (!L->mod) {
         if (!load_if_missing)
@@ -877,7 +892,11 @@ int ucb_precompile_lle2d(const ucb_lle2d_request* req, char* err_out, int err_le
         return UCB_E_INVALID;
     }
     LleLaunch L;
-    CompileRequest rq = lle_compile_request(*req, plan, L);
+    CompileRequest rq;
+    if (!lle_tuned_request(nullptr, *req, plan, L, rq, err)) {
+        if (err_out && err_len > 0) std::snprintf(err_out, (size_t)err_len, "%s", err.c_str());
+        return UCB_E_INVALID;
+    }
     if (!precompile_to_disk(rq, err)) {
         if (err_out && err_len > 0) std::snprintf(err_out, (size_t)err_len, "%s", err.c_str());
         return UCB_E_COMPILE;
@@ -925,6 +944,68 @@ int ucb_lle2d_cells(ucb_engine* e, const ucb_lle2d_request* req, const long long
     res->n_pts = req->n_pts;
     res->ok = 1;
     return UCB_OK;
+}
+
+int ucb_autotune_lle2d(ucb_engine* e, const ucb_lle2d_request* req, int32_t force, ucb_tune_report* rep) {
+    if (!e || !req || !rep) return UCB_E_INVALID;
+    std::memset(rep, 0, sizeof *rep);
+    LlePlan plan;
+    std::string err;
+    auto bad = [&](int code, const std::string& m) {
+        e->last_error = m;
+        std::snprintf(rep->error, sizeof rep->error, "%s", m.c_str());
+        return code;
+    };
+    if (!plan_lle2d(*req, plan, err)) return bad(UCB_E_INVALID, err);
+    if (!ensure_init(e, err)) return bad(UCB_E_NOGPU, err);
+    // the kernel build of the request itself (its key), shape fields cleared
+    ucb_lle2d_request base = *req;
+    base.opt.block_threads = base.opt.max_registers = base.opt.unroll = 0;
+    base.csv_output_path = nullptr;
+    base.cancel = nullptr;
+    base.progress = nullptr;
+    LleLaunch L0;
+    const std::string key = tune_key(lle_compile_request(base, plan, L0));
+    // trial workload: the same window on a grid of at most 768^2 cells (a few resident
+    // waves), horizon scaled to about 1.2e10 steps in all
+    ucb_lle2d_request t = base;
+    t.n_pts = std::min(base.n_pts, 768);
+    const double steps_cell =
+        plan.amountOfPointsForSkip + (double)plan.amountOfPointsInBlock * 2.0 * (double)(plan.nt_steps + 1);
+    const double f = trial_scale((double)t.n_pts * t.n_pts, steps_cell);
+    if (f < 1.0) {
+        t.t_max = std::max(base.NT, std::floor(base.t_max * f / base.NT) * base.NT);
+        t.transient_time = base.transient_time * f;
+    }
+    LlePlan tp;
+    if (!plan_lle2d(t, tp, err)) return bad(UCB_E_INVALID, "trial request: " + err);
+    std::vector<double> vals((size_t)t.n_pts * t.n_pts);
+    std::vector<int32_t> flags(vals.size());
+    auto with = [&](const TuneConfig& c) {
+        ucb_lle2d_request q = t;
+        q.opt.block_threads = c.block;
+        q.opt.max_registers = c.maxreg;
+        q.opt.unroll = c.unroll;
+        return q;
+    };
+    auto trial = [&](const TuneConfig& c) -> double {
+        ucb_lle2d_request q = with(c);
+        ucb_lle2d_result r{};
+        r.values = vals.data();
+        r.flags = flags.data();
+        return ucb_run_lle2d(e, &q, &r) == UCB_OK ? r.kernel_ms : -1.0;
+    };
+    auto build = [&](const TuneConfig& c) {
+        ucb_lle2d_request q = with(c);
+        LleLaunch L;
+        CompileRequest rq;
+        std::string e2;
+        lle_tuned_request(e, q, tp, L, rq, e2);
+        return rq;
+    };
+    const int rc = autotune_search(e, key, 128, force != 0, trial, build, rep);
+    rep->trial_n_pts = t.n_pts;
+    return rc;
 }
 
 }  // extern "C"

@@ -85,6 +85,11 @@ extern "C" int ucb_precompile_ls2d(const ucb_ls2d_request* req, char* err_out, i
         if (err_out && err_len > 0) std::snprintf(err_out, (size_t)err_len, "%s", sys.note.c_str());
         return UCB_E_INVALID;
     }
+    TuneConfig shape;
+    if (!tune_request(nullptr, req->opt, 128, rq, shape, err)) {
+        if (err_out && err_len > 0) std::snprintf(err_out, (size_t)err_len, "%s", err.c_str());
+        return UCB_E_INVALID;
+    }
     if (!precompile_to_disk(rq, err)) {
         if (err_out && err_len > 0) std::snprintf(err_out, (size_t)err_len, "%s", err.c_str());
         return UCB_E_COMPILE;
@@ -116,6 +121,8 @@ int ls_run(ucb_engine* e, const ucb_ls2d_request& q, const SweepMap& m, int n_bl
     CompileRequest rq = ls_compile_request(q, m, sys);
     if (dp5 && !sys.has_jvp)
         return fail(e, res, UCB_E_INVALID, "the DP5 method needs a recognised RK4 body: " + sys.note);
+    TuneConfig shape;
+    if (!tune_request(e, q.opt, 128, rq, shape, err)) return fail(e, res, UCB_E_INVALID, err);
     auto mod = e->modules.get(rq, err);
     if (!mod) return fail(e, res, UCB_E_COMPILE, err);
     CUfunction fn = mod->functions["ucb_ls_kernel"];
@@ -169,7 +176,7 @@ int ls_run(ucb_engine* e, const ucb_ls2d_request& q, const SweepMap& m, int n_bl
     pk.put<void*>(d_flags);
     pk.put<void*>(ws);
     pk.put<void*>(ws + 8);
-    const int block = 128;
+    const int block = shape.block;
     const int grid = persistent_grid(e, fn, block, total);
     cudaEventRecord(e->ev0, e->stream);
     int rc = launch_packed(e, fn, grid, block, e->stream, pk, err) ? UCB_OK : UCB_E_CUDA;
@@ -333,4 +340,78 @@ extern "C" int ucb_run_ls1d(ucb_engine* e, const ucb_ls1d_request* req, ucb_ls1d
     if (q1.progress) *q1.progress = 1.0f;
     res->ok = 1;
     return UCB_OK;
+}
+
+extern "C" int ucb_autotune_ls2d(ucb_engine* e, const ucb_ls2d_request* req, int32_t force, ucb_tune_report* rep) {
+    if (!e || !req || !rep) return UCB_E_INVALID;
+    std::memset(rep, 0, sizeof *rep);
+    std::string err;
+    auto bad = [&](int code, const std::string& msg) {
+        e->last_error = msg;
+        std::snprintf(rep->error, sizeof rep->error, "%s", msg.c_str());
+        return code;
+    };
+    SweepMap m;
+    int n_blocks = 0, skip = 0;
+    long long nt = 0;
+    if (!plan_sweep2d(as_lle(*req), m, n_blocks, skip, nt, err)) return bad(UCB_E_INVALID, err);
+    if (!ensure_init(e, err)) return bad(UCB_E_NOGPU, err);
+    ucb_ls2d_request base = *req;
+    base.opt.block_threads = base.opt.max_registers = base.opt.unroll = 0;
+    base.csv_output_path = nullptr;
+    base.cancel = nullptr;
+    base.progress = nullptr;
+    SystemCode sys;
+    const std::string key = tune_key(ls_compile_request(base, m, sys));
+    // trial: the same window on at most 384^2 cells, horizon scaled to about 1.2e10 steps
+    // (fixed step) or the DP5 interval cut to 50 time units
+    ucb_ls2d_request t = base;
+    t.n_pts = std::min(base.n_pts, 384);
+    const int nx = base.amount_of_x;
+    if (base.method == UCB_LS_DP5) {
+        const double t_end = base.t_end > 0 ? base.t_end : base.t_max;
+        t.t_end = std::min(t_end, 50.0);
+        t.t_max = std::min(base.t_max, t.t_end);
+        t.transient_time = std::min(base.transient_time, 50.0);
+    } else {
+        const double steps_cell = skip + (double)n_blocks * (nx + 1) * (double)(nt + 1);
+        const double f = trial_scale((double)t.n_pts * t.n_pts, steps_cell);
+        if (f < 1.0) {
+            t.t_max = std::max(base.NT, std::floor(base.t_max * f / base.NT) * base.NT);
+            t.transient_time = base.transient_time * f;
+        }
+    }
+    SweepMap tm;
+    if (!plan_sweep2d(as_lle(t), tm, n_blocks, skip, nt, err)) return bad(UCB_E_INVALID, "trial request: " + err);
+    std::vector<double> vals((size_t)t.n_pts * t.n_pts * nx);
+    std::vector<int32_t> flags((size_t)t.n_pts * t.n_pts);
+    std::vector<double> mn(nx), mx(nx);
+    auto with = [&](const TuneConfig& c) {
+        ucb_ls2d_request q = t;
+        q.opt.block_threads = c.block;
+        q.opt.max_registers = c.maxreg;
+        q.opt.unroll = c.unroll;
+        return q;
+    };
+    auto trial = [&](const TuneConfig& c) -> double {
+        ucb_ls2d_request q = with(c);
+        ucb_ls2d_result r{};
+        r.values = vals.data();
+        r.flags = flags.data();
+        r.min_val = mn.data();
+        r.max_val = mx.data();
+        return ucb_run_ls2d(e, &q, &r) == UCB_OK ? r.kernel_ms : -1.0;
+    };
+    auto build = [&](const TuneConfig& c) {
+        ucb_ls2d_request q = with(c);
+        SystemCode s2;
+        CompileRequest rq = ls_compile_request(q, tm, s2);
+        TuneConfig shape;
+        std::string e2;
+        tune_request(e, q.opt, 128, rq, shape, e2);
+        return rq;
+    };
+    const int rc = autotune_search(e, key, 128, force != 0, trial, build, rep);
+    rep->trial_n_pts = t.n_pts;
+    return rc;
 }

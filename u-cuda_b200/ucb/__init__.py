@@ -17,6 +17,7 @@ LIB_PATH = HERE / "libucb.so"
 
 UCB_OK, UCB_E_INVALID, UCB_E_COMPILE, UCB_E_CUDA, UCB_E_CANCELLED, UCB_E_NOGPU = range(6)
 PREC_F64, PREC_F32 = 0, 1
+PEAK_F32X2 = 2  # ucb_measure_fma_peak: packed FP32 pairs
 MODE_NATIVE, MODE_EXACT = 0, 1
 LLE_AUTO, LLE_SHADOW, LLE_TANGENT = 0, 1, 2
 
@@ -29,7 +30,20 @@ class UcbError(RuntimeError):
 
 class Options(C.Structure):
     _fields_ = [("precision", C.c_int32), ("mode", C.c_int32), ("lle_method", C.c_int32),
-                ("nominal_steps", C.c_int32), ("block_threads", C.c_int32), ("reserved", C.c_int32 * 3)]
+                ("nominal_steps", C.c_int32), ("block_threads", C.c_int32), ("max_registers", C.c_int32),
+                ("unroll", C.c_int32), ("reserved", C.c_int32 * 1)]
+
+
+class TuneReport(C.Structure):
+    _fields_ = [("block_threads", C.c_int32), ("max_registers", C.c_int32), ("unroll", C.c_int32),
+                ("candidates", C.c_int32), ("registers", C.c_int32), ("blocks_per_sm", C.c_int32),
+                ("best_ms", C.c_double), ("default_ms", C.c_double), ("wall_ms", C.c_double),
+                ("trial_n_pts", C.c_int32), ("from_table", C.c_int32), ("key", C.c_char * 32),
+                ("error", C.c_char * 256)]
+
+    def as_dict(self):
+        return {f: (getattr(self, f).decode() if f in ("key", "error") else getattr(self, f))
+                for f, _ in self._fields_}
 
 
 class Lle2dRequest(C.Structure):
@@ -318,6 +332,10 @@ def load():
     L.ucb_run_basins_recluster.restype = C.c_int
     L.ucb_run_basins_recluster.argtypes = [C.c_void_p, C.POINTER(BasinsReclusterRequest),
                                            C.POINTER(BasinsReclusterResult)]
+    for fn, req in (("ucb_autotune_lle2d", Lle2dRequest), ("ucb_autotune_ls2d", Ls2dRequest),
+                    ("ucb_autotune_basins", BasinsRequest), ("ucb_autotune_bif2d", Bif2dRequest)):
+        getattr(L, fn).restype = C.c_int
+        getattr(L, fn).argtypes = [C.c_void_p, C.POINTER(req), C.c_int32, C.POINTER(TuneReport)]
     L.ucb_run_lle1d.restype = C.c_int
     L.ucb_run_lle1d.argtypes = [C.c_void_p, C.POINTER(Lle1dRequest), C.POINTER(Lle1dResult)]
     L.ucb_run_ls1d.restype = C.c_int
@@ -355,11 +373,14 @@ def _dptr(a):
     return a.ctypes.data_as(C.POINTER(C.c_double))
 
 
-def options(precision=PREC_F64, mode=MODE_NATIVE, lle_method=LLE_AUTO, nominal_steps=False, block_threads=0):
+def options(precision=PREC_F64, mode=MODE_NATIVE, lle_method=LLE_AUTO, nominal_steps=False, block_threads=0,
+            max_registers=0, unroll=0):
+    """Run options; the launch-shape fields at 0 take the autotuned shape (or the default)."""
     o = Options()
     load().ucb_default_options(C.byref(o))
     o.precision, o.mode, o.lle_method = precision, mode, lle_method
     o.nominal_steps, o.block_threads = int(nominal_steps), block_threads
+    o.max_registers, o.unroll = max_registers, unroll
     return o
 
 
@@ -654,6 +675,18 @@ class Engine:
         if rc != UCB_OK:
             raise UcbError(rc, res.error.decode())
         return labels, res
+
+    # ------------------------------------------------------------------ autotuning
+    def autotune(self, req, force=False) -> dict:
+        """Launch-shape search for the kernel `req` would run (ucb_autotune_*); later runs
+        with the shape fields of their options at 0 use the result."""
+        fn = {Lle2dRequest: "ucb_autotune_lle2d", Ls2dRequest: "ucb_autotune_ls2d",
+              BasinsRequest: "ucb_autotune_basins", Bif2dRequest: "ucb_autotune_bif2d"}[type(req)]
+        rep = TuneReport()
+        rc = getattr(self.lib, fn)(self.h, C.byref(req), int(force), C.byref(rep))
+        if rc != UCB_OK:
+            raise UcbError(rc, rep.error.decode() or self.last_error())
+        return rep.as_dict()
 
     # ------------------------------------------------------------------ bifurcation 1D
     @staticmethod
