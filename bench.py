@@ -317,13 +317,15 @@ def _timed(fn, reps=1):
 OTHER_CONFIGS = ("bif", "spectrum", "basins", "bif2d", "basins_dbscan")
 
 
-def run_other_configs(eng, which=OTHER_CONFIGS):
+def run_other_configs(eng, which=OTHER_CONFIGS, args=None):
     """The other hot-path configurations at their full sizes (one run each after a
     compiling warm-up), with parity summaries against the oracle on sampled cells."""
     import ucb
     from helpers import DUFFING, HYPER_ROSSLER, LORENZ, rk4_body
     from oracle import oracle as O
     out = {}
+    tune = not (args and args.no_autotune)
+    n2 = args.bif2d_n if args else 512
     # Lorenz bifurcation: rho over 1024 values in [20, 200], x0 = (0.1, 0.1, 0.1), h = 0.01,
     # 5,000 transient steps then 20,000 recorded, up to 64 maxima of x per rho.
     body = rk4_body(LORENZ)
@@ -398,7 +400,7 @@ def run_other_configs(eng, which=OTHER_CONFIGS):
                                              period=2 * np.pi, steps_per_period=200, max_periods=2000,
                                              match_count=20, match_tol=1e-6, phase_var=2, max_value=1e6,
                                              opt=ucb.options(precision=prec))
-        shape = eng.autotune(breq(4096))
+        shape = eng.autotune(breq(4096)) if tune else None
         eng.run_basins(breq(8))
         (labels, periods, iters, att, res), ms = _timed(lambda: eng.run_basins(breq(4096)))
         out.setdefault("basins_duffing_4096", {})[name] = {
@@ -409,7 +411,7 @@ def run_other_configs(eng, which=OTHER_CONFIGS):
             ref_labels = labels
         else:
             out["basins_duffing_4096"]["fp32_label_agreement"] = float((labels == ref_labels).mean())
-    # Lorenz period map (run_bifurcation_2d): rho in [20, 200] x sigma in [5, 15] on 512 x 512,
+    # Lorenz period map (run_bifurcation_2d): rho in [20, 200] x sigma in [5, 15] on n x n (512),
     # x0 = (0.1, 0.1, 0.1), h = 0.01, 5,000 transient + 20,000 recorded steps, the peaks of x
     # clustered per cell with eps 0.1.
     for name, opt in (("plain_fp64_exact", dict(precision=ucb.PREC_F64, mode=ucb.MODE_EXACT)),
@@ -423,11 +425,11 @@ def run_other_configs(eng, which=OTHER_CONFIGS):
                                             param_index_2=1, param_lo=20.0, param_hi=200.0, param_lo_2=5.0,
                                             param_hi_2=15.0, h=0.01, transient_time=50.0, t_max=200.0,
                                             eps_dbscan=0.1, writable_var=0, opt=ucb.options(**opt))
-        shape = eng.autotune(b2req(512))
+        shape = eng.autotune(b2req(n2)) if tune else None
         eng.run_bif2d(b2req(4))
-        (vals, flags, res), ms = _timed(lambda: eng.run_bif2d(b2req(512)))
-        out.setdefault("bif2d_lorenz_512", {})[name] = {
-            "wall_ms": ms, "kernel_ms": res.kernel_ms, "cells_per_s": 512 * 512 / (res.kernel_ms * 1e-3),
+        (vals, flags, res), ms = _timed(lambda: eng.run_bif2d(b2req(n2)))
+        out.setdefault(f"bif2d_lorenz_{n2}", {})[name] = {
+            "wall_ms": ms, "kernel_ms": res.kernel_ms, "cells_per_s": n2 * n2 / (res.kernel_ms * 1e-3),
             "rk4_steps_per_s": res.steps / (res.kernel_ms * 1e-3), "max_period": res.max_val, "launch_shape": shape,
             "fixed_point_cells": int((flags < 0).sum())}
     # Basins by the reference's method (run_basins, its request defaults t_max = 1000,
@@ -499,6 +501,9 @@ def main():
                     help="also time the bifurcation, spectrum and basins configurations at full size")
     ap.add_argument("--no-autotune", action="store_true",
                     help="run the default launch shape (128 threads) instead of the autotuned one")
+    ap.add_argument("--no-headline", action="store_true",
+                    help="time only the --configs selection (no LLE headline, surrogate or e2e)")
+    ap.add_argument("--bif2d-n", type=int, default=512, help="grid of the Bif-2D period map configuration")
     ap.add_argument("--configs", default="",
                     help=f"comma-separated subset of {','.join(OTHER_CONFIGS)} to time (instead of --all-configs)")
     ap.add_argument("--surrogate-chen", type=int, default=0, metavar="N",
@@ -539,11 +544,16 @@ def main():
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu = run_cpu_baseline(args.n, args.cpu_stride, 0)
-    results, clocks, launches, e2e_ms = run_ours(args, rank, world, local)
     import ucb
-    surrogate_chen = None
     which = OTHER_CONFIGS if args.all_configs else tuple(c for c in args.configs.split(",") if c)
-    other_configs = run_other_configs(ucb.Engine(local), which) if which and rank == 0 else None
+    if args.no_headline:
+        # only the selected configurations (profiling runs of one kernel), one JSON line
+        if rank == 0:
+            print(json.dumps({"other_configs": run_other_configs(ucb.Engine(local), which, args)}))
+        return
+    results, clocks, launches, e2e_ms = run_ours(args, rank, world, local)
+    surrogate_chen = None
+    other_configs = run_other_configs(ucb.Engine(local), which, args) if which and rank == 0 else None
     if args.surrogate_chen and rank == 0:
         surrogate_chen = [run_surrogate_chen(ucb.Engine(local), torch.device("cuda", local), args.surrogate_chen,
                                              tol, cov) for tol, cov in ((2e-3, 0.995), (2e-2, 0.99))]

@@ -757,11 +757,14 @@ int orc_ls2d_dp5(void* hrhs, void* hdual, int nPts, int par_or_var, int idx0, in
 // counterpart): per cell, RK4 steps_per_period steps per forcing period, the phase
 // variable reset after each period, stroboscopic point P_n = the other state variables;
 // converged when for the smallest k <= 8 |P_n - P_{n-k}|_inf < tol for match_count
-// consecutive periods; canonical point = smallest first (then second) coordinate of the
-// k points of the cycle. out_period: k, 0 (not converged by max_periods), -1 (diverged).
+// consecutive periods, k then reduced to its smallest divisor d with |P_n - P_{n-d}|_inf <=
+// merge (the merge radius of the attractor table); canonical point = smallest first (then
+// second) coordinate of the k points of the cycle. out_period: k, 0 (not converged by
+// max_periods), -1 (diverged).
 int orc_basins(void* h, int nPts, int ax, int ay, double lox, double hix, double loy, double hiy, const double* ic,
                int nv, const double* vals, double period, int steps_per_period, int max_periods, int match_count,
-               double tol, int phase_var, double maxv, const long long* cells, long long ncells, int* out_period,
+               double tol, int phase_var, double maxv, double merge, const long long* cells, long long ncells,
+               int* out_period,
                double* out_cx, double* out_cy, int* out_iters, int nthreads) {
     Krs* k = static_cast<Krs*>(h);
     if (k->numb_bytes != 8) { g_err = "basins oracle is FP64"; return -1; }
@@ -801,6 +804,17 @@ int orc_basins(void* h, int nPts, int ax, int ay, double lox, double hix, double
                 }
             }
             if (found) {
+                // a cycle repeating after a divisor d of its length to within the merge
+                // radius is the period-d orbit
+                for (int dd = 1; dd < found; ++dd) {
+                    if (found % dd) continue;
+                    double d = 0;
+                    for (size_t i = 0; i < P.size(); ++i) d = std::max(d, std::fabs(P[i] - hist[dd - 1][i]));
+                    if (d <= merge) {
+                        found = dd;
+                        break;
+                    }
+                }
                 per = found;
                 cx = P[0];
                 cy = P.size() > 1 ? P[1] : 0.0;

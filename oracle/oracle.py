@@ -68,8 +68,8 @@ def lib():
         L.orc_basins.restype = C.c_int
         L.orc_basins.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_double, C.c_double, C.c_double,
                                  C.c_double, C.c_void_p, C.c_int, C.c_void_p, C.c_double, C.c_int, C.c_int, C.c_int,
-                                 C.c_double, C.c_int, C.c_double, C.c_void_p, C.c_longlong, C.c_void_p, C.c_void_p,
-                                 C.c_void_p, C.c_void_p, C.c_int]
+                                 C.c_double, C.c_int, C.c_double, C.c_double, C.c_void_p, C.c_longlong, C.c_void_p,
+                                 C.c_void_p, C.c_void_p, C.c_void_p, C.c_int]
         L.orc_basins_ref.restype = C.c_int
         L.orc_basins_ref.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_void_p, C.c_void_p, C.c_int,
                                      C.c_void_p, C.c_double, C.c_double, C.c_double, C.c_int, C.c_int, C.c_double,
@@ -310,7 +310,8 @@ def basins(krs: Krs, b: dict, cells=None, nthreads=0):
     rc = lib().orc_basins(krs.h, n, b["axis_x_var"], b["axis_y_var"], b["axis_x_lo"], b["axis_x_hi"],
                           b["axis_y_lo"], b["axis_y_hi"], _ptr(ic), len(vals), _ptr(vals), b["period"],
                           b["steps_per_period"], b["max_periods"], b["match_count"], b["match_tol"],
-                          b.get("phase_var", -1), b["max_value"], _ptr(cells), m if cells is not None else 0,
+                          b.get("phase_var", -1), b["max_value"], b.get("merge_radius", 0.0) or 1e-4, _ptr(cells),
+                          m if cells is not None else 0,
                           _ptr(per), _ptr(cx), _ptr(cy), _ptr(it), nthreads)
     if rc != 0:
         raise RuntimeError(lib().orc_last_error().decode())

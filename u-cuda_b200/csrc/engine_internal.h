@@ -75,6 +75,8 @@ struct SystemCode {
     int flops_rhs = 0;    // FLOPs of one right-hand-side evaluation (recognised bodies)
     int flops_jvp = 0;    // FLOPs of one J(x) v product (recognised bodies)
     std::string note;     // why the exact form was chosen, when native was requested
+    int trig_phase = -1;  // native form: forcing phase variable (ucb_rhs_trig), -1 none
+    double trig_rate = 0; // its constant rate (dX[p]/dt)
 };
 
 bool ensure_init(ucb_engine* e, std::string& err);

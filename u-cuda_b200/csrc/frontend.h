@@ -85,6 +85,13 @@ PNode parse_c_expr(const std::string& text, const std::string& state);
 //   ucb_jvp(const numb* X1, const numb* a, const numb* V, numb* dV)   (dV = J(X1) V)
 std::string emit_rhs_device(const Rhs& r, bool single_precision);
 std::string emit_jvp_device(const Rhs& r, bool single_precision);
+// A forcing phase: a variable p whose right-hand side is a constant `rate` (so it advances
+// by rate * h per step) and whose sin / cos appear in the system. False if there is none
+// (or more than one).
+bool find_trig_phase(const Rhs& r, int& p, double& rate);
+// ucb_rhs_trig(X1, a, dX, cph, sph): ucb_rhs with cos(X1[p]) / sin(X1[p]) taken from the
+// arguments (the forcing evaluated by the caller, e.g. from a table of the stage phases).
+std::string emit_rhs_trig_device(const Rhs& r, int p, bool single_precision);
 // Host C++ source of the same two functions for numb = double (used by the CPU tools).
 std::string emit_rhs_host(const Rhs& r);
 

@@ -490,7 +490,13 @@ PNode directional_derivative(const PNode& e) { return simplify(dir(e)); }
 // ------------------------------------------------------------------ native emitters
 namespace {
 
-void emit_native(const PNode& n, std::ostream& o, bool sp) {
+// trig_p >= 0: cos(X1[trig_p]) / sin(X1[trig_p]) are emitted as the names cph / sph.
+void emit_native(const PNode& n, std::ostream& o, bool sp, int trig_p = -1) {
+    if (trig_p >= 0 && n->kind == Node::Call && n->args.size() == 1 && n->args[0]->kind == Node::Var &&
+        n->args[0]->index == trig_p && (n->name == "cos" || n->name == "sin")) {
+        o << (n->name == "cos" ? "cph" : "sph");
+        return;
+    }
     switch (n->kind) {
         case Node::Num: {
             char buf[64];
@@ -507,11 +513,11 @@ void emit_native(const PNode& n, std::ostream& o, bool sp) {
             if (n->index >= 1000) o << "V[" << (n->index - 1000) << "]";
             else o << "a[" << n->index << "]";
             break;
-        case Node::Neg: o << "(-"; emit_native(n->a, o, sp); o << ")"; break;
-        case Node::Add: o << "("; emit_native(n->a, o, sp); o << " + "; emit_native(n->b, o, sp); o << ")"; break;
-        case Node::Sub: o << "("; emit_native(n->a, o, sp); o << " - "; emit_native(n->b, o, sp); o << ")"; break;
-        case Node::Mul: o << "("; emit_native(n->a, o, sp); o << " * "; emit_native(n->b, o, sp); o << ")"; break;
-        case Node::Div: o << "("; emit_native(n->a, o, sp); o << " / "; emit_native(n->b, o, sp); o << ")"; break;
+        case Node::Neg: o << "(-"; emit_native(n->a, o, sp, trig_p); o << ")"; break;
+        case Node::Add: o << "("; emit_native(n->a, o, sp, trig_p); o << " + "; emit_native(n->b, o, sp, trig_p); o << ")"; break;
+        case Node::Sub: o << "("; emit_native(n->a, o, sp, trig_p); o << " - "; emit_native(n->b, o, sp, trig_p); o << ")"; break;
+        case Node::Mul: o << "("; emit_native(n->a, o, sp, trig_p); o << " * "; emit_native(n->b, o, sp, trig_p); o << ")"; break;
+        case Node::Div: o << "("; emit_native(n->a, o, sp, trig_p); o << " / "; emit_native(n->b, o, sp, trig_p); o << ")"; break;
         case Node::Pow: {
             if (n->b->kind == Node::Num) {
                 const double e = n->b->num;
@@ -520,16 +526,16 @@ void emit_native(const PNode& n, std::ostream& o, bool sp) {
                     o << "(";
                     for (int k = 0; k < ie; ++k) {
                         if (k) o << " * ";
-                        emit_native(n->a, o, sp);
+                        emit_native(n->a, o, sp, trig_p);
                     }
                     o << ")";
                     break;
                 }
             }
             o << "pow(";
-            emit_native(n->a, o, sp);
+            emit_native(n->a, o, sp, trig_p);
             o << ", ";
-            emit_native(n->b, o, sp);
+            emit_native(n->b, o, sp, trig_p);
             o << ")";
             break;
         }
@@ -539,7 +545,7 @@ void emit_native(const PNode& n, std::ostream& o, bool sp) {
             o << f << "(";
             for (size_t k = 0; k < n->args.size(); ++k) {
                 if (k) o << ", ";
-                emit_native(n->args[k], o, sp);
+                emit_native(n->args[k], o, sp, trig_p);
             }
             o << ")";
             break;
@@ -558,6 +564,46 @@ std::string emit_rhs_device(const Rhs& r, bool sp) {
         o << ";\n";
     }
     o << "}\n";
+    return o.str();
+}
+
+static bool uses_trig_of(const PNode& n, int p) {
+    if (!n) return false;
+    if (n->kind == Node::Call && n->args.size() == 1 && n->args[0]->kind == Node::Var && n->args[0]->index == p &&
+        (n->name == "cos" || n->name == "sin"))
+        return true;
+    if (uses_trig_of(n->a, p) || uses_trig_of(n->b, p)) return true;
+    for (const auto& c : n->args)
+        if (uses_trig_of(c, p)) return true;
+    return false;
+}
+
+bool find_trig_phase(const Rhs& r, int& p, double& rate) {
+    int found = -1;
+    for (int i = 0; i < r.nx; ++i) {
+        if (r.f[i]->kind != Node::Num) continue;
+        bool used = false;
+        for (const auto& f : r.f) used = used || uses_trig_of(f, i);
+        if (!used) continue;
+        if (found >= 0) return false;
+        found = i;
+    }
+    if (found < 0) return false;
+    p = found;
+    rate = r.f[found]->num;
+    return true;
+}
+
+std::string emit_rhs_trig_device(const Rhs& r, int p, bool sp) {
+    std::ostringstream o;
+    o << "__device__ __forceinline__ void ucb_rhs_trig(const numb* X1, const numb* a, numb* dX, numb cph, numb sph) "
+         "{\n";
+    for (int i = 0; i < r.nx; ++i) {
+        o << "    dX[" << i << "] = ";
+        emit_native(r.f[i], o, sp, p);
+        o << ";\n";
+    }
+    o << "    (void)cph;\n    (void)sph;\n}\n";
     return o.str();
 }
 

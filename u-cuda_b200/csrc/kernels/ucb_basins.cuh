@@ -44,6 +44,11 @@ struct UcbBasinsParams {
     int* overflow;             // set when the table is full
     unsigned long long* counter;
     unsigned long long* steps;
+    // Native form with a forcing phase (UCB_TRIG_PHASE == UCB_PHASE): (cos, sin) of the
+    // phase at ic + rate * m * h / 2, m = 0 .. 2 steps_per_period (the phase restarts every
+    // period, so a step's three stage phases are the same in every period and cell); null:
+    // the step evaluates them itself.
+    const numb* trig;
 };
 
 namespace ucbdev {
@@ -104,8 +109,16 @@ __device__ __forceinline__ void basins_cell(const UcbBasinsParams& p, long long 
     for (int k = 0; k < UCB_MAXK; ++k) run[k] = 0;
     int label = 0, period = 0, n = 0;
     for (n = 1; n <= p.max_periods; ++n) {
-        UCB_STEP_LOOP
-        for (int s = 0; s < p.steps_per_period; ++s) st.step(x, a, p.h);
+#if defined(UCB_TRIG_PHASE) && !defined(UCB_EXACT) && UCB_PHASE == UCB_TRIG_PHASE
+        if (p.trig) {
+            UCB_STEP_LOOP
+            for (int s = 0; s < p.steps_per_period; ++s) st.step_trig(x, a, p.h, p.trig + 4 * s);
+        } else
+#endif
+        {
+            UCB_STEP_LOOP
+            for (int s = 0; s < p.steps_per_period; ++s) st.step(x, a, p.h);
+        }
         ns += p.steps_per_period;
 #if UCB_PHASE >= 0
         x[UCB_PHASE] = p.ic[UCB_PHASE];
@@ -129,6 +142,22 @@ __device__ __forceinline__ void basins_cell(const UcbBasinsParams& p, long long 
             }
         }
         if (found) {
+            // A cycle that repeats after a divisor d of its length to within the merge
+            // radius is the period-d orbit (a rounding-level cycle around a fixed point of
+            // the stroboscopic map, as FP32 can settle into, counts as that fixed point).
+            bool reduced = false;
+#pragma unroll
+            for (int d = 1; d < UCB_MAXK; ++d) {
+                if (!reduced && d < found && found % d == 0) {
+                    numb dd = 0;
+#pragma unroll
+                    for (int i = 0; i < UCB_NS; ++i) dd = fmax(dd, fabs(P[i] - hist[d - 1][i]));
+                    if ((double)dd <= p.quantum) {
+                        found = d;
+                        reduced = true;
+                    }
+                }
+            }
             period = found;
             // canonical point: the smallest first coordinate (then second) of the cycle
             // P_n, P_{n-1}, ..., P_{n-k+1}

@@ -140,6 +140,26 @@ struct Stepper {
 #pragma unroll
         for (int i = 0; i < UCB_NX; ++i) x[i] = fma(h6, (k1[i] + k4[i]) + (numb)2 * (k2[i] + k3[i]), x[i]);
     }
+#ifdef UCB_TRIG_PHASE
+    // The same step with the forcing's (cos, sin) at the three stage phases t, t + h/2 and
+    // t + h given by the caller: tc[0..1], tc[2..3], tc[4..5].
+    __device__ __forceinline__ void step_trig(numb* x, const numb* a, numb h, const numb* tc) const {
+        numb k1[UCB_NX], k2[UCB_NX], k3[UCB_NX], k4[UCB_NX], xt[UCB_NX];
+        const numb c0 = tc[0], s0 = tc[1], c1 = tc[2], s1 = tc[3], c2 = tc[4], s2 = tc[5];
+        ucb_rhs_trig(x, a, k1, c0, s0);
+#pragma unroll
+        for (int i = 0; i < UCB_NX; ++i) xt[i] = fma(hh, k1[i], x[i]);
+        ucb_rhs_trig(xt, a, k2, c1, s1);
+#pragma unroll
+        for (int i = 0; i < UCB_NX; ++i) xt[i] = fma(hh, k2[i], x[i]);
+        ucb_rhs_trig(xt, a, k3, c1, s1);
+#pragma unroll
+        for (int i = 0; i < UCB_NX; ++i) xt[i] = fma(h, k3[i], x[i]);
+        ucb_rhs_trig(xt, a, k4, c2, s2);
+#pragma unroll
+        for (int i = 0; i < UCB_NX; ++i) x[i] = fma(h6, (k1[i] + k4[i]) + (numb)2 * (k2[i] + k3[i]), x[i]);
+    }
+#endif
 #ifdef UCB_HAS_JVP
     // RK4 of the tangent-linear system (x' = f(x), v' = J(x) v) in one sweep.
     __device__ __forceinline__ void step_tangent(numb* x, numb* v, const numb* a, numb h) const {

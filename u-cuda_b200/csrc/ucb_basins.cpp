@@ -126,7 +126,12 @@ extern "C" int ucb_run_basins(ucb_engine* e, const ucb_basins_request* req, ucb_
     const size_t off_pts = off_keys + kTableSlots * 8;
     const size_t off_per = off_pts + kTableSlots * 16;
     const size_t off_map = off_per + kTableSlots * 4;
-    const size_t ws_need = off_map + kTableSlots * 4 + 256;
+    // forcing-phase table of the native form: (cos, sin) at the 2 steps_per_period + 1
+    // half-step phases of a period (ucb_basins.cuh)
+    const bool use_trig = !sys.exact && sys.trig_phase >= 0 && sys.trig_phase == q.phase_var;
+    const size_t trig_count = use_trig ? 2 * ((size_t)2 * q.steps_per_period + 1) : 0;
+    const size_t off_trig = ((off_map + kTableSlots * 4 + 255) / 256) * 256;
+    const size_t ws_need = off_trig + trig_count * esz + 256;
     if (!ensure_workspace(e, ws_need, err)) return fail(e, res, UCB_E_CUDA, err);
     char* ws = static_cast<char*>(e->ws);
     cudaStream_t st = e->stream;
@@ -136,6 +141,20 @@ extern "C" int ucb_run_basins(ucb_engine* e, const ucb_basins_request* req, ucb_
                     cudaMemcpyHostToDevice, st);
     cudaMemsetAsync(ws, 0, 32, st);
     cudaMemsetAsync(ws + off_keys, 0, kTableSlots * 8, st);
+    std::vector<double> trig_d;
+    std::vector<float> trig_f;
+    if (use_trig) {
+        const double half = 0.5 * (q.period / q.steps_per_period);
+        const double ph0 = q.initial_conditions[q.phase_var];
+        for (int m = 0; m <= 2 * q.steps_per_period; ++m) {
+            const double ph = ph0 + sys.trig_rate * (m * half);
+            trig_d.push_back(std::cos(ph));
+            trig_d.push_back(std::sin(ph));
+        }
+        trig_f.assign(trig_d.begin(), trig_d.end());
+        cudaMemcpyAsync(ws + off_trig, prec == UCB_PREC_F64 ? (const void*)trig_d.data() : (const void*)trig_f.data(),
+                        trig_count * esz, cudaMemcpyHostToDevice, st);
+    }
     int32_t *d_labels = nullptr, *d_periods = nullptr, *d_iters = nullptr;
     cudaError_t ce;
     if ((ce = dev_alloc(e, (void**)&d_labels, (size_t)total * 4, st)) != cudaSuccess ||
@@ -169,6 +188,7 @@ extern "C" int ucb_run_basins(ucb_engine* e, const ucb_basins_request* req, ucb_
     pk.put<void*>(ws + 16);
     pk.put<void*>(ws);
     pk.put<void*>(ws + 8);
+    pk.put<const void*>(use_trig ? (const void*)(ws + off_trig) : nullptr);
     const int block = shape.block;
     cudaEventRecord(e->ev0, st);
     int rc = launch_packed(e, fn, persistent_grid(e, fn, block, total), block, st, pk, err) ? UCB_OK : UCB_E_CUDA;

@@ -179,6 +179,14 @@ SystemCode make_system_code(const std::string& krs_body, int nx, int nv, int pre
                 s.has_jvp = true;
                 s.flops_step = fe::rk4_tangent_step_flops(r) / 2;  // per trajectory-step
             }
+            int p = -1;
+            double rate = 0;
+            if (fe::find_trig_phase(r, p, rate)) {
+                s.code += fe::emit_rhs_trig_device(r, p, precision == UCB_PREC_F32);
+                s.code += "#define UCB_TRIG_PHASE " + std::to_string(p) + "\n";
+                s.trig_phase = p;
+                s.trig_rate = rate;
+            }
             return s;
         }
         s.note = "native form unavailable (" + why + "); using the exact form";
