@@ -585,7 +585,11 @@ def main():
         "rk4_steps_per_s": world * r32["steps"] / (r32["ms"] * 1e-3),
         "forms": forms,
         "roofline": {"bound": "fp32", "achieved": ach, "peak": peak32, "unit": "TFLOP/s", "frac": ach / peak32,
-                     "traffic": None,
+                     # DRAM bytes per launch from one ncu capture of this kernel (384^2 map,
+                     # 147,456 cells: 151 KB read, 0 B written — the outputs stay in L2),
+                     # scaled by the cells of this map
+                     "traffic": 151e3 / 147456 * cells,
+                     "traffic_source": "ncu capture of the FP32 kernel at 384^2, scaled by cells",
                      "peak_source": "measured FMA probe (ucb_measure_fma_peak) on this GPU in this run",
                      "plain_fp64": {"bound": "fp64", "achieved": ach64, "peak": peak64, "frac": ach64 / peak64}},
         "surrogate": results["surrogate"],

@@ -257,19 +257,14 @@ struct Bif2dSink {
     }
 };
 
-__device__ __forceinline__ numb dbscan_distance(numb x1, numb y1, numb x2, numb y2) {
-    if (x1 == x2 && y1 == y2) return 0;
-    const numb dx = fabs(x2 - x1), dy = fabs(y2 - y1);
-    return sqrt(dx * dx + dy * dy);
-}
-
 // The reference's dbscan step for step, one warp per cell: labels (helpful[0, P)) and the
 // stack slots (helpful[P, 2P)) as integers — they only ever hold cluster numbers and
 // indices below 2,500, exact in numb — with the slots written at P + k and popped at
 // P + NumNeibor - 1, inner bound P - 1, result cluster - 1. Peaks enter times mult_peak (1)
-// and intervals times mult_interval (0) (configCUDA.h). Within one scan each k touches only
-// its own label and slot and NumNeibor only counts, so the lanes take k = lane, lane + 32,
-// ... and the hits are summed with a ballot.
+// and intervals times mult_interval (0) (configCUDA.h), so the distance is that of the
+// peak values. Within one scan each k touches only its own label and slot and NumNeibor
+// only counts, so the lanes take k = lane, lane + 32, ... and the hits are summed with a
+// ballot.
 __device__ __forceinline__ int dbscan_warp(const numb* peaks, int P, int* lab, int* stk, numb eps, int lane) {
     if (P == -1) return -1;
     if (P == 0) return 0;
@@ -279,7 +274,6 @@ __device__ __forceinline__ int dbscan_warp(const numb* peaks, int P, int* lab, i
         stk[k] = 0;
     }
     __syncwarp();
-    const numb y = (numb)0.0 * (numb)0.0;
     int cluster = 0, nn = 0;
     for (unsigned long long i = 0; i < (unsigned long long)P; i++) {
         if (nn >= 1) {
@@ -297,13 +291,15 @@ __device__ __forceinline__ int dbscan_warp(const numb* peaks, int P, int* lab, i
             continue;
         }
         __syncwarp();
-        const numb xi = peaks[i] * (numb)1.0;
+        const numb xi = peaks[i];
         int hits = 0;
         for (int k0 = 0; k0 < P - 1; k0 += 32) {
             const int k = k0 + lane;
             bool hit = false;
-            if (k < P - 1 && i != (unsigned long long)k && lab[k] == 0)
-                hit = dbscan_distance(xi, y, peaks[k] * (numb)1.0, y) < eps;
+            // the reference's distance sqrt(dx * dx + 0 * 0) = sqrt(fl(dx * dx)) is exactly
+            // |dx| in binary floating point (correctly rounded product and square root; an
+            // overflowing or underflowing dx * dx still compares the same against eps)
+            if (k < P - 1 && i != (unsigned long long)k && lab[k] == 0) hit = fabs(peaks[k] - xi) < eps;
             if (hit) {
                 lab[k] = cluster;
                 stk[k] = k;
