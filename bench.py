@@ -357,15 +357,16 @@ def run_other_configs(eng, which=OTHER_CONFIGS, args=None):
     # 512 x 512, DP5(4) with 4 tangent vectors, modified Gram-Schmidt every 10 accepted
     # steps, t_end = 2e4, rtol 1e-8 (FP64) / 1e-5 (FP32).
     hb = rk4_body(HYPER_ROSSLER)
+    t_end = args.spectrum_t_end if args else 2e4
     for name, prec, rtol in (("fp64_rtol1e-8", ucb.PREC_F64, 1e-8), ("fp32_rtol1e-5", ucb.PREC_F32, 1e-5)):
         if "spectrum" not in which:
             break
 
         def lreq(n):
             return ucb.Engine.ls2d_request(hb, 4, (-10.0, -6.0, 0.0, 10.0), (0, 0.25, 0.05), method=ucb.LS_DP5,
-                                           gs_every=10, rtol=rtol, t_end=2e4, n_pts=n, param_index=1,
+                                           gs_every=10, rtol=rtol, t_end=t_end, n_pts=n, param_index=1,
                                            param_index_2=2, param_lo=0.1, param_hi=0.35, param_lo_2=0.01,
-                                           param_hi_2=0.1, h=0.01, transient_time=0.0, t_max=2e4, NT=1.0, eps=1e-6,
+                                           param_hi_2=0.1, h=0.01, transient_time=0.0, t_max=t_end, NT=1.0, eps=1e-6,
                                            opt=ucb.options(precision=prec))
         warm = ucb.Engine.ls2d_request(hb, 4, (-10.0, -6.0, 0.0, 10.0), (0, 0.25, 0.05), method=ucb.LS_DP5,
                                        gs_every=10, rtol=rtol, t_end=10.0, n_pts=4, param_index=1, param_index_2=2,
@@ -376,8 +377,11 @@ def run_other_configs(eng, which=OTHER_CONFIGS, args=None):
         # max_value through ever smaller steps, and the map takes about as long as its
         # slowest cell while the grid fits the resident threads (~220k), so the full grid
         # runs only when the small one ended within 150 s.
-        (_, _, pre), _ = _timed(lambda: eng.run_ls2d(lreq(64)))
-        n_ls = 512 if pre.kernel_ms < 150e3 else 128
+        if args and args.spectrum_n:
+            n_ls = args.spectrum_n
+        else:
+            (_, _, pre), _ = _timed(lambda: eng.run_ls2d(lreq(64)))
+            n_ls = 512 if pre.kernel_ms < 150e3 else 128
         (vals, flags, res), ms = _timed(lambda: eng.run_ls2d(lreq(n_ls)))
         v = vals.reshape(4, -1)
         ok = flags == 1
@@ -504,6 +508,11 @@ def main():
     ap.add_argument("--no-headline", action="store_true",
                     help="time only the --configs selection (no LLE headline, surrogate or e2e)")
     ap.add_argument("--bif2d-n", type=int, default=512, help="grid of the Bif-2D period map configuration")
+    ap.add_argument("--spectrum-t-end", type=float, default=2e4,
+                    help="measured interval of the spectrum configuration (shorter only for profiling)")
+    ap.add_argument("--spectrum-n", type=int, default=0,
+                    help="grid of the spectrum configuration (default: 512 if a 64^2 pass ends within 150 s, "
+                         "else 128)")
     ap.add_argument("--configs", default="",
                     help=f"comma-separated subset of {','.join(OTHER_CONFIGS)} to time (instead of --all-configs)")
     ap.add_argument("--surrogate-chen", type=int, default=0, metavar="N",

@@ -79,7 +79,10 @@ typedef struct ucb_options {
     int32_t block_threads; /* threads per block, multiple of 32, 32..1024 */
     int32_t max_registers; /* registers per thread cap (--maxrregcount), 0 = compiler's choice */
     int32_t unroll;        /* steps per unrolled chunk of the run-time-length step loops, 1..16 */
-    int32_t reserved[1];
+    int32_t paired_cells;  /* 1: the FP32 tangent LLE kernel integrates two cells per thread in
+                              packed FP32 pairs (FFMA2 / FADD2 / FMUL2; bit-identical results).
+                              Off by default: on B200 it measured 12 % slower than one cell per
+                              thread (fewer resident warps, FFMA2 pipe rate 94 % of FFMA) */
 } ucb_options;
 
 typedef struct ucb_engine ucb_engine;
@@ -358,6 +361,8 @@ typedef struct ucb_ls2d_result {
     int32_t* flags;          /* n_pts^2: 1 ok, -1 diverged (sentinel 999 in every plane) */
     double* min_val;         /* amount_of_x (may be NULL) */
     double* max_val;         /* amount_of_x (may be NULL) */
+    long long* cell_steps;   /* n_pts^2 (may be NULL): work per cell, as `steps` counts it
+                                (no reference counterpart; the cost map of a run) */
     int32_t ok, cancelled, n_pts, n_exponents;
     double kernel_ms;
     long long steps;         /* FIXED: trajectory steps; DP5: step attempts */

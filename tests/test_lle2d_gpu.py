@@ -157,3 +157,17 @@ def test_device_entry_matches_host_entry(eng):
     torch.cuda.synchronize()
     np.testing.assert_array_equal(dv.cpu().numpy(), hv)
     np.testing.assert_array_equal(df.cpu().numpy(), hf)
+
+
+@pytest.mark.parametrize("n", [33, 48])
+def test_fp32_paired_cells_match_one_cell_per_thread(eng, n):
+    """paired_cells: the FP32 tangent kernel integrates two cells per thread in packed FP32
+    pairs (FFMA2 / FADD2 / FMUL2), the same arithmetic as one cell per thread with scalar
+    instructions: flags and exponents bit-identical (33^2 leaves an odd tail pair with one
+    cell), the same step count."""
+    c = lle2d_case(n=n, t_max=20.0, transient=10.0)
+    v2, f2, r2 = eng.run_lle2d(engine_request(ucb, c, precision=ucb.PREC_F32, paired_cells=True))
+    v1, f1, r1 = eng.run_lle2d(engine_request(ucb, c, precision=ucb.PREC_F32))
+    np.testing.assert_array_equal(f2, f1)
+    np.testing.assert_array_equal(v2, v1)
+    assert r2.steps == r1.steps

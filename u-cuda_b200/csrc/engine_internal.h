@@ -70,6 +70,7 @@ struct SweepMap {
 struct SystemCode {
     bool exact = true;
     bool has_jvp = false;
+    bool has_packed = false; // ucb_rhs2 / ucb_jvp2 (packed FP32 pairs) emitted too
     std::string code;     // device source defining calculateDiscreteModel or ucb_rhs/ucb_jvp
     int flops_step = 0;   // algorithmic FLOPs of one step (native form; 0 if unknown)
     int flops_rhs = 0;    // FLOPs of one right-hand-side evaluation (recognised bodies)

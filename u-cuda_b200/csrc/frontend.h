@@ -85,6 +85,9 @@ PNode parse_c_expr(const std::string& text, const std::string& state);
 //   ucb_jvp(const numb* X1, const numb* a, const numb* V, numb* dV)   (dV = J(X1) V)
 std::string emit_rhs_device(const Rhs& r, bool single_precision);
 std::string emit_jvp_device(const Rhs& r, bool single_precision);
+// Packed FP32 forms for two cells at once (sm_100 FFMA2 / FADD2 / FMUL2 on float2):
+// ucb_rhs2(X1, a, dX) and ucb_jvp2(X1, a, V, dV) over float2, every a * b + c fused.
+std::string emit_packed_device(const Rhs& r);
 // A forcing phase: a variable p whose right-hand side is a constant `rate` (so it advances
 // by rate * h per step) and whose sin / cos appear in the system. False if there is none
 // (or more than one).

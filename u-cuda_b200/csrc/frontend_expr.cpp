@@ -567,6 +567,120 @@ std::string emit_rhs_device(const Rhs& r, bool sp) {
     return o.str();
 }
 
+// ------------------------------------------------------------------ packed FP32 emitter
+namespace {
+
+void emit_packed(const PNode& n, std::ostream& o) {
+    auto is_mul = [](const PNode& x) { return x->kind == Node::Mul; };
+    switch (n->kind) {
+        case Node::Num: {
+            char buf[64];
+            std::snprintf(buf, sizeof buf, "%.17g", n->num);
+            o << "ucb_p2((float)" << buf << ")";
+            break;
+        }
+        case Node::Sym: o << "ucb_p2(" << n->name << ")"; break;
+        case Node::Var: o << "X1[" << n->index << "]"; break;
+        case Node::Par:
+            if (n->index >= 1000) o << "V[" << (n->index - 1000) << "]";
+            else o << "a[" << n->index << "]";
+            break;
+        case Node::Neg: o << "ucb_neg2("; emit_packed(n->a, o); o << ")"; break;
+        case Node::Add:
+            if (is_mul(n->a) || is_mul(n->b)) {
+                const PNode& m = is_mul(n->a) ? n->a : n->b;
+                const PNode& c = is_mul(n->a) ? n->b : n->a;
+                o << "__ffma2_rn("; emit_packed(m->a, o); o << ", "; emit_packed(m->b, o); o << ", ";
+                emit_packed(c, o); o << ")";
+            } else {
+                o << "__fadd2_rn("; emit_packed(n->a, o); o << ", "; emit_packed(n->b, o); o << ")";
+            }
+            break;
+        case Node::Sub:
+            if (is_mul(n->a)) {  // p q - c
+                o << "__ffma2_rn("; emit_packed(n->a->a, o); o << ", "; emit_packed(n->a->b, o);
+                o << ", ucb_neg2("; emit_packed(n->b, o); o << "))";
+            } else if (is_mul(n->b)) {  // c - p q
+                o << "__ffma2_rn(ucb_neg2("; emit_packed(n->b->a, o); o << "), "; emit_packed(n->b->b, o);
+                o << ", "; emit_packed(n->a, o); o << ")";
+            } else {
+                o << "__fadd2_rn("; emit_packed(n->a, o); o << ", ucb_neg2("; emit_packed(n->b, o); o << "))";
+            }
+            break;
+        case Node::Mul: o << "__fmul2_rn("; emit_packed(n->a, o); o << ", "; emit_packed(n->b, o); o << ")"; break;
+        case Node::Div: o << "ucb_div2("; emit_packed(n->a, o); o << ", "; emit_packed(n->b, o); o << ")"; break;
+        case Node::Pow: {
+            if (n->b->kind == Node::Num) {
+                const double e = n->b->num;
+                const int ie = (int)e;
+                if (e == (double)ie && ie >= 2 && ie <= 8) {
+                    // left to right, as the scalar form's a * a * ... * a
+                    for (int k = 1; k < ie; ++k) o << "__fmul2_rn(";
+                    emit_packed(n->a, o);
+                    for (int k = 1; k < ie; ++k) {
+                        o << ", ";
+                        emit_packed(n->a, o);
+                        o << ")";
+                    }
+                    break;
+                }
+            }
+            o << "ucb_call2b(powf, ";
+            emit_packed(n->a, o);
+            o << ", ";
+            emit_packed(n->b, o);
+            o << ")";
+            break;
+        }
+        case Node::Call: {
+            std::string f = n->name;
+            if (f == "abs") f = "fabs";
+            if (n->args.size() == 1) {
+                o << "ucb_call2(" << f << ", ";
+                emit_packed(n->args[0], o);
+                o << ")";
+            } else if (n->args.size() == 2) {
+                o << "ucb_call2b(" << f << ", ";
+                emit_packed(n->args[0], o);
+                o << ", ";
+                emit_packed(n->args[1], o);
+                o << ")";
+            } else {
+                throw std::runtime_error("packed form: call with " + std::to_string(n->args.size()) + " arguments");
+            }
+            break;
+        }
+    }
+}
+
+}  // namespace
+
+std::string emit_packed_device(const Rhs& r) {
+    std::ostringstream o;
+    o << "#define UCB_PACKED_CODE 1\n"
+         "__device__ __forceinline__ float2 ucb_p2(float c) { return make_float2(c, c); }\n"
+         "__device__ __forceinline__ float2 ucb_neg2(float2 x) { return make_float2(-x.x, -x.y); }\n"
+         "__device__ __forceinline__ float2 ucb_div2(float2 x, float2 y) { return make_float2(x.x / y.x, x.y / y.y); }\n"
+         "#define ucb_call2(f, x) ([&]() { const float2 ucb_t = (x); return make_float2(f(ucb_t.x), f(ucb_t.y)); }())\n"
+         "#define ucb_call2b(f, x, y) ([&]() { const float2 ucb_t = (x), ucb_u = (y); "
+         "return make_float2(f(ucb_t.x, ucb_u.x), f(ucb_t.y, ucb_u.y)); }())\n";
+    o << "__device__ __forceinline__ void ucb_rhs2(const float2* X1, const float2* a, float2* dX) {\n";
+    for (int i = 0; i < r.nx; ++i) {
+        o << "    dX[" << i << "] = ";
+        emit_packed(r.f[i], o);
+        o << ";\n";
+    }
+    o << "}\n";
+    o << "__device__ __forceinline__ void ucb_jvp2(const float2* X1, const float2* a, const float2* V, float2* dV) {\n";
+    for (int i = 0; i < r.nx; ++i) {
+        o << "    dV[" << i << "] = ";
+        emit_packed(directional_derivative(r.f[i]), o);
+        o << ";\n";
+    }
+    o << "}\n";
+    return o.str();
+}
+
 static bool uses_trig_of(const PNode& n, int p) {
     if (!n) return false;
     if (n->kind == Node::Call && n->args.size() == 1 && n->args[0]->kind == Node::Var && n->args[0]->index == p &&

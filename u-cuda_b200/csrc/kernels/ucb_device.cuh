@@ -187,6 +187,78 @@ struct Stepper {
     }
 #endif
 };
+
+#if defined(UCB_PACKED_CODE)
+// Two cells per thread in packed FP32 pairs (.x one cell, .y the other): the same FMA-
+// ordered RK4 as Stepper with every add / multiply / fused multiply-add issued as one
+// FADD2 / FMUL2 / FFMA2 for both cells (sm_100), half the instructions per cell-step.
+struct Stepper2 {
+    float2 hh, h6, hf;
+    __device__ __forceinline__ explicit Stepper2(float h)
+        : hh(ucb_p2(h * 0.5f)), h6(ucb_p2(h * (float)(1.0 / 6.0))), hf(ucb_p2(h)) {}
+    __device__ __forceinline__ static float2 comb(float2 k1, float2 k2, float2 k3, float2 k4) {
+        // (k1 + k4) + 2 (k2 + k3)
+        return __ffma2_rn(ucb_p2(2.0f), __fadd2_rn(k2, k3), __fadd2_rn(k1, k4));
+    }
+    __device__ __forceinline__ void step(float2* x, const float2* a) const {
+        float2 k1[UCB_NX], k2[UCB_NX], k3[UCB_NX], k4[UCB_NX], xt[UCB_NX];
+        ucb_rhs2(x, a, k1);
+#pragma unroll
+        for (int i = 0; i < UCB_NX; ++i) xt[i] = __ffma2_rn(hh, k1[i], x[i]);
+        ucb_rhs2(xt, a, k2);
+#pragma unroll
+        for (int i = 0; i < UCB_NX; ++i) xt[i] = __ffma2_rn(hh, k2[i], x[i]);
+        ucb_rhs2(xt, a, k3);
+#pragma unroll
+        for (int i = 0; i < UCB_NX; ++i) xt[i] = __ffma2_rn(hf, k3[i], x[i]);
+        ucb_rhs2(xt, a, k4);
+#pragma unroll
+        for (int i = 0; i < UCB_NX; ++i) x[i] = __ffma2_rn(h6, comb(k1[i], k2[i], k3[i], k4[i]), x[i]);
+    }
+    __device__ __forceinline__ void step_tangent(float2* x, float2* v, const float2* a) const {
+        float2 k1[UCB_NX], k2[UCB_NX], k3[UCB_NX], k4[UCB_NX], xt[UCB_NX];
+        float2 l1[UCB_NX], l2[UCB_NX], l3[UCB_NX], l4[UCB_NX], vt[UCB_NX];
+        ucb_rhs2(x, a, k1);
+        ucb_jvp2(x, a, v, l1);
+#pragma unroll
+        for (int i = 0; i < UCB_NX; ++i) {
+            xt[i] = __ffma2_rn(hh, k1[i], x[i]);
+            vt[i] = __ffma2_rn(hh, l1[i], v[i]);
+        }
+        ucb_rhs2(xt, a, k2);
+        ucb_jvp2(xt, a, vt, l2);
+#pragma unroll
+        for (int i = 0; i < UCB_NX; ++i) {
+            xt[i] = __ffma2_rn(hh, k2[i], x[i]);
+            vt[i] = __ffma2_rn(hh, l2[i], v[i]);
+        }
+        ucb_rhs2(xt, a, k3);
+        ucb_jvp2(xt, a, vt, l3);
+#pragma unroll
+        for (int i = 0; i < UCB_NX; ++i) {
+            xt[i] = __ffma2_rn(hf, k3[i], x[i]);
+            vt[i] = __ffma2_rn(hf, l3[i], v[i]);
+        }
+        ucb_rhs2(xt, a, k4);
+        ucb_jvp2(xt, a, vt, l4);
+#pragma unroll
+        for (int i = 0; i < UCB_NX; ++i) {
+            x[i] = __ffma2_rn(h6, comb(k1[i], k2[i], k3[i], k4[i]), x[i]);
+            v[i] = __ffma2_rn(h6, comb(l1[i], l2[i], l3[i], l4[i]), v[i]);
+        }
+    }
+};
+
+// The divergence test of one cell of a pair (diverged(), component c of each entry).
+__device__ __forceinline__ bool diverged2(const float2* x, float maxValue, int c) {
+    float checker = 0;
+#pragma unroll
+    for (int j = 0; j < UCB_NX; ++j) checker = checker + fabsf(c ? x[j].y : x[j].x);
+    if (isnan(checker) || isinf(checker)) return true;
+    if (maxValue != 0 && fabsf(checker) > maxValue) return true;
+    return false;
+}
+#endif
 #endif
 
 // ---------------------------------------------------------------------------

@@ -201,11 +201,149 @@ __device__ __forceinline__ double lle_cell_tangent(const UcbLleParams& p, long l
 }
 #endif
 
+#if defined(UCB_TANGENT) && defined(UCB_PACKED) && defined(UCB_PACKED_CODE) && defined(UCB_NT) && \
+    UCB_HAXIS == -1 && !defined(UCB_EXACT)
+// lle_cell_tangent for two cells at once (FP32 state and tangent in float2 pairs; per-cell
+// divergence tests, norms, FP64 log products and rescaling as in lle_cell_tangent). A cell
+// that diverges keeps being stepped with its pair (its lanes of the packed operations are
+// independent of the other cell's) but counts no further steps and stores 999.
+__device__ __forceinline__ void lle_pair_tangent(const UcbLleParams& p, long long k0, long long k1, bool two,
+                                                 double* out, long long& ns) {
+    const float h = p.h;
+    float2 x[UCB_NX], v[UCB_NX], a[UCB_NV];
+    {
+        numb xa[UCB_NX], aa[UCB_NV], xb[UCB_NX], ab[UCB_NV];
+#pragma unroll
+        for (int i = 0; i < UCB_NX; ++i) xa[i] = xb[i] = p.ic[i];
+#pragma unroll
+        for (int i = 0; i < UCB_NV; ++i) aa[i] = ab[i] = p.vals[i];
+        apply_sweep(cell_axes(k0, p.n_pts), p.axis0, p.axis1, xa, aa);
+        apply_sweep(cell_axes(two ? k1 : k0, p.n_pts), p.axis0, p.axis1, xb, ab);
+#pragma unroll
+        for (int i = 0; i < UCB_NX; ++i) x[i] = make_float2(xa[i], xb[i]);
+#pragma unroll
+        for (int i = 0; i < UCB_NV; ++i) a[i] = make_float2(aa[i], ab[i]);
+    }
+    out[0] = out[1] = 999.0;
+    bool live[2] = {true, two};
+    const int n_live = two ? 2 : 1;
+    const Stepper2 st(h);
+    // transient (loop_single: a divergence test after steps 1, 101, 201, ..., the extra step)
+    for (long long i0 = 0; i0 < p.skip; i0 += kCheckInterval) {
+        st.step(x, a);
+        ns += (live[0] ? 1 : 0) + (live[1] ? 1 : 0);
+#pragma unroll
+        for (int c = 0; c < 2; ++c)
+            if (live[c] && diverged2(x, p.maxv, c)) live[c] = false;
+        if (!live[0] && !live[1]) return;
+        const int n = (p.skip - i0 < kCheckInterval) ? (int)(p.skip - i0) : kCheckInterval;
+        UCB_STEP_LOOP
+        for (int i = 1; i < n; ++i) st.step(x, a);
+        ns += (long long)(n - 1) * ((live[0] ? 1 : 0) + (live[1] ? 1 : 0));
+    }
+#if UCB_EXTRA_STEP
+    st.step(x, a);
+    ns += (live[0] ? 1 : 0) + (live[1] ? 1 : 0);
+#endif
+    (void)n_live;
+    {
+        numb za[UCB_NX], zb[UCB_NX];
+        probe_direction((unsigned long long)k0, za);
+        probe_direction((unsigned long long)(two ? k1 : k0), zb);
+#pragma unroll
+        for (int i = 0; i < UCB_NX; ++i) v[i] = make_float2(za[i], zb[i]);
+    }
+    LogProduct end2[2], start2[2];
+    double n2[2] = {0.0, 0.0};
+#pragma unroll
+    for (int j = 0; j < UCB_NX; ++j) {
+        n2[0] = fma((double)v[j].x, (double)v[j].x, n2[0]);
+        n2[1] = fma((double)v[j].y, (double)v[j].y, n2[1]);
+    }
+    for (int b = 0; b < p.n_blocks; ++b) {
+#pragma unroll
+        for (int c = 0; c < 2; ++c)
+            if (live[c]) start2[c].mul(n2[c]);
+        // loop_tangent with the compile-time block length: first step, divergence test,
+        // the remaining UCB_NT - 1 steps, the extra step
+        st.step_tangent(x, v, a);
+        int now = (live[0] ? 1 : 0) + (live[1] ? 1 : 0);
+        ns += 2 * now;
+#pragma unroll
+        for (int c = 0; c < 2; ++c)
+            if (live[c] && (diverged2(x, p.maxv, c) || diverged2(v, 0.0f, c))) live[c] = false;
+        if (!live[0] && !live[1]) return;
+        now = (live[0] ? 1 : 0) + (live[1] ? 1 : 0);
+#pragma unroll
+        for (int i = 1; i < UCB_NT; ++i) st.step_tangent(x, v, a);
+        ns += 2 * (UCB_NT - 1) * now;
+#if UCB_EXTRA_STEP
+        st.step_tangent(x, v, a);
+        ns += 2 * now;
+#endif
+        double d2[2] = {0.0, 0.0};
+#pragma unroll
+        for (int l = 0; l < UCB_NX; ++l) {
+            d2[0] = fma((double)v[l].x, (double)v[l].x, d2[0]);
+            d2[1] = fma((double)v[l].y, (double)v[l].y, d2[1]);
+        }
+        float inv[2];
+#pragma unroll
+        for (int c = 0; c < 2; ++c) {
+            if (d2[c] < 1e-28) {  // the reference's floor of the norm at 1e-14
+                d2[c] = 1e-28;
+                const float v0 = c ? v[0].y : v[0].x;
+                if (!(fabsf(v0) > 0)) {
+                    if (c) v[0].y = 1e-14f;
+                    else v[0].x = 1e-14f;
+                }
+            }
+            if (live[c]) end2[c].mul(d2[c]);
+            inv[c] = (float)rsqrt(d2[c]);
+        }
+        n2[0] = n2[1] = 0.0;
+        const float2 iv = make_float2(inv[0], inv[1]);
+#pragma unroll
+        for (int j = 0; j < UCB_NX; ++j) {
+            v[j] = __fmul2_rn(v[j], iv);
+            n2[0] = fma((double)v[j].x, (double)v[j].x, n2[0]);
+            n2[1] = fma((double)v[j].y, (double)v[j].y, n2[1]);
+        }
+    }
+#pragma unroll
+    for (int c = 0; c < 2; ++c)
+        if (live[c]) out[c] = 0.5 * (end2[c].log_value() - start2[c].log_value()) / (double)p.tmax;
+}
+#define UCB_LLE_PAIRED 1
+#endif
+
 }  // namespace ucbdev
 
 extern "C" __global__ void __launch_bounds__(UCB_BLOCK) ucb_lle_kernel(const UcbLleParams p) {
     const int lane = threadIdx.x & 31;
     long long ns = 0;
+#if defined(UCB_LLE_PAIRED)
+    // 64 cells per warp fetch: lane l takes cells base + l and base + 32 + l (both halves
+    // of a warp's stores stay coalesced)
+    for (;;) {
+        unsigned long long b = 0;
+        if (lane == 0) b = atomicAdd(p.counter, 64ULL);
+        const long long base = (long long)__shfl_sync(0xffffffffu, b, 0);
+        if (base >= p.total) break;
+        const long long i0 = base + lane, i1 = base + 32 + lane;
+        if (i0 < p.total) {
+            const bool two = i1 < p.total;
+            const long long k0 = p.cell_list ? p.cell_list[i0] : p.cell_offset + i0;
+            const long long k1 = two ? (p.cell_list ? p.cell_list[i1] : p.cell_offset + i1) : k0;
+            double v[2];
+            ucbdev::lle_pair_tangent(p, k0, k1, two, v, ns);
+            ucbdev::store_cell(p, i0, k0, v[0]);
+            if (two) ucbdev::store_cell(p, i1, k1, v[1]);
+        }
+    }
+    ucbdev::warp_add_steps(p.steps, ns, lane);
+    return;
+#endif
     for (;;) {
         const long long base = ucbdev::warp_fetch(p.counter, lane);
         if (base >= p.total) break;

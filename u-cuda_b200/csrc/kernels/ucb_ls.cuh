@@ -42,6 +42,7 @@ struct UcbLsParams {
     int* out_flags;
     unsigned long long* counter;
     unsigned long long* steps;
+    long long* out_cell_steps;  // per cell: steps (fixed) / step attempts (DP5); may be null
 };
 
 namespace ucbdev {
@@ -457,11 +458,13 @@ extern "C" __global__ void __launch_bounds__(UCB_BLOCK) ucb_ls_kernel(const UcbL
         if (base >= p.total) break;
         const long long i = base + lane;
         if (i < p.total) {
+            const long long ns0 = ns;
 #if defined(UCB_LS_DP5)
             ucbdev::ls_cell_dp5(p, p.cell_offset + i, ns);
 #else
             ucbdev::ls_cell_fixed(p, p.cell_offset + i, ns);
 #endif
+            if (p.out_cell_steps) p.out_cell_steps[ucbdev::ls_out_cell(p, p.cell_offset + i)] = ns - ns0;
         }
     }
     ucbdev::warp_add_steps(p.steps, ns, lane);

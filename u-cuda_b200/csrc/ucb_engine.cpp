@@ -178,6 +178,14 @@ SystemCode make_system_code(const std::string& krs_body, int nx, int nv, int pre
                 s.code += fe::emit_jvp_device(r, precision == UCB_PREC_F32);
                 s.has_jvp = true;
                 s.flops_step = fe::rk4_tangent_step_flops(r) / 2;  // per trajectory-step
+                if (precision == UCB_PREC_F32) {
+                    try {
+                        s.code += fe::emit_packed_device(r);
+                        s.has_packed = true;
+                    } catch (const std::exception&) {
+                        s.has_packed = false;  // a call the packed form does not cover
+                    }
+                }
             }
             int p = -1;
             double rate = 0;
@@ -404,6 +412,11 @@ CompileRequest lle_compile_request(const ucb_lle2d_request& q, const LlePlan& pl
     L.tangent = tangent;
     std::vector<std::string> defs;
     if (tangent) defs.push_back("UCB_TANGENT 1");
+    // Two cells per thread in packed FP32 pairs (on request): FP32 tangent form with a
+    // uniform step and a compile-time block length.
+    if (tangent && prec == UCB_PREC_F32 && L.sys.has_packed && plan.map.h_axis == -1 && plan.nt_steps >= 1 &&
+        plan.nt_steps <= 100 && q.opt.paired_cells)
+        defs.push_back("UCB_PACKED 1");
     // Block length known at compile time (no h sweep): the block loop unrolls fully.
     if (plan.map.h_axis == -1 && plan.nt_steps >= 1 && plan.nt_steps <= 100)
         defs.push_back("UCB_NT " + std::to_string(plan.nt_steps));

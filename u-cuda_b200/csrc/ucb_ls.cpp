@@ -145,10 +145,17 @@ int ls_run(ucb_engine* e, const ucb_ls2d_request& q, const SweepMap& m, int n_bl
     cudaMemsetAsync(ws, 0, 16, e->stream);
     double* d_values = nullptr;
     int32_t* d_flags = nullptr;
+    long long* d_cell_steps = nullptr;
     cudaError_t ce;
     if ((ce = dev_alloc(e, (void**)&d_values, (size_t)total * nx * 8, e->stream)) != cudaSuccess ||
-        (ce = dev_alloc(e, (void**)&d_flags, (size_t)total * 4, e->stream)) != cudaSuccess)
+        (ce = dev_alloc(e, (void**)&d_flags, (size_t)total * 4, e->stream)) != cudaSuccess ||
+        (res->cell_steps &&
+         (ce = dev_alloc(e, (void**)&d_cell_steps, (size_t)total * 8, e->stream)) != cudaSuccess)) {
+        if (d_values) cudaFreeAsync(d_values, e->stream);
+        if (d_flags) cudaFreeAsync(d_flags, e->stream);
+        cudaStreamSynchronize(e->stream);
         return fail(e, res, UCB_E_CUDA, std::string("cudaMallocAsync: ") + cudaGetErrorString(ce));
+    }
 
     const double rtol = q.rtol > 0 ? q.rtol : (prec == UCB_PREC_F64 ? 1e-8 : 1e-5);
     const double atol = q.atol > 0 ? q.atol : rtol;
@@ -176,6 +183,7 @@ int ls_run(ucb_engine* e, const ucb_ls2d_request& q, const SweepMap& m, int n_bl
     pk.put<void*>(d_flags);
     pk.put<void*>(ws);
     pk.put<void*>(ws + 8);
+    pk.put<void*>(d_cell_steps);
     const int block = shape.block;
     const int grid = persistent_grid(e, fn, block, total);
     cudaEventRecord(e->ev0, e->stream);
@@ -188,6 +196,8 @@ int ls_run(ucb_engine* e, const ucb_ls2d_request& q, const SweepMap& m, int n_bl
             (ce = cudaMemcpyAsync(res->flags, d_flags, (size_t)total * 4, cudaMemcpyDeviceToHost, e->stream)) !=
                 cudaSuccess ||
             (ce = cudaMemcpyAsync(&steps, ws + 8, 8, cudaMemcpyDeviceToHost, e->stream)) != cudaSuccess ||
+            (d_cell_steps && (ce = cudaMemcpyAsync(res->cell_steps, d_cell_steps, (size_t)total * 8,
+                                                   cudaMemcpyDeviceToHost, e->stream)) != cudaSuccess) ||
             (ce = cudaStreamSynchronize(e->stream)) != cudaSuccess) {
             rc = UCB_E_CUDA;
             err = std::string("CUDA ls2d: ") + cudaGetErrorString(ce);
@@ -195,6 +205,7 @@ int ls_run(ucb_engine* e, const ucb_ls2d_request& q, const SweepMap& m, int n_bl
     }
     cudaFreeAsync(d_values, e->stream);
     cudaFreeAsync(d_flags, e->stream);
+    if (d_cell_steps) cudaFreeAsync(d_cell_steps, e->stream);
     cudaStreamSynchronize(e->stream);
     if (rc != UCB_OK) return fail(e, res, rc, err);
     float ms = 0;

@@ -31,7 +31,7 @@ class UcbError(RuntimeError):
 class Options(C.Structure):
     _fields_ = [("precision", C.c_int32), ("mode", C.c_int32), ("lle_method", C.c_int32),
                 ("nominal_steps", C.c_int32), ("block_threads", C.c_int32), ("max_registers", C.c_int32),
-                ("unroll", C.c_int32), ("reserved", C.c_int32 * 1)]
+                ("unroll", C.c_int32), ("paired_cells", C.c_int32)]
 
 
 class TuneReport(C.Structure):
@@ -213,6 +213,7 @@ class Ls2dResult(C.Structure):
     _fields_ = [
         ("values", C.POINTER(C.c_double)), ("flags", C.POINTER(C.c_int32)),
         ("min_val", C.POINTER(C.c_double)), ("max_val", C.POINTER(C.c_double)),
+        ("cell_steps", C.POINTER(C.c_longlong)),
         ("ok", C.c_int32), ("cancelled", C.c_int32), ("n_pts", C.c_int32), ("n_exponents", C.c_int32),
         ("kernel_ms", C.c_double), ("steps", C.c_longlong), ("flops", C.c_double), ("error", C.c_char * 1024),
     ]
@@ -374,13 +375,13 @@ def _dptr(a):
 
 
 def options(precision=PREC_F64, mode=MODE_NATIVE, lle_method=LLE_AUTO, nominal_steps=False, block_threads=0,
-            max_registers=0, unroll=0):
+            max_registers=0, unroll=0, paired_cells=False):
     """Run options; the launch-shape fields at 0 take the autotuned shape (or the default)."""
     o = Options()
     load().ucb_default_options(C.byref(o))
     o.precision, o.mode, o.lle_method = precision, mode, lle_method
     o.nominal_steps, o.block_threads = int(nominal_steps), block_threads
-    o.max_registers, o.unroll = max_registers, unroll
+    o.max_registers, o.unroll, o.paired_cells = max_registers, unroll, int(paired_cells)
     return o
 
 
@@ -554,7 +555,9 @@ class Engine:
             max_steps
         return r
 
-    def run_ls2d(self, req: Ls2dRequest):
+    def run_ls2d(self, req: Ls2dRequest, cell_steps=False):
+        """-> (values[k, cell], flags, result); with cell_steps=True result.cell_work holds the
+        per-cell steps (fixed) / step attempts (DP5)."""
         n, nx = req.n_pts, req.amount_of_x
         values = np.empty(max(n, 0) ** 2 * nx, dtype=np.float64)
         flags = np.empty(max(n, 0) ** 2, dtype=np.int32)
@@ -565,9 +568,13 @@ class Engine:
         res.flags = flags.ctypes.data_as(C.POINTER(C.c_int32))
         res.min_val = _dptr(mn)
         res.max_val = _dptr(mx)
+        work = np.zeros(max(n, 0) ** 2, dtype=np.int64) if cell_steps else None
+        if cell_steps:
+            res.cell_steps = work.ctypes.data_as(C.POINTER(C.c_longlong))
         rc = self.lib.ucb_run_ls2d(self.h, C.byref(req), C.byref(res))
         if rc != UCB_OK:
             raise UcbError(rc, res.error.decode())
+        res.cell_work = work
         return values.reshape(nx, n * n), flags, res
 
     # ------------------------------------------------------------------ basins
