@@ -54,6 +54,22 @@ def dist_env():
     return rank, world, local
 
 
+def max_over_ranks(x: float, world: int, device=None) -> float:
+    """The slowest rank's value: every multi-rank timing is the max over ranks."""
+    if world <= 1:
+        return float(x)
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([float(x)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def aggregate_rate(world: int, units: float, ms: float) -> float:
+    """Whole-job rate: every one of `world` replicas processes `units` in `ms` (weak scaling)."""
+    return world * units / (ms * 1e-3)
+
+
 class ClockSampler:
     """Samples nvidia-smi SM clocks and throttle reasons while the timed region runs."""
 
@@ -152,11 +168,7 @@ def run_ours(args, rank, world, local):
         if sampler:
             clocks = sampler.summary()
         step_ms = [a.elapsed_time(b) for a, b in ev]
-        ms = float(np.mean(step_ms))
-        if world > 1:
-            t = torch.tensor([ms], device=dev)
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            ms = float(t.item())
+        ms = max_over_ranks(float(np.mean(step_ms)), world, dev)
         launches = eng.launches - l0
         if name == "fp32":
             launches_timed = launches
@@ -180,12 +192,8 @@ def run_ours(args, rank, world, local):
         _, _, r = eng.run_lle2d(req, hv, hf)
         e2e_ms.append((time.perf_counter() - t0) * 1e3)
         e2e_kernel_ms.append(r.kernel_ms)
-    e2e = float(np.mean(e2e_ms))
     results["e2e_detail"] = {"wall_ms": e2e_ms, "kernel_ms": e2e_kernel_ms}
-    if world > 1:
-        t = torch.tensor([e2e], device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e = float(t.item())
+    e2e = max_over_ranks(float(np.mean(e2e_ms)), world, dev)
     return results, clocks, launches_timed, e2e
 
 
@@ -575,13 +583,13 @@ def main():
         return
     cells = args.n * args.n
     r32, r64 = results["fp32"], results["plain_fp64"]
-    value = world * cells / (r32["ms"] * 1e-3)
+    value = aggregate_rate(world, cells, r32["ms"])
     forms = {}
     for name, r in results.items():
         if name in ("e2e_detail", "surrogate"):
             continue
-        forms[name] = {"cells_per_s": world * cells / (r["ms"] * 1e-3),
-                       "rk4_steps_per_s": world * r["steps"] / (r["ms"] * 1e-3), "ms_per_map": r["ms"],
+        forms[name] = {"cells_per_s": aggregate_rate(world, cells, r["ms"]),
+                       "rk4_steps_per_s": aggregate_rate(world, r["steps"], r["ms"]), "ms_per_map": r["ms"],
                        "achieved_tflops": r["flops"] / (r["ms"] * 1e-3) / 1e12, "valid_cells": r["valid_cells"],
                        "launch_shape": r.get("autotune")}
     ach = r32["flops"] / (r32["ms"] * 1e-3) / 1e12
@@ -591,7 +599,7 @@ def main():
         "warmup": args.warmup, "ms_per_step": r32["ms"], "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32 state, f64 norms/log sums", "data": "synthetic grid (no dataset)",
         "config": cfg,
-        "rk4_steps_per_s": world * r32["steps"] / (r32["ms"] * 1e-3),
+        "rk4_steps_per_s": aggregate_rate(world, r32["steps"], r32["ms"]),
         "forms": forms,
         "roofline": {"bound": "fp32", "achieved": ach, "peak": peak32, "unit": "TFLOP/s", "frac": ach / peak32,
                      # DRAM bytes per launch from one ncu capture of this kernel (384^2 map,
@@ -604,7 +612,7 @@ def main():
         "surrogate": results["surrogate"],
         "clocks": clocks,
         "gpu_launches": launches,
-        "e2e": {"value": world * cells / (e2e_ms * 1e-3), "unit": "cells/s", "detail": results["e2e_detail"],
+        "e2e": {"value": aggregate_rate(world, cells, e2e_ms), "unit": "cells/s", "detail": results["e2e_detail"],
                 "h2d_bytes_per_step": 2 * args.n * 4 + 3 * 8 + 4 * 8,
                 "d2h_bytes_per_step": cells * (8 + 4) + 8},
     }
