@@ -293,13 +293,18 @@ __device__ __forceinline__ int dbscan_warp(const numb* peaks, int P, int* lab, i
         __syncwarp();
         const numb xi = peaks[i];
         int hits = 0;
+        // chunks of 32 are independent (each k touches only its own label and slot): both
+        // loads of a lane are issued unconditionally and four chunks are in flight at once
+#pragma unroll 4
         for (int k0 = 0; k0 < P - 1; k0 += 32) {
             const int k = k0 + lane;
-            bool hit = false;
+            const bool in = k < P - 1;
+            const int lk = in ? lab[k] : 1;
+            const numb pk = in ? peaks[k] : xi;
             // the reference's distance sqrt(dx * dx + 0 * 0) = sqrt(fl(dx * dx)) is exactly
             // |dx| in binary floating point (correctly rounded product and square root; an
             // overflowing or underflowing dx * dx still compares the same against eps)
-            if (k < P - 1 && i != (unsigned long long)k && lab[k] == 0) hit = fabs(peaks[k] - xi) < eps;
+            const bool hit = in && i != (unsigned long long)k && lk == 0 && fabs(pk - xi) < eps;
             if (hit) {
                 lab[k] = cluster;
                 stk[k] = k;
