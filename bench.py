@@ -197,13 +197,13 @@ def run_ours(args, rank, world, local):
     return results, clocks, launches_timed, e2e
 
 
-JUDGE_CELLS = 65536
+EVAL_CELLS = 65536
 
 
-def judge_cells(total: int, seed: int = 0):
-    """The held-out subset the surrogate is judged on: 64k cells drawn without
+def eval_cells(total: int, seed: int = 0):
+    """The held-out subset the surrogate is evaluated on: 64k cells drawn without
     replacement with a fixed seed."""
-    return np.sort(np.random.default_rng(seed).choice(total, size=min(JUDGE_CELLS, total), replace=False))
+    return np.sort(np.random.default_rng(seed).choice(total, size=min(EVAL_CELLS, total), replace=False))
 
 
 def error_stats(v, ref, tol=2e-3):
@@ -220,7 +220,7 @@ def surrogate_request(ucb, c, **kw):
 def run_surrogate(eng, c, results, args, dev):
     """Surrogate-refined form of the same map: plain FP64 samples on a 256 x 256 stratified
     partition, BF16 MLP trained on this GPU, held-out calibration at |error| <= 2e-3 for
-    99.5% of predicted cells, everything else re-integrated in the FP32 form. Judged on 64k
+    99.5% of predicted cells, everything else re-integrated in the FP32 form. Evaluated on 64k
     random cells against the plain FP64 map."""
     import torch
     import ucb
@@ -237,7 +237,7 @@ def run_surrogate(eng, c, results, args, dev):
         torch.cuda.synchronize(dev)
         runs.append(res.total_ms)
     ms = float(np.mean(runs))
-    idx = judge_cells(n * n)
+    idx = eval_cells(n * n)
     vals = v.cpu().numpy()[idx]
     ref = results["plain_fp64"]["values"][idx]
     return {"ms_per_map": ms, "cells_per_s": n * n / (ms * 1e-3),
@@ -247,8 +247,8 @@ def run_surrogate(eng, c, results, args, dev):
             "calibration_within_tol": res.calib_within_tol,
             "phases_ms": {"samples": res.sample_ms, "train": res.train_ms, "predict": res.predict_ms,
                           "select": res.select_ms, "refine": res.refine_ms},
-            "judge_64k_vs_plain_fp64": error_stats(vals, ref),
-            "fp32_judge_64k_vs_plain_fp64": error_stats(results["fp32"]["values"][idx], ref),
+            "heldout_64k_vs_plain_fp64": error_stats(vals, ref),
+            "fp32_heldout_64k_vs_plain_fp64": error_stats(results["fp32"]["values"][idx], ref),
             "rule": "predict a cell only when its std is under the held-out-calibrated threshold "
                     "(>= 99.5% of held-out samples within 2e-3) and |mean| >= 0.05 with no neighbour "
                     "in another regime; everything else integrated"}
@@ -265,7 +265,7 @@ def chen_case(n: int) -> dict:
 
 
 def run_surrogate_chen(eng, dev, n: int, tol: float, coverage: float):
-    """Surrogate-refined Chen map at n x n, judged on 64k random cells integrated with the
+    """Surrogate-refined Chen map at n x n, evaluated on 64k random cells integrated with the
     plain FP64 method (whose rate there is the plain FP64 cells/s of the same kernel)."""
     import torch
     import ucb
@@ -278,7 +278,7 @@ def run_surrogate_chen(eng, dev, n: int, tol: float, coverage: float):
     torch.cuda.synchronize(dev)
     res = eng.run_lle2d_surrogate(req, v.data_ptr(), f.data_ptr(), 0)
     torch.cuda.synchronize(dev)
-    idx = judge_cells(n * n)
+    idx = eval_cells(n * n)
     d_idx = torch.from_numpy(idx).to(dev)
     sur = v[d_idx].cpu().numpy()
     out = {}
@@ -306,9 +306,9 @@ def run_surrogate_chen(eng, dev, n: int, tol: float, coverage: float):
             "calibration_within_tol": res.calib_within_tol,
             "phases_ms": {"samples": res.sample_ms, "train": res.train_ms, "predict": res.predict_ms,
                           "select": res.select_ms, "refine": res.refine_ms},
-            "judge_64k_vs_plain_fp64": error_stats(sur, ref),
-            "fp32_judge_64k_vs_plain_fp64": error_stats(out["fp32"][0], ref),
-            "plain_rate_basis": "plain FP64 kernel over the 64k judge cells (same kernel, random cells)"}
+            "heldout_64k_vs_plain_fp64": error_stats(sur, ref),
+            "fp32_heldout_64k_vs_plain_fp64": error_stats(out["fp32"][0], ref),
+            "plain_rate_basis": "plain FP64 kernel over the 64k held-out cells (same kernel, random cells)"}
 
 
 def _timed(fn, reps=1):

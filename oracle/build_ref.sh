@@ -2,7 +2,7 @@
 # Builds the reference's own text front-end (sysparse.cpp + codegen.cpp, compiled as-is
 # from the read-only reference tree) into oracle/_ref/ref_codegen. Test infrastructure:
 # it only regenerates the golden fixtures in tests/golden/. Needs the reference tree;
-# exits 0 without building when it is absent (the GPU box has no reference tree).
+# exits 0 without building when it is absent (machines without the reference tree use the prebuilt files).
 set -euo pipefail
 REF="${UCB_REFERENCE_DIR:-/root/reference/U-CUDA}"
 HERE="$(cd "$(dirname "$0")" && pwd)"

@@ -19,7 +19,7 @@ def rk4_body(case_name):
     return codegen_cases()[case_name]["schemes"]["RK4"]
 
 
-# Reference-generated RK4 bodies of the BASELINE systems.
+# Reference-generated RK4 bodies of the benchmark systems.
 ROSSLER = "rossler_config"      # a=a[1], b=a[2], c=a[3]
 LORENZ = "library_Lorenz"       # sigma=a[1], rho=a[2], beta=a[3]
 CHEN = "chen_config"            # a=a[1], b=a[2], c=a[3]
