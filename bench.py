@@ -350,6 +350,21 @@ def run_other_configs(eng, which=OTHER_CONFIGS, args=None):
             "wall_ms": ms, "kernel_ms": res.kernel_ms, "points_per_s": 1024 / (res.kernel_ms * 1e-3),
             "rk4_steps_per_s": res.steps / (res.kernel_ms * 1e-3), "points_with_peaks": int((counts > 0).sum())}
         if name == "plain_fp64_exact":
+            exact_peaks, exact_counts = peaks.reshape(1024, -1).copy(), counts.copy()
+        else:
+            # error against the FP64 diagram (the exact form equals the oracle bit for bit):
+            # per rho the Hausdorff distance between the two peak sets
+            pk = peaks.reshape(1024, -1)
+            hd = []
+            for i in range(1024):
+                a, b = pk[i][np.isfinite(pk[i])], exact_peaks[i][np.isfinite(exact_peaks[i])]
+                if len(a) and len(b):
+                    d = np.abs(a[:, None] - b[None, :])
+                    hd.append(max(d.min(axis=1).max(), d.min(axis=0).max()))
+            out["bif_lorenz_1024"][name]["peak_set_hausdorff_vs_fp64"] = {
+                "median": float(np.median(hd)), "p90": float(np.quantile(hd, 0.9)), "points": len(hd),
+                "same_class": float((np.sign(counts) == np.sign(exact_counts)).mean())}
+        if name == "plain_fp64_exact":
             b = dict(n_pts=1024, sweep_kind=0, sweep_index=2, lo=20.0, hi=200.0, ic=(0.1, 0.1, 0.1),
                      values=(0, 10.0, 28.0, 8 / 3), h=0.01, transient_time=50.0, t_max=200.0, pre_scaller=1,
                      writable_var=0, max_value=1e6)

@@ -16,6 +16,12 @@ def test_shapes_compile_for_every_kernel(shape):
     for prec, mode in ((ucb.PREC_F64, ucb.MODE_EXACT), (ucb.PREC_F32, ucb.MODE_NATIVE)):
         opt = dict(precision=prec, mode=mode, **shape)
         ucb.precompile(engine_request(ucb, lle2d_case(), **opt))
+        # a system with a transcendental call (its packed FP32 pair form is emitted too)
+        duffing = dict(lle2d_case(), body=rk4_body(DUFFING), ic=(0.0, 0.0, 0.0), values=(0.0,),
+                       sweep_over_var=True, sweep_over_var_2=True, var_sweep_index=0, var_sweep_index_2=1,
+                       param_lo=-1.0, param_hi=1.0, param_lo_2=-1.0, param_hi_2=1.0)
+        for paired in (False, True):
+            ucb.precompile(engine_request(ucb, duffing, paired_cells=paired, **opt))
         ucb.precompile(ucb.Engine.bif2d_request(rk4_body(LORENZ), 3, (0.1, 0.1, 0.1), (0, 10.0, 28.0, 8 / 3),
                                                 n_pts=8, param_index=2, param_index_2=1, param_lo=20, param_hi=30,
                                                 param_lo_2=5, param_hi_2=15, opt=ucb.options(**opt)))

@@ -661,9 +661,10 @@ std::string emit_packed_device(const Rhs& r) {
          "__device__ __forceinline__ float2 ucb_p2(float c) { return make_float2(c, c); }\n"
          "__device__ __forceinline__ float2 ucb_neg2(float2 x) { return make_float2(-x.x, -x.y); }\n"
          "__device__ __forceinline__ float2 ucb_div2(float2 x, float2 y) { return make_float2(x.x / y.x, x.y / y.y); }\n"
-         "#define ucb_call2(f, x) ([&]() { const float2 ucb_t = (x); return make_float2(f(ucb_t.x), f(ucb_t.y)); }())\n"
-         "#define ucb_call2b(f, x, y) ([&]() { const float2 ucb_t = (x), ucb_u = (y); "
-         "return make_float2(f(ucb_t.x, ucb_u.x), f(ucb_t.y, ucb_u.y)); }())\n";
+         "#define ucb_call2(ucb_fn, ucb_arg) ([&]() { const float2 ucb_t = (ucb_arg); "
+         "return make_float2(ucb_fn(ucb_t.x), ucb_fn(ucb_t.y)); }())\n"
+         "#define ucb_call2b(ucb_fn, ucb_arg, ucb_arg2) ([&]() { const float2 ucb_t = (ucb_arg), ucb_u = (ucb_arg2); "
+         "return make_float2(ucb_fn(ucb_t.x, ucb_u.x), ucb_fn(ucb_t.y, ucb_u.y)); }())\n";
     o << "__device__ __forceinline__ void ucb_rhs2(const float2* X1, const float2* a, float2* dX) {\n";
     for (int i = 0; i < r.nx; ++i) {
         o << "    dX[" << i << "] = ";

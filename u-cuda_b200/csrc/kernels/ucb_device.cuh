@@ -119,13 +119,36 @@ struct Stepper {
     }
 };
 #else
+#ifdef UCB_TRIG_PHASE
+__device__ __forceinline__ void ucb_sincos(double v, double* s, double* c) { sincos(v, s, c); }
+__device__ __forceinline__ void ucb_sincos(float v, float* s, float* c) { sincosf(v, s, c); }
+#endif
+
 // Classical RK4 on ucb_rhs, FMA-ordered: the same scheme as codegen.cpp scheme_rk4
 // (k1..k4 at t, t+h/2, t+h/2, t+h; x += h/6 (k1 + 2k2 + 2k3 + k4)) with the half/sixth
 // step factors hoisted and every update written as a fused multiply-add.
+// With a forcing phase p (dX[p]/dt = UCB_TRIG_RATE, sin / cos of X[p] in the system) a step
+// takes one sincos of X[p] and rotates it by the constant stage offsets rate h/2 and rate h
+// for the other stages, instead of evaluating the forcing at every stage.
 struct Stepper {
     numb hh, h6;
+#ifdef UCB_TRIG_PHASE
+    numb ch, sh, cf, sf;  // cos / sin of rate h/2 and of rate h
+    __device__ __forceinline__ explicit Stepper(numb h) : hh(h * (numb)0.5), h6(h * (numb)(1.0 / 6.0)) {
+        ucb_sincos((numb)((numb)UCB_TRIG_RATE * hh), &sh, &ch);
+        ucb_sincos((numb)((numb)UCB_TRIG_RATE * h), &sf, &cf);
+    }
+#else
     __device__ __forceinline__ explicit Stepper(numb h) : hh(h * (numb)0.5), h6(h * (numb)(1.0 / 6.0)) {}
+#endif
     __device__ __forceinline__ void step(numb* x, const numb* a, numb h) const {
+#ifdef UCB_TRIG_PHASE
+        numb s0, c0;
+        ucb_sincos(x[UCB_TRIG_PHASE], &s0, &c0);
+        const numb tc[6] = {c0, s0, fma(c0, ch, -s0 * sh), fma(s0, ch, c0 * sh), fma(c0, cf, -s0 * sf),
+                            fma(s0, cf, c0 * sf)};
+        step_trig(x, a, h, tc);
+#else
         numb k1[UCB_NX], k2[UCB_NX], k3[UCB_NX], k4[UCB_NX], xt[UCB_NX];
         ucb_rhs(x, a, k1);
 #pragma unroll
@@ -139,6 +162,7 @@ struct Stepper {
         ucb_rhs(xt, a, k4);
 #pragma unroll
         for (int i = 0; i < UCB_NX; ++i) x[i] = fma(h6, (k1[i] + k4[i]) + (numb)2 * (k2[i] + k3[i]), x[i]);
+#endif
     }
 #ifdef UCB_TRIG_PHASE
     // The same step with the forcing's (cos, sin) at the three stage phases t, t + h/2 and

@@ -191,7 +191,9 @@ SystemCode make_system_code(const std::string& krs_body, int nx, int nv, int pre
             double rate = 0;
             if (fe::find_trig_phase(r, p, rate)) {
                 s.code += fe::emit_rhs_trig_device(r, p, precision == UCB_PREC_F32);
-                s.code += "#define UCB_TRIG_PHASE " + std::to_string(p) + "\n";
+                char rbuf[64];
+                std::snprintf(rbuf, sizeof rbuf, "%.17g", rate);
+                s.code += "#define UCB_TRIG_PHASE " + std::to_string(p) + "\n#define UCB_TRIG_RATE " + rbuf + "\n";
                 s.trig_phase = p;
                 s.trig_rate = rate;
             }
