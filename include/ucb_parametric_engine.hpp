@@ -5,7 +5,7 @@
 // conventions (ok / cancelled / error, NaN or sentinel + flags, row-major iy*n+ix, plane-
 // major spectra), same shared_ptr<atomic<...>> cancel / progress tokens. Every call goes
 // through the C ABI in ucb.h (libucb.so): run_bifurcation_1d, run_bifurcation_2d,
-// run_lle_2d, run_ls_2d, run_basins, run_basins_recluster.
+// run_lle_1d, run_ls_1d, run_lle_2d, run_ls_2d, run_basins, run_basins_recluster.
 // Entry points of the reference that are not on this path (DFT, Fast Synchro,
 // continuation sweeps) are not provided.
 //
@@ -36,6 +36,18 @@ struct LLE2DSnapshot {
     int indexOfMutVar = 0, indexOfMutVar2 = 0;
     double range1_lo = 0.0, range1_hi = 0.0, range2_lo = 0.0, range2_hi = 0.0;
     int n_pts = 0;
+};
+struct LLE1DSnapshot {
+    std::vector<double> values, initial_conditions;
+    double tMax = 0.0, NT = 0.0, transientTime = 0.0, h = 0.0, eps = 0.0;
+    int indexOfMutVar = 0;
+    double range_lo = 0.0, range_hi = 0.0;
+};
+struct LS1DSnapshot {
+    std::vector<double> values, initial_conditions;
+    double tMax = 0.0, NT = 0.0, transientTime = 0.0, h = 0.0, eps = 0.0;
+    int indexOfMutVar = 0;
+    double range_lo = 0.0, range_hi = 0.0;
 };
 struct Bif2DSnapshot {
     std::vector<double> values, initial_conditions;
@@ -107,6 +119,91 @@ struct Bifurcation1DResult {
     std::vector<std::vector<double>> peak_times;
     std::vector<int> flags;
     data_export::Bif1DSnapshot snapshot;
+};
+
+// LLE 1D / LS 1D (parametric_engine.h:235-387): one swept parameter, initial condition or
+// step h. lyapunov[i] is NaN where the kernel flagged the point (flags[i] = -1);
+// spectrum[i][k] keeps the 999 / -999 sentinels. Continuation sweeps (sequential, CPU in
+// the reference) are answered with ok = false; use_cpu is ignored (no CPU path here).
+struct LLE1DRequest {
+    std::string krs_body;
+    int amountOfX = 0;
+    std::vector<double> initial_conditions;
+    std::vector<double> base_values;
+    bool sweep_over_var = false;
+    int var_sweep_index = 0;
+    bool sweep_over_h = false;
+    bool log_scale = false;
+    int param_index = 0;
+    bool continuation = false;
+    bool continuation_reverse = false;
+    bool use_cpu = false;
+    double param_lo = 0.0;
+    double param_hi = 1.0;
+    int n_pts = 500;
+    double h = 0.01;
+    double transient_time = 0.0;
+    double t_max = 100.0;
+    double NT = 1.0;
+    double eps = 1.0e-4;
+    double max_value = 1.0e6;
+    std::string csv_output_path;
+    std::shared_ptr<std::atomic<bool>> cancel;
+    std::shared_ptr<std::atomic<float>> progress;
+};
+
+struct LLE1DResult {
+    bool ok = false;
+    bool cancelled = false;
+    std::string error;
+    int n_pts = 0;
+    double param_lo = 0.0;
+    double param_hi = 1.0;
+    bool continuation_reverse = false;
+    std::vector<double> lyapunov;
+    std::vector<int> flags;
+    data_export::LLE1DSnapshot snapshot;
+};
+
+struct LS1DRequest {
+    std::string krs_body;
+    int amountOfX = 0;
+    std::vector<double> initial_conditions;
+    std::vector<double> base_values;
+    bool sweep_over_var = false;
+    int var_sweep_index = 0;
+    bool sweep_over_h = false;
+    bool continuation = false;
+    bool continuation_reverse = false;
+    bool use_cpu = false;
+    bool log_scale = false;
+    int param_index = 0;
+    double param_lo = 0.0;
+    double param_hi = 1.0;
+    int n_pts = 500;
+    double h = 0.01;
+    double transient_time = 0.0;
+    double t_max = 100.0;
+    double NT = 1.0;
+    double eps = 1.0e-4;
+    double max_value = 1.0e6;
+    std::string csv_output_path;
+    std::shared_ptr<std::atomic<bool>> cancel;
+    std::shared_ptr<std::atomic<float>> progress;
+};
+
+struct LS1DResult {
+    bool ok = false;
+    bool cancelled = false;
+    std::string error;
+    int n_pts = 0;
+    int n_exponents = 0;
+    double param_lo = 0.0;
+    double param_hi = 1.0;
+    bool continuation_reverse = false;
+    std::vector<std::vector<double>> spectrum;
+    std::vector<int> flags;
+    data_export::LS1DSnapshot snapshot;
 };
 
 struct LLE2DRequest {
@@ -409,6 +506,63 @@ public:
         s.indexOfMutVar = r.sweep_over_var ? r.var_sweep_index : r.param_index;
         s.range_lo = r.param_lo;
         s.range_hi = r.param_hi;
+        return res;
+    }
+
+    LLE1DResult run_lle_1d(const LLE1DRequest& r) {
+        LLE1DResult res;
+        if (!check_1d(r, res.error)) return res;
+        int32_t cancel_now = 0;
+        float prog = 0.0f;
+        ucb_lle1d_request q = request_1d(r, &cancel_now, &prog);
+        const size_t n = r.n_pts > 0 ? (size_t)r.n_pts : 0;
+        res.lyapunov.assign(n, 0.0);
+        std::vector<int32_t> f32(n);
+        ucb_lle1d_result o{};
+        o.values = res.lyapunov.data();
+        o.flags = f32.data();
+        ucb_run_lle1d(e_, &q, &o);
+        if (r.progress) r.progress->store(prog);
+        res.ok = o.ok != 0;
+        res.cancelled = o.cancelled != 0;
+        res.error = o.error;
+        if (!res.ok) return res;
+        res.flags.assign(f32.begin(), f32.end());
+        res.n_pts = o.n_pts;
+        res.param_lo = o.param_lo;
+        res.param_hi = o.param_hi;
+        snapshot_1d(r, res.snapshot);
+        return res;
+    }
+
+    LS1DResult run_ls_1d(const LS1DRequest& r) {
+        LS1DResult res;
+        if (!check_1d(r, res.error)) return res;
+        int32_t cancel_now = 0;
+        float prog = 0.0f;
+        ucb_ls1d_request q = request_1d(r, &cancel_now, &prog);
+        const size_t n = r.n_pts > 0 ? (size_t)r.n_pts : 0;
+        const size_t nx = r.amountOfX > 0 ? (size_t)r.amountOfX : 0;
+        std::vector<double> flat(n * nx);
+        std::vector<int32_t> f32(n);
+        ucb_ls1d_result o{};
+        o.values = flat.data();
+        o.flags = f32.data();
+        ucb_run_ls1d(e_, &q, &o);
+        if (r.progress) r.progress->store(prog);
+        res.ok = o.ok != 0;
+        res.cancelled = o.cancelled != 0;
+        res.error = o.error;
+        if (!res.ok) return res;
+        res.flags.assign(f32.begin(), f32.end());
+        res.n_pts = o.n_pts;
+        res.n_exponents = o.n_exponents;
+        res.param_lo = o.param_lo;
+        res.param_hi = o.param_hi;
+        res.spectrum.resize(n);
+        for (size_t i = 0; i < n; ++i)
+            res.spectrum[i].assign(flat.begin() + i * nx, flat.begin() + (i + 1) * nx);
+        snapshot_1d(r, res.snapshot);
         return res;
     }
 
@@ -789,6 +943,64 @@ public:
     }
 
 private:
+    // LLE1DRequest and LS1DRequest carry the same fields (parametric_engine.h:235, :332).
+    template <class Req>
+    static bool check_1d(const Req& r, std::string& error) {
+        if (r.continuation) {
+            error = "continuation sweeps are not supported by this engine";
+            return false;
+        }
+        if ((int)r.initial_conditions.size() != r.amountOfX) {
+            error = "initial_conditions.size() != amountOfX";
+            return false;
+        }
+        return true;
+    }
+
+    template <class Req>
+    ucb_lle1d_request request_1d(const Req& r, int32_t* cancel_now, float* prog) const {
+        ucb_lle1d_request q{};
+        q.krs_body = r.krs_body.c_str();
+        q.amount_of_x = r.amountOfX;
+        q.initial_conditions = r.initial_conditions.data();
+        q.base_values = r.base_values.data();
+        q.n_values = (int)r.base_values.size();
+        q.sweep_over_var = r.sweep_over_var;
+        q.var_sweep_index = r.var_sweep_index;
+        q.sweep_over_h = r.sweep_over_h;
+        q.log_scale = r.log_scale;
+        q.param_index = r.param_index;
+        q.param_lo = r.param_lo;
+        q.param_hi = r.param_hi;
+        q.n_pts = r.n_pts;
+        q.h = r.h;
+        q.transient_time = r.transient_time;
+        q.t_max = r.t_max;
+        q.NT = r.NT;
+        q.eps = r.eps;
+        q.max_value = r.max_value;
+        q.csv_output_path = r.csv_output_path.c_str();
+        *cancel_now = (r.cancel && r.cancel->load()) ? 1 : 0;
+        q.cancel = cancel_now;
+        q.progress = prog;
+        q.opt = opt_;
+        return q;
+    }
+
+    template <class Req, class Snap>
+    static void snapshot_1d(const Req& r, Snap& s) {
+        s.values = r.base_values;
+        s.initial_conditions = r.initial_conditions;
+        s.tMax = r.t_max;
+        s.NT = r.NT;
+        s.transientTime = r.transient_time;
+        s.h = r.h;
+        s.eps = r.eps;
+        s.indexOfMutVar = r.sweep_over_var ? r.var_sweep_index : r.param_index;
+        s.range_lo = r.param_lo;
+        s.range_hi = r.param_hi;
+    }
+
     ucb_engine* e_;
     ucb_options opt_;
 };

@@ -1,8 +1,7 @@
 // Drives the header-only ParametricEngine shim the way the reference's session layer
 // calls ParametricEngine (analysis_session.cpp builds a Request, calls run_*, reads the
-// Result). argv[1] = "invalid" (no GPU needed) or "lle2d" / "ls2d" / "bif1d" / "bif2d" / "basins" (GPU);
-// the RK4 body
-// is read from stdin.
+// Result). argv[1] = "invalid" / "continuation" (no GPU needed) or "lle1d" / "ls1d" / "lle2d" /
+// "ls2d" / "bif1d" / "bif2d" / "basins" (GPU); the RK4 body is read from stdin.
 #include <cstdio>
 #include <cstring>
 #include <iostream>
@@ -32,6 +31,40 @@ int main(int argc, char** argv) {
                     res.min_val, res.max_val, r.progress->load());
         if (mode == "lle2d")
             for (size_t i = 0; i < res.values.size(); ++i) std::printf("%.17g %d\n", res.values[i], res.flags[i]);
+        return 0;
+    }
+    if (mode == "lle1d" || mode == "continuation") {
+        LLE1DRequest r;
+        r.krs_body = body;
+        r.amountOfX = 3;
+        r.initial_conditions = {0.1, 0.1, 0.1};
+        r.base_values = {0, 10.0, 28.0, 8.0 / 3.0};
+        r.param_index = 2;
+        r.param_lo = 20; r.param_hi = 200; r.n_pts = 16;
+        r.h = 0.01; r.transient_time = 5; r.t_max = 20; r.NT = 0.5;
+        r.continuation = mode == "continuation";
+        r.progress = std::make_shared<std::atomic<float>>(0.0f);
+        LLE1DResult res = eng.run_lle_1d(r);
+        std::printf("ok=%d error=%s n=%d lo=%g hi=%g idx=%d progress=%.1f\n", (int)res.ok, res.error.c_str(), res.n_pts,
+                    res.param_lo, res.param_hi, res.snapshot.indexOfMutVar, r.progress->load());
+        for (size_t i = 0; i < res.lyapunov.size(); ++i) std::printf("%.17g %d\n", res.lyapunov[i], res.flags[i]);
+        return 0;
+    }
+    if (mode == "ls1d") {
+        LS1DRequest r;
+        r.krs_body = body;
+        r.amountOfX = 3;
+        r.initial_conditions = {0.1, 0.1, 0.1};
+        r.base_values = {0, 10.0, 28.0, 8.0 / 3.0};
+        r.sweep_over_var = true;
+        r.var_sweep_index = 0;
+        r.param_lo = -5; r.param_hi = 5; r.n_pts = 10;
+        r.h = 0.01; r.transient_time = 5; r.t_max = 20; r.NT = 0.5;
+        LS1DResult res = eng.run_ls_1d(r);
+        std::printf("ok=%d error=%s n=%d k=%d idx=%d\n", (int)res.ok, res.error.c_str(), res.n_pts, res.n_exponents,
+                    res.snapshot.indexOfMutVar);
+        for (size_t i = 0; i < res.spectrum.size(); ++i)
+            for (double v : res.spectrum[i]) std::printf("%.17g\n", v);
         return 0;
     }
     if (mode == "bif2d") {

@@ -31,6 +31,40 @@ def test_shim_reports_validation_error(driver):
     assert out.startswith("ok=0 error=n_pts must be > 0")
 
 
+def test_shim_rejects_continuation(driver):
+    out = run(driver, "continuation", rk4_body(LORENZ))
+    assert out.startswith("ok=0 error=continuation sweeps are not supported")
+
+
+@pytest.mark.gpu
+def test_shim_lle1d_equals_c_abi(driver):
+    """run_lle_1d through the shim returns what ucb_run_lle1d returns."""
+    out = run(driver, "lle1d", rk4_body(LORENZ)).splitlines()
+    assert out[0].startswith("ok=1 error= n=16 lo=20 hi=200 idx=2") and "progress=1.0" in out[0]
+    rows = [l.split() for l in out[1:]]
+    eng = ucb.Engine(0)
+    req = eng.lle1d_request(rk4_body(LORENZ), 3, (0.1, 0.1, 0.1), (0, 10.0, 28.0, 8.0 / 3.0), n_pts=16, param_index=2,
+                            param_lo=20, param_hi=200, h=0.01, transient_time=5, t_max=20, NT=0.5,
+                            opt=ucb.options(precision=ucb.PREC_F64))
+    ref, flags = eng.run_lle1d(req)[:2]
+    np.testing.assert_array_equal([float(r[0]) for r in rows], ref)
+    np.testing.assert_array_equal([int(r[1]) for r in rows], flags)
+
+
+@pytest.mark.gpu
+def test_shim_ls1d_equals_c_abi(driver):
+    """run_ls_1d through the shim returns ucb_run_ls1d's point-major spectrum as spectrum[i][k]."""
+    out = run(driver, "ls1d", rk4_body(LORENZ)).splitlines()
+    assert out[0].startswith("ok=1 error= n=10 k=3 idx=0")
+    vals = np.array([float(l) for l in out[1:]])
+    eng = ucb.Engine(0)
+    req = eng.lle1d_request(rk4_body(LORENZ), 3, (0.1, 0.1, 0.1), (0, 10.0, 28.0, 8.0 / 3.0), n_pts=10,
+                            sweep_over_var=True, var_sweep_index=0, param_lo=-5, param_hi=5, h=0.01,
+                            transient_time=5, t_max=20, NT=0.5, opt=ucb.options(precision=ucb.PREC_F64))
+    ref = eng.run_ls1d(req)[0]
+    np.testing.assert_array_equal(vals, np.asarray(ref).ravel())
+
+
 @pytest.mark.gpu
 def test_shim_lle2d_runs(driver):
     out = run(driver, "lle2d", rk4_body(ROSSLER)).splitlines()
