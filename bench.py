@@ -381,6 +381,7 @@ def run_other_configs(eng, which=OTHER_CONFIGS, args=None):
     # steps, t_end = 2e4, rtol 1e-8 (FP64) / 1e-5 (FP32).
     hb = rk4_body(HYPER_ROSSLER)
     t_end = args.spectrum_t_end if args else 2e4
+    max_steps = args.spectrum_max_steps if args else 0
     for name, prec, rtol in (("fp64_rtol1e-8", ucb.PREC_F64, 1e-8), ("fp32_rtol1e-5", ucb.PREC_F32, 1e-5)):
         if "spectrum" not in which:
             break
@@ -390,12 +391,13 @@ def run_other_configs(eng, which=OTHER_CONFIGS, args=None):
                                            gs_every=10, rtol=rtol, t_end=t_end, n_pts=n, param_index=1,
                                            param_index_2=2, param_lo=0.1, param_hi=0.35, param_lo_2=0.01,
                                            param_hi_2=0.1, h=0.01, transient_time=0.0, t_max=t_end, NT=1.0, eps=1e-6,
-                                           opt=ucb.options(precision=prec))
+                                           max_steps=max_steps, opt=ucb.options(precision=prec))
         warm = ucb.Engine.ls2d_request(hb, 4, (-10.0, -6.0, 0.0, 10.0), (0, 0.25, 0.05), method=ucb.LS_DP5,
                                        gs_every=10, rtol=rtol, t_end=10.0, n_pts=4, param_index=1, param_index_2=2,
                                        param_lo=0.1, param_hi=0.35, param_lo_2=0.01, param_hi_2=0.1, h=0.01,
                                        t_max=10.0, NT=1.0, eps=1e-6, opt=ucb.options(precision=prec))
         eng.run_ls2d(warm)
+        shape = eng.autotune(lreq(512)) if tune else None
         # A 64 x 64 grid over the same window first. Most cells of this window escape to
         # max_value through ever smaller steps, and the map takes about as long as its
         # slowest cell while the grid fits the resident threads (~220k), so the full grid
@@ -409,7 +411,7 @@ def run_other_configs(eng, which=OTHER_CONFIGS, args=None):
         v = vals.reshape(4, -1)
         ok = flags == 1
         out.setdefault("ls_hyper_rossler_512_dp5", {})[name] = {
-            "grid": n_ls, "wall_ms": ms, "kernel_ms": res.kernel_ms,
+            "grid": n_ls, "wall_ms": ms, "kernel_ms": res.kernel_ms, "launch_shape": shape,
             "cells_per_s": n_ls * n_ls / (res.kernel_ms * 1e-3),
             "rhs_evals_per_s": res.steps / (res.kernel_ms * 1e-3), "valid_cells": int(ok.sum()),
             "median_spectrum": [float(np.median(v[k][ok])) for k in range(4)],
@@ -533,6 +535,9 @@ def main():
     ap.add_argument("--bif2d-n", type=int, default=512, help="grid of the Bif-2D period map configuration")
     ap.add_argument("--spectrum-t-end", type=float, default=2e4,
                     help="measured interval of the spectrum configuration (shorter only for profiling)")
+    ap.add_argument("--spectrum-max-steps", type=int, default=0,
+                    help="step-attempt cap per cell of the spectrum configuration (default 2e7; lower only "
+                         "for profiling)")
     ap.add_argument("--spectrum-n", type=int, default=0,
                     help="grid of the spectrum configuration (default: 512 if a 64^2 pass ends within 150 s, "
                          "else 128)")

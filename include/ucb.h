@@ -77,7 +77,9 @@ typedef struct ucb_options {
      * cache), else the default (128 threads, the compiler's register choice, 1 step per
      * chunk). Set explicitly, a field overrides the tuned value. None changes results. */
     int32_t block_threads; /* threads per block, multiple of 32, 32..1024 */
-    int32_t max_registers; /* registers per thread cap (--maxrregcount), 0 = compiler's choice */
+    int32_t max_registers; /* registers per thread cap, 0 = compiler's choice; applied as the
+                              resident blocks per SM it allows (__launch_bounds__ minimum
+                              blocks), so the build may use fewer registers than the cap */
     int32_t unroll;        /* steps per unrolled chunk of the run-time-length step loops, 1..16 */
     int32_t paired_cells;  /* 1: the FP32 tangent LLE kernel integrates two cells per thread in
                               packed FP32 pairs (FFMA2 / FADD2 / FMUL2; bit-identical results).

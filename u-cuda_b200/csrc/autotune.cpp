@@ -92,6 +92,10 @@ int blocks_by_registers(int regs, int block) {
     return std::max(0, std::min({by_regs, by_threads, 32}));
 }
 
+// Resident blocks per SM to request so that the compiler keeps to `maxreg` registers per
+// thread or fewer: the occupancy level that cap allows (at least one block).
+int min_blocks_for(int maxreg, int block) { return std::max(1, blocks_by_registers(maxreg, block)); }
+
 // Main kernel of a loaded build (the first one the request names) and its registers.
 CUfunction main_kernel(const Module& m, const CompileRequest& rq) {
     auto it = rq.kernels.empty() ? m.functions.end() : m.functions.find(rq.kernels[0]);
@@ -147,8 +151,9 @@ void apply_tuning(CompileRequest& rq, const TuneConfig& c) {
     std::string defs;
     if (c.block != 128) defs += "#define UCB_BLOCK " + std::to_string(c.block) + "\n";
     if (c.unroll != 1) defs += "#define UCB_UNROLL " + std::to_string(c.unroll) + "\n";
+    // the cap as the number of resident blocks it allows (see UCB_LAUNCH_BOUNDS)
+    if (c.maxreg > 0) defs += "#define UCB_MIN_BLOCKS " + std::to_string(min_blocks_for(c.maxreg, c.block)) + "\n";
     rq.source = defs + rq.source;
-    if (c.maxreg > 0) rq.options.push_back("--maxrregcount=" + std::to_string(c.maxreg));
 }
 
 bool tune_request(ucb_engine* e, const ucb_options& o, int default_block, CompileRequest& rq, TuneConfig& out,

@@ -191,7 +191,7 @@ __device__ __forceinline__ void basins_cell(const UcbBasinsParams& p, long long 
 
 }  // namespace ucbdev
 
-extern "C" __global__ void __launch_bounds__(UCB_BLOCK) ucb_basins_kernel(const UcbBasinsParams p) {
+extern "C" __global__ void UCB_LAUNCH_BOUNDS ucb_basins_kernel(const UcbBasinsParams p) {
     const int lane = threadIdx.x & 31;
     long long ns = 0;
     for (;;) {

@@ -150,7 +150,7 @@ __device__ __forceinline__ void basins_ref_cell(const UcbBasinsRefParams& p, lon
 
 }  // namespace ucbdev
 
-extern "C" __global__ void __launch_bounds__(UCB_BLOCK) ucb_basins_ref_kernel(const UcbBasinsRefParams p) {
+extern "C" __global__ void UCB_LAUNCH_BOUNDS ucb_basins_ref_kernel(const UcbBasinsRefParams p) {
     const int lane = threadIdx.x & 31;
     long long ns = 0;
     for (;;) {

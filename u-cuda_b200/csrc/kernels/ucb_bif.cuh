@@ -160,7 +160,7 @@ __device__ __forceinline__ int loop_transient(const S& st, numb* x, const numb* 
 }  // namespace ucbdev
 
 #if !defined(UCB_BIF2D) && !defined(UCB_BIF_NO_KERNELS)
-extern "C" __global__ void __launch_bounds__(UCB_BLOCK) ucb_bif_kernel(const UcbBifParams p) {
+extern "C" __global__ void UCB_LAUNCH_BOUNDS ucb_bif_kernel(const UcbBifParams p) {
     const long long cell = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     const int lane = threadIdx.x & 31;
     long long ns = 0;
@@ -367,7 +367,7 @@ __device__ __forceinline__ int bif2d_peaks(const UcbBif2dParams& p, long long ki
 
 }  // namespace ucbdev
 
-extern "C" __global__ void __launch_bounds__(UCB_BLOCK) ucb_bif2d_kernel(const UcbBif2dParams p) {
+extern "C" __global__ void UCB_LAUNCH_BOUNDS ucb_bif2d_kernel(const UcbBif2dParams p) {
     const int lane = threadIdx.x & 31;
     const long long warp = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     numb* slot = p.peaks + warp * 32 * (long long)p.cap;

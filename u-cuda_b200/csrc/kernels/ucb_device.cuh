@@ -44,6 +44,14 @@ typedef unsigned long long uint64_t;
 #ifndef UCB_UNROLL
 #define UCB_UNROLL 1
 #endif
+// A register cap is a residency request: __launch_bounds__(UCB_BLOCK, UCB_MIN_BLOCKS) asks
+// for UCB_MIN_BLOCKS resident blocks per SM, which bounds the registers per thread (a
+// --maxrregcount option does not apply to kernels that carry launch bounds).
+#ifdef UCB_MIN_BLOCKS
+#define UCB_LAUNCH_BOUNDS __launch_bounds__(UCB_BLOCK, UCB_MIN_BLOCKS)
+#else
+#define UCB_LAUNCH_BOUNDS __launch_bounds__(UCB_BLOCK)
+#endif
 #define UCB_STR_(x) #x
 #define UCB_PRAGMA_(x) _Pragma(UCB_STR_(x))
 #define UCB_STEP_LOOP UCB_PRAGMA_(unroll UCB_UNROLL)

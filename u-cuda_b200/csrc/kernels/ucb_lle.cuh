@@ -319,7 +319,7 @@ __device__ __forceinline__ void lle_pair_tangent(const UcbLleParams& p, long lon
 
 }  // namespace ucbdev
 
-extern "C" __global__ void __launch_bounds__(UCB_BLOCK) ucb_lle_kernel(const UcbLleParams p) {
+extern "C" __global__ void UCB_LAUNCH_BOUNDS ucb_lle_kernel(const UcbLleParams p) {
     const int lane = threadIdx.x & 31;
     long long ns = 0;
 #if defined(UCB_LLE_PAIRED)
@@ -363,7 +363,7 @@ extern "C" __global__ void __launch_bounds__(UCB_BLOCK) ucb_lle_kernel(const Ucb
 
 // Final state of every cell after `skip` plain steps from its initial condition (no
 // divergence checks, no extra step): a trajectory-parity aid over the same grid.
-extern "C" __global__ void __launch_bounds__(UCB_BLOCK) ucb_state_kernel(const UcbLleParams p) {
+extern "C" __global__ void UCB_LAUNCH_BOUNDS ucb_state_kernel(const UcbLleParams p) {
     const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= p.total) return;
     const long long kidx = p.cell_offset + i;

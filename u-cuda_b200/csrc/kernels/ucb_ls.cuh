@@ -274,92 +274,153 @@ __device__ __forceinline__ bool mgs(numb (*V)[UCB_NX], double* acc) {
     return true;
 }
 
+// The Butcher rows scaled by the step once per attempt, so that every stage point is a
+// chain of fused multiply-adds from the base point: x + sum_j (h a_ij) k_j.
+struct Dp5Coef {
+    numb c21, c31, c32, c41, c42, c43, c51, c52, c53, c54, c61, c62, c63, c64, c65, b1, b3, b4, b5, b6;
+    double e1, e3, e4, e5, e6, e7;  // h times the error weights (FP64: the error norm is FP64)
+};
+
+__device__ __forceinline__ Dp5Coef dp5_coef(numb hn, double h) {
+    Dp5Coef c;
+    c.c21 = hn * (numb)DP_A21;
+    c.c31 = hn * (numb)DP_A31; c.c32 = hn * (numb)DP_A32;
+    c.c41 = hn * (numb)DP_A41; c.c42 = hn * (numb)DP_A42; c.c43 = hn * (numb)DP_A43;
+    c.c51 = hn * (numb)DP_A51; c.c52 = hn * (numb)DP_A52; c.c53 = hn * (numb)DP_A53; c.c54 = hn * (numb)DP_A54;
+    c.c61 = hn * (numb)DP_A61; c.c62 = hn * (numb)DP_A62; c.c63 = hn * (numb)DP_A63; c.c64 = hn * (numb)DP_A64;
+    c.c65 = hn * (numb)DP_A65;
+    c.b1 = hn * (numb)DP_B1; c.b3 = hn * (numb)DP_B3; c.b4 = hn * (numb)DP_B4; c.b5 = hn * (numb)DP_B5;
+    c.b6 = hn * (numb)DP_B6;
+    c.e1 = h * DP_E1; c.e3 = h * DP_E3; c.e4 = h * DP_E4; c.e5 = h * DP_E5; c.e6 = h * DP_E6; c.e7 = h * DP_E7;
+    return c;
+}
+
+// sum_i (e_i / s_i)^2 for s_i > 0, one division per group of four: 1 / (s0 s1 s2 s3) times
+// the other three scales gives each 1 / s_i. A group whose product leaves the normal range
+// (scales below 1e-75 or above 1e75) divides component by component.
+template <int N>
+__device__ __forceinline__ double scaled_sum_sq(const double* e, const double* s) {
+    double acc = 0.0;
+#pragma unroll
+    for (int g = 0; g < N; g += 4) {
+        const int m = (N - g) < 4 ? (N - g) : 4;
+        if (m == 1) {
+            const double q = e[g] / s[g];
+            acc = fma(q, q, acc);
+            continue;
+        }
+        double pre[4], suf[4];  // products of the scales before / after position i
+        pre[0] = 1.0;
+#pragma unroll
+        for (int i = 1; i < m; ++i) pre[i] = pre[i - 1] * s[g + i - 1];
+        suf[m - 1] = 1.0;
+#pragma unroll
+        for (int i = m - 2; i >= 0; --i) suf[i] = suf[i + 1] * s[g + i + 1];
+        const double prod = pre[m - 1] * s[g + m - 1];
+        if (prod > 1e-300 && prod < 1e300) {
+            const double r = 1.0 / prod;
+#pragma unroll
+            for (int i = 0; i < m; ++i) {
+                const double q = e[g + i] * (r * (pre[i] * suf[i]));
+                acc = fma(q, q, acc);
+            }
+        } else {
+#pragma unroll
+            for (int i = 0; i < m; ++i) {
+                const double q = e[g + i] / s[g + i];
+                acc = fma(q, q, acc);
+            }
+        }
+    }
+    return acc;
+}
+
+// Step-size factor 0.9 err^(-1/5) of the controller, from err^2. A heuristic factor (it is
+// clamped to [0.2, facmax] next), so the power is taken in FP32 (relative error ~1e-6),
+// off the FP64 pipe; err^2 below the FP32 range gives +inf (clamped to facmax) and above it
+// 0 (clamped to 0.2), as the FP64 power would after clamping.
+__device__ __forceinline__ double dp5_factor(double err2) {
+    return 0.9 * (double)__powf((float)err2, -0.1f);
+}
+
 // One DP5 step of the state: stage points X2..X6, the 5th-order solution xn and its
-// derivative k7 (FSAL), and the RMS error norm of the embedded 4th-order difference.
+// derivative k7 (FSAL), and the sum of squared scaled errors of the embedded 4th-order
+// difference.
 struct Dp5State {
     numb X[6][UCB_NX];  // stage points X1 (= x) .. X6
     numb k1[UCB_NX], k7[UCB_NX], xn[UCB_NX];
 };
 
-__device__ __forceinline__ double dp5_state_step(Dp5State& S, const numb* a, numb hn, double h, double rtol,
-                                                 double atol) {  // returns the sum of squared scaled errors
+__device__ __forceinline__ double dp5_state_step(Dp5State& S, const numb* a, const Dp5Coef& c, double rtol,
+                                                 double atol) {
     numb k2[UCB_NX], k3[UCB_NX], k4[UCB_NX], k5[UCB_NX], k6[UCB_NX];
     const numb* x = S.X[0];
 #pragma unroll
-    for (int i = 0; i < UCB_NX; ++i) S.X[1][i] = x[i] + hn * ((numb)DP_A21 * S.k1[i]);
+    for (int i = 0; i < UCB_NX; ++i) S.X[1][i] = fma(c.c21, S.k1[i], x[i]);
     ucb_rhs(S.X[1], a, k2);
 #pragma unroll
-    for (int i = 0; i < UCB_NX; ++i) S.X[2][i] = x[i] + hn * ((numb)DP_A31 * S.k1[i] + (numb)DP_A32 * k2[i]);
+    for (int i = 0; i < UCB_NX; ++i) S.X[2][i] = fma(c.c32, k2[i], fma(c.c31, S.k1[i], x[i]));
     ucb_rhs(S.X[2], a, k3);
 #pragma unroll
-    for (int i = 0; i < UCB_NX; ++i)
-        S.X[3][i] = x[i] + hn * ((numb)DP_A41 * S.k1[i] + (numb)DP_A42 * k2[i] + (numb)DP_A43 * k3[i]);
+    for (int i = 0; i < UCB_NX; ++i) S.X[3][i] = fma(c.c43, k3[i], fma(c.c42, k2[i], fma(c.c41, S.k1[i], x[i])));
     ucb_rhs(S.X[3], a, k4);
 #pragma unroll
     for (int i = 0; i < UCB_NX; ++i)
-        S.X[4][i] = x[i] + hn * ((numb)DP_A51 * S.k1[i] + (numb)DP_A52 * k2[i] + (numb)DP_A53 * k3[i] +
-                                 (numb)DP_A54 * k4[i]);
+        S.X[4][i] = fma(c.c54, k4[i], fma(c.c53, k3[i], fma(c.c52, k2[i], fma(c.c51, S.k1[i], x[i]))));
     ucb_rhs(S.X[4], a, k5);
 #pragma unroll
     for (int i = 0; i < UCB_NX; ++i)
-        S.X[5][i] = x[i] + hn * ((numb)DP_A61 * S.k1[i] + (numb)DP_A62 * k2[i] + (numb)DP_A63 * k3[i] +
-                                 (numb)DP_A64 * k4[i] + (numb)DP_A65 * k5[i]);
+        S.X[5][i] = fma(c.c65, k5[i], fma(c.c64, k4[i], fma(c.c63, k3[i], fma(c.c62, k2[i], fma(c.c61, S.k1[i], x[i])))));
     ucb_rhs(S.X[5], a, k6);
 #pragma unroll
     for (int i = 0; i < UCB_NX; ++i)
-        S.xn[i] = x[i] + hn * ((numb)DP_B1 * S.k1[i] + (numb)DP_B3 * k3[i] + (numb)DP_B4 * k4[i] +
-                               (numb)DP_B5 * k5[i] + (numb)DP_B6 * k6[i]);
+        S.xn[i] = fma(c.b6, k6[i], fma(c.b5, k5[i], fma(c.b4, k4[i], fma(c.b3, k3[i], fma(c.b1, S.k1[i], x[i])))));
     ucb_rhs(S.xn, a, S.k7);
-    double err2 = 0;
+    double e[UCB_NX], sc[UCB_NX];
 #pragma unroll
     for (int i = 0; i < UCB_NX; ++i) {
-        const double e = h * ((double)DP_E1 * S.k1[i] + (double)DP_E3 * k3[i] + (double)DP_E4 * k4[i] +
-                              (double)DP_E5 * k5[i] + (double)DP_E6 * k6[i] + (double)DP_E7 * S.k7[i]);
-        const double sc = atol + rtol * fmax(fabs((double)x[i]), fabs((double)S.xn[i]));
-        err2 += (e / sc) * (e / sc);
+        e[i] = fma(c.e7, (double)S.k7[i], fma(c.e6, (double)k6[i], fma(c.e5, (double)k5[i],
+               fma(c.e4, (double)k4[i], fma(c.e3, (double)k3[i], c.e1 * (double)S.k1[i])))));
+        sc[i] = fma(rtol, fmax(fabs((double)x[i]), fabs((double)S.xn[i])), atol);
     }
-    return err2;
+    return scaled_sum_sq<UCB_NX>(e, sc);
 }
 
 // One tangent vector through the same DP5 stages (v' = J(x) v with J at the stored stage
 // points): writes the 5th-order vn and returns its sum of squared scaled errors.
-__device__ __forceinline__ double dp5_tangent_step(const Dp5State& S, const numb* a, numb hn, double h, double rtol,
+__device__ __forceinline__ double dp5_tangent_step(const Dp5State& S, const numb* a, const Dp5Coef& c, double rtol,
                                                    double atol, const numb* v, numb* vn) {
     numb L1[UCB_NX], L2[UCB_NX], L3[UCB_NX], L4[UCB_NX], L5[UCB_NX], L6[UCB_NX], vt[UCB_NX];
     ucb_jvp(S.X[0], a, v, L1);
 #pragma unroll
-    for (int i = 0; i < UCB_NX; ++i) vt[i] = v[i] + hn * ((numb)DP_A21 * L1[i]);
+    for (int i = 0; i < UCB_NX; ++i) vt[i] = fma(c.c21, L1[i], v[i]);
     ucb_jvp(S.X[1], a, vt, L2);
 #pragma unroll
-    for (int i = 0; i < UCB_NX; ++i) vt[i] = v[i] + hn * ((numb)DP_A31 * L1[i] + (numb)DP_A32 * L2[i]);
+    for (int i = 0; i < UCB_NX; ++i) vt[i] = fma(c.c32, L2[i], fma(c.c31, L1[i], v[i]));
     ucb_jvp(S.X[2], a, vt, L3);
 #pragma unroll
-    for (int i = 0; i < UCB_NX; ++i)
-        vt[i] = v[i] + hn * ((numb)DP_A41 * L1[i] + (numb)DP_A42 * L2[i] + (numb)DP_A43 * L3[i]);
+    for (int i = 0; i < UCB_NX; ++i) vt[i] = fma(c.c43, L3[i], fma(c.c42, L2[i], fma(c.c41, L1[i], v[i])));
     ucb_jvp(S.X[3], a, vt, L4);
 #pragma unroll
     for (int i = 0; i < UCB_NX; ++i)
-        vt[i] = v[i] + hn * ((numb)DP_A51 * L1[i] + (numb)DP_A52 * L2[i] + (numb)DP_A53 * L3[i] + (numb)DP_A54 * L4[i]);
+        vt[i] = fma(c.c54, L4[i], fma(c.c53, L3[i], fma(c.c52, L2[i], fma(c.c51, L1[i], v[i]))));
     ucb_jvp(S.X[4], a, vt, L5);
 #pragma unroll
     for (int i = 0; i < UCB_NX; ++i)
-        vt[i] = v[i] + hn * ((numb)DP_A61 * L1[i] + (numb)DP_A62 * L2[i] + (numb)DP_A63 * L3[i] +
-                             (numb)DP_A64 * L4[i] + (numb)DP_A65 * L5[i]);
+        vt[i] = fma(c.c65, L5[i], fma(c.c64, L4[i], fma(c.c63, L3[i], fma(c.c62, L2[i], fma(c.c61, L1[i], v[i])))));
     ucb_jvp(S.X[5], a, vt, L6);
 #pragma unroll
     for (int i = 0; i < UCB_NX; ++i)
-        vn[i] = v[i] + hn * ((numb)DP_B1 * L1[i] + (numb)DP_B3 * L3[i] + (numb)DP_B4 * L4[i] + (numb)DP_B5 * L5[i] +
-                             (numb)DP_B6 * L6[i]);
+        vn[i] = fma(c.b6, L6[i], fma(c.b5, L5[i], fma(c.b4, L4[i], fma(c.b3, L3[i], fma(c.b1, L1[i], v[i])))));
     ucb_jvp(S.xn, a, vn, L2);  // L7, reusing L2's registers
-    double err2 = 0;
+    double e[UCB_NX], sc[UCB_NX];
 #pragma unroll
     for (int i = 0; i < UCB_NX; ++i) {
-        const double e = h * ((double)DP_E1 * L1[i] + (double)DP_E3 * L3[i] + (double)DP_E4 * L4[i] +
-                              (double)DP_E5 * L5[i] + (double)DP_E6 * L6[i] + (double)DP_E7 * L2[i]);
-        const double sc = atol + rtol * fmax(fabs((double)v[i]), fabs((double)vn[i]));
-        err2 += (e / sc) * (e / sc);
+        e[i] = fma(c.e7, (double)L2[i], fma(c.e6, (double)L6[i], fma(c.e5, (double)L5[i],
+               fma(c.e4, (double)L4[i], fma(c.e3, (double)L3[i], c.e1 * (double)L1[i])))));
+        sc[i] = fma(rtol, fmax(fabs((double)v[i]), fabs((double)vn[i])), atol);
     }
-    return err2;
+    return scaled_sum_sq<UCB_NX>(e, sc);
 }
 
 __device__ __forceinline__ void ls_cell_dp5(const UcbLsParams& p, long long kidx, long long& ns) {
@@ -400,19 +461,20 @@ __device__ __forceinline__ void ls_cell_dp5(const UcbLsParams& p, long long kidx
         const double t_target = measuring ? t_stop : (double)p.transient;
         bool last = false;
         if (t + h >= t_target) { h = t_target - t; last = true; }
-        const numb hn = (numb)h;
-        const double ex2 = dp5_state_step(S, a, hn, h, p.rtol, p.atol);
+        const Dp5Coef cf = dp5_coef((numb)h, h);
+        const double ex2 = dp5_state_step(S, a, cf, p.rtol, p.atol);
         ns += 1;
-        double err = sqrt(ex2 / UCB_NX);
+        // err^2: the mean of the squared scaled errors (the RMS norm, squared)
+        double err2 = ex2 * (1.0 / UCB_NX);
         numb Vn[UCB_NX][UCB_NX];
-        if (err <= 1.0 && measuring) {
+        if (err2 <= 1.0 && measuring) {
             double ev2 = 0;
 #pragma unroll
-            for (int k = 0; k < UCB_NX; ++k) ev2 += dp5_tangent_step(S, a, hn, h, p.rtol, p.atol, V[k], Vn[k]);
-            err = sqrt((ex2 + ev2) / (UCB_NX + UCB_NX * UCB_NX));
+            for (int k = 0; k < UCB_NX; ++k) ev2 += dp5_tangent_step(S, a, cf, p.rtol, p.atol, V[k], Vn[k]);
+            err2 = (ex2 + ev2) * (1.0 / (UCB_NX + UCB_NX * UCB_NX));
         }
-        if (!isfinite(err)) { ok = false; break; }
-        if (err <= 1.0) {
+        if (!isfinite(err2)) { ok = false; break; }
+        if (err2 <= 1.0) {
             if (measuring) {
 #pragma unroll
                 for (int k = 0; k < UCB_NX; ++k)
@@ -433,11 +495,11 @@ __device__ __forceinline__ void ls_cell_dp5(const UcbLsParams& p, long long kidx
                 spread = fmax(0.0, (acc[0] - acc[UCB_NX - 1]) / t_meas);
             }
             if (last && !measuring) measuring = true;
-            const double fac = (err > 0) ? 0.9 * pow(err, -0.2) : facmax;
+            const double fac = (err2 > 0) ? dp5_factor(err2) : facmax;
             h *= fmin(facmax, fmax(0.2, fac));
             facmax = 5.0;
         } else {
-            h *= fmax(0.2, 0.9 * pow(err, -0.2));
+            h *= fmax(0.2, dp5_factor(err2));
             facmax = 2.0;
             if (!(h > 1e-14)) { ok = false; break; }
         }
@@ -450,7 +512,7 @@ __device__ __forceinline__ void ls_cell_dp5(const UcbLsParams& p, long long kidx
 
 }  // namespace ucbdev
 
-extern "C" __global__ void __launch_bounds__(UCB_BLOCK) ucb_ls_kernel(const UcbLsParams p) {
+extern "C" __global__ void UCB_LAUNCH_BOUNDS ucb_ls_kernel(const UcbLsParams p) {
     const int lane = threadIdx.x & 31;
     long long ns = 0;
     for (;;) {

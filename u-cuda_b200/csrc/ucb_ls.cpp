@@ -375,7 +375,8 @@ extern "C" int ucb_autotune_ls2d(ucb_engine* e, const ucb_ls2d_request* req, int
     SystemCode sys;
     const std::string key = tune_key(ls_compile_request(base, m, sys));
     // trial: the same window on at most 384^2 cells, horizon scaled to about 1.2e10 steps
-    // (fixed step) or the DP5 interval cut to 50 time units
+    // (fixed step) or the DP5 interval cut to 50 time units and 20,000 attempts per cell
+    // (cells that turn stiff would otherwise run to the full attempt cap in every trial)
     ucb_ls2d_request t = base;
     t.n_pts = std::min(base.n_pts, 384);
     const int nx = base.amount_of_x;
@@ -384,6 +385,7 @@ extern "C" int ucb_autotune_ls2d(ucb_engine* e, const ucb_ls2d_request* req, int
         t.t_end = std::min(t_end, 50.0);
         t.t_max = std::min(base.t_max, t.t_end);
         t.transient_time = std::min(base.transient_time, 50.0);
+        t.max_steps = std::min(base.max_steps > 0 ? base.max_steps : 20000LL, 20000LL);
     } else {
         const double steps_cell = skip + (double)n_blocks * (nx + 1) * (double)(nt + 1);
         const double f = trial_scale((double)t.n_pts * t.n_pts, steps_cell);
