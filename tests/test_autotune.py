@@ -89,3 +89,29 @@ def test_autotune_basins_and_bif2d(tmp_path, monkeypatch):
     assert rep2["candidates"] >= 3
     np.testing.assert_array_equal(eng.run_bif2d(b2)[0], ref2)
     eng.close()
+
+
+def test_forced_system_compiles_in_every_form():
+    """A system with a clock (a variable of constant derivative) gets the compensated FP32
+    clock in the kernels whose Stepper serves one trajectory (tangent LLE, bifurcation,
+    reference-method basins, DP5) and none in those that step several trajectories on one
+    Stepper (shadow LLE, the fixed LS method): every combination compiles."""
+    from helpers import DUFFING
+    duffing = dict(lle2d_case(), body=rk4_body(DUFFING), ic=(0.0, 0.0, 0.0), values=(0.0,),
+                   sweep_over_var=True, sweep_over_var_2=True, var_sweep_index=0, var_sweep_index_2=1,
+                   param_lo=-1.0, param_hi=1.0, param_lo_2=-1.0, param_hi_2=1.0)
+    body = rk4_body(DUFFING)
+    grid = dict(n_pts=4, sweep_over_var=True, sweep_over_var_2=True, var_sweep_index=0, var_sweep_index_2=1,
+                param_lo=-1, param_hi=1, param_lo_2=-1, param_hi_2=1)
+    for prec in (ucb.PREC_F32, ucb.PREC_F64):
+        opt = ucb.options(precision=prec)
+        for method in (ucb.LLE_AUTO, ucb.LLE_SHADOW):
+            ucb.precompile(engine_request(ucb, duffing, precision=prec, lle_method=method))
+        ucb.precompile(ucb.Engine.ls2d_request(body, 3, (0.0, 0.0, 0.0), (0.0,), method=ucb.LS_DP5, t_end=10.0,
+                                               t_max=10.0, opt=opt, **grid))
+        ucb.precompile(ucb.Engine.ls2d_request(body, 3, (0.0, 0.0, 0.0), (0.0,), method=ucb.LS_FIXED, t_max=10.0,
+                                               opt=opt, **grid))
+        ucb.precompile(ucb.Engine.bif2d_request(body, 3, (0.0, 0.0, 0.0), (0.0,), opt=opt, **grid))
+        ucb.precompile(ucb.Engine.basins_dbscan_request(body, 3, (0, 0, 0), (0.0,), n_pts=4, opt=opt))
+        ucb.precompile(ucb.Engine.bif1d_request(body, 3, (0.0, 0.0, 0.0), (0.0,), n_pts=4, sweep_over_var=True,
+                                                var_sweep_index=0, param_lo=-1, param_hi=1, opt=opt))

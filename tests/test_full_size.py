@@ -8,7 +8,7 @@ well-conditioned."""
 import numpy as np
 import pytest
 
-import oracle as O
+from oracle import oracle as O
 import ucb
 from helpers import engine_request, kernel_grid, lle2d_case
 

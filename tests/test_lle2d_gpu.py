@@ -120,6 +120,31 @@ def test_native_forced_system_trajectory_parity(eng, prec, rtol):
         np.testing.assert_allclose(xs[cell], ref, rtol=rtol, atol=rtol)
 
 
+def test_fp32_forced_clock_is_compensated(eng):
+    """FP32 native form over a long horizon: the forced, damped linear oscillator
+    x'' + 0.5 x' + x = cos(s), s' = 1 settles on x = 2 sin(t), v = 2 cos(t). After 3.5e5 steps
+    (t ~ 1.1e4) a plain FP32 clock would have fallen ~30 rad behind (each add rounds to the
+    ulp of the growing phase); the compensated clock stays within two ulps of n h, and the
+    state within a few 1e-3 of FP64 (which is within 1e-4 of the closed form)."""
+    import math
+    body = ucb.codegen(r"\dot{x} = v \\ \dot{v} = -0.5 v - x + \cos(s) \\ \dot{s} = 1", "x,v,s")[0]
+    h = 2 * math.pi / 200
+    c = dict(body=body, nx=3, ic=(0.0, 0.0, 0.0), values=(0.0,), n_pts=4, sweep_over_var=True,
+             sweep_over_var_2=True, var_sweep_index=0, var_sweep_index_2=1, param_index=1, param_index_2=1,
+             param_lo=-1.0, param_hi=1.0, param_lo_2=-1.0, param_hi_2=1.0, h=h, transient_time=1.0, t_max=2.0,
+             NT=0.1, eps=1e-4, max_value=1e6)
+    n_steps = 350_000
+    x32 = eng.lle2d_states(engine_request(ucb, c, precision=ucb.PREC_F32, mode=ucb.MODE_NATIVE), n_steps)
+    x64 = eng.lle2d_states(engine_request(ucb, c, precision=ucb.PREC_F64, mode=ucb.MODE_NATIVE), n_steps)
+    clock = n_steps * float(np.float32(h))
+    ulp = float(np.spacing(np.float32(clock)))
+    np.testing.assert_allclose(x32[:, 2], clock, atol=2 * ulp, rtol=0)
+    t = n_steps * h
+    np.testing.assert_allclose(x64[:, 0], 2 * math.sin(t), atol=1e-4)
+    np.testing.assert_allclose(x64[:, 1], 2 * math.cos(t), atol=1e-4)
+    np.testing.assert_allclose(x32[:, :2], x64[:, :2], atol=5e-3, rtol=0)
+
+
 def test_exact_trajectory_bitwise(eng):
     c = lle2d_case(n=4)
     xs = eng.lle2d_states(engine_request(ucb, c, precision=ucb.PREC_F64, mode=ucb.MODE_EXACT), 3000)

@@ -530,7 +530,9 @@ CompileRequest features_request(const ucb_basins_dbscan_request& q, SystemCode& 
     sys = make_system_code(q.krs_body, q.amount_of_x, q.n_values, q.opt.precision, q.opt.mode, false);
     CompileRequest rq;
     rq.name = "ucb_basins_ref.cu";
-    rq.source = make_prelude(q.opt.precision, q.amount_of_x, q.n_values, m, true, sys, {"UCB_BIF_NO_KERNELS 1"}) +
+    std::vector<std::string> defs = clock_defines(sys);
+    defs.push_back("UCB_BIF_NO_KERNELS 1");
+    rq.source = make_prelude(q.opt.precision, q.amount_of_x, q.n_values, m, true, sys, defs) +
                 "#include \"ucb_device.cuh\"\n#include \"ucb_bif.cuh\"\n#include \"ucb_basins_ref.cuh\"\n";
     rq.headers = device_headers();
     rq.options.push_back(sys.exact ? "--fmad=false" : "--fmad=true");

@@ -78,7 +78,13 @@ struct SystemCode {
     std::string note;     // why the exact form was chosen, when native was requested
     int trig_phase = -1;  // native form: forcing phase variable (ucb_rhs_trig), -1 none
     double trig_rate = 0; // its constant rate (dX[p]/dt)
+    int clock_var = -1;   // native FP32 form: a variable with a constant derivative (-1 none)
+    double clock_rate = 0;
 };
+// The define that turns on the compensated clock of the native FP32 step
+// (UCB_KAHAN_CLOCK), for kernels where each Stepper serves one trajectory; empty if the
+// build has no clock.
+std::vector<std::string> clock_defines(const SystemCode& sys);
 
 bool ensure_init(ucb_engine* e, std::string& err);
 bool ensure_workspace(ucb_engine* e, size_t bytes, std::string& err);

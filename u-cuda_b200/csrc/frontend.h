@@ -92,6 +92,9 @@ std::string emit_packed_device(const Rhs& r);
 // by rate * h per step) and whose sin / cos appear in the system. False if there is none
 // (or more than one).
 bool find_trig_phase(const Rhs& r, int& p, double& rate);
+// A clock: the first variable p whose right-hand side is a nonzero constant `rate` (time
+// itself, or a forcing phase). False if there is none.
+bool find_clock(const Rhs& r, int& p, double& rate);
 // ucb_rhs_trig(X1, a, dX, cph, sph): ucb_rhs with cos(X1[p]) / sin(X1[p]) taken from the
 // arguments (the forcing evaluated by the caller, e.g. from a table of the stage phases).
 std::string emit_rhs_trig_device(const Rhs& r, int p, bool single_precision);

@@ -709,6 +709,16 @@ bool find_trig_phase(const Rhs& r, int& p, double& rate) {
     return true;
 }
 
+bool find_clock(const Rhs& r, int& p, double& rate) {
+    for (int i = 0; i < r.nx; ++i) {
+        if (r.f[i]->kind != Node::Num || r.f[i]->num == 0.0) continue;
+        p = i;
+        rate = r.f[i]->num;
+        return true;
+    }
+    return false;
+}
+
 std::string emit_rhs_trig_device(const Rhs& r, int p, bool sp) {
     std::ostringstream o;
     o << "__device__ __forceinline__ void ucb_rhs_trig(const numb* X1, const numb* a, numb* dX, numb cph, numb sph) "

@@ -132,6 +132,14 @@ __device__ __forceinline__ void ucb_sincos(double v, double* s, double* c) { sin
 __device__ __forceinline__ void ucb_sincos(float v, float* s, float* c) { sincosf(v, s, c); }
 #endif
 
+#ifdef UCB_KAHAN_CLOCK
+#define UCB_CLOCK_SAVE(x) const numb clock_prev_ = (x)[UCB_CLOCK_VAR]
+#define UCB_CLOCK_ADVANCE(x) (x)[UCB_CLOCK_VAR] = clock_next(clock_prev_)
+#else
+#define UCB_CLOCK_SAVE(x) (void)0
+#define UCB_CLOCK_ADVANCE(x) (void)0
+#endif
+
 // Classical RK4 on ucb_rhs, FMA-ordered: the same scheme as codegen.cpp scheme_rk4
 // (k1..k4 at t, t+h/2, t+h/2, t+h; x += h/6 (k1 + 2k2 + 2k3 + k4)) with the half/sixth
 // step factors hoisted and every update written as a fused multiply-add.
@@ -142,17 +150,47 @@ struct Stepper {
     numb hh, h6;
 #ifdef UCB_TRIG_PHASE
     numb ch, sh, cf, sf;  // cos / sin of rate h/2 and of rate h
+#endif
+#ifdef UCB_KAHAN_CLOCK
+    // Compensated clock (FP32 builds with a variable of constant derivative, one trajectory
+    // per Stepper): X[UCB_CLOCK_VAR] gains h * rate per step, and a plain FP32 add loses up
+    // to half an ulp of the growing clock every step — at t ~ 1e4 with h = 2 pi / 200 a
+    // forcing phase falls about 30 rad behind in 3.5e5 steps, i.e. the forcing runs at the
+    // wrong frequency. Kahan summation carries the rounding error in kc (the stored clock
+    // exceeds the exact sum by kc), so the clock stays within an ulp of x0 + n h rate.
+    numb hr;
+    mutable numb kc;
+#endif
     __device__ __forceinline__ explicit Stepper(numb h) : hh(h * (numb)0.5), h6(h * (numb)(1.0 / 6.0)) {
+#ifdef UCB_TRIG_PHASE
         ucb_sincos((numb)((numb)UCB_TRIG_RATE * hh), &sh, &ch);
         ucb_sincos((numb)((numb)UCB_TRIG_RATE * h), &sf, &cf);
+#endif
+#ifdef UCB_KAHAN_CLOCK
+        hr = h * (numb)UCB_CLOCK_RATE;
+        kc = (numb)0;
+#endif
     }
-#else
-    __device__ __forceinline__ explicit Stepper(numb h) : hh(h * (numb)0.5), h6(h * (numb)(1.0 / 6.0)) {}
+#ifdef UCB_KAHAN_CLOCK
+    // The clock after one step from xc (Kahan's compensated sum).
+    __device__ __forceinline__ numb clock_next(numb xc) const {
+        const numb y = hr - kc;
+        const numb t = xc + y;
+        kc = (t - xc) - y;
+        return t;
+    }
 #endif
     __device__ __forceinline__ void step(numb* x, const numb* a, numb h) const {
 #ifdef UCB_TRIG_PHASE
         numb s0, c0;
         ucb_sincos(x[UCB_TRIG_PHASE], &s0, &c0);
+#if defined(UCB_KAHAN_CLOCK) && UCB_CLOCK_VAR == UCB_TRIG_PHASE
+        {  // the forcing at the compensated phase x - kc (first order in kc <= half an ulp)
+            const numb cc = fma(kc, s0, c0);
+            s0 = fma(-kc, c0, s0);
+            c0 = cc;
+        }
+#endif
         const numb tc[6] = {c0, s0, fma(c0, ch, -s0 * sh), fma(s0, ch, c0 * sh), fma(c0, cf, -s0 * sf),
                             fma(s0, cf, c0 * sf)};
         step_trig(x, a, h, tc);
@@ -168,8 +206,10 @@ struct Stepper {
 #pragma unroll
         for (int i = 0; i < UCB_NX; ++i) xt[i] = fma(h, k3[i], x[i]);
         ucb_rhs(xt, a, k4);
+        UCB_CLOCK_SAVE(x);
 #pragma unroll
         for (int i = 0; i < UCB_NX; ++i) x[i] = fma(h6, (k1[i] + k4[i]) + (numb)2 * (k2[i] + k3[i]), x[i]);
+        UCB_CLOCK_ADVANCE(x);
 #endif
     }
 #ifdef UCB_TRIG_PHASE
@@ -188,8 +228,10 @@ struct Stepper {
 #pragma unroll
         for (int i = 0; i < UCB_NX; ++i) xt[i] = fma(h, k3[i], x[i]);
         ucb_rhs_trig(xt, a, k4, c2, s2);
+        UCB_CLOCK_SAVE(x);
 #pragma unroll
         for (int i = 0; i < UCB_NX; ++i) x[i] = fma(h6, (k1[i] + k4[i]) + (numb)2 * (k2[i] + k3[i]), x[i]);
+        UCB_CLOCK_ADVANCE(x);
     }
 #endif
 #ifdef UCB_HAS_JVP
@@ -211,11 +253,13 @@ struct Stepper {
         for (int i = 0; i < UCB_NX; ++i) { xt[i] = fma(h, k3[i], x[i]); vt[i] = fma(h, l3[i], v[i]); }
         ucb_rhs(xt, a, k4);
         ucb_jvp(xt, a, vt, l4);
+        UCB_CLOCK_SAVE(x);
 #pragma unroll
         for (int i = 0; i < UCB_NX; ++i) {
             x[i] = fma(h6, (k1[i] + k4[i]) + (numb)2 * (k2[i] + k3[i]), x[i]);
             v[i] = fma(h6, (l1[i] + l4[i]) + (numb)2 * (l2[i] + l3[i]), v[i]);
         }
+        UCB_CLOCK_ADVANCE(x);  // (the tangent's clock component has derivative 0)
     }
 #endif
 };

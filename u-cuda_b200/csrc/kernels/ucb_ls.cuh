@@ -433,6 +433,10 @@ __device__ __forceinline__ void ls_cell_dp5(const UcbLsParams& p, long long kidx
 #pragma unroll
     for (int i = 0; i < UCB_NV; ++i) a[i] = p.vals[i];
     apply_sweep(c, p.axis0, p.axis1, S.X[0], a);
+#ifdef UCB_KAHAN_CLOCK
+    // the clock of an FP32 build is set from the FP64 time after every accepted step
+    const double clock0 = (double)S.X[0][UCB_CLOCK_VAR];
+#endif
     numb V[UCB_NX][UCB_NX];
     {
         Rng st;
@@ -486,6 +490,9 @@ __device__ __forceinline__ void ls_cell_dp5(const UcbLsParams& p, long long kidx
             t = t_new;
 #pragma unroll
             for (int i = 0; i < UCB_NX; ++i) { S.X[0][i] = S.xn[i]; S.k1[i] = S.k7[i]; }
+#ifdef UCB_KAHAN_CLOCK
+            S.X[0][UCB_CLOCK_VAR] = (numb)fma((double)UCB_CLOCK_RATE, t, clock0);
+#endif
             if (diverged(S.X[0], p.maxv)) { ok = false; break; }
             if (measuring && (++since_gs >= p.gs_every || last || t_gs * spread > UCB_GS_BUDGET)) {
                 ok = mgs(V, acc);

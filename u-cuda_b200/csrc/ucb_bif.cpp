@@ -53,7 +53,7 @@ CompileRequest bif_compile_request(const ucb_bif1d_request& q, SystemCode& sys) 
     sys = make_system_code(q.krs_body, q.amount_of_x, q.n_values, q.opt.precision, q.opt.mode, false);
     CompileRequest rq;
     rq.name = "ucb_bif1d.cu";
-    rq.source = make_prelude(q.opt.precision, q.amount_of_x, q.n_values, m, true, sys, {}) +
+    rq.source = make_prelude(q.opt.precision, q.amount_of_x, q.n_values, m, true, sys, clock_defines(sys)) +
                 "#include \"ucb_device.cuh\"\n#include \"ucb_bif.cuh\"\n";
     rq.headers = device_headers();
     rq.options.push_back(sys.exact ? "--fmad=false" : "--fmad=true");

@@ -91,7 +91,9 @@ CompileRequest bif2d_compile_request(const ucb_bif2d_request& q, const SweepMap&
     sys = make_system_code(q.krs_body, q.amount_of_x, q.n_values, q.opt.precision, q.opt.mode, false);
     CompileRequest rq;
     rq.name = "ucb_bif2d.cu";
-    rq.source = make_prelude(q.opt.precision, q.amount_of_x, q.n_values, m, true, sys, {"UCB_BIF2D 1"}) +
+    std::vector<std::string> defs = clock_defines(sys);
+    defs.push_back("UCB_BIF2D 1");
+    rq.source = make_prelude(q.opt.precision, q.amount_of_x, q.n_values, m, true, sys, defs) +
                 "#include \"ucb_device.cuh\"\n#include \"ucb_bif.cuh\"\n";
     rq.headers = device_headers();
     rq.options.push_back(sys.exact ? "--fmad=false" : "--fmad=true");

@@ -155,6 +155,11 @@ std::string make_prelude(int precision, int nx, int nv, const SweepMap& m, bool 
     return o.str();
 }
 
+std::vector<std::string> clock_defines(const SystemCode& sys) {
+    if (sys.exact || sys.clock_var < 0) return {};
+    return {"UCB_KAHAN_CLOCK 1"};
+}
+
 SystemCode make_system_code(const std::string& krs_body, int nx, int nv, int precision, int mode,
                             bool want_jvp) {
     SystemCode s;
@@ -189,6 +194,13 @@ SystemCode make_system_code(const std::string& krs_body, int nx, int nv, int pre
             }
             int p = -1;
             double rate = 0;
+            if (precision == UCB_PREC_F32 && fe::find_clock(r, p, rate)) {
+                char rbuf[64];
+                std::snprintf(rbuf, sizeof rbuf, "%.17g", rate);
+                s.code += "#define UCB_CLOCK_VAR " + std::to_string(p) + "\n#define UCB_CLOCK_RATE " + rbuf + "\n";
+                s.clock_var = p;
+                s.clock_rate = rate;
+            }
             if (fe::find_trig_phase(r, p, rate)) {
                 s.code += fe::emit_rhs_trig_device(r, p, precision == UCB_PREC_F32);
                 char rbuf[64];
@@ -414,10 +426,14 @@ CompileRequest lle_compile_request(const ucb_lle2d_request& q, const LlePlan& pl
     L.tangent = tangent;
     std::vector<std::string> defs;
     if (tangent) defs.push_back("UCB_TANGENT 1");
+    // The tangent form steps one trajectory per cell (the shadow form two, on one Stepper)
+    if (tangent)
+        for (auto& d : clock_defines(L.sys)) defs.push_back(d);
     // Two cells per thread in packed FP32 pairs (on request): FP32 tangent form with a
-    // uniform step and a compile-time block length.
+    // uniform step and a compile-time block length, for systems without a clock (the pair
+    // step has no compensated clock).
     if (tangent && prec == UCB_PREC_F32 && L.sys.has_packed && plan.map.h_axis == -1 && plan.nt_steps >= 1 &&
-        plan.nt_steps <= 100 && q.opt.paired_cells)
+        plan.nt_steps <= 100 && q.opt.paired_cells && L.sys.clock_var < 0)
         defs.push_back("UCB_PACKED 1");
     // Block length known at compile time (no h sweep): the block loop unrolls fully.
     if (plan.map.h_axis == -1 && plan.nt_steps >= 1 && plan.nt_steps <= 100)

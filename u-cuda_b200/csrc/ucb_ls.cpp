@@ -58,9 +58,12 @@ CompileRequest ls_compile_request(const ucb_ls2d_request& q, const SweepMap& m, 
     sys = make_system_code(q.krs_body, q.amount_of_x, q.n_values, prec, dp5 ? UCB_MODE_NATIVE : q.opt.mode, dp5);
     CompileRequest rq;
     rq.name = "ucb_ls2d.cu";
-    rq.source = make_prelude(prec, q.amount_of_x, q.n_values, m, q.opt.nominal_steps == 0, sys,
-                             {dp5 ? "UCB_LS_DP5 1" : "UCB_LS_FIXED 1",
-                              prec == UCB_PREC_F64 ? "UCB_GS_BUDGET 20.0" : "UCB_GS_BUDGET 8.0"}) +
+    // DP5 keeps the clock from its FP64 time; the fixed method steps N + 1 trajectories on
+    // one Stepper, so it has no compensated clock
+    std::vector<std::string> defs = dp5 ? clock_defines(sys) : std::vector<std::string>{};
+    defs.push_back(dp5 ? "UCB_LS_DP5 1" : "UCB_LS_FIXED 1");
+    defs.push_back(prec == UCB_PREC_F64 ? "UCB_GS_BUDGET 20.0" : "UCB_GS_BUDGET 8.0");
+    rq.source = make_prelude(prec, q.amount_of_x, q.n_values, m, q.opt.nominal_steps == 0, sys, defs) +
                 "#include \"ucb_device.cuh\"\n#include \"ucb_ls.cuh\"\n";
     rq.headers = device_headers();
     rq.options.push_back(sys.exact ? "--fmad=false" : "--fmad=true");
