@@ -481,6 +481,14 @@ def run_other_configs(eng, which=OTHER_CONFIGS, args=None):
             "rk4_steps_per_s": res.steps / (res.kernel_ms * 1e-3),
             "oscillating_clusters": res.n_clusters, "fixed_point_clusters": -res.min_cluster_idx,
             "classes": {str(k): int((cls == k).sum()) for k in (-1, 0, 1)}}
+        if name == "plain_fp64_native":
+            ref_bd = (lab, f1, f2)
+        else:
+            def rel(a, b):
+                return float(np.median(np.abs(a - b) / np.maximum(np.abs(b), 1e-300)))
+            out["basins_dbscan_duffing_1024"]["fp32_vs_fp64"] = {
+                "label_agreement": float((lab == ref_bd[0]).mean()),
+                "feature1_median_rel_diff": rel(f1, ref_bd[1]), "feature2_median_rel_diff": rel(f2, ref_bd[2])}
     return out
 
 
