@@ -429,17 +429,18 @@ def run_other_configs(eng, which=OTHER_CONFIGS, args=None):
                                              period=2 * np.pi, steps_per_period=200, max_periods=2000,
                                              match_count=20, match_tol=1e-6, phase_var=2, max_value=1e6,
                                              opt=ucb.options(precision=prec))
-        shape = eng.autotune(breq(4096)) if tune else None
+        nb = args.basins_n if args else 4096
+        shape = eng.autotune(breq(nb)) if tune else None
         eng.run_basins(breq(8))
-        (labels, periods, iters, att, res), ms = _timed(lambda: eng.run_basins(breq(4096)))
-        out.setdefault("basins_duffing_4096", {})[name] = {
-            "wall_ms": ms, "kernel_ms": res.kernel_ms, "cells_per_s": 4096 * 4096 / (res.kernel_ms * 1e-3),
+        (labels, periods, iters, att, res), ms = _timed(lambda: eng.run_basins(breq(nb)))
+        out.setdefault(f"basins_duffing_{nb}", {})[name] = {
+            "wall_ms": ms, "kernel_ms": res.kernel_ms, "cells_per_s": nb * nb / (res.kernel_ms * 1e-3),
             "rk4_steps_per_s": res.steps / (res.kernel_ms * 1e-3), "attractors": att, "launch_shape": shape,
             "converged_fraction": float((labels > 0).mean()), "mean_periods": float(iters.mean())}
         if name == "plain_fp64":
             ref_labels = labels
         else:
-            out["basins_duffing_4096"]["fp32_label_agreement"] = float((labels == ref_labels).mean())
+            out[f"basins_duffing_{nb}"]["fp32_label_agreement"] = float((labels == ref_labels).mean())
     # Lorenz period map (run_bifurcation_2d): rho in [20, 200] x sigma in [5, 15] on n x n (512),
     # x0 = (0.1, 0.1, 0.1), h = 0.01, 5,000 transient + 20,000 recorded steps, the peaks of x
     # clustered per cell with eps 0.1.
@@ -474,10 +475,11 @@ def run_other_configs(eng, which=OTHER_CONFIGS, args=None):
                                                     t_max=1000.0, transient_time=10000.0, eps_dbscan=0.5,
                                                     opt=ucb.options(precision=prec))
         eng.run_basins_dbscan(bdreq(4))
-        (lab, f1, f2, cls, res), ms = _timed(lambda: eng.run_basins_dbscan(bdreq(1024)))
-        out.setdefault("basins_dbscan_duffing_1024", {})[name] = {
+        nd = args.basins_dbscan_n if args else 1024
+        (lab, f1, f2, cls, res), ms = _timed(lambda: eng.run_basins_dbscan(bdreq(nd)))
+        out.setdefault(f"basins_dbscan_duffing_{nd}", {})[name] = {
             "wall_ms": ms, "features_kernel_ms": res.kernel_ms, "cluster_ms": res.cluster_ms,
-            "cells_per_s": 1024 * 1024 / ((res.kernel_ms + res.cluster_ms) * 1e-3),
+            "cells_per_s": nd * nd / ((res.kernel_ms + res.cluster_ms) * 1e-3),
             "rk4_steps_per_s": res.steps / (res.kernel_ms * 1e-3),
             "oscillating_clusters": res.n_clusters, "fixed_point_clusters": -res.min_cluster_idx,
             "classes": {str(k): int((cls == k).sum()) for k in (-1, 0, 1)}}
@@ -486,7 +488,7 @@ def run_other_configs(eng, which=OTHER_CONFIGS, args=None):
         else:
             def rel(a, b):
                 return float(np.median(np.abs(a - b) / np.maximum(np.abs(b), 1e-300)))
-            out["basins_dbscan_duffing_1024"]["fp32_vs_fp64"] = {
+            out[f"basins_dbscan_duffing_{nd}"]["fp32_vs_fp64"] = {
                 "label_agreement": float((lab == ref_bd[0]).mean()),
                 "feature1_median_rel_diff": rel(f1, ref_bd[1]), "feature2_median_rel_diff": rel(f2, ref_bd[2])}
     return out
@@ -541,6 +543,10 @@ def main():
     ap.add_argument("--no-headline", action="store_true",
                     help="time only the --configs selection (no LLE headline, surrogate or e2e)")
     ap.add_argument("--bif2d-n", type=int, default=512, help="grid of the Bif-2D period map configuration")
+    ap.add_argument("--basins-n", type=int, default=4096,
+                    help="grid of the stroboscopic basins configuration (smaller only for profiling)")
+    ap.add_argument("--basins-dbscan-n", type=int, default=1024,
+                    help="grid of the reference-method basins configuration (smaller only for profiling)")
     ap.add_argument("--spectrum-t-end", type=float, default=2e4,
                     help="measured interval of the spectrum configuration (shorter only for profiling)")
     ap.add_argument("--spectrum-max-steps", type=int, default=0,
