@@ -115,3 +115,35 @@ def test_forced_system_compiles_in_every_form():
         ucb.precompile(ucb.Engine.basins_dbscan_request(body, 3, (0, 0, 0), (0.0,), n_pts=4, opt=opt))
         ucb.precompile(ucb.Engine.bif1d_request(body, 3, (0.0, 0.0, 0.0), (0.0,), n_pts=4, sweep_over_var=True,
                                                 var_sweep_index=0, param_lo=-1, param_hi=1, opt=opt))
+
+
+def test_register_cap_reaches_the_compiled_kernel(tmp_path):
+    """A register cap changes the build: the DP5 spectrum kernel (about 250 registers
+    uncapped in FP64) is compiled within a 128-register cap. Checked on the compiler's own
+    report, in a child process with a fresh CUBIN cache."""
+    import re
+    import subprocess
+    import sys
+    from pathlib import Path
+    root = Path(__file__).resolve().parents[1]
+    code = f"""
+import sys
+sys.path.insert(0, {str(root / 'u-cuda_b200')!r}); sys.path.insert(0, {str(root / 'tests')!r})
+import ucb
+from helpers import HYPER_ROSSLER, rk4_body
+cap = int(sys.argv[1])
+ucb.precompile(ucb.Engine.ls2d_request(rk4_body(HYPER_ROSSLER), 4, (-10.0, -6.0, 0.0, 10.0), (0, 0.25, 0.05),
+                                       method=ucb.LS_DP5, t_end=10.0, n_pts=4, param_index=1, param_index_2=2,
+                                       param_lo=0.1, param_hi=0.35, param_lo_2=0.01, param_hi_2=0.1, t_max=10.0,
+                                       opt=ucb.options(precision=ucb.PREC_F64, max_registers=cap)))
+"""
+    used = {}
+    for cap in (0, 128):
+        env = dict(__import__("os").environ, UCB_PTXAS_VERBOSE="1", UCB_CUBIN_CACHE=str(tmp_path / f"c{cap}"))
+        r = subprocess.run([sys.executable, "-c", code, str(cap)], env=env, capture_output=True, text=True,
+                           timeout=600)
+        assert r.returncode == 0, r.stderr[-2000:]
+        regs = [int(m) for m in re.findall(r"Used (\d+) registers", r.stderr)]
+        assert regs, r.stderr[-2000:]
+        used[cap] = max(regs)
+    assert used[0] > 128 and used[128] <= 128
