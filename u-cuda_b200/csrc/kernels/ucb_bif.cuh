@@ -122,11 +122,22 @@ __device__ __forceinline__ void scan_push(PeakScan& s, long long q, numb v, long
 template <class S, class Sink>
 __device__ __forceinline__ int loop_record(const S& st, numb* x, const numb* a, numb h, long long iters, int pre,
                                            int wv, numb maxv, PeakScan& scan, const Sink& sink, long long& ns) {
-    for (long long i = 0; i < iters; ++i) {
-        scan_push(scan, i, recorded_value(x, wv), iters, sink);
-        for (int j = 0; j < pre; ++j) st.step(x, a, h);
+    // Chunks of kCheckInterval samples, the divergence test after the first one's steps
+    // (i % kCheckInterval == 0), so the per-sample loop carries no 64-bit modulo: these
+    // launches run a warp or so per SM, where every instruction of a sample is latency.
+    for (long long i0 = 0; i0 < iters; i0 += kCheckInterval) {
+        scan_push(scan, i0, recorded_value(x, wv), iters, sink);
+        st.step(x, a, h);
+        for (int j = 1; j < pre; ++j) st.step(x, a, h);
         ns += pre;
-        if (i % kCheckInterval == 0 && diverged(x, maxv)) return 0;
+        if (diverged(x, maxv)) return 0;
+        const int n = (iters - i0 < kCheckInterval) ? (int)(iters - i0) : kCheckInterval;
+        for (int c = 1; c < n; ++c) {
+            scan_push(scan, i0 + c, recorded_value(x, wv), iters, sink);
+            st.step(x, a, h);
+            for (int j = 1; j < pre; ++j) st.step(x, a, h);
+        }
+        ns += (long long)pre * (n - 1);
     }
     numb xPrev[UCB_NX];
 #pragma unroll
