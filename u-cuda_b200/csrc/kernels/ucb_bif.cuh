@@ -57,7 +57,13 @@ __device__ __forceinline__ numb recorded_value(const numb* x, int wv) {
         return x[0];
 #endif
     }
-    return x[wv];
+    // a select over the components, not x[wv]: a run-time index would move the state out
+    // of registers into local memory (wv is validated to [0, N) by the host)
+    numb r = x[0];
+#pragma unroll
+    for (int j = 1; j < UCB_NX; ++j)
+        if (wv == j) r = x[j];
+    return r;
 }
 
 // Where the peaks of one point go: the first max_out peaks and intervals of a 1-D
