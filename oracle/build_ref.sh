@@ -1,16 +1,23 @@
 #!/usr/bin/env bash
-# Builds the reference's own text front-end (sysparse.cpp + codegen.cpp, compiled as-is
-# from the read-only reference tree) into oracle/_ref/ref_codegen. Test infrastructure:
-# it only regenerates the golden fixtures in tests/golden/. Needs the reference tree;
-# exits 0 without building when it is absent (machines without the reference tree use the prebuilt files).
+# Builds, from the reference's own sources where they lie (read-only; nothing is copied),
+# into oracle/_ref/:
+#   * ref_codegen: the reference's text front-end (sysparse.cpp + codegen.cpp, compiled
+#     as-is), which regenerates the golden fixtures in tests/golden/;
+#   * refk_*.cubin + refk_manifest.json: the reference's NVRTC integrator kernels,
+#     unchanged (oracle/build_ref_kernels.py), which the GPU parity tests launch through
+#     oracle/_ref/libucb_refharness.so.
+# Test infrastructure. Usage: build_ref.sh <path to the reference's U-CUDA directory>
+# (or UCB_REFERENCE_DIR). Exits 0 without building when no reference tree is given or
+# found: machines without it use the prebuilt files.
 set -euo pipefail
-REF="${UCB_REFERENCE_DIR:-/root/reference/U-CUDA}"
+REF="${1:-${UCB_REFERENCE_DIR:-}}"
 HERE="$(cd "$(dirname "$0")" && pwd)"
-if [ ! -f "$REF/codegen.cpp" ]; then
-  echo "reference tree not found at $REF; skipping oracle/_ref" >&2
+if [ -z "$REF" ] || [ ! -f "$REF/codegen.cpp" ]; then
+  echo "reference tree not given or not found (${REF:-unset}); skipping oracle/_ref" >&2
   exit 0
 fi
 mkdir -p "$HERE/_ref"
 g++ -O2 -std=c++17 -I"$REF" "$HERE/ref_codegen_main.cpp" "$REF/codegen.cpp" "$REF/sysparse.cpp" \
     -o "$HERE/_ref/ref_codegen"
 echo "built $HERE/_ref/ref_codegen"
+python "$HERE/build_ref_kernels.py" "$REF" "$HERE/_ref"

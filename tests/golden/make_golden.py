@@ -2,10 +2,10 @@
 
 Runs oracle/_ref/ref_codegen (built by oracle/build_ref.sh from the reference's
 sysparse.cpp + codegen.cpp, compiled as-is) on each case below and records the parsed
-variables / parameters and the step body of every scheme. Needs the reference tree; the
-committed JSON is what the tests read.
+variables / parameters and the step body of every scheme. Needs the reference tree (its
+U-CUDA directory, for the library presets); the committed JSON is what the tests read.
 
-    python tests/golden/make_golden.py
+    python tests/golden/make_golden.py <reference U-CUDA directory>   (or UCB_REFERENCE_DIR)
 """
 import json
 import subprocess
@@ -14,7 +14,7 @@ from pathlib import Path
 
 ROOT = Path(__file__).resolve().parents[2]
 REF_BIN = ROOT / "oracle" / "_ref" / "ref_codegen"
-LIB = Path("/root/reference/U-CUDA/library_template")
+LIB = None  # <reference U-CUDA directory>/library_template, set by main()
 
 # (name, text, alphabet, order, funcdefs)
 CASES = [
@@ -94,8 +94,14 @@ def run_case(text, alphabet, order, funcs):
 
 
 def main():
+    global LIB
+    import os
+    ref = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("UCB_REFERENCE_DIR", "")
+    if not ref or not (Path(ref) / "library_template").is_dir():
+        sys.exit("usage: make_golden.py <reference U-CUDA directory> (or UCB_REFERENCE_DIR)")
+    LIB = Path(ref) / "library_template"
     if not REF_BIN.exists():
-        sys.exit("oracle/_ref/ref_codegen missing: run oracle/build_ref.sh first")
+        sys.exit("oracle/_ref/ref_codegen missing: run oracle/build_ref.sh <reference U-CUDA directory> first")
     cases = []
     for name, text, alpha, order, funcs in CASES + library_cases():
         r = run_case(text, alpha, order, funcs)
