@@ -9,8 +9,12 @@
  * parametric_engine.cpp:2589-2600 and the *_CHECK macros at :2766-2786):
  *   - nothing throws across the ABI; a failure sets result->ok = 0 and a message in
  *     result->error, and the call returns a non-zero UCB_E* code;
- *   - a set *cancel (polled between launches) ends the call with result->cancelled = 1;
- *   - *progress (if non-NULL) is written with a value in [0, 1];
+ *   - a set *cancel ends the call with result->cancelled = 1 and UCB_E_CANCELLED. It is
+ *     checked before the first launch and, while the map runs, mirrored into the kernels'
+ *     run control: warps take no more cells from the work queue (an adaptive DP5 cell also
+ *     abandons its steps), so the call returns after the cells in flight;
+ *   - *progress (if non-NULL) is written with a value in [0, 1] while the call waits for
+ *     the map (the share of cells handed out by the work queue) and 1 at the end;
  *   - output arrays are allocated by the caller with the sizes documented per call;
  *   - one engine may be driven from one host thread at a time (the reference's
  *     session layer enforces the same, analysis_session.cpp:918-966).
@@ -544,12 +548,16 @@ UCB_API int ucb_autotune_bif2d(ucb_engine* e, const ucb_bif2d_request* req, int3
  *
  * Limits and rules:
  *   - n_pts <= UCB_NOALLOC_MAX_PTS, otherwise UCB_E_INVALID with a message;
- *   - ucb_prepare_lle2d() must have been called for an equivalent request (same body,
- *     sizes, sweep kinds and options) on this engine: it compiles and loads the kernel,
- *     which allocates, and looks up the scratch array's device address; the no-alloc
- *     call returns UCB_E_INVALID otherwise. If only the scratch address is missing for
- *     the device, the first no-alloc call on that device looks it up; make that first
- *     call before any stream capture;
+ *   - ucb_prepare_lle2d() must have been called on this engine for an equivalent request
+ *     (same body, sizes, sweep kinds and options; the swept ranges, step and horizon may
+ *     differ): it compiles and loads the kernel (which allocates), pins that kernel and
+ *     its launch shape on the engine (a later autotune does not change what the
+ *     allocation-free call launches), and looks up the scratch array's device address on
+ *     the engine's device. Without it the call returns UCB_E_INVALID ("not prepared").
+ *     After a cudaDeviceReset() in the process, call ucb_prepare_lle2d() again: it looks
+ *     the address up anew;
+ *   - the axis tables are passed to the device as kernel parameters and the counters are
+ *     cleared with cudaMemsetAsync, all on `stream`, before the kernel;
  *   - all calls share the one array and it keeps the last call's contents; every call
  *     resets the counters it needs, but calls that overlap on the GPU (other streams,
  *     other engines in the process) race on it and must be serialised by the caller. */
@@ -686,6 +694,11 @@ typedef struct ucb_surrogate_request {
     double sigma_max;           /* cap on the std threshold, 0 = none */
     double lle_band;            /* default 0.05; 0 = no band / regime rule */
     double jump;                /* default 0 = off */
+    double min_predictable;     /* gate (default 0.05): the network is trained only when this share
+                                   of the pilot samples (a 32^2..64^2 subgrid of the sample blocks,
+                                   integrated first) is predictable from its neighbours at tol /
+                                   coverage; otherwise every other cell is integrated in
+                                   refine_precision */
     ucb_mlp_config mlp;
 } ucb_surrogate_request;
 
@@ -695,6 +708,9 @@ typedef struct ucb_surrogate_result {
     long long n_samples, n_calib, n_refined, n_predicted, n_diverged;
     double sigma_threshold;     /* calibrated std threshold (-1: nothing predicted) */
     double calib_within_tol;    /* fraction of held-out samples under the threshold within tol */
+    double pilot_predictable;   /* the gate's share of predictable pilot samples */
+    int32_t gated;              /* 1: below min_predictable, no network trained */
+    int32_t pad1;
     double sample_ms, train_ms, predict_ms, select_ms, refine_ms, total_ms;
     float final_loss;
     float pad0;

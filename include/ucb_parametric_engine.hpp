@@ -6,18 +6,21 @@
 // major spectra), same shared_ptr<atomic<...>> cancel / progress tokens. Every call goes
 // through the C ABI in ucb.h (libucb.so): run_bifurcation_1d, run_bifurcation_2d,
 // run_lle_1d, run_ls_1d, run_lle_2d, run_ls_2d, run_basins, run_basins_recluster.
-// Entry points of the reference that are not on this path (DFT, Fast Synchro,
-// continuation sweeps) are not provided.
+// Entry points of the reference that are not on this path: run_dft_1d and run_fastsync
+// are declared and return ok = false with a message; continuation sweeps are rejected by
+// validation (continuation = true is an error).
 //
 // Extension: ParametricEngine::options() selects the arithmetic of the B200 engine
 // (UCB_PREC_F64 plain form by default; UCB_PREC_F32 state form; exact or native step).
 #pragma once
 
 #include <atomic>
+#include <chrono>
 #include <cmath>
 #include <limits>
 #include <memory>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "ucb.h"
@@ -76,6 +79,30 @@ struct LS2DSnapshot {
     int indexOfMutVar = 0, indexOfMutVar2 = 0;
     double range1_lo = 0.0, range1_hi = 0.0, range2_lo = 0.0, range2_hi = 0.0;
     int n_pts = 0, n_exponents = 0;
+};
+// Snapshots of the two analyses this engine does not run (declared for the session layer).
+struct Dft1DSnapshot {
+    std::vector<double> values, initial_conditions;
+    double tMax = 0.0, transientTime = 0.0, h = 0.0;
+    int preScaller = 0, writableVar = 0, indexOfMutVar = 0;
+    double range_lo = 0.0, range_hi = 0.0;
+    int n_freq = 0;
+    double freq_lo = 0.0, freq_hi = 0.0;
+    int window_type = 1;
+};
+struct FastSyncSnapshot {
+    int mode = 0;
+    std::vector<double> values, ic_master, ic_slave, k_forward, k_backward;
+    std::vector<std::string> var_names;
+    double h = 0.0;
+    int iter_of_synchr = 0, preScaller = 0;
+    double window = 0.0;
+    int type_of_synch = 0, error_estim = 0;
+    double fs_error_trs = 0.0;
+    double tMax = 0.0, transientTime = 0.0;
+    int axis_x_var = 0, axis_y_var = 0;
+    double axis_x_lo = 0.0, axis_x_hi = 0.0, axis_y_lo = 0.0, axis_y_hi = 0.0;
+    int n_pts = 0;
 };
 }  // namespace data_export
 
@@ -423,6 +450,131 @@ struct BasinsReclusterResult {
     int min_cluster_idx = 0;
 };
 
+// Requests / results of the reference's DFT sweep and Fast Synchro analyses
+// (parametric_engine.h:140-227, :767-842). They are not on this engine's path; the
+// types and the two entry points exist so that the session layer compiles unchanged,
+// and every call returns ok = false with an error message.
+struct Dft1DRequest {
+    std::string krs_body;
+    int amountOfX = 0;
+    std::vector<double> initial_conditions, base_values;
+    int param_index = 0;
+    bool sweep_over_var = false;
+    int var_sweep_index = 0;
+    bool sweep_over_h = false, log_scale = false, continuation = false, continuation_reverse = false;
+    bool use_cpu = false;
+    double param_lo = 0.0, param_hi = 1.0;
+    int n_pts = 1000;
+    int writable_var = 0;
+    double h = 0.01, transient_time = 0.0, t_max = 0.0;
+    int pre_scaller = 1;
+    double max_value = 1.0e6;
+    int n_freq = 200;
+    double freq_lo = 0.0, freq_hi = 10.0;
+    bool freq_log_scale = false;
+    int window_type = 1;
+    std::string csv_output_path;
+    std::shared_ptr<std::atomic<bool>> cancel;
+    std::shared_ptr<std::atomic<float>> progress;
+};
+
+struct Dft1DResult {
+    bool ok = false;
+    bool cancelled = false;
+    std::string error;
+    bool continuation_reverse = false;
+    double param_lo = 0.0, param_hi = 1.0;
+    int n_pts = 0, n_freq = 0;
+    double freq_lo = 0.0, freq_hi = 0.0;
+    std::vector<double> ak_cos, bk_sin;
+    std::vector<int> flags;
+    data_export::Dft1DSnapshot snapshot;
+};
+
+struct FastSyncRequest {
+    std::string krs_body;
+    int amountOfX = 0;
+    std::vector<double> values;
+    int mode = 0;
+    double h = 0.01;
+    int iter_of_synchr = 100, pre_scaller = 1;
+    double max_value = 1e6;
+    std::vector<double> k_forward, k_backward, ic_master, ic_slave;
+    double t_max = 100.0, transient_time = 0.0;
+    float window = 50.0f;  // the reference's numb (float)
+    int axis_x_var = 0, axis_y_var = 1;
+    double axis_x_lo = -10.0, axis_x_hi = 10.0, axis_y_lo = -10.0, axis_y_hi = 10.0;
+    int n_pts = 200;
+    bool grid_swap_master_slave = false;
+    int type_of_synch = 0, error_estim = 2;
+    double fs_error_trs = 1e-12;
+    std::string csv_output_path;
+    std::vector<std::string> var_names;
+    std::shared_ptr<std::atomic<bool>> cancel;
+    std::shared_ptr<std::atomic<float>> progress;
+};
+
+struct FastSyncResult {
+    bool ok = false;
+    bool cancelled = false;
+    std::string error;
+    int mode = 0;
+    int n_pts_traj = 0, amountOfX_traj = 0;
+    std::vector<double> traj_full, sync_error;
+    int n_pts_grid = 0;
+    double axis_x_lo = 0.0, axis_x_hi = 0.0, axis_y_lo = 0.0, axis_y_hi = 0.0;
+    int axis_x_var = 0, axis_y_var = 1;
+    std::vector<double> heatmap;
+    double min_val = 0.0, max_val = 0.0;
+    data_export::FastSyncSnapshot snapshot;
+};
+
+// The session's cancel / progress tokens (shared_ptr<atomic<...>>, parametric_engine.h)
+// mirrored into the C ABI's words for the duration of one call: a watcher thread copies
+// a raised cancel token into the word the engine polls while the map runs, and the
+// engine's progress into the session's token (the reference updates both between chunks,
+// parametric_engine.cpp:2780-2786). Without tokens no thread is started.
+class TokenBridge {
+public:
+    TokenBridge(const std::shared_ptr<std::atomic<bool>>& cancel, const std::shared_ptr<std::atomic<float>>& progress,
+                const std::shared_ptr<std::atomic<int>>& phase = nullptr)
+        : c_(cancel), p_(progress), ph_(phase) {
+        cancel_ = (c_ && c_->load(std::memory_order_relaxed)) ? 1 : 0;
+        if (c_ || p_ || ph_) th_ = std::thread([this] { watch(); });
+    }
+    ~TokenBridge() { finish(); }
+    TokenBridge(const TokenBridge&) = delete;
+    TokenBridge& operator=(const TokenBridge&) = delete;
+    const volatile int32_t* cancel() const { return &cancel_; }
+    volatile float* progress() { return &prog_; }
+    volatile int32_t* phase() { return &phase_; }
+    // Stops the watcher and stores the final progress / phase in the session's tokens.
+    void finish() {
+        stop_.store(true);
+        if (th_.joinable()) th_.join();
+        if (p_) p_->store(prog_, std::memory_order_relaxed);
+        if (ph_) ph_->store(phase_, std::memory_order_relaxed);
+    }
+
+private:
+    void watch() {
+        while (!stop_.load()) {
+            if (c_ && c_->load(std::memory_order_relaxed)) cancel_ = 1;
+            if (p_) p_->store(prog_, std::memory_order_relaxed);
+            if (ph_) ph_->store(phase_, std::memory_order_relaxed);
+            std::this_thread::sleep_for(std::chrono::milliseconds(2));
+        }
+    }
+    std::shared_ptr<std::atomic<bool>> c_;
+    std::shared_ptr<std::atomic<float>> p_;
+    std::shared_ptr<std::atomic<int>> ph_;
+    volatile int32_t cancel_ = 0;
+    volatile float prog_ = 0.0f;
+    volatile int32_t phase_ = 0;
+    std::atomic<bool> stop_{false};
+    std::thread th_;
+};
+
 class ParametricEngine {
 public:
     ParametricEngine() : e_(ucb_create(0)) { ucb_default_options(&opt_); }
@@ -466,10 +618,9 @@ public:
         q.max_peaks = mp;
         q.csv_output_path = r.csv_output_path.c_str();
         q.opt = opt_;
-        int32_t cancel_now = (r.cancel && r.cancel->load()) ? 1 : 0;
-        q.cancel = &cancel_now;
-        float prog = 0.0f;
-        q.progress = &prog;
+        TokenBridge tokens(r.cancel, r.progress);
+        q.cancel = tokens.cancel();
+        q.progress = tokens.progress();
         const size_t n = r.n_pts > 0 ? (size_t)r.n_pts : 0;
         std::vector<int32_t> counts(n);
         std::vector<double> peaks(n * mp), intervals(n * mp);
@@ -478,7 +629,7 @@ public:
         o.peaks = peaks.data();
         o.intervals = intervals.data();
         ucb_run_bif1d(e_, &q, &o);
-        if (r.progress) r.progress->store(prog);
+        tokens.finish();
         res.ok = o.ok != 0;
         res.cancelled = o.cancelled != 0;
         res.error = o.error;
@@ -512,9 +663,8 @@ public:
     LLE1DResult run_lle_1d(const LLE1DRequest& r) {
         LLE1DResult res;
         if (!check_1d(r, res.error)) return res;
-        int32_t cancel_now = 0;
-        float prog = 0.0f;
-        ucb_lle1d_request q = request_1d(r, &cancel_now, &prog);
+        TokenBridge tokens(r.cancel, r.progress);
+        ucb_lle1d_request q = request_1d(r, tokens);
         const size_t n = r.n_pts > 0 ? (size_t)r.n_pts : 0;
         res.lyapunov.assign(n, 0.0);
         std::vector<int32_t> f32(n);
@@ -522,7 +672,7 @@ public:
         o.values = res.lyapunov.data();
         o.flags = f32.data();
         ucb_run_lle1d(e_, &q, &o);
-        if (r.progress) r.progress->store(prog);
+        tokens.finish();
         res.ok = o.ok != 0;
         res.cancelled = o.cancelled != 0;
         res.error = o.error;
@@ -538,9 +688,8 @@ public:
     LS1DResult run_ls_1d(const LS1DRequest& r) {
         LS1DResult res;
         if (!check_1d(r, res.error)) return res;
-        int32_t cancel_now = 0;
-        float prog = 0.0f;
-        ucb_ls1d_request q = request_1d(r, &cancel_now, &prog);
+        TokenBridge tokens(r.cancel, r.progress);
+        ucb_ls1d_request q = request_1d(r, tokens);
         const size_t n = r.n_pts > 0 ? (size_t)r.n_pts : 0;
         const size_t nx = r.amountOfX > 0 ? (size_t)r.amountOfX : 0;
         std::vector<double> flat(n * nx);
@@ -549,7 +698,7 @@ public:
         o.values = flat.data();
         o.flags = f32.data();
         ucb_run_ls1d(e_, &q, &o);
-        if (r.progress) r.progress->store(prog);
+        tokens.finish();
         res.ok = o.ok != 0;
         res.cancelled = o.cancelled != 0;
         res.error = o.error;
@@ -600,10 +749,9 @@ public:
         q.eps = r.eps;
         q.max_value = r.max_value;
         q.csv_output_path = r.csv_output_path.c_str();
-        int32_t cancel_now = (r.cancel && r.cancel->load()) ? 1 : 0;
-        q.cancel = &cancel_now;
-        float prog = 0.0f;
-        q.progress = &prog;
+        TokenBridge tokens(r.cancel, r.progress);
+        q.cancel = tokens.cancel();
+        q.progress = tokens.progress();
         q.opt = opt_;
         const size_t n = r.n_pts > 0 ? (size_t)r.n_pts * (size_t)r.n_pts : 0;
         res.values.assign(n, 0.0);
@@ -613,7 +761,7 @@ public:
         o.values = res.values.data();
         o.flags = f32.data();
         ucb_run_lle2d(e_, &q, &o);
-        if (r.progress) r.progress->store(prog);
+        tokens.finish();
         res.ok = o.ok != 0;
         res.cancelled = o.cancelled != 0;
         res.error = o.error;
@@ -680,10 +828,9 @@ public:
         q.max_value = r.max_value;
         q.eps_dbscan = r.eps_dbscan;
         q.csv_output_path = r.csv_output_path.c_str();
-        int32_t cancel_now = (r.cancel && r.cancel->load()) ? 1 : 0;
-        q.cancel = &cancel_now;
-        float prog = 0.0f;
-        q.progress = &prog;
+        TokenBridge tokens(r.cancel, r.progress);
+        q.cancel = tokens.cancel();
+        q.progress = tokens.progress();
         q.opt = opt_;
         const size_t cells = r.n_pts > 0 ? (size_t)r.n_pts * (size_t)r.n_pts : 0;
         res.values.assign(cells, 0.0);
@@ -692,7 +839,7 @@ public:
         o.values = res.values.data();
         o.flags = f32.data();
         ucb_run_bif2d(e_, &q, &o);
-        if (r.progress) r.progress->store(prog);
+        tokens.finish();
         res.ok = o.ok != 0;
         res.cancelled = o.cancelled != 0;
         res.error = o.error;
@@ -759,10 +906,9 @@ public:
         q.eps = r.eps;
         q.max_value = r.max_value;
         q.csv_output_path = r.csv_output_path.c_str();
-        int32_t cancel_now = (r.cancel && r.cancel->load()) ? 1 : 0;
-        q.cancel = &cancel_now;
-        float prog = 0.0f;
-        q.progress = &prog;
+        TokenBridge tokens(r.cancel, r.progress);
+        q.cancel = tokens.cancel();
+        q.progress = tokens.progress();
         q.opt = opt_;
         q.method = UCB_LS_FIXED;
         const size_t cells = r.n_pts > 0 ? (size_t)r.n_pts * (size_t)r.n_pts : 0;
@@ -777,7 +923,7 @@ public:
         o.min_val = res.min_val.data();
         o.max_val = res.max_val.data();
         ucb_run_ls2d(e_, &q, &o);
-        if (r.progress) r.progress->store(prog);
+        tokens.finish();
         res.ok = o.ok != 0;
         res.cancelled = o.cancelled != 0;
         res.error = o.error;
@@ -840,12 +986,10 @@ public:
         q.mult1 = r.mult1;
         q.mult2 = r.mult2;
         q.csv_output_path = r.csv_output_path.c_str();
-        int32_t cancel_now = (r.cancel && r.cancel->load()) ? 1 : 0;
-        q.cancel = &cancel_now;
-        float prog = 0.0f;
-        int32_t phase = 0;
-        q.progress = &prog;
-        q.progress_phase = &phase;
+        TokenBridge tokens(r.cancel, r.progress, r.progress_phase);
+        q.cancel = tokens.cancel();
+        q.progress = tokens.progress();
+        q.progress_phase = tokens.phase();
         q.opt = opt_;
         const size_t cells = r.n_pts > 0 ? (size_t)r.n_pts * (size_t)r.n_pts : 0;
         std::vector<int32_t> labels(cells), classes(cells);
@@ -857,8 +1001,7 @@ public:
         o.avg_intervals = res.avg_intervals.data();
         o.classes = classes.data();
         ucb_run_basins_dbscan(e_, &q, &o);
-        if (r.progress) r.progress->store(prog);
-        if (r.progress_phase) r.progress_phase->store(phase);
+        tokens.finish();
         res.ok = o.ok != 0;
         res.cancelled = o.cancelled != 0;
         res.error = o.error;
@@ -905,6 +1048,19 @@ public:
         return res;
     }
 
+    // Not on this engine's path (see Dft1DRequest): ok = false with a message.
+    Dft1DResult run_dft_1d(const Dft1DRequest&) {
+        Dft1DResult res;
+        res.error = "run_dft_1d is not supported by this engine (per-cell integration path only)";
+        return res;
+    }
+    FastSyncResult run_fastsync(const FastSyncRequest& r) {
+        FastSyncResult res;
+        res.mode = r.mode;
+        res.error = "run_fastsync is not supported by this engine (per-cell integration path only)";
+        return res;
+    }
+
     BasinsReclusterResult run_basins_recluster(const BasinsReclusterRequest& r) {
         BasinsReclusterResult res;
         const size_t cells = r.n_pts > 0 ? (size_t)r.n_pts * (size_t)r.n_pts : 0;
@@ -922,15 +1078,14 @@ public:
         q.avg_peaks = r.avg_peaks.data();
         q.avg_intervals = r.avg_intervals.data();
         q.classes = classes.data();
-        int32_t cancel_now = (r.cancel && r.cancel->load()) ? 1 : 0;
-        q.cancel = &cancel_now;
-        float prog = 0.0f;
-        q.progress = &prog;
+        TokenBridge tokens(r.cancel, r.progress);
+        q.cancel = tokens.cancel();
+        q.progress = tokens.progress();
         q.opt = opt_;
         ucb_basins_recluster_result o{};
         o.labels = labels.data();
         ucb_run_basins_recluster(e_, &q, &o);
-        if (r.progress) r.progress->store(prog);
+        tokens.finish();
         res.ok = o.ok != 0;
         res.cancelled = o.cancelled != 0;
         res.error = o.error;
@@ -958,7 +1113,7 @@ private:
     }
 
     template <class Req>
-    ucb_lle1d_request request_1d(const Req& r, int32_t* cancel_now, float* prog) const {
+    ucb_lle1d_request request_1d(const Req& r, TokenBridge& tokens) const {
         ucb_lle1d_request q{};
         q.krs_body = r.krs_body.c_str();
         q.amount_of_x = r.amountOfX;
@@ -980,9 +1135,8 @@ private:
         q.eps = r.eps;
         q.max_value = r.max_value;
         q.csv_output_path = r.csv_output_path.c_str();
-        *cancel_now = (r.cancel && r.cancel->load()) ? 1 : 0;
-        q.cancel = cancel_now;
-        q.progress = prog;
+        q.cancel = tokens.cancel();
+        q.progress = tokens.progress();
         q.opt = opt_;
         return q;
     }

@@ -1,9 +1,12 @@
 // Drives the header-only ParametricEngine shim the way the reference's session layer
 // calls ParametricEngine (analysis_session.cpp builds a Request, calls run_*, reads the
-// Result). argv[1] = "invalid" / "continuation" (no GPU needed) or "lle1d" / "ls1d" / "lle2d" /
-// "ls2d" / "bif1d" / "bif2d" / "basins" (GPU); the RK4 body is read from stdin.
+// Result). argv[1] = "invalid" / "continuation" / "dft" / "fastsync" (no GPU needed) or "lle1d" /
+// "ls1d" / "lle2d" / "ls2d" / "bif1d" / "bif2d" / "basins" / "cancel" (GPU); the RK4 body is
+// read from stdin.
+#include <chrono>
 #include <cstdio>
 #include <cstring>
+#include <thread>
 #include <iostream>
 #include <iterator>
 #include <string>
@@ -14,6 +17,47 @@ int main(int argc, char** argv) {
     const std::string mode = argc > 1 ? argv[1] : "invalid";
     std::string body((std::istreambuf_iterator<char>(std::cin)), std::istreambuf_iterator<char>());
     ParametricEngine eng;
+    if (mode == "dft") {
+        Dft1DRequest r;
+        r.krs_body = body;
+        r.amountOfX = 3;
+        Dft1DResult res = eng.run_dft_1d(r);
+        std::printf("ok=%d error=%s\n", (int)res.ok, res.error.c_str());
+    }
+    if (mode == "fastsync") {
+        FastSyncRequest r;
+        r.krs_body = body;
+        r.mode = 1;
+        FastSyncResult res = eng.run_fastsync(r);
+        std::printf("ok=%d mode=%d error=%s\n", (int)res.ok, res.mode, res.error.c_str());
+    }
+    if (mode == "cancel") {
+        // the session's cancel token raised from another thread 150 ms into a long map
+        LLE2DRequest r;
+        r.krs_body = body;
+        r.amountOfX = 3;
+        r.initial_conditions = {1, 1, 1};
+        r.base_values = {0, 0.2, 0.2, 5.7};
+        r.param_index = 2;
+        r.param_index_2 = 3;
+        r.param_lo = 0.05; r.param_hi = 2.0; r.param_lo_2 = 2.0; r.param_hi_2 = 20.0;
+        r.n_pts = 1024;
+        r.h = 0.01; r.transient_time = 100; r.t_max = 2000; r.NT = 0.1;
+        r.cancel = std::make_shared<std::atomic<bool>>(false);
+        r.progress = std::make_shared<std::atomic<float>>(0.0f);
+        float seen = 0.0f;
+        std::thread raiser([&] {
+            std::this_thread::sleep_for(std::chrono::milliseconds(150));
+            seen = r.progress->load();
+            r.cancel->store(true);
+        });
+        const auto t0 = std::chrono::steady_clock::now();
+        LLE2DResult res = eng.run_lle_2d(r);
+        const double ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+        raiser.join();
+        std::printf("ok=%d cancelled=%d ms=%.0f progress_at_cancel=%.3f error=%s\n", (int)res.ok, (int)res.cancelled,
+                    ms, seen, res.error.c_str());
+    }
     if (mode == "invalid" || mode == "lle2d") {
         LLE2DRequest r;
         r.krs_body = body;

@@ -2,6 +2,7 @@
 (tcgen05 GEMMs, loss, GELU backward) are checked against it; training reduces the loss on
 a known function; the surrogate-refined map is checked against the full plain map."""
 import ctypes as C
+import time
 
 import numpy as np
 import pytest
@@ -168,50 +169,112 @@ def _lorenz_stable_case(n):
                 h=0.01, transient_time=10.0, t_max=2000.0, NT=0.1, eps=1e-4, max_value=1e6)
 
 
+def _full_map(ucb_engine, c, prec):
+    import torch
+    import ucb
+    from helpers import engine_request
+    n = c["n_pts"]
+    v = torch.empty(n * n, dtype=torch.float64, device="cuda")
+    f = torch.empty(n * n, dtype=torch.int32, device="cuda")
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    ucb_engine.lle2d_device(engine_request(ucb, c, precision=prec), v.data_ptr(), f.data_ptr(), 0)
+    torch.cuda.synchronize()
+    ms = (time.perf_counter() - t0) * 1e3
+    return v.cpu().numpy(), f.cpu().numpy(), ms
+
+
+def _surrogate(ucb_engine, c, **kw):
+    import torch
+    import ucb
+    from helpers import engine_request
+    n = c["n_pts"]
+    req = ucb.surrogate_request(engine_request(ucb, c, precision=ucb.PREC_F32), **kw)
+    v = torch.empty(n * n, dtype=torch.float64, device="cuda")
+    f = torch.empty(n * n, dtype=torch.int32, device="cuda")
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    res = ucb_engine.run_lle2d_surrogate(req, v.data_ptr(), f.data_ptr(), 0)
+    torch.cuda.synchronize()
+    ms = (time.perf_counter() - t0) * 1e3
+    return v.cpu().numpy(), f.cpu().numpy(), res, ms
+
+
+LORENZ_NET = dict(batch=1024, train_steps=1500, fourier_scale=1.0, seed=3)
+
+
 @pytest.mark.gpu
 def test_surrogate_map_gain_and_calibrated_error(ucb_engine):
     """What the trained network gains: on a map with smooth regions it vouches for a large
     share of the cells, so only the samples and the rest are integrated, and the cells it
-    predicts are within the calibrated tolerance of the full plain (FP64) map. Training is
-    not bit-reproducible (the split-K weight gradients accumulate with atomics), so the
-    predicted share varies from run to run (0.50-0.73 observed); the bound is below that."""
-    import torch
+    predicts are within the calibrated tolerance (2e-3 on 99.5 % of them) of the full plain
+    (FP64) map. Training is reproducible (split-K partial tiles and per-block sums are added
+    in a fixed order), so a second call gives the same map bit for bit."""
     import ucb
-    from helpers import engine_request
-    n = 128
-    c = _lorenz_stable_case(n)
-    dev = torch.device("cuda")
-
-    def full(prec):
-        v = torch.empty(n * n, dtype=torch.float64, device=dev)
-        f = torch.empty(n * n, dtype=torch.int32, device=dev)
-        ucb_engine.lle2d_device(engine_request(ucb, c, precision=prec), v.data_ptr(), f.data_ptr(), 0)
-        torch.cuda.synchronize()
-        return v.cpu().numpy(), f.cpu().numpy()
-
-    ref64, f64 = full(ucb.PREC_F64)
-    ref32, _ = full(ucb.PREC_F32)
+    c = _lorenz_stable_case(128)
+    ref64, f64, _ = _full_map(ucb_engine, c, ucb.PREC_F64)
+    ref32, _, _ = _full_map(ucb_engine, c, ucb.PREC_F32)
     assert (f64 == 1).all()
-    req = ucb.surrogate_request(engine_request(ucb, c, precision=ucb.PREC_F32), train_pts=32, tol=2e-3,
-                                coverage=0.995, lle_band=0.0,
-                                mlp=dict(batch=1024, train_steps=1500, fourier_scale=1.0, seed=3))
-    v = torch.empty(n * n, dtype=torch.float64, device=dev)
-    f = torch.empty(n * n, dtype=torch.int32, device=dev)
-    res = ucb_engine.run_lle2d_surrogate(req, v.data_ptr(), f.data_ptr(), 0)
-    torch.cuda.synchronize()
-    vals, flags = v.cpu().numpy(), f.cpu().numpy()
-    assert res.n_samples == 32 * 32 and res.n_samples + res.n_refined + res.n_predicted == n * n
+    kw = dict(train_pts=32, tol=2e-3, coverage=0.995, lle_band=0.0, mlp=LORENZ_NET)
+    vals, flags, res, _ = _surrogate(ucb_engine, c, **kw)
+    vals2, flags2, res2, _ = _surrogate(ucb_engine, c, **kw)
+    np.testing.assert_array_equal(flags2, flags)
+    np.testing.assert_array_equal(vals2, vals)
+    assert res.gated == 0 and res.pilot_predictable >= 0.05
+    assert res.n_samples == 32 * 32 and res.n_samples + res.n_refined + res.n_predicted == 128 * 128
     assert set(np.unique(flags)) <= {1, 2}
     pred = flags == 2
     print("predicted", pred.mean(), "threshold", res.sigma_threshold, "calibration", res.calib_within_tol,
-          "train ms", res.train_ms)
-    # the gain: well over a third of the map is not integrated
-    assert pred.mean() >= 0.4, pred.mean()
+          "pilot share", res.pilot_predictable, "train ms", res.train_ms)
+    # the gain: at least half of the map is not integrated
+    assert pred.mean() >= 0.5, pred.mean()
     err = np.abs(vals[pred] - ref64[pred])
-    assert (err <= 2e-3).mean() >= 0.98, ((err <= 2e-3).mean(), err.max())
+    assert (err <= 2e-3).mean() >= 0.995, ((err <= 2e-3).mean(), err.max())
     # integrated cells: samples carry the FP64 value, re-integrated cells the FP32 value
     integ = flags == 1
     is64 = vals[integ] == ref64[integ]
     is32 = vals[integ] == ref32[integ]
     assert (is64 | is32).all()
     assert is64.sum() >= res.n_samples - 1
+
+
+@pytest.mark.gpu
+def test_surrogate_wall_clock_gain_over_the_fp32_map(ucb_engine):
+    """The same smooth map at 1024^2 with t_max = 2000: the surrogate-refined call (samples,
+    training on this GPU, prediction, re-integration of the rest) takes less wall-clock time
+    than integrating the whole map in the FP32 form, and its predicted cells keep the 2e-3
+    tolerance against the FP64 map on 99.5 % of them."""
+    import ucb
+    c = _lorenz_stable_case(1024)
+    ref64, _, _ = _full_map(ucb_engine, c, ucb.PREC_F64)
+    _full_map(ucb_engine, c, ucb.PREC_F32)  # compiled and warm
+    _, _, ms32 = _full_map(ucb_engine, c, ucb.PREC_F32)
+    kw = dict(train_pts=256, tol=2e-3, coverage=0.995, lle_band=0.0, mlp=LORENZ_NET)
+    _surrogate(ucb_engine, c, **kw)  # network buffers and the captured training step exist
+    vals, flags, res, ms = _surrogate(ucb_engine, c, **kw)
+    pred = flags == 2
+    print(f"surrogate {ms:.0f} ms vs FP32 map {ms32:.0f} ms; predicted {pred.mean():.3f}, "
+          f"pilot share {res.pilot_predictable:.3f}, train {res.train_ms:.0f} ms")
+    assert res.gated == 0
+    assert ms < ms32, (ms, ms32)
+    err = np.abs(vals[pred] - ref64[pred])
+    assert (err <= 2e-3).mean() >= 0.995, ((err <= 2e-3).mean(), err.max())
+
+
+@pytest.mark.gpu
+def test_surrogate_gate_skips_training_on_a_chaotic_map(ucb_engine):
+    """On the chaotic Rossler map no smooth predictor can vouch for cells at 2e-3 / 99.5 %:
+    the pilot samples show it before any training, so no network is trained and every other
+    cell is integrated in the FP32 form (the call costs the FP32 map plus the pilot)."""
+    import ucb
+    from helpers import lle2d_case
+    c = lle2d_case(n=256, t_max=200.0, transient=50.0)
+    ref64, _, _ = _full_map(ucb_engine, c, ucb.PREC_F64)
+    ref32, _, _ = _full_map(ucb_engine, c, ucb.PREC_F32)
+    vals, flags, res, _ = _surrogate(ucb_engine, c, train_pts=64, tol=2e-3, coverage=0.995, lle_band=0.05)
+    assert res.gated == 1 and res.pilot_predictable < 0.05
+    assert res.n_predicted == 0 and res.train_ms < 1.0
+    assert not (flags == 2).any()
+    pilots = vals == ref64
+    assert pilots.sum() >= res.n_samples - 1
+    np.testing.assert_array_equal(vals[~pilots], ref32[~pilots])

@@ -31,6 +31,24 @@ def test_shim_reports_validation_error(driver):
     assert out.startswith("ok=0 error=n_pts must be > 0")
 
 
+def test_shim_dft_and_fastsync_are_declared_and_not_supported(driver):
+    # the session layer calls run_dft_1d / run_fastsync (analysis_session.cpp); the shim
+    # declares them with the reference's types and answers ok=false with a message
+    assert run(driver, "dft", rk4_body(LORENZ)).startswith("ok=0 error=run_dft_1d is not supported")
+    assert run(driver, "fastsync", rk4_body(LORENZ)).startswith("ok=0 mode=1 error=run_fastsync is not supported")
+
+
+@pytest.mark.gpu
+def test_shim_cancel_token_stops_a_running_map(driver):
+    # 1024^2 Rossler map with t_max = 2000 (about 1.1 s in FP64); the session's cancel token
+    # is raised 150 ms in and the call must come back cancelled well before the map's time
+    out = run(driver, "cancel", rk4_body(ROSSLER))
+    kv = dict(p.split("=", 1) for p in out.split(" ")[:4])
+    assert kv["ok"] == "0" and kv["cancelled"] == "1", out
+    assert float(kv["ms"]) < 700, out
+    assert 0.0 < float(kv["progress_at_cancel"]) < 1.0, out
+
+
 def test_shim_rejects_continuation(driver):
     out = run(driver, "continuation", rk4_body(LORENZ))
     assert out.startswith("ok=0 error=continuation sweeps are not supported")

@@ -655,10 +655,16 @@ extern "C" int ucb_run_basins_dbscan(ucb_engine* e, const ucb_basins_dbscan_requ
     pk.put<void*>(ws);
     pk.put<void*>(ws + 8);
     EventPair cev;
+    begin_run(e);
     cudaEventRecord(e->ev0, st);
     if (!launch_packed(e, fn, persistent_grid(e, fn, shape.block, total), shape.block, st, pk, err))
         return fail(e, res, UCB_E_CUDA, err);
     cudaEventRecord(e->ev1, st);
+    {
+        const int wr = wait_run(e, e->ev1, q.cancel, q.progress, total, err);
+        if (wr == UCB_E_CANCELLED) res->cancelled = 1;
+        if (wr != UCB_OK) return fail(e, res, wr, err);
+    }
 
     // 2. clustering of the features
     if (q.cancel && *q.cancel) {

@@ -27,6 +27,14 @@ struct TuneConfig {
 };
 }  // namespace ucb
 
+// Host view of the run-control block the kernels poll (kernels/ucb_device.cuh UcbControl):
+// page-locked host memory mapped into the device's address space.
+struct ucb_run_control {
+    volatile int32_t cancel;
+    int32_t pad;
+    volatile unsigned long long fetched;
+};
+
 struct ucb_engine {
     int device = 0;
     bool initialized = false;
@@ -49,6 +57,12 @@ struct ucb_engine {
     // Network of the last surrogate-refined map, kept for reuse by the next call with the
     // same configuration (owned; released with the engine).
     std::shared_ptr<void> surrogate_net;
+    // LLE kernels pinned by ucb_prepare_lle2d for ucb_lle2d_device_noalloc: module, kernel
+    // and launch shape as resolved at prepare time, by kernel-build key (an autotune after
+    // the prepare does not change what the allocation-free call launches).
+    std::map<std::string, std::shared_ptr<void>> pinned_lle;
+    // Run control of the host-buffer entry points (null when mapped memory is unavailable).
+    ucb_run_control* control = nullptr;
 };
 
 namespace ucb {
@@ -178,13 +192,33 @@ ucb_lle2d_request as_lle2d(const ucb_lle1d_request& q);
 // Launch helper: persistent grid size for a kernel.
 int persistent_grid(ucb_engine* e, CUfunction f, int block, long long work_items);
 
+// Run control of the host-buffer entry points (ucb_run_*). begin_run resets the queue
+// position before a launch. wait_run waits for `done` (an event recorded after the run's
+// main kernel); while it waits it mirrors the caller's *cancel into the control block (the
+// kernels' warps then take no more cells and an adaptive cell abandons its steps) and
+// writes the queue position / work_items to *progress. Without cancel and progress words
+// it simply synchronises. Returns UCB_OK, UCB_E_CANCELLED (the control block is clear
+// again once the kernel has ended) or UCB_E_CUDA.
+void begin_run(ucb_engine* e);
+int wait_run(ucb_engine* e, cudaEvent_t done, const volatile int32_t* cancel, volatile float* progress,
+             long long work_items, std::string& err);
+
 // LLE-2D launch pieces for entry points outside ucb_engine.cpp. plan / launch are opaque
 // (released with lle2d_release); load_if_missing = false only looks up an already loaded
 // module (no allocation).
 int lle2d_plan_and_find(ucb_engine* e, const ucb_lle2d_request& q, bool load_if_missing, std::string& err,
                         void** plan_out, void** launch_out);
+// Allocation-free launch pieces (noalloc.cu). lle2d_pin compiles / loads the kernel of a
+// request and pins it on the engine (allocates); lle2d_find_pinned looks the pinned kernel
+// up again (no allocation; UCB_E_INVALID "not prepared" when absent).
+int lle2d_pin(ucb_engine* e, const ucb_lle2d_request& q, std::string& err);
+int lle2d_find_pinned(ucb_engine* e, const ucb_lle2d_request& q, std::string& err, void** plan_out,
+                      void** launch_out);
+// Copies `bytes` (a multiple of 4) from host memory to device memory in stream order.
+typedef int (*TableUpload)(void* dst, const void* src, size_t bytes, cudaStream_t stream, std::string& err);
 int lle2d_enqueue_with_scratch(ucb_engine* e, const ucb_lle2d_request& q, void* plan, void* launch, double* d_values,
-                               int32_t* d_flags, cudaStream_t stream, char* scratch, std::string& err);
+                               int32_t* d_flags, cudaStream_t stream, char* scratch, std::string& err,
+                               TableUpload upload = nullptr);
 // Cells d_cells[0..n_cells) of the grid; compact: entry i is stored at d_values[i],
 // otherwise at the cell's map position.
 int lle2d_enqueue_cells(ucb_engine* e, const ucb_lle2d_request& q, void* plan, void* launch, const long long* d_cells,

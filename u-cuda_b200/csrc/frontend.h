@@ -110,10 +110,15 @@ PNode simplify(const PNode& e);
 // arguments, pow with a small integer exponent as the multiplications it expands to.
 int flops(const PNode& e);
 int rhs_flops(const Rhs& r);
-// One RK4 step of the native integrator: 4 right-hand sides + 14 N updates
-// (3 stage updates of 2 N, the final combination of 8 N).
-int rk4_step_flops(const Rhs& r);
-int rk4_tangent_step_flops(const Rhs& r);
+// One RK4 step of the native integrator: 4 right-hand sides + 12 N updates per
+// component (3 stage FMAs of 2, the combination (k1 + k4) + 2 (k2 + k3) of 4, the final
+// FMA of 2). With trig_phase >= 0, the sin / cos calls of that forcing phase are not
+// counted: the native kernels take them from a table or rotate one sincos per step.
+int rk4_step_flops(const Rhs& r, int trig_phase = -1);
+// The same for the state and its tangent vector v' = J(x) v: 4 (F_rhs + F_jvp) + 24 N.
+int rk4_tangent_step_flops(const Rhs& r, int trig_phase = -1);
+// sin / cos calls of variable p in one right-hand-side evaluation.
+int trig_phase_calls(const Rhs& r, int p);
 
 }  // namespace fe
 }  // namespace ucb

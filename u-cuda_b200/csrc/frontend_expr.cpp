@@ -801,12 +801,32 @@ int rhs_flops(const Rhs& r) {
     return s;
 }
 
-int rk4_step_flops(const Rhs& r) { return 4 * rhs_flops(r) + 14 * r.nx; }
+static int trig_calls_of(const PNode& n, int p) {
+    if (!n) return 0;
+    int c = (n->kind == Node::Call && n->args.size() == 1 && n->args[0]->kind == Node::Var &&
+             n->args[0]->index == p && (n->name == "cos" || n->name == "sin"))
+                ? 1
+                : 0;
+    c += trig_calls_of(n->a, p) + trig_calls_of(n->b, p);
+    for (const auto& a : n->args) c += trig_calls_of(a, p);
+    return c;
+}
 
-int rk4_tangent_step_flops(const Rhs& r) {
+int trig_phase_calls(const Rhs& r, int p) {
+    int c = 0;
+    for (auto& f : r.f) c += trig_calls_of(f, p);
+    return c;
+}
+
+int rk4_step_flops(const Rhs& r, int trig_phase) {
+    const int trig = trig_phase >= 0 ? trig_phase_calls(r, trig_phase) : 0;
+    return 4 * (rhs_flops(r) - trig) + 12 * r.nx;
+}
+
+int rk4_tangent_step_flops(const Rhs& r, int trig_phase) {
     int j = 0;
     for (auto& f : r.f) j += flops(directional_derivative(f));
-    return 4 * (rhs_flops(r) + j) + 28 * r.nx;
+    return rk4_step_flops(r, trig_phase) + 4 * j + 12 * r.nx;
 }
 
 }  // namespace fe

@@ -48,6 +48,8 @@ Driver& driver() {
         UCB_LOAD(cuCtxSetCurrent, "cuCtxSetCurrent", "cuCtxSetCurrent");
         UCB_LOAD(cuOccupancyMaxActiveBlocksPerMultiprocessor, "cuOccupancyMaxActiveBlocksPerMultiprocessor",
                  "cuOccupancyMaxActiveBlocksPerMultiprocessor");
+        UCB_LOAD(cuModuleGetGlobal, "cuModuleGetGlobal_v2", "cuModuleGetGlobal");
+        UCB_LOAD(cuMemcpyHtoD, "cuMemcpyHtoD_v2", "cuMemcpyHtoD");
 #undef UCB_LOAD
         if (!d.cuInit || !d.cuModuleLoadDataEx || !d.cuModuleGetFunction || !d.cuLaunchKernel ||
             !d.cuModuleUnload || !d.cuGetErrorString) {
@@ -223,6 +225,17 @@ std::shared_ptr<Module> ModuleCache::get(const CompileRequest& rq, std::string& 
         }
         m->functions[k] = f;
         if (d.cuFuncGetAttribute) d.cuFuncGetAttribute(&m->registers, CU_FUNC_ATTRIBUTE_NUM_REGS, f);
+    }
+    if (control_ && d.cuModuleGetGlobal && d.cuMemcpyHtoD) {
+        CUdeviceptr g = 0;
+        size_t gsz = 0;
+        if (d.cuModuleGetGlobal(&g, &gsz, m->module, "ucb_control") == CUDA_SUCCESS && gsz == sizeof(void*)) {
+            r = d.cuMemcpyHtoD(g, &control_, sizeof(void*));
+            if (r != CUDA_SUCCESS) {
+                err = "binding the run-control block: " + cu_error_string(r);
+                return nullptr;
+            }
+        }
     }
     std::lock_guard<std::mutex> lk(mu_);
     cache_[key] = m;

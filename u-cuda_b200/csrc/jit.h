@@ -38,6 +38,8 @@ struct Driver {
     CUresult (*cuCtxGetCurrent)(CUcontext*) = nullptr;
     CUresult (*cuCtxSetCurrent)(CUcontext) = nullptr;
     CUresult (*cuOccupancyMaxActiveBlocksPerMultiprocessor)(int*, CUfunction, int, size_t) = nullptr;
+    CUresult (*cuModuleGetGlobal)(CUdeviceptr*, size_t*, CUmodule, const char*) = nullptr;
+    CUresult (*cuMemcpyHtoD)(CUdeviceptr, const void*, size_t) = nullptr;
 };
 
 Driver& driver();
@@ -70,6 +72,9 @@ bool precompile_to_disk(const CompileRequest& rq, std::string& err);
 // Thread-safe cache of loaded modules (needs a current CUDA context to load).
 class ModuleCache {
 public:
+    // Device address of the owner's run-control block (ucb_device.cuh UcbControl); every
+    // module loaded afterwards that defines the global `ucb_control` gets it.
+    void set_control(void* device_ptr) { control_ = device_ptr; }
     std::shared_ptr<Module> get(const CompileRequest& rq, std::string& err);
     // Already-loaded module for this request, or nullptr (never compiles or loads).
     std::shared_ptr<Module> find(const CompileRequest& rq) const;
@@ -79,6 +84,7 @@ public:
 private:
     mutable std::mutex mu_;
     std::map<uint64_t, std::shared_ptr<Module>> cache_;
+    void* control_ = nullptr;
 };
 
 uint64_t fnv1a64(const std::string& s, uint64_t h = 1469598103934665603ULL);

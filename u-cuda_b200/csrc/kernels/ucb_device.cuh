@@ -487,12 +487,45 @@ __device__ __forceinline__ void warp_add_steps(unsigned long long* counter, long
     if (lane == 0 && counter) atomicAdd(counter, v);
 }
 
-// Work distribution: one warp takes 32 consecutive cells per atomic fetch from a
+// Run control shared with the host: a block of page-locked host memory mapped into the
+// device's address space, one per engine, whose address the engine writes into this
+// module's `ucb_control` after loading it (null: no control). The host sets `cancel`
+// while it waits for a run whose caller cancelled it; `fetched` receives the queue
+// position of the latest fetch (the host reads it as progress).
+struct UcbControl {
+    int cancel;
+    int pad;
+    unsigned long long fetched;
+};
+
+}  // namespace ucbdev
+
+extern "C" __device__ ucbdev::UcbControl* ucb_control = nullptr;
+
+namespace ucbdev {
+
+// True once the host asked the running call to stop (a warp then takes no more work).
+__device__ __forceinline__ bool run_cancelled() {
+    const UcbControl* c = ucb_control;
+    return c && *(const volatile int*)&c->cancel != 0;
+}
+
+// Work distribution: one warp takes `batch` consecutive cells per atomic fetch from a
 // device counter, so cells of uneven cost (divergence, early exit) balance across a
-// persistent grid. The counter is zeroed by the host before each launch.
-__device__ __forceinline__ long long warp_fetch(unsigned long long* counter, int lane) {
+// persistent grid. The counter is zeroed by the host before each launch. A cancelled
+// run hands out no more work (the returned position is past every grid).
+__device__ __forceinline__ long long warp_fetch(unsigned long long* counter, int lane,
+                                                unsigned long long batch = 32ULL) {
     unsigned long long base = 0;
-    if (lane == 0) base = atomicAdd(counter, 32ULL);
+    if (lane == 0) {
+        UcbControl* c = ucb_control;
+        if (c && *(volatile int*)&c->cancel) {
+            base = 0x7fffffffffffffffULL;
+        } else {
+            base = atomicAdd(counter, batch);
+            if (c) *(volatile unsigned long long*)&c->fetched = base + batch;
+        }
+    }
     base = __shfl_sync(0xffffffffu, base, 0);
     return (long long)base;
 }

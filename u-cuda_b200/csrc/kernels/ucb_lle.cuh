@@ -326,9 +326,7 @@ extern "C" __global__ void UCB_LAUNCH_BOUNDS ucb_lle_kernel(const UcbLleParams p
     // 64 cells per warp fetch: lane l takes cells base + l and base + 32 + l (both halves
     // of a warp's stores stay coalesced)
     for (;;) {
-        unsigned long long b = 0;
-        if (lane == 0) b = atomicAdd(p.counter, 64ULL);
-        const long long base = (long long)__shfl_sync(0xffffffffu, b, 0);
+        const long long base = ucbdev::warp_fetch(p.counter, lane, 64ULL);
         if (base >= p.total) break;
         const long long i0 = base + lane, i1 = base + 32 + lane;
         if (i0 < p.total) {

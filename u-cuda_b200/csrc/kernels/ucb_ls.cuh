@@ -462,6 +462,8 @@ __device__ __forceinline__ void ls_cell_dp5(const UcbLsParams& p, long long kidx
     ucb_rhs(S.X[0], a, S.k1);
     while (ok && t < t_stop) {
         if (++attempts > p.max_steps) { ok = false; break; }
+        // a cell can take millions of attempts: a cancelled run abandons it
+        if ((attempts & 4095) == 0 && run_cancelled()) { ok = false; break; }
         const double t_target = measuring ? t_stop : (double)p.transient;
         bool last = false;
         if (t + h >= t_target) { h = t_target - t; last = true; }

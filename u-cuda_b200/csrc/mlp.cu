@@ -9,8 +9,10 @@
 // 128-column TMEM accumulator and commits to the buffer's mbarrier (waits are bounded;
 // on a timeout the kernel records an error, drains and frees TMEM). The epilogue reads
 // TMEM with tcgen05.ld (32 data-path lanes x 32 bit: thread t owns row t) and applies
-// bias / GELU, storing FP32, BF16 and / or transposed BF16 copies; split-K launches add
-// their partial tiles atomically. Backward products are the same TN GEMM on transposed
+// bias / GELU, storing FP32, BF16 and / or transposed BF16 copies; a split-K launch stores
+// each split's partial tile in its own slice of a buffer, and a second kernel adds the
+// slices in split order (so a training step gives the same bits every time it runs).
+// Backward products are the same TN GEMM on transposed
 // copies, which the forward epilogue and the GELU-backward kernel write as they go.
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
@@ -72,7 +74,8 @@ struct Epilogue {
     int gelu;           // outh / outt receive GELU(v) instead of v
     float* outf;        // FP32 result (pre-activation), row stride ldf
     int ldf;
-    int atomic;         // outf += v (split-K partial tiles)
+    int atomic;         // split-K: the host redirects outf to a partial-tile buffer
+    long long split_stride;  // floats between the slices of consecutive splits (blockIdx.z)
     bf16* outh;         // BF16 copy, row stride ldh
     int ldh;
     bf16* outt;         // BF16 transposed copy outt[n * ldt + m]
@@ -239,6 +242,7 @@ __global__ void __launch_bounds__(128) gemm_tn_kernel(const bf16* __restrict__ A
         const int row = warp * 32 + lane;
         const uint32_t taddr = ss.tmem_base + ((uint32_t)(warp * 32) << 16);
         float* stage = ss.stage;
+        float* const outf = ep.outf ? ep.outf + (size_t)blockIdx.z * ep.split_stride : nullptr;
 #pragma unroll 1
         for (int c0 = 0; c0 < kBN; c0 += 32) {
             uint32_t r[32];
@@ -270,10 +274,10 @@ __global__ void __launch_bounds__(128) gemm_tn_kernel(const bf16* __restrict__ A
             }
         }
         __syncwarp();
-        if (ep.outf || ep.outh) {
+        if (outf || ep.outh) {
             // vector path: whole 128-column rows, 16-byte FP32 / 8-byte BF16 stores
             const bool full = n0 + kBN <= ep.n_store;
-            const bool vf = !ep.outf || ((ep.ldf & 3) == 0 && (reinterpret_cast<uintptr_t>(ep.outf) & 15) == 0);
+            const bool vf = !outf || ((ep.ldf & 3) == 0 && (reinterpret_cast<uintptr_t>(outf) & 15) == 0);
             const bool vh = !ep.outh || ((ep.ldh & 3) == 0 && (reinterpret_cast<uintptr_t>(ep.outh) & 7) == 0);
             const int c = lane * 4;
             // staged values carry the bias already when the transposed copy was written
@@ -293,17 +297,7 @@ __global__ void __launch_bounds__(128) gemm_tn_kernel(const bf16* __restrict__ A
                 q.w += b[3];
                 const float x[4] = {q.x, q.y, q.z, q.w};
                 if (full && vf && vh) {
-                    if (ep.outf) {
-                        float* p = ep.outf + (size_t)m * ep.ldf + n0 + c;
-                        if (ep.atomic) {
-                            atomicAdd(p, x[0]);
-                            atomicAdd(p + 1, x[1]);
-                            atomicAdd(p + 2, x[2]);
-                            atomicAdd(p + 3, x[3]);
-                        } else {
-                            *reinterpret_cast<float4*>(p) = q;
-                        }
-                    }
+                    if (outf) *reinterpret_cast<float4*>(outf + (size_t)m * ep.ldf + n0 + c) = q;
                     if (ep.outh) {
                         float y[4];
 #pragma unroll
@@ -320,11 +314,7 @@ __global__ void __launch_bounds__(128) gemm_tn_kernel(const bf16* __restrict__ A
                     for (int j = 0; j < 4; ++j) {
                         const int n = n0 + c + j;
                         if (n >= ep.n_store) continue;
-                        if (ep.outf) {
-                            float* p = ep.outf + (size_t)m * ep.ldf + n;
-                            if (ep.atomic) atomicAdd(p, x[j]);
-                            else *p = x[j];
-                        }
+                        if (outf) outf[(size_t)m * ep.ldf + n] = x[j];
                         if (ep.outh) ep.outh[(size_t)m * ep.ldh + n] = bf16(ep.gelu ? gelu(x[j]) : x[j]);
                     }
                 }
@@ -412,9 +402,11 @@ __global__ void features_kernel(FeatureArgs a) {
 
 // Gaussian NLL of the standardised target with beta weighting. out: rows x 2 (mean,
 // log-variance). Writes dOut (rows x 64, columns >= 2 stay zero), dOut^T rows 0 and 1
-// (128 x rows, other rows stay zero), the output-layer bias gradient and the mean loss.
+// (128 x rows, other rows stay zero), and per block the sums of the two output-layer bias
+// gradients and of the loss into blk[3 blockIdx.x + 0..2] (added in block order by
+// ordered_sum_kernel).
 __global__ void nll_kernel(const float* out, const float* yb, int rows, int n_valid, float beta, bf16* dout,
-                           bf16* doutT, float* db, float* loss) {
+                           bf16* doutT, float* blk) {
     const int r = blockIdx.x * blockDim.x + threadIdx.x;
     float g0 = 0.f, g1 = 0.f, l = 0.f;
     if (r < rows && r < n_valid) {
@@ -450,15 +442,27 @@ __global__ void nll_kernel(const float* out, const float* yb, int rows, int n_va
         __syncthreads();
     }
     if (threadIdx.x == 0) {
-        atomicAdd(&db[0], s0[0]);
-        atomicAdd(&db[1], s1[0]);
-        atomicAdd(loss, sl[0]);
+        blk[3 * blockIdx.x] = s0[0];
+        blk[3 * blockIdx.x + 1] = s1[0];
+        blk[3 * blockIdx.x + 2] = sl[0];
     }
 }
 
-// dZ = dH * GELU'(Z) -> BF16 dZ (rows x N) and dZ^T (N x rows); db[c] += sum_r dZ[r, c]
-// (of the BF16-rounded values the GEMMs use). Block 32 x 8 over a 32 x 32 tile.
-__global__ void gelu_back_kernel(const float* dH, const float* Z, int rows, int N, bf16* dZ, bf16* dZt, float* db) {
+// out[j] = sum over i = 0 .. count - 1, in that order, of part[i * stride + j] (j < width):
+// the fixed-order reduction of partial sums (split-K tiles, per-block bias gradients).
+__global__ void ordered_sum_kernel(const float* part, int count, long long stride, long long width, float* out) {
+    for (long long j = (long long)blockIdx.x * blockDim.x + threadIdx.x; j < width;
+         j += (long long)gridDim.x * blockDim.x) {
+        float s = 0.f;
+        for (int i = 0; i < count; ++i) s += part[(size_t)i * stride + j];
+        out[j] = s;
+    }
+}
+
+// dZ = dH * GELU'(Z) -> BF16 dZ (rows x N) and dZ^T (N x rows); dbp[blockIdx.y * N + c] =
+// the sum over this block's 32 rows of dZ[r, c] (of the BF16-rounded values the GEMMs
+// use), added in block order by ordered_sum_kernel. Block 32 x 8 over a 32 x 32 tile.
+__global__ void gelu_back_kernel(const float* dH, const float* Z, int rows, int N, bf16* dZ, bf16* dZt, float* dbp) {
     __shared__ float tile[32][33];
     const int c0 = blockIdx.x * 32, r0 = blockIdx.y * 32;
     const int tx = threadIdx.x, ty = threadIdx.y;
@@ -480,7 +484,7 @@ __global__ void gelu_back_kernel(const float* dH, const float* Z, int rows, int 
     if (ty == 0 && c0 + tx < N) {
         float s = 0.f;
         for (int k = 0; k < 32; ++k) s += tile[k][tx];
-        atomicAdd(&db[c0 + tx], s);
+        dbp[(size_t)blockIdx.y * N + c0 + tx] = s;
     }
 }
 
@@ -558,6 +562,8 @@ using ucbmlp::bf16;
 
 namespace {
 
+constexpr int kMaxSplits = 64;  // split-K slices per weight-gradient tile
+
 bool cu_ok(cudaError_t e, std::string& err, const char* what) {
     if (e == cudaSuccess) return true;
     err = std::string(what) + ": " + cudaGetErrorString(e);
@@ -601,6 +607,12 @@ struct Mlp {
     float* yb = nullptr;
     bf16 *dout = nullptr, *doutT = nullptr, *dZ = nullptr, *dZt = nullptr;
     float* dH = nullptr;
+    // partial sums reduced in a fixed order: split-K weight-gradient tiles, per-block NLL /
+    // bias-gradient sums
+    float* part = nullptr;
+    long long part_floats = 0;
+    float* blk = nullptr;
+    float* dbp = nullptr;
     // prediction buffers (ping-pong activations, no backward copies)
     std::vector<void*> pred_owned;
     int pred_rows = 0;
@@ -640,9 +652,20 @@ bool set_gemm_attributes(int device, std::string& err) {
     return true;
 }
 
-// C = A B^T (+ epilogue); split-K when the epilogue accumulates atomically.
-bool gemm(Mlp& m, const bf16* A, const bf16* B, int M, int N, int K, const ucbmlp::Epilogue& ep, cudaStream_t st,
+bool ordered_sum(Mlp& m, const float* part, int count, long long stride, long long width, float* out,
+                 cudaStream_t st, std::string& err) {
+    const unsigned blocks = (unsigned)std::min<long long>((width + 255) / 256, 1024);
+    ucbmlp::ordered_sum_kernel<<<blocks, 256, 0, st>>>(part, count, stride, width, out);
+    m.e->launches += 1;
+    return cu_ok(cudaPeekAtLastError(), err, "ordered_sum launch");
+}
+
+// C = A B^T (+ epilogue). ep.atomic: split K over up to kMaxSplits CTAs per tile; each
+// split writes its partial tile into m.part and ordered_sum adds them in split order into
+// ep.outf (rows < m_store, columns < n_store; other entries of ep.outf are left alone).
+bool gemm(Mlp& m, const bf16* A, const bf16* B, int M, int N, int K, const ucbmlp::Epilogue& ep_in, cudaStream_t st,
           std::string& err) {
+    ucbmlp::Epilogue ep = ep_in;
     if (M <= 0 || N <= 0 || K <= 0 || M % ucbmlp::kBM || N % ucbmlp::kBN || K % ucbmlp::kBK) {
         err = "gemm: unsupported shape " + std::to_string(M) + "x" + std::to_string(N) + "x" + std::to_string(K);
         return false;
@@ -651,14 +674,31 @@ bool gemm(Mlp& m, const bf16* A, const bf16* B, int M, int N, int K, const ucbml
     const int kt = K / ucbmlp::kBK;
     int per = kt;
     if (ep.atomic) {
-        const int want = std::max(1, std::min(kt, (2 * std::max(m.e->sm_count, 1) + tiles - 1) / tiles));
+        const int want =
+            std::max(1, std::min({kt, kMaxSplits, (2 * std::max(m.e->sm_count, 1) + tiles - 1) / tiles}));
         per = (kt + want - 1) / want;
     }
     const int splits = (kt + per - 1) / per;
+    const long long m_eff = std::min(M, ep.m_store), n_eff = std::min(N, ep.n_store);
+    float* const out = ep.outf;
+    if (ep.atomic) {
+        if (ep.ldf < n_eff || (long long)splits * m_eff * ep.ldf > m.part_floats) {
+            err = "gemm: split-K partial buffer too small";
+            return false;
+        }
+        ep.outf = m.part;
+        ep.split_stride = m_eff * ep.ldf;
+    }
     dim3 grid(M / ucbmlp::kBM, N / ucbmlp::kBN, splits);
     ucbmlp::gemm_tn_kernel<<<grid, 128, gemm_smem_bytes(), st>>>(A, B, M, N, K, per, ep, m.err);
     m.e->launches += 1;
-    return cu_ok(cudaPeekAtLastError(), err, "gemm launch");
+    if (!cu_ok(cudaPeekAtLastError(), err, "gemm launch")) return false;
+    if (!ep.atomic) return true;
+    if (n_eff == ep.ldf) return ordered_sum(m, m.part, splits, ep.split_stride, m_eff * ep.ldf, out, st, err);
+    for (long long r = 0; r < m_eff; ++r)  // rows with a gap beyond n_eff: one reduction per row
+        if (!ordered_sum(m, m.part + r * ep.ldf, splits, ep.split_stride, n_eff, out + r * ep.ldf, st, err))
+            return false;
+    return true;
 }
 
 ucbmlp::Epilogue epi() {
@@ -697,6 +737,11 @@ bool ensure_rows(Mlp& m, int rows, std::string& err) {
         !(m.dout = dalloc<bf16>(R * 64, o, err, "dOut")) || !(m.doutT = dalloc<bf16>(R * 128, o, err, "dOut^T")) ||
         !(m.dZ = dalloc<bf16>(R * m.H, o, err, "dZ")) || !(m.dZt = dalloc<bf16>(R * m.H, o, err, "dZ^T")) ||
         !(m.dH = dalloc<float>(R * m.H, o, err, "dH")))
+        return false;
+    m.part_floats = (long long)kMaxSplits * m.H * std::max(m.H, m.F);
+    if (!(m.part = dalloc<float>((size_t)m.part_floats, o, err, "split-K partials")) ||
+        !(m.blk = dalloc<float>((R + 255) / 256 * 3, o, err, "NLL block sums")) ||
+        !(m.dbp = dalloc<float>((R + 31) / 32 * m.H, o, err, "bias-gradient partials")))
         return false;
     m.rows = rows;
     return true;
@@ -821,10 +866,13 @@ bool backward(Mlp& m, int rows, int n_valid, cudaStream_t st, std::string& err) 
     if (!cu_ok(cudaMemsetAsync(m.g, 0, sizeof(float) * m.n_params, st), err, "memset grad") ||
         !cu_ok(cudaMemsetAsync(m.loss, 0, sizeof(float), st), err, "memset loss"))
         return false;
-    ucbmlp::nll_kernel<<<(rows + 255) / 256, 256, 0, st>>>(m.outp, m.yb, rows, n_valid, m.cfg.beta_nll, m.dout,
-                                                          m.doutT, m.g + m.b_off[m.L], m.loss);
+    const int nblk = (rows + 255) / 256;
+    ucbmlp::nll_kernel<<<nblk, 256, 0, st>>>(m.outp, m.yb, rows, n_valid, m.cfg.beta_nll, m.dout, m.doutT, m.blk);
     m.e->launches += 1;
-    if (!cu_ok(cudaPeekAtLastError(), err, "nll launch")) return false;
+    if (!cu_ok(cudaPeekAtLastError(), err, "nll launch") ||
+        !ordered_sum(m, m.blk, nblk, 3, 2, m.g + m.b_off[m.L], st, err) ||
+        !ordered_sum(m, m.blk + 2, nblk, 3, 1, m.loss, st, err))
+        return false;
     const int Lo = m.L;
     // output layer: dH = dOut W (K padded to 64), dW = dOut^T H (M padded to 128)
     {
@@ -841,10 +889,11 @@ bool backward(Mlp& m, int rows, int n_valid, cudaStream_t st, std::string& err) 
     }
     for (int l = Lo - 1; l >= 0; --l) {
         dim3 gb((m.H + 31) / 32, (rows + 31) / 32);
-        ucbmlp::gelu_back_kernel<<<gb, dim3(32, 8), 0, st>>>(m.dH, m.Z[l], rows, m.H, m.dZ, m.dZt,
-                                                             m.g + m.b_off[l]);
+        ucbmlp::gelu_back_kernel<<<gb, dim3(32, 8), 0, st>>>(m.dH, m.Z[l], rows, m.H, m.dZ, m.dZt, m.dbp);
         m.e->launches += 1;
-        if (!cu_ok(cudaPeekAtLastError(), err, "gelu_back launch")) return false;
+        if (!cu_ok(cudaPeekAtLastError(), err, "gelu_back launch") ||
+            !ordered_sum(m, m.dbp, (int)gb.y, m.H, m.H, m.g + m.b_off[l], st, err))
+            return false;
         const bf16* prevT = l > 0 ? m.Ht[l - 1] : m.Xt;
         const int in = m.in[l];
         ucbmlp::Epilogue eg = epi();

@@ -156,6 +156,88 @@ struct LaunchHandle {
     }
 };
 
+// Pilot samples: every pilot_stride(tp)-th block of the tp x tp sample partition along both
+// axes: a 32 x 32 .. 64 x 64 pilot grid (all samples when tp <= 32).
+int pilot_stride(int tp) { return std::max(1, std::min(4, tp / 32)); }
+
+// The predictability gate, computed from the pilot samples alone before any training.
+// v / f: the pilot samples' integrated values and flags on their tq x tq block grid
+// (row-major), cells: their map cells (kernel order, iy * n + ix). Each pilot sample with
+// a full 5 x 5 pilot neighbourhood is predicted by the least-squares plane through its 24
+// neighbours (at their cell positions) evaluated at its own cell: the prediction of a
+// smooth predictor that averages out the per-cell probe term, as the network does. It is a
+// candidate when all 25 are valid, lie in one regime and the prediction is at least `band`
+// from zero (the selection rules select_kernel applies to the network's predictions).
+// Ordered by the plane's RMS residual, the longest prefix of candidates of which
+// >= coverage lie within tol of the integrated value (and at least 32) is the share of the
+// pilot such a predictor could vouch for at the requested coverage. Returns that share of
+// all pilot samples.
+double pilot_share(const std::vector<double>& v, const std::vector<int>& f, const std::vector<long long>& cells,
+                   int n, int tq, double tol, double coverage, double band) {
+    struct Cand {
+        double spread;
+        bool good;
+    };
+    std::vector<Cand> cand;
+    auto regime = [&](double x) { return band > 0 ? (x > band ? 1 : (x < -band ? -1 : 0)) : 0; };
+    constexpr int R = 2;
+    for (int qy = R; qy + R < tq; ++qy)
+        for (int qx = R; qx + R < tq; ++qx) {
+            const int c = qy * tq + qx;
+            if (f[c] != 1 || !std::isfinite(v[c])) continue;
+            const double cx = (double)(cells[c] % n), cy = (double)(cells[c] / n);
+            // normal equations of v ~ p0 + p1 (x - cx) + p2 (y - cy) over the neighbours
+            double S[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}}, b[3] = {0, 0, 0};
+            bool ok = true;
+            for (int dy = -R; dy <= R && ok; ++dy)
+                for (int dx = -R; dx <= R && ok; ++dx) {
+                    if (!dx && !dy) continue;
+                    const int k = (qy + dy) * tq + qx + dx;
+                    ok = f[k] == 1 && std::isfinite(v[k]) && regime(v[k]) == regime(v[c]);
+                    const double a[3] = {1.0, (double)(cells[k] % n) - cx, (double)(cells[k] / n) - cy};
+                    for (int i = 0; i < 3; ++i) {
+                        b[i] += a[i] * v[k];
+                        for (int j = 0; j < 3; ++j) S[i][j] += a[i] * a[j];
+                    }
+                }
+            if (!ok) continue;
+            // 3 x 3 solve by Cramer's rule
+            auto det3 = [](const double M[3][3]) {
+                return M[0][0] * (M[1][1] * M[2][2] - M[1][2] * M[2][1]) -
+                       M[0][1] * (M[1][0] * M[2][2] - M[1][2] * M[2][0]) +
+                       M[0][2] * (M[1][0] * M[2][1] - M[1][1] * M[2][0]);
+            };
+            const double d = det3(S);
+            if (!(std::fabs(d) > 0)) continue;
+            double p[3];
+            for (int col = 0; col < 3; ++col) {
+                double M[3][3];
+                for (int i = 0; i < 3; ++i)
+                    for (int j = 0; j < 3; ++j) M[i][j] = j == col ? b[i] : S[i][j];
+                p[col] = det3(M) / d;
+            }
+            double rss = 0;
+            for (int dy = -R; dy <= R; ++dy)
+                for (int dx = -R; dx <= R; ++dx) {
+                    if (!dx && !dy) continue;
+                    const int k = (qy + dy) * tq + qx + dx;
+                    const double r = v[k] - (p[0] + p[1] * ((double)(cells[k] % n) - cx) +
+                                             p[2] * ((double)(cells[k] / n) - cy));
+                    rss += r * r;
+                }
+            if (band > 0 && std::fabs(p[0]) < band) continue;
+            cand.push_back({std::sqrt(rss / 24.0), std::fabs(p[0] - v[c]) <= tol});
+        }
+    std::sort(cand.begin(), cand.end(), [](const Cand& a, const Cand& b) { return a.spread < b.spread; });
+    long long good = 0, best = 0;
+    for (size_t k = 0; k < cand.size(); ++k) {
+        good += cand[k].good;
+        const long long cnt = (long long)k + 1;
+        if (cnt >= 32 && (double)good >= coverage * (double)cnt) best = cnt;
+    }
+    return v.empty() ? 0.0 : (double)best / (double)v.size();
+}
+
 }  // namespace
 }  // namespace ucb
 
@@ -175,6 +257,7 @@ void ucb_default_surrogate_request(ucb_surrogate_request* r) {
     r->sigma_max = 0.0;
     r->lle_band = 0.05;
     r->jump = 0.0;
+    r->min_predictable = 0.05;
     ucb_mlp_default_config(&r->mlp);
 }
 
@@ -198,8 +281,9 @@ int ucb_run_lle2d_surrogate(ucb_engine* e, const ucb_surrogate_request* rq, doub
     if (!prec_ok(r.sample_precision) || !prec_ok(r.refine_precision))
         return fail(UCB_E_INVALID, "sample_precision / refine_precision must be UCB_PREC_F64 or UCB_PREC_F32");
     if (!(r.sigma_max >= 0) || !(r.lle_band >= 0) || !(r.jump >= 0) || !(r.tol > 0) ||
-        !(r.coverage > 0 && r.coverage <= 1))
-        return fail(UCB_E_INVALID, "need tol > 0, 0 < coverage <= 1, sigma_max / lle_band / jump >= 0");
+        !(r.coverage > 0 && r.coverage <= 1) || !(r.min_predictable >= 0))
+        return fail(UCB_E_INVALID,
+                    "need tol > 0, 0 < coverage <= 1, sigma_max / lle_band / jump / min_predictable >= 0");
     std::string err;
     if (!ensure_init(e, err)) return fail(UCB_E_NOGPU, err);
     cudaStream_t st = stream ? (cudaStream_t)stream : e->stream;
@@ -241,22 +325,83 @@ int ucb_run_lle2d_surrogate(ucb_engine* e, const ucb_surrogate_request* rq, doub
     cudaMemsetAsync(d_mask, 0, total, st);
     cudaMemsetAsync(d_count, 0, 2 * sizeof(unsigned long long), st);
 
-    // 1. samples
+    // 1. samples: one random cell per block of the tp x tp partition. The pilot subset
+    // (every pilot_stride-th block along both axes) is integrated first and decides whether
+    // a network is worth training (pilot_share); the other samples are integrated only then.
     cudaEventRecord(ev[0], st);
     ucbsur::sample_cells_kernel<<<(unsigned)((ns + 255) / 256), 256, 0, st>>>(n, tp, r.mlp.seed ^ 0xC0FFEEULL,
                                                                              d_cells);
     e->launches += 1;
-    rc = lle2d_enqueue_cells(e, qs, hs.plan, hs.launch, d_cells, ns, true, d_sv, d_sf, st, err);
-    if (rc != UCB_OK) return fail(rc, err);
-    cudaEventRecord(ev[1], st);
     std::vector<long long> hc(ns);
+    if (cudaMemcpyAsync(hc.data(), d_cells, ns * 8, cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+        cudaStreamSynchronize(st) != cudaSuccess)
+        return fail(UCB_E_CUDA, std::string("sample cells: ") + cudaGetErrorString(cudaGetLastError()));
+    const int ps = pilot_stride(tp);
+    const int tq = (tp + ps - 1) / ps;
+    std::vector<char> is_pilot(ns, 0);
+    std::vector<long long> pilot_idx, rest_idx;
+    for (int qy = 0; qy < tq; ++qy)
+        for (int qx = 0; qx < tq; ++qx) {
+            const long long i = (long long)(qy * ps) * tp + qx * ps;
+            pilot_idx.push_back(i);
+            is_pilot[i] = 1;
+        }
+    for (long long i = 0; i < ns; ++i)
+        if (!is_pilot[i]) rest_idx.push_back(i);
+    const long long np = (long long)pilot_idx.size(), nr = (long long)rest_idx.size();
+    auto integrate = [&](const std::vector<long long>& idx, long long*& d_c, double*& d_v, int*& d_f,
+                         std::vector<double>& v, std::vector<int>& f) -> int {
+        const long long m = (long long)idx.size();
+        std::vector<long long> cells(m);
+        for (long long k = 0; k < m; ++k) cells[k] = hc[idx[k]];
+        d_c = mem.alloc<long long>(m, err, "sample cells");
+        d_v = mem.alloc<double>(m, err, "sample values");
+        d_f = mem.alloc<int>(m, err, "sample flags");
+        if (!d_c || !d_v || !d_f) return UCB_E_CUDA;
+        v.resize(m);
+        f.resize(m);
+        if (m == 0) return UCB_OK;
+        cudaMemcpyAsync(d_c, cells.data(), m * 8, cudaMemcpyHostToDevice, st);
+        const int q = lle2d_enqueue_cells(e, qs, hs.plan, hs.launch, d_c, m, true, d_v, d_f, st, err);
+        if (q != UCB_OK) return q;
+        if (cudaMemcpyAsync(v.data(), d_v, m * 8, cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+            cudaMemcpyAsync(f.data(), d_f, m * 4, cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+            cudaStreamSynchronize(st) != cudaSuccess) {
+            err = std::string("samples: ") + cudaGetErrorString(cudaGetLastError());
+            return UCB_E_CUDA;
+        }
+        return UCB_OK;
+    };
+    long long *d_pc = nullptr, *d_rc = nullptr;
+    double *d_pv = nullptr, *d_rv = nullptr;
+    int *d_pf = nullptr, *d_rf = nullptr;
+    std::vector<double> pv, rv;
+    std::vector<int> pf, rf;
+    rc = integrate(pilot_idx, d_pc, d_pv, d_pf, pv, pf);
+    if (rc != UCB_OK) return fail(rc, err);
+    {
+        std::vector<long long> pcells(np);
+        for (long long k = 0; k < np; ++k) pcells[k] = hc[pilot_idx[k]];
+        res->pilot_predictable = pilot_share(pv, pf, pcells, n, tq, r.tol, r.coverage, r.lle_band);
+    }
+    res->gated = res->pilot_predictable < r.min_predictable ? 1 : 0;
     std::vector<double> hv(ns);
     std::vector<int> hf(ns);
-    if (cudaMemcpyAsync(hc.data(), d_cells, ns * 8, cudaMemcpyDeviceToHost, st) != cudaSuccess ||
-        cudaMemcpyAsync(hv.data(), d_sv, ns * 8, cudaMemcpyDeviceToHost, st) != cudaSuccess ||
-        cudaMemcpyAsync(hf.data(), d_sf, ns * 4, cudaMemcpyDeviceToHost, st) != cudaSuccess ||
-        cudaStreamSynchronize(st) != cudaSuccess)
-        return fail(UCB_E_CUDA, std::string("samples: ") + cudaGetErrorString(cudaGetLastError()));
+    if (!res->gated) {
+        rc = integrate(rest_idx, d_rc, d_rv, d_rf, rv, rf);
+        if (rc != UCB_OK) return fail(rc, err);
+        for (long long k = 0; k < np; ++k) {
+            hv[pilot_idx[k]] = pv[k];
+            hf[pilot_idx[k]] = pf[k];
+        }
+        for (long long k = 0; k < nr; ++k) {
+            hv[rest_idx[k]] = rv[k];
+            hf[rest_idx[k]] = rf[k];
+        }
+        cudaMemcpyAsync(d_sv, hv.data(), ns * 8, cudaMemcpyHostToDevice, st);
+        cudaMemcpyAsync(d_sf, hf.data(), ns * 4, cudaMemcpyHostToDevice, st);
+    }
+    cudaEventRecord(ev[1], st);
     // One sample in eight (by a hash of its block) is held out for calibration.
     std::vector<float> hu, hy;
     std::vector<long long> cal_cells;
@@ -264,7 +409,7 @@ int ucb_run_lle2d_surrogate(ucb_engine* e, const ucb_surrogate_request* rq, doub
     hu.reserve(2 * ns);
     hy.reserve(ns);
     const float inv = 1.0f / (float)(n - 1);
-    for (long long i = 0; i < ns; ++i) {
+    for (long long i = 0; i < ns && !res->gated; ++i) {
         if (hf[i] != 1 || !std::isfinite(hv[i])) continue;
         unsigned long long z = (unsigned long long)i * 0x9E3779B97F4A7C15ULL + r.mlp.seed;
         z ^= z >> 31;
@@ -279,7 +424,7 @@ int ucb_run_lle2d_surrogate(ucb_engine* e, const ucb_surrogate_request* rq, doub
     }
     const long long n_train = (long long)hy.size();
     const long long n_cal = (long long)cal_y.size();
-    res->n_samples = ns;
+    res->n_samples = res->gated ? np : ns;
     res->n_calib = n_cal;
 
     // 2. training (the engine keeps the network's buffers between calls with the same
@@ -356,8 +501,12 @@ int ucb_run_lle2d_surrogate(ucb_engine* e, const ucb_surrogate_request* rq, doub
     cudaEventRecord(ev[3], st);
 
     // 4. selection
-    ucbsur::scatter_samples_kernel<<<(unsigned)((ns + 255) / 256), 256, 0, st>>>(
-        d_cells, ns, d_sv, d_sf, n, map.swap_xy ? 1 : 0, d_mask, d_values, d_flags);
+    if (res->gated)  // only the pilot samples were integrated: everything else is
+        ucbsur::scatter_samples_kernel<<<(unsigned)((np + 255) / 256), 256, 0, st>>>(
+            d_pc, np, d_pv, d_pf, n, map.swap_xy ? 1 : 0, d_mask, d_values, d_flags);
+    else
+        ucbsur::scatter_samples_kernel<<<(unsigned)((ns + 255) / 256), 256, 0, st>>>(
+            d_cells, ns, d_sv, d_sf, n, map.swap_xy ? 1 : 0, d_mask, d_values, d_flags);
     const float sigma = (float)thr;  // < 0 (no network or no calibrated threshold): refine all
     ucbsur::select_kernel<<<(unsigned)((total + 255) / 256), 256, 0, st>>>(
         d_mean, d_sd, d_mask, n, map.swap_xy ? 1 : 0, sigma, (float)r.lle_band, (float)r.jump, d_list, d_count,
@@ -387,7 +536,7 @@ int ucb_run_lle2d_surrogate(ucb_engine* e, const ucb_surrogate_request* rq, doub
     res->select_ms = ms[3];
     res->refine_ms = ms[4];
     res->n_refined = (long long)n_ref;
-    res->n_predicted = total - ns - (long long)n_ref;  // sample cells are integrated
+    res->n_predicted = total - res->n_samples - (long long)n_ref;  // sample cells are integrated
     res->n_diverged = (long long)n_div;
     res->n_pts = n;
     res->total_ms =

@@ -190,8 +190,14 @@ extern "C" int ucb_run_basins(ucb_engine* e, const ucb_basins_request* req, ucb_
     pk.put<void*>(ws + 8);
     pk.put<const void*>(use_trig ? (const void*)(ws + off_trig) : nullptr);
     const int block = shape.block;
+    begin_run(e);
     cudaEventRecord(e->ev0, st);
     int rc = launch_packed(e, fn, persistent_grid(e, fn, block, total), block, st, pk, err) ? UCB_OK : UCB_E_CUDA;
+    if (rc == UCB_OK) {
+        cudaEventRecord(e->ev1, st);
+        rc = wait_run(e, e->ev1, q.cancel, q.progress, total, err);
+        if (rc == UCB_E_CANCELLED) res->cancelled = 1;
+    }
     // attractor table -> host: merge, order, map
     std::vector<unsigned long long> keys(kTableSlots);
     std::vector<double> pts(2 * kTableSlots);

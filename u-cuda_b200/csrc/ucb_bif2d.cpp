@@ -226,9 +226,12 @@ extern "C" int ucb_run_bif2d(ucb_engine* e, const ucb_bif2d_request* req, ucb_bi
     pk.put<void*>(d_flags);
     pk.put<void*>(ws);
     pk.put<void*>(ws + 8);
+    begin_run(e);
     cudaEventRecord(e->ev0, e->stream);
     if (!launch_packed(e, fn, grid, block, e->stream, pk, err)) rc = UCB_E_CUDA;
     cudaEventRecord(e->ev1, e->stream);
+    if (rc == UCB_OK) rc = wait_run(e, e->ev1, q.cancel, q.progress, total, err);
+    if (rc == UCB_E_CANCELLED) res->cancelled = 1;
     unsigned long long steps = 0;
     if (rc == UCB_OK) {
         if ((ce = cudaMemcpyAsync(res->values, d_values, (size_t)total * 8, cudaMemcpyDeviceToHost, e->stream)) !=

@@ -16,6 +16,8 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <chrono>
+#include <thread>
 #include <fstream>
 #include <iomanip>
 #include <limits>
@@ -78,8 +80,68 @@ bool ensure_init(ucb_engine* e, std::string& err) {
         err = std::string("stream/event creation: ") + cudaGetErrorString(ce);
         return false;
     }
+    {
+        // run control: cancel word and queue position shared with the kernels
+        void* h = nullptr;
+        void* dptr = nullptr;
+        if (cudaHostAlloc(&h, sizeof(ucb_run_control), cudaHostAllocMapped) == cudaSuccess &&
+            cudaHostGetDevicePointer(&dptr, h, 0) == cudaSuccess) {
+            std::memset(h, 0, sizeof(ucb_run_control));
+            e->control = static_cast<ucb_run_control*>(h);
+            e->modules.set_control(dptr);
+        } else {
+            if (h) cudaFreeHost(h);
+            cudaGetLastError();
+        }
+    }
     e->initialized = true;
     return true;
+}
+
+void begin_run(ucb_engine* e) {
+    if (e->control) e->control->fetched = 0;
+}
+
+int wait_run(ucb_engine* e, cudaEvent_t done, const volatile int32_t* cancel, volatile float* progress,
+             long long work_items, std::string& err) {
+    ucb_run_control* c = e->control;
+    cudaError_t ce;
+    if (!c || (!cancel && !progress)) {
+        if ((ce = cudaEventSynchronize(done)) != cudaSuccess) {
+            err = std::string("CUDA: ") + cudaGetErrorString(ce);
+            return UCB_E_CUDA;
+        }
+        return UCB_OK;
+    }
+    bool cancelled = false;
+    const auto t0 = std::chrono::steady_clock::now();
+    for (;;) {
+        ce = cudaEventQuery(done);
+        if (ce == cudaSuccess) break;
+        if (ce != cudaErrorNotReady) {
+            err = std::string("CUDA: ") + cudaGetErrorString(ce);
+            if (cancelled) c->cancel = 0;
+            return UCB_E_CUDA;
+        }
+        if (cancel && *cancel && !cancelled) {
+            c->cancel = 1;
+            cancelled = true;
+        }
+        if (progress && work_items > 0) {
+            const double f = (double)c->fetched / (double)work_items;
+            *progress = (float)std::min(f, 0.999);
+        }
+        if (std::chrono::steady_clock::now() - t0 < std::chrono::milliseconds(2))
+            std::this_thread::yield();
+        else
+            std::this_thread::sleep_for(std::chrono::microseconds(200));
+    }
+    if (cancelled) {
+        c->cancel = 0;
+        err = "Cancelled by user";
+        return UCB_E_CANCELLED;
+    }
+    return UCB_OK;
 }
 
 bool ensure_workspace(ucb_engine* e, size_t bytes, std::string& err) {
@@ -202,6 +264,7 @@ SystemCode make_system_code(const std::string& krs_body, int nx, int nv, int pre
                 s.clock_rate = rate;
             }
             if (fe::find_trig_phase(r, p, rate)) {
+                s.flops_step = s.has_jvp ? fe::rk4_tangent_step_flops(r, p) / 2 : fe::rk4_step_flops(r, p);
                 s.code += fe::emit_rhs_trig_device(r, p, precision == UCB_PREC_F32);
                 char rbuf[64];
                 std::snprintf(rbuf, sizeof rbuf, "%.17g", rate);
@@ -470,7 +533,7 @@ bool prepare_lle(ucb_engine* e, const ucb_lle2d_request& q, const LlePlan& plan,
 int enqueue_lle_fn(ucb_engine* e, const ucb_lle2d_request& q, const LlePlan& plan, const LleLaunch& L,
                    double* d_values, int32_t* d_flags, cudaStream_t stream, std::string& err, long long skip_override,
                    bool persistent, char* scratch, const long long* d_cell_list = nullptr, long long n_list = 0,
-                   bool list_compact = false) {
+                   bool list_compact = false, TableUpload upload = nullptr) {
     const int n = q.n_pts;
     const int prec = q.opt.precision;
     const size_t esz = prec == UCB_PREC_F64 ? 8 : 4;
@@ -488,9 +551,17 @@ int enqueue_lle_fn(ucb_engine* e, const ucb_lle2d_request& q, const LlePlan& pla
     const void* h0 = prec == UCB_PREC_F64 ? (const void*)t0d.data() : (const void*)t0f.data();
     const void* h1 = prec == UCB_PREC_F64 ? (const void*)t1d.data() : (const void*)t1f.data();
     cudaError_t ce;
-    if ((ce = cudaMemcpyAsync(ws + off_ax0, h0, tab_bytes, cudaMemcpyHostToDevice, stream)) != cudaSuccess ||
-        (ce = cudaMemcpyAsync(ws + off_ax1, h1, tab_bytes, cudaMemcpyHostToDevice, stream)) != cudaSuccess ||
-        (ce = cudaMemsetAsync(ws, 0, 16, stream)) != cudaSuccess) {
+    if (upload) {
+        if (upload(ws + off_ax0, h0, tab_bytes, stream, err) != UCB_OK ||
+            upload(ws + off_ax1, h1, tab_bytes, stream, err) != UCB_OK)
+            return UCB_E_CUDA;
+        if ((ce = cudaMemsetAsync(ws, 0, 16, stream)) != cudaSuccess) {
+            err = std::string("CUDA upload: ") + cudaGetErrorString(ce);
+            return UCB_E_CUDA;
+        }
+    } else if ((ce = cudaMemcpyAsync(ws + off_ax0, h0, tab_bytes, cudaMemcpyHostToDevice, stream)) != cudaSuccess ||
+               (ce = cudaMemcpyAsync(ws + off_ax1, h1, tab_bytes, cudaMemcpyHostToDevice, stream)) != cudaSuccess ||
+               (ce = cudaMemsetAsync(ws, 0, 16, stream)) != cudaSuccess) {
         err = std::string("CUDA upload: ") + cudaGetErrorString(ce);
         return UCB_E_CUDA;
     }
@@ -655,10 +726,48 @@ int lle2d_plan_and_find(ucb_engine* e, const ucb_lle2d_request& q, bool load_if_
     return UCB_OK;
 }
 
+int lle2d_pin(ucb_engine* e, const ucb_lle2d_request& q, std::string& err) {
+    LlePlan plan;
+    if (!plan_lle2d(q, plan, err)) return UCB_E_INVALID;
+    if (!ensure_init(e, err)) return UCB_E_NOGPU;
+    auto L = std::make_shared<LleLaunch>();
+    CompileRequest rq = lle_compile_request(q, plan, *L);
+    const std::string key = tune_key(rq);
+    if (!tune_request(e, q.opt, 128, rq, L->shape, err)) return UCB_E_INVALID;
+    L->mod = e->modules.get(rq, err);
+    if (!L->mod) return UCB_E_COMPILE;
+    L->fn = L->mod->functions["ucb_lle_kernel"];
+    e->pinned_lle[key] = L;
+    return UCB_OK;
+}
+
+int lle2d_find_pinned(ucb_engine* e, const ucb_lle2d_request& q, std::string& err, void** plan_out,
+                      void** launch_out) {
+    auto plan = std::make_unique<LlePlan>();
+    if (!plan_lle2d(q, *plan, err)) return UCB_E_INVALID;
+    if (!e->initialized) {
+        err = "engine not prepared: call ucb_prepare_lle2d first";
+        return UCB_E_INVALID;
+    }
+    cudaSetDevice(e->device);
+    LleLaunch probe;
+    const std::string key = tune_key(lle_compile_request(q, *plan, probe));
+    auto it = e->pinned_lle.find(key);
+    if (it == e->pinned_lle.end()) {
+        err = "kernel not prepared for this request: call ucb_prepare_lle2d first (loading a module allocates "
+              "device memory)";
+        return UCB_E_INVALID;
+    }
+    *launch_out = new LleLaunch(*static_cast<LleLaunch*>(it->second.get()));
+    *plan_out = plan.release();
+    return UCB_OK;
+}
+
 int lle2d_enqueue_with_scratch(ucb_engine* e, const ucb_lle2d_request& q, void* plan, void* launch, double* d_values,
-                               int32_t* d_flags, cudaStream_t stream, char* scratch, std::string& err) {
+                               int32_t* d_flags, cudaStream_t stream, char* scratch, std::string& err,
+                               TableUpload upload) {
     return enqueue_lle_fn(e, q, *static_cast<LlePlan*>(plan), *static_cast<LleLaunch*>(launch), d_values, d_flags,
-                          stream, err, -1, true, scratch);
+                          stream, err, -1, true, scratch, nullptr, 0, false, upload);
 }
 
 int lle2d_enqueue_cells(ucb_engine* e, const ucb_lle2d_request& q, void* plan, void* launch, const long long* d_cells,
@@ -709,6 +818,8 @@ void ucb_destroy(ucb_engine* e) {
         if (e->ev1) cudaEventDestroy(e->ev1);
         if (e->stream) cudaStreamDestroy(e->stream);
         if (e->pool) cudaMemPoolDestroy(e->pool);
+        e->pinned_lle.clear();
+        if (e->control) cudaFreeHost(e->control);
     }
     delete e;
 }
@@ -762,9 +873,12 @@ int ucb_run_lle2d(ucb_engine* e, const ucb_lle2d_request* req, ucb_lle2d_result*
     if ((ce = dev_alloc(e, (void**)&d_values, total * sizeof(double), e->stream)) != cudaSuccess ||
         (ce = dev_alloc(e, (void**)&d_flags, total * sizeof(int32_t), e->stream)) != cudaSuccess)
         return fail(e, res->error, &res->ok, UCB_E_CUDA, std::string("cudaMallocAsync: ") + cudaGetErrorString(ce));
+    begin_run(e);
     cudaEventRecord(e->ev0, e->stream);
     int rc = enqueue_lle(e, q, plan, L, d_values, d_flags, e->stream, err);
     cudaEventRecord(e->ev1, e->stream);
+    if (rc == UCB_OK) rc = wait_run(e, e->ev1, q.cancel, q.progress, (long long)total, err);
+    if (rc == UCB_E_CANCELLED) res->cancelled = 1;
     if (rc == UCB_OK) {
         unsigned long long steps = 0;
         if ((ce = cudaMemcpyAsync(res->values, d_values, total * sizeof(double), cudaMemcpyDeviceToHost, e->stream)) != cudaSuccess ||
@@ -847,9 +961,12 @@ int ucb_run_lle1d(ucb_engine* e, const ucb_lle1d_request* req, ucb_lle1d_result*
     if ((ce = dev_alloc(e, (void**)&d_values, (size_t)n * sizeof(double), e->stream)) != cudaSuccess ||
         (ce = dev_alloc(e, (void**)&d_flags, (size_t)n * sizeof(int32_t), e->stream)) != cudaSuccess)
         return fail(e, res->error, &res->ok, UCB_E_CUDA, std::string("cudaMallocAsync: ") + cudaGetErrorString(ce));
+    begin_run(e);
     cudaEventRecord(e->ev0, e->stream);
     int rc = enqueue_lle(e, q, plan, L, d_values, d_flags, e->stream, err);
     cudaEventRecord(e->ev1, e->stream);
+    if (rc == UCB_OK) rc = wait_run(e, e->ev1, q1.cancel, q1.progress, (long long)n, err);
+    if (rc == UCB_E_CANCELLED) res->cancelled = 1;
     unsigned long long steps = 0;
     if (rc == UCB_OK) {
         if ((ce = cudaMemcpyAsync(res->values, d_values, (size_t)n * sizeof(double), cudaMemcpyDeviceToHost,

@@ -189,9 +189,12 @@ int ls_run(ucb_engine* e, const ucb_ls2d_request& q, const SweepMap& m, int n_bl
     pk.put<void*>(d_cell_steps);
     const int block = shape.block;
     const int grid = persistent_grid(e, fn, block, total);
+    begin_run(e);
     cudaEventRecord(e->ev0, e->stream);
     int rc = launch_packed(e, fn, grid, block, e->stream, pk, err) ? UCB_OK : UCB_E_CUDA;
     cudaEventRecord(e->ev1, e->stream);
+    if (rc == UCB_OK) rc = wait_run(e, e->ev1, q.cancel, q.progress, total, err);
+    if (rc == UCB_E_CANCELLED) res->cancelled = 1;
     unsigned long long steps = 0;
     if (rc == UCB_OK) {
         if ((ce = cudaMemcpyAsync(res->values, d_values, (size_t)total * nx * 8, cudaMemcpyDeviceToHost, e->stream)) !=

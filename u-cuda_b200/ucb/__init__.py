@@ -253,13 +253,15 @@ class MlpConfig(C.Structure):
 class SurrogateRequest(C.Structure):
     _fields_ = [("map", Lle2dRequest), ("train_pts", C.c_int32), ("sample_precision", C.c_int32),
                 ("refine_precision", C.c_int32), ("pad0", C.c_int32), ("tol", C.c_double), ("coverage", C.c_double),
-                ("sigma_max", C.c_double), ("lle_band", C.c_double), ("jump", C.c_double), ("mlp", MlpConfig)]
+                ("sigma_max", C.c_double), ("lle_band", C.c_double), ("jump", C.c_double),
+                ("min_predictable", C.c_double), ("mlp", MlpConfig)]
 
 
 class SurrogateResult(C.Structure):
     _fields_ = [("ok", C.c_int32), ("n_pts", C.c_int32), ("n_samples", C.c_longlong), ("n_calib", C.c_longlong),
                 ("n_refined", C.c_longlong), ("n_predicted", C.c_longlong), ("n_diverged", C.c_longlong),
-                ("sigma_threshold", C.c_double), ("calib_within_tol", C.c_double), ("sample_ms", C.c_double),
+                ("sigma_threshold", C.c_double), ("calib_within_tol", C.c_double),
+                ("pilot_predictable", C.c_double), ("gated", C.c_int32), ("pad1", C.c_int32), ("sample_ms", C.c_double),
                 ("train_ms", C.c_double), ("predict_ms", C.c_double), ("select_ms", C.c_double),
                 ("refine_ms", C.c_double), ("total_ms", C.c_double), ("final_loss", C.c_float),
                 ("pad0", C.c_float), ("error", C.c_char * 1024)]
