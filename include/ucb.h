@@ -594,6 +594,8 @@ UCB_API int ucb_measure_fma_peak(int precision, double* tflops);
 #define UCB_SCHEME_EULER_CROMER 1
 #define UCB_SCHEME_MIDPOINT 2
 #define UCB_SCHEME_RK4 3
+#define UCB_SCHEME_DOPRI78 4 /* Dormand-Prince 8(7), 13 stages (codegen.cpp:611-675) */
+#define UCB_SCHEME_CD 5      /* composition D-method, symmetry coefficient a[0] (codegen.cpp:686-754) */
 UCB_API int ucb_codegen(const char* text, const char* alphabet, int order_as_in_system, const char* func_defs,
                         int scheme, char* out, int out_len, char* vars_out, int vars_len, char* params_out,
                         int params_len);

@@ -9,7 +9,7 @@ import pytest
 import ucb
 from helpers import codegen_cases
 
-SCHEMES = ["Euler", "Euler-Cromer", "Explicit Midpoint", "RK4"]
+SCHEMES = ["Euler", "Euler-Cromer", "Explicit Midpoint", "RK4", "DOPRI78", "CD"]
 
 
 @pytest.mark.parametrize("name", sorted(codegen_cases()))

@@ -700,8 +700,8 @@ extern "C" int ucb_run_basins_dbscan(ucb_engine* e, const ucb_basins_dbscan_requ
     minmax_features(res->avg_intervals, total, res->avg_intervals_min, res->avg_intervals_max);
     res->n_pts = n;
     if (q.csv_output_path && *q.csv_output_path) {
-        csv::Common cc{std::vector<double>(q.base_values, q.base_values + q.n_values),
-                       std::vector<double>(q.initial_conditions, q.initial_conditions + q.amount_of_x)};
+        const csv::Common cc = csv::common(q.base_values, q.n_values, q.initial_conditions, q.amount_of_x,
+                                           q.opt.precision == UCB_PREC_F32);
         csv::basins(q.csv_output_path, cc, q.t_max, q.transient_time, q.h, q.pre_scaller, q.eps_dbscan,
                     q.writable_var, q.axis_x_var, q.axis_y_var, q.axis_x_lo, q.axis_x_hi, q.axis_y_lo, q.axis_y_hi, n,
                     res->labels, res->avg_peaks, res->avg_intervals, res->classes);

@@ -14,6 +14,18 @@ struct Common {
     std::vector<double> ic;      // X0[]
 };
 
+// A value as the kernels used it: narrowed to float when the engine's numb is float
+// (precision UCB_PREC_F32), as the reference stages requests to its numb (to_numb,
+// parametric_engine.cpp:2256-2265), and unchanged in the FP64 form.
+inline double numb_value(double v, bool f32) { return f32 ? (double)(float)v : v; }
+// a[] and X0[] for the config files, as the kernels used them (numb_value).
+inline Common common(const double* a, int na, const double* x0, int nx, bool f32) {
+    Common c;
+    for (int i = 0; i < na; ++i) c.values.push_back(numb_value(a[i], f32));
+    for (int i = 0; i < nx; ++i) c.ic.push_back(numb_value(x0[i], f32));
+    return c;
+}
+
 void bif1d(const std::string& path, const Common& c, double tMax, double transient, double h, int pre,
            int writable_var, int index_of_mut_var, double lo, double hi, int n_pts, const int* counts,
            const double* peaks, const double* intervals, int max_peaks);

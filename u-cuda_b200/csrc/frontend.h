@@ -45,6 +45,10 @@ struct System {
     std::vector<std::string> vars;    // state variables -> X[0..N-1]
     std::vector<std::string> params;  // parameters -> a[1..M] (a[0] reserved)
     std::vector<PNode> rhs;           // bound right-hand sides (Var / Par / Num / pi)
+    // A name that is neither a variable, a parameter nor pi fails every scheme that binds
+    // names (the message is kept here and rhs holds it as a plain symbol); the CD scheme
+    // works on the plain text and passes it through, as the reference does.
+    std::string bind_error;
 };
 
 struct FuncDef {
@@ -53,7 +57,7 @@ struct FuncDef {
 };
 using FuncDefs = std::map<std::string, FuncDef>;
 
-enum class Scheme { Euler, EulerCromer, ExplicitMidpoint, RK4, DOPRI78 };
+enum class Scheme { Euler, EulerCromer, ExplicitMidpoint, RK4, DOPRI78, CD };
 
 // Parses a multi-line LaTeX (or plain-syntax) system with the given alphabet. Throws
 // std::runtime_error with a message on malformed input.
@@ -63,8 +67,12 @@ FuncDefs parse_func_defs(const std::string& text);
 
 // Step body of a scheme, in the reference's text form.
 std::string emit_scheme(const System& s, Scheme sc);
+// The CD scheme's body (frontend_cd.cpp).
+std::string emit_cd(const System& s);
 // C expression of one right-hand side over `state` (e.g. "X1") and a[].
 std::string emit_expr(const PNode& n, const std::string& state);
+// Plain text of an expression: variable / parameter names, powers printed as a^b.
+std::string emit_plain(const PNode& n, const std::vector<std::string>& vars, const std::vector<std::string>& params);
 
 // ------------------------------------------------------------------ recognition
 struct Rhs {

@@ -51,6 +51,8 @@ extern "C" UCB_API int ucb_codegen(const char* text, const char* alphabet, int o
             case UCB_SCHEME_EULER_CROMER: sc = Scheme::EulerCromer; break;
             case UCB_SCHEME_MIDPOINT: sc = Scheme::ExplicitMidpoint; break;
             case UCB_SCHEME_RK4: sc = Scheme::RK4; break;
+            case UCB_SCHEME_DOPRI78: sc = Scheme::DOPRI78; break;
+            case UCB_SCHEME_CD: sc = Scheme::CD; break;
             default: throw std::runtime_error("scheme not generated by this front-end");
         }
         const std::string body = emit_scheme(s, sc);

@@ -145,6 +145,47 @@ std::string emit_expr(const PNode& n, const std::string& state) {
     return o.str();
 }
 
+// Plain form: the names of variables and parameters, powers as a^b (both operands bound
+// tighter than every other operator), numbers and the other operators as in the C form.
+static void print_plain(const PNode& n, const std::vector<std::string>& vars, const std::vector<std::string>& pars,
+                        std::ostream& o);
+static void print_plain_at(const PNode& n, const std::vector<std::string>& vars, const std::vector<std::string>& pars,
+                           std::ostream& o, int level) {
+    const bool paren = binding(n->kind) < level;
+    if (paren) o << "(";
+    print_plain(n, vars, pars, o);
+    if (paren) o << ")";
+}
+static void print_plain(const PNode& n, const std::vector<std::string>& vars, const std::vector<std::string>& pars,
+                        std::ostream& o) {
+    switch (n->kind) {
+        case Node::Num: o << fmt_number(n->num); break;
+        case Node::Sym: o << n->name; break;
+        case Node::Var: o << vars.at(n->index); break;
+        case Node::Par: o << pars.at(n->index - 1); break;
+        case Node::Neg: o << "-"; print_plain_at(n->a, vars, pars, o, 3); break;
+        case Node::Add: print_plain_at(n->a, vars, pars, o, 1); o << " + "; print_plain_at(n->b, vars, pars, o, 1); break;
+        case Node::Sub: print_plain_at(n->a, vars, pars, o, 1); o << " - "; print_plain_at(n->b, vars, pars, o, 2); break;
+        case Node::Mul: print_plain_at(n->a, vars, pars, o, 2); o << " * "; print_plain_at(n->b, vars, pars, o, 2); break;
+        case Node::Div: print_plain_at(n->a, vars, pars, o, 2); o << " / "; print_plain_at(n->b, vars, pars, o, 3); break;
+        case Node::Pow: print_plain_at(n->a, vars, pars, o, 4); o << "^"; print_plain_at(n->b, vars, pars, o, 4); break;
+        case Node::Call:
+            o << n->name << "(";
+            for (size_t k = 0; k < n->args.size(); ++k) {
+                if (k) o << ", ";
+                print_plain(n->args[k], vars, pars, o);
+            }
+            o << ")";
+            break;
+    }
+}
+
+std::string emit_plain(const PNode& n, const std::vector<std::string>& vars, const std::vector<std::string>& params) {
+    std::ostringstream o;
+    print_plain(n, vars, params, o);
+    return o.str();
+}
+
 // ------------------------------------------------------------------ C expression parser
 namespace {
 

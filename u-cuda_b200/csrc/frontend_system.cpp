@@ -395,10 +395,15 @@ const std::map<std::string, std::string>& greek() {
 
 struct Names {
     std::map<std::string, PNode> bind;  // name -> Var / Par / Sym(pi)
+    bool lenient = false;               // unknown names become plain symbols
     PNode resolve(const std::string& n) const {
         auto it = bind.find(n);
-        if (it == bind.end()) throw std::runtime_error("unknown symbol: " + n);
-        return it->second;
+        if (it != bind.end()) return it->second;
+        if (!lenient) throw std::runtime_error("unknown symbol: " + n);
+        auto s = std::make_shared<Node>();
+        s->kind = Node::Sym;
+        s->name = n;
+        return s;
     }
 };
 
@@ -735,8 +740,9 @@ static TextSystem parse_text_system(const std::string& text, const std::vector<s
     return sys;
 }
 
-static std::vector<PNode> bind_rhs(const TextSystem& t) {
+static std::vector<PNode> bind_rhs(const TextSystem& t, bool lenient) {
     Names nm;
+    nm.lenient = lenient;
     for (size_t i = 0; i < t.vars.size(); ++i) nm.bind[t.vars[i]] = var((int)i);
     for (size_t j = 0; j < t.params.size(); ++j) nm.bind[t.params[j]] = par(1 + (int)j);
     {
@@ -759,11 +765,20 @@ System parse_system(const std::string& text, const std::vector<std::string>& alp
     System s;
     s.vars = t.vars;
     s.params = t.params;
-    s.rhs = bind_rhs(t);
+    try {
+        s.rhs = bind_rhs(t, false);
+    } catch (const std::runtime_error& e) {
+        const std::string msg = e.what();
+        if (msg.rfind("unknown symbol: ", 0) != 0) throw;
+        s.bind_error = msg;
+        s.rhs = bind_rhs(t, true);
+    }
     return s;
 }
 
 std::string emit_scheme(const System& s, Scheme sc) {
+    if (sc == Scheme::CD) return emit_cd(s);
+    if (!s.bind_error.empty()) throw std::runtime_error(s.bind_error);
     const int N = (int)s.vars.size();
     if ((int)s.rhs.size() != N) throw std::runtime_error("vars/rhs size mismatch");
     std::ostringstream o;
@@ -806,8 +821,59 @@ std::string emit_scheme(const System& s, Scheme sc) {
                  "k[i][j];\n            }\n        }\n    }\n";
             break;
         }
-        case Scheme::DOPRI78:
-            throw std::runtime_error("DOPRI78 bodies are not generated by this front-end");
+        case Scheme::DOPRI78: {
+            // Dormand-Prince 8(7), 13 stages (Prince & Dormand 1981): the stage matrix and
+            // the two weight rows as the reference body prints them (12 to 13 significant
+            // digits), then the 8th-order update; the 7th-order solution z is computed and
+            // left unused, as in the reference body (codegen.cpp:611-675).
+            static const char* const kM[13] = {
+                "0,0,0,0,0,0,0,0,0,0,0,0",
+                "0.05555555555556,0,0,0,0,0,0,0,0,0,0,0",
+                "0.02083333333333,0.0625,0,0,0,0,0,0,0,0,0,0",
+                "0.03125,0,0.09375,0,0,0,0,0,0,0,0,0",
+                "0.3125,0,-1.171875,1.171875,0,0,0,0,0,0,0,0",
+                "0.0375,0,0,0.1875,0.15,0,0,0,0,0,0,0",
+                "0.04791013711111,0,0,0.1122487127778,-0.02550567377778,0.01284682388889,0,0,0,0,0,0",
+                "0.01691798978729,0,0,0.387848278486,0.0359773698515,0.1969702142157,-0.1727138523405,0,0,0,0,0",
+                "0.06909575335919,0,0,-0.6342479767289,-0.1611975752246,0.1386503094588,0.9409286140358,"
+                "0.2116363264819,0,0,0,0",
+                "0.183556996839,0,0,-2.468768084316,-0.2912868878163,-0.02647302023312,2.847838764193,"
+                "0.2813873314699,0.1237448998633,0,0,0",
+                "-1.215424817396,0,0,16.67260866595,0.9157418284168,-6.056605804357,-16.00357359416,"
+                "14.8493030863,-13.37157573529,5.13418264818,0,0",
+                "0.2588609164383,0,0,-4.774485785489,-0.435093013777,-3.049483332072,5.577920039936,"
+                "6.155831589861,-5.062104586737,2.193926173181,0.1346279986593,0",
+                "0.8224275996265,0,0,-11.65867325728,-0.7576221166909,0.7139735881596,12.07577498689,"
+                "-2.12765911392,1.990166207049,-0.234286471544,0.1758985777079,0"};
+            static const char* const kB[2] = {
+                "0.04174749114153,0,0,0,0,-0.05545232861124,0.2393128072012,0.7035106694034,-0.7597596138145,"
+                "0.6605630309223,0.1581874825101,-0.2381095387529,0.25",
+                "0.02955321367635,0,0,0,0,-0.8286062764878,0.3112409000511,2.4673451906,-2.546941651842,"
+                "1.443548583677,0.07941559588113,0.04444444444444,0"};
+            auto k = f("X1");
+            o << "    static const numb M[13][12] = {\n";
+            for (int r = 0; r < 13; ++r) o << "        {" << kM[r] << "}" << (r < 12 ? ",\n" : "\n");
+            o << "    };\n    static const numb B[2][13] = {\n";
+            for (int r = 0; r < 2; ++r) o << "        {" << kB[r] << "}" << (r < 1 ? ",\n" : "\n");
+            o << "    };\n";
+            for (const char* arr : {"X1", "X2", "y", "z"}) o << "    numb " << arr << "[" << N << "];\n";
+            o << "    numb k[" << N << "][13];\n    int N = " << N << ";\n    int i, j, l;\n";
+            o << "    for (i = 0; i < N; ++i) X1[i] = X[i];\n    for (i = 0; i < 13; ++i) {\n";
+            for (int v = 0; v < N; ++v) o << "        k[" << v << "][i] = (" << k[v] << ");\n";
+            o << "        if (i != 12) {\n            for (l = 0; l < N; ++l) X2[l] = 0;\n"
+                 "            for (j = 0; j < i + 1; ++j)\n                for (l = 0; l < N; ++l)\n"
+                 "                    X2[l] += M[i + 1][j] * k[l][j];\n            for (l = 0; l < N; ++l)\n"
+                 "                X1[l] = X[l] + h * X2[l];\n        }\n    }\n";
+            for (int w = 0; w < 2; ++w)
+                o << "    for (l = 0; l < N; ++l) X2[l] = 0;\n    for (i = 0; i < 13; ++i)\n"
+                     "        for (l = 0; l < N; ++l)\n            X2[l] += B["
+                  << w << "][i] * k[l][i];\n    for (l = 0; l < N; ++l)\n        " << (w ? "z" : "y")
+                  << "[l] = X[l] + h * X2[l];\n";
+            o << "    (void)z[0];\n    for (l = 0; l < N; ++l) X[l] = y[l];\n";
+            break;
+        }
+        case Scheme::CD:
+            break;  // emit_cd above
     }
     return o.str();
 }

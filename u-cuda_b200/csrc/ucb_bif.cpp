@@ -214,8 +214,8 @@ extern "C" int ucb_run_bif1d(ucb_engine* e, const ucb_bif1d_request* req, ucb_bi
     res->param_lo = q.param_lo;
     res->param_hi = q.param_hi;
     if (q.csv_output_path && *q.csv_output_path) {
-        csv::Common cc{std::vector<double>(q.base_values, q.base_values + q.n_values),
-                       std::vector<double>(q.initial_conditions, q.initial_conditions + q.amount_of_x)};
+        const bool f32 = q.opt.precision == UCB_PREC_F32;
+        const csv::Common cc = csv::common(q.base_values, q.n_values, q.initial_conditions, q.amount_of_x, f32);
         csv::bif1d(q.csv_output_path, cc, q.t_max, q.transient_time, q.h, q.pre_scaller, q.writable_var,
                    q.sweep_over_var ? q.var_sweep_index : q.param_index, lo_n, hi_n, n, res->counts, res->peaks,
                    res->intervals, mo);

@@ -271,8 +271,8 @@ extern "C" int ucb_run_bif2d(ucb_engine* e, const ucb_bif2d_request* req, ucb_bi
     res->param_lo_2 = q.param_lo_2;
     res->param_hi_2 = q.param_hi_2;
     if (q.csv_output_path && *q.csv_output_path) {
-        csv::Common cc{std::vector<double>(q.base_values, q.base_values + q.n_values),
-                       std::vector<double>(q.initial_conditions, q.initial_conditions + q.amount_of_x)};
+        const csv::Common cc = csv::common(q.base_values, q.n_values, q.initial_conditions, q.amount_of_x,
+                                           q.opt.precision == UCB_PREC_F32);
         csv::bif2d(q.csv_output_path, cc, m.par_or_var, q.t_max, q.transient_time, q.h, q.pre_scaller, q.eps_dbscan,
                    q.writable_var, q.sweep_over_var ? q.var_sweep_index : q.param_index,
                    q.sweep_over_var_2 ? q.var_sweep_index_2 : q.param_index_2, q.param_lo, q.param_hi, q.param_lo_2,

@@ -920,8 +920,8 @@ int ucb_run_lle2d(ucb_engine* e, const ucb_lle2d_request* req, ucb_lle2d_result*
         res->min_val = res->max_val = 0.0;
     }
     if (q.csv_output_path && *q.csv_output_path) {
-        csv::Common cc{std::vector<double>(q.base_values, q.base_values + q.n_values),
-                       std::vector<double>(q.initial_conditions, q.initial_conditions + q.amount_of_x)};
+        const csv::Common cc = csv::common(q.base_values, q.n_values, q.initial_conditions, q.amount_of_x,
+                                           q.opt.precision == UCB_PREC_F32);
         csv::lle2d(q.csv_output_path, cc, plan.map.par_or_var, q.t_max, q.NT, q.transient_time, q.h, q.eps,
                    q.sweep_over_var ? q.var_sweep_index : q.param_index,
                    q.sweep_over_var_2 ? q.var_sweep_index_2 : q.param_index_2, q.param_lo, q.param_hi, q.param_lo_2,
@@ -996,10 +996,11 @@ int ucb_run_lle1d(ucb_engine* e, const ucb_lle1d_request* req, ucb_lle1d_result*
     res->param_lo = q1.param_lo;
     res->param_hi = q1.param_hi;
     if (q1.csv_output_path && *q1.csv_output_path) {
-        csv::Common cc{std::vector<double>(q1.base_values, q1.base_values + q1.n_values),
-                       std::vector<double>(q1.initial_conditions, q1.initial_conditions + q1.amount_of_x)};
+        const bool f32 = q1.opt.precision == UCB_PREC_F32;
+        const csv::Common cc = csv::common(q1.base_values, q1.n_values, q1.initial_conditions, q1.amount_of_x, f32);
         csv::curve1d(q1.csv_output_path, "1D LLE", cc, q1.t_max, q1.NT, q1.transient_time, q1.h, q1.eps,
-                     plan.map.idx[0], q1.param_lo, q1.param_hi, q1.log_scale != 0, n, 1, res->values);
+                     plan.map.idx[0], csv::numb_value(q1.param_lo, f32), csv::numb_value(q1.param_hi, f32),
+                     q1.log_scale != 0, n, 1, res->values);
     }
     if (q1.progress) *q1.progress = 1.0f;
     if (!L.sys.note.empty()) e->last_error = L.sys.note;

@@ -263,8 +263,8 @@ extern "C" int ucb_run_ls2d(ucb_engine* e, const ucb_ls2d_request* req, ucb_ls2d
     if (rc != UCB_OK) return rc;
     const int n = q.n_pts, nx = q.amount_of_x;
     if (q.csv_output_path && *q.csv_output_path) {
-        csv::Common cc{std::vector<double>(q.base_values, q.base_values + q.n_values),
-                       std::vector<double>(q.initial_conditions, q.initial_conditions + nx)};
+        const csv::Common cc = csv::common(q.base_values, q.n_values, q.initial_conditions, nx,
+                                           q.opt.precision == UCB_PREC_F32);
         csv::ls2d(q.csv_output_path, cc, m.par_or_var, q.t_max, q.NT, q.transient_time, q.h, q.eps,
                   q.sweep_over_var ? q.var_sweep_index : q.param_index,
                   q.sweep_over_var_2 ? q.var_sweep_index_2 : q.param_index_2, q.param_lo, q.param_hi, q.param_lo_2,
@@ -349,10 +349,11 @@ extern "C" int ucb_run_ls1d(ucb_engine* e, const ucb_ls1d_request* req, ucb_ls1d
     res->steps = r2.steps;
     res->flops = r2.flops;
     if (q1.csv_output_path && *q1.csv_output_path) {
-        csv::Common cc{std::vector<double>(q1.base_values, q1.base_values + q1.n_values),
-                       std::vector<double>(q1.initial_conditions, q1.initial_conditions + nx)};
+        const bool f32 = q1.opt.precision == UCB_PREC_F32;
+        const csv::Common cc = csv::common(q1.base_values, q1.n_values, q1.initial_conditions, nx, f32);
         csv::curve1d(q1.csv_output_path, "1D LS", cc, q1.t_max, q1.NT, q1.transient_time, q1.h, q1.eps, m.idx[0],
-                     q1.param_lo, q1.param_hi, q1.log_scale != 0, n, nx, res->values);
+                     csv::numb_value(q1.param_lo, f32), csv::numb_value(q1.param_hi, f32), q1.log_scale != 0, n, nx,
+                     res->values);
     }
     if (q1.progress) *q1.progress = 1.0f;
     res->ok = 1;

@@ -905,7 +905,7 @@ def measure_fma_peak(precision=PREC_F64) -> float:
     return v.value
 
 
-SCHEMES = {"Euler": 0, "Euler-Cromer": 1, "Explicit Midpoint": 2, "RK4": 3}
+SCHEMES = {"Euler": 0, "Euler-Cromer": 1, "Explicit Midpoint": 2, "RK4": 3, "DOPRI78": 4, "CD": 5}
 
 
 def codegen(text: str, alphabet: str, scheme: str = "RK4", order_as_in_system=False, func_defs: str | None = None):
