@@ -300,7 +300,8 @@ def run_surrogate(eng, c, results, args, dev):
     vals = all_vals[idx]
     ref = results["plain_fp64"]["values"][idx]
     return {"ms_per_map": ms, "cells_per_s": n * n / (ms * 1e-3),
-            "vs_plain_fp64": results["plain_fp64"]["ms"] / ms,
+            "vs_plain_fp64": results["plain_fp64"]["ms"] / ms, "vs_fp32": results["fp32"]["ms"] / ms,
+            "gated": int(res.gated), "pilot_predictable": res.pilot_predictable,
             "predicted_fraction": res.n_predicted / (n * n), "refined_cells": res.n_refined,
             "samples": res.n_samples, "sigma_threshold": res.sigma_threshold,
             "calibration_within_tol": res.calib_within_tol,
@@ -361,6 +362,8 @@ def run_surrogate_chen(eng, dev, n: int, tol: float, coverage: float):
             "ms_per_map": res.total_ms, "cells_per_s": total / (res.total_ms * 1e-3),
             "plain_fp64_cells_per_s": plain_rate, "fp32_cells_per_s": out["fp32"][1],
             "vs_plain_fp64": (total / (res.total_ms * 1e-3)) / plain_rate,
+            "vs_fp32": (total / (res.total_ms * 1e-3)) / out["fp32"][1],
+            "gated": int(res.gated), "pilot_predictable": res.pilot_predictable,
             "predicted_fraction": res.n_predicted / total, "refined_cells": res.n_refined,
             "samples": res.n_samples, "sigma_threshold": res.sigma_threshold,
             "calibration_within_tol": res.calib_within_tol,
@@ -400,11 +403,30 @@ def run_mlp(eng, rows: int = 1 << 20, steps: int = 200):
         torch.cuda.synchronize()
         fit.append((time.perf_counter() - t0) * 1e3 / max(steps, 1))
     net.close()
-    # GEMM FLOPs of one prediction (2 M N K per layer): 128 Fourier features -> 256, three
-    # 256 -> 256 layers, 256 -> 2 outputs
+    # Algorithmic work of one prediction through the five GEMMs (128 Fourier features -> 256,
+    # three 256 -> 256 layers, 256 -> 2 outputs): 2 M N K FLOPs, and the HBM bytes of their
+    # operands and results (BF16 activations read once and written once per layer, FP32
+    # outputs). At these shapes the prediction is HBM-bound: 0.55 TFLOP against 4.4 KB per row.
     flops = 2.0 * rows * (128 * 256 + 3 * 256 * 256 + 256 * 2)
-    return {"predict_rows": rows, "predict_ms": min(pred[1:]), "train_step_ms": min(fit),
-            "predict_gemm_tflops": flops / (min(pred[1:]) * 1e-3) / 1e12, "loss": float(loss)}
+    bytes_ = rows * ((128 + 3 * 256 + 256) * 2 + 4 * 256 * 2 + 2 * 4)
+    ms = min(pred[1:])
+    peaks = measured_peaks()
+    out = {"predict_rows": rows, "predict_ms": ms, "train_step_ms": min(fit),
+           "predict_gemm_tflops": flops / (ms * 1e-3) / 1e12, "predict_gbs": bytes_ / (ms * 1e-3) / 1e9,
+           "predict_bytes": bytes_, "loss": float(loss)}
+    if peaks.get("hbm_gbs"):
+        out["roofline"] = {"bound": "hbm", "achieved": out["predict_gbs"], "peak": peaks["hbm_gbs"], "unit": "GB/s",
+                           "frac": out["predict_gbs"] / peaks["hbm_gbs"],
+                           "peak_source": "MEASURED_PEAKS.json hbm_gbs (of measured)"}
+    return out
+
+
+def measured_peaks() -> dict:
+    p = ROOT / "MEASURED_PEAKS.json"
+    try:
+        return json.loads(p.read_text()) if p.exists() else {}
+    except Exception:
+        return {}
 
 
 def _timed(fn, reps=1):
@@ -507,7 +529,8 @@ def run_other_configs(eng, which=OTHER_CONFIGS, args=None):
         v = vals.reshape(4, -1)
         ok = flags == 1
         out.setdefault("ls_hyper_rossler_512_dp5", {})[name] = {
-            "grid": n_ls, "wall_ms": ms, "kernel_ms": res.kernel_ms, "launch_shape": shape,
+            "grid": n_ls, "t_end": t_end, "max_attempts_per_cell": max_steps or 20000000,
+            "wall_ms": ms, "kernel_ms": res.kernel_ms, "launch_shape": shape,
             "cells_per_s": n_ls * n_ls / (res.kernel_ms * 1e-3),
             "rhs_evals_per_s": res.steps / (res.kernel_ms * 1e-3), "valid_cells": int(ok.sum()),
             "median_spectrum": [float(np.median(v[k][ok])) for k in range(4)],
@@ -634,7 +657,9 @@ def main():
     ap.add_argument("--cpu-stride", type=int, default=6)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--all-configs", action="store_true",
-                    help="also time the bifurcation, spectrum and basins configurations at full size")
+                    help="time every other configuration (the default; kept for older command lines)")
+    ap.add_argument("--no-other-configs", action="store_true",
+                    help="time only the LLE headline (no bifurcation, spectrum, basins or period-map configurations)")
     ap.add_argument("--no-autotune", action="store_true",
                     help="run the default launch shape (128 threads) instead of the autotuned one")
     ap.add_argument("--no-headline", action="store_true",
@@ -644,20 +669,22 @@ def main():
                     help="grid of the stroboscopic basins configuration (smaller only for profiling)")
     ap.add_argument("--basins-dbscan-n", type=int, default=1024,
                     help="grid of the reference-method basins configuration (smaller only for profiling)")
-    ap.add_argument("--spectrum-t-end", type=float, default=2e4,
-                    help="measured interval of the spectrum configuration (shorter only for profiling)")
-    ap.add_argument("--spectrum-max-steps", type=int, default=0,
-                    help="step-attempt cap per cell of the spectrum configuration (default 2e7; lower only "
-                         "for profiling)")
-    ap.add_argument("--spectrum-n", type=int, default=0,
-                    help="grid of the spectrum configuration (default: 512 if a 64^2 pass ends within 150 s, "
-                         "else 128)")
+    ap.add_argument("--spectrum-t-end", type=float, default=200.0,
+                    help="measured interval of the spectrum configuration (default 200, a bounded run; the "
+                         "configuration's own t_end is 2e4)")
+    ap.add_argument("--spectrum-max-steps", type=int, default=2_000_000,
+                    help="step-attempt cap per cell of the spectrum configuration (default 2e6 for the bounded "
+                         "run; 0 = the engine's 2e7)")
+    ap.add_argument("--spectrum-n", type=int, default=128,
+                    help="grid of the spectrum configuration (default 128 for the bounded run; 0: 512 if a 64^2 "
+                         "pass ends within 150 s, else 128)")
     ap.add_argument("--configs", default="",
                     help=f"comma-separated subset of {','.join(OTHER_CONFIGS)} to time (instead of --all-configs)")
     ap.add_argument("--mlp-rows", type=int, default=1 << 20,
                     help="rows of the surrogate-network prediction timing (the MLP line of the JSON)")
-    ap.add_argument("--surrogate-chen", type=int, default=0, metavar="N",
-                    help="also run the surrogate-refined Chen map at N x N (e.g. 8192)")
+    ap.add_argument("--surrogate-chen", type=int, default=2048, metavar="N",
+                    help="grid of the surrogate-refined Chen map (default 2048, a bounded run; the configuration's "
+                         "own grid is 8192; 0 = skip)")
     args = ap.parse_args()
     rank, world, local = dist_env()
     cfg = {"workload": f"Rossler LLE map {args.n}x{args.n} (b in [0.05,2] x c in [2,20], a=0.2), RK4 h=0.01, "
@@ -709,7 +736,10 @@ def main():
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu = run_cpu_baseline(args.n, args.cpu_stride, 0)
     import ucb
-    which = OTHER_CONFIGS if args.all_configs else tuple(c for c in args.configs.split(",") if c in OTHER_CONFIGS)
+    if args.configs:
+        which = tuple(c for c in args.configs.split(",") if c in OTHER_CONFIGS)
+    else:
+        which = () if args.no_other_configs else OTHER_CONFIGS
     if args.no_headline:
         # only the selected configurations (profiling runs of one kernel), one JSON line
         if rank == 0:

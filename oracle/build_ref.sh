@@ -27,6 +27,6 @@ echo "built $HERE/_ref/ref_codegen"
 PSTL="$(dirname "$(find /usr/include/c++ -name execution_defs.h 2>/dev/null | head -1)")"
 CUDA_HOME="${CUDA_HOME:-/usr/local/cuda}"
 g++ -O1 -std=c++17 -I"$HERE/ref_stubs" -I- -I"$REF" -I"$CUDA_HOME/include" ${PSTL:+-I"$PSTL"} \
-    "$HERE/ref_csv_main.cpp" "$REF/data_export.cpp" -o "$HERE/_ref/ref_csv" 2>&1 | grep -v "obsolete option '-I-'" || true
+    "$HERE/ref_csv_main.cpp" "$REF/data_export.cpp" -o "$HERE/_ref/ref_csv" 2>&1 | grep -v "obsolete option" || true
 test -x "$HERE/_ref/ref_csv" && echo "built $HERE/_ref/ref_csv"
 python "$HERE/build_ref_kernels.py" "$REF" "$HERE/_ref"

@@ -524,7 +524,7 @@ void ls_cell_dp5_cpu(RhsFn f, RhsDualFn fd, int nx, const double* x0, const doub
     // Early orthonormalisation when the accumulated spread (time since the last pass x
     // running lambda_1 - lambda_N) exceeds the FP64 budget of 20 nats.
     double t_gs = 0.0, t_meas = 0.0, spread = 1e300;
-    long long attempts = 0;
+    long long attempts = 0, accepted = 0;
     std::vector<double> stage((size_t)6 * nx);  // stage points X1..X6
     f(x.data(), av, &K[0]);
     while (ok && t < t_stop) {
@@ -597,6 +597,9 @@ void ls_cell_dp5_cpu(RhsFn f, RhsDualFn fd, int nx, const double* x0, const doub
             double checker = 0;
             for (int i = 0; i < nx; ++i) checker += std::fabs(x[i]);
             if (std::isnan(checker) || std::isinf(checker) || (maxv != 0 && checker > maxv)) { ok = false; break; }
+            // escape test (the kernel's): every 16 accepted steps, a cell whose remaining
+            // horizon needs more than 8x its remaining attempts at the step just taken ends
+            if ((++accepted & 15) == 0 && t_stop - t > 8.0 * h * (double)(max_steps - attempts)) { ok = false; break; }
             if (measuring && (++since >= gs_every || last || t_gs * spread > 20.0)) {
                 ok = mgs_cpu(V, nx, acc.data());
                 since = 0;

@@ -423,6 +423,10 @@ __device__ __forceinline__ double dp5_tangent_step(const Dp5State& S, const numb
     return scaled_sum_sq<UCB_NX>(e, sc);
 }
 
+// An adaptive cell whose remaining horizon needs more than this many times its remaining
+// step attempts (at the current step size) is given up as escaping.
+constexpr double kEscapeFactor = 8.0;
+
 __device__ __forceinline__ void ls_cell_dp5(const UcbLsParams& p, long long kidx, long long& ns) {
     double outv[UCB_NX];
     const CellAxes c = cell_axes(kidx, p.n_pts);
@@ -458,7 +462,7 @@ __device__ __forceinline__ void ls_cell_dp5(const UcbLsParams& p, long long kidx
     int since_gs = 0;
     double t_gs = 0.0, t_meas = 0.0, spread = 1e300;  // spread: running lambda_1 - lambda_N
     bool measuring = !((double)p.transient > 0);
-    long long attempts = 0;
+    long long attempts = 0, accepted = 0;
     ucb_rhs(S.X[0], a, S.k1);
     while (ok && t < t_stop) {
         if (++attempts > p.max_steps) { ok = false; break; }
@@ -496,6 +500,14 @@ __device__ __forceinline__ void ls_cell_dp5(const UcbLsParams& p, long long kidx
             S.X[0][UCB_CLOCK_VAR] = (numb)fma((double)UCB_CLOCK_RATE, t, clock0);
 #endif
             if (diverged(S.X[0], p.maxv)) { ok = false; break; }
+            // Escape test, every 16 accepted steps: at the step size just taken the rest of the
+            // horizon would need more than kEscapeFactor times the attempts left. Such a cell
+            // (in practice one escaping towards max_value through ever stiffer, ever smaller
+            // steps) would end at the attempt cap with the same flag; it ends here instead.
+            if ((++accepted & 15) == 0 && t_stop - t > kEscapeFactor * h * (double)(p.max_steps - attempts)) {
+                ok = false;
+                break;
+            }
             if (measuring && (++since_gs >= p.gs_every || last || t_gs * spread > UCB_GS_BUDGET)) {
                 ok = mgs(V, acc);
                 since_gs = 0;

@@ -2,18 +2,21 @@
 // prediction host code (no reference counterpart).
 //
 // GEMM: C[M, N] = A[M, K] B[N, K]^T with A and B K-contiguous ("TN"), M % 128 == 0,
-// N % 128 == 0, K % 64 == 0. One CTA of 128 threads computes a 128 x 128 tile: the K loop
-// stages 128 x 64 tiles of A and B into 128-byte-swizzled shared memory (two buffers, so
-// the copy of tile k+1 overlaps the MMAs of tile k), one elected thread issues
-// tcgen05.mma (CuTe SM100_MMA_F16BF16_SS, cta_group::1, BF16 x BF16 -> FP32) into a
-// 128-column TMEM accumulator and commits to the buffer's mbarrier (waits are bounded;
-// on a timeout the kernel records an error, drains and frees TMEM). The epilogue reads
-// TMEM with tcgen05.ld (32 data-path lanes x 32 bit: thread t owns row t) and applies
-// bias / GELU, storing FP32, BF16 and / or transposed BF16 copies; a split-K launch stores
+// N % 128 == 0, K % 64 == 0. A persistent kernel (one CTA of 192 threads per SM) walks
+// tiles of 128 x 256 (128 x 128 when N is not a multiple of 256, so A is read once per row
+// block either way) and K splits: warp 0 streams 64-wide K chunks of A and B with TMA
+// (128-byte swizzle, no multicast) into a ring of shared-memory stages, warp 1 issues
+// tcgen05.mma (CuTe SM100_MMA_F16BF16_SS, cta_group::1, BF16 x BF16 -> FP32) from one
+// elected lane into one of two TMEM accumulators, and warps 2-5 read a finished
+// accumulator with tcgen05.ld (one 32-lane TMEM quadrant each; thread t owns row t) while
+// the next tile's MMAs run, apply bias / GELU and store FP32, BF16 and / or transposed BF16
+// copies straight from registers. Waits are bounded; on a timeout the kernel records an
+// error, waits for its own copies and MMAs, frees TMEM and returns. A split-K launch stores
 // each split's partial tile in its own slice of a buffer, and a second kernel adds the
 // slices in split order (so a training step gives the same bits every time it runs).
 // Backward products are the same TN GEMM on transposed
 // copies, which the forward epilogue and the GELU-backward kernel write as they go.
+#include <cuda.h>
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
 
@@ -42,30 +45,29 @@ namespace ucbmlp {
 using namespace cute;
 using bf16 = cutlass::bfloat16_t;
 
-constexpr int kBM = 128;
-constexpr int kBN = 128;
-constexpr int kBK = 64;
+constexpr int kBM = 128;   // rows of a tile (UMMA M, one TMEM lane per row)
+constexpr int kBK = 64;    // K per pipeline stage: one 128-byte swizzle row of BF16
 constexpr long long kWaitLimit = 1LL << 22;  // try_wait polls before a wait gives up
+constexpr int kGemmThreads = 192;  // warp 0 TMA, warp 1 MMA, warps 2-5 epilogue
 
-using MmaOp = SM100_MMA_F16BF16_SS<bf16, bf16, float, kBM, kBN, UMMA::Major::K, UMMA::Major::K>;
-using TiledMma = decltype(make_tiled_mma(MmaOp{}));
-using SmemLayoutA = decltype(UMMA::tile_to_mma_shape(
-    UMMA::Layout_K_SW128_Atom<bf16>{}, partition_shape_A(TiledMma{}, make_shape(Int<kBM>{}, Int<kBK>{}))));
-using SmemLayoutB = decltype(UMMA::tile_to_mma_shape(
-    UMMA::Layout_K_SW128_Atom<bf16>{}, partition_shape_B(TiledMma{}, make_shape(Int<kBN>{}, Int<kBK>{}))));
-
-constexpr int kStageLd = kBN + 4;  // staging row stride (floats): 16-byte rows, conflict-free float4 access
-
-struct GemmSmem {
-    union {
-        struct {
-            alignas(1024) cute::ArrayEngine<bf16, cosize_v<SmemLayoutA>> A[2];
-            alignas(1024) cute::ArrayEngine<bf16, cosize_v<SmemLayoutB>> B[2];
-        } ab;
-        float stage[kBM * kStageLd];  // epilogue staging (after the last MMA has completed)
-    };
-    alignas(16) cute::uint64_t bar[2];
-    alignas(16) cute::uint32_t tmem_base;
+// Shapes and shared-memory layout of the persistent GEMM for a tile width BN (128 or 256).
+template <int BN>
+struct GemmCfg {
+    using MmaOp = SM100_MMA_F16BF16_SS<bf16, bf16, float, kBM, BN, UMMA::Major::K, UMMA::Major::K>;
+    using TiledMma = decltype(make_tiled_mma(MmaOp{}));
+    using LayoutA = decltype(UMMA::tile_to_mma_shape(
+        UMMA::Layout_K_SW128_Atom<bf16>{}, partition_shape_A(TiledMma{}, make_shape(Int<kBM>{}, Int<kBK>{}))));
+    using LayoutB = decltype(UMMA::tile_to_mma_shape(
+        UMMA::Layout_K_SW128_Atom<bf16>{}, partition_shape_B(TiledMma{}, make_shape(Int<BN>{}, Int<kBK>{}))));
+    static constexpr int kStages = BN == 256 ? 4 : 6;
+    static constexpr int kABytes = kBM * kBK * 2;
+    static constexpr int kBBytes = BN * kBK * 2;
+    static constexpr int kStageBytes = kABytes + kBBytes;  // multiple of 1024: every stage stays 1024-aligned
+    // barriers: full / empty per stage, accumulator full / empty per TMEM buffer, drain
+    static constexpr int kBarriers = 2 * kStages + 2 + 2 + 1;
+    static constexpr int kSmem = 1024 + kStages * kStageBytes + 8 * kBarriers + 16;
+    static_assert(kStageBytes % 1024 == 0, "swizzled stages need 1024-byte alignment");
+    static_assert(2 * BN <= 512, "two accumulators must fit in TMEM");
 };
 
 struct Epilogue {
@@ -75,7 +77,7 @@ struct Epilogue {
     float* outf;        // FP32 result (pre-activation), row stride ldf
     int ldf;
     int atomic;         // split-K: the host redirects outf to a partial-tile buffer
-    long long split_stride;  // floats between the slices of consecutive splits (blockIdx.z)
+    long long split_stride;  // floats between the slices of consecutive splits
     bf16* outh;         // BF16 copy, row stride ldh
     int ldh;
     bf16* outt;         // BF16 transposed copy outt[n * ldt + m]
@@ -83,43 +85,46 @@ struct Epilogue {
     int m_store, n_store;  // only rows m < m_store and columns n < n_store are stored
 };
 
+// Work of one launch: items are (M tile, N tile, K split) triples, handed out round robin
+// over the persistent grid (every role of a CTA walks the same sequence).
+struct GemmWork {
+    int tiles_n, splits, kt_total, kt_per_split;
+    int items;
+};
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) { return cute::cast_smem_ptr_to_uint(p); }
+
 // mbarrier phase wait with a poll limit (each try_wait itself suspends for a bounded time).
-__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, int phase) {
-    const uint32_t addr = cute::cast_smem_ptr_to_uint(bar);
+__device__ __forceinline__ bool mbar_wait_bounded(uint32_t bar, uint32_t parity) {
     for (long long i = 0; i < kWaitLimit; ++i) {
         uint32_t done;
         asm volatile(
             "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
             : "=r"(done)
-            : "r"(addr), "r"(phase)
+            : "r"(bar), "r"(parity)
             : "memory");
         if (done) return true;
     }
     return false;
 }
-
-__device__ __forceinline__ void cp_async16(uint32_t smem_addr, const void* gptr) {
-    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(smem_addr), "l"(gptr) : "memory");
+__device__ __forceinline__ void mbar_init(uint32_t bar, uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar), "r"(count) : "memory");
 }
-__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
-template <int N>
-__device__ __forceinline__ void cp_async_wait() {
-    asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
+__device__ __forceinline__ void mbar_arrive(uint32_t bar) {
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(bar) : "memory");
 }
-
-// One 128 x 64 BF16 tile (rows row0.., columns kt*64..) of a K-contiguous matrix into the
-// 128-byte-swizzled K-major shared-memory layout of the MMA (Layout_K_SW128_Atom): row r
-// occupies bytes [128 r, 128 r + 128) of the tile and its 16-byte chunk j sits at chunk
-// j ^ (r % 8). Eight threads read one row's 128 bytes (coalesced 16-byte accesses).
-__device__ __forceinline__ void load_tile(uint32_t smem, const bf16* X, int K, int row0, int kt) {
-    const char* g = reinterpret_cast<const char*>(X + (size_t)row0 * K + (size_t)kt * kBK);
-#pragma unroll
-    for (int it = 0; it < 8; ++it) {
-        const int c = it * 128 + (int)threadIdx.x;
-        const int r = c >> 3, j = c & 7;
-        cp_async16(smem + r * 128 + ((j ^ (r & 7)) << 4), g + (size_t)r * K * 2 + j * 16);
-    }
+__device__ __forceinline__ void mbar_expect_tx(uint32_t bar, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes) : "memory");
 }
+// 2-D tiled TMA load of one box into this CTA's shared memory, completing on `bar`.
+__device__ __forceinline__ void tma_load_2d(uint32_t dst, const CUtensorMap* map, uint32_t bar, int x, int y) {
+    asm volatile(
+        "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%3, %4}], [%2];"
+        ::"r"(dst), "l"(reinterpret_cast<uint64_t>(map)), "r"(bar), "r"(x), "r"(y)
+        : "memory");
+}
+__device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
 
 // GELU in its tanh form, 0.5 z (1 + tanh(sqrt(2/pi) (z + 0.044715 z^3))) (Hendrycks and
 // Gimpel, 2016), with the hardware tanh (tanh.approx.f32, relative error about 2^-11, far
@@ -141,190 +146,245 @@ __device__ __forceinline__ float gelu_grad(float z) {
     return 0.5f * (1.0f + t) + 0.5f * z * (1.0f - t * t) * kGeluC0 * fmaf(3.0f * kGeluC1, z2, 1.0f);
 }
 
-__global__ void __launch_bounds__(128) gemm_tn_kernel(const bf16* __restrict__ A, const bf16* __restrict__ B, int M,
-                                                      int N, int K, int kt_per_split, Epilogue ep, int* err) {
-    TiledMma tiled_mma;
-    const int m0 = blockIdx.x * kBM, n0 = blockIdx.y * kBN;
-    Tensor cC = make_identity_tensor(make_shape(M, N));
-    Tensor gcC = local_tile(cC, make_shape(Int<kBM>{}, Int<kBN>{}, Int<kBK>{}), make_coord(blockIdx.x, blockIdx.y, _),
-                            Step<_1, _1, X>{});
+// One 32-column chunk of one accumulator row (this thread's) through the epilogue: bias,
+// the FP32 / BF16 / transposed BF16 stores. v: the raw accumulator values.
+__device__ __forceinline__ void epilogue_chunk(const Epilogue& ep, float* outf, int m, int n0, float (&v)[32]) {
+    if (ep.bias) {
+#pragma unroll
+        for (int j = 0; j < 32; ++j)
+            if (n0 + j < ep.nb) v[j] += __ldg(ep.bias + n0 + j);
+    }
+    const bool row_ok = m < ep.m_store;
+    const bool full = n0 + 32 <= ep.n_store;
+    if (outf && row_ok) {
+        float* p = outf + (size_t)m * ep.ldf + n0;
+        if (full && (ep.ldf & 3) == 0 && (reinterpret_cast<uintptr_t>(outf) & 15) == 0) {
+#pragma unroll
+            for (int j = 0; j < 32; j += 4)
+                *reinterpret_cast<float4*>(p + j) = make_float4(v[j], v[j + 1], v[j + 2], v[j + 3]);
+        } else {
+#pragma unroll
+            for (int j = 0; j < 32; ++j)
+                if (n0 + j < ep.n_store) p[j] = v[j];
+        }
+    }
+    if (!ep.outh && !ep.outt) return;
+    float g[32];
+#pragma unroll
+    for (int j = 0; j < 32; ++j) g[j] = ep.gelu ? gelu(v[j]) : v[j];
+    if (ep.outh && row_ok) {
+        bf16* p = ep.outh + (size_t)m * ep.ldh + n0;
+        if (full && (ep.ldh & 7) == 0 && (reinterpret_cast<uintptr_t>(ep.outh) & 15) == 0) {
+#pragma unroll
+            for (int j = 0; j < 32; j += 8) {
+                uint4 q;
+                __nv_bfloat162 h0 = __floats2bfloat162_rn(g[j], g[j + 1]), h1 = __floats2bfloat162_rn(g[j + 2], g[j + 3]);
+                __nv_bfloat162 h2 = __floats2bfloat162_rn(g[j + 4], g[j + 5]), h3 = __floats2bfloat162_rn(g[j + 6], g[j + 7]);
+                q.x = *reinterpret_cast<uint32_t*>(&h0);
+                q.y = *reinterpret_cast<uint32_t*>(&h1);
+                q.z = *reinterpret_cast<uint32_t*>(&h2);
+                q.w = *reinterpret_cast<uint32_t*>(&h3);
+                *reinterpret_cast<uint4*>(p + j) = q;
+            }
+        } else {
+#pragma unroll
+            for (int j = 0; j < 32; ++j)
+                if (n0 + j < ep.n_store) p[j] = bf16(g[j]);
+        }
+    }
+    if (ep.outt && row_ok) {
+        // consecutive threads own consecutive rows: each column's stores are contiguous
+#pragma unroll
+        for (int j = 0; j < 32; ++j)
+            if (n0 + j < ep.n_store) ep.outt[(size_t)(n0 + j) * ep.ldt + m] = bf16(g[j]);
+    }
+}
 
-    extern __shared__ __align__(1024) char smem_raw[];
-    GemmSmem& ss = *reinterpret_cast<GemmSmem*>(smem_raw);
-    Tensor sA0 = make_tensor(make_smem_ptr(ss.ab.A[0].begin()), SmemLayoutA{});
-    Tensor sA1 = make_tensor(make_smem_ptr(ss.ab.A[1].begin()), SmemLayoutA{});
-    Tensor sB0 = make_tensor(make_smem_ptr(ss.ab.B[0].begin()), SmemLayoutB{});
-    Tensor sB1 = make_tensor(make_smem_ptr(ss.ab.B[1].begin()), SmemLayoutB{});
-    const uint32_t uA[2] = {cute::cast_smem_ptr_to_uint(ss.ab.A[0].begin()),
-                            cute::cast_smem_ptr_to_uint(ss.ab.A[1].begin())};
-    const uint32_t uB[2] = {cute::cast_smem_ptr_to_uint(ss.ab.B[0].begin()),
-                            cute::cast_smem_ptr_to_uint(ss.ab.B[1].begin())};
-
-    ThrMMA cta_mma = tiled_mma.get_slice(0);
-    Tensor tCcC = cta_mma.partition_C(gcC);
-    Tensor fA0 = cta_mma.make_fragment_A(sA0);
-    Tensor fA1 = cta_mma.make_fragment_A(sA1);
-    Tensor fB0 = cta_mma.make_fragment_B(sB0);
-    Tensor fB1 = cta_mma.make_fragment_B(sB1);
-    Tensor tAcc = cta_mma.make_fragment_C(tCcC);
+// C = A B^T, A [M, K] and B [N, K] K-contiguous BF16, FP32 accumulation in TMEM.
+// Persistent and warp-specialised: warp 0 streams K chunks of A and B into a ring of
+// shared-memory stages with TMA (128-byte swizzle, the layout the MMA descriptors read),
+// warp 1 issues tcgen05.mma from one elected lane into one of two TMEM accumulators and
+// commits to the stage's and the accumulator's mbarriers, warps 2-5 (one per 32-lane TMEM
+// quadrant) read finished accumulators with tcgen05.ld, run the epilogue and hand the
+// accumulator back, so the epilogue of one tile overlaps the MMAs of the next. Every wait
+// is bounded; on a timeout the CTA records an error, stops, waits (bounded) for its own
+// copies and MMAs in flight, frees TMEM and returns.
+template <int BN>
+__global__ void __launch_bounds__(kGemmThreads, 1)
+    gemm_tma_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB, GemmWork w,
+                    Epilogue ep, int* err) {
+    using Cfg = GemmCfg<BN>;
+    constexpr int S = Cfg::kStages;
+    typename Cfg::TiledMma tiled_mma;
+    extern __shared__ char smem_raw[];
+    char* base = reinterpret_cast<char*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+    uint64_t* bars = reinterpret_cast<uint64_t*>(base + S * Cfg::kStageBytes);
+    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bars + Cfg::kBarriers);
+    volatile int* abort_flag = reinterpret_cast<volatile int*>(tmem_slot + 1);
+    auto full_bar = [&](int s) { return smem_u32(bars + s); };
+    auto empty_bar = [&](int s) { return smem_u32(bars + S + s); };
+    auto accf_bar = [&](int b) { return smem_u32(bars + 2 * S + b); };
+    auto acce_bar = [&](int b) { return smem_u32(bars + 2 * S + 2 + b); };
+    const uint32_t drain_bar = smem_u32(bars + 2 * S + 4);
 
     const int warp = threadIdx.x / 32, lane = threadIdx.x & 31;
     cute::TMEM::Allocator1Sm tmem;
-    if (warp == 0) tmem.allocate(kBN, &ss.tmem_base);
+    if (warp == 0) tmem.allocate(2 * BN, tmem_slot);
     if (threadIdx.x == 0) {
-        cute::initialize_barrier(ss.bar[0], 1);
-        cute::initialize_barrier(ss.bar[1], 1);
+        for (int s = 0; s < S; ++s) {
+            mbar_init(full_bar(s), 1);
+            mbar_init(empty_bar(s), 1);
+        }
+        for (int b = 0; b < 2; ++b) {
+            mbar_init(accf_bar(b), 1);
+            mbar_init(acce_bar(b), 4);
+        }
+        mbar_init(drain_bar, 1);
+        *abort_flag = 0;
         cutlass::arch::fence_barrier_init();
     }
     __syncthreads();
-    tAcc.data() = ss.tmem_base;
-
-    const int kt_total = K / kBK;
-    const int kt0 = blockIdx.z * kt_per_split;
-    const int nk = min(kt_total, kt0 + kt_per_split) - kt0;
-    tiled_mma.accumulate_ = UMMA::ScaleOut::Zero;
-    auto issue = [&](auto const& fA, auto const& fB) {
-        CUTE_UNROLL
-        for (int kb = 0; kb < size<2>(fA); ++kb) {
-            gemm(tiled_mma, fA(_, _, kb), fB(_, _, kb), tAcc);
-            tiled_mma.accumulate_ = UMMA::ScaleOut::One;
-        }
+    tc_fence_after();
+    const uint32_t tmem_base = *tmem_slot;
+    auto fail = [&]() {
+        *abort_flag = 1;
+        atomicExch(err, 1);
     };
-    // Two-stage pipeline: the copy of tile i+1 is in flight while the MMAs of tile i run;
-    // a buffer is refilled only after the commit of the MMAs that read it has arrived.
-    bool failed = false;
-    int issued = 0;
-    if (nk > 0) {
-        load_tile(uA[0], A, K, m0, kt0);
-        load_tile(uB[0], B, K, n0, kt0);
-        cp_async_commit();
-    }
-    for (int i = 0; i < nk; ++i) {
-        const int s = i & 1;
-        bool timed_out = false;
-        if (i + 1 < nk) {
-            if (i >= 1) timed_out = !mbar_wait_bounded(&ss.bar[s ^ 1], ((i - 1) >> 1) & 1);
-            if (!timed_out) {
-                load_tile(uA[s ^ 1], A, K, m0, kt0 + i + 1);
-                load_tile(uB[s ^ 1], B, K, n0, kt0 + i + 1);
+
+    if (warp == 0) {
+        // ---- TMA producer (lane 0)
+        if (lane == 0) {
+            asm volatile("prefetch.tensormap [%0];" ::"l"(reinterpret_cast<uint64_t>(&tmA)) : "memory");
+            asm volatile("prefetch.tensormap [%0];" ::"l"(reinterpret_cast<uint64_t>(&tmB)) : "memory");
+            int stage = 0;
+            uint32_t phase = 0;
+            int issued[S];
+#pragma unroll
+            for (int s = 0; s < S; ++s) issued[s] = 0;
+            for (int item = blockIdx.x; item < w.items && !*abort_flag; item += gridDim.x) {
+                const int sp = item % w.splits, tile = item / w.splits;
+                const int tn = tile % w.tiles_n, tm = tile / w.tiles_n;
+                const int kt0 = sp * w.kt_per_split;
+                const int nk = min(w.kt_total, kt0 + w.kt_per_split) - kt0;
+                for (int i = 0; i < nk; ++i) {
+                    if (*abort_flag || !mbar_wait_bounded(empty_bar(stage), phase ^ 1)) {
+                        fail();
+                        break;
+                    }
+                    const uint32_t a_dst = smem_u32(base + stage * Cfg::kStageBytes);
+                    mbar_expect_tx(full_bar(stage), Cfg::kStageBytes);
+                    tma_load_2d(a_dst, &tmA, full_bar(stage), (kt0 + i) * kBK, tm * kBM);
+                    tma_load_2d(a_dst + Cfg::kABytes, &tmB, full_bar(stage), (kt0 + i) * kBK, tn * BN);
+                    ++issued[stage];
+                    if (++stage == S) {
+                        stage = 0;
+                        phase ^= 1;
+                    }
+                }
             }
-            cp_async_commit();
-            cp_async_wait<1>();
-        } else {
-            cp_async_wait<0>();
+            // copies in flight when stopping early: wait (bounded) until each stage's last
+            // load has landed
+            if (*abort_flag)
+                for (int s = 0; s < S; ++s)
+                    if (issued[s] > 0) mbar_wait_bounded(full_bar(s), (uint32_t)((issued[s] - 1) & 1));
         }
-        cutlass::arch::fence_view_async_shared();
-        if (__syncthreads_or(timed_out)) {
-            failed = true;
-            break;
+    } else if (warp == 1) {
+        // ---- MMA issuer (the whole warp follows; one elected lane issues)
+        int stage = 0, buf = 0;
+        uint32_t phase = 0, acc_phase = 0;
+        for (int item = blockIdx.x; item < w.items && !*abort_flag; item += gridDim.x) {
+            const int sp = item % w.splits;
+            const int kt0 = sp * w.kt_per_split;
+            const int nk = min(w.kt_total, kt0 + w.kt_per_split) - kt0;
+            if (!mbar_wait_bounded(acce_bar(buf), acc_phase ^ 1)) {
+                fail();
+                break;
+            }
+            tc_fence_after();
+            ThrMMA cta_mma = tiled_mma.get_slice(0);
+            Tensor tAcc = cta_mma.make_fragment_C(cta_mma.partition_C(
+                make_identity_tensor(make_shape(Int<kBM>{}, Int<BN>{}))));
+            tAcc.data() = tmem_base + (uint32_t)(buf * BN);
+            tiled_mma.accumulate_ = UMMA::ScaleOut::Zero;
+            bool ok = true;
+            for (int i = 0; i < nk; ++i) {
+                if (*abort_flag || !mbar_wait_bounded(full_bar(stage), phase)) {
+                    ok = false;
+                    break;
+                }
+                tc_fence_after();
+                bf16* a_ptr = reinterpret_cast<bf16*>(base + stage * Cfg::kStageBytes);
+                Tensor sA = make_tensor(make_smem_ptr(a_ptr), typename Cfg::LayoutA{});
+                Tensor sB = make_tensor(make_smem_ptr(a_ptr + Cfg::kABytes / 2), typename Cfg::LayoutB{});
+                Tensor fA = cta_mma.make_fragment_A(sA);
+                Tensor fB = cta_mma.make_fragment_B(sB);
+                CUTE_UNROLL
+                for (int kb = 0; kb < size<2>(fA); ++kb) {
+                    gemm(tiled_mma, fA(_, _, kb), fB(_, _, kb), tAcc);
+                    tiled_mma.accumulate_ = UMMA::ScaleOut::One;
+                }
+                cutlass::arch::umma_arrive(bars + S + stage);  // the stage is free once these MMAs ran
+                if (++stage == S) {
+                    stage = 0;
+                    phase ^= 1;
+                }
+            }
+            if (!ok) {
+                fail();
+                break;
+            }
+            cutlass::arch::umma_arrive(bars + 2 * S + buf);  // accumulator complete
+            if (++buf == 2) {
+                buf = 0;
+                acc_phase ^= 1;
+            }
         }
-        if (warp == 0) {
-            if (s == 0) issue(fA0, fB0);
-            else issue(fA1, fB1);
-            cutlass::arch::umma_arrive(&ss.bar[s]);
-        }
-        issued = i + 1;
-    }
-    cp_async_wait<0>();
-    // The last commit covers every MMA issued before it.
-    if (issued > 0) {
-        const int j = issued - 1;
-        const bool timed_out = !mbar_wait_bounded(&ss.bar[j & 1], (j >> 1) & 1);
-        failed = __syncthreads_or(timed_out) || failed;
-    }
-    if (failed) {
-        if (threadIdx.x == 0) atomicExch(err, 1);
-    } else if (issued > 0) {
-        // TMEM -> registers, 32 columns at a time (tcgen05.ld 32x32b.x32: thread t of warp w
-        // holds row 32 w + t), bias; the transposed copy is stored straight from registers
-        // (consecutive threads write consecutive rows); the row-major outputs go through a
-        // per-warp staging block so that each warp stores whole 512-byte row segments.
-        const int row = warp * 32 + lane;
-        const uint32_t taddr = ss.tmem_base + ((uint32_t)(warp * 32) << 16);
-        float* stage = ss.stage;
-        float* const outf = ep.outf ? ep.outf + (size_t)blockIdx.z * ep.split_stride : nullptr;
+        // every MMA this warp issued has completed before TMEM can be released
+        cutlass::arch::umma_arrive(bars + 2 * S + 4);
+        if (!mbar_wait_bounded(drain_bar, 0)) fail();
+    } else {
+        // ---- epilogue: warp 2..5 reads TMEM lanes 32 (warp % 4) .. + 31
+        const int quad = warp & 3;
+        const int row = quad * 32 + lane;
+        int buf = 0;
+        uint32_t acc_phase = 0;
+        for (int item = blockIdx.x; item < w.items && !*abort_flag; item += gridDim.x) {
+            const int sp = item % w.splits, tile = item / w.splits;
+            const int tn = tile % w.tiles_n, tm = tile / w.tiles_n;
+            if (!mbar_wait_bounded(accf_bar(buf), acc_phase)) {
+                fail();
+                break;
+            }
+            tc_fence_after();
+            float* outf = ep.outf ? ep.outf + (size_t)sp * ep.split_stride : nullptr;
+            const int m = tm * kBM + row;
+            const uint32_t taddr = tmem_base + (uint32_t)(buf * BN) + ((uint32_t)(quad * 32) << 16);
 #pragma unroll 1
-        for (int c0 = 0; c0 < kBN; c0 += 32) {
-            uint32_t r[32];
-            asm volatile("tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15, %16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31}, [%32];\n"
-                         : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]), "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]), "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
-                         : "r"(taddr + (uint32_t)c0));
-            asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
-            // The bias is added here only for the transposed copy; the row-major pass adds it
-            // per lane (each lane owns 4 fixed columns).
-            float v[32];
+            for (int c0 = 0; c0 < BN; c0 += 32) {
+                uint32_t r[32];
+                asm volatile("tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15, %16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31}, [%32];\n"
+                             : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]), "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]), "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
+                             : "r"(taddr + (uint32_t)c0));
+                asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
+                float v[32];
 #pragma unroll
-            for (int j = 0; j < 32; ++j) v[j] = __uint_as_float(r[j]);
-            if (ep.outt && ep.bias) {
-#pragma unroll
-                for (int j = 0; j < 32; ++j) {
-                    const int n = n0 + c0 + j;
-                    if (n < ep.nb) v[j] += ep.bias[n];
-                }
+                for (int j = 0; j < 32; ++j) v[j] = __uint_as_float(r[j]);
+                epilogue_chunk(ep, outf, m, tn * BN + c0, v);
             }
-#pragma unroll
-            for (int j = 0; j < 32; j += 4)
-                *reinterpret_cast<float4*>(&stage[row * kStageLd + c0 + j]) = make_float4(v[j], v[j + 1], v[j + 2], v[j + 3]);
-            if (ep.outt && m0 + row < ep.m_store) {  // v holds the biased values here
-#pragma unroll
-                for (int j = 0; j < 32; ++j) {
-                    const int n = n0 + c0 + j;
-                    if (n < ep.n_store) ep.outt[(size_t)n * ep.ldt + m0 + row] = bf16(ep.gelu ? gelu(v[j]) : v[j]);
-                }
-            }
-        }
-        __syncwarp();
-        if (outf || ep.outh) {
-            // vector path: whole 128-column rows, 16-byte FP32 / 8-byte BF16 stores
-            const bool full = n0 + kBN <= ep.n_store;
-            const bool vf = !outf || ((ep.ldf & 3) == 0 && (reinterpret_cast<uintptr_t>(outf) & 15) == 0);
-            const bool vh = !ep.outh || ((ep.ldh & 3) == 0 && (reinterpret_cast<uintptr_t>(ep.outh) & 7) == 0);
-            const int c = lane * 4;
-            // staged values carry the bias already when the transposed copy was written
-            float b[4];
-#pragma unroll
-            for (int j = 0; j < 4; ++j)
-                b[j] = (ep.bias && !ep.outt && n0 + c + j < ep.nb) ? ep.bias[n0 + c + j] : 0.f;
-#pragma unroll 2
-            for (int rr = 0; rr < 32; ++rr) {
-                const int r = warp * 32 + rr;
-                const int m = m0 + r;
-                if (m >= ep.m_store) break;
-                float4 q = *reinterpret_cast<const float4*>(&stage[r * kStageLd + c]);
-                q.x += b[0];
-                q.y += b[1];
-                q.z += b[2];
-                q.w += b[3];
-                const float x[4] = {q.x, q.y, q.z, q.w};
-                if (full && vf && vh) {
-                    if (outf) *reinterpret_cast<float4*>(outf + (size_t)m * ep.ldf + n0 + c) = q;
-                    if (ep.outh) {
-                        float y[4];
-#pragma unroll
-                        for (int j = 0; j < 4; ++j) y[j] = ep.gelu ? gelu(x[j]) : x[j];
-                        __nv_bfloat162 lo = __floats2bfloat162_rn(y[0], y[1]);
-                        __nv_bfloat162 hi = __floats2bfloat162_rn(y[2], y[3]);
-                        uint2 pk;
-                        pk.x = *reinterpret_cast<uint32_t*>(&lo);
-                        pk.y = *reinterpret_cast<uint32_t*>(&hi);
-                        *reinterpret_cast<uint2*>(ep.outh + (size_t)m * ep.ldh + n0 + c) = pk;
-                    }
-                } else {
-#pragma unroll
-                    for (int j = 0; j < 4; ++j) {
-                        const int n = n0 + c + j;
-                        if (n >= ep.n_store) continue;
-                        if (outf) outf[(size_t)m * ep.ldf + n] = x[j];
-                        if (ep.outh) ep.outh[(size_t)m * ep.ldh + n] = bf16(ep.gelu ? gelu(x[j]) : x[j]);
-                    }
-                }
+            tc_fence_before();
+            __syncwarp();
+            if (lane == 0) mbar_arrive(acce_bar(buf));
+            if (++buf == 2) {
+                buf = 0;
+                acc_phase ^= 1;
             }
         }
     }
     __syncthreads();
     if (warp == 0) {
+        tc_fence_after();
         tmem.release_allocation_lock();
-        tmem.free(ss.tmem_base, kBN);
+        tmem.free(tmem_base, 2 * BN);
     }
 }
 
@@ -638,17 +698,60 @@ namespace {
 std::mutex g_attr_mu;
 std::vector<int> g_attr_devices;
 
-int gemm_smem_bytes() { return (int)sizeof(ucbmlp::GemmSmem); }
-
 // Dynamic shared memory above 48 KB is opted in once per device, before launches and
 // before any stream capture.
 bool set_gemm_attributes(int device, std::string& err) {
     std::lock_guard<std::mutex> lk(g_attr_mu);
     if (std::find(g_attr_devices.begin(), g_attr_devices.end(), device) != g_attr_devices.end()) return true;
-    const cudaError_t ce = cudaFuncSetAttribute(ucbmlp::gemm_tn_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                                gemm_smem_bytes());
-    if (!cu_ok(ce, err, "cudaFuncSetAttribute(gemm)")) return false;
+    cudaError_t ce = cudaFuncSetAttribute(ucbmlp::gemm_tma_kernel<128>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                          ucbmlp::GemmCfg<128>::kSmem);
+    if (!cu_ok(ce, err, "cudaFuncSetAttribute(gemm 128)")) return false;
+    ce = cudaFuncSetAttribute(ucbmlp::gemm_tma_kernel<256>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                              ucbmlp::GemmCfg<256>::kSmem);
+    if (!cu_ok(ce, err, "cudaFuncSetAttribute(gemm 256)")) return false;
     g_attr_devices.push_back(device);
+    return true;
+}
+
+// cuTensorMapEncodeTiled from the driver the runtime has loaded (no link-time dependency on
+// libcuda, so the library still loads on machines without a driver).
+using EncodeTiled = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                                 const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
+                                 CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+EncodeTiled encode_tiled(std::string& err) {
+    static EncodeTiled fn = nullptr;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q{};
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = reinterpret_cast<EncodeTiled>(p);
+    });
+    if (!fn) err = "cuTensorMapEncodeTiled is not available from the CUDA driver";
+    return fn;
+}
+
+// Tensor map of a K-contiguous BF16 matrix [rows, K]: boxes of 64 (K) x box_rows with the
+// 128-byte swizzle the MMA's shared-memory descriptors expect.
+bool tensor_map(CUtensorMap* map, const bf16* ptr, int rows, int K, int box_rows, std::string& err) {
+    EncodeTiled fn = encode_tiled(err);
+    if (!fn) return false;
+    if ((reinterpret_cast<uintptr_t>(ptr) & 15) != 0 || K % ucbmlp::kBK) {
+        err = "gemm: operand not 16-byte aligned or K not a multiple of 64";
+        return false;
+    }
+    const cuuint64_t dims[2] = {(cuuint64_t)K, (cuuint64_t)rows};
+    const cuuint64_t strides[1] = {(cuuint64_t)K * sizeof(bf16)};
+    const cuuint32_t box[2] = {(cuuint32_t)ucbmlp::kBK, (cuuint32_t)box_rows};
+    const cuuint32_t estr[2] = {1, 1};
+    const CUresult r = fn(map, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, const_cast<bf16*>(ptr), dims, strides, box, estr,
+                          CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
+                          CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) {
+        err = "cuTensorMapEncodeTiled failed (" + std::to_string((int)r) + ")";
+        return false;
+    }
     return true;
 }
 
@@ -660,22 +763,24 @@ bool ordered_sum(Mlp& m, const float* part, int count, long long stride, long lo
     return cu_ok(cudaPeekAtLastError(), err, "ordered_sum launch");
 }
 
-// C = A B^T (+ epilogue). ep.atomic: split K over up to kMaxSplits CTAs per tile; each
-// split writes its partial tile into m.part and ordered_sum adds them in split order into
-// ep.outf (rows < m_store, columns < n_store; other entries of ep.outf are left alone).
+// C = A B^T (+ epilogue). Tiles of 128 x 256 when N allows (A is then read once), else
+// 128 x 128. ep.atomic: split K over up to kMaxSplits slices per tile; each slice writes its
+// partial tile into m.part and ordered_sum adds them in slice order into ep.outf (rows <
+// m_store, columns < n_store; other entries of ep.outf are left alone).
 bool gemm(Mlp& m, const bf16* A, const bf16* B, int M, int N, int K, const ucbmlp::Epilogue& ep_in, cudaStream_t st,
           std::string& err) {
     ucbmlp::Epilogue ep = ep_in;
-    if (M <= 0 || N <= 0 || K <= 0 || M % ucbmlp::kBM || N % ucbmlp::kBN || K % ucbmlp::kBK) {
+    if (M <= 0 || N <= 0 || K <= 0 || M % ucbmlp::kBM || N % 128 || K % ucbmlp::kBK) {
         err = "gemm: unsupported shape " + std::to_string(M) + "x" + std::to_string(N) + "x" + std::to_string(K);
         return false;
     }
-    const int tiles = (M / ucbmlp::kBM) * (N / ucbmlp::kBN);
+    const int bn = N % 256 == 0 ? 256 : 128;
+    const int tiles = (M / ucbmlp::kBM) * (N / bn);
     const int kt = K / ucbmlp::kBK;
+    const int sms = std::max(m.e->sm_count, 1);
     int per = kt;
     if (ep.atomic) {
-        const int want =
-            std::max(1, std::min({kt, kMaxSplits, (2 * std::max(m.e->sm_count, 1) + tiles - 1) / tiles}));
+        const int want = std::max(1, std::min({kt, kMaxSplits, (sms + tiles - 1) / tiles}));
         per = (kt + want - 1) / want;
     }
     const int splits = (kt + per - 1) / per;
@@ -688,9 +793,19 @@ bool gemm(Mlp& m, const bf16* A, const bf16* B, int M, int N, int K, const ucbml
         }
         ep.outf = m.part;
         ep.split_stride = m_eff * ep.ldf;
+    } else {
+        ep.split_stride = 0;
     }
-    dim3 grid(M / ucbmlp::kBM, N / ucbmlp::kBN, splits);
-    ucbmlp::gemm_tn_kernel<<<grid, 128, gemm_smem_bytes(), st>>>(A, B, M, N, K, per, ep, m.err);
+    CUtensorMap ta, tb;
+    if (!tensor_map(&ta, A, M, K, ucbmlp::kBM, err) || !tensor_map(&tb, B, N, K, bn, err)) return false;
+    ucbmlp::GemmWork w{N / bn, splits, kt, per, tiles * splits};
+    const int grid = std::min(w.items, sms);
+    if (bn == 256)
+        ucbmlp::gemm_tma_kernel<256><<<grid, ucbmlp::kGemmThreads, ucbmlp::GemmCfg<256>::kSmem, st>>>(ta, tb, w, ep,
+                                                                                                      m.err);
+    else
+        ucbmlp::gemm_tma_kernel<128><<<grid, ucbmlp::kGemmThreads, ucbmlp::GemmCfg<128>::kSmem, st>>>(ta, tb, w, ep,
+                                                                                                      m.err);
     m.e->launches += 1;
     if (!cu_ok(cudaPeekAtLastError(), err, "gemm launch")) return false;
     if (!ep.atomic) return true;
