@@ -671,12 +671,17 @@ UCB_API int ucb_mlp_predict(ucb_mlp* m, const float* d_u, long long n, float* d_
  * map.n_pts) is computed as:
  *   1. samples: one cell drawn at random in each block of a train_pts x train_pts
  *      partition of the grid, integrated with sample_precision (UCB_PREC_F64: the plain
- *      method); one in eight (by a hash of the block) is held out for calibration;
+ *      method). A pilot subset (a 32^2..64^2 subgrid of the blocks) is integrated first;
+ *      when a local plane fit through its neighbours predicts less than min_predictable of
+ *      it at tol / coverage, no network is trained and every other cell is integrated with
+ *      refine_precision (result->gated = 1). Otherwise the rest is integrated and one in
+ *      eight samples (by a hash of the block; more, up to half, when that leaves fewer than
+ *      1,024) is held out for calibration;
  *   2. the MLP (mlp) is trained on the others on this GPU;
  *   3. it predicts mean and standard deviation for every cell;
  *   4. calibration: the held-out samples, ordered by predicted std, give the largest std
- *      threshold below which at least `coverage` of them lie within `tol` of their
- *      integrated value (capped by sigma_max when > 0);
+ *      threshold below which the one-sided 90 % Wilson lower bound of the fraction within
+ *      `tol` of their integrated value reaches `coverage` (capped by sigma_max when > 0);
  *   5. cells with std above the threshold, |mean| < lle_band, or a 4-neighbour in another
  *      regime (lambda < -lle_band, |lambda| <= lle_band, lambda > lle_band) or differing
  *      by more than jump (when jump > 0) are re-integrated with refine_precision straight

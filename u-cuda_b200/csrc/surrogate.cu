@@ -402,7 +402,10 @@ int ucb_run_lle2d_surrogate(ucb_engine* e, const ucb_surrogate_request* rq, doub
         cudaMemcpyAsync(d_sf, hf.data(), ns * 4, cudaMemcpyHostToDevice, st);
     }
     cudaEventRecord(ev[1], st);
-    // One sample in eight (by a hash of its block) is held out for calibration.
+    // Samples held out for calibration (by a hash of their block): one in eight, more when
+    // that leaves fewer than 1,024 (up to half), so that the calibration's confidence bound
+    // can reach the requested coverage at all.
+    const long long hold = std::max<long long>(512, std::min<long long>(2048, (1024LL * 4096 + ns - 1) / std::max<long long>(ns, 1)));
     std::vector<float> hu, hy;
     std::vector<long long> cal_cells;
     std::vector<double> cal_y;
@@ -413,7 +416,7 @@ int ucb_run_lle2d_surrogate(ucb_engine* e, const ucb_surrogate_request* rq, doub
         if (hf[i] != 1 || !std::isfinite(hv[i])) continue;
         unsigned long long z = (unsigned long long)i * 0x9E3779B97F4A7C15ULL + r.mlp.seed;
         z ^= z >> 31;
-        if (z % 8 == 0) {
+        if ((long long)(z % 4096) < hold) {
             cal_cells.push_back(hc[i]);
             cal_y.push_back(hv[i]);
             continue;
@@ -482,13 +485,21 @@ int ucb_run_lle2d_surrogate(ucb_engine* e, const ucb_surrogate_request* rq, doub
         std::vector<long long> order(n_cal);
         for (long long i = 0; i < n_cal; ++i) order[i] = i;
         std::sort(order.begin(), order.end(), [&](long long a, long long b) { return gs[a] < gs[b]; });
+        // The std threshold is the largest one under which the held-out samples certify the
+        // coverage: the one-sided 90 % Wilson lower bound of the fraction within tol must
+        // reach it (a point estimate from a few hundred samples would let a per-cell outlier
+        // rate of half a percent through).
         long long good = 0;
         const long long min_count = std::min<long long>(n_cal, 32);
+        auto wilson_lower = [](double k, double n) {
+            const double z = 1.2815515655446004, z2 = z * z, ph = k / n;
+            return (ph + z2 / (2 * n) - z * std::sqrt(ph * (1 - ph) / n + z2 / (4 * n * n))) / (1 + z2 / n);
+        };
         for (long long k = 0; k < n_cal; ++k) {
             const long long i = order[k];
             good += std::fabs((double)gm[i] - cal_y[i]) <= r.tol;
             const long long cnt = k + 1;
-            if (cnt >= min_count && (double)good >= r.coverage * (double)cnt &&
+            if (cnt >= min_count && wilson_lower((double)good, (double)cnt) >= r.coverage &&
                 (k + 1 == n_cal || gs[order[k + 1]] > gs[i])) {
                 thr = gs[i];
                 within = (double)good / (double)cnt;
