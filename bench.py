@@ -403,21 +403,21 @@ def run_mlp(eng, rows: int = 1 << 20, steps: int = 200):
         torch.cuda.synchronize()
         fit.append((time.perf_counter() - t0) * 1e3 / max(steps, 1))
     net.close()
-    # Algorithmic work of one prediction through the five GEMMs (128 Fourier features -> 256,
-    # three 256 -> 256 layers, 256 -> 2 outputs): 2 M N K FLOPs, and the HBM bytes of their
-    # operands and results (BF16 activations read once and written once per layer, FP32
-    # outputs). At these shapes the prediction is HBM-bound: 0.55 TFLOP against 4.4 KB per row.
+    # Algorithmic work of one prediction (128 Fourier features -> 256, three 256 -> 256 layers,
+    # 256 -> 2 outputs): 2 M N K FLOPs. The fused kernel keeps the activations on chip, so HBM
+    # carries 16 bytes per row (two FP32 inputs, two FP32 outputs); the bound is the tensor
+    # pipe and the epilogue's BF16 / GELU work beside it.
     flops = 2.0 * rows * (128 * 256 + 3 * 256 * 256 + 256 * 2)
-    bytes_ = rows * ((128 + 3 * 256 + 256) * 2 + 4 * 256 * 2 + 2 * 4)
+    bytes_ = rows * 16
     ms = min(pred[1:])
     peaks = measured_peaks()
     out = {"predict_rows": rows, "predict_ms": ms, "train_step_ms": min(fit),
-           "predict_gemm_tflops": flops / (ms * 1e-3) / 1e12, "predict_gbs": bytes_ / (ms * 1e-3) / 1e9,
-           "predict_bytes": bytes_, "loss": float(loss)}
-    if peaks.get("hbm_gbs"):
-        out["roofline"] = {"bound": "hbm", "achieved": out["predict_gbs"], "peak": peaks["hbm_gbs"], "unit": "GB/s",
-                           "frac": out["predict_gbs"] / peaks["hbm_gbs"],
-                           "peak_source": "MEASURED_PEAKS.json hbm_gbs (of measured)"}
+           "predict_tflops": flops / (ms * 1e-3) / 1e12, "predict_hbm_bytes": bytes_,
+           "predict_rows_per_s": rows / (ms * 1e-3), "loss": float(loss)}
+    if peaks.get("bf16_tflops"):
+        out["roofline"] = {"bound": "tensor", "achieved": out["predict_tflops"], "peak": peaks["bf16_tflops"],
+                           "unit": "TFLOP/s", "frac": out["predict_tflops"] / peaks["bf16_tflops"],
+                           "peak_source": "MEASURED_PEAKS.json bf16_tflops (burst, of measured)"}
     return out
 
 
@@ -440,7 +440,7 @@ def _timed(fn, reps=1):
     return out, t
 
 
-OTHER_CONFIGS = ("bif", "spectrum", "basins", "bif2d", "basins_dbscan")
+OTHER_CONFIGS = ("bif", "spectrum", "ls_fixed", "basins", "bif2d", "basins_dbscan", "recluster")
 
 
 def run_other_configs(eng, which=OTHER_CONFIGS, args=None):
@@ -535,6 +535,29 @@ def run_other_configs(eng, which=OTHER_CONFIGS, args=None):
             "rhs_evals_per_s": res.steps / (res.kernel_ms * 1e-3), "valid_cells": int(ok.sum()),
             "median_spectrum": [float(np.median(v[k][ok])) for k in range(4)],
             "median_sum": float(np.median(v[:, ok].sum(axis=0)))}
+    # The reference's spectrum method (run_ls_2d: fixed-step RK4, Gram-Schmidt of the four
+    # tangent vectors every NT) on the hyper-chaotic window (0.25, 0.05) +- (0.01, 0.005) of
+    # the same system, 256 x 256 cells, h = 0.01, 10 transient + 100 measured time units.
+    for name, opt in (("plain_fp64_exact", dict(precision=ucb.PREC_F64, mode=ucb.MODE_EXACT)),
+                      ("plain_fp64_native", dict(precision=ucb.PREC_F64, mode=ucb.MODE_NATIVE)),
+                      ("fp32_native", dict(precision=ucb.PREC_F32, mode=ucb.MODE_NATIVE))):
+        if "ls_fixed" not in which:
+            break
+
+        def lfreq(n):
+            return ucb.Engine.ls2d_request(hb, 4, (-10.0, -6.0, 0.0, 10.0), (0, 0.25, 0.05), method=ucb.LS_FIXED,
+                                           n_pts=n, param_index=1, param_index_2=2, param_lo=0.24, param_hi=0.26,
+                                           param_lo_2=0.045, param_hi_2=0.055, h=0.01, transient_time=10.0,
+                                           t_max=100.0, NT=0.1, eps=1e-6, opt=ucb.options(**opt))
+        eng.run_ls2d(lfreq(8))
+        (vals, flags, res), ms = _timed(lambda: eng.run_ls2d(lfreq(256)))
+        v = vals.reshape(4, -1)
+        ok = flags == 1
+        out.setdefault("ls_fixed_hyper_rossler_256", {})[name] = {
+            "wall_ms": ms, "kernel_ms": res.kernel_ms, "cells_per_s": 256 * 256 / (res.kernel_ms * 1e-3),
+            "rk4_steps_per_s": res.steps / (res.kernel_ms * 1e-3), "valid_cells": int(ok.sum()),
+            "finite_cells": int((ok & np.isfinite(v).all(axis=0)).sum()),
+            "median_spectrum": [float(np.median(v[k][ok & np.isfinite(v[k])])) for k in range(4)]}
     # Forced Duffing basins: 4096 x 4096 initial conditions (x, x') in [-2.5, 2.5]^2,
     # RK4 h = 2 pi / 200, 20 consecutive period matches to 1e-6, 2,000-period cap.
     db = rk4_body(DUFFING)
@@ -603,13 +626,35 @@ def run_other_configs(eng, which=OTHER_CONFIGS, args=None):
             "oscillating_clusters": res.n_clusters, "fixed_point_clusters": -res.min_cluster_idx,
             "classes": {str(k): int((cls == k).sum()) for k in (-1, 0, 1)}}
         if name == "plain_fp64_native":
-            ref_bd = (lab, f1, f2)
+            ref_bd = (lab, f1, f2, cls)
         else:
             def rel(a, b):
                 return float(np.median(np.abs(a - b) / np.maximum(np.abs(b), 1e-300)))
             out[f"basins_dbscan_duffing_{nd}"]["fp32_vs_fp64"] = {
                 "label_agreement": float((lab == ref_bd[0]).mean()),
                 "feature1_median_rel_diff": rel(f1, ref_bd[1]), "feature2_median_rel_diff": rel(f2, ref_bd[2])}
+    # The DBSCAN alone (run_basins_recluster) over 1024 x 1024 cells: the FP64 features of the
+    # reference-method basins above when they ran, else seeded synthetic features (uniform on
+    # [-5, 5]^2, classes -1 / 0 / 1 in proportions 1:1:2); eps 0.5 and 0.25, best of 3 each.
+    if "recluster" in which:
+        nr = 1024
+        if "basins_dbscan" in which and (args.basins_dbscan_n if args else 1024) == nr:
+            f1r, f2r, clr = ref_bd[1], ref_bd[2], ref_bd[3]
+            src = "features of the FP64 reference-method basins (1024 x 1024)"
+        else:
+            rng = np.random.default_rng(0)
+            f1r, f2r = rng.uniform(-5, 5, nr * nr), rng.uniform(-5, 5, nr * nr)
+            clr = rng.choice([-1, 1, 1, 0], nr * nr).astype(np.int32)
+            src = "synthetic uniform features on [-5, 5]^2, seed 0"
+        rec = {"cells": nr * nr, "features": src}
+        for eps in (0.5, 0.25):
+            best = None
+            for _ in range(3):
+                labr, rres = eng.run_basins_recluster(db, 3, nr, eps, f1r, f2r, clr)
+                best = rres.cluster_ms if best is None else min(best, rres.cluster_ms)
+            rec[f"eps_{eps}"] = {"cluster_ms": best, "cells_per_s": nr * nr / (best * 1e-3),
+                                 "oscillating_clusters": rres.n_clusters, "fixed_point_clusters": -rres.min_cluster_idx}
+        out["basins_recluster_1024"] = rec
     return out
 
 

@@ -108,6 +108,13 @@ typedef struct ucb_tune_report {
     int32_t from_table;        /* 1: found in the tuned table, nothing timed */
     char key[32];              /* kernel build identity (hash) */
     char error[256];
+    /* When the trial's winner is not the default shape, both are timed again on a
+     * confirmation workload (the request itself when one run of it takes about a second or
+     * less, else its window at the full horizon on a smaller grid); the winner is kept only if
+     * it still wins by 2 %. 0 when no confirmation ran. */
+    double confirm_default_ms, confirm_best_ms;
+    int32_t confirm_n_pts;
+    int32_t pad0;
 } ucb_tune_report;
 
 /* Creates an engine bound to CUDA device `device` (the reference always uses device 0,

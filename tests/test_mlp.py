@@ -122,6 +122,37 @@ def test_gpu_prediction_matches_oracle(ucb_engine):
 
 
 @pytest.mark.gpu
+@pytest.mark.parametrize("n", [1, 127, 129, 40000])
+def test_gpu_fused_prediction_matches_oracle_at_the_surrogate_size(ucb_engine, n):
+    """The fused prediction kernel (features, hidden layers and output of a 128-row tile in
+    one CTA, activations in shared memory) on the surrogate's network (64 Fourier features,
+    4 x 256 GELU): ragged row counts, and at 40,000 rows (313 tiles) every CTA runs a second
+    pair of tiles with one slot empty at the end."""
+    import torch
+    import ucb
+    net = ucb.Mlp(ucb_engine, fourier=64, hidden=256, layers=4, fourier_scale=2.0, seed=11, batch=1024,
+                  train_steps=1)
+    rng = np.random.default_rng(n)
+    p = _rand_params(rng, 64, 256, 4, scale=0.8)
+    net.set_params(p.astype(np.float32))
+    net.set_target_scale(0.3, 1.5)
+    u = rng.uniform(size=(n, 2)).astype(np.float32)
+    du = torch.from_numpy(u).cuda()
+    dm = torch.full((n + 1,), 7.0, device="cuda")
+    ds = torch.full((n + 1,), 7.0, device="cuda")
+    net.predict(du.data_ptr(), n, dm.data_ptr(), ds.data_ptr())
+    torch.cuda.synchronize()
+    m_ref, s_ref = MO.predict(net.get_params(), net.fourier(), u, 256, 4, y_mean=0.3, y_std=1.5)
+    m, s = dm.cpu().numpy(), ds.cpu().numpy()
+    assert m[n] == 7.0 and s[n] == 7.0  # nothing written past the last row
+    scale = np.abs(m_ref).max()
+    assert np.max(np.abs(m[:n] - m_ref)) < 1e-2 * scale + 1e-5
+    assert np.mean(np.abs(m[:n] - m_ref)) < 1e-3 * scale + 1e-6
+    assert np.max(np.abs(s[:n] / s_ref - 1)) < 1e-2
+    net.close()
+
+
+@pytest.mark.gpu
 def test_gpu_training_fits_smooth_function(ucb_engine):
     import torch
     import ucb

@@ -165,7 +165,8 @@ bool tune_request(ucb_engine* e, const ucb_options& o, int default_block, Compil
 
 int autotune_search(ucb_engine* e, const std::string& key, int default_block, bool force,
                     const std::function<double(const TuneConfig&)>& trial,
-                    const std::function<CompileRequest(const TuneConfig&)>& build, ucb_tune_report* rep) {
+                    const std::function<CompileRequest(const TuneConfig&)>& build, ucb_tune_report* rep,
+                    const std::function<double(const TuneConfig&)>& confirm) {
     const auto t0 = std::chrono::steady_clock::now();
     std::memset(rep, 0, sizeof *rep);
     std::snprintf(rep->key, sizeof rep->key, "%s", key.c_str());
@@ -249,6 +250,21 @@ int autotune_search(ucb_engine* e, const std::string& key, int default_block, bo
                     ++found;
                 }
             }
+        }
+    }
+    TuneConfig dflt;
+    dflt.block = default_block;
+    if (confirm && !(best == dflt)) {
+        auto twice = [&](const TuneConfig& c) {
+            const double a = confirm(c), b = confirm(c);
+            return (a < 0 || b < 0) ? -1.0 : std::min(a, b);
+        };
+        const double dm = twice(dflt), bm = twice(best);
+        rep->confirm_default_ms = dm;
+        rep->confirm_best_ms = bm;
+        if (!(dm > 0 && bm > 0 && bm < 0.98 * dm)) {
+            best = dflt;
+            best_ms = rep->default_ms;
         }
     }
     store(e, key, best, best_ms);

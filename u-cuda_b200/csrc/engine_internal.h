@@ -126,9 +126,13 @@ bool tune_request(ucb_engine* e, const ucb_options& o, int default_block, Compil
 // kernel milliseconds (< 0: the shape failed); `build` gives the compile request of a
 // shape (for the register count and occupancy of the chosen build). The best shape is
 // stored for `key` (engine + on-disk table). force = false returns a stored shape as is.
+// `confirm` (optional) times a shape on a workload closer to the real run; when the trial's
+// winner is not the default shape, it must also win there by 2 % to be kept (a short trial
+// can rank shapes differently from a full-horizon run).
 int autotune_search(ucb_engine* e, const std::string& key, int default_block, bool force,
                     const std::function<double(const TuneConfig&)>& trial,
-                    const std::function<CompileRequest(const TuneConfig&)>& build, ucb_tune_report* rep);
+                    const std::function<CompileRequest(const TuneConfig&)>& build, ucb_tune_report* rep,
+                    const std::function<double(const TuneConfig&)>& confirm = nullptr);
 
 // Horizon factor of an autotuning trial: about `target_steps` steps over `cells` cells of
 // `steps_per_cell` steps each (1 when the request is already that small).

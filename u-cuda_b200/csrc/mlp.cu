@@ -1,21 +1,26 @@
-// BF16 MLP surrogate: tcgen05 tensor-core GEMMs, elementwise kernels and the training /
-// prediction host code (no reference counterpart).
+// BF16 MLP surrogate: tcgen05 tensor-core GEMMs, the fused prediction kernel, elementwise
+// kernels and the training / prediction host code (no reference counterpart).
 //
-// GEMM: C[M, N] = A[M, K] B[N, K]^T with A and B K-contiguous ("TN"), M % 128 == 0,
-// N % 128 == 0, K % 64 == 0. A persistent kernel (one CTA of 192 threads per SM) walks
-// tiles of 128 x 256 (128 x 128 when N is not a multiple of 256, so A is read once per row
-// block either way) and K splits: warp 0 streams 64-wide K chunks of A and B with TMA
-// (128-byte swizzle, no multicast) into a ring of shared-memory stages, warp 1 issues
-// tcgen05.mma (CuTe SM100_MMA_F16BF16_SS, cta_group::1, BF16 x BF16 -> FP32) from one
-// elected lane into one of two TMEM accumulators, and warps 2-5 read a finished
-// accumulator with tcgen05.ld (one 32-lane TMEM quadrant each; thread t owns row t) while
-// the next tile's MMAs run, apply bias / GELU and store FP32, BF16 and / or transposed BF16
-// copies straight from registers. Waits are bounded; on a timeout the kernel records an
-// error, waits for its own copies and MMAs, frees TMEM and returns. A split-K launch stores
-// each split's partial tile in its own slice of a buffer, and a second kernel adds the
-// slices in split order (so a training step gives the same bits every time it runs).
-// Backward products are the same TN GEMM on transposed
-// copies, which the forward epilogue and the GELU-backward kernel write as they go.
+// GEMM (training): C[M, N] = A[M, K] B[N, K]^T with A and B K-contiguous ("TN"),
+// M % 128 == 0, N % 128 == 0, K % 64 == 0. A persistent kernel (one CTA of 320 threads per
+// SM) walks tiles of 128 x 256 or 128 x 128 (the narrower tile when N is not a multiple of
+// 256 or when the wide tiles would leave SMs idle) and K splits: warp 0 streams 64-wide K
+// chunks of A and B with TMA (128-byte swizzle, no multicast) into a ring of shared-memory
+// stages, warp 1 issues tcgen05.mma (CuTe SM100_MMA_F16BF16_SS, cta_group::1, BF16 x BF16
+// -> FP32) from one elected lane into one of two TMEM accumulators, and warps 2-9 read a
+// finished accumulator with tcgen05.ld (two warps per 32-lane TMEM quadrant, one half of
+// the columns each; thread t of a quadrant owns row t) while the next tile's MMAs run,
+// apply bias / GELU and store FP32, BF16 and / or transposed BF16 copies straight from
+// registers. Waits are bounded; on a timeout the kernel records an error, waits for its
+// own copies and MMAs, frees TMEM and returns. A split-K launch stores each split's partial
+// tile in its own slice of a buffer, and a second kernel adds the slices in split order (so
+// a training step gives the same bits every time it runs). Backward products are the same
+// TN GEMM on transposed copies, which the forward epilogue and the GELU-backward kernel
+// write as they go.
+//
+// Prediction: one fused kernel per call (mlp_infer_kernel) runs features, every hidden
+// layer and the output transform of a 128-row tile inside one CTA, with the activations in
+// shared memory; HBM sees the inputs and the two outputs per row only.
 #include <cuda.h>
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
@@ -48,7 +53,9 @@ using bf16 = cutlass::bfloat16_t;
 constexpr int kBM = 128;   // rows of a tile (UMMA M, one TMEM lane per row)
 constexpr int kBK = 64;    // K per pipeline stage: one 128-byte swizzle row of BF16
 constexpr long long kWaitLimit = 1LL << 22;  // try_wait polls before a wait gives up
-constexpr int kGemmThreads = 192;  // warp 0 TMA, warp 1 MMA, warps 2-5 epilogue
+constexpr int kEpiWarps = 8;      // two per 32-lane TMEM quadrant, each half of the columns
+constexpr int kGemmThreads = 64 + 32 * kEpiWarps;  // warp 0 TMA, warp 1 MMA, warps 2-9 epilogue
+constexpr int kMaxLayers = 9;     // hidden layers + the output layer
 
 // Shapes and shared-memory layout of the persistent GEMM for a tile width BN (128 or 256).
 template <int BN>
@@ -76,13 +83,32 @@ struct Epilogue {
     int gelu;           // outh / outt receive GELU(v) instead of v
     float* outf;        // FP32 result (pre-activation), row stride ldf
     int ldf;
-    int atomic;         // split-K: the host redirects outf to a partial-tile buffer
+    int atomic;         // split-K: outf is a buffer of partial tiles, one slice per K split
     long long split_stride;  // floats between the slices of consecutive splits
     bf16* outh;         // BF16 copy, row stride ldh
     int ldh;
     bf16* outt;         // BF16 transposed copy outt[n * ldt + m]
     int ldt;
     int m_store, n_store;  // only rows m < m_store and columns n < n_store are stored
+    // backward through GELU: the product is dL/dH of a hidden layer; outh / outt receive
+    // dZ = dL/dH GELU'(Z) with Z = zin (FP32, row stride ldz)
+    const float* zin;
+    int ldz;
+    // sums over each 32-row block of the BF16 values stored to outh / outt (the bias gradient
+    // of dZ): colsum[(m / 32) ldc + n]
+    float* colsum;
+    int ldc;
+    // output layer of a training batch (columns 0 = mean, 1 = log-variance): the beta-NLL
+    // against the standardised targets yb of the first n_valid of `rows` rows -> dout (row
+    // stride 64, columns 0 and 1), doutT (rows 0 and 1 of a [128, rows] matrix), and per
+    // 32-row block the sums of the two BF16 gradients and of the loss in blk[3 (m / 32) + 0..2]
+    int nll;
+    const float* yb;
+    int n_valid, rows;
+    float beta;
+    bf16* dout;
+    bf16* doutT;
+    float* blk;
 };
 
 // Work of one launch: items are (M tile, N tile, K split) triples, handed out round robin
@@ -136,9 +162,15 @@ __device__ __forceinline__ float tanh_hw(float x) {
 }
 constexpr float kGeluC0 = 0.7978845608028654f;  // sqrt(2 / pi)
 constexpr float kGeluC1 = 0.044715f;
-__device__ __forceinline__ float gelu(float z) {
-    const float t = tanh_hw(kGeluC0 * fmaf(kGeluC1 * z * z, z, z));
-    return 0.5f * z * (1.0f + t);
+// Two GELUs in packed FP32 pairs (fma / mul .f32x2: half the FP32 issue slots), the form
+// both training and prediction use: h + h tanh(c0 (z + c1 z^3)) with h = z / 2.
+__device__ __forceinline__ float2 gelu2(float2 z) {
+    const float2 z2 = __fmul2_rn(z, z);
+    const float2 u = __ffma2_rn(__fmul2_rn(z2, make_float2(kGeluC1, kGeluC1)), z, z);
+    const float2 w = __fmul2_rn(u, make_float2(kGeluC0, kGeluC0));
+    const float2 t = make_float2(tanh_hw(w.x), tanh_hw(w.y));
+    const float2 h = __fmul2_rn(z, make_float2(0.5f, 0.5f));
+    return __ffma2_rn(h, t, h);
 }
 __device__ __forceinline__ float gelu_grad(float z) {
     const float z2 = z * z;
@@ -146,13 +178,79 @@ __device__ __forceinline__ float gelu_grad(float z) {
     return 0.5f * (1.0f + t) + 0.5f * z * (1.0f - t * t) * kGeluC0 * fmaf(3.0f * kGeluC1, z2, 1.0f);
 }
 
+// Sums over the 32 lanes of a warp of each of the 32 values v[0..31] (lane = one row):
+// five exchange rounds in a fixed order (each round hands half of a lane's partial sums to
+// the partner lane), after which lane l holds the sum of column l in v[returned index].
+__device__ __forceinline__ int column_sums32(float (&v)[32]) {
+    const int lane = threadIdx.x & 31;
+#pragma unroll
+    for (int w = 16; w >= 1; w >>= 1) {
+        const bool upper = (lane & w) != 0;
+#pragma unroll
+        for (int j = 0; j < w; ++j) {
+            const float send = upper ? v[j] : v[j + w];
+            const float keep = upper ? v[j + w] : v[j];
+            v[j] = keep + __shfl_xor_sync(0xffffffffu, send, w);
+        }
+    }
+    return 0;
+}
+
+// Beta-NLL of one output row (mean mu, log-variance lv_raw) of a training batch, the
+// gradients dout / doutT, and the fixed-order sums over the warp's 32 rows into blk.
+__device__ __forceinline__ void nll_rows(const Epilogue& ep, int r, float mu, float lv_raw) {
+    float g0 = 0.f, g1 = 0.f, l = 0.f;
+    if (r < ep.rows && r < ep.n_valid) {
+        const float lv = fminf(fmaxf(lv_raw, -16.f), 16.f);
+        const float iv = expf(-lv);
+        const float d = mu - ep.yb[r];
+        const float w = ep.beta > 0.f ? expf(ep.beta * lv) : 1.f;  // constant weight sigma^(2 beta)
+        const float inv_n = 1.f / (float)ep.n_valid;
+        l = w * 0.5f * (lv + d * d * iv) * inv_n;
+        g0 = w * d * iv * inv_n;
+        g1 = (lv_raw == lv) ? w * 0.5f * (1.f - d * d * iv) * inv_n : 0.f;
+    }
+    const bf16 b0 = bf16(g0), b1 = bf16(g1);
+    if (r < ep.rows) {
+        ep.dout[(size_t)r * 64] = b0;
+        ep.dout[(size_t)r * 64 + 1] = b1;
+        ep.doutT[r] = b0;
+        ep.doutT[(size_t)ep.rows + r] = b1;
+    }
+    float s0 = float(b0), s1 = float(b1), sl = l;
+#pragma unroll
+    for (int w = 16; w >= 1; w >>= 1) {
+        s0 += __shfl_xor_sync(0xffffffffu, s0, w);
+        s1 += __shfl_xor_sync(0xffffffffu, s1, w);
+        sl += __shfl_xor_sync(0xffffffffu, sl, w);
+    }
+    if ((threadIdx.x & 31) == 0) {
+        ep.blk[3 * (r >> 5)] = s0;
+        ep.blk[3 * (r >> 5) + 1] = s1;
+        ep.blk[3 * (r >> 5) + 2] = sl;
+    }
+}
+
 // One 32-column chunk of one accumulator row (this thread's) through the epilogue: bias,
 // the FP32 / BF16 / transposed BF16 stores. v: the raw accumulator values.
 __device__ __forceinline__ void epilogue_chunk(const Epilogue& ep, float* outf, int m, int n0, float (&v)[32]) {
     if (ep.bias) {
+        if (n0 + 32 <= ep.nb && (reinterpret_cast<uintptr_t>(ep.bias + n0) & 15) == 0) {
+            // every lane reads the same 32 values: eight broadcast 16-byte loads
+            const float4* b4 = reinterpret_cast<const float4*>(ep.bias + n0);
 #pragma unroll
-        for (int j = 0; j < 32; ++j)
-            if (n0 + j < ep.nb) v[j] += __ldg(ep.bias + n0 + j);
+            for (int q = 0; q < 8; ++q) {
+                const float4 b = __ldg(b4 + q);
+                v[4 * q] += b.x;
+                v[4 * q + 1] += b.y;
+                v[4 * q + 2] += b.z;
+                v[4 * q + 3] += b.w;
+            }
+        } else {
+#pragma unroll
+            for (int j = 0; j < 32; ++j)
+                if (n0 + j < ep.nb) v[j] += __ldg(ep.bias + n0 + j);
+        }
     }
     const bool row_ok = m < ep.m_store;
     const bool full = n0 + 32 <= ep.n_store;
@@ -168,10 +266,36 @@ __device__ __forceinline__ void epilogue_chunk(const Epilogue& ep, float* outf, 
                 if (n0 + j < ep.n_store) p[j] = v[j];
         }
     }
+    if (ep.nll && n0 == 0) nll_rows(ep, m, v[0], v[1]);
     if (!ep.outh && !ep.outt) return;
     float g[32];
+    if (ep.zin) {
+        if (row_ok && full && (ep.ldz & 3) == 0) {
+            const float4* z4 = reinterpret_cast<const float4*>(ep.zin + (size_t)m * ep.ldz + n0);
 #pragma unroll
-    for (int j = 0; j < 32; ++j) g[j] = ep.gelu ? gelu(v[j]) : v[j];
+            for (int q = 0; q < 8; ++q) {
+                const float4 z = __ldg(z4 + q);
+                g[4 * q] = v[4 * q] * gelu_grad(z.x);
+                g[4 * q + 1] = v[4 * q + 1] * gelu_grad(z.y);
+                g[4 * q + 2] = v[4 * q + 2] * gelu_grad(z.z);
+                g[4 * q + 3] = v[4 * q + 3] * gelu_grad(z.w);
+            }
+        } else {
+#pragma unroll
+            for (int j = 0; j < 32; ++j)
+                g[j] = (row_ok && n0 + j < ep.n_store) ? v[j] * gelu_grad(ep.zin[(size_t)m * ep.ldz + n0 + j]) : 0.f;
+        }
+    } else if (ep.gelu) {
+#pragma unroll
+        for (int j = 0; j < 32; j += 2) {
+            const float2 q = gelu2(make_float2(v[j], v[j + 1]));
+            g[j] = q.x;
+            g[j + 1] = q.y;
+        }
+    } else {
+#pragma unroll
+        for (int j = 0; j < 32; ++j) g[j] = v[j];
+    }
     if (ep.outh && row_ok) {
         bf16* p = ep.outh + (size_t)m * ep.ldh + n0;
         if (full && (ep.ldh & 7) == 0 && (reinterpret_cast<uintptr_t>(ep.outh) & 15) == 0) {
@@ -198,13 +322,22 @@ __device__ __forceinline__ void epilogue_chunk(const Epilogue& ep, float* outf, 
         for (int j = 0; j < 32; ++j)
             if (n0 + j < ep.n_store) ep.outt[(size_t)(n0 + j) * ep.ldt + m] = bf16(g[j]);
     }
+    if (ep.colsum) {
+        // column sums over the warp's 32 rows of the BF16-rounded values (rows past m_store
+        // add 0): a fixed butterfly that leaves column n0 + lane in lane `lane`
+#pragma unroll
+        for (int j = 0; j < 32; ++j) g[j] = row_ok ? float(bf16(g[j])) : 0.f;
+        const int s = column_sums32(g);
+        if (n0 + (threadIdx.x & 31) < ep.n_store)
+            ep.colsum[(size_t)(m >> 5) * ep.ldc + n0 + (threadIdx.x & 31)] = g[s];
+    }
 }
 
 // C = A B^T, A [M, K] and B [N, K] K-contiguous BF16, FP32 accumulation in TMEM.
 // Persistent and warp-specialised: warp 0 streams K chunks of A and B into a ring of
 // shared-memory stages with TMA (128-byte swizzle, the layout the MMA descriptors read),
 // warp 1 issues tcgen05.mma from one elected lane into one of two TMEM accumulators and
-// commits to the stage's and the accumulator's mbarriers, warps 2-5 (one per 32-lane TMEM
+// commits to the stage's and the accumulator's mbarriers, warps 2-9 (two per 32-lane TMEM
 // quadrant) read finished accumulators with tcgen05.ld, run the epilogue and hand the
 // accumulator back, so the epilogue of one tile overlaps the MMAs of the next. Every wait
 // is bounded; on a timeout the CTA records an error, stops, waits (bounded) for its own
@@ -237,7 +370,7 @@ __global__ void __launch_bounds__(kGemmThreads, 1)
         }
         for (int b = 0; b < 2; ++b) {
             mbar_init(accf_bar(b), 1);
-            mbar_init(acce_bar(b), 4);
+            mbar_init(acce_bar(b), kEpiWarps);
         }
         mbar_init(drain_bar, 1);
         *abort_flag = 0;
@@ -343,8 +476,9 @@ __global__ void __launch_bounds__(kGemmThreads, 1)
         cutlass::arch::umma_arrive(bars + 2 * S + 4);
         if (!mbar_wait_bounded(drain_bar, 0)) fail();
     } else {
-        // ---- epilogue: warp 2..5 reads TMEM lanes 32 (warp % 4) .. + 31
-        const int quad = warp & 3;
+        // ---- epilogue: warp w reads TMEM lanes 32 (w % 4) .. + 31 (the lanes its quadrant may
+        // access) and, with (w - 2) / 4, one half of the columns
+        const int quad = warp & 3, half = (warp - 2) >> 2;
         const int row = quad * 32 + lane;
         int buf = 0;
         uint32_t acc_phase = 0;
@@ -360,7 +494,7 @@ __global__ void __launch_bounds__(kGemmThreads, 1)
             const int m = tm * kBM + row;
             const uint32_t taddr = tmem_base + (uint32_t)(buf * BN) + ((uint32_t)(quad * 32) << 16);
 #pragma unroll 1
-            for (int c0 = 0; c0 < BN; c0 += 32) {
+            for (int c0 = half * (BN / 2); c0 < (half + 1) * (BN / 2); c0 += 32) {
                 uint32_t r[32];
                 asm volatile("tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15, %16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31}, [%32];\n"
                              : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]), "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]), "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
@@ -415,16 +549,27 @@ __device__ __forceinline__ unsigned long long mix64(unsigned long long z) {
     return z ^ (z >> 31);
 }
 
-__device__ __forceinline__ void input_point(const FeatureArgs& a, long long i, float& u0, float& u1) {
-    if (a.u) {
-        u0 = a.u[2 * i];
-        u1 = a.u[2 * i + 1];
+__device__ __forceinline__ void input_point(const float* u, const long long* cells, int grid_n, long long i,
+                                            float& u0, float& u1) {
+    if (u) {
+        u0 = u[2 * i];
+        u1 = u[2 * i + 1];
     } else {
-        const long long c = a.cells ? a.cells[i] : i;
-        const float inv = a.grid_n > 1 ? 1.0f / (float)(a.grid_n - 1) : 0.0f;
-        u0 = (float)(c % a.grid_n) * inv;
-        u1 = (float)(c / a.grid_n) * inv;
+        const long long c = cells ? cells[i] : i;
+        const float inv = grid_n > 1 ? 1.0f / (float)(grid_n - 1) : 0.0f;
+        u0 = (float)(c % grid_n) * inv;
+        u1 = (float)(c / grid_n) * inv;
     }
+}
+__device__ __forceinline__ void input_point(const FeatureArgs& a, long long i, float& u0, float& u1) {
+    input_point(a.u, a.cells, a.grid_n, i, u0, u1);
+}
+
+// Phase 2 pi (u0 B[2j] + u1 B[2j+1]) of frequency j, rounded in one fixed order (no
+// contraction left to the compiler), so that the training batches and the fused prediction
+// see the same features.
+__device__ __forceinline__ float feature_phase(float u0, float u1, const float* Bf, int j) {
+    return __fmul_rn(6.283185307179586f, __fmaf_rn(u0, __ldg(Bf + 2 * j), __fmul_rn(u1, __ldg(Bf + 2 * j + 1))));
 }
 
 // One thread per (row, frequency): X[r, j] = sin(2 pi u.B_j), X[r, F/2 + j] = cos(...).
@@ -447,8 +592,7 @@ __global__ void features_kernel(FeatureArgs a) {
     if (valid) {
         float u0, u1;
         input_point(a, i, u0, u1);
-        const float ph = 6.283185307179586f * (u0 * a.Bf[2 * j] + u1 * a.Bf[2 * j + 1]);
-        sincosf(ph, &s, &c);
+        sincosf(feature_phase(u0, u1, a.Bf, j), &s, &c);
     }
     const int F = 2 * a.fourier;
     a.X[(size_t)r * F + j] = bf16(s);
@@ -460,126 +604,104 @@ __global__ void features_kernel(FeatureArgs a) {
     if (j == 0 && a.yb) a.yb[r] = valid ? (a.y[i] - a.y_mean) * a.y_inv_std : 0.f;
 }
 
-// Gaussian NLL of the standardised target with beta weighting. out: rows x 2 (mean,
-// log-variance). Writes dOut (rows x 64, columns >= 2 stay zero), dOut^T rows 0 and 1
-// (128 x rows, other rows stay zero), and per block the sums of the two output-layer bias
-// gradients and of the loss into blk[3 blockIdx.x + 0..2] (added in block order by
-// ordered_sum_kernel).
-__global__ void nll_kernel(const float* out, const float* yb, int rows, int n_valid, float beta, bf16* dout,
-                           bf16* doutT, float* blk) {
-    const int r = blockIdx.x * blockDim.x + threadIdx.x;
-    float g0 = 0.f, g1 = 0.f, l = 0.f;
-    if (r < rows && r < n_valid) {
-        const float mu = out[2 * r];
-        const float lv_raw = out[2 * r + 1];
-        const float lv = fminf(fmaxf(lv_raw, -16.f), 16.f);
-        const float iv = expf(-lv);
-        const float d = mu - yb[r];
-        const float w = beta > 0.f ? expf(beta * lv) : 1.f;  // constant weight sigma^(2 beta)
-        const float inv_n = 1.f / (float)n_valid;
-        l = w * 0.5f * (lv + d * d * iv) * inv_n;
-        g0 = w * d * iv * inv_n;
-        g1 = (lv_raw == lv) ? w * 0.5f * (1.f - d * d * iv) * inv_n : 0.f;
-    }
-    if (r < rows) {
-        dout[(size_t)r * 64] = bf16(g0);
-        dout[(size_t)r * 64 + 1] = bf16(g1);
-        doutT[r] = bf16(g0);
-        doutT[(size_t)rows + r] = bf16(g1);
-    }
-    // block sums of the (BF16-rounded, as the GEMMs see them) bias gradients and the loss
-    __shared__ float s0[256], s1[256], sl[256];
-    s0[threadIdx.x] = float(bf16(g0));
-    s1[threadIdx.x] = float(bf16(g1));
-    sl[threadIdx.x] = l;
-    __syncthreads();
-    for (int w = blockDim.x / 2; w > 0; w >>= 1) {
-        if (threadIdx.x < w) {
-            s0[threadIdx.x] += s0[threadIdx.x + w];
-            s1[threadIdx.x] += s1[threadIdx.x + w];
-            sl[threadIdx.x] += sl[threadIdx.x + w];
-        }
-        __syncthreads();
-    }
-    if (threadIdx.x == 0) {
-        blk[3 * blockIdx.x] = s0[0];
-        blk[3 * blockIdx.x + 1] = s1[0];
-        blk[3 * blockIdx.x + 2] = sl[0];
-    }
-}
+// Gradient of a run of parameters as fixed-order sums of partial results: parameter off + e
+// (row o = e / cols, column c = e % cols) has the gradient
+//   sum over sp = 0 .. slices - 1, in that order, of part[sp * slice_stride + o * ld + c].
+// Weight runs read the split-K slices of their weight-gradient GEMM, bias runs the per-32-row
+// block sums of the epilogues (rows = 1). layer >= 0: a weight run whose BF16 copies
+// (W, W^T) are rewritten after the update.
+struct GradRun {
+    long long off, count;
+    int cols, ld;
+    const float* part;
+    long long slice_stride;
+    int slices, layer;
+};
 
-// out[j] = sum over i = 0 .. count - 1, in that order, of part[i * stride + j] (j < width):
-// the fixed-order reduction of partial sums (split-K tiles, per-block bias gradients).
-__global__ void ordered_sum_kernel(const float* part, int count, long long stride, long long width, float* out) {
-    for (long long j = (long long)blockIdx.x * blockDim.x + threadIdx.x; j < width;
-         j += (long long)gridDim.x * blockDim.x) {
-        float s = 0.f;
-        for (int i = 0; i < count; ++i) s += part[(size_t)i * stride + j];
-        out[j] = s;
-    }
-}
-
-// dZ = dH * GELU'(Z) -> BF16 dZ (rows x N) and dZ^T (N x rows); dbp[blockIdx.y * N + c] =
-// the sum over this block's 32 rows of dZ[r, c] (of the BF16-rounded values the GEMMs
-// use), added in block order by ordered_sum_kernel. Block 32 x 8 over a 32 x 32 tile.
-__global__ void gelu_back_kernel(const float* dH, const float* Z, int rows, int N, bf16* dZ, bf16* dZt, float* dbp) {
-    __shared__ float tile[32][33];
-    const int c0 = blockIdx.x * 32, r0 = blockIdx.y * 32;
-    const int tx = threadIdx.x, ty = threadIdx.y;
-    for (int k = 0; k < 32; k += 8) {
-        const int r = r0 + ty + k, c = c0 + tx;
-        float v = 0.f;
-        if (r < rows && c < N) {
-            const bf16 b = bf16(dH[(size_t)r * N + c] * gelu_grad(Z[(size_t)r * N + c]));
-            dZ[(size_t)r * N + c] = b;
-            v = float(b);
-        }
-        tile[ty + k][tx] = v;
-    }
-    __syncthreads();
-    for (int k = 0; k < 32; k += 8) {
-        const int c = c0 + ty + k, r = r0 + tx;
-        if (c < N && r < rows) dZt[(size_t)c * rows + r] = bf16(tile[tx][ty + k]);
-    }
-    if (ty == 0 && c0 + tx < N) {
-        float s = 0.f;
-        for (int k = 0; k < 32; ++k) s += tile[k][tx];
-        dbp[(size_t)blockIdx.y * N + c0 + tx] = s;
-    }
-}
-
-// Adam with cosine learning-rate decay; the step counter lives on the device so that a
-// captured training step replays unchanged.
+// One training step's optimiser: every parameter's gradient from its partial sums (the same
+// bits whatever the launch order of the backward kernels), Adam with cosine learning-rate
+// decay, and the BF16 copies of the updated weights (W for the forward products, W^T for the
+// backward ones). Thread n_params adds up the loss. update = 0: only the gradient is written
+// (to grad) and the loss; nothing else changes. The step counter lives on the device so that
+// a captured step replays unchanged; the last block to finish advances it, after every
+// block has read it.
 struct AdamArgs {
     float* w;
-    const float* g;
     float* m;
     float* v;
+    float* grad;  // optional copy of the gradient
     long long n;
-    const unsigned long long* step;
+    GradRun run[2 * kMaxLayers];
+    int n_runs;
+    const float* blk;  // loss partials: blk[3 sp + 2], sp < n_blk
+    int n_blk;
+    float* loss;
+    unsigned long long* step;
+    unsigned int* done;  // block tickets (zero between launches)
+    int update;
     int total_steps;
     float lr0, lr1, b1, b2, eps;
+    bf16* W[kMaxLayers];
+    bf16* Wt[kMaxLayers];
+    int in[kMaxLayers], outk[kMaxLayers];
 };
 
 __global__ void adam_kernel(AdamArgs a) {
     const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= a.n) return;
     const unsigned long long t = *a.step;  // 0-based
-    const float frac = a.total_steps > 1 ? fminf((float)t / (float)(a.total_steps - 1), 1.f) : 1.f;
-    const float lr = a.lr1 + 0.5f * (a.lr0 - a.lr1) * (1.f + cospif(frac));
-    const float c1 = 1.f - powf(a.b1, (float)(t + 1));
-    const float c2 = 1.f - powf(a.b2, (float)(t + 1));
-    const float gi = a.g[i];
-    const float mi = a.b1 * a.m[i] + (1.f - a.b1) * gi;
-    const float vi = a.b2 * a.v[i] + (1.f - a.b2) * gi * gi;
-    a.m[i] = mi;
-    a.v[i] = vi;
-    a.w[i] -= lr * (mi / c1) / (sqrtf(vi / c2) + a.eps);
+    if (i < a.n) {
+        int k = 0;
+        while (k + 1 < a.n_runs && i >= a.run[k + 1].off) ++k;
+        const GradRun& r = a.run[k];
+        const long long e = i - r.off;
+        const int o = (int)(e / r.cols), c = (int)(e % r.cols);
+        const float* p = r.part + (size_t)o * r.ld + c;
+        float gi = 0.f;
+        int sp = 0;
+        for (; sp + 4 <= r.slices; sp += 4) {
+            float q[4];
+#pragma unroll
+            for (int u = 0; u < 4; ++u) q[u] = p[(size_t)(sp + u) * r.slice_stride];
+#pragma unroll
+            for (int u = 0; u < 4; ++u) gi += q[u];
+        }
+        for (; sp < r.slices; ++sp) gi += p[(size_t)sp * r.slice_stride];
+        if (a.grad) a.grad[i] = gi;
+        if (a.update) {
+            const float frac = a.total_steps > 1 ? fminf((float)t / (float)(a.total_steps - 1), 1.f) : 1.f;
+            const float lr = a.lr1 + 0.5f * (a.lr0 - a.lr1) * (1.f + cospif(frac));
+            const float c1 = 1.f - powf(a.b1, (float)(t + 1));
+            const float c2 = 1.f - powf(a.b2, (float)(t + 1));
+            const float mi = a.b1 * a.m[i] + (1.f - a.b1) * gi;
+            const float vi = a.b2 * a.v[i] + (1.f - a.b2) * gi * gi;
+            a.m[i] = mi;
+            a.v[i] = vi;
+            const float wi = a.w[i] - lr * (mi / c1) / (sqrtf(vi / c2) + a.eps);
+            a.w[i] = wi;
+            if (r.layer >= 0) {
+                const int l = r.layer;
+                a.W[l][(size_t)o * a.in[l] + c] = bf16(wi);
+                if (a.Wt[l] && o < a.outk[l]) a.Wt[l][(size_t)c * a.outk[l] + o] = bf16(wi);
+            }
+        }
+    } else if (i == a.n) {
+        float s = 0.f;
+        for (int b = 0; b < a.n_blk; ++b) s += a.blk[3 * b + 2];
+        *a.loss = s;
+    }
+    if (!a.update) return;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        __threadfence();
+        if (atomicAdd(a.done, 1u) == gridDim.x - 1) {
+            *a.step = t + 1;
+            *a.done = 0;
+        }
+    }
 }
 
 // BF16 copies of every layer's weights: W (out_pad x in, rows >= out zero) for the
 // forward product and W^T (in x outk, columns >= out zero) for the backward product.
-constexpr int kMaxLayers = 9;
 struct RefreshArgs {
     int n_layers;
     const float* p;
@@ -588,12 +710,10 @@ struct RefreshArgs {
     bf16* W[kMaxLayers];
     bf16* Wt[kMaxLayers];
     long long start[kMaxLayers + 1];  // prefix sums of out_pad * in
-    unsigned long long* step;         // incremented once per call when non-null
 };
 
 __global__ void refresh_kernel(RefreshArgs a) {
     const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (t == 0 && a.step) *a.step += 1;
     if (t >= a.start[a.n_layers]) return;
     int l = 0;
     while (t >= a.start[l + 1]) ++l;
@@ -609,8 +729,362 @@ __global__ void unscale_kernel(const float* out, int rows, long long n_left, flo
                                float* sd) {
     const int r = blockIdx.x * blockDim.x + threadIdx.x;
     if (r >= rows || r >= n_left) return;
-    mean[r] = out[2 * r] * y_std + y_mean;
-    sd[r] = expf(0.5f * fminf(fmaxf(out[2 * r + 1], -16.f), 16.f)) * y_std;
+    mean[r] = __fmaf_rn(out[2 * r], y_std, y_mean);
+    sd[r] = __fmul_rn(expf(0.5f * fminf(fmaxf(out[2 * r + 1], -16.f), 16.f)), y_std);
+}
+
+// ------------------------------------------------------------------ fused prediction
+// Prediction of every input row in one launch. A CTA takes 128-row tiles and runs, for
+// each, the Fourier features, the L hidden layers (bias + GELU) and the output transform
+// back to back with the tile's activations in shared memory (BF16, in the 64-column,
+// 128-byte-swizzled K-major chunks the MMA descriptors read), so HBM carries the two input
+// coordinates and the two outputs of a row and nothing else. Each CTA keeps two tiles in
+// flight (slots 0 and 1, one TMEM accumulator of H columns each): while warps 2-17 (four per
+// TMEM lane quadrant, a quarter of the columns each) turn one slot's accumulator into its
+// next activations, warp 1 runs the other slot's layer on the tensor cores. Warp 0 streams
+// every layer's weights (64-wide K chunks, TMA with the 128-byte swizzle) through a ring of
+// stages, once per tile and layer; they stay in L2.
+// The epilogue writes a layer's output over the activations its MMAs have finished
+// reading, so one activation buffer per slot suffices. Waits are bounded as in the GEMM.
+struct InferMaps {
+    CUtensorMap w[kMaxLayers];  // layer l's BF16 weights [rows, K]: boxes of 64 (K) x H rows (16 for the output layer)
+};
+
+struct InferArgs {
+    const float* u;          // n x 2 inputs, or nullptr: points from cells / grid (input_point)
+    const long long* cells;
+    long long n;
+    int grid_n;
+    const float* Bf;         // fourier x 2 frequency matrix
+    int fourier;
+    int layers;              // hidden layers L (the output layer is layer L)
+    const float* params;     // FP32 parameters; layer l's bias at params + b_off[l]
+    long long b_off[kMaxLayers];
+    float y_mean, y_std;
+    float* mean;             // n predictions of the mean
+    float* sd;               // n predictions of the standard deviation
+    long long tiles;         // ceil(n / 128)
+};
+
+constexpr int kInferEpiWarps = 16;  // four per 32-lane TMEM quadrant, a quarter of the columns each
+constexpr int kInferThreads = 64 + 32 * kInferEpiWarps;
+
+template <int H>
+struct InferCfg {
+    static constexpr int kOutN = 16;                         // MMA width of the output layer (2 used)
+    static constexpr int kChunkBytes = kBM * kBK * 2;        // one 128 x 64 operand chunk (16 KB)
+    static constexpr int kActBytes = (H / kBK) * kChunkBytes; // one slot's activations
+    static constexpr int kWBytes = H * kBK * 2;              // one weight stage: H rows x 64 K
+    static constexpr int kWStages = H == 256 ? 3 : 6;
+    // barriers: weight full / empty per stage, accumulator full and epilogue done per slot, drain
+    static constexpr int kBarriers = 2 * kWStages + 4 + 1;
+    static constexpr int kSmem = 1024 + 2 * kActBytes + kWStages * kWBytes + 8 * kBarriers + 16;
+    using MmaH = SM100_MMA_F16BF16_SS<bf16, bf16, float, kBM, H, UMMA::Major::K, UMMA::Major::K>;
+    using MmaO = SM100_MMA_F16BF16_SS<bf16, bf16, float, kBM, kOutN, UMMA::Major::K, UMMA::Major::K>;
+    using TiledH = decltype(make_tiled_mma(MmaH{}));
+    using TiledO = decltype(make_tiled_mma(MmaO{}));
+    using LayoutA = decltype(UMMA::tile_to_mma_shape(
+        UMMA::Layout_K_SW128_Atom<bf16>{}, partition_shape_A(TiledH{}, make_shape(Int<kBM>{}, Int<kBK>{}))));
+    using LayoutAO = decltype(UMMA::tile_to_mma_shape(
+        UMMA::Layout_K_SW128_Atom<bf16>{}, partition_shape_A(TiledO{}, make_shape(Int<kBM>{}, Int<kBK>{}))));
+    using LayoutBH = decltype(UMMA::tile_to_mma_shape(
+        UMMA::Layout_K_SW128_Atom<bf16>{}, partition_shape_B(TiledH{}, make_shape(Int<H>{}, Int<kBK>{}))));
+    using LayoutBO = decltype(UMMA::tile_to_mma_shape(
+        UMMA::Layout_K_SW128_Atom<bf16>{}, partition_shape_B(TiledO{}, make_shape(Int<kOutN>{}, Int<kBK>{}))));
+    static_assert(H == 128 || H == 256, "fused prediction: hidden width 128 or 256");
+    static_assert(kSmem <= 232448, "fused prediction: shared memory above the per-CTA limit");
+    static_assert(kWBytes % 1024 == 0 && kChunkBytes % 1024 == 0, "swizzled operands need 1024-byte alignment");
+};
+
+__device__ __forceinline__ uint32_t pack_bf16x2(float lo, float hi) {
+    __nv_bfloat162 h = __floats2bfloat162_rn(lo, hi);
+    return *reinterpret_cast<uint32_t*>(&h);
+}
+// Shared-memory byte offset of the 8-column segment holding column `col` (a multiple of 8)
+// of row r in a K-major 128-row BF16 operand stored as 64-column chunks of 16 KB with the
+// 128-byte swizzle (16-byte unit u of a row's 128 bytes sits at unit u ^ (r mod 8)), the
+// layout TMA's SWIZZLE_128B writes and the UMMA descriptors of the GEMM read.
+__device__ __forceinline__ uint32_t act_offset(int r, int col) {
+    return (uint32_t)((col >> 6) * (kBM * kBK * 2) + r * 128 + ((((col & 63) >> 3) ^ (r & 7)) << 4));
+}
+__device__ __forceinline__ void st_shared_v4(uint32_t addr, uint32_t x, uint32_t y, uint32_t z, uint32_t w) {
+    asm volatile("st.shared.v4.b32 [%0], {%1, %2, %3, %4};" ::"r"(addr), "r"(x), "r"(y), "r"(z), "r"(w) : "memory");
+}
+__device__ __forceinline__ void tmem_ld32(uint32_t taddr, uint32_t (&r)[32]) {
+    asm volatile("tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15, %16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31}, [%32];\n"
+                 : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]), "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]), "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
+                 : "r"(taddr));
+    asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
+}
+
+template <int H>
+__global__ void __launch_bounds__(kInferThreads, 1)
+    mlp_infer_kernel(const __grid_constant__ InferMaps maps, const InferArgs a, int* err) {
+    using Cfg = InferCfg<H>;
+    constexpr int S = Cfg::kWStages;
+    typename Cfg::TiledH mma_h;
+    typename Cfg::TiledO mma_o;
+    extern __shared__ char smem_raw[];
+    char* base = reinterpret_cast<char*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+    char* wst = base + 2 * Cfg::kActBytes;
+    uint64_t* bars = reinterpret_cast<uint64_t*>(wst + S * Cfg::kWBytes);
+    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bars + Cfg::kBarriers);
+    volatile int* abort_flag = reinterpret_cast<volatile int*>(tmem_slot + 1);
+    auto wfull = [&](int i) { return smem_u32(bars + i); };
+    auto wempty = [&](int i) { return smem_u32(bars + S + i); };
+    auto accf = [&](int t) { return smem_u32(bars + 2 * S + t); };
+    auto epid = [&](int t) { return smem_u32(bars + 2 * S + 2 + t); };
+    const uint32_t drain_bar = smem_u32(bars + 2 * S + 4);
+
+    const int warp = threadIdx.x / 32, lane = threadIdx.x & 31;
+    cute::TMEM::Allocator1Sm tmem;
+    if (warp == 0) tmem.allocate(2 * H, tmem_slot);
+    if (threadIdx.x == 0) {
+        for (int i = 0; i < S; ++i) {
+            mbar_init(wfull(i), 1);
+            mbar_init(wempty(i), 1);
+        }
+        for (int t = 0; t < 2; ++t) {
+            mbar_init(accf(t), 1);
+            mbar_init(epid(t), kInferEpiWarps);
+        }
+        mbar_init(drain_bar, 1);
+        *abort_flag = 0;
+        cutlass::arch::fence_barrier_init();
+    }
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem_base = *tmem_slot;
+    auto fail = [&]() {
+        *abort_flag = 1;
+        atomicExch(err, 1);
+    };
+
+    const int L = a.layers, F = 2 * a.fourier;
+    // slot s of this CTA takes tiles 2 blockIdx.x + s + 2 gridDim.x i, i = 0, 1, ...; every
+    // role walks the same (i, layer, slot) sequence and skips a slot whose tile is past the end
+    const long long stride = 2LL * gridDim.x;
+    auto tile_of = [&](int s, long long i) { return 2LL * blockIdx.x + s + i * stride; };
+    const long long iters = (a.tiles - 2LL * blockIdx.x + stride - 1) / stride;
+
+    if (warp == 0) {
+        // ---- weight producer (lane 0)
+        if (lane == 0) {
+            for (int l = 0; l <= L; ++l)
+                asm volatile("prefetch.tensormap [%0];" ::"l"(reinterpret_cast<uint64_t>(&maps.w[l])) : "memory");
+            int stage = 0;
+            uint32_t phase = 0;
+            int issued[S];
+#pragma unroll
+            for (int i = 0; i < S; ++i) issued[i] = 0;
+            bool stop = false;
+            for (long long i = 0; i < iters && !stop; ++i)
+                for (int l = 0; l <= L && !stop; ++l)
+                    for (int s = 0; s < 2 && !stop; ++s) {
+                        if (tile_of(s, i) >= a.tiles) continue;
+                        const int nk = (l == 0 ? F : H) / kBK;
+                        const uint32_t bytes = (uint32_t)((l == L ? Cfg::kOutN : H) * kBK * 2);
+                        for (int kc = 0; kc < nk; ++kc) {
+                            if (*abort_flag || !mbar_wait_bounded(wempty(stage), phase ^ 1)) {
+                                fail();
+                                stop = true;
+                                break;
+                            }
+                            mbar_expect_tx(wfull(stage), bytes);
+                            tma_load_2d(smem_u32(wst + stage * Cfg::kWBytes), &maps.w[l], wfull(stage), kc * kBK, 0);
+                            ++issued[stage];
+                            if (++stage == S) {
+                                stage = 0;
+                                phase ^= 1;
+                            }
+                        }
+                    }
+            if (*abort_flag)
+                for (int i = 0; i < S; ++i)
+                    if (issued[i] > 0) mbar_wait_bounded(wfull(i), (uint32_t)((issued[i] - 1) & 1));
+        }
+    } else if (warp == 1) {
+        // ---- MMA issuer (the whole warp follows; one elected lane issues)
+        ThrMMA th = mma_h.get_slice(0);
+        ThrMMA to = mma_o.get_slice(0);
+        int stage = 0;
+        uint32_t phase = 0, ep_phase[2] = {0, 0};
+        bool stop = false;
+        for (long long i = 0; i < iters && !stop; ++i)
+            for (int l = 0; l <= L && !stop; ++l)
+                for (int s = 0; s < 2 && !stop; ++s) {
+                    if (tile_of(s, i) >= a.tiles) continue;
+                    // the slot's activations for this layer are written and its accumulator is free
+                    if (*abort_flag || !mbar_wait_bounded(epid(s), ep_phase[s])) {
+                        fail();
+                        stop = true;
+                        break;
+                    }
+                    ep_phase[s] ^= 1;
+                    tc_fence_after();
+                    const int nk = (l == 0 ? F : H) / kBK;
+                    char* act = base + s * Cfg::kActBytes;
+                    const uint32_t acc = tmem_base + (uint32_t)(s * H);
+                    for (int kc = 0; kc < nk; ++kc) {
+                        if (*abort_flag || !mbar_wait_bounded(wfull(stage), phase)) {
+                            fail();
+                            stop = true;
+                            break;
+                        }
+                        tc_fence_after();
+                        bf16* a_ptr = reinterpret_cast<bf16*>(act + kc * Cfg::kChunkBytes);
+                        bf16* b_ptr = reinterpret_cast<bf16*>(wst + stage * Cfg::kWBytes);
+                        if (l < L) {
+                            Tensor tAcc = th.make_fragment_C(
+                                th.partition_C(make_identity_tensor(make_shape(Int<kBM>{}, Int<H>{}))));
+                            tAcc.data() = acc;
+                            Tensor fA = th.make_fragment_A(make_tensor(make_smem_ptr(a_ptr), typename Cfg::LayoutA{}));
+                            Tensor fB = th.make_fragment_B(make_tensor(make_smem_ptr(b_ptr), typename Cfg::LayoutBH{}));
+                            mma_h.accumulate_ = kc == 0 ? UMMA::ScaleOut::Zero : UMMA::ScaleOut::One;
+                            CUTE_UNROLL
+                            for (int kb = 0; kb < size<2>(fA); ++kb) {
+                                gemm(mma_h, fA(_, _, kb), fB(_, _, kb), tAcc);
+                                mma_h.accumulate_ = UMMA::ScaleOut::One;
+                            }
+                        } else {
+                            Tensor tAcc = to.make_fragment_C(
+                                to.partition_C(make_identity_tensor(make_shape(Int<kBM>{}, Int<Cfg::kOutN>{}))));
+                            tAcc.data() = acc;
+                            Tensor fA = to.make_fragment_A(make_tensor(make_smem_ptr(a_ptr), typename Cfg::LayoutAO{}));
+                            Tensor fB = to.make_fragment_B(make_tensor(make_smem_ptr(b_ptr), typename Cfg::LayoutBO{}));
+                            mma_o.accumulate_ = kc == 0 ? UMMA::ScaleOut::Zero : UMMA::ScaleOut::One;
+                            CUTE_UNROLL
+                            for (int kb = 0; kb < size<2>(fA); ++kb) {
+                                gemm(mma_o, fA(_, _, kb), fB(_, _, kb), tAcc);
+                                mma_o.accumulate_ = UMMA::ScaleOut::One;
+                            }
+                        }
+                        cutlass::arch::umma_arrive(bars + S + stage);  // the weight stage is free once these ran
+                        if (++stage == S) {
+                            stage = 0;
+                            phase ^= 1;
+                        }
+                    }
+                    if (stop) break;
+                    cutlass::arch::umma_arrive(bars + 2 * S + s);  // the slot's accumulator is complete
+                }
+        cutlass::arch::umma_arrive(bars + 2 * S + 4);  // every MMA issued here has completed
+        if (!mbar_wait_bounded(drain_bar, 0)) fail();
+    } else {
+        // ---- features and epilogues: warp w owns TMEM lanes / tile rows 32 (w % 4) .. + 31
+        // and, with (w - 2) / 4, one quarter of the columns
+        const int quad = warp & 3, part = (warp - 2) >> 2;
+        const int r = quad * 32 + lane;
+        uint32_t acc_phase[2] = {0, 0};
+        auto signal = [&](int s) {
+            // generic-proxy stores to shared memory become visible to the MMAs (async proxy)
+            asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+            tc_fence_before();
+            __syncwarp();
+            if (lane == 0) mbar_arrive(epid(s));
+        };
+        // X[r, j] = sin(phase_j), X[r, fourier + j] = cos(phase_j), zero past the last input
+        auto features = [&](int s, long long t) {
+            const uint32_t act = smem_u32(base + s * Cfg::kActBytes);
+            const long long i = t * kBM + r;
+            const bool valid = i < a.n;
+            float u0 = 0.f, u1 = 0.f;
+            if (valid) input_point(a.u, a.cells, a.grid_n, i, u0, u1);
+            const int fq = a.fourier / 4;
+            for (int g = 0; g < fq; g += 8) {
+                const int j0 = part * fq + g;
+                uint32_t ps[4], pc[4];
+#pragma unroll
+                for (int q = 0; q < 4; ++q) {
+                    float s0 = 0.f, c0 = 0.f, s1 = 0.f, c1 = 0.f;
+                    if (valid) {
+                        sincosf(feature_phase(u0, u1, a.Bf, j0 + 2 * q), &s0, &c0);
+                        sincosf(feature_phase(u0, u1, a.Bf, j0 + 2 * q + 1), &s1, &c1);
+                    }
+                    ps[q] = pack_bf16x2(s0, s1);
+                    pc[q] = pack_bf16x2(c0, c1);
+                }
+                st_shared_v4(act + act_offset(r, j0), ps[0], ps[1], ps[2], ps[3]);
+                st_shared_v4(act + act_offset(r, a.fourier + j0), pc[0], pc[1], pc[2], pc[3]);
+            }
+        };
+        for (int s = 0; s < 2; ++s)
+            if (tile_of(s, 0) < a.tiles) {
+                features(s, tile_of(s, 0));
+                signal(s);
+            }
+        bool stop = false;
+        for (long long i = 0; i < iters && !stop; ++i)
+            for (int l = 0; l <= L && !stop; ++l)
+                for (int s = 0; s < 2; ++s) {
+                    const long long t = tile_of(s, i);
+                    if (t >= a.tiles) continue;
+                    if (*abort_flag || !mbar_wait_bounded(accf(s), acc_phase[s])) {
+                        fail();
+                        stop = true;
+                        break;
+                    }
+                    acc_phase[s] ^= 1;
+                    tc_fence_after();
+                    const uint32_t tq = tmem_base + (uint32_t)(s * H) + ((uint32_t)(quad * 32) << 16);
+                    if (l < L) {
+                        // bias + GELU -> BF16 activations of layer l + 1, over this slot's buffer
+                        const uint32_t act = smem_u32(base + s * Cfg::kActBytes);
+                        const float4* b4 = reinterpret_cast<const float4*>(a.params + a.b_off[l]);
+#pragma unroll 1
+                        for (int c0 = part * (H / 4); c0 < (part + 1) * (H / 4); c0 += 32) {
+                            uint32_t rv[32];
+                            tmem_ld32(tq + (uint32_t)c0, rv);
+                            uint32_t pk[16];
+#pragma unroll
+                            for (int q = 0; q < 8; ++q) {
+                                const float4 b = __ldg(b4 + c0 / 4 + q);
+                                const float2 g0 = gelu2(__fadd2_rn(
+                                    make_float2(__uint_as_float(rv[4 * q]), __uint_as_float(rv[4 * q + 1])),
+                                    make_float2(b.x, b.y)));
+                                const float2 g1 = gelu2(__fadd2_rn(
+                                    make_float2(__uint_as_float(rv[4 * q + 2]), __uint_as_float(rv[4 * q + 3])),
+                                    make_float2(b.z, b.w)));
+                                pk[2 * q] = pack_bf16x2(g0.x, g0.y);
+                                pk[2 * q + 1] = pack_bf16x2(g1.x, g1.y);
+                            }
+#pragma unroll
+                            for (int q = 0; q < 4; ++q)
+                                st_shared_v4(act + act_offset(r, c0 + 8 * q), pk[4 * q], pk[4 * q + 1], pk[4 * q + 2],
+                                             pk[4 * q + 3]);
+                        }
+                        signal(s);
+                    } else {
+                        // output layer: mean = mu std_y + mean_y, sd = exp(clamp(lv) / 2) std_y
+                        if (part == 0) {
+                            uint32_t o0, o1;
+                            asm volatile("tcgen05.ld.sync.aligned.32x32b.x2.b32 {%0, %1}, [%2];\n"
+                                         : "=r"(o0), "=r"(o1)
+                                         : "r"(tq));
+                            asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
+                            const float* bo = a.params + a.b_off[L];
+                            const float mu = __uint_as_float(o0) + __ldg(bo);
+                            const float lv = __uint_as_float(o1) + __ldg(bo + 1);
+                            const long long row = t * kBM + r;
+                            if (row < a.n) {
+                                a.mean[row] = __fmaf_rn(mu, a.y_std, a.y_mean);
+                                a.sd[row] = __fmul_rn(expf(0.5f * fminf(fmaxf(lv, -16.f), 16.f)), a.y_std);
+                            }
+                        }
+                        const long long tn = tile_of(s, i + 1);
+                        if (tn < a.tiles) {
+                            features(s, tn);
+                            signal(s);
+                        }
+                    }
+                }
+    }
+    __syncthreads();
+    if (warp == 0) {
+        tc_fence_after();
+        tmem.release_allocation_lock();
+        tmem.free(tmem_base, 2 * H);
+    }
 }
 
 }  // namespace ucbmlp
@@ -622,7 +1096,7 @@ using ucbmlp::bf16;
 
 namespace {
 
-constexpr int kMaxSplits = 64;  // split-K slices per weight-gradient tile
+constexpr int kMaxSplits = 32;  // split-K slices per weight-gradient tile
 
 bool cu_ok(cudaError_t e, std::string& err, const char* what) {
     if (e == cudaSuccess) return true;
@@ -665,14 +1139,18 @@ struct Mlp {
     std::vector<bf16*> Hb, Ht;
     float* outp = nullptr;         // rows x 2
     float* yb = nullptr;
-    bf16 *dout = nullptr, *doutT = nullptr, *dZ = nullptr, *dZt = nullptr;
-    float* dH = nullptr;
-    // partial sums reduced in a fixed order: split-K weight-gradient tiles, per-block NLL /
-    // bias-gradient sums
-    float* part = nullptr;
-    long long part_floats = 0;
+    bf16 *dout = nullptr, *doutT = nullptr;
+    bf16* dZ[2] = {nullptr, nullptr};   // dL/dZ of consecutive hidden layers (ping-pong)
+    bf16* dZt[2] = {nullptr, nullptr};  // and its transposed copy
+    // partial sums that the optimiser kernel adds in a fixed order: per layer the split-K
+    // slices of the weight gradient, per hidden layer the bias-gradient sums of 32-row
+    // blocks, and the output layer's per-block NLL sums
+    std::vector<float*> part;
+    std::vector<long long> part_cap;
+    std::vector<int> splits;
+    std::vector<float*> dbp;
     float* blk = nullptr;
-    float* dbp = nullptr;
+    unsigned int* done = nullptr;
     // prediction buffers (ping-pong activations, no backward copies)
     std::vector<void*> pred_owned;
     int pred_rows = 0;
@@ -709,6 +1187,12 @@ bool set_gemm_attributes(int device, std::string& err) {
     ce = cudaFuncSetAttribute(ucbmlp::gemm_tma_kernel<256>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                               ucbmlp::GemmCfg<256>::kSmem);
     if (!cu_ok(ce, err, "cudaFuncSetAttribute(gemm 256)")) return false;
+    ce = cudaFuncSetAttribute(ucbmlp::mlp_infer_kernel<128>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                              ucbmlp::InferCfg<128>::kSmem);
+    if (!cu_ok(ce, err, "cudaFuncSetAttribute(infer 128)")) return false;
+    ce = cudaFuncSetAttribute(ucbmlp::mlp_infer_kernel<256>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                              ucbmlp::InferCfg<256>::kSmem);
+    if (!cu_ok(ce, err, "cudaFuncSetAttribute(infer 256)")) return false;
     g_attr_devices.push_back(device);
     return true;
 }
@@ -755,44 +1239,39 @@ bool tensor_map(CUtensorMap* map, const bf16* ptr, int rows, int K, int box_rows
     return true;
 }
 
-bool ordered_sum(Mlp& m, const float* part, int count, long long stride, long long width, float* out,
-                 cudaStream_t st, std::string& err) {
-    const unsigned blocks = (unsigned)std::min<long long>((width + 255) / 256, 1024);
-    ucbmlp::ordered_sum_kernel<<<blocks, 256, 0, st>>>(part, count, stride, width, out);
-    m.e->launches += 1;
-    return cu_ok(cudaPeekAtLastError(), err, "ordered_sum launch");
-}
-
-// C = A B^T (+ epilogue). Tiles of 128 x 256 when N allows (A is then read once), else
-// 128 x 128. ep.atomic: split K over up to kMaxSplits slices per tile; each slice writes its
-// partial tile into m.part and ordered_sum adds them in slice order into ep.outf (rows <
-// m_store, columns < n_store; other entries of ep.outf are left alone).
+// C = A B^T (+ epilogue). ep.atomic: K is split into up to kMaxSplits slices per tile and
+// each slice's partial tile (rows < m_store, columns < n_store) is stored at
+// ep.outf + slice * m_eff * ep.ldf (m_eff = min(M, m_store)); *splits_out receives the
+// number of slices and part_cap bounds the buffer (floats). The slices are added later, in
+// slice order, by the optimiser kernel.
 bool gemm(Mlp& m, const bf16* A, const bf16* B, int M, int N, int K, const ucbmlp::Epilogue& ep_in, cudaStream_t st,
-          std::string& err) {
+          std::string& err, int* splits_out = nullptr, long long part_cap = 0) {
     ucbmlp::Epilogue ep = ep_in;
     if (M <= 0 || N <= 0 || K <= 0 || M % ucbmlp::kBM || N % 128 || K % ucbmlp::kBK) {
         err = "gemm: unsupported shape " + std::to_string(M) + "x" + std::to_string(N) + "x" + std::to_string(K);
         return false;
     }
-    const int bn = N % 256 == 0 ? 256 : 128;
+    const int sms = std::max(m.e->sm_count, 1);
+    // 256-wide tiles read A once; below one wide tile per SM the 128-wide tiles keep twice
+    // as many SMs busy (and halve each CTA's epilogue)
+    const int bn = (N % 256 == 0 && (M / ucbmlp::kBM) * (N / 256) >= sms) ? 256 : 128;
     const int tiles = (M / ucbmlp::kBM) * (N / bn);
     const int kt = K / ucbmlp::kBK;
-    const int sms = std::max(m.e->sm_count, 1);
     int per = kt;
     if (ep.atomic) {
-        const int want = std::max(1, std::min({kt, kMaxSplits, (sms + tiles - 1) / tiles}));
+        // about one (tile, slice) item per SM: more slices only add partial-tile traffic
+        const int want = std::max(1, std::min({kt, kMaxSplits, sms / tiles}));
         per = (kt + want - 1) / want;
     }
     const int splits = (kt + per - 1) / per;
     const long long m_eff = std::min(M, ep.m_store), n_eff = std::min(N, ep.n_store);
-    float* const out = ep.outf;
     if (ep.atomic) {
-        if (ep.ldf < n_eff || (long long)splits * m_eff * ep.ldf > m.part_floats) {
+        if (!splits_out || ep.ldf < n_eff || (long long)splits * m_eff * ep.ldf > part_cap) {
             err = "gemm: split-K partial buffer too small";
             return false;
         }
-        ep.outf = m.part;
         ep.split_stride = m_eff * ep.ldf;
+        *splits_out = splits;
     } else {
         ep.split_stride = 0;
     }
@@ -807,13 +1286,7 @@ bool gemm(Mlp& m, const bf16* A, const bf16* B, int M, int N, int K, const ucbml
         ucbmlp::gemm_tma_kernel<128><<<grid, ucbmlp::kGemmThreads, ucbmlp::GemmCfg<128>::kSmem, st>>>(ta, tb, w, ep,
                                                                                                       m.err);
     m.e->launches += 1;
-    if (!cu_ok(cudaPeekAtLastError(), err, "gemm launch")) return false;
-    if (!ep.atomic) return true;
-    if (n_eff == ep.ldf) return ordered_sum(m, m.part, splits, ep.split_stride, m_eff * ep.ldf, out, st, err);
-    for (long long r = 0; r < m_eff; ++r)  // rows with a gap beyond n_eff: one reduction per row
-        if (!ordered_sum(m, m.part + r * ep.ldf, splits, ep.split_stride, n_eff, out + r * ep.ldf, st, err))
-            return false;
-    return true;
+    return cu_ok(cudaPeekAtLastError(), err, "gemm launch");
 }
 
 ucbmlp::Epilogue epi() {
@@ -849,14 +1322,24 @@ bool ensure_rows(Mlp& m, int rows, std::string& err) {
         m.Ht.push_back(ht);
     }
     if (!(m.outp = dalloc<float>(R * 2, o, err, "out")) || !(m.yb = dalloc<float>(R, o, err, "y batch")) ||
-        !(m.dout = dalloc<bf16>(R * 64, o, err, "dOut")) || !(m.doutT = dalloc<bf16>(R * 128, o, err, "dOut^T")) ||
-        !(m.dZ = dalloc<bf16>(R * m.H, o, err, "dZ")) || !(m.dZt = dalloc<bf16>(R * m.H, o, err, "dZ^T")) ||
-        !(m.dH = dalloc<float>(R * m.H, o, err, "dH")))
+        !(m.dout = dalloc<bf16>(R * 64, o, err, "dOut")) || !(m.doutT = dalloc<bf16>(R * 128, o, err, "dOut^T")))
         return false;
-    m.part_floats = (long long)kMaxSplits * m.H * std::max(m.H, m.F);
-    if (!(m.part = dalloc<float>((size_t)m.part_floats, o, err, "split-K partials")) ||
-        !(m.blk = dalloc<float>((R + 255) / 256 * 3, o, err, "NLL block sums")) ||
-        !(m.dbp = dalloc<float>((R + 31) / 32 * m.H, o, err, "bias-gradient partials")))
+    for (int b = 0; b < 2; ++b)
+        if (!(m.dZ[b] = dalloc<bf16>(R * m.H, o, err, "dZ")) || !(m.dZt[b] = dalloc<bf16>(R * m.H, o, err, "dZ^T")))
+            return false;
+    m.part.assign(m.L + 1, nullptr);
+    m.part_cap.assign(m.L + 1, 0);
+    m.splits.assign(m.L + 1, 0);
+    m.dbp.assign(m.L, nullptr);
+    for (int l = 0; l <= m.L; ++l) {
+        // split-K slices of layer l's weight gradient: [splits][rows of W][in]
+        m.part_cap[l] = (long long)kMaxSplits * (l == m.L ? 2 : m.H) * m.in[l];
+        if (!(m.part[l] = dalloc<float>((size_t)m.part_cap[l], o, err, "split-K partials"))) return false;
+    }
+    for (int l = 0; l < m.L; ++l)
+        if (!(m.dbp[l] = dalloc<float>((R + 31) / 32 * m.H, o, err, "bias-gradient partials"))) return false;
+    if (!(m.blk = dalloc<float>((R + 31) / 32 * 3, o, err, "NLL block sums")) ||
+        !(m.done = dalloc<unsigned int>(1, o, err, "block tickets")))
         return false;
     m.rows = rows;
     return true;
@@ -876,7 +1359,7 @@ bool ensure_pred_rows(Mlp& m, int rows, std::string& err) {
     return true;
 }
 
-bool refresh(Mlp& m, cudaStream_t st, bool count_step, std::string& err) {
+bool refresh(Mlp& m, cudaStream_t st, std::string& err) {
     ucbmlp::RefreshArgs a{};
     a.n_layers = m.L + 1;
     a.p = m.p;
@@ -891,7 +1374,6 @@ bool refresh(Mlp& m, cudaStream_t st, bool count_step, std::string& err) {
         a.Wt[l] = m.Wt[l];
         a.start[l + 1] = a.start[l] + (long long)m.out_pad[l] * m.in[l];
     }
-    a.step = count_step ? m.step : nullptr;
     const long long total = a.start[a.n_layers];
     ucbmlp::refresh_kernel<<<(unsigned)((total + 255) / 256), 256, 0, st>>>(a);
     m.e->launches += 1;
@@ -924,8 +1406,9 @@ bool features(Mlp& m, const ucbmlp::FeatureArgs& a, cudaStream_t st, std::string
     return cu_ok(cudaPeekAtLastError(), err, "features launch");
 }
 
-// Forward pass over `rows` rows of m.X. keep: store Z and H^T for the backward pass.
-bool forward(Mlp& m, int rows, bool keep, cudaStream_t st, std::string& err) {
+// Forward pass over `rows` rows of m.X. keep: store Z and H^T for the backward pass and
+// evaluate the loss of the first n_valid rows against m.yb (dOut, dOut^T, block sums).
+bool forward(Mlp& m, int rows, bool keep, cudaStream_t st, std::string& err, int n_valid = 0) {
     const bf16* x = m.X;
     int k = m.F;
     for (int l = 0; l < m.L; ++l) {
@@ -949,6 +1432,16 @@ bool forward(Mlp& m, int rows, bool keep, cudaStream_t st, std::string& err) {
     ep.outf = m.outp;
     ep.ldf = 2;
     ep.n_store = 2;
+    if (keep) {
+        ep.nll = 1;
+        ep.yb = m.yb;
+        ep.n_valid = n_valid;
+        ep.rows = rows;
+        ep.beta = m.cfg.beta_nll;
+        ep.dout = m.dout;
+        ep.doutT = m.doutT;
+        ep.blk = m.blk;
+    }
     return gemm(m, x, m.W[m.L], rows, m.out_pad[m.L], m.H, ep, st, err);
 }
 
@@ -976,60 +1469,114 @@ bool forward_infer(Mlp& m, int rows, cudaStream_t st, std::string& err) {
     return gemm(m, x, m.W[m.L], rows, m.out_pad[m.L], m.H, ep, st, err);
 }
 
-// Loss, backward pass and gradient (m.g) for the batch in m.X / m.yb (n_valid rows).
-bool backward(Mlp& m, int rows, int n_valid, cudaStream_t st, std::string& err) {
-    if (!cu_ok(cudaMemsetAsync(m.g, 0, sizeof(float) * m.n_params, st), err, "memset grad") ||
-        !cu_ok(cudaMemsetAsync(m.loss, 0, sizeof(float), st), err, "memset loss"))
-        return false;
-    const int nblk = (rows + 255) / 256;
-    ucbmlp::nll_kernel<<<nblk, 256, 0, st>>>(m.outp, m.yb, rows, n_valid, m.cfg.beta_nll, m.dout, m.doutT, m.blk);
-    m.e->launches += 1;
-    if (!cu_ok(cudaPeekAtLastError(), err, "nll launch") ||
-        !ordered_sum(m, m.blk, nblk, 3, 2, m.g + m.b_off[m.L], st, err) ||
-        !ordered_sum(m, m.blk + 2, nblk, 3, 1, m.loss, st, err))
-        return false;
+// Backward pass for the batch of the last forward(keep) (which already left dL/dOut in
+// dOut / dOut^T and the NLL block sums in blk): every product stores partial results only
+// (split-K slices of the weight gradients, 32-row block sums of the bias gradients); the
+// optimiser kernel adds them. dL/dZ of a hidden layer comes straight out of the epilogue of
+// the product that gives dL/dH (GELU backward fused), ping-ponging between two buffers.
+bool backward(Mlp& m, int rows, cudaStream_t st, std::string& err) {
     const int Lo = m.L;
-    // output layer: dH = dOut W (K padded to 64), dW = dOut^T H (M padded to 128)
+    int cur = 0;
+    // dL/dZ of the last hidden layer = (dOut W_out) GELU'(Z), K padded to 64
     {
         ucbmlp::Epilogue ep = epi();
-        ep.outf = m.dH;
-        ep.ldf = m.H;
+        ep.zin = m.Z[Lo - 1];
+        ep.ldz = m.H;
+        ep.outh = m.dZ[cur];
+        ep.ldh = m.H;
+        ep.outt = m.dZt[cur];
+        ep.ldt = rows;
+        ep.colsum = m.dbp[Lo - 1];
+        ep.ldc = m.H;
         if (!gemm(m, m.dout, m.Wt[Lo], rows, m.H, 64, ep, st, err)) return false;
+        // output-layer weight gradient dOut^T H (M padded to 128, rows 0 and 1 stored)
         ucbmlp::Epilogue eg = epi();
-        eg.outf = m.g + m.w_off[Lo];
+        eg.outf = m.part[Lo];
         eg.ldf = m.H;
         eg.atomic = 1;
         eg.m_store = 2;
-        if (!gemm(m, m.doutT, m.Ht[Lo - 1], 128, m.H, rows, eg, st, err)) return false;
+        if (!gemm(m, m.doutT, m.Ht[Lo - 1], 128, m.H, rows, eg, st, err, &m.splits[Lo], m.part_cap[Lo])) return false;
     }
     for (int l = Lo - 1; l >= 0; --l) {
-        dim3 gb((m.H + 31) / 32, (rows + 31) / 32);
-        ucbmlp::gelu_back_kernel<<<gb, dim3(32, 8), 0, st>>>(m.dH, m.Z[l], rows, m.H, m.dZ, m.dZt, m.dbp);
-        m.e->launches += 1;
-        if (!cu_ok(cudaPeekAtLastError(), err, "gelu_back launch") ||
-            !ordered_sum(m, m.dbp, (int)gb.y, m.H, m.H, m.g + m.b_off[l], st, err))
-            return false;
         const bf16* prevT = l > 0 ? m.Ht[l - 1] : m.Xt;
         const int in = m.in[l];
         ucbmlp::Epilogue eg = epi();
-        eg.outf = m.g + m.w_off[l];
+        eg.outf = m.part[l];
         eg.ldf = in;
         eg.atomic = 1;
-        if (!gemm(m, m.dZt, prevT, m.H, in, rows, eg, st, err)) return false;
+        if (!gemm(m, m.dZt[cur], prevT, m.H, in, rows, eg, st, err, &m.splits[l], m.part_cap[l])) return false;
         if (l > 0) {
             ucbmlp::Epilogue ep = epi();
-            ep.outf = m.dH;
-            ep.ldf = m.H;
-            if (!gemm(m, m.dZ, m.Wt[l], rows, in, m.H, ep, st, err)) return false;
+            ep.zin = m.Z[l - 1];
+            ep.ldz = m.H;
+            ep.outh = m.dZ[cur ^ 1];
+            ep.ldh = m.H;
+            ep.outt = m.dZt[cur ^ 1];
+            ep.ldt = rows;
+            ep.colsum = m.dbp[l - 1];
+            ep.ldc = m.H;
+            if (!gemm(m, m.dZ[cur], m.Wt[l], rows, in, m.H, ep, st, err)) return false;
+            cur ^= 1;
         }
     }
     return true;
 }
 
-bool adam(Mlp& m, cudaStream_t st, std::string& err) {
-    ucbmlp::AdamArgs a{m.p, m.g, m.m1, m.m2, m.n_params, m.step, m.cfg.train_steps,
-                       m.cfg.lr, m.cfg.lr_final, 0.9f, 0.999f, 1e-8f};
-    ucbmlp::adam_kernel<<<(unsigned)((m.n_params + 255) / 256), 256, 0, st>>>(a);
+// The optimiser kernel over the partial results of the last backward(rows): update = true
+// runs Adam and refreshes the BF16 weights; false only writes the gradient to m.g. Both
+// write the loss.
+bool adam(Mlp& m, int rows, bool update, cudaStream_t st, std::string& err) {
+    ucbmlp::AdamArgs a{};
+    a.w = m.p;
+    a.m = m.m1;
+    a.v = m.m2;
+    a.grad = update ? nullptr : m.g;
+    a.n = m.n_params;
+    const int nblk = (rows + 31) / 32;
+    int k = 0;
+    for (int l = 0; l <= m.L; ++l) {
+        const bool out = l == m.L;
+        ucbmlp::GradRun w{};
+        w.off = m.w_off[l];
+        w.count = (long long)m.out[l] * m.in[l];
+        w.cols = m.in[l];
+        w.ld = m.in[l];
+        w.part = m.part[l];
+        w.slice_stride = (long long)(out ? 2 : m.H) * m.in[l];
+        w.slices = m.splits[l];
+        w.layer = l;
+        a.run[k++] = w;
+        ucbmlp::GradRun b{};
+        b.off = m.b_off[l];
+        b.count = m.out[l];
+        b.cols = m.out[l];
+        b.ld = 0;
+        b.part = out ? m.blk : m.dbp[l];
+        b.slice_stride = out ? 3 : m.H;
+        b.slices = nblk;
+        b.layer = -1;
+        a.run[k++] = b;
+    }
+    a.n_runs = k;
+    a.blk = m.blk;
+    a.n_blk = nblk;
+    a.loss = m.loss;
+    a.step = m.step;
+    a.done = m.done;
+    a.update = update ? 1 : 0;
+    a.total_steps = m.cfg.train_steps;
+    a.lr0 = m.cfg.lr;
+    a.lr1 = m.cfg.lr_final;
+    a.b1 = 0.9f;
+    a.b2 = 0.999f;
+    a.eps = 1e-8f;
+    for (int l = 0; l <= m.L; ++l) {
+        a.W[l] = m.W[l];
+        a.Wt[l] = m.Wt[l];
+        a.in[l] = m.in[l];
+        a.outk[l] = m.outk[l];
+    }
+    ucbmlp::adam_kernel<<<(unsigned)((m.n_params + 1 + 255) / 256), 256, 0, st>>>(a);
     m.e->launches += 1;
     return cu_ok(cudaPeekAtLastError(), err, "adam launch");
 }
@@ -1046,15 +1593,17 @@ bool check_kernel_error(Mlp& m, cudaStream_t st, std::string& err) {
     return true;
 }
 
-// One training step (features of a random batch, forward, loss, backward, Adam, BF16
-// refresh + step count): the sequence that is captured into a CUDA graph.
+// One training step (features of a random batch, forward with the loss in the output
+// layer's epilogue, backward, and the optimiser kernel: gradient sums, Adam, BF16 weights,
+// step count): the sequence that is captured into a CUDA graph, 16 kernels for 4 hidden
+// layers.
 bool train_step(Mlp& m, const MlpInputs& in, const float* d_y, cudaStream_t st, std::string& err) {
     const int rows = m.cfg.batch;
     ucbmlp::FeatureArgs fa = feature_args(m, in, 0, rows, true);
     fa.y = d_y;
     fa.yb = m.yb;
-    return features(m, fa, st, err) && forward(m, rows, true, st, err) && backward(m, rows, rows, st, err) &&
-           adam(m, st, err) && refresh(m, st, true, err);
+    return features(m, fa, st, err) && forward(m, rows, true, st, err, rows) && backward(m, rows, st, err) &&
+           adam(m, rows, true, st, err);
 }
 
 }  // namespace
@@ -1126,7 +1675,7 @@ bool mlp_reinit(Mlp* m, std::string& err) {
                "upload params") ||
         !cu_ok(cudaMemcpy(m->Bf, hb.data(), hb.size() * sizeof(float), cudaMemcpyHostToDevice), err, "upload B"))
         return false;
-    return refresh(*m, m->e->stream, false, err) && cu_ok(cudaStreamSynchronize(m->e->stream), err, "init");
+    return refresh(*m, m->e->stream, err) && cu_ok(cudaStreamSynchronize(m->e->stream), err, "init");
 }
 
 const ucb_mlp_config& mlp_config(const Mlp* m) { return m->cfg; }
@@ -1140,8 +1689,53 @@ void mlp_destroy(Mlp* m) {
 long long mlp_param_count(const Mlp* m) { return m ? m->n_params : 0; }
 int mlp_features(const Mlp* m) { return m ? m->F : 0; }
 
+// Whether the fused prediction kernel covers this network (hidden width 128 or 256, features
+// no wider than a hidden layer).
+static bool fused_predict_supported(const Mlp& m) {
+    return (m.H == 128 || m.H == 256) && m.F <= m.H && m.F % ucbmlp::kBK == 0 && (m.F / 2) % 32 == 0 &&
+           m.L + 1 <= ucbmlp::kMaxLayers;
+}
+
+static bool predict_fused(Mlp& m, const MlpInputs& in, float* d_mean, float* d_std, cudaStream_t st, std::string& err) {
+    ucbmlp::InferMaps maps;
+    std::memset(&maps, 0, sizeof maps);
+    for (int l = 0; l < m.L; ++l)
+        if (!tensor_map(&maps.w[l], m.W[l], m.H, m.in[l], m.H, err)) return false;
+    if (!tensor_map(&maps.w[m.L], m.W[m.L], m.out_pad[m.L], m.H, ucbmlp::InferCfg<256>::kOutN, err)) return false;
+    ucbmlp::InferArgs a{};
+    a.u = in.u;
+    a.cells = in.cells;
+    a.n = in.n;
+    a.grid_n = in.grid_n;
+    a.Bf = m.Bf;
+    a.fourier = m.cfg.fourier;
+    a.layers = m.L;
+    a.params = m.p;
+    for (int l = 0; l <= m.L; ++l) {
+        if (m.b_off[l] % 4) {
+            err = "fused prediction: bias not 16-byte aligned";
+            return false;
+        }
+        a.b_off[l] = m.b_off[l];
+    }
+    a.y_mean = m.y_mean;
+    a.y_std = m.y_std;
+    a.mean = d_mean;
+    a.sd = d_std;
+    a.tiles = (in.n + ucbmlp::kBM - 1) / ucbmlp::kBM;
+    const long long pairs = (a.tiles + 1) / 2;
+    const int grid = (int)std::min<long long>(pairs, std::max(m.e->sm_count, 1));
+    if (m.H == 256)
+        ucbmlp::mlp_infer_kernel<256><<<grid, ucbmlp::kInferThreads, ucbmlp::InferCfg<256>::kSmem, st>>>(maps, a, m.err);
+    else
+        ucbmlp::mlp_infer_kernel<128><<<grid, ucbmlp::kInferThreads, ucbmlp::InferCfg<128>::kSmem, st>>>(maps, a, m.err);
+    m.e->launches += 1;
+    return cu_ok(cudaPeekAtLastError(), err, "fused prediction launch");
+}
+
 bool mlp_predict(Mlp* m, const MlpInputs& in, float* d_mean, float* d_std, cudaStream_t st, std::string& err) {
     if (in.n <= 0) return true;
+    if (fused_predict_supported(*m)) return predict_fused(*m, in, d_mean, d_std, st, err);
     const long long chunk = 1 << 18;
     const long long rows_needed = std::min<long long>(chunk, ((in.n + 127) / 128) * 128);
     if (!ensure_pred_rows(*m, (int)rows_needed, err)) return false;
@@ -1285,7 +1879,7 @@ int ucb_mlp_set_params(ucb_mlp* m, const float* in, long long n) {
     cudaSetDevice(m->e->device);
     std::string err;
     if (cudaMemcpy(m->m->p, in, n * sizeof(float), cudaMemcpyHostToDevice) != cudaSuccess) return UCB_E_CUDA;
-    if (!refresh(*m->m, m->e->stream, false, err) || cudaStreamSynchronize(m->e->stream) != cudaSuccess) {
+    if (!refresh(*m->m, m->e->stream, err) || cudaStreamSynchronize(m->e->stream) != cudaSuccess) {
         m->e->last_error = err;
         return UCB_E_CUDA;
     }
@@ -1328,8 +1922,8 @@ int ucb_mlp_loss_grad(ucb_mlp* h, const float* u, const float* y, long long n, f
         fa.Xt = m.Xt;
         fa.y = dy;
         fa.yb = m.yb;
-        if (!features(m, fa, st, err) || !forward(m, rows, true, st, err) || !backward(m, rows, (int)n, st, err) ||
-            !check_kernel_error(m, st, err) ||
+        if (!features(m, fa, st, err) || !forward(m, rows, true, st, err, (int)n) || !backward(m, rows, st, err) ||
+            !adam(m, rows, false, st, err) || !check_kernel_error(m, st, err) ||
             !cu_ok(cudaMemcpy(grad, m.g, m.n_params * sizeof(float), cudaMemcpyDeviceToHost), err, "read grad") ||
             !cu_ok(cudaMemcpy(loss, m.loss, sizeof(float), cudaMemcpyDeviceToHost), err, "read loss"))
             rc = UCB_E_CUDA;

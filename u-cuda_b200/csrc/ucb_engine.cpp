@@ -1160,7 +1160,33 @@ int ucb_autotune_lle2d(ucb_engine* e, const ucb_lle2d_request* req, int32_t forc
         lle_tuned_request(e, q, tp, L, rq, e2);
         return rq;
     };
-    const int rc = autotune_search(e, key, 128, force != 0, trial, build, rep);
+    // confirmation: the request's own window and horizon, on its grid when one run is
+    // estimated at <= 1.5 s from the trial's default time, else on the largest grid that is
+    std::vector<double> cvals;
+    std::vector<int32_t> cflags;
+    ucb_lle2d_request cq = base;
+    auto confirm = [&](const TuneConfig& c) -> double {
+        if (cvals.empty()) {
+            const double trial_steps = (double)t.n_pts * t.n_pts *
+                                       (tp.amountOfPointsForSkip +
+                                        (double)tp.amountOfPointsInBlock * 2.0 * (double)(tp.nt_steps + 1));
+            const double ms_per_cell = rep->default_ms / trial_steps * steps_cell;
+            const double cells = std::min((double)base.n_pts * base.n_pts, 1500.0 / std::max(ms_per_cell, 1e-12));
+            cq.n_pts = std::max(64, std::min(base.n_pts, (int)std::floor(std::sqrt(cells))));
+            rep->confirm_n_pts = cq.n_pts;
+            cvals.resize((size_t)cq.n_pts * cq.n_pts);
+            cflags.resize(cvals.size());
+        }
+        ucb_lle2d_request q = cq;
+        q.opt.block_threads = c.block;
+        q.opt.max_registers = c.maxreg;
+        q.opt.unroll = c.unroll;
+        ucb_lle2d_result r{};
+        r.values = cvals.data();
+        r.flags = cflags.data();
+        return ucb_run_lle2d(e, &q, &r) == UCB_OK ? r.kernel_ms : -1.0;
+    };
+    const int rc = autotune_search(e, key, 128, force != 0, trial, build, rep, confirm);
     rep->trial_n_pts = t.n_pts;
     return rc;
 }

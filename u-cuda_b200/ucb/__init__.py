@@ -39,7 +39,8 @@ class TuneReport(C.Structure):
                 ("candidates", C.c_int32), ("registers", C.c_int32), ("blocks_per_sm", C.c_int32),
                 ("best_ms", C.c_double), ("default_ms", C.c_double), ("wall_ms", C.c_double),
                 ("trial_n_pts", C.c_int32), ("from_table", C.c_int32), ("key", C.c_char * 32),
-                ("error", C.c_char * 256)]
+                ("error", C.c_char * 256), ("confirm_default_ms", C.c_double), ("confirm_best_ms", C.c_double),
+                ("confirm_n_pts", C.c_int32), ("pad0", C.c_int32)]
 
     def as_dict(self):
         return {f: (getattr(self, f).decode() if f in ("key", "error") else getattr(self, f))
