@@ -145,6 +145,8 @@ def run_ours(args, rank, world, local):
     launches_timed = 0
     tuned = {}
     for name, opt in forms.items():
+        if args.no_autotune:
+            opt = dict(opt, block_threads=128)  # the default shape, not a stored tuned one
         req = engine_request(ucb, c, **opt)
         # launch-shape search (once per kernel build and device; reused from the table
         # beside the CUBIN cache afterwards), outside the timed region like compilation
