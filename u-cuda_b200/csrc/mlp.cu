@@ -149,6 +149,13 @@ __device__ __forceinline__ void tma_load_2d(uint32_t dst, const CUtensorMap* map
         ::"r"(dst), "l"(reinterpret_cast<uint64_t>(map)), "r"(bar), "r"(x), "r"(y)
         : "memory");
 }
+// Programmatic dependent launch: a kernel launched with programmatic stream serialisation may
+// start while its predecessor in the stream still runs. launch_dependents lets the next
+// kernel's CTAs start their prologue once every CTA of this grid has issued it; wait blocks
+// until the predecessor grid has completed and its memory is visible. Without the launch
+// attribute both are no-ops.
+__device__ __forceinline__ void griddep_launch_dependents() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
+__device__ __forceinline__ void griddep_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
 __device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
 __device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
 
@@ -233,8 +240,23 @@ __device__ __forceinline__ void nll_rows(const Epilogue& ep, int r, float mu, fl
 
 // One 32-column chunk of one accumulator row (this thread's) through the epilogue: bias,
 // the FP32 / BF16 / transposed BF16 stores. v: the raw accumulator values.
+// Epilogue features compiled into a GEMM instantiation (a launch only runs the code of its
+// own mode: with one tile per CTA, as in a training step, every CTA executes the epilogue
+// once, so code it does not need costs instruction fetches from L2).
+enum : int {
+    kEpBias = 1, kEpGelu = 2, kEpOutF = 4, kEpOutH = 8, kEpOutT = 16, kEpZin = 32, kEpColsum = 64, kEpNll = 128,
+    kEpAll = 255,
+    kModeForward = kEpBias | kEpGelu | kEpOutF | kEpOutH | kEpOutT,  // hidden layer of a training batch
+    kModeLoss = kEpBias | kEpOutF | kEpNll,                           // output layer of a training batch
+    kModeDz = kEpZin | kEpOutH | kEpOutT | kEpColsum,                 // dL/dZ of a hidden layer
+    kModeSplit = kEpOutF,                                             // split-K slices
+    kModeHidden = kEpBias | kEpGelu | kEpOutH,                        // prediction, hidden layer
+    kModeOut = kEpBias | kEpOutF,                                     // prediction, output layer
+};
+
+template <int MODE>
 __device__ __forceinline__ void epilogue_chunk(const Epilogue& ep, float* outf, int m, int n0, float (&v)[32]) {
-    if (ep.bias) {
+    if ((MODE & kEpBias) && ep.bias) {
         if (n0 + 32 <= ep.nb && (reinterpret_cast<uintptr_t>(ep.bias + n0) & 15) == 0) {
             // every lane reads the same 32 values: eight broadcast 16-byte loads
             const float4* b4 = reinterpret_cast<const float4*>(ep.bias + n0);
@@ -254,7 +276,7 @@ __device__ __forceinline__ void epilogue_chunk(const Epilogue& ep, float* outf, 
     }
     const bool row_ok = m < ep.m_store;
     const bool full = n0 + 32 <= ep.n_store;
-    if (outf && row_ok) {
+    if ((MODE & kEpOutF) && outf && row_ok) {
         float* p = outf + (size_t)m * ep.ldf + n0;
         if (full && (ep.ldf & 3) == 0 && (reinterpret_cast<uintptr_t>(outf) & 15) == 0) {
 #pragma unroll
@@ -266,10 +288,10 @@ __device__ __forceinline__ void epilogue_chunk(const Epilogue& ep, float* outf, 
                 if (n0 + j < ep.n_store) p[j] = v[j];
         }
     }
-    if (ep.nll && n0 == 0) nll_rows(ep, m, v[0], v[1]);
-    if (!ep.outh && !ep.outt) return;
+    if ((MODE & kEpNll) && ep.nll && n0 == 0) nll_rows(ep, m, v[0], v[1]);
+    if (!(MODE & (kEpOutH | kEpOutT)) || (!ep.outh && !ep.outt)) return;
     float g[32];
-    if (ep.zin) {
+    if ((MODE & kEpZin) && ep.zin) {
         if (row_ok && full && (ep.ldz & 3) == 0) {
             const float4* z4 = reinterpret_cast<const float4*>(ep.zin + (size_t)m * ep.ldz + n0);
 #pragma unroll
@@ -285,7 +307,7 @@ __device__ __forceinline__ void epilogue_chunk(const Epilogue& ep, float* outf, 
             for (int j = 0; j < 32; ++j)
                 g[j] = (row_ok && n0 + j < ep.n_store) ? v[j] * gelu_grad(ep.zin[(size_t)m * ep.ldz + n0 + j]) : 0.f;
         }
-    } else if (ep.gelu) {
+    } else if ((MODE & kEpGelu) && ep.gelu) {
 #pragma unroll
         for (int j = 0; j < 32; j += 2) {
             const float2 q = gelu2(make_float2(v[j], v[j + 1]));
@@ -296,7 +318,7 @@ __device__ __forceinline__ void epilogue_chunk(const Epilogue& ep, float* outf, 
 #pragma unroll
         for (int j = 0; j < 32; ++j) g[j] = v[j];
     }
-    if (ep.outh && row_ok) {
+    if ((MODE & kEpOutH) && ep.outh && row_ok) {
         bf16* p = ep.outh + (size_t)m * ep.ldh + n0;
         if (full && (ep.ldh & 7) == 0 && (reinterpret_cast<uintptr_t>(ep.outh) & 15) == 0) {
 #pragma unroll
@@ -316,13 +338,13 @@ __device__ __forceinline__ void epilogue_chunk(const Epilogue& ep, float* outf, 
                 if (n0 + j < ep.n_store) p[j] = bf16(g[j]);
         }
     }
-    if (ep.outt && row_ok) {
+    if ((MODE & kEpOutT) && ep.outt && row_ok) {
         // consecutive threads own consecutive rows: each column's stores are contiguous
 #pragma unroll
         for (int j = 0; j < 32; ++j)
             if (n0 + j < ep.n_store) ep.outt[(size_t)(n0 + j) * ep.ldt + m] = bf16(g[j]);
     }
-    if (ep.colsum) {
+    if ((MODE & kEpColsum) && ep.colsum) {
         // column sums over the warp's 32 rows of the BF16-rounded values (rows past m_store
         // add 0): a fixed butterfly that leaves column n0 + lane in lane `lane`
 #pragma unroll
@@ -342,7 +364,7 @@ __device__ __forceinline__ void epilogue_chunk(const Epilogue& ep, float* outf, 
 // accumulator back, so the epilogue of one tile overlaps the MMAs of the next. Every wait
 // is bounded; on a timeout the CTA records an error, stops, waits (bounded) for its own
 // copies and MMAs in flight, frees TMEM and returns.
-template <int BN>
+template <int BN, int MODE>
 __global__ void __launch_bounds__(kGemmThreads, 1)
     gemm_tma_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB, GemmWork w,
                     Epilogue ep, int* err) {
@@ -383,6 +405,10 @@ __global__ void __launch_bounds__(kGemmThreads, 1)
         *abort_flag = 1;
         atomicExch(err, 1);
     };
+    // prologue done: the next kernel may start its own; nothing of the predecessor's output is
+    // read (operands, bias, Z) or overwritten before it has completed
+    griddep_launch_dependents();
+    griddep_wait();
 
     if (warp == 0) {
         // ---- TMA producer (lane 0)
@@ -485,6 +511,14 @@ __global__ void __launch_bounds__(kGemmThreads, 1)
         for (int item = blockIdx.x; item < w.items && !*abort_flag; item += gridDim.x) {
             const int sp = item % w.splits, tile = item / w.splits;
             const int tn = tile % w.tiles_n, tm = tile / w.tiles_n;
+            if ((MODE & kEpZin) && ep.zin && tm * kBM + row < ep.m_store) {
+                // this thread's Z row segment is independent of the MMAs: start its loads now
+                const char* zr = reinterpret_cast<const char*>(ep.zin + (size_t)(tm * kBM + row) * ep.ldz +
+                                                               tn * BN + half * (BN / 2));
+#pragma unroll
+                for (int b = 0; b < (BN / 2) * 4; b += 128)
+                    asm volatile("prefetch.global.L1 [%0];" ::"l"(zr + b));
+            }
             if (!mbar_wait_bounded(accf_bar(buf), acc_phase)) {
                 fail();
                 break;
@@ -503,7 +537,7 @@ __global__ void __launch_bounds__(kGemmThreads, 1)
                 float v[32];
 #pragma unroll
                 for (int j = 0; j < 32; ++j) v[j] = __uint_as_float(r[j]);
-                epilogue_chunk(ep, outf, m, tn * BN + c0, v);
+                epilogue_chunk<MODE>(ep, outf, m, tn * BN + c0, v);
             }
             tc_fence_before();
             __syncwarp();
@@ -572,12 +606,17 @@ __device__ __forceinline__ float feature_phase(float u0, float u1, const float* 
     return __fmul_rn(6.283185307179586f, __fmaf_rn(u0, __ldg(Bf + 2 * j), __fmul_rn(u1, __ldg(Bf + 2 * j + 1))));
 }
 
-// One thread per (row, frequency): X[r, j] = sin(2 pi u.B_j), X[r, F/2 + j] = cos(...).
+// X[r, j] = sin(2 pi u.B_j), X[r, fourier + j] = cos(...). One thread per (row, group of
+// 8 frequencies); consecutive threads take consecutive rows of one group, so the transposed
+// copy's stores are contiguous across a warp and each row's 8 values go out as 16 bytes.
 __global__ void features_kernel(FeatureArgs a) {
+    griddep_launch_dependents();
+    griddep_wait();
     const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= (long long)a.rows * a.fourier) return;
-    const int r = (int)(t / a.fourier);
-    const int j = (int)(t % a.fourier);
+    const int groups = a.fourier / 8;
+    if (t >= (long long)a.rows * groups) return;
+    const int r = (int)(t % a.rows);
+    const int j0 = 8 * (int)(t / a.rows);
     long long i;
     bool valid;
     if (a.step) {
@@ -588,30 +627,47 @@ __global__ void features_kernel(FeatureArgs a) {
         i = a.row0 + r;
         valid = i < a.n;
     }
-    float s = 0.f, c = 0.f;
-    if (valid) {
-        float u0, u1;
-        input_point(a, i, u0, u1);
-        sincosf(feature_phase(u0, u1, a.Bf, j), &s, &c);
+    float u0 = 0.f, u1 = 0.f;
+    if (valid) input_point(a, i, u0, u1);
+    float sv[8], cv[8];
+#pragma unroll
+    for (int q = 0; q < 8; ++q) {
+        sv[q] = cv[q] = 0.f;
+        if (valid) sincosf(feature_phase(u0, u1, a.Bf, j0 + q), &sv[q], &cv[q]);
     }
     const int F = 2 * a.fourier;
-    a.X[(size_t)r * F + j] = bf16(s);
-    a.X[(size_t)r * F + a.fourier + j] = bf16(c);
+    uint4 ps, pc;
+    __nv_bfloat162 h;
+#define UCB_PACK(dst, v, k)                               \
+    h = __floats2bfloat162_rn(v[2 * k], v[2 * k + 1]); \
+    dst = *reinterpret_cast<uint32_t*>(&h);
+    UCB_PACK(ps.x, sv, 0) UCB_PACK(ps.y, sv, 1) UCB_PACK(ps.z, sv, 2) UCB_PACK(ps.w, sv, 3)
+    UCB_PACK(pc.x, cv, 0) UCB_PACK(pc.y, cv, 1) UCB_PACK(pc.z, cv, 2) UCB_PACK(pc.w, cv, 3)
+#undef UCB_PACK
+    *reinterpret_cast<uint4*>(a.X + (size_t)r * F + j0) = ps;
+    *reinterpret_cast<uint4*>(a.X + (size_t)r * F + a.fourier + j0) = pc;
     if (a.Xt) {
-        a.Xt[(size_t)j * a.rows + r] = bf16(s);
-        a.Xt[(size_t)(a.fourier + j) * a.rows + r] = bf16(c);
+#pragma unroll
+        for (int q = 0; q < 8; ++q) {
+            a.Xt[(size_t)(j0 + q) * a.rows + r] = bf16(sv[q]);
+            a.Xt[(size_t)(a.fourier + j0 + q) * a.rows + r] = bf16(cv[q]);
+        }
     }
-    if (j == 0 && a.yb) a.yb[r] = valid ? (a.y[i] - a.y_mean) * a.y_inv_std : 0.f;
+    if (j0 == 0 && a.yb) a.yb[r] = valid ? (a.y[i] - a.y_mean) * a.y_inv_std : 0.f;
 }
 
 // Gradient of a run of parameters as fixed-order sums of partial results: parameter off + e
 // (row o = e / cols, column c = e % cols) has the gradient
-//   sum over sp = 0 .. slices - 1, in that order, of part[sp * slice_stride + o * ld + c].
-// Weight runs read the split-K slices of their weight-gradient GEMM, bias runs the per-32-row
-// block sums of the epilogues (rows = 1). layer >= 0: a weight run whose BF16 copies
-// (W, W^T) are rewritten after the update.
+//   sum over sp = 0 .. slices - 1 of part[sp * slice_stride + o * ld + c],
+// added in a fixed order. Weight runs read the split-K slices of their weight-gradient GEMM
+// (a few; one thread per parameter adds them in slice order), bias runs the per-32-row block
+// sums of the epilogues (hundreds, rows = 1: one warp per parameter, lane l adding slices
+// l, l + 32, ... in order, then a fixed five-round shuffle tree whose lane-0 result is used).
+// layer >= 0: a weight run whose BF16 copies (W, W^T) are rewritten after the update.
+// base: the run's first index within its section (threads for weight runs, warps for bias
+// runs).
 struct GradRun {
-    long long off, count;
+    long long off, count, base;
     int cols, ld;
     const float* part;
     long long slice_stride;
@@ -621,18 +677,20 @@ struct GradRun {
 // One training step's optimiser: every parameter's gradient from its partial sums (the same
 // bits whatever the launch order of the backward kernels), Adam with cosine learning-rate
 // decay, and the BF16 copies of the updated weights (W for the forward products, W^T for the
-// backward ones). Thread n_params adds up the loss. update = 0: only the gradient is written
-// (to grad) and the loss; nothing else changes. The step counter lives on the device so that
-// a captured step replays unchanged; the last block to finish advances it, after every
-// block has read it.
+// backward ones). The grid's first `thread_blocks` blocks take the weight runs, one thread
+// per parameter; the rest take the bias runs, one warp per parameter, and one more warp adds
+// up the loss. update = 0: only the gradient is written (to grad) and the loss; nothing
+// else changes. The step counter lives on the device so that a captured step replays
+// unchanged; the last block to finish advances it, after every block has read it.
 struct AdamArgs {
     float* w;
     float* m;
     float* v;
     float* grad;  // optional copy of the gradient
-    long long n;
     GradRun run[2 * kMaxLayers];
-    int n_runs;
+    int n_wruns, n_runs;  // runs [0, n_wruns) weights, [n_wruns, n_runs) biases
+    long long n_wparams, n_bparams;
+    int thread_blocks;
     const float* blk;  // loss partials: blk[3 sp + 2], sp < n_blk
     int n_blk;
     float* loss;
@@ -646,48 +704,73 @@ struct AdamArgs {
     int in[kMaxLayers], outk[kMaxLayers];
 };
 
-__global__ void adam_kernel(AdamArgs a) {
-    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    const unsigned long long t = *a.step;  // 0-based
-    if (i < a.n) {
-        int k = 0;
-        while (k + 1 < a.n_runs && i >= a.run[k + 1].off) ++k;
-        const GradRun& r = a.run[k];
-        const long long e = i - r.off;
+__device__ __forceinline__ void adam_update(const AdamArgs& a, const GradRun& r, long long e, float gi,
+                                            unsigned long long t) {
+    const long long i = r.off + e;
+    if (a.grad) a.grad[i] = gi;
+    if (!a.update) return;
+    const float frac = a.total_steps > 1 ? fminf((float)t / (float)(a.total_steps - 1), 1.f) : 1.f;
+    const float lr = a.lr1 + 0.5f * (a.lr0 - a.lr1) * (1.f + cospif(frac));
+    const float c1 = 1.f - powf(a.b1, (float)(t + 1));
+    const float c2 = 1.f - powf(a.b2, (float)(t + 1));
+    const float mi = a.b1 * a.m[i] + (1.f - a.b1) * gi;
+    const float vi = a.b2 * a.v[i] + (1.f - a.b2) * gi * gi;
+    a.m[i] = mi;
+    a.v[i] = vi;
+    const float wi = a.w[i] - lr * (mi / c1) / (sqrtf(vi / c2) + a.eps);
+    a.w[i] = wi;
+    if (r.layer >= 0) {
+        const int l = r.layer;
         const int o = (int)(e / r.cols), c = (int)(e % r.cols);
-        const float* p = r.part + (size_t)o * r.ld + c;
-        float gi = 0.f;
-        int sp = 0;
-        for (; sp + 4 <= r.slices; sp += 4) {
-            float q[4];
+        a.W[l][(size_t)o * a.in[l] + c] = bf16(wi);
+        if (a.Wt[l] && o < a.outk[l]) a.Wt[l][(size_t)c * a.outk[l] + o] = bf16(wi);
+    }
+}
+
+__global__ void adam_kernel(AdamArgs a) {
+    griddep_wait();
+    const unsigned long long t = *a.step;  // 0-based
+    if ((int)blockIdx.x < a.thread_blocks) {
+        const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+        if (i < a.n_wparams) {
+            int k = 0;
+            while (k + 1 < a.n_wruns && i >= a.run[k + 1].base) ++k;
+            const GradRun& r = a.run[k];
+            const long long e = i - r.base;
+            const float* p = r.part + (size_t)(e / r.cols) * r.ld + (e % r.cols);
+            float gi = 0.f;
+            int sp = 0;
+            for (; sp + 4 <= r.slices; sp += 4) {
+                float q[4];
 #pragma unroll
-            for (int u = 0; u < 4; ++u) q[u] = p[(size_t)(sp + u) * r.slice_stride];
+                for (int u = 0; u < 4; ++u) q[u] = p[(size_t)(sp + u) * r.slice_stride];
 #pragma unroll
-            for (int u = 0; u < 4; ++u) gi += q[u];
-        }
-        for (; sp < r.slices; ++sp) gi += p[(size_t)sp * r.slice_stride];
-        if (a.grad) a.grad[i] = gi;
-        if (a.update) {
-            const float frac = a.total_steps > 1 ? fminf((float)t / (float)(a.total_steps - 1), 1.f) : 1.f;
-            const float lr = a.lr1 + 0.5f * (a.lr0 - a.lr1) * (1.f + cospif(frac));
-            const float c1 = 1.f - powf(a.b1, (float)(t + 1));
-            const float c2 = 1.f - powf(a.b2, (float)(t + 1));
-            const float mi = a.b1 * a.m[i] + (1.f - a.b1) * gi;
-            const float vi = a.b2 * a.v[i] + (1.f - a.b2) * gi * gi;
-            a.m[i] = mi;
-            a.v[i] = vi;
-            const float wi = a.w[i] - lr * (mi / c1) / (sqrtf(vi / c2) + a.eps);
-            a.w[i] = wi;
-            if (r.layer >= 0) {
-                const int l = r.layer;
-                a.W[l][(size_t)o * a.in[l] + c] = bf16(wi);
-                if (a.Wt[l] && o < a.outk[l]) a.Wt[l][(size_t)c * a.outk[l] + o] = bf16(wi);
+                for (int u = 0; u < 4; ++u) gi += q[u];
             }
+            for (; sp < r.slices; ++sp) gi += p[(size_t)sp * r.slice_stride];
+            adam_update(a, r, e, gi, t);
         }
-    } else if (i == a.n) {
-        float s = 0.f;
-        for (int b = 0; b < a.n_blk; ++b) s += a.blk[3 * b + 2];
-        *a.loss = s;
+    } else {
+        const long long wi = ((long long)(blockIdx.x - a.thread_blocks) * blockDim.x + threadIdx.x) / 32;
+        const int lane = threadIdx.x & 31;
+        if (wi < a.n_bparams) {
+            int k = a.n_wruns;
+            while (k + 1 < a.n_runs && wi >= a.run[k + 1].base) ++k;
+            const GradRun& r = a.run[k];
+            const long long e = wi - r.base;
+            float part = 0.f;
+            for (int sp = lane; sp < r.slices; sp += 32) part += r.part[(size_t)sp * r.slice_stride + e];
+#pragma unroll
+            for (int w = 16; w >= 1; w >>= 1) part += __shfl_xor_sync(0xffffffffu, part, w);
+            const float gi = __shfl_sync(0xffffffffu, part, 0);
+            if (lane == 0) adam_update(a, r, e, gi, t);
+        } else if (wi == a.n_bparams) {
+            float part = 0.f;
+            for (int b = lane; b < a.n_blk; b += 32) part += a.blk[3 * b + 2];
+#pragma unroll
+            for (int w = 16; w >= 1; w >>= 1) part += __shfl_xor_sync(0xffffffffu, part, w);
+            if (lane == 0) *a.loss = part;
+        }
     }
     if (!a.update) return;
     __syncthreads();
@@ -1096,12 +1179,31 @@ using ucbmlp::bf16;
 
 namespace {
 
-constexpr int kMaxSplits = 32;  // split-K slices per weight-gradient tile
+constexpr int kMaxSplits = 16;  // split-K slices per weight-gradient tile
 
 bool cu_ok(cudaError_t e, std::string& err, const char* what) {
     if (e == cudaSuccess) return true;
     err = std::string(what) + ": " + cudaGetErrorString(e);
     return false;
+}
+
+// Kernel launch, with programmatic stream serialisation when pdl is set (the kernel may start
+// while its predecessor in the stream finishes; the kernels wait with griddepcontrol before
+// touching memory).
+template <typename... KArgs, typename... Args>
+bool launch(bool pdl, void (*kernel)(KArgs...), dim3 grid, dim3 block, size_t smem, cudaStream_t st,
+            std::string& err, const char* what, Args&&... args) {
+    cudaLaunchConfig_t cfg{};
+    cfg.gridDim = grid;
+    cfg.blockDim = block;
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = st;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = pdl ? 1 : 0;
+    return cu_ok(cudaLaunchKernelEx(&cfg, kernel, std::forward<Args>(args)...), err, what);
 }
 
 template <class T>
@@ -1140,8 +1242,12 @@ struct Mlp {
     float* outp = nullptr;         // rows x 2
     float* yb = nullptr;
     bf16 *dout = nullptr, *doutT = nullptr;
-    bf16* dZ[2] = {nullptr, nullptr};   // dL/dZ of consecutive hidden layers (ping-pong)
-    bf16* dZt[2] = {nullptr, nullptr};  // and its transposed copy
+    std::vector<bf16*> dZ, dZt;    // dL/dZ of each hidden layer and its transposed copy
+    // training-step launches: programmatic dependent launch on, and a second stream for the
+    // weight-gradient products (forked from / joined to the caller's stream with events)
+    bool pdl = false;
+    cudaStream_t side = nullptr;
+    std::vector<cudaEvent_t> ev;
     // partial sums that the optimiser kernel adds in a fixed order: per layer the split-K
     // slices of the weight gradient, per hidden layer the bias-gradient sums of 32-row
     // blocks, and the output layer's per-block NLL sums
@@ -1165,6 +1271,8 @@ struct Mlp {
 
     ~Mlp() {
         if (graph) cudaGraphExecDestroy(graph);
+        for (cudaEvent_t x : ev) cudaEventDestroy(x);
+        if (side) cudaStreamDestroy(side);
         for (void* q : act_owned) cudaFree(q);
         for (void* q : pred_owned) cudaFree(q);
         for (void* q : owned) cudaFree(q);
@@ -1176,17 +1284,49 @@ namespace {
 std::mutex g_attr_mu;
 std::vector<int> g_attr_devices;
 
+// Every compiled GEMM instantiation: tile width x epilogue mode (the modes a training step
+// and the layer-by-layer prediction use, and one with every feature for anything else).
+constexpr int kGemmModes[] = {ucbmlp::kModeForward, ucbmlp::kModeLoss, ucbmlp::kModeDz, ucbmlp::kModeSplit,
+                              ucbmlp::kModeHidden,  ucbmlp::kModeOut,  ucbmlp::kEpAll};
+template <int BN, int I = 0, class F>
+void for_each_mode(F&& f) {
+    if constexpr (I < (int)(sizeof(kGemmModes) / sizeof(kGemmModes[0]))) {
+        f(ucbmlp::gemm_tma_kernel<BN, kGemmModes[I]>, ucbmlp::GemmCfg<BN>::kSmem, kGemmModes[I]);
+        for_each_mode<BN, I + 1>(f);
+    }
+}
+template <class F>
+void for_each_gemm(F&& f) {
+    for_each_mode<128>([&](auto k, int smem, int) { f(k, smem); });
+    for_each_mode<256>([&](auto k, int smem, int) { f(k, smem); });
+}
+// The epilogue mode of a launch: the smallest compiled one that covers the features it uses.
+int gemm_mode(const ucbmlp::Epilogue& ep) {
+    int need = 0;
+    if (ep.bias) need |= ucbmlp::kEpBias;
+    if (ep.gelu) need |= ucbmlp::kEpGelu;
+    if (ep.outf) need |= ucbmlp::kEpOutF;
+    if (ep.outh) need |= ucbmlp::kEpOutH;
+    if (ep.outt) need |= ucbmlp::kEpOutT;
+    if (ep.zin) need |= ucbmlp::kEpZin;
+    if (ep.colsum) need |= ucbmlp::kEpColsum;
+    if (ep.nll) need |= ucbmlp::kEpNll;
+    int best = ucbmlp::kEpAll;
+    for (int md : kGemmModes)
+        if ((need & ~md) == 0 && __builtin_popcount(md) < __builtin_popcount(best)) best = md;
+    return best;
+}
+
 // Dynamic shared memory above 48 KB is opted in once per device, before launches and
 // before any stream capture.
 bool set_gemm_attributes(int device, std::string& err) {
     std::lock_guard<std::mutex> lk(g_attr_mu);
     if (std::find(g_attr_devices.begin(), g_attr_devices.end(), device) != g_attr_devices.end()) return true;
-    cudaError_t ce = cudaFuncSetAttribute(ucbmlp::gemm_tma_kernel<128>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                          ucbmlp::GemmCfg<128>::kSmem);
-    if (!cu_ok(ce, err, "cudaFuncSetAttribute(gemm 128)")) return false;
-    ce = cudaFuncSetAttribute(ucbmlp::gemm_tma_kernel<256>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                              ucbmlp::GemmCfg<256>::kSmem);
-    if (!cu_ok(ce, err, "cudaFuncSetAttribute(gemm 256)")) return false;
+    cudaError_t ce = cudaSuccess;
+    for_each_gemm([&](auto kernel, int smem) {
+        if (ce == cudaSuccess) ce = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    });
+    if (!cu_ok(ce, err, "cudaFuncSetAttribute(gemm)")) return false;
     ce = cudaFuncSetAttribute(ucbmlp::mlp_infer_kernel<128>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                               ucbmlp::InferCfg<128>::kSmem);
     if (!cu_ok(ce, err, "cudaFuncSetAttribute(infer 128)")) return false;
@@ -1279,14 +1419,21 @@ bool gemm(Mlp& m, const bf16* A, const bf16* B, int M, int N, int K, const ucbml
     if (!tensor_map(&ta, A, M, K, ucbmlp::kBM, err) || !tensor_map(&tb, B, N, K, bn, err)) return false;
     ucbmlp::GemmWork w{N / bn, splits, kt, per, tiles * splits};
     const int grid = std::min(w.items, sms);
-    if (bn == 256)
-        ucbmlp::gemm_tma_kernel<256><<<grid, ucbmlp::kGemmThreads, ucbmlp::GemmCfg<256>::kSmem, st>>>(ta, tb, w, ep,
-                                                                                                      m.err);
-    else
-        ucbmlp::gemm_tma_kernel<128><<<grid, ucbmlp::kGemmThreads, ucbmlp::GemmCfg<128>::kSmem, st>>>(ta, tb, w, ep,
-                                                                                                      m.err);
     m.e->launches += 1;
-    return cu_ok(cudaPeekAtLastError(), err, "gemm launch");
+    const int mode = gemm_mode(ep);
+    bool ok = false, found = false;
+    auto go = [&](auto kernel, int smem, int md) {
+        if (found || md != mode) return;
+        found = true;
+        ok = launch(m.pdl, kernel, dim3(grid), dim3(ucbmlp::kGemmThreads), smem, st, err, "gemm launch", ta, tb, w,
+                    ep, m.err);
+    };
+    if (bn == 256)
+        for_each_mode<256>(go);
+    else
+        for_each_mode<128>(go);
+    if (!found) err = "gemm: no compiled epilogue mode";
+    return ok;
 }
 
 ucbmlp::Epilogue epi() {
@@ -1324,8 +1471,10 @@ bool ensure_rows(Mlp& m, int rows, std::string& err) {
     if (!(m.outp = dalloc<float>(R * 2, o, err, "out")) || !(m.yb = dalloc<float>(R, o, err, "y batch")) ||
         !(m.dout = dalloc<bf16>(R * 64, o, err, "dOut")) || !(m.doutT = dalloc<bf16>(R * 128, o, err, "dOut^T")))
         return false;
-    for (int b = 0; b < 2; ++b)
-        if (!(m.dZ[b] = dalloc<bf16>(R * m.H, o, err, "dZ")) || !(m.dZt[b] = dalloc<bf16>(R * m.H, o, err, "dZ^T")))
+    m.dZ.assign(m.L, nullptr);
+    m.dZt.assign(m.L, nullptr);
+    for (int l = 0; l < m.L; ++l)
+        if (!(m.dZ[l] = dalloc<bf16>(R * m.H, o, err, "dZ")) || !(m.dZt[l] = dalloc<bf16>(R * m.H, o, err, "dZ^T")))
             return false;
     m.part.assign(m.L + 1, nullptr);
     m.part_cap.assign(m.L + 1, 0);
@@ -1400,10 +1549,10 @@ ucbmlp::FeatureArgs feature_args(Mlp& m, const MlpInputs& in, long long row0, in
 }
 
 bool features(Mlp& m, const ucbmlp::FeatureArgs& a, cudaStream_t st, std::string& err) {
-    const long long t = (long long)a.rows * a.fourier;
-    ucbmlp::features_kernel<<<(unsigned)((t + 255) / 256), 256, 0, st>>>(a);
+    const long long t = (long long)a.rows * (a.fourier / 8);
     m.e->launches += 1;
-    return cu_ok(cudaPeekAtLastError(), err, "features launch");
+    return launch(m.pdl, ucbmlp::features_kernel, dim3((unsigned)((t + 255) / 256)), dim3(256), 0, st, err,
+                  "features launch", a);
 }
 
 // Forward pass over `rows` rows of m.X. keep: store Z and H^T for the backward pass and
@@ -1473,53 +1622,50 @@ bool forward_infer(Mlp& m, int rows, cudaStream_t st, std::string& err) {
 // dOut / dOut^T and the NLL block sums in blk): every product stores partial results only
 // (split-K slices of the weight gradients, 32-row block sums of the bias gradients); the
 // optimiser kernel adds them. dL/dZ of a hidden layer comes straight out of the epilogue of
-// the product that gives dL/dH (GELU backward fused), ping-ponging between two buffers.
+// the product that gives dL/dH (GELU backward fused). The weight-gradient products run on a
+// second stream beside that chain (each one forked when its dL/dZ is written, all joined
+// before the caller's stream goes on), so only the dL/dZ chain is on the critical path.
 bool backward(Mlp& m, int rows, cudaStream_t st, std::string& err) {
     const int Lo = m.L;
-    int cur = 0;
-    // dL/dZ of the last hidden layer = (dOut W_out) GELU'(Z), K padded to 64
-    {
-        ucbmlp::Epilogue ep = epi();
-        ep.zin = m.Z[Lo - 1];
-        ep.ldz = m.H;
-        ep.outh = m.dZ[cur];
-        ep.ldh = m.H;
-        ep.outt = m.dZt[cur];
-        ep.ldt = rows;
-        ep.colsum = m.dbp[Lo - 1];
-        ep.ldc = m.H;
-        if (!gemm(m, m.dout, m.Wt[Lo], rows, m.H, 64, ep, st, err)) return false;
-        // output-layer weight gradient dOut^T H (M padded to 128, rows 0 and 1 stored)
-        ucbmlp::Epilogue eg = epi();
-        eg.outf = m.part[Lo];
-        eg.ldf = m.H;
-        eg.atomic = 1;
-        eg.m_store = 2;
-        if (!gemm(m, m.doutT, m.Ht[Lo - 1], 128, m.H, rows, eg, st, err, &m.splits[Lo], m.part_cap[Lo])) return false;
-    }
-    for (int l = Lo - 1; l >= 0; --l) {
-        const bf16* prevT = l > 0 ? m.Ht[l - 1] : m.Xt;
-        const int in = m.in[l];
+    int evi = 0;
+    auto fork = [&]() {
+        cudaEvent_t e = m.ev[evi++];
+        return cu_ok(cudaEventRecord(e, st), err, "fork record") &&
+               cu_ok(cudaStreamWaitEvent(m.side, e, 0), err, "fork wait");
+    };
+    auto weight_grad = [&](int l, const bf16* At, const bf16* prevT) {
         ucbmlp::Epilogue eg = epi();
         eg.outf = m.part[l];
-        eg.ldf = in;
+        eg.ldf = m.in[l];
         eg.atomic = 1;
-        if (!gemm(m, m.dZt[cur], prevT, m.H, in, rows, eg, st, err, &m.splits[l], m.part_cap[l])) return false;
-        if (l > 0) {
-            ucbmlp::Epilogue ep = epi();
-            ep.zin = m.Z[l - 1];
-            ep.ldz = m.H;
-            ep.outh = m.dZ[cur ^ 1];
-            ep.ldh = m.H;
-            ep.outt = m.dZt[cur ^ 1];
-            ep.ldt = rows;
-            ep.colsum = m.dbp[l - 1];
-            ep.ldc = m.H;
-            if (!gemm(m, m.dZ[cur], m.Wt[l], rows, in, m.H, ep, st, err)) return false;
-            cur ^= 1;
+        int M = m.H;
+        if (l == Lo) {  // dOut^T H: M padded to 128, rows 0 and 1 stored
+            eg.m_store = 2;
+            M = 128;
         }
+        return gemm(m, At, prevT, M, m.in[l], rows, eg, m.side, err, &m.splits[l], m.part_cap[l]);
+    };
+    auto dz = [&](int l, const bf16* A, const bf16* Bt, int K) {  // dL/dZ of hidden layer l
+        ucbmlp::Epilogue ep = epi();
+        ep.zin = m.Z[l];
+        ep.ldz = m.H;
+        ep.outh = m.dZ[l];
+        ep.ldh = m.H;
+        ep.outt = m.dZt[l];
+        ep.ldt = rows;
+        ep.colsum = m.dbp[l];
+        ep.ldc = m.H;
+        return gemm(m, A, Bt, rows, m.H, K, ep, st, err);
+    };
+    // output layer: its weight gradient needs only dOut^T; dL/dZ of the last hidden layer is
+    // (dOut W_out) GELU'(Z), K padded to 64
+    if (!fork() || !weight_grad(Lo, m.doutT, m.Ht[Lo - 1]) || !dz(Lo - 1, m.dout, m.Wt[Lo], 64)) return false;
+    for (int l = Lo - 1; l >= 0; --l) {
+        if (!fork() || !weight_grad(l, m.dZt[l], l > 0 ? m.Ht[l - 1] : m.Xt)) return false;
+        if (l > 0 && !dz(l - 1, m.dZ[l], m.Wt[l], m.H)) return false;
     }
-    return true;
+    cudaEvent_t j = m.ev[evi++];
+    return cu_ok(cudaEventRecord(j, m.side), err, "join record") && cu_ok(cudaStreamWaitEvent(st, j, 0), err, "join wait");
 }
 
 // The optimiser kernel over the partial results of the last backward(rows): update = true
@@ -1531,24 +1677,32 @@ bool adam(Mlp& m, int rows, bool update, cudaStream_t st, std::string& err) {
     a.m = m.m1;
     a.v = m.m2;
     a.grad = update ? nullptr : m.g;
-    a.n = m.n_params;
     const int nblk = (rows + 31) / 32;
     int k = 0;
-    for (int l = 0; l <= m.L; ++l) {
-        const bool out = l == m.L;
+    long long base = 0;
+    for (int l = 0; l <= m.L; ++l) {  // weight runs: one thread per parameter
         ucbmlp::GradRun w{};
         w.off = m.w_off[l];
         w.count = (long long)m.out[l] * m.in[l];
+        w.base = base;
         w.cols = m.in[l];
         w.ld = m.in[l];
         w.part = m.part[l];
-        w.slice_stride = (long long)(out ? 2 : m.H) * m.in[l];
+        w.slice_stride = (long long)(l == m.L ? 2 : m.H) * m.in[l];
         w.slices = m.splits[l];
         w.layer = l;
         a.run[k++] = w;
+        base += w.count;
+    }
+    a.n_wruns = k;
+    a.n_wparams = base;
+    base = 0;
+    for (int l = 0; l <= m.L; ++l) {  // bias runs: one warp per parameter
+        const bool out = l == m.L;
         ucbmlp::GradRun b{};
         b.off = m.b_off[l];
         b.count = m.out[l];
+        b.base = base;
         b.cols = m.out[l];
         b.ld = 0;
         b.part = out ? m.blk : m.dbp[l];
@@ -1556,8 +1710,12 @@ bool adam(Mlp& m, int rows, bool update, cudaStream_t st, std::string& err) {
         b.slices = nblk;
         b.layer = -1;
         a.run[k++] = b;
+        base += b.count;
     }
     a.n_runs = k;
+    a.n_bparams = base;
+    a.thread_blocks = (int)((a.n_wparams + 255) / 256);
+    const long long warp_blocks = ((a.n_bparams + 1) * 32 + 255) / 256;  // + the loss warp
     a.blk = m.blk;
     a.n_blk = nblk;
     a.loss = m.loss;
@@ -1576,9 +1734,9 @@ bool adam(Mlp& m, int rows, bool update, cudaStream_t st, std::string& err) {
         a.in[l] = m.in[l];
         a.outk[l] = m.outk[l];
     }
-    ucbmlp::adam_kernel<<<(unsigned)((m.n_params + 1 + 255) / 256), 256, 0, st>>>(a);
     m.e->launches += 1;
-    return cu_ok(cudaPeekAtLastError(), err, "adam launch");
+    return launch(m.pdl, ucbmlp::adam_kernel, dim3((unsigned)(a.thread_blocks + warp_blocks)), dim3(256), 0, st,
+                  err, "adam launch", a);
 }
 
 bool check_kernel_error(Mlp& m, cudaStream_t st, std::string& err) {
@@ -1652,6 +1810,11 @@ Mlp* mlp_create(ucb_engine* e, const ucb_mlp_config& c, std::string& err) {
         m->W.push_back(w);
         m->Wt.push_back(wt);
     }
+    if (!cu_ok(cudaStreamCreateWithFlags(&m->side, cudaStreamNonBlocking), err, "weight-gradient stream"))
+        return nullptr;
+    m->ev.assign(m->L + 2, nullptr);
+    for (auto& x : m->ev)
+        if (!cu_ok(cudaEventCreateWithFlags(&x, cudaEventDisableTiming), err, "event")) return nullptr;
     if (!mlp_reinit(m.get(), err)) return nullptr;
     return m.release();
 }
@@ -1796,7 +1959,9 @@ bool mlp_fit(Mlp* m, const MlpInputs& in, const float* d_y, cudaStream_t st, flo
         cudaGraph_t g = nullptr;
         bool ok = cu_ok(cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal), err, "begin capture");
         if (ok) {
+            m->pdl = true;
             ok = train_step(*m, in, d_y, cs, err);
+            m->pdl = false;
             const cudaError_t ce = cudaStreamEndCapture(cs, &g);
             ok = ok && cu_ok(ce, err, "end capture");
         }
