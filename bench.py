@@ -863,7 +863,7 @@ def main():
                      # DRAM bytes per launch from one ncu capture of this kernel (384^2 map,
                      # 147,456 cells: 151 KB read, 0 B written — the outputs stay in L2),
                      # scaled by the cells of this map
-                     "traffic": 90.88e3 / 147456 * cells,
+                     "traffic": 41.98e3 / 147456 * cells,
                      "traffic_source": "scaled constant: dram__bytes_read + dram__bytes_write of one ncu capture "
                                        "of this FP32 kernel build at 384^2 (128-thread blocks), times cells / 384^2",
                      "peak_source": "measured FMA probe (ucb_measure_fma_peak) on this GPU in this run",

@@ -625,11 +625,16 @@ UCB_API int ucb_lle2d_cells(ucb_engine* e, const ucb_lle2d_request* req, const l
  * BF16 MLP surrogate (no counterpart in the reference). Input: a point u in [0, 1]^2 (the
  * two sweep coordinates of a map, normalised); Fourier features sin / cos(2 pi u B^T)
  * with a fixed Gaussian B (fourier x 2, std fourier_scale); `layers` hidden layers of
- * width `hidden` with exact GELU; outputs mean and log-variance of the target, trained on
- * the Gaussian negative log-likelihood (beta-NLL weighting: each row's loss is scaled by
- * a constant sigma^(2 beta)) with Adam and a cosine learning-rate decay. Matrix products
- * run on the tensor cores (tcgen05.mma, BF16 operands, FP32 accumulation in tensor
- * memory); masters and Adam moments are FP32.
+ * width `hidden` with GELU in its tanh form, 0.5 z (1 + tanh(sqrt(2/pi) (z + 0.044715 z^3)));
+ * outputs mean and log-variance of the target, trained on the Gaussian negative
+ * log-likelihood (beta-NLL weighting: each row's loss is scaled by a constant
+ * sigma^(2 beta)) with Adam and a cosine learning-rate decay. Matrix products run on the
+ * tensor cores (tcgen05.mma, BF16 operands, FP32 accumulation in tensor memory); masters
+ * and Adam moments are FP32. Training adds every partial sum in a fixed order (no
+ * floating-point atomics): a fit gives the same parameters bit for bit on every run.
+ * Prediction is one fused kernel per call when hidden is 128 or 256 and 2 * fourier <=
+ * hidden (features, every layer and the output of 128 rows in one CTA, activations in
+ * shared memory); other shapes run layer by layer. */
  *
  * Parameter vector layout (ucb_mlp_get_params): for each layer l = 0..layers (the last is
  * the output layer with 2 outputs), W_l[out][in] row-major, then b_l[out].

@@ -210,6 +210,7 @@ std::string make_prelude(int precision, int nx, int nv, const SweepMap& m, bool 
     if (sys.has_jvp) o << "#define UCB_HAS_JVP 1\n";
     for (auto& d : extra_defines) o << "#define " << d << "\n";
     o << "typedef " << (precision == UCB_PREC_F64 ? "double" : "float") << " numb;\n";
+    if (precision != UCB_PREC_F64) o << "#define UCB_NUMB_F32 1\n";
     // configCUDA.h pi / euler, visible to step bodies as in the reference template.
     o << "constexpr numb pi = (numb)3.1415926535897932384626433832795;\n";
     o << "constexpr numb euler = (numb)2.7182818284590452353602874713527;\n";
