@@ -634,7 +634,7 @@ UCB_API int ucb_lle2d_cells(ucb_engine* e, const ucb_lle2d_request* req, const l
  * floating-point atomics): a fit gives the same parameters bit for bit on every run.
  * Prediction is one fused kernel per call when hidden is 128 or 256 and 2 * fourier <=
  * hidden (features, every layer and the output of 128 rows in one CTA, activations in
- * shared memory); other shapes run layer by layer. */
+ * shared memory); other shapes run layer by layer.
  *
  * Parameter vector layout (ucb_mlp_get_params): for each layer l = 0..layers (the last is
  * the output layer with 2 outputs), W_l[out][in] row-major, then b_l[out].
