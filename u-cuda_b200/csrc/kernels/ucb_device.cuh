@@ -140,6 +140,52 @@ __device__ __forceinline__ void ucb_sincos(float v, float* s, float* c) { sincos
 #define UCB_CLOCK_ADVANCE(x) (void)0
 #endif
 
+#if defined(UCB_NUMB_F32) && !defined(UCB_SCALAR_STEP)
+// FP32 RK4 updates two components per packed instruction (FFMA2 / FADD2, sm_100): every
+// component of a stage point or of the final combination uses the same coefficient, and the
+// packed forms round each lane as the scalar ones do, so the results are unchanged.
+// out[i] = c k[i] + x[i]
+__device__ __forceinline__ void rk4_axpy(float c, const float* k, const float* x, float* out) {
+    const float2 cc = make_float2(c, c);
+#pragma unroll
+    for (int i = 0; i + 1 < UCB_NX; i += 2) {
+        const float2 t = __ffma2_rn(cc, make_float2(k[i], k[i + 1]), make_float2(x[i], x[i + 1]));
+        out[i] = t.x;
+        out[i + 1] = t.y;
+    }
+    if (UCB_NX & 1) out[UCB_NX - 1] = fmaf(c, k[UCB_NX - 1], x[UCB_NX - 1]);
+}
+// x[i] = h6 ((k1[i] + k4[i]) + 2 (k2[i] + k3[i])) + x[i]
+__device__ __forceinline__ void rk4_combine(float h6, const float* k1, const float* k2, const float* k3,
+                                            const float* k4, float* x) {
+    const float2 c6 = make_float2(h6, h6), two = make_float2(2.0f, 2.0f);
+#pragma unroll
+    for (int i = 0; i + 1 < UCB_NX; i += 2) {
+        const float2 s14 = __fadd2_rn(make_float2(k1[i], k1[i + 1]), make_float2(k4[i], k4[i + 1]));
+        const float2 s23 = __fadd2_rn(make_float2(k2[i], k2[i + 1]), make_float2(k3[i], k3[i + 1]));
+        const float2 t = __ffma2_rn(c6, __ffma2_rn(two, s23, s14), make_float2(x[i], x[i + 1]));
+        x[i] = t.x;
+        x[i + 1] = t.y;
+    }
+    if (UCB_NX & 1) {
+        const int i = UCB_NX - 1;
+        x[i] = fmaf(h6, (k1[i] + k4[i]) + 2.0f * (k2[i] + k3[i]), x[i]);
+    }
+}
+#define UCB_RK4_AXPY(c, k, x, out) rk4_axpy((c), (k), (x), (out))
+#define UCB_RK4_COMBINE(h6, k1, k2, k3, k4, x) rk4_combine((h6), (k1), (k2), (k3), (k4), (x))
+#else
+#define UCB_RK4_AXPY(c, k, x, out)                                              \
+    do {                                                                        \
+        _Pragma("unroll") for (int i_ = 0; i_ < UCB_NX; ++i_)(out)[i_] = fma((c), (k)[i_], (x)[i_]); \
+    } while (0)
+#define UCB_RK4_COMBINE(h6, k1, k2, k3, k4, x)                                                     \
+    do {                                                                                           \
+        _Pragma("unroll") for (int i_ = 0; i_ < UCB_NX; ++i_)(x)[i_] =                             \
+            fma((h6), ((k1)[i_] + (k4)[i_]) + (numb)2 * ((k2)[i_] + (k3)[i_]), (x)[i_]);          \
+    } while (0)
+#endif
+
 // Classical RK4 on ucb_rhs, FMA-ordered: the same scheme as codegen.cpp scheme_rk4
 // (k1..k4 at t, t+h/2, t+h/2, t+h; x += h/6 (k1 + 2k2 + 2k3 + k4)) with the half/sixth
 // step factors hoisted and every update written as a fused multiply-add.
@@ -197,18 +243,14 @@ struct Stepper {
 #else
         numb k1[UCB_NX], k2[UCB_NX], k3[UCB_NX], k4[UCB_NX], xt[UCB_NX];
         ucb_rhs(x, a, k1);
-#pragma unroll
-        for (int i = 0; i < UCB_NX; ++i) xt[i] = fma(hh, k1[i], x[i]);
+        UCB_RK4_AXPY(hh, k1, x, xt);
         ucb_rhs(xt, a, k2);
-#pragma unroll
-        for (int i = 0; i < UCB_NX; ++i) xt[i] = fma(hh, k2[i], x[i]);
+        UCB_RK4_AXPY(hh, k2, x, xt);
         ucb_rhs(xt, a, k3);
-#pragma unroll
-        for (int i = 0; i < UCB_NX; ++i) xt[i] = fma(h, k3[i], x[i]);
+        UCB_RK4_AXPY(h, k3, x, xt);
         ucb_rhs(xt, a, k4);
         UCB_CLOCK_SAVE(x);
-#pragma unroll
-        for (int i = 0; i < UCB_NX; ++i) x[i] = fma(h6, (k1[i] + k4[i]) + (numb)2 * (k2[i] + k3[i]), x[i]);
+        UCB_RK4_COMBINE(h6, k1, k2, k3, k4, x);
         UCB_CLOCK_ADVANCE(x);
 #endif
     }
@@ -219,18 +261,14 @@ struct Stepper {
         numb k1[UCB_NX], k2[UCB_NX], k3[UCB_NX], k4[UCB_NX], xt[UCB_NX];
         const numb c0 = tc[0], s0 = tc[1], c1 = tc[2], s1 = tc[3], c2 = tc[4], s2 = tc[5];
         ucb_rhs_trig(x, a, k1, c0, s0);
-#pragma unroll
-        for (int i = 0; i < UCB_NX; ++i) xt[i] = fma(hh, k1[i], x[i]);
+        UCB_RK4_AXPY(hh, k1, x, xt);
         ucb_rhs_trig(xt, a, k2, c1, s1);
-#pragma unroll
-        for (int i = 0; i < UCB_NX; ++i) xt[i] = fma(hh, k2[i], x[i]);
+        UCB_RK4_AXPY(hh, k2, x, xt);
         ucb_rhs_trig(xt, a, k3, c1, s1);
-#pragma unroll
-        for (int i = 0; i < UCB_NX; ++i) xt[i] = fma(h, k3[i], x[i]);
+        UCB_RK4_AXPY(h, k3, x, xt);
         ucb_rhs_trig(xt, a, k4, c2, s2);
         UCB_CLOCK_SAVE(x);
-#pragma unroll
-        for (int i = 0; i < UCB_NX; ++i) x[i] = fma(h6, (k1[i] + k4[i]) + (numb)2 * (k2[i] + k3[i]), x[i]);
+        UCB_RK4_COMBINE(h6, k1, k2, k3, k4, x);
         UCB_CLOCK_ADVANCE(x);
     }
 #endif
