@@ -122,6 +122,41 @@ def test_gpu_prediction_matches_oracle(ucb_engine):
 
 
 @pytest.mark.gpu
+def test_gpu_layer_by_layer_path_matches_oracle(ucb_engine):
+    """A hidden width the fused kernels do not cover (384) runs the features kernel and one
+    GEMM per layer, for training and prediction alike: gradients and predictions against
+    the oracle."""
+    import torch
+    import ucb
+    hidden, layers = 384, 2
+    net = ucb.Mlp(ucb_engine, fourier=FOURIER, hidden=hidden, layers=layers, fourier_scale=3.0, seed=5, batch=1024,
+                  train_steps=1)
+    rng = np.random.default_rng(21)
+    net.set_params(_rand_params(rng, FOURIER, hidden, layers).astype(np.float32))
+    n = 2000
+    u = rng.uniform(size=(n, 2)).astype(np.float32)
+    y = (np.sin(4 * u[:, 0]) + 0.1 * rng.normal(size=n)).astype(np.float32)
+    net.set_target_scale(0.1, 0.8)
+    p = net.get_params()
+    B = net.fourier()
+    loss, g = net.loss_grad(u, y)
+    lo, go = MO.loss_and_grad(p, B, u, y, hidden, layers, beta=0.5, y_mean=0.1, y_std=0.8, bf16=True)
+    assert abs(loss - lo) <= 2e-3 * abs(lo) + 1e-6
+    rel = np.linalg.norm(g - go) / np.linalg.norm(go)
+    assert rel < 2e-2, rel
+    du = torch.from_numpy(u).cuda()
+    dm = torch.empty(n, device="cuda")
+    ds = torch.empty(n, device="cuda")
+    net.predict(du.data_ptr(), n, dm.data_ptr(), ds.data_ptr())
+    torch.cuda.synchronize()
+    m_ref, s_ref = MO.predict(p, B, u, hidden, layers, y_mean=0.1, y_std=0.8)
+    scale = np.abs(m_ref).max()
+    assert np.max(np.abs(dm.cpu().numpy() - m_ref)) < 1e-2 * scale + 1e-5
+    assert np.max(np.abs(ds.cpu().numpy() / s_ref - 1)) < 1e-2
+    net.close()
+
+
+@pytest.mark.gpu
 @pytest.mark.parametrize("n", [1, 127, 129, 40000])
 def test_gpu_fused_prediction_matches_oracle_at_the_surrogate_size(ucb_engine, n):
     """The fused prediction kernel (features, hidden layers and output of a 128-row tile in
