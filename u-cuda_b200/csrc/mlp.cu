@@ -2,21 +2,21 @@
 // kernels and the training / prediction host code (no reference counterpart).
 //
 // GEMM (training): C[M, N] = A[M, K] B[N, K]^T with A and B K-contiguous ("TN"),
-// M % 128 == 0, N % 128 == 0, K % 64 == 0. A persistent kernel (one CTA of 320 threads per
+// M % 128 == 0, N % 128 == 0, K % 64 == 0. A persistent kernel (one CTA of 576 threads per
 // SM) walks tiles of 128 x 256 or 128 x 128 (the narrower tile when N is not a multiple of
 // 256 or when the wide tiles would leave SMs idle) and K splits: warp 0 streams 64-wide K
 // chunks of A and B with TMA (128-byte swizzle, no multicast) into a ring of shared-memory
 // stages, warp 1 issues tcgen05.mma (CuTe SM100_MMA_F16BF16_SS, cta_group::1, BF16 x BF16
-// -> FP32) from one elected lane into one of two TMEM accumulators, and warps 2-9 read a
-// finished accumulator with tcgen05.ld (two warps per 32-lane TMEM quadrant, one half of
+// -> FP32) from one elected lane into one of two TMEM accumulators, and warps 2-17 read a
+// finished accumulator with tcgen05.ld (four warps per 32-lane TMEM quadrant, a quarter of
 // the columns each; thread t of a quadrant owns row t) while the next tile's MMAs run,
-// apply bias / GELU and store FP32, BF16 and / or transposed BF16 copies straight from
-// registers. Waits are bounded; on a timeout the kernel records an error, waits for its
-// own copies and MMAs, frees TMEM and returns. A split-K launch stores each split's partial
-// tile in its own slice of a buffer, and a second kernel adds the slices in split order (so
-// a training step gives the same bits every time it runs). Backward products are the same
-// TN GEMM on transposed copies, which the forward epilogue and the GELU-backward kernel
-// write as they go.
+// apply bias / GELU and store FP32, BF16 and / or transposed BF16 copies through a per-warp
+// shared-memory staging buffer (whole 16-byte pieces per store instruction). Waits are
+// bounded; on a timeout the kernel records an error, waits for its own copies and MMAs,
+// frees TMEM and returns. A split-K launch stores each split's partial tile in its own
+// slice of a buffer, and the optimiser kernel adds the slices in split order (so a
+// training step gives the same bits every time it runs). Backward products are the same TN
+// GEMM on transposed copies, which the forward and dL/dZ epilogues write as they go.
 //
 // Prediction: one fused kernel per call (mlp_infer_kernel) runs features, every hidden
 // layer and the output transform of a 128-row tile inside one CTA, with the activations in
@@ -53,8 +53,8 @@ using bf16 = cutlass::bfloat16_t;
 constexpr int kBM = 128;   // rows of a tile (UMMA M, one TMEM lane per row)
 constexpr int kBK = 64;    // K per pipeline stage: one 128-byte swizzle row of BF16
 constexpr long long kWaitLimit = 1LL << 22;  // try_wait polls before a wait gives up
-constexpr int kEpiWarps = 8;      // two per 32-lane TMEM quadrant, each half of the columns
-constexpr int kGemmThreads = 64 + 32 * kEpiWarps;  // warp 0 TMA, warp 1 MMA, warps 2-9 epilogue
+constexpr int kEpiWarps = 16;     // four per 32-lane TMEM quadrant, a quarter of the columns each
+constexpr int kGemmThreads = 64 + 32 * kEpiWarps;  // warp 0 TMA, warp 1 MMA, warps 2-17 epilogue
 constexpr int kMaxLayers = 9;     // hidden layers + the output layer
 
 // Shapes and shared-memory layout of the persistent GEMM for a tile width BN (128 or 256).
@@ -66,13 +66,15 @@ struct GemmCfg {
         UMMA::Layout_K_SW128_Atom<bf16>{}, partition_shape_A(TiledMma{}, make_shape(Int<kBM>{}, Int<kBK>{}))));
     using LayoutB = decltype(UMMA::tile_to_mma_shape(
         UMMA::Layout_K_SW128_Atom<bf16>{}, partition_shape_B(TiledMma{}, make_shape(Int<BN>{}, Int<kBK>{}))));
-    static constexpr int kStages = BN == 256 ? 4 : 6;
+    static constexpr int kStages = BN == 256 ? 3 : 4;
     static constexpr int kABytes = kBM * kBK * 2;
     static constexpr int kBBytes = BN * kBK * 2;
     static constexpr int kStageBytes = kABytes + kBBytes;  // multiple of 1024: every stage stays 1024-aligned
     // barriers: full / empty per stage, accumulator full / empty per TMEM buffer, drain
     static constexpr int kBarriers = 2 * kStages + 2 + 2 + 1;
-    static constexpr int kSmem = 1024 + kStages * kStageBytes + 8 * kBarriers + 16;
+    static constexpr int kEpiStage = 4096;  // per epilogue warp: staging of one 32 x 32 chunk
+    static constexpr int kSmem = 1024 + kStages * kStageBytes + kEpiWarps * kEpiStage + 8 * kBarriers + 16;
+    static_assert(kSmem <= 232448, "GEMM shared memory above the per-CTA limit");
     static_assert(kStageBytes % 1024 == 0, "swizzled stages need 1024-byte alignment");
     static_assert(2 * BN <= 512, "two accumulators must fit in TMEM");
 };
@@ -254,8 +256,55 @@ enum : int {
     kModeOut = kEpBias | kEpOutF,                                     // prediction, output layer
 };
 
+// Stores of a warp's 32 x 32 chunk (one row per lane) through the warp's 4 KB staging buffer
+// in shared memory, so that each global store instruction writes whole 16-byte pieces of a
+// few rows (or columns) instead of one scattered piece per lane.
+//
+// Row-major: 32 rows of W 32-bit words (lane r's row is vals) to g + r * stride (bytes; g is
+// row 0 of the warp). 16-byte unit q of row r sits at unit q ^ swz(r) of the row in the
+// buffer, which keeps both the writes (one row per lane) and the reads (whole rows) free of
+// bank conflicts.
+template <int W>
+__device__ __forceinline__ void rows_staged(uint32_t* stage, const uint32_t (&vals)[W], char* g, size_t stride) {
+    constexpr int U = W / 4;  // 16-byte units per row: 8 (FP32) or 4 (BF16)
+    const int lane = threadIdx.x & 31;
+    auto swz = [](int r) { return U == 8 ? (r & 7) : ((r >> 1) & 3); };
+    uint4* s4 = reinterpret_cast<uint4*>(stage);
+#pragma unroll
+    for (int q = 0; q < U; ++q)
+        s4[lane * U + (q ^ swz(lane))] = make_uint4(vals[4 * q], vals[4 * q + 1], vals[4 * q + 2], vals[4 * q + 3]);
+    __syncwarp();
+#pragma unroll
+    for (int pass = 0; pass < U; ++pass) {
+        const int r = pass * (32 / U) + lane / U, q = lane % U;
+        *reinterpret_cast<uint4*>(g + (size_t)r * stride + q * 16) = s4[r * U + (q ^ swz(r))];
+    }
+    __syncwarp();
+}
+// Transposed BF16: column j of the chunk (its 32 rows) to outt + j * ld (elements; outt points
+// at column 0, row 0 of the warp). The buffer holds the chunk column-major, so each column's
+// 64 bytes are contiguous; a store instruction writes 16-byte pieces of eight columns.
+__device__ __forceinline__ void cols_staged(uint32_t* stage, const float (&g)[32], bf16* outt, size_t ld) {
+    const int lane = threadIdx.x & 31;
+    unsigned short* s2 = reinterpret_cast<unsigned short*>(stage);
+#pragma unroll
+    for (int j = 0; j < 32; ++j) {
+        const bf16 b = bf16(g[j]);
+        s2[j * 32 + lane] = *reinterpret_cast<const unsigned short*>(&b);
+    }
+    __syncwarp();
+    const uint4* s4 = reinterpret_cast<const uint4*>(stage);
+#pragma unroll
+    for (int pass = 0; pass < 4; ++pass) {
+        const int j = pass * 8 + lane / 4, q = lane % 4;
+        *reinterpret_cast<uint4*>(outt + (size_t)j * ld + q * 8) = s4[j * 4 + q];
+    }
+    __syncwarp();
+}
+
 template <int MODE>
-__device__ __forceinline__ void epilogue_chunk(const Epilogue& ep, float* outf, int m, int n0, float (&v)[32]) {
+__device__ __forceinline__ void epilogue_chunk(const Epilogue& ep, float* outf, int m, int n0, float (&v)[32],
+                                               uint32_t* stage) {
     if ((MODE & kEpBias) && ep.bias) {
         if (n0 + 32 <= ep.nb && (reinterpret_cast<uintptr_t>(ep.bias + n0) & 15) == 0) {
             // every lane reads the same 32 values: eight broadcast 16-byte loads
@@ -276,7 +325,16 @@ __device__ __forceinline__ void epilogue_chunk(const Epilogue& ep, float* outf, 
     }
     const bool row_ok = m < ep.m_store;
     const bool full = n0 + 32 <= ep.n_store;
-    if ((MODE & kEpOutF) && outf && row_ok) {
+    // the whole warp's 32 rows are stored: the staged (coalesced) paths apply
+    const bool warp_rows = __all_sync(0xffffffffu, row_ok);
+    const int m0 = m - (int)(threadIdx.x & 31);
+    if ((MODE & kEpOutF) && outf && warp_rows && full && (ep.ldf & 3) == 0 &&
+        (reinterpret_cast<uintptr_t>(outf) & 15) == 0) {
+        uint32_t w[32];
+#pragma unroll
+        for (int j = 0; j < 32; ++j) w[j] = __float_as_uint(v[j]);
+        rows_staged<32>(stage, w, reinterpret_cast<char*>(outf + (size_t)m0 * ep.ldf + n0), (size_t)ep.ldf * 4);
+    } else if ((MODE & kEpOutF) && outf && row_ok) {
         float* p = outf + (size_t)m * ep.ldf + n0;
         if (full && (ep.ldf & 3) == 0 && (reinterpret_cast<uintptr_t>(outf) & 15) == 0) {
 #pragma unroll
@@ -318,7 +376,16 @@ __device__ __forceinline__ void epilogue_chunk(const Epilogue& ep, float* outf, 
 #pragma unroll
         for (int j = 0; j < 32; ++j) g[j] = v[j];
     }
-    if ((MODE & kEpOutH) && ep.outh && row_ok) {
+    if ((MODE & kEpOutH) && ep.outh && warp_rows && full && (ep.ldh & 7) == 0 &&
+        (reinterpret_cast<uintptr_t>(ep.outh) & 15) == 0) {
+        uint32_t w[16];
+#pragma unroll
+        for (int j = 0; j < 32; j += 2) {
+            __nv_bfloat162 h = __floats2bfloat162_rn(g[j], g[j + 1]);
+            w[j / 2] = *reinterpret_cast<uint32_t*>(&h);
+        }
+        rows_staged<16>(stage, w, reinterpret_cast<char*>(ep.outh + (size_t)m0 * ep.ldh + n0), (size_t)ep.ldh * 2);
+    } else if ((MODE & kEpOutH) && ep.outh && row_ok) {
         bf16* p = ep.outh + (size_t)m * ep.ldh + n0;
         if (full && (ep.ldh & 7) == 0 && (reinterpret_cast<uintptr_t>(ep.outh) & 15) == 0) {
 #pragma unroll
@@ -338,7 +405,10 @@ __device__ __forceinline__ void epilogue_chunk(const Epilogue& ep, float* outf, 
                 if (n0 + j < ep.n_store) p[j] = bf16(g[j]);
         }
     }
-    if ((MODE & kEpOutT) && ep.outt && row_ok) {
+    if ((MODE & kEpOutT) && ep.outt && warp_rows && full && (ep.ldt & 7) == 0 &&
+        (reinterpret_cast<uintptr_t>(ep.outt) & 15) == 0) {
+        cols_staged(stage, g, ep.outt + (size_t)n0 * ep.ldt + m0, (size_t)ep.ldt);
+    } else if ((MODE & kEpOutT) && ep.outt && row_ok) {
         // consecutive threads own consecutive rows: each column's stores are contiguous
 #pragma unroll
         for (int j = 0; j < 32; ++j)
@@ -359,7 +429,7 @@ __device__ __forceinline__ void epilogue_chunk(const Epilogue& ep, float* outf, 
 // Persistent and warp-specialised: warp 0 streams K chunks of A and B into a ring of
 // shared-memory stages with TMA (128-byte swizzle, the layout the MMA descriptors read),
 // warp 1 issues tcgen05.mma from one elected lane into one of two TMEM accumulators and
-// commits to the stage's and the accumulator's mbarriers, warps 2-9 (two per 32-lane TMEM
+// commits to the stage's and the accumulator's mbarriers, warps 2-17 (four per 32-lane TMEM
 // quadrant) read finished accumulators with tcgen05.ld, run the epilogue and hand the
 // accumulator back, so the epilogue of one tile overlaps the MMAs of the next. Every wait
 // is bounded; on a timeout the CTA records an error, stops, waits (bounded) for its own
@@ -373,7 +443,8 @@ __global__ void __launch_bounds__(kGemmThreads, 1)
     typename Cfg::TiledMma tiled_mma;
     extern __shared__ char smem_raw[];
     char* base = reinterpret_cast<char*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
-    uint64_t* bars = reinterpret_cast<uint64_t*>(base + S * Cfg::kStageBytes);
+    char* epi_stage = base + S * Cfg::kStageBytes;
+    uint64_t* bars = reinterpret_cast<uint64_t*>(epi_stage + kEpiWarps * Cfg::kEpiStage);
     uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bars + Cfg::kBarriers);
     volatile int* abort_flag = reinterpret_cast<volatile int*>(tmem_slot + 1);
     auto full_bar = [&](int s) { return smem_u32(bars + s); };
@@ -504,7 +575,7 @@ __global__ void __launch_bounds__(kGemmThreads, 1)
     } else {
         // ---- epilogue: warp w reads TMEM lanes 32 (w % 4) .. + 31 (the lanes its quadrant may
         // access) and, with (w - 2) / 4, one half of the columns
-        const int quad = warp & 3, half = (warp - 2) >> 2;
+        const int quad = warp & 3, part = (warp - 2) >> 2;
         const int row = quad * 32 + lane;
         int buf = 0;
         uint32_t acc_phase = 0;
@@ -514,9 +585,9 @@ __global__ void __launch_bounds__(kGemmThreads, 1)
             if ((MODE & kEpZin) && ep.zin && tm * kBM + row < ep.m_store) {
                 // this thread's Z row segment is independent of the MMAs: start its loads now
                 const char* zr = reinterpret_cast<const char*>(ep.zin + (size_t)(tm * kBM + row) * ep.ldz +
-                                                               tn * BN + half * (BN / 2));
+                                                               tn * BN + part * (BN / 4));
 #pragma unroll
-                for (int b = 0; b < (BN / 2) * 4; b += 128)
+                for (int b = 0; b < (BN / 4) * 4; b += 128)
                     asm volatile("prefetch.global.L1 [%0];" ::"l"(zr + b));
             }
             if (!mbar_wait_bounded(accf_bar(buf), acc_phase)) {
@@ -528,7 +599,7 @@ __global__ void __launch_bounds__(kGemmThreads, 1)
             const int m = tm * kBM + row;
             const uint32_t taddr = tmem_base + (uint32_t)(buf * BN) + ((uint32_t)(quad * 32) << 16);
 #pragma unroll 1
-            for (int c0 = half * (BN / 2); c0 < (half + 1) * (BN / 2); c0 += 32) {
+            for (int c0 = part * (BN / 4); c0 < (part + 1) * (BN / 4); c0 += 32) {
                 uint32_t r[32];
                 asm volatile("tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15, %16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31}, [%32];\n"
                              : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]), "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]), "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
@@ -537,7 +608,8 @@ __global__ void __launch_bounds__(kGemmThreads, 1)
                 float v[32];
 #pragma unroll
                 for (int j = 0; j < 32; ++j) v[j] = __uint_as_float(r[j]);
-                epilogue_chunk<MODE>(ep, outf, m, tn * BN + c0, v);
+                epilogue_chunk<MODE>(ep, outf, m, tn * BN + c0, v,
+                                     reinterpret_cast<uint32_t*>(epi_stage + (warp - 2) * Cfg::kEpiStage));
             }
             tc_fence_before();
             __syncwarp();
