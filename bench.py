@@ -567,6 +567,17 @@ def run_other_configs(eng, which=OTHER_CONFIGS, args=None):
             "rhs_evals_per_s": res.steps / (res.kernel_ms * 1e-3), "valid_cells": int(ok.sum()),
             "median_spectrum": [float(np.median(v[k][ok])) for k in range(4)],
             "median_sum": float(np.median(v[:, ok].sum(axis=0)))}
+        if prec == ucb.PREC_F64:
+            dp5_fp64 = (v.copy(), ok.copy())
+        else:
+            # the FP32 form (rtol 1e-5) against the FP64 one (rtol 1e-8), cell by cell
+            v64, ok64 = dp5_fp64
+            both = ok & ok64
+            out["ls_hyper_rossler_512_dp5"]["fp32_vs_fp64"] = {
+                "valid_in_both": int(both.sum()), "valid_fp64_only": int((ok64 & ~ok).sum()),
+                "valid_fp32_only": int((ok & ~ok64).sum()),
+                "median_abs_diff": [float(np.median(np.abs(v[k][both] - v64[k][both]))) if both.any() else None
+                                    for k in range(4)]}
     # The reference's spectrum method (run_ls_2d: fixed-step RK4, Gram-Schmidt of the four
     # tangent vectors every NT) on the hyper-chaotic window (0.25, 0.05) +- (0.01, 0.005) of
     # the same system, 256 x 256 cells, h = 0.01, 10 transient + 100 measured time units.

@@ -60,6 +60,42 @@ def test_fixed_exact_matches_oracle(eng, case):
     assert res.steps > 0
 
 
+def test_fixed_fp32_tangent_lorenz_divergence_identity(eng):
+    """The native FP32 form of the fixed method follows tangent vectors (FP64 Gram-Schmidt,
+    norms and log sums): for Lorenz, whose divergence is the constant -(sigma + 1 + beta),
+    the spectrum sums to it exactly, times (NT/h + 1)/(NT/h) for the extra step of every
+    block, on every cell of a sigma sweep."""
+    c = lorenz_case(n=4, t_max=50.0)
+    v, f, res = eng.run_ls2d(ls_request(c, ucb.LS_FIXED, precision=ucb.PREC_F32, mode=ucb.MODE_NATIVE))
+    assert (f == 1).all() and np.isfinite(v).all()
+    n = c["n_pts"]
+    # cells in kernel order: axis 0 (sigma, param_index 1) varies fastest
+    sig = np.tile(np.linspace(c["param_lo"], c["param_hi"], n), n)
+    expect = -(sig + 1 + 8 / 3) * (0.1 / 0.01 + 1) / (0.1 / 0.01)
+    np.testing.assert_allclose(v.sum(axis=0), expect, atol=5e-3)
+    assert (v[0] > 0.5).all()
+
+
+def test_fixed_fp32_tangent_against_fp64_on_the_hyperchaotic_window(eng):
+    """On the hyper-chaotic Rossler window with eps = 1e-6 (where FP32 shadow differences
+    vanish), the FP32 tangent form stays finite and follows the FP64 map. Cells are chaotic,
+    so single cells part after a few Lyapunov times: the spectrum sum (the time average of the
+    Jacobian's trace along the trajectory) is compared per cell within 1 % at the median, and
+    each exponent through its median over the map."""
+    c = hyper_case(n=8, param_lo=0.24, param_hi=0.26, param_lo_2=0.045, param_hi_2=0.055, transient_time=10.0,
+                   t_max=100.0)
+    v64, f64, _ = eng.run_ls2d(ls_request(c, ucb.LS_FIXED, precision=ucb.PREC_F64, mode=ucb.MODE_NATIVE))
+    v32, f32, _ = eng.run_ls2d(ls_request(c, ucb.LS_FIXED, precision=ucb.PREC_F32, mode=ucb.MODE_NATIVE))
+    both = (f64 == 1) & (f32 == 1)
+    assert both.sum() >= 0.9 * both.size
+    assert np.isfinite(v32[:, both]).all()
+    s32, s64 = v32[:, both].sum(axis=0), v64[:, both].sum(axis=0)
+    assert np.median(np.abs(s32 / s64 - 1)) < 1e-2
+    m32, m64 = np.median(v32[:, both], axis=1), np.median(v64[:, both], axis=1)
+    np.testing.assert_allclose(m32[:3], m64[:3], atol=1e-2)
+    assert abs(m32[3] / m64[3] - 1) < 2e-2
+
+
 def test_fixed_swap_and_min_max(eng):
     c = hyper_case(sweep_over_var_2=True, var_sweep_index_2=0, param_lo_2=-11.0, param_hi_2=-9.0)
     v, f, res = eng.run_ls2d(ls_request(c, ucb.LS_FIXED, precision=ucb.PREC_F64, mode=ucb.MODE_EXACT))

@@ -132,6 +132,119 @@ __device__ __forceinline__ int loop_probes(const S& s, numb* x, numb (*y)[UCB_NX
     return 1;
 }
 
+#if defined(UCB_LS_TANGENT) && defined(UCB_HAS_JVP) && !defined(UCB_EXACT)
+// Tangent-vector form of the fixed method (native FP32 builds): instead of N shadow
+// trajectories x + eps z, whose differences from x fall below FP32 resolution for small eps,
+// the N tangent vectors v' = J(x) v are advanced with x in one RK4 sweep (the stage sums
+// accumulated stage by stage), and the block's Gram-Schmidt, norms and log sums are FP64.
+__device__ __forceinline__ void ls_tangent_step(numb* x, numb (*V)[UCB_NX], const numb* a, numb h) {
+    const numb hh = h * (numb)0.5, h6 = h * (numb)(1.0 / 6.0), two = (numb)2;
+    numb k[UCB_NX], l[UCB_NX], xt[UCB_NX], sx[UCB_NX];
+    numb vt[UCB_NX][UCB_NX], sv[UCB_NX][UCB_NX];
+    ucb_rhs(x, a, k);
+#pragma unroll
+    for (int j = 0; j < UCB_NX; ++j) {
+        ucb_jvp(x, a, V[j], l);
+#pragma unroll
+        for (int i = 0; i < UCB_NX; ++i) {
+            sv[j][i] = l[i];
+            vt[j][i] = fma(hh, l[i], V[j][i]);
+        }
+    }
+#pragma unroll
+    for (int i = 0; i < UCB_NX; ++i) {
+        sx[i] = k[i];
+        xt[i] = fma(hh, k[i], x[i]);
+    }
+#pragma unroll
+    for (int stage = 2; stage <= 3; ++stage) {
+        const numb c = stage == 2 ? hh : h;
+        ucb_rhs(xt, a, k);
+#pragma unroll
+        for (int j = 0; j < UCB_NX; ++j) {
+            ucb_jvp(xt, a, vt[j], l);
+#pragma unroll
+            for (int i = 0; i < UCB_NX; ++i) {
+                sv[j][i] = fma(two, l[i], sv[j][i]);
+                vt[j][i] = fma(c, l[i], V[j][i]);
+            }
+        }
+#pragma unroll
+        for (int i = 0; i < UCB_NX; ++i) {
+            sx[i] = fma(two, k[i], sx[i]);
+            xt[i] = fma(c, k[i], x[i]);
+        }
+    }
+    ucb_rhs(xt, a, k);
+#pragma unroll
+    for (int j = 0; j < UCB_NX; ++j) {
+        ucb_jvp(xt, a, vt[j], l);
+#pragma unroll
+        for (int i = 0; i < UCB_NX; ++i) V[j][i] = fma(h6, sv[j][i] + l[i], V[j][i]);
+    }
+#pragma unroll
+    for (int i = 0; i < UCB_NX; ++i) x[i] = fma(h6, sx[i] + k[i], x[i]);
+}
+
+// Classical Gram-Schmidt of the rows of V in FP64 (the reference's gramSchmidtProcess
+// order): V becomes orthonormal (rounded to numb), dens[i] the norm of row i after
+// removing its projections on the earlier rows.
+__device__ __forceinline__ void gs_classical_f64(numb (*V)[UCB_NX], double* dens) {
+    double b[UCB_NX][UCB_NX];
+#pragma unroll
+    for (int i = 0; i < UCB_NX; ++i) {
+#pragma unroll
+        for (int l = 0; l < UCB_NX; ++l) b[i][l] = (double)V[i][l];
+#pragma unroll
+        for (int j = 0; j < i; ++j) {
+            double num = 0, den = 0;
+#pragma unroll
+            for (int l = 0; l < UCB_NX; ++l) {
+                num = fma((double)V[i][l], b[j][l], num);
+                den = fma(b[j][l], b[j][l], den);
+            }
+            const double frac = den == 0 ? 0 : num / den;
+#pragma unroll
+            for (int l = 0; l < UCB_NX; ++l) b[i][l] = fma(-frac, b[j][l], b[i][l]);
+        }
+    }
+#pragma unroll
+    for (int i = 0; i < UCB_NX; ++i) {
+        double den = 0;
+#pragma unroll
+        for (int l = 0; l < UCB_NX; ++l) den = fma(b[i][l], b[i][l], den);
+        den = sqrt(den);
+        const double inv = den == 0 ? 0 : 1.0 / den;
+#pragma unroll
+        for (int l = 0; l < UCB_NX; ++l) V[i][l] = (numb)(b[i][l] * inv);
+        dens[i] = den;
+    }
+}
+
+// NT-step block of x and the tangent vectors with the divergence test of loop_probes
+// (tangent vectors: non-finite only). 0 if anything diverged.
+__device__ __forceinline__ int loop_tangents(numb* x, numb (*V)[UCB_NX], const numb* a, numb h, long long iters,
+                                             numb maxValue, long long& ns) {
+    for (long long i0 = 0; i0 < iters; i0 += kCheckInterval) {
+        ls_tangent_step(x, V, a, h);
+        ns += UCB_NX + 1;
+        bool bad = diverged(x, maxValue);
+#pragma unroll
+        for (int j = 0; j < UCB_NX; ++j) bad = bad || diverged(V[j], (numb)0);
+        if (bad) return 0;
+        const long long n = (iters - i0 < kCheckInterval) ? iters - i0 : kCheckInterval;
+        for (long long i = 1; i < n; ++i) ls_tangent_step(x, V, a, h);
+        ns += (long long)(UCB_NX + 1) * (n - 1);
+    }
+#if UCB_EXTRA_STEP
+    ls_tangent_step(x, V, a, h);
+    ns += UCB_NX + 1;
+#endif
+    return 1;
+}
+#define UCB_LS_FIXED_TANGENT 1
+#endif
+
 __device__ __forceinline__ void ls_cell_fixed(const UcbLsParams& p, long long kidx, long long& ns) {
     double outv[UCB_NX];
     const CellAxes c = cell_axes(kidx, p.n_pts);
@@ -183,6 +296,31 @@ __device__ __forceinline__ void ls_cell_fixed(const UcbLsParams& p, long long ki
         ls_store(p, kidx, outv);
         return;
     }
+#if defined(UCB_LS_FIXED_TANGENT)
+    {
+        double d[UCB_NX], sum[UCB_NX];
+        gs_classical_f64(z, d);  // the same random start, orthonormal
+#pragma unroll
+        for (int k = 0; k < UCB_NX; ++k) sum[k] = 0.0;
+        for (int b = 0; b < p.n_blocks; ++b) {
+            if (loop_tangents(x, z, a, h, nt, p.maxv, ns) == 0) {
+#pragma unroll
+                for (int m = 0; m < UCB_NX; ++m) outv[m] = 999.0;
+                ls_store(p, kidx, outv);
+                return;
+            }
+            gs_classical_f64(z, d);
+#pragma unroll
+            for (int k = 0; k < UCB_NX; ++k) sum[k] += log(d[k]);
+        }
+        (void)y;
+        (void)dens;
+#pragma unroll
+        for (int k = 0; k < UCB_NX; ++k) result[k] = sum[k] / (double)p.tmax;
+        ls_store(p, kidx, result);
+        return;
+    }
+#endif
     gram_schmidt_classical(z, y, nullptr);
 #pragma unroll
     for (int j = 0; j < UCB_NX; ++j)

@@ -55,13 +55,18 @@ ucb_lle2d_request as_lle(const ucb_ls2d_request& q) {
 CompileRequest ls_compile_request(const ucb_ls2d_request& q, const SweepMap& m, SystemCode& sys) {
     const bool dp5 = q.method == UCB_LS_DP5;
     const int prec = q.opt.precision;
-    sys = make_system_code(q.krs_body, q.amount_of_x, q.n_values, prec, dp5 ? UCB_MODE_NATIVE : q.opt.mode, dp5);
+    // the native FP32 form of the fixed method follows tangent vectors (v' = J(x) v) instead
+    // of FP32 shadow trajectories, whose differences from x vanish below FP32 resolution
+    const bool tangent = !dp5 && prec == UCB_PREC_F32 && q.opt.mode == UCB_MODE_NATIVE;
+    sys = make_system_code(q.krs_body, q.amount_of_x, q.n_values, prec, dp5 ? UCB_MODE_NATIVE : q.opt.mode,
+                           dp5 || tangent);
     CompileRequest rq;
     rq.name = "ucb_ls2d.cu";
     // DP5 keeps the clock from its FP64 time; the fixed method steps N + 1 trajectories on
     // one Stepper, so it has no compensated clock
     std::vector<std::string> defs = dp5 ? clock_defines(sys) : std::vector<std::string>{};
     defs.push_back(dp5 ? "UCB_LS_DP5 1" : "UCB_LS_FIXED 1");
+    if (tangent && sys.has_jvp) defs.push_back("UCB_LS_TANGENT 1");
     defs.push_back(prec == UCB_PREC_F64 ? "UCB_GS_BUDGET 20.0" : "UCB_GS_BUDGET 8.0");
     rq.source = make_prelude(prec, q.amount_of_x, q.n_values, m, q.opt.nominal_steps == 0, sys, defs) +
                 "#include \"ucb_device.cuh\"\n#include \"ucb_ls.cuh\"\n";
