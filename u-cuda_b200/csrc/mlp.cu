@@ -173,17 +173,29 @@ constexpr float kGeluC0 = 0.7978845608028654f;  // sqrt(2 / pi)
 constexpr float kGeluC1 = 0.044715f;
 // Two GELUs in packed FP32 pairs (fma / mul .f32x2: half the FP32 issue slots), the form
 // both training and prediction use: h + h tanh(c0 (z + c1 z^3)) with h = z / 2.
+constexpr float kGeluC01 = kGeluC0 * kGeluC1;
+// tanh's argument c0 (z + c1 z^3) as z (c0 + c0 c1 z^2): two packed operations.
+__device__ __forceinline__ float2 gelu_arg2(float2 z) {
+    return __fmul2_rn(__ffma2_rn(__fmul2_rn(z, z), make_float2(kGeluC01, kGeluC01), make_float2(kGeluC0, kGeluC0)),
+                      z);
+}
 __device__ __forceinline__ float2 gelu2(float2 z) {
-    const float2 z2 = __fmul2_rn(z, z);
-    const float2 u = __ffma2_rn(__fmul2_rn(z2, make_float2(kGeluC1, kGeluC1)), z, z);
-    const float2 w = __fmul2_rn(u, make_float2(kGeluC0, kGeluC0));
+    const float2 w = gelu_arg2(z);
     const float2 t = make_float2(tanh_hw(w.x), tanh_hw(w.y));
     const float2 h = __fmul2_rn(z, make_float2(0.5f, 0.5f));
     return __ffma2_rn(h, t, h);
 }
+// 2 gelu(z) = z + z tanh(w), one packed operation fewer than gelu2. Scaling by two commutes
+// with every rounding on the way (the BF16 packing and the FP32 accumulation of the next
+// layer's MMA), so a consumer that multiplies by 0.5 sees the bits gelu2 would have given.
+__device__ __forceinline__ float2 gelu2_twice(float2 z) {
+    const float2 w = gelu_arg2(z);
+    const float2 t = make_float2(tanh_hw(w.x), tanh_hw(w.y));
+    return __ffma2_rn(z, t, z);
+}
 __device__ __forceinline__ float gelu_grad(float z) {
     const float z2 = z * z;
-    const float t = tanh_hw(kGeluC0 * fmaf(kGeluC1 * z2, z, z));
+    const float t = tanh_hw(z * fmaf(kGeluC01, z2, kGeluC0));
     return 0.5f * (1.0f + t) + 0.5f * z * (1.0f - t * t) * kGeluC0 * fmaf(3.0f * kGeluC1, z2, 1.0f);
 }
 
@@ -1186,6 +1198,10 @@ __global__ void __launch_bounds__(kInferThreads, 1)
                         // bias + GELU -> BF16 activations of layer l + 1, over this slot's buffer
                         const uint32_t act = smem_u32(base + s * Cfg::kActBytes);
                         const float4* b4 = reinterpret_cast<const float4*>(a.params + a.b_off[l]);
+                        // hidden activations are stored doubled (gelu2_twice): layers after the
+                        // first take half their accumulator
+                        const float in_scale = l == 0 ? 1.0f : 0.5f;
+                        const float2 sc = make_float2(in_scale, in_scale);
 #pragma unroll 1
                         for (int c0 = part * (H / 4); c0 < (part + 1) * (H / 4); c0 += 32) {
                             uint32_t rv[32];
@@ -1194,11 +1210,11 @@ __global__ void __launch_bounds__(kInferThreads, 1)
 #pragma unroll
                             for (int q = 0; q < 8; ++q) {
                                 const float4 b = __ldg(b4 + c0 / 4 + q);
-                                const float2 g0 = gelu2(__fadd2_rn(
-                                    make_float2(__uint_as_float(rv[4 * q]), __uint_as_float(rv[4 * q + 1])),
+                                const float2 g0 = gelu2_twice(__ffma2_rn(
+                                    make_float2(__uint_as_float(rv[4 * q]), __uint_as_float(rv[4 * q + 1])), sc,
                                     make_float2(b.x, b.y)));
-                                const float2 g1 = gelu2(__fadd2_rn(
-                                    make_float2(__uint_as_float(rv[4 * q + 2]), __uint_as_float(rv[4 * q + 3])),
+                                const float2 g1 = gelu2_twice(__ffma2_rn(
+                                    make_float2(__uint_as_float(rv[4 * q + 2]), __uint_as_float(rv[4 * q + 3])), sc,
                                     make_float2(b.z, b.w)));
                                 pk[2 * q] = pack_bf16x2(g0.x, g0.y);
                                 pk[2 * q + 1] = pack_bf16x2(g1.x, g1.y);
@@ -1218,8 +1234,8 @@ __global__ void __launch_bounds__(kInferThreads, 1)
                                          : "r"(tq));
                             asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
                             const float* bo = a.params + a.b_off[L];
-                            const float mu = __uint_as_float(o0) + __ldg(bo);
-                            const float lv = __uint_as_float(o1) + __ldg(bo + 1);
+                            const float mu = __fmaf_rn(__uint_as_float(o0), 0.5f, __ldg(bo));
+                            const float lv = __fmaf_rn(__uint_as_float(o1), 0.5f, __ldg(bo + 1));
                             const long long row = t * kBM + r;
                             if (row < a.n) {
                                 a.mean[row] = __fmaf_rn(mu, a.y_std, a.y_mean);
