@@ -683,11 +683,14 @@ __device__ __forceinline__ void input_point(const FeatureArgs& a, long long i, f
     input_point(a.u, a.cells, a.grid_n, i, u0, u1);
 }
 
-// Phase 2 pi (u0 B[2j] + u1 B[2j+1]) of frequency j, rounded in one fixed order (no
-// contraction left to the compiler), so that the training batches and the fused prediction
-// see the same features.
-__device__ __forceinline__ float feature_phase(float u0, float u1, const float* Bf, int j) {
-    return __fmul_rn(6.283185307179586f, __fmaf_rn(u0, __ldg(Bf + 2 * j), __fmul_rn(u1, __ldg(Bf + 2 * j + 1))));
+// sin and cos of the phase 2 pi (u0 B[2j] + u1 B[2j+1]) of frequency j. The phase in turns
+// is reduced to [-1/2, 1/2] exactly (x - rint(x)); the hardware sine and cosine on [-pi, pi]
+// then err by less than 2^-21, far below the BF16 resolution the features are stored in.
+// Every step rounds in one fixed order (no contraction left to the compiler), so the
+// training batches and the fused prediction see the same features.
+__device__ __forceinline__ void feature_sincos(float u0, float u1, const float* Bf, int j, float& s, float& c) {
+    const float x = __fmaf_rn(u0, __ldg(Bf + 2 * j), __fmul_rn(u1, __ldg(Bf + 2 * j + 1)));
+    __sincosf(__fmul_rn(6.283185307179586f, __fsub_rn(x, rintf(x))), &s, &c);
 }
 
 // X[r, j] = sin(2 pi u.B_j), X[r, fourier + j] = cos(...). One thread per (row, group of
@@ -717,7 +720,7 @@ __global__ void features_kernel(FeatureArgs a) {
 #pragma unroll
     for (int q = 0; q < 8; ++q) {
         sv[q] = cv[q] = 0.f;
-        if (valid) sincosf(feature_phase(u0, u1, a.Bf, j0 + q), &sv[q], &cv[q]);
+        if (valid) feature_sincos(u0, u1, a.Bf, j0 + q, sv[q], cv[q]);
     }
     const int F = 2 * a.fourier;
     uint4 ps, pc;
@@ -1165,8 +1168,8 @@ __global__ void __launch_bounds__(kInferThreads, 1)
                 for (int q = 0; q < 4; ++q) {
                     float s0 = 0.f, c0 = 0.f, s1 = 0.f, c1 = 0.f;
                     if (valid) {
-                        sincosf(feature_phase(u0, u1, a.Bf, j0 + 2 * q), &s0, &c0);
-                        sincosf(feature_phase(u0, u1, a.Bf, j0 + 2 * q + 1), &s1, &c1);
+                        feature_sincos(u0, u1, a.Bf, j0 + 2 * q, s0, c0);
+                        feature_sincos(u0, u1, a.Bf, j0 + 2 * q + 1, s1, c1);
                     }
                     ps[q] = pack_bf16x2(s0, s1);
                     pc[q] = pack_bf16x2(c0, c1);
