@@ -96,6 +96,18 @@ def test_fixed_fp32_tangent_against_fp64_on_the_hyperchaotic_window(eng):
     assert abs(m32[3] / m64[3] - 1) < 2e-2
 
 
+def test_fixed_fp32_tangent_flags_escaping_cells_like_fp64(eng):
+    """On the wide hyper-chaotic window at t_max 30 about a third of the cells escape to
+    max_value (47 of 144 in the oracle). The FP32 tangent form flags the same cells as the
+    FP64 form, but for a few near the escape boundary, and its bounded cells are finite."""
+    c = hyper_case(n=12, t_max=30.0)
+    v64, f64, _ = eng.run_ls2d(ls_request(c, ucb.LS_FIXED, precision=ucb.PREC_F64, mode=ucb.MODE_NATIVE))
+    v32, f32, _ = eng.run_ls2d(ls_request(c, ucb.LS_FIXED, precision=ucb.PREC_F32, mode=ucb.MODE_NATIVE))
+    assert (f64 != 1).sum() >= 30
+    assert (f32 == f64).mean() >= 0.95
+    assert np.isfinite(v32[:, f32 == 1]).all()
+
+
 def test_fixed_swap_and_min_max(eng):
     c = hyper_case(sweep_over_var_2=True, var_sweep_index_2=0, param_lo_2=-11.0, param_hi_2=-9.0)
     v, f, res = eng.run_ls2d(ls_request(c, ucb.LS_FIXED, precision=ucb.PREC_F64, mode=ucb.MODE_EXACT))
