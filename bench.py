@@ -770,9 +770,9 @@ def main():
                     help=f"comma-separated subset of {','.join(OTHER_CONFIGS)} to time (instead of --all-configs)")
     ap.add_argument("--mlp-rows", type=int, default=1 << 20,
                     help="rows of the surrogate-network prediction timing (the MLP line of the JSON)")
-    ap.add_argument("--surrogate-chen", type=int, default=2048, metavar="N",
-                    help="grid of the surrogate-refined Chen map (default 2048, a bounded run; the configuration's "
-                         "own grid is 8192; 0 = skip)")
+    ap.add_argument("--surrogate-chen", type=int, default=8192, metavar="N",
+                    help="grid of the surrogate-refined Chen map (default 8192, the configuration's own grid: about "
+                         "90 s for both tolerances; 2048 is a shorter stand-in; 0 = skip)")
     args = ap.parse_args()
     rank, world, local = dist_env()
     cfg = {"workload": f"Rossler LLE map {args.n}x{args.n} (b in [0.05,2] x c in [2,20], a=0.2), RK4 h=0.01, "
