@@ -837,19 +837,21 @@ def main():
             print(json.dumps(out))
         return
     results, clocks, launches, e2e_ms = run_ours(args, rank, world, local)
-    surrogate_chen = None
-    other_configs = run_other_configs(ucb.Engine(local), which, args) if which and rank == 0 else None
-    if args.surrogate_chen and rank == 0:
-        surrogate_chen = [run_surrogate_chen(ucb.Engine(local), torch.device("cuda", local), args.surrogate_chen,
-                                             tol, cov) for tol, cov in ((2e-3, 0.995), (2e-2, 0.99))]
-    mlp = run_mlp(ucb.Engine(local), args.mlp_rows) if rank == 0 else None
-    peak64 = ucb.measure_fma_peak(ucb.PREC_F64)
-    peak32 = ucb.measure_fma_peak(ucb.PREC_F32)
+    # The collective part ends here: the other ranks leave before rank 0 runs the single-GPU
+    # legs below (minutes of work that a waiting rank's process-group timeout would not cover).
     if world > 1:
         dist.barrier()
         dist.destroy_process_group()
     if rank != 0:
         return
+    surrogate_chen = None
+    other_configs = run_other_configs(ucb.Engine(local), which, args) if which else None
+    if args.surrogate_chen:
+        surrogate_chen = [run_surrogate_chen(ucb.Engine(local), torch.device("cuda", local), args.surrogate_chen,
+                                             tol, cov) for tol, cov in ((2e-3, 0.995), (2e-2, 0.99))]
+    mlp = run_mlp(ucb.Engine(local), args.mlp_rows)
+    peak64 = ucb.measure_fma_peak(ucb.PREC_F64)
+    peak32 = ucb.measure_fma_peak(ucb.PREC_F32)
     cells = args.n * args.n
     r32, r64 = results["fp32"], results["plain_fp64"]
     value = aggregate_rate(world, cells, r32["ms"])
